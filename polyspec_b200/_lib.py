@@ -1,0 +1,70 @@
+"""ctypes binding of libpscuda.so (the C ABI declared in include/pscuda.h).
+
+The library is built in-tree by ``python -m polyspec_b200.build`` (or
+``__graft_entry__.build()``).  There is no CPU fallback: if the library is
+missing or cannot be loaded, importing the CUDA backend raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpscuda.so")
+
+PS_OK = 0
+PS_ERR_NOT_CONVERGED = -6
+PS_PREC_FP64 = 0
+PS_PREC_MIXED = 1
+
+_c_int, _c_int64, _c_double, _c_size_t, _c_void_p = (ctypes.c_int, ctypes.c_int64, ctypes.c_double,
+                                                      ctypes.c_size_t, ctypes.c_void_p)
+
+# name -> (restype, argtypes); every entry point declared in include/pscuda.h
+SIGNATURES = {
+    "ps_error_string": (ctypes.c_char_p, [_c_int]),
+    "ps_version": (_c_int, []),
+    "ps_device_sm_count": (_c_int, [ctypes.POINTER(_c_int)]),
+    "ps_plan_create": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_c_void_p)]),
+    "ps_plan_destroy": (_c_int, [_c_void_p]),
+    "ps_plan_info": (_c_int, [_c_void_p, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int),
+                              ctypes.POINTER(_c_int64), ctypes.POINTER(_c_int64)]),
+    "ps_sht_workspace_bytes": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, ctypes.POINTER(_c_size_t)]),
+    "ps_synthesis": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p, _c_size_t,
+                              _c_void_p]),
+    "ps_adjoint": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_double, _c_void_p,
+                            _c_size_t, _c_void_p]),
+}
+
+_lib = None
+
+
+class PSError(RuntimeError):
+    def __init__(self, func, code):
+        msg = lib().ps_error_string(code).decode() if _lib is not None else str(code)
+        super().__init__("%s failed: %s (%d)" % (func, msg, code))
+        self.code = code
+
+
+def lib():
+    """Load libpscuda.so (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libpscuda.so is not built: run `python -m polyspec_b200.build` "
+                          "(the CUDA backend has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(func, code):
+    if code != PS_OK:
+        raise PSError(func, code)
+    return code
+
+
+def call(name, *args):
+    return check(name, getattr(lib(), name)(*args))

@@ -1,0 +1,359 @@
+// Plans and the SHT entry points of the C ABI (include/pscuda.h).
+//
+// A plan holds the read-only tables of one (nside, lmax) geometry: the
+// HEALPix RING table, the Legendre seed normalisations, the FFT twiddles,
+// the Bluestein chirp spectra and the grouping of rings into FFT length
+// classes.  Everything else (transposed alm, the ring/order "phase" array,
+// the adjoint's per-tile partial sums) lives in caller-owned workspace.
+#include <vector>
+#include <complex>
+#include <map>
+#include <algorithm>
+#include <new>
+
+#include "ps_common.cuh"
+
+namespace ps {
+int launch_legendre_synth_f64(const Plan& P, const double2* almT, double2* phase, int B, int spin, cudaStream_t st);
+int launch_legendre_adjoint_f64(const Plan& P, const double2* phase, double2* partial, int B, int spin,
+                                cudaStream_t st);
+int adjoint_tiles(const Plan& P);
+int launch_alm_to_T(const double2* alm, double2* almT, int B, int ncomp, int64_t nalm, int sms, cudaStream_t st);
+int launch_reduce_partials(const double2* partial, double2* alm, int ntiles, int B, int ncomp, int64_t nalm,
+                           double scale, int sms, cudaStream_t st);
+int launch_ring_synth_f64(const Plan& P, const int* d_list, int nrings, int work_len, const double2* phase,
+                          double* map, int nf, cudaStream_t st);
+int launch_ring_adjoint_f64(const Plan& P, const int* d_list, int nrings, int work_len, const double* map,
+                            double2* phase, int nf, cudaStream_t st);
+}  // namespace ps
+
+struct ps_plan {
+  ps::Plan p;
+  // FFT length classes: rings with the same work length share a launch
+  std::vector<int> cls_len, cls_off, cls_cnt;
+  int* d_ring_lists = nullptr;
+  std::vector<void*> owned;  // device allocations to free
+};
+
+namespace {
+
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+int next_pow2(int n) { int m = 1; while (m < n) m <<= 1; return m; }
+
+// host radix-2 FFT (sign -1), natural order in and out; used once per plan to
+// build the Bluestein kernel spectra
+void host_fft(std::vector<std::complex<double>>& a) {
+  const int n = (int)a.size();
+  for (int i = 1, j = 0; i < n; ++i) {
+    int bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  for (int len = 2; len <= n; len <<= 1) {
+    for (int j = 0; j < len / 2; ++j) {
+      const double ang = -2.0 * M_PI * double(j) / double(len);
+      const std::complex<double> w(std::cos(ang), std::sin(ang));
+      for (int i = 0; i < n; i += len) {
+        const std::complex<double> u = a[i + j], v = a[i + j + len / 2] * w;
+        a[i + j] = u + v;
+        a[i + j + len / 2] = u - v;
+      }
+    }
+  }
+}
+
+int host_bitrev(int i, int logn) {
+  int r = 0;
+  for (int b = 0; b < logn; ++b) { r = (r << 1) | (i & 1); i >>= 1; }
+  return r;
+}
+
+template <class T>
+T* dev_upload(ps_plan* pl, const std::vector<T>& v, int& err) {
+  if (v.empty()) return nullptr;
+  void* d = nullptr;
+  if (cudaMalloc(&d, v.size() * sizeof(T)) != cudaSuccess) { err = PS_ERR_NOMEM; return nullptr; }
+  pl->owned.push_back(d);
+  if (cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) err = PS_ERR_CUDA;
+  return static_cast<T*>(d);
+}
+
+// sqrt of a Scaled value
+ps::Scaled ssqrt(ps::Scaled s) {
+  double v = s.v; int e = s.e;
+  if (e & 1) { v *= 2.0; e -= 1; }
+  ps::Scaled r = ps::snorm(std::sqrt(v));
+  r.e += e / 2;
+  return r;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+extern "C" {
+
+const char* ps_error_string(int code) {
+  switch (code) {
+    case PS_OK: return "ok";
+    case PS_ERR_INVALID: return "invalid argument";
+    case PS_ERR_UNSUPPORTED: return "unsupported configuration";
+    case PS_ERR_NOMEM: return "device allocation failed";
+    case PS_ERR_CUDA: return "CUDA runtime error";
+    case PS_ERR_WORKSPACE: return "workspace too small";
+    case PS_ERR_NOT_CONVERGED: return "solver did not converge";
+    default: return "unknown error";
+  }
+}
+
+int ps_version(void) { return 100; }
+
+int ps_device_sm_count(int* count) {
+  if (!count) return PS_ERR_INVALID;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return PS_ERR_CUDA;
+  if (cudaDeviceGetAttribute(count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return PS_ERR_CUDA;
+  return PS_OK;
+}
+
+int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_plan** out) {
+  if (!out) return PS_ERR_INVALID;
+  *out = nullptr;
+  if (nside < 1 || nside > 8192 || lmax < 0 || mmax != lmax || (prec != PS_PREC_FP64 && prec != PS_PREC_MIXED))
+    return PS_ERR_INVALID;
+  if (spin_mask & ~0xF) return PS_ERR_UNSUPPORTED;  // spins 0..3
+  ps_plan* pl = new (std::nothrow) ps_plan();
+  if (!pl) return PS_ERR_NOMEM;
+  ps::Plan& P = pl->p;
+  P.nside = nside; P.lmax = lmax; P.mmax = mmax; P.prec = prec; P.spin_mask = spin_mask | 1;
+  P.R = 4 * nside - 1; P.Rh = 2 * nside;
+  P.npix = 12 * int64_t(nside) * nside;
+  P.nalm = int64_t(lmax + 1) * (lmax + 2) / 2;
+  for (int s = 0; s < 4; ++s) P.d_seed[s] = nullptr;
+  if (ps_device_sm_count(&P.num_sms) != PS_OK) { delete pl; return PS_ERR_CUDA; }
+  int err = PS_OK;
+
+  // ---- ring table (HEALPix RING, Gorski et al. 2005)
+  std::vector<ps::RingInfo> rings(P.R);
+  std::map<int, int> bs_slot;  // nphi -> slot
+  std::vector<int> bs_n;
+  const int64_t ns = nside;
+  for (int ir = 0; ir < P.R; ++ir) {
+    const int64_t i = ir + 1;
+    const bool north = i <= 2 * ns;
+    const int64_t ii = north ? i : 4 * ns - i;
+    ps::RingInfo g{};
+    if (ii < ns) {
+      const double t = double(ii * ii) / (3.0 * double(ns * ns));
+      g.z = north ? 1.0 - t : t - 1.0;
+      g.omz = north ? t : 2.0 - t;
+      g.opz = north ? 2.0 - t : t;
+      g.sth = std::sqrt(t * (2.0 - t));
+      g.nphi = int(4 * ii);
+      g.phi_num = 1; g.phi_den = int(4 * ii);
+      g.start = north ? 2 * ii * (ii - 1) : P.npix - 2 * ii * (ii + 1);
+    } else {
+      const double z = double(2 * ns - i) * 2.0 / (3.0 * double(ns));
+      g.z = z; g.omz = 1.0 - z; g.opz = 1.0 + z;
+      g.sth = std::sqrt(g.omz * g.opz);
+      g.nphi = int(4 * ns);
+      g.phi_num = ((i - ns) % 2 == 0) ? 1 : 0;
+      g.phi_den = int(4 * ns);
+      g.start = 2 * ns * (ns - 1) + (i - ns) * 4 * ns;
+    }
+    if (is_pow2(g.nphi)) { g.bs_slot = -1; g.bs_m = 0; }
+    else {
+      auto it = bs_slot.find(g.nphi);
+      if (it == bs_slot.end()) { it = bs_slot.emplace(g.nphi, (int)bs_n.size()).first; bs_n.push_back(g.nphi); }
+      g.bs_slot = it->second;
+      g.bs_m = next_pow2(2 * g.nphi - 1);
+    }
+    rings[ir] = g;
+  }
+
+  // ---- FFT classes and twiddles
+  std::map<int, std::vector<int>> classes;
+  int max_fft = 2;
+  for (int ir = 0; ir < P.R; ++ir) {
+    const int w = rings[ir].bs_slot >= 0 ? rings[ir].bs_m : rings[ir].nphi;
+    classes[w].push_back(ir);
+    max_fft = std::max(max_fft, w);
+  }
+  P.max_fft = max_fft;
+  if (prec == PS_PREC_FP64) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (size_t(max_fft) * sizeof(double2) > size_t(optin)) { delete pl; return PS_ERR_UNSUPPORTED; }
+  }
+  std::vector<int> lists;
+  for (auto& kv : classes) {
+    pl->cls_len.push_back(kv.first);
+    pl->cls_off.push_back((int)lists.size());
+    pl->cls_cnt.push_back((int)kv.second.size());
+    // largest rings first inside a class does not matter: all have equal work
+    lists.insert(lists.end(), kv.second.begin(), kv.second.end());
+  }
+  std::vector<double2> tw(max_fft / 2);
+  for (int k = 0; k < max_fft / 2; ++k) {
+    const double ang = -2.0 * M_PI * double(k) / double(max_fft);
+    tw[k] = make_double2(std::cos(ang), std::sin(ang));
+  }
+  // ---- Bluestein spectra: b_n = e^{+i pi n^2 / N}, |n| < N, wrapped to M; FFT_M, bit-reversed order
+  std::vector<double2> bs_spec;
+  std::vector<int64_t> bs_off;
+  for (int N : bs_n) {
+    const int M = next_pow2(2 * N - 1);
+    int logM = 0; while ((1 << logM) < M) ++logM;
+    std::vector<std::complex<double>> b(M, 0.0);
+    for (int n = 0; n < N; ++n) {
+      const int64_t q = (int64_t(n) * n) % (2 * int64_t(N));
+      const double ang = M_PI * double(q) / double(N);
+      const std::complex<double> v(std::cos(ang), std::sin(ang));
+      b[n] = v;
+      if (n > 0) b[M - n] = v;
+    }
+    host_fft(b);
+    bs_off.push_back((int64_t)bs_spec.size());
+    const size_t o = bs_spec.size();
+    bs_spec.resize(o + M);
+    for (int p = 0; p < M; ++p) {
+      const std::complex<double> v = b[host_bitrev(p, logM)];
+      bs_spec[o + p] = make_double2(v.real(), v.imag());
+    }
+  }
+  P.n_bs_slots = (int)bs_n.size();
+  P.bs_total = (int64_t)bs_spec.size();
+
+  // ---- Legendre seed normalisations
+  std::vector<double> mnorm(mmax + 1);
+  {
+    double p = 1.0;
+    for (int m = 0; m <= mmax; ++m) {
+      if (m > 0) p *= (2.0 * m - 1.0) / (2.0 * m);
+      mnorm[m] = std::sqrt((2.0 * m + 1.0) / (4.0 * M_PI) * p);
+    }
+  }
+  std::vector<ps::SeedNorm> seeds[4];
+  for (int s = 1; s <= 3; ++s) {
+    if (!((spin_mask >> s) & 1)) continue;
+    seeds[s].resize(mmax + 1);
+    // C(2m, m+s) for m >= s, incrementally; C(2s, s+m) for m < s directly
+    ps::Scaled binom = ps::snorm(1.0);
+    for (int m = 0; m <= mmax; ++m) {
+      ps::Scaled nrm;
+      if (m < s) {
+        ps::Scaled c = ps::snorm(1.0);
+        for (int j = 1; j <= s - m; ++j) c = ps::smul(c, ps::snorm(double(s + m + j) / double(j)));
+        nrm = ps::smul(c, ps::snorm((2.0 * s + 1.0) / (4.0 * M_PI)));
+      } else {
+        if (m > s)
+          binom = ps::smul(binom, ps::snorm((2.0 * m) * (2.0 * m - 1.0) / (double(m + s) * double(m - s))));
+        nrm = ps::smul(binom, ps::snorm((2.0 * m + 1.0) / (4.0 * M_PI)));
+      }
+      ps::Scaled r = ssqrt(nrm);
+      seeds[s][m].v = r.v; seeds[s][m].e = r.e; seeds[s][m].pad = 0;
+    }
+  }
+
+  P.d_rings = dev_upload(pl, rings, err);
+  P.d_mnorm0 = dev_upload(pl, mnorm, err);
+  for (int s = 1; s <= 3; ++s) if (!seeds[s].empty()) P.d_seed[s] = dev_upload(pl, seeds[s], err);
+  P.d_twiddle = dev_upload(pl, tw, err);
+  P.d_bs_spec = dev_upload(pl, bs_spec, err);
+  P.d_bs_off = dev_upload(pl, bs_off, err);
+  pl->d_ring_lists = dev_upload(pl, lists, err);
+  if (err != PS_OK) { ps_plan_destroy(pl); return err; }
+  *out = pl;
+  return PS_OK;
+}
+
+int ps_plan_destroy(ps_plan* plan) {
+  if (!plan) return PS_ERR_INVALID;
+  for (void* d : plan->owned) cudaFree(d);
+  delete plan;
+  return PS_OK;
+}
+
+int ps_plan_info(const ps_plan* plan, int* nside, int* lmax, int64_t* npix, int64_t* nalm) {
+  if (!plan) return PS_ERR_INVALID;
+  if (nside) *nside = plan->p.nside;
+  if (lmax) *lmax = plan->p.lmax;
+  if (npix) *npix = plan->p.npix;
+  if (nalm) *nalm = plan->p.nalm;
+  return PS_OK;
+}
+
+static size_t sht_ws_bytes(const ps::Plan& P, int batch, int spin, int adjoint) {
+  const size_t nf = size_t(batch) * (spin == 0 ? 1 : 2);
+  const size_t phase = align256(size_t(P.R) * (P.mmax + 1) * nf * sizeof(double2));
+  if (!adjoint) return align256(size_t(P.nalm) * nf * sizeof(double2)) + phase;
+  return phase + align256(size_t(ps::adjoint_tiles(P)) * P.nalm * nf * sizeof(double2));
+}
+
+int ps_sht_workspace_bytes(const ps_plan* plan, int batch, int spin, int adjoint, size_t* bytes) {
+  if (!plan || !bytes || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  *bytes = sht_ws_bytes(plan->p, batch, spin, adjoint);
+  return PS_OK;
+}
+
+int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch, int spin, void* workspace,
+                 size_t workspace_bytes, cudaStream_t stream) {
+  if (!plan || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  if (batch == 0) return PS_OK;
+  if (!alm || !map || !workspace) return PS_ERR_INVALID;
+  const ps::Plan& P = plan->p;
+  if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
+  if (P.prec != PS_PREC_FP64) return PS_ERR_UNSUPPORTED;
+  if (workspace_bytes < sht_ws_bytes(P, batch, spin, 0)) return PS_ERR_WORKSPACE;
+  const int ncomp = spin == 0 ? 1 : 2;
+  const int nf = batch * ncomp;
+  char* ws = static_cast<char*>(workspace);
+  double2* almT = reinterpret_cast<double2*>(ws);
+  double2* phase = reinterpret_cast<double2*>(ws + align256(size_t(P.nalm) * nf * sizeof(double2)));
+  int rc;
+  if (nf == 1) {
+    almT = reinterpret_cast<double2*>(const_cast<double*>(alm));
+  } else {
+    rc = ps::launch_alm_to_T(reinterpret_cast<const double2*>(alm), almT, batch, ncomp, P.nalm, P.num_sms, stream);
+    if (rc) return rc;
+  }
+  rc = ps::launch_legendre_synth_f64(P, almT, phase, batch, spin, stream);
+  if (rc) return rc;
+  for (size_t c = 0; c < plan->cls_len.size(); ++c) {
+    rc = ps::launch_ring_synth_f64(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c], plan->cls_len[c],
+                                   phase, map, nf, stream);
+    if (rc) return rc;
+  }
+  return PS_OK;
+}
+
+int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, int spin, double scale,
+               void* workspace, size_t workspace_bytes, cudaStream_t stream) {
+  if (!plan || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  if (batch == 0) return PS_OK;
+  if (!alm || !map || !workspace) return PS_ERR_INVALID;
+  const ps::Plan& P = plan->p;
+  if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
+  if (P.prec != PS_PREC_FP64) return PS_ERR_UNSUPPORTED;
+  if (workspace_bytes < sht_ws_bytes(P, batch, spin, 1)) return PS_ERR_WORKSPACE;
+  const int ncomp = spin == 0 ? 1 : 2;
+  const int nf = batch * ncomp;
+  char* ws = static_cast<char*>(workspace);
+  const size_t phase_bytes = align256(size_t(P.R) * (P.mmax + 1) * nf * sizeof(double2));
+  double2* phase = reinterpret_cast<double2*>(ws);
+  double2* partial = reinterpret_cast<double2*>(ws + phase_bytes);
+  int rc;
+  for (size_t c = 0; c < plan->cls_len.size(); ++c) {
+    rc = ps::launch_ring_adjoint_f64(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c], plan->cls_len[c],
+                                     map, phase, nf, stream);
+    if (rc) return rc;
+  }
+  rc = ps::launch_legendre_adjoint_f64(P, phase, partial, batch, spin, stream);
+  if (rc) return rc;
+  return ps::launch_reduce_partials(partial, reinterpret_cast<double2*>(alm), ps::adjoint_tiles(P), batch, ncomp,
+                                    P.nalm, scale, P.num_sms, stream);
+}
+
+}  // extern "C"
