@@ -1,0 +1,269 @@
+"""S^-1 weighting on the GPU (mirror of polyspec/weighting.py).
+
+``Weightings(base, mask, Cl_raw, noise_cov=None, inpainting_mask=None)``
+builds the same quantities as the reference (polyspec/weighting.py:6-85):
+the inverse noise covariance, the isotropic noise level ``Nl_iso``, the
+signal covariance and its inverse per (l, m) and the harmonic preconditioner
+``Sigmalm``; ``applySinv_ideal`` and ``applySinv_optimal`` keep their
+signatures and return harmonic coefficients truncated at ``lmax``.
+
+All arrays live on the GPU; the transforms are libpscuda SHTs.  numpy inputs
+give numpy outputs; CUDA-tensor inputs give CUDA-tensor outputs.
+``CGD`` is the reference's preconditioned conjugate-gradient solver
+(polyspec/weighting.py:217-367) with vectors, dot products and the A and M
+operators evaluated on the device.
+"""
+import numpy as np
+import torch
+
+
+def _per_lm(base, mat_l):
+    """Per-l matrices [a, b, lmax+1] -> complex device tensor [a, b, nlm] (indexed by base.l_arr)."""
+    t = torch.as_tensor(np.ascontiguousarray(mat_l), device=base.device)
+    return t[..., base.dev('l_arr')].to(torch.complex128).contiguous()
+
+
+class Weightings:
+    def __init__(self, base, mask, Cl_raw, noise_cov=None, inpainting_mask=None):
+        self.base = base
+        self.mask = mask
+        self.Cl_raw = Cl_raw
+        self.pol = self.base.pol
+        self.pixel_area = 4. * np.pi / (12 * self.base.Nside ** 2)
+        nf = 1 + 2 * self.pol
+        dev = base.device
+
+        if noise_cov is not None:
+            self.noise_cov = noise_cov
+            self.noise_icov = np.zeros_like(self.noise_cov)
+            self.noise_icov[self.noise_cov != 0] = 1. / self.noise_cov[self.noise_cov != 0]
+
+        if inpainting_mask is not None:
+            assert np.mean(inpainting_mask) == np.mean(inpainting_mask ** 2), "Inpainting mask should be a boolean array!"
+            self.inpainting_mask = inpainting_mask
+            if np.mean(1. * self.inpainting_mask) > 0.5:
+                print("## %.2f%% of the pixels will be inpainted: is this mask correct?" % (np.mean(1. * self.inpainting_mask) * 100))
+            if self.pol:
+                assert len(self.inpainting_mask) == 3, "Must supply one mask for each polarization!"
+            else:
+                if len(self.inpainting_mask) != 1:
+                    self.inpainting_mask = self.inpainting_mask.reshape(1, -1)
+
+        self.beam_lm = self.base.beam_lm
+        ls = np.arange(self.base.lmax + 1)
+
+        if hasattr(self, 'noise_cov'):
+            self.Nl_iso = np.zeros(nf)
+            for i in range(nf):
+                self.Nl_iso[i] = np.mean(self.noise_cov[i][np.asarray(self.mask)[i] > 0.99]) * self.pixel_area
+            # per-l signal covariance and its inverse (polyspec/weighting.py:52-73)
+            if self.pol:
+                assert len(Cl_raw.keys()) == 6 or len(Cl_raw.keys()) == 4, \
+                    "Must specify four or six input spectra: {ClTT, ClTE, ClEE, ClBB} or {ClTT, ClTE, ClTB, ClEE, ClEB, ClBB}"
+                if len(Cl_raw.keys()) == 4:
+                    Cl_raw['TB'] = Cl_raw['EB'] = 0. * Cl_raw['TT']
+                C = np.asarray([[Cl_raw['TT'][ls], Cl_raw['TE'][ls], Cl_raw['TB'][ls]],
+                                [Cl_raw['TE'][ls], Cl_raw['EE'][ls], Cl_raw['EB'][ls]],
+                                [Cl_raw['TB'][ls], Cl_raw['EB'][ls], Cl_raw['BB'][ls]]])  # [3,3,l]
+                Cl_l = np.moveaxis(C, 2, 0)  # [l,3,3]
+                inv_l = np.zeros((3, 3, len(ls)))
+                if np.sum(Cl_raw['BB']) == 0:
+                    good_l = np.linalg.det(Cl_l[:, :2, :2]) > 0
+                    inv_l[:2, :2, good_l] = np.moveaxis(np.linalg.inv(Cl_l[good_l, :2, :2]), 0, 2)
+                else:
+                    good_l = np.linalg.det(Cl_l) > 0
+                    inv_l[:, :, good_l] = np.moveaxis(np.linalg.inv(Cl_l[good_l]), 0, 2)
+            else:
+                Cl_l = Cl_raw['TT'][ls].reshape(-1, 1, 1)
+                good_l = Cl_l[:, 0, 0] > 0
+                inv_l = np.zeros((1, 1, len(ls)))
+                inv_l[:, :, good_l] = np.moveaxis(np.linalg.inv(Cl_l[good_l]), 0, 2)
+            self.Cl_l_mat = Cl_l            # [l, a, b]
+            self.inv_Cl_l_mat = inv_l       # [a, b, l]
+            # harmonic preconditioner (polyspec/weighting.py:76-78), per l
+            beam_l = self.base.beam[:, :len(ls)]
+            inv_S = inv_l + np.einsum('il,jl,ij->ijl', beam_l, beam_l, np.diag(1. / self.Nl_iso))
+            inv_S[:, :, :2] = inv_S[:, :, 2:3]
+            self.Sigma_l = np.moveaxis(np.linalg.inv(np.moveaxis(inv_S, 2, 0)), 0, 2)  # [a, b, l]
+            # device, per (l, m)
+            self.d_inv_Cl = _per_lm(base, self.inv_Cl_l_mat)
+            self.d_Sigma = _per_lm(base, self.Sigma_l)
+            self.d_noise_cov = torch.as_tensor(np.asarray(self.noise_cov, dtype=np.float64).reshape(nf, -1), device=dev)
+            self.d_noise_icov = torch.as_tensor(np.asarray(self.noise_icov, dtype=np.float64).reshape(nf, -1), device=dev)
+            # x0 operator C B C_tot^-1 (polyspec/weighting.py:174), per l
+            self.x0_l = np.einsum('lab,bl,bcl->acl', Cl_l, beam_l, self.base.inv_Cl_tot_mat[:, :, :len(ls)])
+            self.d_x0op = _per_lm(base, self.x0_l)
+
+        if not (type(mask) == float or type(mask) == int):
+            if len(mask) == 1 or len(mask) == 3:
+                assert len(mask[0]) == self.base.Npix, f'Mask has incorrect shape: {np.shape(mask)}'
+            else:
+                assert len(mask) == self.base.Npix, f'Mask has incorrect shape: {np.shape(mask)}'
+        m = np.asarray(mask, dtype=np.float64)
+        self.d_mask = torch.as_tensor(m.reshape(-1, self.base.Npix) if m.ndim else m, device=dev)
+        if hasattr(self, 'noise_cov'):
+            # W N^-1 W / A_pix  (the A_pix of to_lm cancels it: polyspec/weighting.py:277, :290)
+            self.d_WNW = (self.d_mask ** 2 * self.d_noise_icov).contiguous()
+
+    # ------------------------------------------------------------------
+    def inpaint_map(self, input_map, n_average=50):
+        """Neighbour-average inpainting (polyspec/weighting.py:87-146) is not part
+        of this build's GPU path."""
+        raise NotImplementedError("inpainting is not implemented in the CUDA backend")
+
+    def applySinv_optimal(self, input_map, preconditioner='pseudo_inverse', nstep=25, thresh=1e-4, verb=False,
+                          input_type='map', lmax=None):
+        """Optimal S^-1 by preconditioned CG from the ideal (Wiener) start
+        (polyspec/weighting.py:148-184).  Output in harmonic space, l <= lmax."""
+        assert input_type == 'map', "Optimal weighting should be applied only to pixel-space data!"
+        if not hasattr(self, 'noise_cov'):
+            raise Exception("The CGD solver requires a pixel-space noise covariance")
+        if lmax is None:
+            lmax = self.base.lmax
+        d, as_torch = self.base._in(input_map, torch.float64)
+        if hasattr(self, 'inpainting_mask'):
+            d = self.inpaint_map(d)
+        x0 = torch.einsum('abi,bi->ai', self.d_x0op, self.base.to_lm(d))
+        cgd = CGD(self, d, x0=x0, preconditioner=preconditioner, verb=verb)
+        cgd.run(nstep=nstep, thresh=thresh)
+        self.last_cgd = cgd
+        lfilt = torch.as_tensor(self.base.l_arr <= lmax, device=self.base.device)
+        return self.base._out(cgd.get_ivar_lm()[:, lfilt], as_torch)
+
+    def applySinv_ideal(self, input_map, input_type='map', lmax=None):
+        """Ideal S^-1 = beam C_tot^-1 Y^dagger W (polyspec/weighting.py:186-214)."""
+        if lmax is None:
+            lmax = self.base.lmax
+        lfilt = torch.as_tensor(self.base.l_arr <= lmax, device=self.base.device)
+        icov = self.base.dev('inv_Cl_tot_lm_mat')
+        beam = self.base.dev('beam_lm')
+        if input_type == 'harmonic':
+            assert np.mean(self.mask) == 1, "Harmonic-space S^-1 requires a unit mask!"
+            x, as_torch = self.base._in(input_map, torch.complex128)
+            out = beam[:, lfilt] * torch.einsum("abl,bl->al", icov[:, :, lfilt], x)
+            return self.base._out(out, as_torch)
+        x, as_torch = self.base._in(input_map, torch.float64)
+        if hasattr(self, 'inpainting_mask'):
+            x = self.inpaint_map(x)
+        input_lm = self.base.to_lm(x)
+        out = beam[:, lfilt] * torch.einsum("abl,bl->al", icov[:, :, lfilt], input_lm[:, lfilt])
+        return self.base._out(out, as_torch)
+
+
+class CGD:
+    """Preconditioned CG for A x = b, A = C^-1 + P^dagger N^-1 P, P = W Y B
+    (polyspec/weighting.py:217-367), on device tensors."""
+
+    def __init__(self, weightings, d, x0=[], test_b=[], preconditioner='pseudo_inverse', verb=False):
+        self.preconditioner = preconditioner
+        self.base = weightings.base
+        self.weightings = weightings
+        self.verb = verb
+        if len(test_b) == 0:
+            b0 = self._get_b(d.clone())
+        else:
+            print("Running in test mode!")
+            assert len(d) == 0, "Cannot specify both d and test_b!"
+            b0, _ = self.base._in(test_b, torch.complex128)
+            b0 = b0.clone()
+        if len(x0) != 0:
+            self.x0 = x0
+            b = b0 - self._apply_A(self.x0)
+        else:
+            self.x0 = 0.
+            b = b0
+        self.x = torch.zeros_like(b)
+        self.r = b.clone()
+        self.w = self.base.dev('m_weight')
+        z = self._apply_M(self.r)
+        self.rz = self.dot(self.r, z)
+        self.rz0 = float(self.dot(b0, self._apply_M(b0)))
+        self.p = z
+        self.i = 0
+        self.err = self.rz / self.rz0
+
+    def dot(self, a, b):
+        """m-weighted real inner product sum a b^* (1 + [m > 0]) (polyspec/weighting.py:255)."""
+        return float(torch.sum((a * b.conj()).real * self.w))
+
+    # filtering
+    def _apply_beam(self, ilm):
+        return ilm * self.base.dev('beam_lm')
+
+    def _apply_mask(self, imap):
+        return imap * self.weightings.d_mask
+
+    def _apply_Ninv(self, imap):
+        return imap * self.weightings.d_noise_icov / self.weightings.pixel_area
+
+    def _apply_Cinv(self, ilm):
+        return torch.einsum('abi,bi->ai', self.weightings.d_inv_Cl, ilm)
+
+    def _pointing(self, ilm):
+        return self._apply_mask(self.base.to_map(self._apply_beam(ilm)))
+
+    def _pointing_adjoint(self, imap):
+        return self._apply_beam(self.base.to_lm(self._apply_mask(imap)))
+
+    def _get_b(self, d):
+        return self._pointing_adjoint(self._apply_Ninv(d))
+
+    def _apply_A(self, ilm):
+        # C^-1 p + B Y^dagger W N^-1 W Y B p; W and N^-1 fused into one pixel weight
+        m = self.base.to_map(self._apply_beam(ilm))
+        m = m * (self.weightings.d_WNW / self.weightings.pixel_area)
+        return self._apply_Cinv(ilm) + self._apply_beam(self.base.to_lm(m))
+
+    def _apply_M(self, ilm):
+        Sig = self.weightings.d_Sigma
+        if self.preconditioner == 'harmonic':
+            return torch.einsum('abi,bi->ai', Sig, ilm)
+        elif self.preconditioner == 'pseudo_inverse':
+            W = self.weightings
+            alm = torch.einsum('abi,bi->ai', Sig, ilm)
+            alm_signal = torch.einsum('abi,bi->ai', W.d_inv_Cl, alm)
+            Nl = torch.as_tensor(W.Nl_iso, device=self.base.device)[:, None]
+            alm_noise = alm * self.base.dev('beam_lm') / Nl
+            alm_noise = self.base.to_lm(W.d_noise_cov * self.base.to_map(alm_noise)) * W.pixel_area
+            alm_noise = alm_noise * self.base.dev('beam_lm') / Nl
+            return torch.einsum('abi,bi->ai', Sig, alm_noise + alm_signal)
+        else:
+            raise Exception("Unknown preconditioner %s specified!" % self.preconditioner)
+
+    def step(self):
+        Ap = self._apply_A(self.p)
+        alpha = self.rz / self.dot(self.p, Ap)
+        self.x += alpha * self.p
+        self.r -= alpha * Ap
+        del Ap
+        z = self._apply_M(self.r)
+        next_rz = self.dot(self.r, z)
+        self.err = next_rz / self.rz0
+        beta = next_rz / self.rz
+        self.rz = next_rz
+        self.p = z + beta * self.p
+        self.i += 1
+
+    def run(self, nstep=10, thresh=1e-6):
+        for i in range(nstep):
+            self.step()
+            if self.verb:
+                print("CGD step %d: error = %.2e" % (self.i, self.err))
+            if self.err < thresh:
+                if self.verb:
+                    print("CGD terminating at step %d" % self.i)
+                break
+        if i == nstep - 1 and self.err > thresh:
+            print("CGD did not converge to %.2e threshold after %d steps. Final error = %.2e" % (thresh, nstep, self.err))
+
+    def get_wiener_lm(self):
+        return self.x + self.x0
+
+    def get_wiener_map(self):
+        return self.base.to_map(self.x + self.x0)
+
+    def get_ivar_lm(self):
+        return self._apply_Cinv(self.x + self.x0)
+
+    def get_ivar_map(self):
+        return self.base.to_map(self._apply_Cinv(self.x + self.x0))

@@ -1,0 +1,119 @@
+"""Seeded synthetic inputs of the benchmark workloads (no datasets are used).
+
+Stand-ins for the Planck-like inputs of the reference's scripts
+(run_planck_local_trispectra.py, run_planck_binned_bispectrum.py):
+
+* fiducial spectra  C_l^TT = 1000/(l+10)^2 uK^2, C^EE = 0.05 C^TT,
+  C^TE = 0.3 sqrt(C^TT C^EE), C^BB = 1e-6 C^EE, C^TB = C^EB = 0;
+* Gaussian beams  b_l = exp(-l(l+1) sigma^2/2), sigma = FWHM/sqrt(8 ln 2);
+* masks: a Galactic-latitude cut with a cosine taper, and a boolean sky cut
+  plus circular point-source holes at seeded uniform positions;
+* white noise of a given depth (uK arcmin) per pixel, twice the variance in Q, U.
+
+Pixel positions come from the HEALPix RING formulas (Gorski et al. 2005).
+"""
+import numpy as np
+
+
+def fiducial_cl(lmax, pol=True, amp=1000.0):
+    l = np.arange(lmax + 1, dtype=np.float64)
+    tt = amp / (l + 10.0) ** 2
+    if not pol:
+        return {'TT': tt}
+    ee = 0.05 * tt
+    te = 0.3 * np.sqrt(tt * ee)
+    bb = 1e-6 * ee
+    z = 0.0 * tt
+    return {'TT': tt, 'TE': te, 'TB': z.copy(), 'EE': ee, 'EB': z.copy(), 'BB': bb}
+
+
+def gaussian_beam(lmax, fwhm_arcmin):
+    sigma = np.radians(fwhm_arcmin / 60.0) / np.sqrt(8.0 * np.log(2.0))
+    l = np.arange(lmax + 1, dtype=np.float64)
+    return np.exp(-l * (l + 1.0) * sigma ** 2 / 2.0)
+
+
+def pixel_z_phi(nside):
+    """cos(theta) and longitude of every RING pixel centre."""
+    ns = nside
+    npix = 12 * ns * ns
+    z = np.empty(npix)
+    phi = np.empty(npix)
+    for i in range(1, 4 * ns):
+        north = i <= 2 * ns
+        ii = i if north else 4 * ns - i
+        if ii < ns:
+            t = ii * ii / (3.0 * ns * ns)
+            zz = 1.0 - t if north else t - 1.0
+            n = 4 * ii
+            start = 2 * ii * (ii - 1) if north else npix - 2 * ii * (ii + 1)
+            p = (np.arange(n) + 0.5) * (np.pi / (2.0 * ii))
+        else:
+            zz = (2 * ns - i) * 2.0 / (3.0 * ns)
+            n = 4 * ns
+            start = 2 * ns * (ns - 1) + (i - ns) * 4 * ns
+            shift = 0.5 if (i - ns) % 2 == 0 else 0.0
+            p = (np.arange(n) + shift) * (np.pi / (2.0 * ns))
+        z[start:start + n] = zz
+        phi[start:start + n] = p
+    return z, phi
+
+
+def latitude_mask(nside, cut_deg=15.0, taper_deg=5.0):
+    """0 for |lat| < cut, 1 above cut + taper, 0.5 (1 - cos(pi (|lat|-cut)/taper)) between."""
+    z, _ = pixel_z_phi(nside)
+    lat = np.degrees(np.arcsin(np.clip(z, -1, 1)))
+    a = np.abs(lat)
+    m = np.where(a < cut_deg, 0.0, np.where(a > cut_deg + taper_deg, 1.0,
+                                            0.5 * (1.0 - np.cos(np.pi * (a - cut_deg) / taper_deg))))
+    return m
+
+
+def point_source_mask(nside, cut_deg=5.74, n_holes=500, radius_arcmin=10.0, seed=0):
+    """Boolean mask: |lat| < cut removed, plus n_holes discs at seeded uniform positions."""
+    z, phi = pixel_z_phi(nside)
+    lat = np.degrees(np.arcsin(np.clip(z, -1, 1)))
+    m = np.abs(lat) >= cut_deg
+    rng = np.random.default_rng(seed)
+    zc = rng.uniform(-1.0, 1.0, n_holes)
+    pc = rng.uniform(0.0, 2 * np.pi, n_holes)
+    st = np.sqrt(np.clip(1 - z * z, 0, None))
+    cr = np.cos(np.radians(radius_arcmin / 60.0))
+    for k in range(n_holes):
+        stc = np.sqrt(max(1 - zc[k] ** 2, 0.0))
+        sel = np.abs(z - zc[k]) < 2.0 * np.radians(radius_arcmin / 60.0) + 1e-12
+        idx = np.nonzero(sel)[0]
+        cosd = z[idx] * zc[k] + st[idx] * stc * np.cos(phi[idx] - pc[k])
+        m[idx[cosd > cr]] = False
+    return m.astype(np.float64)
+
+
+def white_noise_cov(nside, depth_uk_arcmin=30.0, pol=True):
+    """Per-pixel noise variance (uK^2): depth^2 / Omega_pix (arcmin^2), x2 for Q and U."""
+    omega = 4 * np.pi / (12 * nside * nside) * (180 * 60 / np.pi) ** 2
+    s2 = depth_uk_arcmin ** 2 / omega
+    npix = 12 * nside * nside
+    if not pol:
+        return np.full((1, npix), s2)
+    return np.stack([np.full(npix, s2), np.full(npix, 2 * s2), np.full(npix, 2 * s2)])
+
+
+def noise_cl(nside, lmax, depth_uk_arcmin=30.0, pol=True):
+    """White-noise power N_l = depth^2 (in uK^2 sr) for T, x2 for E/B."""
+    n = (depth_uk_arcmin * np.pi / (180 * 60)) ** 2
+    out = {'TT': np.full(lmax + 1, n)}
+    if pol:
+        out.update({'EE': np.full(lmax + 1, 2 * n), 'BB': np.full(lmax + 1, 2 * n)})
+    return out
+
+
+def total_cl(cl, beam, nl=None):
+    """C_tot = b^2 C + N (beam-convolved signal plus noise), as the reference's Cl_tot expects."""
+    out = {}
+    for k, v in cl.items():
+        b1 = beam[{'T': 0, 'E': 1, 'B': 2}[k[0]]] if np.ndim(beam) == 2 else beam
+        b2 = beam[{'T': 0, 'E': 1, 'B': 2}[k[1]]] if np.ndim(beam) == 2 else beam
+        out[k] = b1 * b2 * v
+        if nl is not None and k in nl:
+            out[k] = out[k] + nl[k]
+    return out
