@@ -72,6 +72,27 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
 int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, int spin, double scale,
                void* workspace, size_t workspace_bytes, cudaStream_t stream);
 
+/* ------------------------------------------------------------- launch statistics
+ * No reference counterpart beyond its wall-clock SHT timer (polyspec/base.py:113-127,
+ * polyspec/tspec_template.py:453-517): every kernel launch of the library is
+ * counted per kind with its algorithmic flops and bytes; with timing enabled,
+ * CUDA events bracket each launch and ps_stats_get returns the summed device
+ * time (it synchronises on those events). */
+enum {
+  PS_K_LEG_SYNTH = 0,   /* Legendre stage of synthesis (all spins) */
+  PS_K_LEG_ADJOINT = 1, /* Legendre stage of the adjoint */
+  PS_K_FFT_SYNTH = 2,   /* ring transforms of synthesis */
+  PS_K_FFT_ADJOINT = 3, /* ring transforms of the adjoint */
+  PS_K_LAYOUT = 4,      /* alm transposes and partial-sum reductions */
+  PS_K_PIXEL = 5,       /* pixel-space products and sums */
+  PS_K_VECTOR = 6,      /* harmonic-space vector kernels (CG, filters) */
+  PS_K_MLP = 7,         /* learned-preconditioner network */
+  PS_KERNEL_KINDS = 8
+};
+int ps_stats_enable_timing(int on);
+int ps_stats_reset(void);
+int ps_stats_get(int kind, int64_t* launches, double* ms, double* flops, double* bytes);
+
 #ifdef __cplusplus
 }
 #endif

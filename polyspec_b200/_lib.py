@@ -32,7 +32,25 @@ SIGNATURES = {
                               _c_void_p]),
     "ps_adjoint": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_double, _c_void_p,
                             _c_size_t, _c_void_p]),
+    "ps_stats_enable_timing": (_c_int, [_c_int]),
+    "ps_stats_reset": (_c_int, []),
+    "ps_stats_get": (_c_int, [_c_int, ctypes.POINTER(_c_int64), ctypes.POINTER(_c_double),
+                              ctypes.POINTER(_c_double), ctypes.POINTER(_c_double)]),
 }
+
+KERNEL_KINDS = {"leg_synth": 0, "leg_adjoint": 1, "fft_synth": 2, "fft_adjoint": 3, "layout": 4, "pixel": 5,
+                "vector": 6, "mlp": 7}
+
+
+def stats(kind):
+    """(launches, device ms when timing is on, algorithmic flops, algorithmic bytes) of one kernel kind."""
+    n = _c_int64()
+    ms = _c_double()
+    fl = _c_double()
+    by = _c_double()
+    call("ps_stats_get", KERNEL_KINDS[kind] if isinstance(kind, str) else int(kind), ctypes.byref(n),
+         ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(by))
+    return int(n.value), float(ms.value), float(fl.value), float(by.value)
 
 _lib = None
 

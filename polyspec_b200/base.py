@@ -187,6 +187,33 @@ class PolySpec:
             return result
         return wrap_func
 
+    # ------------------------------------------------------------------ batched device transforms
+    def to_map_batch(self, alm, lmax=None):
+        """alm [B, nfield, nlm] (T or T,E,B) -> maps [B, nfield, Npix] (T or T,Q,U), one
+        batched libpscuda call per spin; counts like B calls of to_map."""
+        lmax = self.lmax if lmax is None else int(lmax)
+        P = self.plan(lmax)
+        B, nf = alm.shape[0], alm.shape[1]
+        self.n_SHTs_reverse += B * (1 + (nf == 3))
+        out = torch.empty((B, nf, self.Npix), dtype=torch.float64, device=self.device)
+        out[:, 0] = P.synthesis(alm[:, 0].contiguous(), 0)
+        if nf == 3:
+            out[:, 1:] = P.synthesis(alm[:, 1:].contiguous(), 2)
+        return out
+
+    def to_lm_batch(self, maps, lmax=None):
+        """maps [B, nfield, Npix] -> alm [B, nfield, nlm], scaled as to_lm."""
+        lmax = self.lmax if lmax is None else int(lmax)
+        P = self.plan(lmax)
+        B, nf = maps.shape[0], maps.shape[1]
+        self.n_SHTs_forward += B * (1 + (nf == 3))
+        scale = np.pi / (3. * self.Nside ** 2)
+        out = torch.empty((B, nf, P.nalm), dtype=torch.complex128, device=self.device)
+        out[:, 0] = P.adjoint(maps[:, 0].contiguous(), 0, scale)
+        if nf == 3:
+            out[:, 1:] = P.adjoint(maps[:, 1:].contiguous(), 2, scale)
+        return out
+
     # ------------------------------------------------------------------ SHT wrappers
     @timer_func
     def to_lm(self, input_map, lmax=None):

@@ -8,6 +8,7 @@
 // Rings are launched in classes of equal work length so that each launch
 // sizes its shared memory to its class.
 #include "ps_common.cuh"
+#include "ps_stats.cuh"
 
 namespace ps {
 
@@ -179,6 +180,7 @@ int launch_ring_synth_f64(const Plan& P, const int* d_list, int nrings, int work
   }
   int twlog = 0;
   while ((1 << twlog) < P.max_fft) ++twlog;
+  StatScope sc(PS_K_FFT_SYNTH, 0.0, 0.0, st);
   ring_synth_f64<<<nrings, threads, smem, st>>>(P.d_rings, d_list, phase, map, P.mmax, nf, P.npix, P.d_twiddle,
                                                 twlog, P.d_bs_spec, P.d_bs_off);
   PS_LAUNCH_CHECK();
@@ -197,6 +199,7 @@ int launch_ring_adjoint_f64(const Plan& P, const int* d_list, int nrings, int wo
   }
   int twlog = 0;
   while ((1 << twlog) < P.max_fft) ++twlog;
+  StatScope sc(PS_K_FFT_ADJOINT, 0.0, 0.0, st);
   ring_adjoint_f64<<<nrings, threads, smem, st>>>(P.d_rings, d_list, map, phase, P.mmax, nf, P.npix, P.d_twiddle,
                                                   twlog, P.d_bs_spec, P.d_bs_off);
   PS_LAUNCH_CHECK();

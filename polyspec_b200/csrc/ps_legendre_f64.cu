@@ -17,6 +17,7 @@
 // Layouts: almT [nalm][B][ncomp] (m-major l within, map index and G/C
 // innermost), phase [R][mmax+1][B][ncomp] (ring-major, order m, then maps).
 #include "ps_common.cuh"
+#include "ps_stats.cuh"
 
 namespace ps {
 
@@ -484,8 +485,19 @@ __global__ void reduce_partials(const double2* __restrict__ partial, double2* __
 }
 
 // ---------------------------------------------------------------- launchers
+// algorithmic Legendre work of one transform: 4 Rh nalm flops per spin-0 map,
+// 16 Rh nalm per spin-s (G, C) pair; bytes: alm in + per-ring phases out
+static double leg_flops(const Plan& P, int B, int spin) {
+  return double(spin == 0 ? 4 : 16) * double(P.Rh) * double(P.nalm) * B;
+}
+static double leg_bytes(const Plan& P, int B, int spin) {
+  const double nf = double(B) * (spin == 0 ? 1 : 2);
+  return nf * 16.0 * (double(P.nalm) + double(P.R) * (P.mmax + 1));
+}
+
 int launch_legendre_synth_f64(const Plan& P, const double2* almT, double2* phase, int B, int spin,
                               cudaStream_t st) {
+  StatScope sc(PS_K_LEG_SYNTH, leg_flops(P, B, spin), leg_bytes(P, B, spin), st);
   dim3 grid((P.Rh + SYN_THREADS - 1) / SYN_THREADS, P.mmax + 1, 1);
   if (spin == 0) {
     if (B >= 4) {
@@ -515,6 +527,7 @@ int adjoint_tiles(const Plan& P) { return (P.Rh + ADJ_THREADS - 1) / ADJ_THREADS
 
 int launch_legendre_adjoint_f64(const Plan& P, const double2* phase, double2* partial, int B, int spin,
                                 cudaStream_t st) {
+  StatScope sc(PS_K_LEG_ADJOINT, leg_flops(P, B, spin), leg_bytes(P, B, spin), st);
   dim3 grid(adjoint_tiles(P), P.mmax + 1, 1);
   if (spin == 0) {
     if (B >= 4) {
@@ -541,6 +554,7 @@ int launch_alm_to_T(const double2* alm, double2* almT, int B, int ncomp, int64_t
   const int64_t n = nalm * B * ncomp;
   int blocks = (int)std::min<int64_t>((n + 255) / 256, int64_t(sms) * 8);
   if (blocks < 1) blocks = 1;
+  StatScope sc(PS_K_LAYOUT, 0.0, 32.0 * n, st);
   alm_to_T<<<blocks, 256, 0, st>>>(alm, almT, B, ncomp, nalm);
   PS_LAUNCH_CHECK();
   return PS_OK;
@@ -551,6 +565,7 @@ int launch_reduce_partials(const double2* partial, double2* alm, int ntiles, int
   const int64_t n = nalm * B * ncomp;
   int blocks = (int)std::min<int64_t>((n + 255) / 256, int64_t(sms) * 8);
   if (blocks < 1) blocks = 1;
+  StatScope sc(PS_K_LAYOUT, 0.0, 16.0 * n * (ntiles + 1), st);
   reduce_partials<<<blocks, 256, 0, st>>>(partial, alm, ntiles, B, ncomp, nalm, scale);
   PS_LAUNCH_CHECK();
   return PS_OK;

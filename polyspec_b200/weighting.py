@@ -130,6 +130,38 @@ class Weightings:
         lfilt = torch.as_tensor(self.base.l_arr <= lmax, device=self.base.device)
         return self.base._out(cgd.get_ivar_lm()[:, lfilt], as_torch)
 
+    def batched_applySinv_optimal(self, maps, preconditioner='harmonic', nstep=25, thresh=1e-4, verb=False,
+                                  lmax=None):
+        """applySinv_optimal for a batch of maps [B, nfield, Npix] (CUDA tensor), solved
+        as B lockstep CGs with batched SHTs; returns [B, nfield, nlm(lmax)]."""
+        if lmax is None:
+            lmax = self.base.lmax
+        d = maps.to(device=self.base.device, dtype=torch.float64)
+        x0 = torch.einsum('abi,nbi->nai', self.d_x0op, self.base.to_lm_batch(d))
+        cgd = BatchedCGD(self, d, x0, preconditioner=preconditioner)
+        cgd.run(nstep=nstep, thresh=thresh, verb=verb)
+        self.last_cgd = cgd
+        lfilt = torch.as_tensor(self.base.l_arr <= lmax, device=self.base.device)
+        return cgd.get_ivar_lm()[:, :, lfilt]
+
+    def make_applySinv(self, kind='optimal', **kw):
+        """A callable with the reference applySinv signature and a ``.batched``
+        method (used by PSpecBin.compute_fisher_contribution(batched=True))."""
+        W = self
+
+        class _ApplySinv:
+            def __call__(self, x, input_type='map', lmax=None):
+                if kind == 'ideal':
+                    return W.applySinv_ideal(x, input_type=input_type, lmax=lmax)
+                return W.applySinv_optimal(x, input_type=input_type, lmax=lmax, **kw)
+
+            def batched(self, maps, lmax=None):
+                if kind == 'ideal':
+                    return torch.stack([W.applySinv_ideal(m, lmax=lmax) for m in maps])
+                return W.batched_applySinv_optimal(maps, lmax=lmax, **kw)
+
+        return _ApplySinv()
+
     def applySinv_ideal(self, input_map, input_type='map', lmax=None):
         """Ideal S^-1 = beam C_tot^-1 Y^dagger W (polyspec/weighting.py:186-214)."""
         if lmax is None:
@@ -148,6 +180,95 @@ class Weightings:
         input_lm = self.base.to_lm(x)
         out = beam[:, lfilt] * torch.einsum("abl,bl->al", icov[:, :, lfilt], input_lm[:, lfilt])
         return self.base._out(out, as_torch)
+
+
+class BatchedCGD:
+    """B independent copies of the reference CG (polyspec/weighting.py:217-367) run in
+    lockstep: vectors are [B, nfield, nlm], every A and M application is one batched
+    SHT pair, and each right-hand side keeps its own alpha, beta and stopping test
+    (err_b = rz_b / rz0_b < thresh freezes system b, as a separate run would stop)."""
+
+    def __init__(self, weightings, d, x0, preconditioner='harmonic'):
+        self.base = weightings.base
+        self.W = weightings
+        self.preconditioner = preconditioner
+        self.w = self.base.dev('m_weight')
+        b0 = self._get_b(d)
+        self.x0 = x0
+        b = b0 - self._apply_A(x0)
+        self.x = torch.zeros_like(b)
+        self.r = b.clone()
+        z = self._apply_M(self.r)
+        self.rz = self.dot(self.r, z)
+        self.rz0 = self.dot(b0, self._apply_M(b0))
+        self.p = z
+        self.i = 0
+        self.iters = torch.zeros(b.shape[0], dtype=torch.int64, device=b.device)
+        self.active = torch.ones(b.shape[0], dtype=torch.bool, device=b.device)
+        self.err = self.rz / self.rz0
+
+    def dot(self, a, b):
+        return torch.sum((a * b.conj()).real * self.w, dim=(-2, -1))
+
+    def _get_b(self, d):
+        m = d * self.W.d_noise_icov / self.W.pixel_area
+        return self.base.to_lm_batch(m * self.W.d_mask) * self.base.dev('beam_lm')
+
+    def _apply_Cinv(self, ilm):
+        return torch.einsum('abi,nbi->nai', self.W.d_inv_Cl, ilm)
+
+    def _apply_A(self, ilm):
+        beam = self.base.dev('beam_lm')
+        m = self.base.to_map_batch(ilm * beam)
+        m = m * (self.W.d_WNW / self.W.pixel_area)
+        return self._apply_Cinv(ilm) + self.base.to_lm_batch(m) * beam
+
+    def _apply_M(self, ilm):
+        Sig = self.W.d_Sigma
+        if self.preconditioner == 'harmonic':
+            return torch.einsum('abi,nbi->nai', Sig, ilm)
+        elif self.preconditioner == 'pseudo_inverse':
+            beam = self.base.dev('beam_lm')
+            Nl = torch.as_tensor(self.W.Nl_iso, device=self.base.device)[:, None]
+            alm = torch.einsum('abi,nbi->nai', Sig, ilm)
+            alm_signal = self._apply_Cinv(alm)
+            alm_noise = alm * beam / Nl
+            alm_noise = self.base.to_lm_batch(self.W.d_noise_cov * self.base.to_map_batch(alm_noise)) * self.W.pixel_area
+            alm_noise = alm_noise * beam / Nl
+            return torch.einsum('abi,nbi->nai', Sig, alm_noise + alm_signal)
+        raise Exception("Unknown preconditioner %s specified!" % self.preconditioner)
+
+    def step(self):
+        act = self.active.to(torch.float64)
+        Ap = self._apply_A(self.p)
+        alpha = torch.where(self.active, self.rz / self.dot(self.p, Ap), torch.zeros_like(self.rz))
+        self.x += alpha[:, None, None] * self.p
+        self.r -= alpha[:, None, None] * Ap
+        z = self._apply_M(self.r)
+        next_rz = self.dot(self.r, z)
+        self.err = torch.where(self.active, next_rz / self.rz0, self.err)
+        beta = torch.where(self.active, next_rz / self.rz, torch.zeros_like(next_rz))
+        self.rz = torch.where(self.active, next_rz, self.rz)
+        self.p = torch.where(self.active[:, None, None], z + beta[:, None, None] * self.p, self.p)
+        self.iters += self.active.to(torch.int64)
+        self.i += 1
+        del act
+
+    def run(self, nstep=10, thresh=1e-6, verb=False):
+        for i in range(nstep):
+            self.step()
+            self.active &= ~(self.err < thresh)
+            if verb:
+                print("batched CGD step %d: max error = %.2e, active %d" % (self.i, float(self.err.max()),
+                                                                             int(self.active.sum())))
+            if not bool(self.active.any()):
+                break
+        if bool(self.active.any()):
+            print("CGD did not converge to %.2e threshold after %d steps. Final error = %.2e"
+                  % (thresh, nstep, float(self.err.max())))
+
+    def get_ivar_lm(self):
+        return self._apply_Cinv(self.x + self.x0)
 
 
 class CGD:

@@ -70,21 +70,27 @@ def latitude_mask(nside, cut_deg=15.0, taper_deg=5.0):
 
 
 def point_source_mask(nside, cut_deg=5.74, n_holes=500, radius_arcmin=10.0, seed=0):
-    """Boolean mask: |lat| < cut removed, plus n_holes discs at seeded uniform positions."""
+    """Boolean mask: |lat| < cut removed, plus n_holes discs at seeded uniform positions.
+
+    RING order sorts pixels by decreasing z, so each disc only scans the pixel
+    range of its z band."""
     z, phi = pixel_z_phi(nside)
     lat = np.degrees(np.arcsin(np.clip(z, -1, 1)))
     m = np.abs(lat) >= cut_deg
     rng = np.random.default_rng(seed)
     zc = rng.uniform(-1.0, 1.0, n_holes)
     pc = rng.uniform(0.0, 2 * np.pi, n_holes)
-    st = np.sqrt(np.clip(1 - z * z, 0, None))
-    cr = np.cos(np.radians(radius_arcmin / 60.0))
+    rad = np.radians(radius_arcmin / 60.0)
+    cr = np.cos(rad)
+    negz = -z
     for k in range(n_holes):
         stc = np.sqrt(max(1 - zc[k] ** 2, 0.0))
-        sel = np.abs(z - zc[k]) < 2.0 * np.radians(radius_arcmin / 60.0) + 1e-12
-        idx = np.nonzero(sel)[0]
-        cosd = z[idx] * zc[k] + st[idx] * stc * np.cos(phi[idx] - pc[k])
-        m[idx[cosd > cr]] = False
+        lo = np.searchsorted(negz, -(zc[k] + 1.5 * rad), side="left")
+        hi = np.searchsorted(negz, -(zc[k] - 1.5 * rad), side="right")
+        zz = z[lo:hi]
+        st = np.sqrt(np.clip(1 - zz * zz, 0, None))
+        cosd = zz * zc[k] + st * stc * np.cos(phi[lo:hi] - pc[k])
+        m[lo:hi][cosd > cr] = False
     return m.astype(np.float64)
 
 
@@ -117,3 +123,23 @@ def total_cl(cl, beam, nl=None):
         if nl is not None and k in nl:
             out[k] = out[k] + nl[k]
     return out
+
+
+def cg_fisher_setup(nside=1024, lmax=2048, n_holes=500, depth=30.0, fwhm_arcmin=5.0, nbins=8, seed=0,
+                    fields=('TT', 'TE', 'EE', 'BB')):
+    """The masked-CG PSpecBin workload: TEB at (nside, lmax), white noise of
+    `depth` uK arcmin, a |lat| < 5.74 deg cut (10% of the sky) plus `n_holes`
+    point-source holes of 10' radius, `nbins` linear bins in [2, lmax].
+
+    Returns (cl_raw, cl_tot, beam[3, lmax+1], mask[3, npix], noise_cov[3, npix], l_bins).
+    """
+    cl = fiducial_cl(lmax, True)
+    b = gaussian_beam(lmax, fwhm_arcmin)
+    beam = np.stack([b, b, b])
+    nl = noise_cl(nside, lmax, depth, True)
+    cltot = total_cl(cl, beam, nl)
+    m = point_source_mask(nside, 5.74, n_holes, 10.0, seed)
+    mask = np.stack([m, m, m])
+    noise = white_noise_cov(nside, depth, True)
+    l_bins = np.linspace(2, lmax, nbins + 1).astype(int)
+    return cl, cltot, beam, mask, noise, l_bins
