@@ -72,6 +72,19 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
 int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, int spin, double scale,
                void* workspace, size_t workspace_bytes, cudaStream_t stream);
 
+/* Allocation-free variant of ps_synthesis (no counterpart in the reference).
+ * For callers that cannot allocate device memory at the point of the call (a
+ * framework that owns all device memory through its own fixed allocator, a
+ * real-time loop where a synchronising cudaMalloc is not allowed): the scratch
+ * comes from a static device array of PS_NOALLOC_SCRATCH_BYTES held by every GPU
+ * that loads the library until exit.  Requests needing more scratch than that
+ * (ps_sht_workspace_bytes) return PS_ERR_WORKSPACE before anything runs.  The
+ * first call on a device looks up the array's address and should come before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU race. */
+#define PS_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int ps_synthesis_noalloc(const ps_plan* plan, const double* alm, double* map, int batch, int spin,
+                         cudaStream_t stream);
+
 /* ------------------------------------------------------------- launch statistics
  * No reference counterpart beyond its wall-clock SHT timer (polyspec/base.py:113-127,
  * polyspec/tspec_template.py:453-517): every kernel launch of the library is

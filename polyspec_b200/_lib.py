@@ -32,6 +32,7 @@ SIGNATURES = {
                               _c_void_p]),
     "ps_adjoint": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_double, _c_void_p,
                             _c_size_t, _c_void_p]),
+    "ps_synthesis_noalloc": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p]),
     "ps_stats_enable_timing": (_c_int, [_c_int]),
     "ps_stats_reset": (_c_int, []),
     "ps_stats_get": (_c_int, [_c_int, ctypes.POINTER(_c_int64), ctypes.POINTER(_c_double),
