@@ -56,6 +56,16 @@ int ps_device_sm_count(int* count);
 int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_plan** plan);
 int ps_plan_destroy(ps_plan* plan);
 int ps_plan_info(const ps_plan* plan, int* nside, int* lmax, int64_t* npix, int64_t* nalm);
+/* Device error flag of the plan: kernels set it when a bounded wait expires
+ * (they then return without completing).  Reads it (synchronously, after the
+ * device finishes its work) and optionally clears it.  No reference counterpart. */
+int ps_plan_error_flag(const ps_plan* plan, int* value, int reset);
+
+/* prec = PS_PREC_FP64: every stage in FP64.  prec = PS_PREC_MIXED: the
+ * synthesis' Legendre stage runs on the tensor cores (tcgen05, TF32 split in
+ * three products, FP32 accumulation) from FP64 recurrences; the adjoint's
+ * Legendre stage contracts FP32-rounded FP64 recurrences with FP32 FMAs; the
+ * ring transforms run in FP32; inputs and outputs stay FP64 in both cases. */
 
 /* Scratch bytes needed by ps_synthesis / ps_adjoint for `batch` maps of `spin`. */
 int ps_sht_workspace_bytes(const ps_plan* plan, int batch, int spin, int adjoint, size_t* bytes);

@@ -27,6 +27,7 @@ SIGNATURES = {
     "ps_plan_destroy": (_c_int, [_c_void_p]),
     "ps_plan_info": (_c_int, [_c_void_p, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int),
                               ctypes.POINTER(_c_int64), ctypes.POINTER(_c_int64)]),
+    "ps_plan_error_flag": (_c_int, [_c_void_p, ctypes.POINTER(_c_int), _c_int]),
     "ps_sht_workspace_bytes": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_synthesis": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p, _c_size_t,
                               _c_void_p]),

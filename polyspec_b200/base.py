@@ -15,9 +15,11 @@ CUDA tensors, so estimator pipelines stay on the device).  There is no CPU
 fallback: constructing the class without a GPU or without the built library
 raises.
 
-Extension beyond the reference: an optional ``lmax=`` keyword fixes the
+Extensions beyond the reference (optional keywords): ``lmax=`` fixes the
 harmonic band limit used by default (the reference hard-codes 3 Nside - 1,
-polyspec/base.py:30).
+polyspec/base.py:30); ``prec='mixed'`` runs the SHTs on the mixed-precision
+path (tensor-core Legendre synthesis, FP32 contractions and ring FFTs, FP64
+inputs and outputs) instead of the FP64 path.
 """
 import os
 import time
@@ -62,7 +64,8 @@ def synalm_numpy(cls_rows, lmax, nfield):
 class PolySpec:
     """Base class of PolySpec on one B200 (see module docstring)."""
 
-    def __init__(self, Nside, Cl_tot, beam=[], pol=True, backend="cuda", nthreads=0, lmax=None, device=None):
+    def __init__(self, Nside, Cl_tot, beam=[], pol=True, backend="cuda", nthreads=0, lmax=None, device=None,
+                 prec="fp64"):
         if backend != "cuda":
             raise Exception("polyspec_b200 implements the 'cuda' backend only")
         if not torch.cuda.is_available():
@@ -70,6 +73,9 @@ class PolySpec:
         self.Nside = Nside
         self.pol = pol
         self.backend = backend
+        if prec not in ("fp64", "mixed"):
+            raise ValueError("prec must be 'fp64' or 'mixed'")
+        self.prec = prec
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
 
         self.Npix = 12 * Nside ** 2
@@ -144,7 +150,7 @@ class PolySpec:
         lmax = self.lmax if lmax is None else int(lmax)
         p = self._plans.get(lmax)
         if p is None:
-            p = SHTPlan(self.Nside, lmax, device=self.device)
+            p = SHTPlan(self.Nside, lmax, device=self.device, prec=self.prec)
             self._plans[lmax] = p
         return p
 

@@ -44,6 +44,9 @@ struct Plan {
   SeedNorm* d_seed[4];      // [mmax+1] per spin 1..3 (index 1..3), null if not in spin_mask
   double2* d_twiddle;       // [max_fft/2] e^{-2 pi i k / max_fft}
   double2* d_bs_spec;       // Bluestein spectra (FP64)
+  float2* d_twiddle_f;      // FP32 copies for the mixed-precision ring transforms
+  float2* d_bs_spec_f;
+  int* d_err;               // device error flag raised by kernels whose bounded waits expired
   int64_t* d_bs_off;        // [nslots]
   int n_bs_slots;
   int64_t bs_total;

@@ -1,0 +1,294 @@
+// FP32 ring transforms of the mixed-precision HEALPix SHT (maps stay FP64 in
+// HBM; the per-ring phases and the FFTs run in FP32).  Per ring of nphi pixels:
+//   synthesis  map_j = sum_{|m| <= mmax} F_m e^{i m (phi0 + 2 pi j / nphi)}   (F_{-m} = F_m^*)
+//   adjoint    P_m   = sum_j map_j e^{-i m (phi0 + 2 pi j / nphi)},  m = 0..mmax
+// with the HEALPix m-aliasing (m folded modulo nphi).
+//
+// Two real fields share one complex FFT (their spectra are Hermitian): the
+// synthesis transforms conj(c_a) + i conj(c_b) and reads map_a, map_b from the
+// real and imaginary parts; the adjoint transforms x_a + i x_b and separates
+// X_a = (Z_k + Z*_{N-k})/2, X_b = (Z_k - Z*_{N-k})/(2i).  A CTA runs G such FFTs
+// at once (G = 256 / T threads per FFT), so small rings keep every thread busy.
+// FFTs are radix-2 with stages fused in pairs (one barrier and one shared-memory
+// round trip per two stages): decimation in frequency for power-of-two rings,
+// Bluestein's chirp-z convolution of power-of-two length M >= 2 nphi - 1 for the
+// others.  Rings are launched in classes of equal work length.
+#include "ps_common.cuh"
+#include "ps_stats.cuh"
+
+namespace ps {
+
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 fconj2(float2 a) { return make_float2(a.x, -a.y); }
+
+__device__ __forceinline__ int bitrev_f(int i, int logn) { return (int)(__brev((unsigned)i) >> (32 - logn)); }
+__device__ __forceinline__ int ilog2_f(int n) { return 31 - __clz(n); }
+
+// e^{i pi q / den} for integer q (exact argument reduction modulo 2 den)
+__device__ __forceinline__ float2 expi_pi_ratio_f(int64_t q, int64_t den) {
+  q %= 2 * den;
+  if (q < 0) q += 2 * den;
+  float s, c;
+  sincospif(float(double(q) / double(den)), &s, &c);
+  return make_float2(c, s);
+}
+
+// twiddle e^{sign 2 pi i j / 2^s} from tw[k] = e^{-2 pi i k / 2^twlog}
+__device__ __forceinline__ float2 twid(const float2* __restrict__ tw, int j, int s, int twlog, int sign) {
+  float2 w = tw[j << (twlog - s)];
+  if (sign > 0) w.y = -w.y;
+  return w;
+}
+
+// Decimation in frequency (natural order in, bit-reversed out) on a[0..2^logn),
+// by the T threads with local index u; stages fused in pairs.
+__device__ void fft_dif_f(float2* a, int logn, int sign, const float2* __restrict__ tw, int twlog, int u, int T) {
+  const int n = 1 << logn;
+  int s = logn;
+  for (; s >= 2; s -= 2) {
+    const int q = 1 << (s - 2);
+    for (int t = u; t < n / 4; t += T) {
+      const int blk = t >> (s - 2), j = t & (q - 1);
+      const int i0 = blk * 4 * q + j, i1 = i0 + q, i2 = i0 + 2 * q, i3 = i0 + 3 * q;
+      const float2 x0 = a[i0], x1 = a[i1], x2 = a[i2], x3 = a[i3];
+      const float2 y0 = fadd2(x0, x2), y2 = fmul2(fsub2(x0, x2), twid(tw, j, s, twlog, sign));
+      const float2 y1 = fadd2(x1, x3), y3 = fmul2(fsub2(x1, x3), twid(tw, j + q, s, twlog, sign));
+      const float2 w = twid(tw, j, s - 1, twlog, sign);
+      a[i0] = fadd2(y0, y1);
+      a[i1] = fmul2(fsub2(y0, y1), w);
+      a[i2] = fadd2(y2, y3);
+      a[i3] = fmul2(fsub2(y2, y3), w);
+    }
+    __syncthreads();
+  }
+  if (s == 1) {
+    for (int t = u; t < n / 2; t += T) {
+      const float2 x0 = a[2 * t], x1 = a[2 * t + 1];
+      a[2 * t] = fadd2(x0, x1);
+      a[2 * t + 1] = fsub2(x0, x1);
+    }
+    __syncthreads();
+  }
+}
+
+// Decimation in time (bit-reversed order in, natural out); stages fused in pairs.
+__device__ void fft_dit_f(float2* a, int logn, int sign, const float2* __restrict__ tw, int twlog, int u, int T) {
+  const int n = 1 << logn;
+  int s = 1;
+  if (logn & 1) {
+    for (int t = u; t < n / 2; t += T) {
+      const float2 x0 = a[2 * t], x1 = a[2 * t + 1];
+      a[2 * t] = fadd2(x0, x1);
+      a[2 * t + 1] = fsub2(x0, x1);
+    }
+    __syncthreads();
+    s = 2;
+  }
+  for (; s + 1 <= logn; s += 2) {
+    const int q = 1 << (s - 1);
+    for (int t = u; t < n / 4; t += T) {
+      const int blk = t >> (s - 1), j = t & (q - 1);
+      const int i0 = blk * 4 * q + j, i1 = i0 + q, i2 = i0 + 2 * q, i3 = i0 + 3 * q;
+      const float2 ws = twid(tw, j, s, twlog, sign);
+      const float2 v1 = fmul2(a[i1], ws), v3 = fmul2(a[i3], ws);
+      const float2 x0 = a[i0], x2 = a[i2];
+      const float2 y0 = fadd2(x0, v1), y1 = fsub2(x0, v1), y2 = fadd2(x2, v3), y3 = fsub2(x2, v3);
+      const float2 v2 = fmul2(y2, twid(tw, j, s + 1, twlog, sign));
+      const float2 v3b = fmul2(y3, twid(tw, j + q, s + 1, twlog, sign));
+      a[i0] = fadd2(y0, v2);
+      a[i2] = fsub2(y0, v2);
+      a[i1] = fadd2(y1, v3b);
+      a[i3] = fsub2(y1, v3b);
+    }
+    __syncthreads();
+  }
+}
+
+struct RingDFTf {
+  int N, M, logM;
+  bool bluestein;
+};
+
+__device__ __forceinline__ float2 chirp_f(int j, int N) {
+  const int64_t q = (int64_t(j) * j) % (2 * int64_t(N));
+  return expi_pi_ratio_f(-q, N);
+}
+
+// In-place forward DFT (sign -1) of buf[0..N); read results with dft_get_f.
+__device__ void ring_dft_forward_f(float2* buf, const RingDFTf& d, const float2* __restrict__ tw, int twlog,
+                                   const float2* __restrict__ bspec, int u, int T) {
+  if (!d.bluestein) {
+    fft_dif_f(buf, d.logM, -1, tw, twlog, u, T);
+    return;
+  }
+  for (int j = u; j < d.M; j += T) buf[j] = (j < d.N) ? fmul2(buf[j], chirp_f(j, d.N)) : make_float2(0.f, 0.f);
+  __syncthreads();
+  fft_dif_f(buf, d.logM, -1, tw, twlog, u, T);
+  for (int p = u; p < d.M; p += T) buf[p] = fmul2(buf[p], bspec[p]);
+  __syncthreads();
+  fft_dit_f(buf, d.logM, +1, tw, twlog, u, T);
+}
+
+__device__ __forceinline__ float2 dft_get_f(const float2* buf, const RingDFTf& d, int k) {
+  if (!d.bluestein) return buf[bitrev_f(k, d.logM)];
+  const float2 v = fmul2(buf[k], chirp_f(k, d.N));
+  const float s = 1.0f / float(d.M);
+  return make_float2(v.x * s, v.y * s);
+}
+
+__device__ __forceinline__ RingDFTf make_dft(const RingInfo& g) {
+  RingDFTf d;
+  d.N = g.nphi;
+  d.bluestein = g.bs_slot >= 0;
+  d.M = d.bluestein ? g.bs_m : d.N;
+  d.logM = ilog2_f(d.M);
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// synthesis: phase [R][mmax+1][nf] (complex64) -> map [nf][npix] (float64)
+// grid (rings of the class, ceil(pairs / G)); block T*G threads; smem G*M float2
+__global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list,
+                               const float2* __restrict__ phase, double* __restrict__ map, int mmax, int nf,
+                               int64_t npix, const float2* __restrict__ tw, int twlog,
+                               const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T) {
+  extern __shared__ float2 fbuf[];
+  const int ir = ring_list[blockIdx.x];
+  const RingInfo g = rings[ir];
+  const RingDFTf d = make_dft(g);
+  const float2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
+  const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
+  const int G = blockDim.x / T;
+  const int pair = blockIdx.y * G + grp;
+  const int fa = 2 * pair, fb = 2 * pair + 1;
+  const bool va = fa < nf, vb = fb < nf;
+  float2* buf = fbuf + size_t(grp) * d.M;
+  const int N = d.N;
+  const int64_t pden = g.phi_den;
+  const float2* ph = phase + int64_t(ir) * (mmax + 1) * nf;
+  // buf_k = conj(c_a,k) + i conj(c_b,k);  c_k = sum_{m=k mod N} F_m e^{i m phi0} + sum_{m=-k mod N, m>0} conj(...)
+  for (int kk = u; kk < N; kk += T) {
+    float2 ca = make_float2(0.f, 0.f), cb = ca;
+    if (va) {
+      for (int m = kk; m <= mmax; m += N) {
+        const float2 e = expi_pi_ratio_f(int64_t(m) * g.phi_num, pden);
+        ca = fadd2(ca, fmul2(ph[int64_t(m) * nf + fa], e));
+        if (vb) cb = fadd2(cb, fmul2(ph[int64_t(m) * nf + fb], e));
+      }
+      for (int m = (kk == 0) ? N : N - kk; m <= mmax; m += N) {
+        const float2 e = expi_pi_ratio_f(int64_t(m) * g.phi_num, pden);
+        ca = fadd2(ca, fconj2(fmul2(ph[int64_t(m) * nf + fa], e)));
+        if (vb) cb = fadd2(cb, fconj2(fmul2(ph[int64_t(m) * nf + fb], e)));
+      }
+    }
+    // a real field keeps only Re(c_0) (F_0's imaginary part drops out of the
+    // real map); it must not leak into the partner field of the packed pair
+    if (kk == 0) { ca.y = 0.f; cb.y = 0.f; }
+    // conj(ca) + i conj(cb)
+    buf[kk] = make_float2(ca.x + cb.y, -ca.y + cb.x);
+  }
+  __syncthreads();
+  ring_dft_forward_f(buf, d, tw, twlog, bspec, u, T);
+  if (va) {
+    double* oa = map + int64_t(fa) * npix + g.start;
+    double* ob = map + int64_t(fb) * npix + g.start;
+    for (int j = u; j < N; j += T) {
+      const float2 y = dft_get_f(buf, d, j);
+      oa[j] = double(y.x);
+      if (vb) ob[j] = double(y.y);
+    }
+  }
+}
+
+// adjoint: map [nf][npix] (float64) -> phase [R][mmax+1][nf] (complex64)
+__global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list,
+                                 const double* __restrict__ map, float2* __restrict__ phase, int mmax, int nf,
+                                 int64_t npix, const float2* __restrict__ tw, int twlog,
+                                 const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T) {
+  extern __shared__ float2 fbuf[];
+  const int ir = ring_list[blockIdx.x];
+  const RingInfo g = rings[ir];
+  const RingDFTf d = make_dft(g);
+  const float2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
+  const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
+  const int G = blockDim.x / T;
+  const int pair = blockIdx.y * G + grp;
+  const int fa = 2 * pair, fb = 2 * pair + 1;
+  const bool va = fa < nf, vb = fb < nf;
+  float2* buf = fbuf + size_t(grp) * d.M;
+  const int N = d.N;
+  const int64_t pden = g.phi_den;
+  {
+    const double* ia = map + int64_t(va ? fa : 0) * npix + g.start;
+    const double* ib = map + int64_t(vb ? fb : 0) * npix + g.start;
+    for (int j = u; j < N; j += T) buf[j] = make_float2(va ? float(ia[j]) : 0.f, vb ? float(ib[j]) : 0.f);
+  }
+  __syncthreads();
+  ring_dft_forward_f(buf, d, tw, twlog, bspec, u, T);
+  if (va) {
+    float2* ph = phase + int64_t(ir) * (mmax + 1) * nf;
+    for (int m = u; m <= mmax; m += T) {
+      const int k = m % N, k2 = (N - k) % N;
+      const float2 z = dft_get_f(buf, d, k), z2 = fconj2(dft_get_f(buf, d, k2));
+      const float2 e = expi_pi_ratio_f(-int64_t(m) * g.phi_num, pden);
+      const float2 xa = make_float2(0.5f * (z.x + z2.x), 0.5f * (z.y + z2.y));
+      // (z - z2) / (2i) = -i (z - z2) / 2
+      const float2 xb = make_float2(0.5f * (z.y - z2.y), -0.5f * (z.x - z2.x));
+      ph[int64_t(m) * nf + fa] = fmul2(xa, e);
+      if (vb) ph[int64_t(m) * nf + fb] = fmul2(xb, e);
+    }
+  }
+}
+
+static void fft_shape(int work_len, int nf, int& T, int& G, int& gy) {
+  T = std::max(32, std::min(256, work_len / 4));
+  G = std::max(1, 256 / T);
+  const int pairs = (nf + 1) / 2;
+  G = std::min(G, pairs);
+  gy = (pairs + G - 1) / G;
+}
+
+int launch_ring_synth_f32(const Plan& P, const int* d_list, int nrings, int work_len, const float2* phase,
+                          double* map, int nf, cudaStream_t st) {
+  if (nrings == 0) return PS_OK;
+  int T, G, gy;
+  fft_shape(work_len, nf, T, G, gy);
+  const size_t smem = size_t(work_len) * G * sizeof(float2);
+  if (smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(ring_synth_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return PS_ERR_CUDA;
+  }
+  int twlog = 0;
+  while ((1 << twlog) < P.max_fft) ++twlog;
+  StatScope sc(PS_K_FFT_SYNTH, 0.0, 0.0, st);
+  ring_synth_f32<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, phase, map, P.mmax, nf, P.npix,
+                                                         P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off, T);
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}
+
+int launch_ring_adjoint_f32(const Plan& P, const int* d_list, int nrings, int work_len, const double* map,
+                            float2* phase, int nf, cudaStream_t st) {
+  if (nrings == 0) return PS_OK;
+  int T, G, gy;
+  fft_shape(work_len, nf, T, G, gy);
+  const size_t smem = size_t(work_len) * G * sizeof(float2);
+  if (smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(ring_adjoint_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return PS_ERR_CUDA;
+  }
+  int twlog = 0;
+  while ((1 << twlog) < P.max_fft) ++twlog;
+  StatScope sc(PS_K_FFT_ADJOINT, 0.0, 0.0, st);
+  ring_adjoint_f32<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, map, phase, P.mmax, nf, P.npix,
+                                                           P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off, T);
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}
+
+}  // namespace ps

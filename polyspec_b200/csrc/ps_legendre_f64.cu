@@ -259,14 +259,15 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj0_f64(const RingInfo* __restri
                                                          const double* __restrict__ mnorm,
                                                          const double2* __restrict__ phase,
                                                          double2* __restrict__ partial, int R, int Rh, int lmax,
-                                                         int mmax, int B, int64_t nalm) {
+                                                         int mmax, int B, int bofs, int Bc, int64_t nalm) {
   const int m = blockIdx.y;
   const int tile = blockIdx.x;
   const int tid = threadIdx.x;
   const int rp = tile * ADJ_THREADS + tid;
-  const int b0 = blockIdx.z * NB;
-  __shared__ double s_lam[ADJ_LCH][ADJ_THREADS];
-  __shared__ double2 s_P[ADJ_THREADS][2][NB];  // [ring][even/odd][map]
+  const int b0 = bofs + blockIdx.z * NB;
+  // ring-contiguous layouts (a warp's 8 ring segments read consecutive words)
+  __shared__ double s_lam[ADJ_LCH][ADJ_THREADS + 2];
+  __shared__ double2 s_P[2][NB][ADJ_THREADS];  // [even/odd][map][ring]
   __shared__ double s_a[ADJ_LCH], s_b[ADJ_LCH];
   const bool active = rp < Rh;
   const RingInfo g = rings[active ? rp : 0];
@@ -274,12 +275,12 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj0_f64(const RingInfo* __restri
 #pragma unroll
   for (int i = 0; i < NB; ++i) {
     double2 pn = make_double2(0.0, 0.0), ps = pn;
-    if (active && b0 + i < B) {
+    if (active && b0 + i < bofs + Bc) {
       pn = phase[(int64_t(rp) * (mmax + 1) + m) * B + b0 + i];
       if (rs != rp) ps = phase[(int64_t(rs) * (mmax + 1) + m) * B + b0 + i];
     }
-    s_P[tid][0][i] = cadd(pn, ps);
-    s_P[tid][1][i] = csub(pn, ps);
+    s_P[0][i][tid] = cadd(pn, ps);
+    s_P[1][i][tid] = csub(pn, ps);
   }
   const double x = g.z;
   double cur, prev = 0.0;
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj0_f64(const RingInfo* __restri
       const int r = seg + 8 * t;
       const double lam = s_lam[jr][r];
 #pragma unroll
-      for (int i = 0; i < NB; ++i) acc[i] = cfma(lam, s_P[r][p][i], acc[i]);
+      for (int i = 0; i < NB; ++i) acc[i] = cfma(lam, s_P[p][i][r], acc[i]);
     }
 #pragma unroll
     for (int i = 0; i < NB; ++i) {
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj0_f64(const RingInfo* __restri
       const int64_t idx = base + (l0 - m) + jr;
 #pragma unroll
       for (int i = 0; i < NB; ++i)
-        if (b0 + i < B) partial[(int64_t(tile) * nalm + idx) * B + b0 + i] = acc[i];
+        if (b0 + i < bofs + Bc) partial[(int64_t(tile) * nalm + idx) * Bc + (b0 - bofs) + i] = acc[i];
     }
     __syncthreads();
   }
@@ -342,16 +343,16 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjS_f64(const RingInfo* __restri
                                                          const SeedNorm* __restrict__ seednorm,
                                                          const double2* __restrict__ phase,
                                                          double2* __restrict__ partial, int R, int Rh, int lmax,
-                                                         int mmax, int B, int64_t nalm, int spin) {
+                                                         int mmax, int B, int bofs, int Bc, int64_t nalm, int spin) {
   const int m = blockIdx.y;
   const int tile = blockIdx.x;
   const int tid = threadIdx.x;
   const int rp = tile * ADJ_THREADS + tid;
-  const int b0 = blockIdx.z * NB;
-  __shared__ double s_fp[ADJ_LCH][ADJ_THREADS];
-  __shared__ double s_fm[ADJ_LCH][ADJ_THREADS];
-  __shared__ double2 s_Q[ADJ_THREADS][2][NB];  // [ring][N+S, N-S][map]
-  __shared__ double2 s_U[ADJ_THREADS][2][NB];
+  const int b0 = bofs + blockIdx.z * NB;
+  __shared__ double s_fp[ADJ_LCH][ADJ_THREADS + 2];
+  __shared__ double s_fm[ADJ_LCH][ADJ_THREADS + 2];
+  __shared__ double2 s_Q[2][NB][ADJ_THREADS];  // [N+S, N-S][map][ring]
+  __shared__ double2 s_U[2][NB][ADJ_THREADS];
   __shared__ double s_A[ADJ_LCH], s_D[ADJ_LCH], s_C[ADJ_LCH];
   const bool active = rp < Rh;
   const RingInfo g = rings[active ? rp : 0];
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjS_f64(const RingInfo* __restri
 #pragma unroll
   for (int i = 0; i < NB; ++i) {
     double2 qn = make_double2(0.0, 0.0), qs = qn, un = qn, us = qn;
-    if (active && b0 + i < B) {
+    if (active && b0 + i < bofs + Bc) {
       const int64_t o = ((int64_t(rp) * (mmax + 1) + m) * B + b0 + i) * 2;
       qn = phase[o]; un = phase[o + 1];
       if (rs != rp) {
@@ -367,8 +368,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjS_f64(const RingInfo* __restri
         qs = phase[o2]; us = phase[o2 + 1];
       }
     }
-    s_Q[tid][0][i] = cadd(qn, qs); s_Q[tid][1][i] = csub(qn, qs);
-    s_U[tid][0][i] = cadd(un, us); s_U[tid][1][i] = csub(un, us);
+    s_Q[0][i][tid] = cadd(qn, qs); s_Q[1][i][tid] = csub(qn, qs);
+    s_U[0][i][tid] = cadd(un, us); s_U[1][i][tid] = csub(un, us);
   }
   const double x = g.z;
   const int lmin = max(m, spin);
@@ -418,10 +419,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjS_f64(const RingInfo* __restri
       const double vp = s_fp[jr][r], vm = s_fm[jr][r];
 #pragma unroll
       for (int i = 0; i < NB; ++i) {
-        S1[i] = cfma(vp, s_Q[r][cplus][i], S1[i]);
-        S2[i] = cfma(vm, s_U[r][cminus][i], S2[i]);
-        S3[i] = cfma(vm, s_Q[r][cminus][i], S3[i]);
-        S4[i] = cfma(vp, s_U[r][cplus][i], S4[i]);
+        S1[i] = cfma(vp, s_Q[cplus][i][r], S1[i]);
+        S2[i] = cfma(vm, s_U[cminus][i][r], S2[i]);
+        S3[i] = cfma(vm, s_Q[cminus][i][r], S3[i]);
+        S4[i] = cfma(vp, s_U[cplus][i][r], S4[i]);
       }
     }
 #pragma unroll
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjS_f64(const RingInfo* __restri
       const int64_t idx = base + (l0 - m) + jr;
 #pragma unroll
       for (int i = 0; i < NB; ++i) {
-        if (b0 + i >= B) break;
+        if (b0 + i >= bofs + Bc) break;
         double2 G, C;
         if (!odd) {  // G = -S1 - i S2, C = i S3 - S4
           G = make_double2(-S1[i].x + S2[i].y, -S1[i].y - S2[i].x);
@@ -447,7 +448,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjS_f64(const RingInfo* __restri
           G = make_double2(-S3[i].x + S4[i].y, -S3[i].y - S4[i].x);
           C = make_double2(-S1[i].y - S2[i].x, S1[i].x - S2[i].y);
         }
-        const int64_t o = ((int64_t(tile) * nalm + idx) * B + b0 + i) * 2;
+        const int64_t o = ((int64_t(tile) * nalm + idx) * Bc + (b0 - bofs) + i) * 2;
         partial[o] = G;
         partial[o + 1] = C;
       }
@@ -472,7 +473,7 @@ __global__ void alm_to_T(const double2* __restrict__ alm, double2* __restrict__ 
 
 // sum_t partial[t][nalm][B][ncomp] * scale -> alm [B][ncomp][nalm]
 __global__ void reduce_partials(const double2* __restrict__ partial, double2* __restrict__ alm, int ntiles, int B,
-                                int ncomp, int64_t nalm, double scale) {
+                                int ncomp, int64_t nalm, double scale, int bofs) {
   const int64_t n = nalm * B * ncomp;
   for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x) {
     double2 s = make_double2(0.0, 0.0);
@@ -480,7 +481,7 @@ __global__ void reduce_partials(const double2* __restrict__ partial, double2* __
     const int c = int(t % ncomp);
     const int b = int((t / ncomp) % B);
     const int64_t idx = t / (int64_t(ncomp) * B);
-    alm[(int64_t(b) * ncomp + c) * nalm + idx] = cscale(s, scale);
+    alm[(int64_t(bofs + b) * ncomp + c) * nalm + idx] = cscale(s, scale);
   }
 }
 
@@ -525,26 +526,27 @@ int launch_legendre_synth_f64(const Plan& P, const double2* almT, double2* phase
 
 int adjoint_tiles(const Plan& P) { return (P.Rh + ADJ_THREADS - 1) / ADJ_THREADS; }
 
-int launch_legendre_adjoint_f64(const Plan& P, const double2* phase, double2* partial, int B, int spin,
-                                cudaStream_t st) {
-  StatScope sc(PS_K_LEG_ADJOINT, leg_flops(P, B, spin), leg_bytes(P, B, spin), st);
+// maps [bofs, bofs + Bc) of a batch of B; partial holds [tile][nalm][Bc][ncomp]
+int launch_legendre_adjoint_f64(const Plan& P, const double2* phase, double2* partial, int B, int bofs, int Bc,
+                                int spin, cudaStream_t st) {
+  StatScope sc(PS_K_LEG_ADJOINT, leg_flops(P, Bc, spin), leg_bytes(P, Bc, spin), st);
   dim3 grid(adjoint_tiles(P), P.mmax + 1, 1);
   if (spin == 0) {
-    if (B >= 4) {
-      grid.z = (B + 3) / 4;
+    if (Bc >= 4) {
+      grid.z = (Bc + 3) / 4;
       adj0_f64<4><<<grid, ADJ_THREADS, 0, st>>>(P.d_rings, P.d_mnorm0, phase, partial, P.R, P.Rh, P.lmax, P.mmax,
-                                                B, P.nalm);
+                                                B, bofs, Bc, P.nalm);
     } else {
-      grid.z = B;
+      grid.z = Bc;
       adj0_f64<1><<<grid, ADJ_THREADS, 0, st>>>(P.d_rings, P.d_mnorm0, phase, partial, P.R, P.Rh, P.lmax, P.mmax,
-                                                B, P.nalm);
+                                                B, bofs, Bc, P.nalm);
     }
   } else {
     if (!P.d_seed[spin]) return PS_ERR_INVALID;
     // one map per CTA: two maps would exceed the 48 KB of static shared memory
-    grid.z = B;
+    grid.z = Bc;
     adjS_f64<1><<<grid, ADJ_THREADS, 0, st>>>(P.d_rings, P.d_seed[spin], phase, partial, P.R, P.Rh, P.lmax,
-                                              P.mmax, B, P.nalm, spin);
+                                              P.mmax, B, bofs, Bc, P.nalm, spin);
   }
   PS_LAUNCH_CHECK();
   return PS_OK;
@@ -561,12 +563,12 @@ int launch_alm_to_T(const double2* alm, double2* almT, int B, int ncomp, int64_t
 }
 
 int launch_reduce_partials(const double2* partial, double2* alm, int ntiles, int B, int ncomp, int64_t nalm,
-                           double scale, int sms, cudaStream_t st) {
+                           double scale, int bofs, int sms, cudaStream_t st) {
   const int64_t n = nalm * B * ncomp;
   int blocks = (int)std::min<int64_t>((n + 255) / 256, int64_t(sms) * 8);
   if (blocks < 1) blocks = 1;
   StatScope sc(PS_K_LAYOUT, 0.0, 16.0 * n * (ntiles + 1), st);
-  reduce_partials<<<blocks, 256, 0, st>>>(partial, alm, ntiles, B, ncomp, nalm, scale);
+  reduce_partials<<<blocks, 256, 0, st>>>(partial, alm, ntiles, B, ncomp, nalm, scale, bofs);
   PS_LAUNCH_CHECK();
   return PS_OK;
 }

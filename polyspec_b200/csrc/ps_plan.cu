@@ -15,16 +15,27 @@
 
 namespace ps {
 int launch_legendre_synth_f64(const Plan& P, const double2* almT, double2* phase, int B, int spin, cudaStream_t st);
-int launch_legendre_adjoint_f64(const Plan& P, const double2* phase, double2* partial, int B, int spin,
-                                cudaStream_t st);
+int launch_legendre_adjoint_f64(const Plan& P, const double2* phase, double2* partial, int B, int bofs, int Bc,
+                                int spin, cudaStream_t st);
 int adjoint_tiles(const Plan& P);
 int launch_alm_to_T(const double2* alm, double2* almT, int B, int ncomp, int64_t nalm, int sms, cudaStream_t st);
 int launch_reduce_partials(const double2* partial, double2* alm, int ntiles, int B, int ncomp, int64_t nalm,
-                           double scale, int sms, cudaStream_t st);
+                           double scale, int bofs, int sms, cudaStream_t st);
 int launch_ring_synth_f64(const Plan& P, const int* d_list, int nrings, int work_len, const double2* phase,
                           double* map, int nf, cudaStream_t st);
 int launch_ring_adjoint_f64(const Plan& P, const int* d_list, int nrings, int work_len, const double* map,
                             double2* phase, int nf, cudaStream_t st);
+int launch_ring_synth_f32(const Plan& P, const int* d_list, int nrings, int work_len, const float2* phase,
+                          double* map, int nf, cudaStream_t st);
+int launch_ring_adjoint_f32(const Plan& P, const int* d_list, int nrings, int work_len, const double* map,
+                            float2* phase, int nf, cudaStream_t st);
+int launch_legendre_synth_tc(const Plan& P, const double2* almT, float2* phase, int B, int spin, int* err_flag,
+                             cudaStream_t st);
+int launch_legendre_adjoint_mx(const Plan& P, const float2* phase, float2* partial, int B, int bofs, int Bc,
+                               int spin, cudaStream_t st);
+int mx_adjoint_tiles(const Plan& P);
+int launch_reduce_partials_f32(const float2* partial, double2* alm, int ntiles, int B, int ncomp, int64_t nalm,
+                               double scale, int bofs, int sms, cudaStream_t st);
 }  // namespace ps
 
 struct ps_plan {
@@ -181,11 +192,14 @@ int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_pl
     max_fft = std::max(max_fft, w);
   }
   P.max_fft = max_fft;
-  if (prec == PS_PREC_FP64) {
+  {
+    // the FP64 ring transforms keep a ring's work array (max_fft complex values) in shared memory;
+    // the mixed-precision path uses FP32 work arrays (half the size)
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (size_t(max_fft) * sizeof(double2) > size_t(optin)) { delete pl; return PS_ERR_UNSUPPORTED; }
+    const size_t elem = (prec == PS_PREC_FP64) ? sizeof(double2) : sizeof(float2);
+    if (size_t(max_fft) * elem > size_t(optin)) { delete pl; return PS_ERR_UNSUPPORTED; }
   }
   std::vector<int> lists;
   for (auto& kv : classes) {
@@ -262,6 +276,15 @@ int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_pl
   for (int s = 1; s <= 3; ++s) if (!seeds[s].empty()) P.d_seed[s] = dev_upload(pl, seeds[s], err);
   P.d_twiddle = dev_upload(pl, tw, err);
   P.d_bs_spec = dev_upload(pl, bs_spec, err);
+  {
+    std::vector<float2> twf(tw.size()), bsf(bs_spec.size());
+    for (size_t i = 0; i < tw.size(); ++i) twf[i] = make_float2(float(tw[i].x), float(tw[i].y));
+    for (size_t i = 0; i < bs_spec.size(); ++i) bsf[i] = make_float2(float(bs_spec[i].x), float(bs_spec[i].y));
+    P.d_twiddle_f = dev_upload(pl, twf, err);
+    P.d_bs_spec_f = dev_upload(pl, bsf, err);
+    std::vector<int> zero(1, 0);
+    P.d_err = dev_upload(pl, zero, err);
+  }
   P.d_bs_off = dev_upload(pl, bs_off, err);
   pl->d_ring_lists = dev_upload(pl, lists, err);
   if (err != PS_OK) { ps_plan_destroy(pl); return err; }
@@ -276,6 +299,13 @@ int ps_plan_destroy(ps_plan* plan) {
   return PS_OK;
 }
 
+int ps_plan_error_flag(const ps_plan* plan, int* value, int reset) {
+  if (!plan || !value) return PS_ERR_INVALID;
+  if (cudaMemcpy(value, plan->p.d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return PS_ERR_CUDA;
+  if (reset && cudaMemset(plan->p.d_err, 0, sizeof(int)) != cudaSuccess) return PS_ERR_CUDA;
+  return PS_OK;
+}
+
 int ps_plan_info(const ps_plan* plan, int* nside, int* lmax, int64_t* npix, int64_t* nalm) {
   if (!plan) return PS_ERR_INVALID;
   if (nside) *nside = plan->p.nside;
@@ -285,11 +315,20 @@ int ps_plan_info(const ps_plan* plan, int* nside, int* lmax, int64_t* npix, int6
   return PS_OK;
 }
 
+// maps per Legendre-adjoint pass: the per-ring-tile partial sums of one pass
+// bound the adjoint's workspace independently of the batch size
+static int adjoint_chunk(const ps::Plan& P, int batch, int spin) {
+  const int c = (P.prec == PS_PREC_MIXED) ? (spin == 0 ? 16 : 8) : (spin == 0 ? 8 : 4);
+  return batch < c ? batch : c;
+}
+
 static size_t sht_ws_bytes(const ps::Plan& P, int batch, int spin, int adjoint) {
-  const size_t nf = size_t(batch) * (spin == 0 ? 1 : 2);
+  const size_t ncomp = spin == 0 ? 1 : 2;
+  const size_t nf = size_t(batch) * ncomp;
   const size_t phase = align256(size_t(P.R) * (P.mmax + 1) * nf * sizeof(double2));
   if (!adjoint) return align256(size_t(P.nalm) * nf * sizeof(double2)) + phase;
-  return phase + align256(size_t(ps::adjoint_tiles(P)) * P.nalm * nf * sizeof(double2));
+  const size_t nfc = size_t(adjoint_chunk(P, batch, spin)) * ncomp;
+  return phase + align256(size_t(ps::adjoint_tiles(P)) * P.nalm * nfc * sizeof(double2));
 }
 
 int ps_sht_workspace_bytes(const ps_plan* plan, int batch, int spin, int adjoint, size_t* bytes) {
@@ -305,13 +344,12 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
   if (!alm || !map || !workspace) return PS_ERR_INVALID;
   const ps::Plan& P = plan->p;
   if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
-  if (P.prec != PS_PREC_FP64) return PS_ERR_UNSUPPORTED;
   if (workspace_bytes < sht_ws_bytes(P, batch, spin, 0)) return PS_ERR_WORKSPACE;
   const int ncomp = spin == 0 ? 1 : 2;
   const int nf = batch * ncomp;
   char* ws = static_cast<char*>(workspace);
   double2* almT = reinterpret_cast<double2*>(ws);
-  double2* phase = reinterpret_cast<double2*>(ws + align256(size_t(P.nalm) * nf * sizeof(double2)));
+  char* phase_ptr = ws + align256(size_t(P.nalm) * nf * sizeof(double2));
   int rc;
   if (nf == 1) {
     almT = reinterpret_cast<double2*>(const_cast<double*>(alm));
@@ -319,6 +357,19 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
     rc = ps::launch_alm_to_T(reinterpret_cast<const double2*>(alm), almT, batch, ncomp, P.nalm, P.num_sms, stream);
     if (rc) return rc;
   }
+  if (P.prec == PS_PREC_MIXED) {
+    // tensor-core Legendre stage (TF32 x3, FP32 accumulation) and FP32 ring transforms
+    float2* phase = reinterpret_cast<float2*>(phase_ptr);
+    rc = ps::launch_legendre_synth_tc(P, almT, phase, batch, spin, P.d_err, stream);
+    if (rc) return rc;
+    for (size_t c = 0; c < plan->cls_len.size(); ++c) {
+      rc = ps::launch_ring_synth_f32(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c], plan->cls_len[c],
+                                     phase, map, nf, stream);
+      if (rc) return rc;
+    }
+    return PS_OK;
+  }
+  double2* phase = reinterpret_cast<double2*>(phase_ptr);
   rc = ps::launch_legendre_synth_f64(P, almT, phase, batch, spin, stream);
   if (rc) return rc;
   for (size_t c = 0; c < plan->cls_len.size(); ++c) {
@@ -336,24 +387,49 @@ int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, i
   if (!alm || !map || !workspace) return PS_ERR_INVALID;
   const ps::Plan& P = plan->p;
   if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
-  if (P.prec != PS_PREC_FP64) return PS_ERR_UNSUPPORTED;
   if (workspace_bytes < sht_ws_bytes(P, batch, spin, 1)) return PS_ERR_WORKSPACE;
   const int ncomp = spin == 0 ? 1 : 2;
   const int nf = batch * ncomp;
   char* ws = static_cast<char*>(workspace);
   const size_t phase_bytes = align256(size_t(P.R) * (P.mmax + 1) * nf * sizeof(double2));
+  int rc;
+  if (P.prec == PS_PREC_MIXED) {
+    // FP32 ring transforms, FP64 recurrences with FP32 contractions, FP64 cross-tile sums
+    float2* phase = reinterpret_cast<float2*>(ws);
+    float2* partial = reinterpret_cast<float2*>(ws + phase_bytes);
+    for (size_t c = 0; c < plan->cls_len.size(); ++c) {
+      rc = ps::launch_ring_adjoint_f32(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c],
+                                       plan->cls_len[c], map, phase, nf, stream);
+      if (rc) return rc;
+    }
+    const int ch = adjoint_chunk(P, batch, spin);
+    for (int b0 = 0; b0 < batch; b0 += ch) {
+      const int bc = std::min(ch, batch - b0);
+      rc = ps::launch_legendre_adjoint_mx(P, phase, partial, batch, b0, bc, spin, stream);
+      if (rc) return rc;
+      rc = ps::launch_reduce_partials_f32(partial, reinterpret_cast<double2*>(alm), ps::mx_adjoint_tiles(P), bc,
+                                          ncomp, P.nalm, scale, b0, P.num_sms, stream);
+      if (rc) return rc;
+    }
+    return PS_OK;
+  }
   double2* phase = reinterpret_cast<double2*>(ws);
   double2* partial = reinterpret_cast<double2*>(ws + phase_bytes);
-  int rc;
   for (size_t c = 0; c < plan->cls_len.size(); ++c) {
     rc = ps::launch_ring_adjoint_f64(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c], plan->cls_len[c],
                                      map, phase, nf, stream);
     if (rc) return rc;
   }
-  rc = ps::launch_legendre_adjoint_f64(P, phase, partial, batch, spin, stream);
-  if (rc) return rc;
-  return ps::launch_reduce_partials(partial, reinterpret_cast<double2*>(alm), ps::adjoint_tiles(P), batch, ncomp,
-                                    P.nalm, scale, P.num_sms, stream);
+  const int ch = adjoint_chunk(P, batch, spin);
+  for (int b0 = 0; b0 < batch; b0 += ch) {
+    const int bc = std::min(ch, batch - b0);
+    rc = ps::launch_legendre_adjoint_f64(P, phase, partial, batch, b0, bc, spin, stream);
+    if (rc) return rc;
+    rc = ps::launch_reduce_partials(partial, reinterpret_cast<double2*>(alm), ps::adjoint_tiles(P), bc, ncomp,
+                                    P.nalm, scale, b0, P.num_sms, stream);
+    if (rc) return rc;
+  }
+  return PS_OK;
 }
 
 }  // extern "C"

@@ -51,6 +51,12 @@ class SHTPlan:
             _lib.lib().ps_plan_destroy(h)
             self._h = None
 
+    def error_flag(self, reset=True):
+        """Device error flag of the plan (set by a kernel whose bounded wait expired)."""
+        v = ctypes.c_int()
+        _lib.call("ps_plan_error_flag", self._h, ctypes.byref(v), int(reset))
+        return int(v.value)
+
     # ------------------------------------------------------------ workspace
     def workspace(self, batch, spin, adjoint):
         n = ctypes.c_size_t()
