@@ -9,6 +9,12 @@ test, polyspec/weighting.py:336-347), at most 500 steps; white noise of
 30 uK arcmin; mask = |lat| < 5.74 deg plus 500 point-source holes of 10'.
 One step = one PSpecBin.compute_fisher_contribution (polyspec/pspec_bin.py:94-164):
 a GRF, 33 masked syntheses and 33 CG solves, and the N_p x N_p Fisher GEMM.
+The CUDA arm solves the 33 systems as one batch (BatchedCGD: every A and M
+application is one batched SHT pair of 33 maps per spin).  ``--prec mixed``
+(default) runs the tensor-core / FP32 SHTs; the line also carries one step of
+the plain FP64 GPU backend on the same workload (``plain_fp64_gpu``) and the
+relative error of the mixed backend's binned spectra against FP64 at a fixed
+CG step count (``accuracy``).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference] [--prec fp64|mixed]
 
@@ -34,8 +40,11 @@ FIELDS = ("TT", "TE", "EE", "BB")
 THRESH = 1e-6
 NSTEP = 500
 # CG steps per solve the plain harmonic-preconditioned CG takes on this workload
-# (the CUDA arm reports its own count as cg_iters_per_solve)
-PLAIN_CG_ITERS = 6
+# (measured by the FP64 CUDA arm, one solve at a time: 17.45; the algorithm and its
+# stopping rule are the reference's, so the reference takes the same count)
+PLAIN_CG_ITERS = 17.5
+# fixed CG step count of the accuracy comparison (mixed vs FP64 binned spectra)
+ACC_CG_STEPS = 20
 
 
 def parse():
@@ -44,7 +53,9 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
-    p.add_argument("--prec", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--prec", default="mixed", choices=["fp64", "mixed"])
+    p.add_argument("--unbatched", action="store_true", help="one CG solve at a time (reference structure)")
+    p.add_argument("--no-fp64-compare", action="store_true")
     p.add_argument("--nside", type=int, default=1024)
     p.add_argument("--lmax", type=int, default=2048)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -169,6 +180,62 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------- plain FP64 GPU + accuracy
+def fp64_compare(a, setup, seed):
+    """One Fisher step of the plain FP64 GPU backend (same batched structure,
+    same stopping rule), and the relative error of the mixed backend's binned
+    spectra (Cl_numerator of one masked GRF map) against FP64 with both CG
+    solves run for ACC_CG_STEPS steps, which isolates arithmetic error from the
+    stopping test."""
+    import torch
+    from polyspec_b200 import PolySpec, Weightings, PSpecBin
+    cl, cltot, beam, mask, noise, l_bins = setup
+    out = {}
+
+    def build(prec, nstep, thresh):
+        b = PolySpec(a.nside, dict(cltot), beam=list(beam), pol=True, lmax=a.lmax, prec=prec)
+        w = Weightings(b, mask, dict(cl), noise_cov=noise)
+        ap = w.make_applySinv("optimal", preconditioner="harmonic", nstep=nstep, thresh=thresh)
+        return b, PSpecBin(b, mask, ap, l_bins, fields=list(FIELDS))
+
+    b64, p64 = build("fp64", NSTEP, THRESH)
+    a_lm = b64.generate_data(seed=seed + int(2e7), output_type="harmonic", deconvolve_beam=True, rng="device")
+    b64.to_map(a_lm)  # plan set-up outside the timed region
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    p64.compute_fisher_contribution(seed, a_lm=a_lm, batched=not a.unbatched)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    plain = {"value": 1e3 / ms, "unit": UNIT, "ms_per_step": ms, "steps": 1, "dtype": "f64",
+             "note": "plain FP64 GPU backend (FP64 Legendre + FP64 ring FFTs), same batched CG and stopping rule"}
+    del p64
+    torch.cuda.empty_cache()
+
+    mask_t = torch.as_tensor(np.asarray(mask), device="cuda")
+    data = b64.generate_data(seed=seed + 7, output_type="map", rng="device") * mask_t
+    nums = {}
+    for prec in ("fp64", "mixed"):
+        b, p = build(prec, ACC_CG_STEPS, 0.0)
+        num = p.Cl_numerator(data)
+        nums[prec] = num.cpu().numpy() if isinstance(num, torch.Tensor) else np.asarray(num)
+        del b, p
+        torch.cuda.empty_cache()
+    n64, nmx = nums["fp64"], nums["mixed"]
+    # per field: max over bins of |d| / |C_fp64|; cross spectra (TE) also normalised by sqrt(TT EE)
+    per_field = {f: float(np.max(np.abs(nmx[i] - n64[i]) / np.abs(n64[i]))) for i, f in enumerate(FIELDS)}
+    iTT, iTE, iEE = FIELDS.index("TT"), FIELDS.index("TE"), FIELDS.index("EE")
+    te_norm = float(np.max(np.abs(nmx[iTE] - n64[iTE]) / np.sqrt(np.abs(n64[iTT] * n64[iEE]))))
+    acc = {"binned_cl_max_rel_err": float(np.max(np.abs(nmx - n64) / np.abs(n64))),
+           "binned_cl_rel_l2_err": float(np.linalg.norm(nmx - n64) / np.linalg.norm(n64)),
+           "max_rel_err_per_field": per_field, "TE_err_over_sqrt_TT_EE": te_norm,
+           "tolerance": 1e-6, "cg_steps": ACC_CG_STEPS,
+           "what": "PSpecBin.Cl_numerator (TT, TE, EE, BB x 8 bins) of one masked GRF map, mixed vs FP64 backend, "
+                   "same fixed CG step count"}
+    return plain, acc
+
+
 # ---------------------------------------------------------------------- CUDA arm
 def run_cuda(a):
     import torch
@@ -186,7 +253,7 @@ def run_cuda(a):
 
     setup = Wl.cg_fisher_setup(a.nside, a.lmax)
     cl, cltot, beam, mask, noise, l_bins = setup
-    base = PolySpec(a.nside, dict(cltot), beam=list(beam), pol=True, lmax=a.lmax)
+    base = PolySpec(a.nside, dict(cltot), beam=list(beam), pol=True, lmax=a.lmax, prec=a.prec)
     wts = Weightings(base, mask, dict(cl), noise_cov=noise)
     applySinv = wts.make_applySinv("optimal", preconditioner="harmonic", nstep=NSTEP, thresh=THRESH)
     psb = PSpecBin(base, mask, applySinv, l_bins, fields=list(FIELDS))
@@ -198,11 +265,14 @@ def run_cuda(a):
     torch.cuda.synchronize()
 
     cg_iters = []
+    solve_iters = []
 
     def one(i, a_lm):
         it0 = base.n_SHTs_forward
-        f = psb.compute_fisher_contribution(seeds[i], a_lm=a_lm)
+        f = psb.compute_fisher_contribution(seeds[i], a_lm=a_lm, batched=not a.unbatched)
         cg_iters.append(base.n_SHTs_forward - it0)
+        if not a.unbatched and getattr(wts, "last_cgd", None) is not None:
+            solve_iters.append([int(v) for v in wts.last_cgd.iters.cpu()])
         return f
 
     for i in range(a.warmup):
@@ -248,7 +318,8 @@ def run_cuda(a):
     e0.record()
     t0 = time.time()
     for k in range(a.steps):
-        fish = psb.compute_fisher_contribution(seeds[a.warmup + a.steps + k], a_lm=host_a[k])
+        fish = psb.compute_fisher_contribution(seeds[a.warmup + a.steps + k], a_lm=host_a[k],
+                                               batched=not a.unbatched)
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = max(e0.elapsed_time(e1), (time.time() - t0) * 1e3)
@@ -272,12 +343,23 @@ def run_cuda(a):
     if fl > 0:
         ach = fl / (ms / 1e3) / 1e12
         peak = peaks.get("bf16_tflops", 1590.0)
+        sm_ghz = (clocks.get("sm_mhz") or 1965.0) / 1e3
+        if a.prec == "fp64":
+            pipe, pipe_peak = "FP64 FMA pipe (64 DFMA/clk/SM)", 64 * 2 * 148 * sm_ghz / 1e3
+        elif dom == "leg_synth":
+            # three TF32 MMAs per product (hi.hi + hi.lo + lo.hi): the algorithmic flops are a third of
+            # the tensor-pipe flops; dense TF32 runs at half the bf16 rate
+            pipe, pipe_peak = "tensor pipe, kind::tf32 (x3 split)", peak / 2 / 3
+        else:
+            pipe, pipe_peak = "FP32 FMA pipe (128 FFMA/clk/SM)", 128 * 2 * 148 * sm_ghz / 1e3
         roof = {"bound": "tensor", "kernel": dom, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                "frac": ach / peak, "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback",
-                "fp64_peak_tflops": 36.7, "frac_of_fp64_peak": ach / 36.7,
+                "frac": ach / peak,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), of measured" if peaks else "fallback",
+                "pipe": pipe, "pipe_peak_tflops": pipe_peak, "frac_of_pipe_peak": ach / pipe_peak,
                 "launches": n, "avg_launch_ms": ms / max(n, 1), "traffic": None,
-                "note": "FP64 CUDA-core Legendre kernel: the FP64 FMA pipe (64 DFMA/clk/SM x 148 SMs x 1.94 GHz "
-                        "= 36.7 TFLOP/s) bounds it; the bf16 tensor peak is the contract's denominator"}
+                "algorithmic_flops_per_launch": fl / max(n, 1),
+                "note": "achieved = algorithmic Legendre flops (4 per ring pair, alm and map for spin 0, 16 for a "
+                        "spin-s pair) / CUDA-event time of the kernel inside the timed region"}
     else:
         ach = by / (ms / 1e3) / 1e9 if ms > 0 else 0.0
         peak = peaks.get("hbm_gbs", 6650.0)
@@ -295,7 +377,14 @@ def run_cuda(a):
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clocks,
             "sht_teb_per_step": {"synthesis": rev / 2.0, "adjoint": fwd / 2.0},
             "cg_iters_per_solve": iters_per_solve,
+            "cg_iters_of_each_solve": solve_iters[-1] if solve_iters else None,
             "kernel_ms": {k: round(v[1], 3) for k, v in stats.items() if v[0]}}
+
+    if a.prec != "fp64" and not a.no_fp64_compare:
+        del psb, applySinv, wts, a_dev, base
+        torch.cuda.empty_cache()
+        line["plain_fp64_gpu"], line["accuracy"] = fp64_compare(a, setup, seeds[0])
+        torch.cuda.empty_cache()
 
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         t_pair, cores = cpu_pair_time(a, setup, a.cpu_sample_pairs)

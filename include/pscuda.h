@@ -95,6 +95,83 @@ int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, i
 int ps_synthesis_noalloc(const ps_plan* plan, const double* alm, double* map, int batch, int spin,
                          cudaStream_t stream);
 
+/* ---------------------------------------------------- pixel-space products
+ * Elementwise products of maps of n elements (real = float64, complex =
+ * complex128, all contiguous), the per-element products of the reference's
+ * Cython kernels, which take [N_r, Npix] arrays and return fresh ones:
+ *   op                          inputs (in order)              out   reference
+ *   PS_PIX_MULTIPLY             R1 R2 R3                       R     tauNL_utils.pyx:103-113
+ *   PS_PIX_MULTIPLY_ASYM        R1A R1B R3A R3B                R     tauNL_utils.pyx:116-126
+ *   PS_PIX_MULTIPLYC            R1 R2 C3                       C     tauNL_utils.pyx:129-139
+ *   PS_PIX_MULTIPLYC_ASYM       R1A R1B C3A C3B                C     tauNL_utils.pyx:142-152
+ *   PS_PIX_MULTIPLYCC           R1 R2 C3                       R     tauNL_utils.pyx:155-165
+ *   PS_PIX_MULTIPLYCC_ASYM      R1A R1B R2A R2B C3A C3B        R     tauNL_utils.pyx:168-178
+ *   PS_PIX_MULTIPLY2            B1 B2 C1 C2                    R     tauNL_utils.pyx:181-191
+ *   PS_PIX_MULTIPLY2R           A B                            R     tauNL_utils.pyx:194-204
+ *   PS_PIX_MULTIPLY2C           Ac B                           C     tauNL_utils.pyx:207-217
+ *   PS_PIX_MULTIPLYRC           R C                            C     ideal_fisher.pyx:52-60
+ *   PS_PIX_MULTIPLYRCSTAR       R C          (fac)             C     ideal_fisher.pyx:64-72
+ *   PS_PIX_MULTIPLYRC_SYM       R C R2 C2                      C     ideal_fisher.pyx:76-84
+ *   PS_PIX_MULTIPLYRCSTAR_SYM   R C R2 C2    (fac)             C     ideal_fisher.pyx:88-96
+ *   PS_PIX_MULTIPLYRR           R1 R2                          R     ideal_fisher.pyx:100-108
+ *   PS_PIX_MULTIPLYRR_SYM       R1 R2 R1b R2b                  R     ideal_fisher.pyx:112-120
+ *   PS_PIX_R2C / PS_PIX_R2CSTAR re im                          C     ideal_fisher.pyx:18-38
+ *   PS_PIX_LENS_PHI             U V ([npol][n] complex each)   C[n]  ideal_fisher.pyx:124-139
+ *   PS_PIX_LENS_PHI_SYM         U1 U2 V1 V2                    C[n]  ideal_fisher.pyx:142-157
+ * npol is 1 or 3 for the lensing sums and 1 otherwise; fac is used by the
+ * *STAR products.  The reference's nthreads argument has no counterpart. */
+enum {
+  PS_PIX_MULTIPLY = 0, PS_PIX_MULTIPLY_ASYM, PS_PIX_MULTIPLYC, PS_PIX_MULTIPLYC_ASYM, PS_PIX_MULTIPLYCC,
+  PS_PIX_MULTIPLYCC_ASYM, PS_PIX_MULTIPLY2, PS_PIX_MULTIPLY2R, PS_PIX_MULTIPLY2C, PS_PIX_MULTIPLYRC,
+  PS_PIX_MULTIPLYRCSTAR, PS_PIX_MULTIPLYRC_SYM, PS_PIX_MULTIPLYRCSTAR_SYM, PS_PIX_MULTIPLYRR,
+  PS_PIX_MULTIPLYRR_SYM, PS_PIX_R2C, PS_PIX_R2CSTAR, PS_PIX_LENS_PHI, PS_PIX_LENS_PHI_SYM, PS_PIX_NOPS
+};
+int ps_pix_product(int op, const void* const* inputs, int n_inputs, void* out, int64_t n, int npol, double fac,
+                   cudaStream_t stream);
+
+/* Radial pixel sums  *out = Sum_r w_r tau_r^k Sum_pix f(maps[r][pix])  over maps
+ * [nr][npix] (tauNL_utils.pyx:260-405; device scalar out).  tau is read by the
+ * DOTDOT (k = 4) and DOTDEL (k = 2) kinds only.  Partial sums are added in a
+ * fixed order, so repeated calls give identical results.
+ *   PS_SUM_GNL_LOC          P Q                      P^3 Q
+ *   PS_SUM_GNL_LOC_DISC     P1 P2 Q1 Q2              P1^2 P2 Q2 + P2^2 P1 Q1
+ *   PS_SUM_GNL_CON          R                        R^4
+ *   PS_SUM_GNL_CON_DISC     R1 R2                    R1^2 R2^2
+ *   PS_SUM_GNL_DOTDOT       A                        tau^4 A^4
+ *   PS_SUM_GNL_DOTDOT_DISC  A1 A2                    tau^4 A1^2 A2^2
+ *   PS_SUM_GNL_DOTDEL       A B C(complex)           tau^2 A^2 (B^2 + |C|^2)
+ *   PS_SUM_GNL_DOTDEL_DISC  A1 A2 B1 B2 C1 C2        tau^2 A1 A2 (B1 B2 + Re C1 C2*)
+ *   PS_SUM_GNL_DELDEL       B C                      (B^2 + |C|^2)^2
+ *   PS_SUM_GNL_DELDEL_DISC  B1 B2 B3 B4 C1 C2 C3 C4  (B1 B2 + Re C1 C2*)(B3 B4 + Re C3 C4*) */
+enum {
+  PS_SUM_GNL_LOC = 0, PS_SUM_GNL_LOC_DISC, PS_SUM_GNL_CON, PS_SUM_GNL_CON_DISC, PS_SUM_GNL_DOTDOT,
+  PS_SUM_GNL_DOTDOT_DISC, PS_SUM_GNL_DOTDEL, PS_SUM_GNL_DOTDEL_DISC, PS_SUM_GNL_DELDEL, PS_SUM_GNL_DELDEL_DISC,
+  PS_SUM_NKINDS
+};
+int ps_pix_radial_sum_workspace_bytes(int nr, int64_t npix, size_t* bytes);
+int ps_pix_radial_sum(int kind, const double* r_weights, const double* tau, const void* const* maps, int n_maps,
+                      int nr, int64_t npix, double* out, void* workspace, size_t workspace_bytes,
+                      cudaStream_t stream);
+
+/* out[r][lm] = weight Sum_X flX[l][X][r] h_lm[X][lm], l = ls[lm]  (complex128 h_lm
+ * [npol][nlm], out [nr][nlm]; npol 1 or 2; tauNL_utils.pyx:80-98).  flX is
+ * [lsize][npol][nr]; an lm whose l lies outside [0, lsize) gets zeros. */
+int ps_apply_fl_weights(const double* flX, int lsize, int npol, int nr, const double* h_lm, const int* ls,
+                        int64_t nlm, double weight, double* out, cudaStream_t stream);
+/* out[X][lm] = Sum_r lm_map[r][lm] flXs[l][X][r] w_r (tauNL_utils.pyx:220-237); with
+ * spin1 != 0, lm_map is [2][nr][nlm] and the sum runs over (lm_map[0] - lm_map[1]) / 2
+ * (radial_sum_spin1, tauNL_utils.pyx:240-255).  Complex128 lm_map and out. */
+int ps_radial_sum_lm(const double* lm_map, int spin1, const double* r_weights, const double* flXs, int lsize,
+                     int npol, int nr, const int* ls, int64_t nlm, double* out, cudaStream_t stream);
+
+/* Fisher outer product of two Q4 arrays, complex128 [4][na][nin] and [4][nb][nin]:
+ * fish[a][b] = Re Sum_j (Qa0* Qb0 + Qa1* Qb1 + 9 (Qa2* Qb2 + Qa3* Qb3)
+ *                        - 3 (Qa0* Qb3 + Qa1* Qb2 + Qa3* Qb0 + Qa2* Qb1)) / (24 * 48)
+ * (outer_product, ideal_fisher.pyx:423-460; sym: square, upper triangle mirrored). */
+int ps_outer_product_workspace_bytes(int na, int nb, int64_t nin, size_t* bytes);
+int ps_outer_product(const double* Qa, const double* Qb, int na, int nb, int64_t nin, int sym, double* fish,
+                     void* workspace, size_t workspace_bytes, cudaStream_t stream);
+
 /* ------------------------------------------------------------- launch statistics
  * No reference counterpart beyond its wall-clock SHT timer (polyspec/base.py:113-127,
  * polyspec/tspec_template.py:453-517): every kernel launch of the library is

@@ -34,11 +34,30 @@ SIGNATURES = {
     "ps_adjoint": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_double, _c_void_p,
                             _c_size_t, _c_void_p]),
     "ps_synthesis_noalloc": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p]),
+    "ps_pix_product": (_c_int, [_c_int, ctypes.POINTER(_c_void_p), _c_int, _c_void_p, _c_int64, _c_int, _c_double,
+                                _c_void_p]),
+    "ps_pix_radial_sum_workspace_bytes": (_c_int, [_c_int, _c_int64, ctypes.POINTER(_c_size_t)]),
+    "ps_pix_radial_sum": (_c_int, [_c_int, _c_void_p, _c_void_p, ctypes.POINTER(_c_void_p), _c_int, _c_int, _c_int64,
+                                   _c_void_p, _c_void_p, _c_size_t, _c_void_p]),
+    "ps_apply_fl_weights": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, _c_void_p, _c_void_p, _c_int64, _c_double,
+                                     _c_void_p, _c_void_p]),
+    "ps_radial_sum_lm": (_c_int, [_c_void_p, _c_int, _c_void_p, _c_void_p, _c_int, _c_int, _c_int, _c_void_p,
+                                  _c_int64, _c_void_p, _c_void_p]),
+    "ps_outer_product_workspace_bytes": (_c_int, [_c_int, _c_int, _c_int64, ctypes.POINTER(_c_size_t)]),
+    "ps_outer_product": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_int64, _c_int, _c_void_p, _c_void_p,
+                                  _c_size_t, _c_void_p]),
     "ps_stats_enable_timing": (_c_int, [_c_int]),
     "ps_stats_reset": (_c_int, []),
     "ps_stats_get": (_c_int, [_c_int, ctypes.POINTER(_c_int64), ctypes.POINTER(_c_double),
                               ctypes.POINTER(_c_double), ctypes.POINTER(_c_double)]),
 }
+
+# pixel-product ops and radial-sum kinds (enums of include/pscuda.h, in order)
+PIX_OPS = ["multiply", "multiply_asym", "multiplyC", "multiplyC_asym", "multiplyCC", "multiplyCC_asym", "multiply2",
+           "multiply2R", "multiply2C", "multiplyRC", "multiplyRCstar", "multiplyRC_sym", "multiplyRCstar_sym",
+           "multiplyRR", "multiplyRR_sym", "r2c", "r2cstar", "lens_phi_sum", "lens_phi_sum_sym"]
+SUM_KINDS = ["gnl_loc_sum", "gnl_loc_disc_sum", "gnl_con_sum", "gnl_con_disc_sum", "gnl_dotdot_sum",
+             "gnl_dotdot_disc_sum", "gnl_dotdel_sum", "gnl_dotdel_disc_sum", "gnl_deldel_sum", "gnl_deldel_disc_sum"]
 
 KERNEL_KINDS = {"leg_synth": 0, "leg_adjoint": 1, "fft_synth": 2, "fft_adjoint": 3, "layout": 4, "pixel": 5,
                 "vector": 6, "mlp": 7}

@@ -1,0 +1,292 @@
+"""Pixel-space products, radial sums and harmonic weightings on the GPU.
+
+Mirrors the reference's Cython kernels with the same names and argument
+meaning:
+
+* ``tauNL_utils`` -- the class of polyspec/cython/tauNL_utils.pyx:21-405
+  (``apply_fl_weights``, the ``multiply*`` products, ``radial_sum(_spin1)``
+  and the ``gnl_*`` radial pixel sums);
+* module functions ``r2c``, ``r2cstar``, ``multiplyRC(star)(_sym)``,
+  ``multiplyRR(_sym)``, ``lens_phi_sum(_sym)`` and ``outer_product`` of
+  polyspec/cython/ideal_fisher.pyx:18-460.
+
+Arrays may be numpy arrays (copied to the device; results come back as numpy
+arrays, as the reference returns them) or CUDA tensors (results stay CUDA
+tensors).  The ``nthreads`` arguments are accepted and ignored.  Every call
+runs a libpscuda kernel; there is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_OP = {name: i for i, name in enumerate(_lib.PIX_OPS)}
+_SUM = {name: i for i, name in enumerate(_lib.SUM_KINDS)}
+
+
+def _dev():
+    if not torch.cuda.is_available():
+        raise RuntimeError("the CUDA backend needs a GPU (no CPU fallback)")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _prep(x, dtype):
+    """CUDA tensor of `dtype` (contiguous) and whether the caller passed torch tensors."""
+    if isinstance(x, torch.Tensor):
+        return x.to(device=_dev() if not x.is_cuda else x.device, dtype=dtype).contiguous(), True
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype, device=_dev()), False
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptrs(ts):
+    arr = (ctypes.c_void_p * max(len(ts), 1))()
+    for i, t in enumerate(ts):
+        arr[i] = t.data_ptr()
+    return arr
+
+
+def _ret(t, as_torch):
+    return t if as_torch else t.cpu().numpy()
+
+
+def _product(op, args, kinds, out_complex, fac=0.0, npol=1, out_shape=None):
+    """Run elementwise product `op` over inputs of identical shape ('r' float64, 'c' complex128)."""
+    ts, flags = [], []
+    for a, k in zip(args, kinds):
+        t, f = _prep(a, torch.complex128 if k == "c" else torch.float64)
+        ts.append(t)
+        flags.append(f)
+    shape = ts[0].shape
+    for t in ts[1:]:
+        if t.shape != shape:
+            raise ValueError("all maps of a product must have the same shape")
+    if out_shape is None:
+        out_shape = shape
+        n = ts[0].numel()
+    else:
+        n = int(np.prod(out_shape))
+    out = torch.empty(out_shape, dtype=torch.complex128 if out_complex else torch.float64, device=ts[0].device)
+    _lib.call("ps_pix_product", _OP[op], _ptrs(ts), len(ts), ctypes.c_void_p(out.data_ptr()), n, npol,
+              float(fac), _stream())
+    return _ret(out, all(flags))
+
+
+def _radial_sum(kind, r_weights, tau, maps, kinds):
+    ts, flags = [], []
+    for a, k in zip(maps, kinds):
+        t, f = _prep(a, torch.complex128 if k == "c" else torch.float64)
+        ts.append(t)
+        flags.append(f)
+    nr, npix = ts[0].shape
+    for t in ts[1:]:
+        if tuple(t.shape) != (nr, npix):
+            raise ValueError("all maps of a radial sum must have shape [nr, npix]")
+    w, _ = _prep(r_weights, torch.float64)
+    if w.numel() < nr:
+        raise ValueError("r_weights shorter than the number of radial samples")
+    tt = None
+    if tau is not None:
+        tt, _ = _prep(tau, torch.float64)
+    nb = ctypes.c_size_t()
+    _lib.call("ps_pix_radial_sum_workspace_bytes", nr, npix, ctypes.byref(nb))
+    ws = torch.empty(max(int(nb.value), 8), dtype=torch.uint8, device=ts[0].device)
+    out = torch.empty(1, dtype=torch.float64, device=ts[0].device)
+    _lib.call("ps_pix_radial_sum", _SUM[kind], ctypes.c_void_p(w.data_ptr()),
+              ctypes.c_void_p(tt.data_ptr() if tt is not None else 0), _ptrs(ts), len(ts), nr, npix,
+              ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), int(nb.value), _stream())
+    return float(out.item())
+
+
+class tauNL_utils:
+    """GPU mirror of polyspec/cython/tauNL_utils.pyx:21-78 (constructor) and its kernels.
+
+    Only ``ls`` (the l of every lm of the harmonic arrays) enters the kernels
+    built here; the other constructor arguments are kept for the interface.
+    """
+
+    def __init__(self, nthreads, nr, l_arr, m_arr, Lmin, Lmax, ls, ms, Ls, Ms, nmax_F):
+        self.nthreads = nthreads
+        self.nr = int(nr)
+        self.l_arr = np.asarray(l_arr, dtype=np.int32)
+        self.m_arr = np.asarray(m_arr, dtype=np.int32)
+        self.Lmin, self.Lmax = int(Lmin), int(Lmax)
+        self.ls = np.asarray(ls, dtype=np.int32)
+        self.ms = np.asarray(ms, dtype=np.int32)
+        self.Ls = np.asarray(Ls, dtype=np.int32)
+        self.Ms = np.asarray(Ms, dtype=np.int32)
+        self.nmax_F = nmax_F
+        self.lmin, self.lmax = int(self.ls.min()), int(self.ls.max())
+        self._d_ls = torch.as_tensor(self.ls, device=_dev())
+
+    # ---------------------------------------------------------------- harmonic weightings
+    def apply_fl_weights(self, flX, h_lm, weight):
+        """out[r, lm] = weight Sum_X flX[l, X, r] h_lm[X, lm]   (tauNL_utils.pyx:80-98)."""
+        f, as_torch = _prep(flX, torch.float64)
+        h, _ = _prep(h_lm, torch.complex128)
+        lsize, npol, nr = f.shape
+        nlm = h.shape[1]
+        if nlm > len(self.ls) or h.shape[0] < npol:
+            raise ValueError("h_lm does not match flX / ls")
+        out = torch.empty((nr, nlm), dtype=torch.complex128, device=h.device)
+        _lib.call("ps_apply_fl_weights", ctypes.c_void_p(f.data_ptr()), lsize, npol, nr,
+                  ctypes.c_void_p(h.data_ptr()), ctypes.c_void_p(self._d_ls.data_ptr()), nlm, float(weight),
+                  ctypes.c_void_p(out.data_ptr()), _stream())
+        return _ret(out, as_torch)
+
+    def _radial(self, lm_map, r_weights, flXs, spin1):
+        m, as_torch = _prep(lm_map, torch.complex128)
+        w, _ = _prep(r_weights, torch.float64)
+        f, _ = _prep(flXs, torch.float64)
+        lsize, npol, nrf = f.shape
+        nr, nlm = (m.shape[1], m.shape[2]) if spin1 else (m.shape[0], m.shape[1])
+        if nr > nrf or w.numel() < nr or nlm > len(self.ls):
+            raise ValueError("lm_map does not match r_weights / flXs / ls")
+        if nrf != nr:  # the kernel indexes flXs[l][X][r] with the map's radial count
+            f = f[:, :, :nr].contiguous()
+        out = torch.empty((npol, nlm), dtype=torch.complex128, device=m.device)
+        _lib.call("ps_radial_sum_lm", ctypes.c_void_p(m.data_ptr()), int(spin1), ctypes.c_void_p(w.data_ptr()),
+                  ctypes.c_void_p(f.data_ptr()), lsize, npol, nr, ctypes.c_void_p(self._d_ls.data_ptr()), nlm,
+                  ctypes.c_void_p(out.data_ptr()), _stream())
+        return _ret(out, as_torch)
+
+    def radial_sum(self, lm_map, r_weights, flXs):
+        """out[X, lm] = Sum_r lm_map[r, lm] flXs[l, X, r] w_r   (tauNL_utils.pyx:220-237)."""
+        return self._radial(lm_map, r_weights, flXs, False)
+
+    def radial_sum_spin1(self, lm_map, r_weights, flXs):
+        """out[X, lm] = 1/2 Sum_r (lm_map[0, r, lm] - lm_map[1, r, lm]) flXs[l, X, r] w_r  (:240-255)."""
+        return self._radial(lm_map, r_weights, flXs, True)
+
+    # ---------------------------------------------------------------- map products
+    def multiply(self, map1, map2, map3):
+        return _product("multiply", (map1, map2, map3), "rrr", False)
+
+    def multiply_asym(self, map1A, map1B, map3A, map3B):
+        return _product("multiply_asym", (map1A, map1B, map3A, map3B), "rrrr", False)
+
+    def multiplyC(self, map1, map2, map3c):
+        return _product("multiplyC", (map1, map2, map3c), "rrc", True)
+
+    def multiplyC_asym(self, map1A, map1B, map3cA, map3cB):
+        return _product("multiplyC_asym", (map1A, map1B, map3cA, map3cB), "rrcc", True)
+
+    def multiplyCC(self, map1, map2, map3c):
+        return _product("multiplyCC", (map1, map2, map3c), "rrc", False)
+
+    def multiplyCC_asym(self, map1A, map1B, map2A, map2B, map3cA, map3cB):
+        return _product("multiplyCC_asym", (map1A, map1B, map2A, map2B, map3cA, map3cB), "rrrrcc", False)
+
+    def multiply2(self, B1, B2, C1, C2):
+        return _product("multiply2", (B1, B2, C1, C2), "rrcc", False)
+
+    def multiply2R(self, A, B):
+        return _product("multiply2R", (A, B), "rr", False)
+
+    def multiply2C(self, Ac, B):
+        return _product("multiply2C", (Ac, B), "cr", True)
+
+    # ---------------------------------------------------------------- radial pixel sums
+    def gnl_loc_sum(self, r_weights, P_maps, Q_maps):
+        return _radial_sum("gnl_loc_sum", r_weights, None, (P_maps, Q_maps), "rr")
+
+    def gnl_loc_disc_sum(self, r_weights, P_maps1, P_maps2, Q_maps1, Q_maps2):
+        return _radial_sum("gnl_loc_disc_sum", r_weights, None, (P_maps1, P_maps2, Q_maps1, Q_maps2), "rrrr")
+
+    def gnl_con_sum(self, r_weights, R_maps):
+        return _radial_sum("gnl_con_sum", r_weights, None, (R_maps,), "r")
+
+    def gnl_con_disc_sum(self, r_weights, R_maps1, R_maps2):
+        return _radial_sum("gnl_con_disc_sum", r_weights, None, (R_maps1, R_maps2), "rr")
+
+    def gnl_dotdot_sum(self, rtau_weights, tau_arr, A_maps):
+        return _radial_sum("gnl_dotdot_sum", rtau_weights, tau_arr, (A_maps,), "r")
+
+    def gnl_dotdot_disc_sum(self, rtau_weights, tau_arr, A_maps1, A_maps2):
+        return _radial_sum("gnl_dotdot_disc_sum", rtau_weights, tau_arr, (A_maps1, A_maps2), "rr")
+
+    def gnl_dotdel_sum(self, rtau_weights, tau_arr, A_maps, B_maps, C_maps):
+        return _radial_sum("gnl_dotdel_sum", rtau_weights, tau_arr, (A_maps, B_maps, C_maps), "rrc")
+
+    def gnl_dotdel_disc_sum(self, rtau_weights, tau_arr, A_maps1, A_maps2, B_maps1, B_maps2, C_maps1, C_maps2):
+        return _radial_sum("gnl_dotdel_disc_sum", rtau_weights, tau_arr,
+                           (A_maps1, A_maps2, B_maps1, B_maps2, C_maps1, C_maps2), "rrrrcc")
+
+    def gnl_deldel_sum(self, rtau_weights, B_maps, C_maps):
+        return _radial_sum("gnl_deldel_sum", rtau_weights, None, (B_maps, C_maps), "rc")
+
+    def gnl_deldel_disc_sum(self, rtau_weights, B1_maps, B2_maps, B3_maps, B4_maps, C1_maps, C2_maps, C3_maps,
+                            C4_maps):
+        return _radial_sum("gnl_deldel_disc_sum", rtau_weights, None,
+                           (B1_maps, B2_maps, B3_maps, B4_maps, C1_maps, C2_maps, C3_maps, C4_maps), "rrrrcccc")
+
+
+# -------------------------------------------------------------------- ideal_fisher.pyx mirrors
+def r2c(re_arr, im_arr, nthreads=0):
+    return _product("r2c", (re_arr, im_arr), "rr", True)
+
+
+def r2cstar(re_arr, im_arr, nthreads=0):
+    return _product("r2cstar", (re_arr, im_arr), "rr", True)
+
+
+def multiplyRC(arrR, arrC, nthreads=0):
+    return _product("multiplyRC", (arrR, arrC), "rc", True)
+
+
+def multiplyRCstar(arrR, arrC, fac, nthreads=0):
+    return _product("multiplyRCstar", (arrR, arrC), "rc", True, fac=fac)
+
+
+def multiplyRC_sym(arrR, arrC, arrR2, arrC2, nthreads=0):
+    return _product("multiplyRC_sym", (arrR, arrC, arrR2, arrC2), "rcrc", True)
+
+
+def multiplyRCstar_sym(arrR, arrC, arrR2, arrC2, fac, nthreads=0):
+    return _product("multiplyRCstar_sym", (arrR, arrC, arrR2, arrC2), "rcrc", True, fac=fac)
+
+
+def multiplyRR(arr1, arr2, nthreads=0):
+    return _product("multiplyRR", (arr1, arr2), "rr", False)
+
+
+def multiplyRR_sym(arr1, arr2, arr1b, arr2b, nthreads=0):
+    return _product("multiplyRR_sym", (arr1, arr2, arr1b, arr2b), "rrrr", False)
+
+
+def lens_phi_sum(umap, vmap, nthreads=0):
+    """Pixel sum of U and V maps of the lensing Phi estimator (ideal_fisher.pyx:124-139)."""
+    npol, npix = np.shape(umap)[0], np.shape(umap)[1]
+    return _product("lens_phi_sum", (umap, vmap), "cc", True, npol=npol, out_shape=(npix,))
+
+
+def lens_phi_sum_sym(umap1, umap2, vmap1, vmap2, nthreads=0):
+    """Symmetrised lensing Phi pixel sum (ideal_fisher.pyx:142-157)."""
+    npol, npix = np.shape(umap1)[0], np.shape(umap1)[1]
+    return _product("lens_phi_sum_sym", (umap1, umap2, vmap1, vmap2), "cccc", True, npol=npol, out_shape=(npix,))
+
+
+def outer_product(Q4_a, Q4_b, nthreads=0, sym=False):
+    """Fisher outer product of two [4, n_t, n_in] arrays (ideal_fisher.pyx:423-460)."""
+    a, as_torch = _prep(Q4_a, torch.complex128)
+    b, _ = _prep(Q4_b, torch.complex128)
+    if a.dim() != 3 or b.dim() != 3 or a.shape[0] != 4 or b.shape[0] != 4 or a.shape[2] != b.shape[2]:
+        raise ValueError("Q4 arrays must be [4, n_t, n_in] with equal n_in")
+    na, nb, nin = a.shape[1], b.shape[1], a.shape[2]
+    if sym:
+        assert na == nb, "Matrix must be square!"
+    fish = torch.empty((na, nb), dtype=torch.float64, device=a.device)
+    if nin == 0:
+        fish.zero_()
+        return _ret(fish, as_torch)
+    n = ctypes.c_size_t()
+    _lib.call("ps_outer_product_workspace_bytes", na, nb, nin, ctypes.byref(n))
+    ws = torch.empty(max(int(n.value), 8), dtype=torch.uint8, device=a.device)
+    _lib.call("ps_outer_product", ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(b.data_ptr()), na, nb, nin,
+              int(bool(sym)), ctypes.c_void_p(fish.data_ptr()), ctypes.c_void_p(ws.data_ptr()), int(n.value),
+              _stream())
+    return _ret(fish, as_torch)

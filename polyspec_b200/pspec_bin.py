@@ -110,6 +110,20 @@ class PSpecBin:
             a_lm = self.base.generate_data(seed=seed + int(1e7), output_type='harmonic', deconvolve_beam=True, rng=rng)
         a_lm, _ = self.base._in(a_lm, torch.complex128)
 
+        if batched and not self.ones_mask and hasattr(self.applySinv, 'batched'):
+            # the S^-1 solve of the simulation and the N_p solves of the Q_A rows are
+            # independent: one batched solve of N_p + 1 right-hand sides
+            Uinv_A = self.base.applyAinv(a_lm, input_type='harmonic')
+            rows = self._Q2_rows(Uinv_A)
+            alms = torch.stack([self.d_beam * a_lm] + [self.d_beam * r for r in rows])
+            maps = self.d_mask[None] * self.base.to_map_batch(alms)
+            sol = self.applySinv.batched(maps)
+            Uinv_S = sol[0]
+            Q_S = torch.stack([(self.d_mw * r).reshape(-1) for r in self._Q2_rows(Uinv_S)])
+            Q_A = sol[1:].reshape(len(rows), -1)
+            fish = 0.5 * torch.real(Q_S.conj() @ Q_A.T)
+            return fish.cpu().numpy()
+
         # S^-1 weighting: Q_S rows are m_w * summand
         if self.ones_mask:
             Uinv_S = self.applySinv(self.d_beam * a_lm, input_type='harmonic')
@@ -122,9 +136,6 @@ class PSpecBin:
         rows = self._Q2_rows(Uinv_A)
         if self.ones_mask:
             Q_A = torch.stack([self.applySinv(self.d_beam * r, input_type='harmonic').reshape(-1) for r in rows])
-        elif batched and hasattr(self.applySinv, 'batched'):
-            maps = torch.stack([self.d_mask * self.base.to_map(self.d_beam * r) for r in rows])
-            Q_A = self.applySinv.batched(maps).reshape(len(rows), -1)
         else:
             Q_A = torch.stack([self.applySinv(self.d_mask * self.base.to_map(self.d_beam * r)).reshape(-1)
                                for r in rows])

@@ -183,10 +183,12 @@ class Weightings:
 
 
 class BatchedCGD:
-    """B independent copies of the reference CG (polyspec/weighting.py:217-367) run in
-    lockstep: vectors are [B, nfield, nlm], every A and M application is one batched
-    SHT pair, and each right-hand side keeps its own alpha, beta and stopping test
-    (err_b = rz_b / rz0_b < thresh freezes system b, as a separate run would stop)."""
+    """B independent copies of the reference CG (polyspec/weighting.py:217-367): vectors
+    are [B, nfield, nlm] and each right-hand side keeps its own alpha, beta and stopping
+    test (err_b = rz_b / rz0_b < thresh freezes system b, as a separate run would stop).
+    Every step gathers the systems still active and applies A and M to them as one
+    batched SHT pair, so the work is the sum of the separate runs' work, not B times
+    the slowest run's."""
 
     def __init__(self, weightings, d, x0, preconditioner='harmonic'):
         self.base = weightings.base
@@ -239,20 +241,31 @@ class BatchedCGD:
         raise Exception("Unknown preconditioner %s specified!" % self.preconditioner)
 
     def step(self):
-        act = self.active.to(torch.float64)
-        Ap = self._apply_A(self.p)
-        alpha = torch.where(self.active, self.rz / self.dot(self.p, Ap), torch.zeros_like(self.rz))
-        self.x += alpha[:, None, None] * self.p
-        self.r -= alpha[:, None, None] * Ap
-        z = self._apply_M(self.r)
-        next_rz = self.dot(self.r, z)
-        self.err = torch.where(self.active, next_rz / self.rz0, self.err)
-        beta = torch.where(self.active, next_rz / self.rz, torch.zeros_like(next_rz))
-        self.rz = torch.where(self.active, next_rz, self.rz)
-        self.p = torch.where(self.active[:, None, None], z + beta[:, None, None] * self.p, self.p)
-        self.iters += self.active.to(torch.int64)
+        idx = torch.nonzero(self.active).flatten()
+        if idx.numel() == 0:
+            return
+        full = idx.numel() == self.active.numel()
+        p = self.p if full else self.p[idx]
+        r = self.r if full else self.r[idx]
+        rz = self.rz[idx]
+        Ap = self._apply_A(p)
+        alpha = rz / self.dot(p, Ap)
+        x_new = (self.x if full else self.x[idx]) + alpha[:, None, None] * p
+        r = r - alpha[:, None, None] * Ap
+        z = self._apply_M(r)
+        next_rz = self.dot(r, z)
+        beta = next_rz / rz
+        p = z + beta[:, None, None] * p
+        if full:
+            self.x, self.r, self.p = x_new, r, p
+        else:
+            self.x[idx] = x_new
+            self.r[idx] = r
+            self.p[idx] = p
+        self.err[idx] = next_rz / self.rz0[idx]
+        self.rz[idx] = next_rz
+        self.iters[idx] += 1
         self.i += 1
-        del act
 
     def run(self, nstep=10, thresh=1e-6, verb=False):
         for i in range(nstep):

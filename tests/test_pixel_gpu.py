@@ -1,0 +1,150 @@
+"""libpscuda pixel products, radial sums, harmonic weightings and the Fisher
+outer product against the CPU oracle (numpy restatement of the reference's
+Cython kernels) and, where oracle/_ref is built, the compiled reference itself.
+
+Tolerances (FP64 throughout): 1e-14 of the largest magnitude for elementwise
+products (one or two roundings, FMA contraction may differ), 1e-12 relative for
+the radial pixel sums and the outer product (different summation order)."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import pixel_cases as C
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+from oracle import pixel as O  # noqa: E402
+
+
+def close(a, b, tol):
+    a, b = np.asarray(a), np.asarray(b)
+    assert a.shape == b.shape, (a.shape, b.shape)
+    if a.size == 0:
+        return True
+    return np.max(np.abs(a - b)) <= tol * max(np.max(np.abs(b)), 1e-300)
+
+
+def _ref():
+    d = os.path.join(ROOT, "oracle", "_ref")
+    if d not in sys.path:
+        sys.path.insert(0, d)
+    try:
+        import tauNL_utils as T
+        import ideal_fisher as F
+        return T, F
+    except ImportError:
+        return None, None
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("op", sorted(C.PRODUCTS))
+@pytest.mark.parametrize("shape", [(3, 1001), (1, 5), (24, 12 * 32 ** 2), (2, 0)])
+def test_products(op, shape):
+    from polyspec_b200 import pixel as P
+    kinds, fac = C.PRODUCTS[op]
+    xs = C.maps(kinds, shape, seed=sum(map(ord, op)) + shape[1])
+    extra = () if fac is None else (fac,)
+    if op in C.TAUNL_PRODUCTS:
+        out = getattr(P.tauNL_utils(*C.taunl_args(shape[0], 8)), op)(*xs)
+    else:
+        out = getattr(P, op)(*xs, *extra)
+    assert close(out, getattr(O, op)(*xs, *extra), 1e-14)
+    T, F = _ref()
+    if T is not None and shape[1] > 0:
+        ref = (getattr(T.tauNL_utils(*C.taunl_args(shape[0], 8)), op)(*xs) if op in C.TAUNL_PRODUCTS
+               else getattr(F, op)(*xs, *extra, 2))
+        assert close(out, ref, 1e-14)
+
+
+@pytest.mark.gpu
+def test_products_stay_on_device():
+    import torch
+    from polyspec_b200 import pixel as P
+    a, b = (torch.randn(4, 999, dtype=torch.float64, device="cuda") for _ in range(2))
+    c = torch.randn(4, 999, dtype=torch.complex128, device="cuda")
+    out = P.multiplyRC(a, c)
+    assert isinstance(out, torch.Tensor) and out.is_cuda
+    assert torch.allclose(out, a * c, rtol=0, atol=1e-14 * float(out.abs().max()))
+    t = P.tauNL_utils(*C.taunl_args(4, 8))
+    assert torch.allclose(t.multiply2R(a, b), a * b, rtol=0, atol=1e-14 * float((a * b).abs().max()))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", sorted(C.SUMS))
+@pytest.mark.parametrize("nr,npix", [(5, 3001), (1, 7), (24, 12 * 64 ** 2)])
+def test_radial_sums(kind, nr, npix):
+    from polyspec_b200 import pixel as P
+    kinds, has_tau = C.SUMS[kind]
+    xs = C.maps(kinds, (nr, npix), seed=nr * 7 + npix)
+    rng = np.random.default_rng(nr)
+    w, tau = rng.normal(size=nr), rng.uniform(0.5, 2.0, size=nr)
+    args = (w, tau) if has_tau else (w,)
+    t = P.tauNL_utils(*C.taunl_args(nr, 8))
+    got = getattr(t, kind)(*args, *xs)
+    want = getattr(O, kind)(*args, *xs)
+    scale = getattr(O, kind)(*[np.abs(a) for a in args], *[np.abs(x) for x in xs])
+    assert abs(got - want) <= 1e-12 * scale
+    # fixed-order reduction: repeated calls agree bit for bit
+    assert getattr(t, kind)(*args, *xs) == got
+    T, _ = _ref()
+    if T is not None:
+        ref = getattr(T.tauNL_utils(*C.taunl_args(nr, 8)), kind)(*args, *xs)
+        assert abs(got - ref) <= 1e-12 * scale
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("npol,npix", [(1, 777), (3, 777), (3, 12 * 64 ** 2)])
+def test_lens_phi(npol, npix):
+    from polyspec_b200 import pixel as P
+    U, V, U2, V2 = C.maps("cccc", (npol, npix), seed=npol + npix)
+    assert close(P.lens_phi_sum(U, V), O.lens_phi_sum(U, V), 1e-14)
+    assert close(P.lens_phi_sum_sym(U, U2, V, V2), O.lens_phi_sum_sym(U, U2, V, V2), 1e-14)
+    _, F = _ref()
+    if F is not None:
+        assert close(P.lens_phi_sum(U, V), F.lens_phi_sum(U, V, 2), 1e-14)
+        assert close(P.lens_phi_sum_sym(U, U2, V, V2), F.lens_phi_sum_sym(U, U2, V, V2, 2), 1e-14)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("npol", [1, 2])
+@pytest.mark.parametrize("lmax,nr", [(12, 7), (100, 24)])
+def test_harmonic_weightings(npol, lmax, nr):
+    from polyspec_b200 import pixel as P
+    l, m = C.lm_setup(lmax)
+    rng = np.random.default_rng(npol * 100 + lmax)
+    flX = rng.normal(size=(lmax + 1, npol, nr))
+    h = rng.normal(size=(npol, len(l))) + 1j * rng.normal(size=(npol, len(l)))
+    t = P.tauNL_utils(*C.taunl_args(nr, lmax))
+    assert close(t.apply_fl_weights(flX, h, 0.3), O.apply_fl_weights(l, flX, h, 0.3), 1e-14)
+    lm_map = rng.normal(size=(nr, len(l))) + 1j * rng.normal(size=(nr, len(l)))
+    w = rng.normal(size=nr)
+    assert close(t.radial_sum(lm_map, w, flX), O.radial_sum(l, lm_map, w, flX), 1e-12)
+    lm2 = rng.normal(size=(2, nr, len(l))) + 1j * rng.normal(size=(2, nr, len(l)))
+    assert close(t.radial_sum_spin1(lm2, w, flX), O.radial_sum_spin1(l, lm2, w, flX), 1e-12)
+    T, _ = _ref()
+    if T is not None:
+        r = T.tauNL_utils(*C.taunl_args(nr, lmax))
+        assert close(t.apply_fl_weights(flX, h, 0.3), r.apply_fl_weights(flX, h, 0.3), 1e-14)
+        assert close(t.radial_sum(lm_map, w, flX), r.radial_sum(lm_map, w, flX), 1e-12)
+        assert close(t.radial_sum_spin1(lm2, w, flX), r.radial_sum_spin1(lm2, w, flX), 1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sym", [False, True])
+@pytest.mark.parametrize("na,nb,nin", [(6, 9, 500), (1, 1, 3), (37, 37, 20011), (16, 17, 4096)])
+def test_outer_product(sym, na, nb, nin):
+    from polyspec_b200 import pixel as P
+    if sym:
+        nb = na
+    rng = np.random.default_rng(na * nb + nin)
+    Qa = rng.normal(size=(4, na, nin)) + 1j * rng.normal(size=(4, na, nin))
+    Qb = Qa if sym else rng.normal(size=(4, nb, nin)) + 1j * rng.normal(size=(4, nb, nin))
+    got = P.outer_product(Qa, Qb, 0, sym)
+    assert close(got, O.outer_product(Qa, Qb, sym), 1e-12)
+    if sym:
+        assert np.array_equal(got, got.T)
+    _, F = _ref()
+    if F is not None:
+        assert close(got, F.outer_product(Qa, Qb, 2, sym), 1e-12)
