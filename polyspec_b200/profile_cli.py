@@ -5,6 +5,12 @@
 Each op runs once (no warm-up) so that a launch list or an ncu capture of
 ``-k <kernel> -c 1`` sees exactly one launch per transform stage.
 ops: s0/a0 = spin-0 synthesis/adjoint, s2/a2 = spin-2 synthesis/adjoint.
+
+    python -m polyspec_b200.profile_cli pix --nside 512 --nr 24 [--reps 3]
+
+runs the pixel-product / radial-sum kernels on [nr, Npix] maps (config-3
+sizes by default) and prints each one's device time and achieved HBM GB/s
+(algorithmic bytes / CUDA-event time, best of --reps).
 """
 import argparse
 import sys
@@ -35,6 +41,41 @@ def sht(a):
     print("done", a.ops)
 
 
+def pix(a):
+    from polyspec_b200 import pixel as P
+    npix = 12 * a.nside ** 2
+    nr = a.nr
+    g = torch.Generator(device="cuda").manual_seed(0)
+    R = [torch.randn(nr, npix, dtype=torch.float64, device="cuda", generator=g) for _ in range(3)]
+    Cx = torch.randn(nr, npix, dtype=torch.complex128, device="cuda", generator=g)
+    w = torch.rand(nr, dtype=torch.float64, device="cuda", generator=g)
+    t = P.tauNL_utils(1, nr, [0, 1], [0, 0], 0, 1, [0, 1], [0, 0], [0, 1], [0, 0], 1)
+    lmax = 2 * a.nside
+    nlm = (lmax + 1) * (lmax + 2) // 2
+    Q = torch.randn(4, 16, 3 * nlm, dtype=torch.complex128, device="cuda", generator=g)
+    n = nr * npix
+    cases = [
+        ("multiply", lambda: t.multiply(R[0], R[1], R[2]), 32.0 * n),
+        ("multiplyRC", lambda: P.multiplyRC(R[0], Cx), 40.0 * n),
+        ("multiplyCC", lambda: t.multiplyCC(R[0], R[1], Cx), 40.0 * n),
+        ("gnl_loc_sum", lambda: t.gnl_loc_sum(w, R[0], R[1]), 16.0 * n),
+        ("gnl_dotdel_sum", lambda: t.gnl_dotdel_sum(w, w, R[0], R[1], Cx), 32.0 * n),
+        ("outer_product", lambda: P.outer_product(Q, Q, 0, True), 16.0 * Q.numel()),
+    ]
+    for name, f, nbytes in cases:
+        best = None
+        for _ in range(a.reps):
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record()
+            f()
+            s1.record()
+            torch.cuda.synchronize()
+            ms = s0.elapsed_time(s1)
+            best = ms if best is None else min(best, ms)
+        print("%-16s %8.3f ms  %7.1f GB/s (algorithmic %.2f GB)" % (name, best, nbytes / best / 1e6, nbytes / 1e9),
+              flush=True)
+
+
 def main(argv=None):
     p = argparse.ArgumentParser()
     sub = p.add_subparsers(dest="cmd", required=True)
@@ -44,9 +85,15 @@ def main(argv=None):
     s.add_argument("--batch", type=int, default=1)
     s.add_argument("--prec", default="fp64")
     s.add_argument("--ops", default="s0,a0,s2,a2")
+    q = sub.add_parser("pix")
+    q.add_argument("--nside", type=int, default=512)
+    q.add_argument("--nr", type=int, default=24)
+    q.add_argument("--reps", type=int, default=3)
     a = p.parse_args(argv)
     if a.cmd == "sht":
         sht(a)
+    elif a.cmd == "pix":
+        pix(a)
 
 
 if __name__ == "__main__":
