@@ -46,6 +46,20 @@ SIGNATURES = {
     "ps_outer_product_workspace_bytes": (_c_int, [_c_int, _c_int, _c_int64, ctypes.POINTER(_c_size_t)]),
     "ps_outer_product": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_int64, _c_int, _c_void_p, _c_void_p,
                                   _c_size_t, _c_void_p]),
+    "ps_lbp_dims": (_c_int, [ctypes.POINTER(_c_int)] * 4),
+    "ps_lbp_moments": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int,
+                                _c_int64, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
+    "ps_lbp_loss_grad": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, ctypes.c_float, _c_void_p,
+                                  _c_void_p, _c_void_p, _c_void_p]),
+    "ps_lbp_apply": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int,
+                              _c_int64, _c_void_p]),
+    "ps_mlp_dense_forward": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_int, _c_int, _c_void_p,
+                                      _c_void_p]),
+    "ps_mlp_dense_backward_workspace_bytes": (_c_int, [_c_int, _c_int, _c_int, ctypes.POINTER(_c_size_t)]),
+    "ps_mlp_dense_backward": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_int, _c_int,
+                                       _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_size_t, _c_void_p]),
+    "ps_mlp_adam": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, ctypes.c_float,
+                             ctypes.c_float, ctypes.c_float, ctypes.c_float, _c_int, _c_void_p]),
     "ps_stats_enable_timing": (_c_int, [_c_int]),
     "ps_stats_reset": (_c_int, []),
     "ps_stats_get": (_c_int, [_c_int, ctypes.POINTER(_c_int64), ctypes.POINTER(_c_double),

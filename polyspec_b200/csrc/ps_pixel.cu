@@ -480,10 +480,11 @@ using namespace ps;
 extern "C" int ps_pix_product(int op, const void* const* inputs, int n_inputs, void* out, int64_t n, int npol,
                               double fac, cudaStream_t stream) {
   const OpInfo info = op_info(op, npol);
-  if (info.n_in < 0 || n_inputs != info.n_in || !inputs || !out || n < 0) return PS_ERR_INVALID;
+  if (info.n_in < 0 || n_inputs != info.n_in || n < 0) return PS_ERR_INVALID;
   if ((op == PS_PIX_LENS_PHI || op == PS_PIX_LENS_PHI_SYM) ? (npol != 1 && npol != 3) : (npol != 1))
     return PS_ERR_INVALID;
-  if (n == 0) return PS_OK;
+  if (n == 0) return PS_OK;  // empty maps: nothing to read or write
+  if (!inputs || !out) return PS_ERR_INVALID;
   PixIn a{};
   for (int k = 0; k < n_inputs; ++k) {
     if (!inputs[k]) return PS_ERR_INVALID;
