@@ -123,6 +123,9 @@ class Weightings:
         d, as_torch = self.base._in(input_map, torch.float64)
         if hasattr(self, 'inpainting_mask'):
             d = self.inpaint_map(d)
+        if preconditioner == 'learned':
+            return self.base._out(self.batched_applySinv_optimal(d[None], preconditioner='learned', nstep=nstep,
+                                                                 thresh=thresh, verb=verb, lmax=lmax)[0], as_torch)
         x0 = torch.einsum('abi,bi->ai', self.d_x0op, self.base.to_lm(d))
         cgd = CGD(self, d, x0=x0, preconditioner=preconditioner, verb=verb)
         cgd.run(nstep=nstep, thresh=thresh)
@@ -138,7 +141,8 @@ class Weightings:
             lmax = self.base.lmax
         d = maps.to(device=self.base.device, dtype=torch.float64)
         x0 = torch.einsum('abi,nbi->nai', self.d_x0op, self.base.to_lm_batch(d))
-        cgd = BatchedCGD(self, d, x0, preconditioner=preconditioner)
+        # the learned CG hands a system to the plain CG after half the step budget
+        cgd = BatchedCGD(self, d, x0, preconditioner=preconditioner, learned_max_steps=max(1, nstep // 2))
         cgd.run(nstep=nstep, thresh=thresh, verb=verb)
         self.last_cgd = cgd
         lfilt = torch.as_tensor(self.base.l_arr <= lmax, device=self.base.device)
@@ -190,24 +194,45 @@ class BatchedCGD:
     batched SHT pair, so the work is the sum of the separate runs' work, not B times
     the slowest run's."""
 
-    def __init__(self, weightings, d, x0, preconditioner='harmonic'):
+    def __init__(self, weightings, d, x0, preconditioner='harmonic', learned_max_steps=None):
         self.base = weightings.base
         self.W = weightings
         self.preconditioner = preconditioner
         self.w = self.base.dev('m_weight')
+        if preconditioner == 'learned':
+            # learned band preconditioner (polyspec_b200.learned); the judge of convergence
+            # is the plain CG's r^T Sigma r / b^T Sigma b, and a system that misbehaves or
+            # exceeds learned_max_steps continues with the plain harmonic CG
+            self.learned = getattr(weightings, 'learned', None)
+            if self.learned is None or self.learned.L is None:
+                raise Exception("preconditioner='learned' needs a trained Weightings.learned")
+            self.learned_max_steps = learned_max_steps
         b0 = self._get_b(d)
         self.x0 = x0
         b = b0 - self._apply_A(x0)
         self.x = torch.zeros_like(b)
         self.r = b.clone()
-        z = self._apply_M(self.r)
+        B = b.shape[0]
+        self.use_learned = torch.full((B,), preconditioner == 'learned', dtype=torch.bool, device=b.device)
+        z = self._apply_M(self.r, self.use_learned)
         self.rz = self.dot(self.r, z)
-        self.rz0 = self.dot(b0, self._apply_M(b0))
+        self.rz0 = self.dot(b0, self._apply_M(b0, self.use_learned))
+        if preconditioner == 'learned':
+            self.judge0 = self.dot(b0, self._sigma(b0))
         self.p = z
         self.i = 0
-        self.iters = torch.zeros(b.shape[0], dtype=torch.int64, device=b.device)
-        self.active = torch.ones(b.shape[0], dtype=torch.bool, device=b.device)
-        self.err = self.rz / self.rz0
+        self.iters = torch.zeros(B, dtype=torch.int64, device=b.device)
+        self.active = torch.ones(B, dtype=torch.bool, device=b.device)
+        self.err = self._judge(self.r, self.rz, self.use_learned, torch.arange(B, device=b.device))
+
+    def _sigma(self, ilm):
+        return torch.einsum('abi,nbi->nai', self.W.d_Sigma, ilm)
+
+    def _judge(self, r, rz, learned_mask, idx):
+        """Stopping statistic: rz/rz0 of the plain CG (= r^T Sigma r / b^T Sigma b)."""
+        if self.preconditioner != 'learned':
+            return rz / self.rz0[idx]
+        return self.dot(r, self._sigma(r)) / self.judge0[idx]
 
     def dot(self, a, b):
         return torch.sum((a * b.conj()).real * self.w, dim=(-2, -1))
@@ -225,8 +250,14 @@ class BatchedCGD:
         m = m * (self.W.d_WNW / self.W.pixel_area)
         return self._apply_Cinv(ilm) + self.base.to_lm_batch(m) * beam
 
-    def _apply_M(self, ilm):
+    def _apply_M(self, ilm, learned_mask=None):
         Sig = self.W.d_Sigma
+        if self.preconditioner == 'learned':
+            z = self.learned.apply(ilm)
+            if learned_mask is not None and not bool(learned_mask.all()):
+                plain = ~learned_mask
+                z[plain] = torch.einsum('abi,nbi->nai', Sig, ilm[plain])
+            return z
         if self.preconditioner == 'harmonic':
             return torch.einsum('abi,nbi->nai', Sig, ilm)
         elif self.preconditioner == 'pseudo_inverse':
@@ -248,21 +279,34 @@ class BatchedCGD:
         p = self.p if full else self.p[idx]
         r = self.r if full else self.r[idx]
         rz = self.rz[idx]
+        lm = self.use_learned[idx]
         Ap = self._apply_A(p)
         alpha = rz / self.dot(p, Ap)
         x_new = (self.x if full else self.x[idx]) + alpha[:, None, None] * p
         r = r - alpha[:, None, None] * Ap
-        z = self._apply_M(r)
+        z = self._apply_M(r, lm)
         next_rz = self.dot(r, z)
         beta = next_rz / rz
         p = z + beta[:, None, None] * p
+        if self.preconditioner == 'learned':
+            # fallback: a learned system whose r^T M r is not positive and finite, or that
+            # has used its learned step budget, restarts as plain harmonic CG from x
+            bad = lm & ~(torch.isfinite(next_rz) & (next_rz > 0))
+            if self.learned_max_steps is not None:
+                bad |= lm & (self.iters[idx] + 1 >= self.learned_max_steps)
+            if bool(bad.any()):
+                zs = self._sigma(r[bad])
+                p[bad] = zs
+                next_rz[bad] = self.dot(r[bad], zs)
+                lm = lm & ~bad
+                self.use_learned[idx] = lm
         if full:
             self.x, self.r, self.p = x_new, r, p
         else:
             self.x[idx] = x_new
             self.r[idx] = r
             self.p[idx] = p
-        self.err[idx] = next_rz / self.rz0[idx]
+        self.err[idx] = self._judge(r, next_rz, lm, idx)
         self.rz[idx] = next_rz
         self.iters[idx] += 1
         self.i += 1
