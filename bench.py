@@ -225,11 +225,13 @@ def fp64_compare(a, setup, seed):
     n64, nmx = nums["fp64"], nums["mixed"]
     # per field: max over bins of |d| / |C_fp64|; cross spectra (TE) also normalised by sqrt(TT EE)
     per_field = {f: float(np.max(np.abs(nmx[i] - n64[i]) / np.abs(n64[i]))) for i, f in enumerate(FIELDS)}
+    per_field_l2 = {f: float(np.linalg.norm(nmx[i] - n64[i]) / np.linalg.norm(n64[i])) for i, f in enumerate(FIELDS)}
     iTT, iTE, iEE = FIELDS.index("TT"), FIELDS.index("TE"), FIELDS.index("EE")
     te_norm = float(np.max(np.abs(nmx[iTE] - n64[iTE]) / np.sqrt(np.abs(n64[iTT] * n64[iEE]))))
     acc = {"binned_cl_max_rel_err": float(np.max(np.abs(nmx - n64) / np.abs(n64))),
            "binned_cl_rel_l2_err": float(np.linalg.norm(nmx - n64) / np.linalg.norm(n64)),
-           "max_rel_err_per_field": per_field, "TE_err_over_sqrt_TT_EE": te_norm,
+           "max_rel_err_per_field": per_field, "rel_l2_err_per_field": per_field_l2,
+           "TE_err_over_sqrt_TT_EE": te_norm,
            "tolerance": 1e-6, "cg_steps": ACC_CG_STEPS,
            "what": "PSpecBin.Cl_numerator (TT, TE, EE, BB x 8 bins) of one masked GRF map, mixed vs FP64 backend, "
                    "same fixed CG step count"}

@@ -175,17 +175,19 @@ int ps_outer_product(const double* Qa, const double* Qb, int na, int nb, int64_t
 /* ------------------------------------------- learned band preconditioner (CG)
  * No counterpart in the reference (its CG offers 'harmonic' and
  * 'pseudo_inverse', polyspec/weighting.py:301-324).  M r = Sigma r +
- * S^1/2 L_b L_b^T S^1/2 r on band blocks b = (m, 16 consecutive l, fields
- * T, E, B); S = diag(Sigma) (float64 [3][3][nalm]); L [nb][48][4] float32 is the
- * output of a 3-layer MLP (bf16 weights, FP32 accumulation) trained on
- * (residual, error) pairs of the plain CG.  Blocks are described by the alm
+ * S^1/2 (L_b L_b^T + d_b I) S^1/2 r on band blocks b = (m, 16 consecutive l,
+ * fields T, E, B); S = diag(Sigma) (float64 [3][3][nalm]); the network output per
+ * block, [48*4 + 1] float32 (L_b row-major, then q_b with d_b = 0.5 tanh q_b), comes
+ * from a 3-layer MLP (bf16 weights, FP32 accumulation) trained on (residual,
+ * error) pairs of the plain CG.  Blocks are described by the alm
  * index of their first (l, m) and their number of valid l.
  * ps_lbp_moments accumulates C += Sum w u u^T, G += Sum w sym(u t^T), T += Sum
  * w t^T t per block over the real and imaginary parts of `batch` pairs
  * (u = S^1/2 r, t = S^-1/2 (e - Sigma r); r, e complex128 [batch][3][nalm]).
- * ps_lbp_loss_grad gives the per-block loss tr(B A) - 2 tr(L^T G L) + T and
- * dL = 2 scale (C L A + L B - 2 G L) (A = L^T L, B = L^T C L), and their total
- * (fixed order, device double).  ps_lbp_apply adds the correction to z. */
+ * ps_lbp_loss_grad gives the per-block loss || (L L^T + d I) u - t ||^2 summed
+ * over the pairs (from C, G, T), its gradient with respect to the block's
+ * outputs (times scale) and the total loss (fixed order, device double).
+ * ps_lbp_apply adds the correction to z. */
 int ps_lbp_dims(int* band_l, int* block_dim, int* rank, int* outputs);
 int ps_lbp_moments(const int64_t* blk_idx0, const int* blk_nl, int nb, const double* r, const double* e,
                    const double* w, const double* sigma, int batch, int64_t nalm, float* C, float* G, float* T,
@@ -195,7 +197,7 @@ int ps_lbp_loss_grad(const float* L, const float* C, const float* G, const float
 int ps_lbp_apply(const int64_t* blk_idx0, const int* blk_nl, int nb, const float* L, const double* sigma,
                  const double* r, double* z, int batch, int64_t nalm, cudaStream_t stream);
 /* Dense layer Y[n][o] = act(Sum_i X[n][i] W[o][i] + b[o]) with bf16 W, b and
- * FP32 X, Y, accumulation (in_dim <= 64, out_dim <= 192; act = ReLU or none),
+ * FP32 X, Y, accumulation (in_dim <= 64, out_dim <= 196; act = ReLU or none),
  * its backward pass (dY is overwritten by dY * act'(Y); dX may be null; dW, db
  * reduced over rows in a fixed order) and an Adam step on FP32 master weights
  * that refreshes their bf16 copy. */

@@ -5,7 +5,8 @@ learned preconditioner); the oracle is pinned by finite differences
 (tests/test_learned_oracle.py).
 
 Shapes: features X [n, F]; W1 [H, F], b1 [H]; W2 [H, H], b2 [H]; W3 [O, H], b3 [O];
-O = D * K, L = out.reshape(n, D, K); moments C, G [n, D, D] (symmetric), T [n].
+O = D * K + 1: L = out[:, :D*K].reshape(n, D, K), q = out[:, -1], d = 0.5 tanh(q);
+moments C, G [n, D, D] (symmetric), T [n].
 """
 import numpy as np
 
@@ -18,15 +19,23 @@ def forward(X, params):
     return h1, h2, out
 
 
-def block_loss(L, C, G, T):
-    """J_b = tr(B A) - 2 tr(L^T G L) + T,  A = L^T L, B = L^T C L;  dJ/dL = 2 (C L A + L B - 2 G L)."""
+def block_loss(L, d, C, G, T):
+    """J_b = || (L L^T + d I) u - t ||^2 over the pairs, from the moments:
+    tr(B A) + 2 d tr(B) + d^2 tr(C) - 2 tr(L^T G L) - 2 d tr(G) + T  (A = L^T L, B = L^T C L);
+    dJ/dL = 2 (C L A + L B + 2 d C L - 2 G L),  dJ/dd = 2 (tr(B) + d tr(C) - tr(G))."""
     A = np.einsum("nda,ndc->nac", L, L)
     CL = np.einsum("nde,nea->nda", C, L)
     GL = np.einsum("nde,nea->nda", G, L)
     Bm = np.einsum("nda,ndc->nac", L, CL)
-    J = np.einsum("nac,nca->n", Bm, A) - 2.0 * np.einsum("nda,nda->n", L, GL) + T
-    dL = 2.0 * (np.einsum("nda,nac->ndc", CL, A) + np.einsum("nda,nac->ndc", L, Bm) - 2.0 * GL)
-    return J, dL
+    trB = np.einsum("naa->n", Bm)
+    trC = np.einsum("naa->n", C)
+    trG = np.einsum("naa->n", G)
+    J = (np.einsum("nac,nca->n", Bm, A) + 2 * d * trB + d * d * trC - 2.0 * np.einsum("nda,nda->n", L, GL)
+         - 2 * d * trG + T)
+    dL = 2.0 * (np.einsum("nda,nac->ndc", CL, A) + np.einsum("nda,nac->ndc", L, Bm) + 2 * d[:, None, None] * CL
+                - 2.0 * GL)
+    dd = 2.0 * (trB + d * trC - trG)
+    return J, dL, dd
 
 
 def loss_and_grads(X, params, C, G, T, D, K):
@@ -34,10 +43,11 @@ def loss_and_grads(X, params, C, G, T, D, K):
     W1, b1, W2, b2, W3, b3 = params
     h1, h2, out = forward(X, params)
     n = X.shape[0]
-    L = out.reshape(n, D, K)
-    J, dL = block_loss(L, C, G, T)
+    L = out[:, :D * K].reshape(n, D, K)
+    th = np.tanh(out[:, D * K])
+    J, dL, dd = block_loss(L, 0.5 * th, C, G, T)
     s = 1.0 / np.sum(T)
-    d3 = dL.reshape(n, -1) * s
+    d3 = np.concatenate([dL.reshape(n, -1), (dd * 0.5 * (1 - th * th))[:, None]], axis=1) * s
     gW3, gb3 = d3.T @ h2, d3.sum(0)
     d2 = (d3 @ W3) * (h2 > 0)
     gW2, gb2 = d2.T @ h1, d2.sum(0)
@@ -76,7 +86,8 @@ def moments(blocks, r, e, w, sigma, band_l):
 
 
 def apply(blocks, L, sigma, r, band_l):
-    """M r = Sigma r + S^1/2 L L^T S^1/2 r on every block (see ps_lbp_apply)."""
+    """M r = Sigma r + S^1/2 (L L^T + d I) S^1/2 r on every block (see ps_lbp_apply);
+    L [nb, D*K + 1] network outputs."""
     z = np.einsum("fgi,ngi->nfi", sigma, r)
     S = np.einsum("ffi->fi", sigma)
     D = 3 * band_l
@@ -88,7 +99,8 @@ def apply(blocks, L, sigma, r, band_l):
                 sl = slice(i0, i0 + nl)
                 sq[f * band_l:f * band_l + nl] = np.sqrt(np.maximum(S[f, sl], 0.0))
                 u[f * band_l:f * band_l + nl] = r[n, f, sl]
-            c = sq * (L[b] @ (L[b].T @ (sq * u)))
+            Lb = L[b][:D * K].reshape(D, -1)
+            c = sq * (Lb @ (Lb.T @ (sq * u)) + 0.5 * np.tanh(L[b][D * K]) * (sq * u))
             for f in range(3):
                 z[n, f, i0:i0 + nl] += c[f * band_l:f * band_l + nl]
     return z

@@ -19,7 +19,9 @@ Extensions beyond the reference (optional keywords): ``lmax=`` fixes the
 harmonic band limit used by default (the reference hard-codes 3 Nside - 1,
 polyspec/base.py:30); ``prec='mixed'`` runs the SHTs on the mixed-precision
 path (tensor-core Legendre synthesis, FP32 contractions and ring FFTs, FP64
-inputs and outputs) instead of the FP64 path.
+inputs and outputs) instead of the FP64 path; with ``autotune=True`` (default)
+each transform size runs whichever of the two pipelines measured faster on its
+first call (the FP64 one for a few maps, the mixed one for batches).
 """
 import os
 import time
@@ -65,7 +67,7 @@ class PolySpec:
     """Base class of PolySpec on one B200 (see module docstring)."""
 
     def __init__(self, Nside, Cl_tot, beam=[], pol=True, backend="cuda", nthreads=0, lmax=None, device=None,
-                 prec="fp64"):
+                 prec="fp64", autotune=True):
         if backend != "cuda":
             raise Exception("polyspec_b200 implements the 'cuda' backend only")
         if not torch.cuda.is_available():
@@ -76,6 +78,7 @@ class PolySpec:
         if prec not in ("fp64", "mixed"):
             raise ValueError("prec must be 'fp64' or 'mixed'")
         self.prec = prec
+        self.autotune = autotune
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
 
         self.Npix = 12 * Nside ** 2
@@ -150,7 +153,7 @@ class PolySpec:
         lmax = self.lmax if lmax is None else int(lmax)
         p = self._plans.get(lmax)
         if p is None:
-            p = SHTPlan(self.Nside, lmax, device=self.device, prec=self.prec)
+            p = SHTPlan(self.Nside, lmax, device=self.device, prec=self.prec, autotune=self.autotune)
             self._plans[lmax] = p
         return p
 

@@ -12,15 +12,21 @@
 // recurrence (scaled seeds as in the FP64 kernels), rounds each value to FP32
 // and splits it into two TF32 parts hi + lo (K-major operand, 8-row x 16-byte
 // core matrices, no swizzle).  The a_lm of the chunk are split the same way.
-// Three tcgen05.mma per parity (hi*hi + hi*lo + lo*hi) accumulate in FP32 in
-// TMEM.  Chunks of 16 l (8 per parity) keep a CTA's shared memory small so
-// that several CTAs share an SM and hide the latency of the recurrence chains;
-// two stages of tiles let the tensor cores work on chunk c while the threads
-// generate chunk c+1 (a tcgen05.commit per stage on its mbarrier releases the
-// stage).  The next chunk's a_lm and recurrence coefficients are fetched while
-// the current chunk is generated.  Every mbarrier wait is bounded; on expiry
-// the kernel raises the plan's error flag, waits once more (bounded) for its
-// MMAs and frees its TMEM.
+// Three tcgen05.mma per parity (hi*hi + hi*lo + lo*hi) accumulate one chunk in
+// FP32 in TMEM; after each chunk every thread moves its TMEM row into FP32
+// registers (round-to-nearest adds) and the next chunk starts a fresh TMEM
+// accumulation.  The tensor cores' FP32 accumulation truncates, so a single
+// accumulator running over all l (about 770 MMA steps at lmax 2048) biases the
+// result towards zero by ~1e-5 relative; one chunk (3 steps) keeps that bias
+// below 1e-6.  Chunks of 16 l (8 per parity) keep a CTA's shared memory small
+// so that several CTAs share an SM and hide the latency of the recurrence
+// chains; two stages of tiles let the tensor cores work on chunk c-1 while the
+// threads generate chunk c (a tcgen05.commit per stage on its mbarrier tells
+// when the chunk's MMAs are done), and the chunk is drained just before the
+// next one is issued.  The next chunk's a_lm and recurrence coefficients are
+// fetched while the current chunk is generated.  Every mbarrier wait is
+// bounded; on expiry the kernel raises the plan's error flag, waits once more
+// (bounded) for its MMAs and frees its TMEM.
 #include "ps_common.cuh"
 #include "ps_stats.cuh"
 #include "ps_tc.cuh"
@@ -100,7 +106,7 @@ struct TcSmem {
 };
 
 template <int NOPS, int N>
-__device__ __forceinline__ void issue_stage(uint32_t sbase, int st, uint32_t tmem, bool first) {
+__device__ __forceinline__ void issue_stage(uint32_t sbase, int st, uint32_t tmem) {
   constexpr uint32_t idesc = tc::idesc_tf32(128, N, 0, 0);
   using S = TcSmem<NOPS, N>;
 #pragma unroll
@@ -110,7 +116,7 @@ __device__ __forceinline__ void issue_stage(uint32_t sbase, int st, uint32_t tme
       const uint32_t d = tmem + uint32_t((op * 2 + p) * N);
       const uint64_t a_hi = desc_k8(sbase + S::a(st, op, p, 0)), a_lo = desc_k8(sbase + S::a(st, op, p, 1));
       const uint64_t b_hi = desc_k8(sbase + S::b(st, p, 0)), b_lo = desc_k8(sbase + S::b(st, p, 1));
-      tc::mma_tf32(d, a_hi, b_hi, idesc, first ? 0u : 1u);
+      tc::mma_tf32(d, a_hi, b_hi, idesc, 0u);  // fresh accumulation per chunk
       tc::mma_tf32(d, a_hi, b_lo, idesc, 1u);
       tc::mma_tf32(d, a_lo, b_hi, idesc, 1u);
     }
@@ -241,17 +247,33 @@ __global__ void __launch_bounds__(TC_RT) synth_tc(const RingInfo* __restrict__ r
   const int nchunks = (lmax - m) / TC_LC + 1;
   uint32_t ph[2] = {0u, 0u};
   bool ok = true;
+  // FP32 running sums of this thread's TMEM row (all D regions)
+  constexpr int NSUM = int(NCOLS_NEED);
+  float acc[NSUM];
+#pragma unroll
+  for (int q = 0; q < NSUM; ++q) acc[q] = 0.f;
+  const uint32_t lane_addr = tmem + (uint32_t(warp * 32) << 16);
+  // wait for the MMAs of chunk cc (committed on mbarrier cc & 1) and add D to acc
+  auto drain = [&](int cc) -> bool {
+    const int sb = cc & 1;
+    if (!__syncthreads_and(tc::mbar_wait_bounded(tc::smem_u32(&s_mbar[sb]), ph[sb], TC_WAIT_LIMIT))) return false;
+    ph[sb] ^= 1u;
+    tc::fence_after_sync();
+#pragma unroll
+    for (int cb = 0; cb < NSUM; cb += 16) {
+      float v[16];
+      tc::tmem_ld16(lane_addr + cb, v);
+      tc::tmem_ld_wait();
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc[cb + q] += v[q];
+    }
+    tc::fence_before_sync();
+    return true;
+  };
   for (int c = 0; c < nchunks; ++c) {
     const int st = c & 1;
     const int l0 = m + c * TC_LC;
-    if (c >= 2) {  // stage st was read by the MMAs of chunk c-2
-      if (!__syncthreads_and(tc::mbar_wait_bounded(tc::smem_u32(&s_mbar[st]), ph[st], TC_WAIT_LIMIT))) {
-        ok = false;
-        break;
-      }
-      ph[st] ^= 1u;
-      tc::fence_after_sync();
-    }
+    // stage st was read by the MMAs of chunk c-2, drained (and so finished) in iteration c-1
     // B tiles of this chunk from the prefetched a_lm (l0 + m even: even l - l0 -> parity 0)
 #pragma unroll
     for (int it = 0; it < IPT; ++it) {
@@ -320,32 +342,33 @@ __global__ void __launch_bounds__(TC_RT) synth_tc(const RingInfo* __restrict__ r
           put_a4(smem, S::a(st, 1, p, 1), tid, kc, ml_[j0], ml_[j0 + 2], ml_[j0 + 4], ml_[j0 + 6]);
         }
     }
+    // chunk c-1 must leave TMEM before chunk c's MMAs overwrite it
+    if (c >= 1 && !drain(c - 1)) {
+      ok = false;
+      break;
+    }
     tc::fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
       tc::fence_after_sync();
-      issue_stage<NOPS, N>(sbase, st, tmem, c == 0);
+      issue_stage<NOPS, N>(sbase, st, tmem);
       tc::mma_commit(tc::smem_u32(&s_mbar[st]));
     }
   }
-  // the last commit arrives once every MMA of the CTA has completed
-  const int stl = (nchunks - 1) & 1;
-  if (ok) ok = __syncthreads_and(tc::mbar_wait_bounded(tc::smem_u32(&s_mbar[stl]), ph[stl], TC_WAIT_LIMIT));
+  if (ok) ok = drain(nchunks - 1);
   if (!ok) {
+    // the last commit arrives once every MMA of the CTA has completed
+    const int stl = (nchunks - 1) & 1;
     if (tid == 0) atomicExch(err_flag, 1);
     tc::mbar_wait_bounded(tc::smem_u32(&s_mbar[stl]), ph[stl], TC_WAIT_LIMIT);
   } else {
-    tc::fence_after_sync();
     const int ring = blockIdx.x * TC_RT + warp * 32 + lane;
     const int rs = R - 1 - ring;
-    const uint32_t lane_addr = tmem + (uint32_t(warp * 32) << 16);
     if (NOPS == 1) {
-#pragma unroll 1
+#pragma unroll
       for (int cb = 0; cb < N; cb += 16) {
-        float e[16], o[16];
-        tc::tmem_ld16(lane_addr + cb, e);
-        tc::tmem_ld16(lane_addr + N + cb, o);
-        tc::tmem_ld_wait();
+        const float* e = acc + cb;
+        const float* o = acc + N + cb;
         if (ring < Rh) {
 #pragma unroll
           for (int q = 0; q < 16; q += 2) {
@@ -361,15 +384,13 @@ __global__ void __launch_bounds__(TC_RT) synth_tc(const RingInfo* __restrict__ r
       }
     } else {
       const bool odd = spin & 1;
-#pragma unroll 1
+#pragma unroll
       for (int cb = 0; cb < N; cb += 16) {
         // columns cb..cb+15 = 4 maps x (G re, G im, C re, C im)
-        float p0[16], p1[16], m0[16], m1[16];
-        tc::tmem_ld16(lane_addr + 0 * N + cb, p0);  // F+, parity 0
-        tc::tmem_ld16(lane_addr + 1 * N + cb, p1);  // F+, parity 1
-        tc::tmem_ld16(lane_addr + 2 * N + cb, m0);  // F-, parity 0
-        tc::tmem_ld16(lane_addr + 3 * N + cb, m1);  // F-, parity 1
-        tc::tmem_ld_wait();
+        const float* p0 = acc + 0 * N + cb;  // F+, parity 0
+        const float* p1 = acc + 1 * N + cb;  // F+, parity 1
+        const float* m0 = acc + 2 * N + cb;  // F-, parity 0
+        const float* m1 = acc + 3 * N + cb;  // F-, parity 1
         if (ring < Rh) {
 #pragma unroll
           for (int q = 0; q < 16; q += 4) {
@@ -431,6 +452,7 @@ int launch_legendre_synth_tc(const Plan& P, const double2* almT, float2* phase, 
   const double flops = double(spin == 0 ? 4 : 16) * double(P.Rh) * double(P.nalm) * B;
   const double bytes = double(B) * (spin == 0 ? 1 : 2) * (16.0 * P.nalm + 8.0 * P.R * (P.mmax + 1));
   StatScope sc(PS_K_LEG_SYNTH, flops, bytes, st);
+  // BC (maps per CTA) bounded by the FP32 running sums a thread keeps: 4 BC (spin 0), 16 BC (spin s)
   if (spin == 0) {
     if (B > 16) return launch_synth_tc<1, 32>(P, almT, phase, B, 0, err_flag, st);
     if (B > 8) return launch_synth_tc<1, 16>(P, almT, phase, B, 0, err_flag, st);

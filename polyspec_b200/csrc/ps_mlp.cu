@@ -5,23 +5,28 @@
 //
 // The preconditioner (no counterpart in the reference, whose CG offers the
 // 'harmonic' and 'pseudo_inverse' preconditioners, polyspec/weighting.py:301-324):
-//   M r = Sigma r + S^1/2 L_b L_b^T S^1/2 r      on every band block b
+//   M r = Sigma r + S^1/2 (L_b L_b^T + d_b I) S^1/2 r      on every band block b
 // where Sigma is the harmonic preconditioner (per-l 3x3, weighting.py:76-78),
 // S = diag(Sigma) per (field, lm), and a block b is (one m, LB consecutive l,
 // the three fields T, E, B): D = 3 LB real coordinates, applied to the real and
-// the imaginary parts of the alm alike.  L_b (D x K) is produced by a 3-layer
-// MLP from features of the block (m, l, signal-to-noise, ...), so M is linear,
-// symmetric and M >= Sigma > 0 for any network output: plain PCG stays valid.
+// the imaginary parts of the alm alike.  L_b (D x K) and d_b = 0.5 tanh(q_b) are
+// produced by a 3-layer MLP from features of the block (m, l, signal-to-noise,
+// ...).  Sigma + d S is positive definite for |d| < 1 - rho, rho the largest
+// correlation coefficient of the 3x3 Sigma (the T-E correlation, well below 0.5
+// for CMB spectra), and L L^T adds a positive semi-definite term: M stays
+// symmetric positive definite, so plain PCG remains valid.
 //
 // Training target: for plain-CG iterates x_k of a system with solution x*,
 // e_k = x* - x_k solves A e_k = r_k; the loss is
-//   J = Sum_s w_s || L L^T u_s - t_s ||^2,  u = S^1/2 r,  t = S^-1/2 (e - Sigma r)
+//   J = Sum_s w_s || P u_s - t_s ||^2,  P = L L^T + d I,  u = S^1/2 r,  t = S^-1/2 (e - Sigma r)
 // per block, i.e. the error of M r_k against e_k in the S^-1 norm.  With
-// C = Sum w u u^T, G = Sym(Sum w u t^T), T = Sum w t^T t (accumulated once):
-//   J_b = tr(B A) - 2 tr(L^T G L) + T,  A = L^T L, B = L^T C L
-//   dJ_b/dL = 2 (C L A + L B - 2 G L).
-// Layouts: C, G [nb][D][D] float32 (row-major, C and G symmetric); L [nb][D][K]
-// float32; alm vectors complex128 [B][3][nalm] (m-major alm order).
+// C = Sum w u u^T, G = Sym(Sum w u t^T), T = Sum w t^T t (accumulated once),
+// A = L^T L, B = L^T C L, E = tr(L^T G L):
+//   J_b = tr(B A) + 2 d tr(B) + d^2 tr(C) - 2 E - 2 d tr(G) + T
+//   dJ_b/dL = 2 (C L A + L B + 2 d C L - 2 G L),  dJ_b/dd = 2 (tr(B) + d tr(C) - tr(G)).
+// Layouts: C, G [nb][D][D] float32 (row-major, C and G symmetric); network
+// output per block [D*K + 1] float32 (L row-major, then q); alm vectors
+// complex128 [B][3][nalm] (m-major alm order).
 #include <cuda_bf16.h>
 
 #include "ps_common.cuh"
@@ -33,7 +38,10 @@ namespace {
 constexpr int LB = 16;        // l per band
 constexpr int DB = 3 * LB;    // real coordinates per block (T, E, B)
 constexpr int KR = 4;         // rank of the learned correction
-constexpr int OUT = DB * KR;  // network outputs per block
+constexpr int OUT = DB * KR + 1;  // network outputs per block: L, then q (d = 0.5 tanh q)
+constexpr float D_MAX = 0.5f;
+
+__device__ __forceinline__ float d_of_q(float q) { return D_MAX * tanhf(q); }
 
 struct BlockDesc {
   const int64_t* idx0;  // alm index of (l0, m)
@@ -135,15 +143,26 @@ __global__ void __launch_bounds__(LG_WARPS * 32) lbp_loss_grad_kernel(const floa
   __shared__ float sL[LG_WARPS][DB][KR];
   if (b >= nb) return;  // whole warp leaves together; no block-wide barrier below
   const float* Lb = L + int64_t(b) * OUT;
-  for (int k = lane; k < OUT; k += 32) sL[warp][k / KR][k % KR] = Lb[k];
+  for (int k = lane; k < DB * KR; k += 32) sL[warp][k / KR][k % KR] = Lb[k];
+  const float q = Lb[DB * KR];
+  const float dd = d_of_q(q);
   __syncwarp();
   const float* Cb = C + int64_t(b) * DB * DB;
   const float* Gb = G + int64_t(b) * DB * DB;
   float cl[2][KR], gl[2][KR], lr[2][KR];
+  float trC = 0.f, trG = 0.f;
 #pragma unroll
-  for (int h = 0; h < 2; ++h)
+  for (int h = 0; h < 2; ++h) {
+    const int row = lane + 32 * h;
+    if (row < DB) { trC += Cb[row * DB + row]; trG += Gb[row * DB + row]; }
 #pragma unroll
     for (int a = 0; a < KR; ++a) { cl[h][a] = 0.f; gl[h][a] = 0.f; lr[h][a] = 0.f; }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    trC += __shfl_xor_sync(0xffffffffu, trC, off);
+    trG += __shfl_xor_sync(0xffffffffu, trG, off);
+  }
   for (int j = 0; j < DB; ++j) {
     // C and G are symmetric: row `row`, column j = C[j][row] (coalesced over lanes)
 #pragma unroll
@@ -192,20 +211,27 @@ __global__ void __launch_bounds__(LG_WARPS * 32) lbp_loss_grad_kernel(const floa
     for (int off = 16; off > 0; off >>= 1) ve += __shfl_xor_sync(0xffffffffu, ve, off);
     E = ve;
   }
-  float trBA = 0.f;
+  float trBA = 0.f, trB = 0.f;
 #pragma unroll
-  for (int a = 0; a < KR; ++a)
+  for (int a = 0; a < KR; ++a) {
+    trB += Bm[a][a];
 #pragma unroll
     for (int c = 0; c < KR; ++c) trBA += Bm[a][c] * A[c][a];
-  if (lane == 0) loss_blk[b] = trBA - 2.f * E + T[b];
-  // dL = 2 (C L A + L B - 2 G L) * scale
+  }
+  if (lane == 0) {
+    loss_blk[b] = trBA + 2.f * dd * trB + dd * dd * trC - 2.f * E - 2.f * dd * trG + T[b];
+    const float dJdd = 2.f * (trB + dd * trC - trG);
+    const float th = dd / D_MAX;
+    dL[int64_t(b) * OUT + DB * KR] = dJdd * D_MAX * (1.f - th * th) * scale;
+  }
+  // dL = 2 (C L A + L B + 2 d C L - 2 G L) * scale
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int row = lane + 32 * h;
     if (row >= DB) continue;
 #pragma unroll
     for (int c = 0; c < KR; ++c) {
-      float v = -2.f * gl[h][c];
+      float v = -2.f * gl[h][c] + 2.f * dd * cl[h][c];
 #pragma unroll
       for (int a = 0; a < KR; ++a) v += cl[h][a] * A[a][c] + lr[h][a] * Bm[a][c];
       dL[int64_t(b) * OUT + row * KR + c] = 2.f * v * scale;
@@ -237,7 +263,7 @@ constexpr int DN_ROWS = 32;
 constexpr int DB_ROWS = 16;
 constexpr int DN_THREADS = 256;
 constexpr int DN_MAXI = 64;
-constexpr int DN_MAXO = 192;
+constexpr int DN_MAXO = 196;
 
 __global__ void __launch_bounds__(DN_THREADS) dense_fwd_kernel(const float* __restrict__ X,
                                                              const __nv_bfloat16* __restrict__ W,
@@ -338,7 +364,7 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
 }
 
 // ------------------------------------------------------------------ application
-// z[n][f][lm] += S_f(lm)^1/2 (L_b L_b^T u)_f,  u = S^1/2 r, real and imaginary parts
+// z[n][f][lm] += S_f(lm)^1/2 ((L_b L_b^T + d_b I) u)_f,  u = S^1/2 r, real and imaginary parts
 __global__ void __launch_bounds__(128) lbp_apply_kernel(BlockDesc bd, int nb, const float* __restrict__ L,
                                                         const double* __restrict__ Sig, const double2* __restrict__ r,
                                                         double2* __restrict__ z, int B, int64_t nalm) {
@@ -365,6 +391,7 @@ __global__ void __launch_bounds__(128) lbp_apply_kernel(BlockDesc bd, int nb, co
 #pragma unroll
     for (int a = 0; a < KR; ++a) lr[h][a] = (row < DB) ? L[int64_t(b) * OUT + row * KR + a] : 0.f;
   }
+  const float dd = d_of_q(L[int64_t(b) * OUT + DB * KR]);
   for (int n = 0; n < B; ++n) {
     double2 u[2];
 #pragma unroll
@@ -392,7 +419,7 @@ __global__ void __launch_bounds__(128) lbp_apply_kernel(BlockDesc bd, int nb, co
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       if (!ok[h]) continue;
-      float cr = 0.f, ci = 0.f;
+      float cr = dd * float(u[h].x), ci = dd * float(u[h].y);
 #pragma unroll
       for (int a = 0; a < KR; ++a) { cr += lr[h][a] * yr[a]; ci += lr[h][a] * yi[a]; }
       double2* zp = z + int64_t(n) * 3 * nalm + off[h];

@@ -157,7 +157,8 @@ class LearnedBandPreconditioner:
         snr = [Cl[:, k, k] * beam[k][:len(Cl)] ** 2 / weightings.Nl_iso[k] for k in range(3)]
         self.X = torch.as_tensor(block_features(lmax, ms, l0s, nls, snr), device=dev)
         self.mlp = MLP(self.OUT, dev, seed=seed)
-        self.sigma = weightings.d_Sigma.contiguous()  # [3, 3, nlm] float64
+        self.sigma_c = weightings.d_Sigma                     # [3, 3, nlm] complex128 (for einsum with alm)
+        self.sigma = weightings.d_Sigma.real.contiguous()     # [3, 3, nlm] float64 (kernel argument)
         self.L = None
         self.history = []
         self._reset_moments()
@@ -237,7 +238,7 @@ class LearnedBandPreconditioner:
     # ---------------------------------------------------------------- application
     def apply(self, r):
         """M r for r complex128 [B, 3, nlm]."""
-        z = torch.einsum('abi,nbi->nai', self.sigma, r).contiguous()
+        z = torch.einsum('abi,nbi->nai', self.sigma_c, r).contiguous()
         if self.L is None:
             return z
         r = r.contiguous()

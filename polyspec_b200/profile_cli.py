@@ -20,7 +20,7 @@ import torch
 
 def sht(a):
     from polyspec_b200.sht import SHTPlan
-    P = SHTPlan(a.nside, a.lmax, prec=a.prec)
+    P = SHTPlan(a.nside, a.lmax, prec=a.prec, autotune=False)
     B = a.batch
     alm0 = torch.randn(B, P.nalm, dtype=torch.complex128, device="cuda")
     map0 = torch.randn(B, P.npix, dtype=torch.float64, device="cuda")

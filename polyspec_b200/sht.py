@@ -9,6 +9,13 @@ return CUDA tensors in the ducc0 layout used by the reference
   (components G, C <-> Q, U)
 
 ``adjoint`` is ducc0's ``adjoint_synthesis`` times ``scale``.
+
+With ``prec='mixed'`` the plan also holds an FP64 plan and autotunes, per
+(direction, spin, batch size), which of the two pipelines runs: the first call
+of each kind times both (CUDA events, after one untimed run each) and keeps
+the faster one.  The tensor-core pipeline wins at large batches; for one or
+a few maps the FP64 CUDA-core kernels are faster (and exact to FP64).  The
+choices are visible in ``SHTPlan.tuned``.
 """
 import ctypes
 
@@ -22,7 +29,7 @@ def nalm(lmax):
 
 
 class SHTPlan:
-    def __init__(self, nside, lmax=None, spins=(0, 1, 2, 3), prec="fp64", device=None):
+    def __init__(self, nside, lmax=None, spins=(0, 1, 2, 3), prec="fp64", device=None, autotune=True):
         if not torch.cuda.is_available():
             raise RuntimeError("the CUDA backend needs a GPU (no CPU fallback)")
         self.nside = int(nside)
@@ -41,15 +48,56 @@ class SHTPlan:
                       _lib.PS_PREC_FP64 if prec == "fp64" else _lib.PS_PREC_MIXED, ctypes.byref(h))
         self._h = h
         self._ws = None
+        # mixed precision: an FP64 plan beside it for the autotuned small-batch path
+        self._h64 = None
+        self.tuned = {}
+        if prec != "fp64" and autotune:
+            h64 = ctypes.c_void_p()
+            with torch.cuda.device(self.device):
+                _lib.call("ps_plan_create", self.nside, self.lmax, self.lmax, mask, _lib.PS_PREC_FP64,
+                          ctypes.byref(h64))
+            self._h64 = h64
         # counters of transforms issued through this plan
         self.n_synthesis = 0
         self.n_adjoint = 0
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib.lib().ps_plan_destroy(h)
-            self._h = None
+        for name in ("_h", "_h64"):
+            h = getattr(self, name, None)
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().ps_plan_destroy(h)
+                setattr(self, name, None)
+
+    # ------------------------------------------------------------ autotuning
+    @staticmethod
+    def _bucket(B):
+        if B <= 8:
+            return B
+        b = 16
+        while b < B:
+            b *= 2
+        return b
+
+    def _pick(self, key, run):
+        """Plan handle for `key` = (direction, spin, batch bucket); `run(handle)` issues
+        the transform.  Times both pipelines on the first call of a key."""
+        if self._h64 is None:
+            return self._h
+        choice = self.tuned.get(key)
+        if choice is None:
+            times = {}
+            for name, h in (("mixed", self._h), ("fp64", self._h64)):
+                run(h)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                run(h)
+                e1.record()
+                torch.cuda.synchronize()
+                times[name] = e0.elapsed_time(e1)
+            choice = min(times, key=times.get)
+            self.tuned[key] = choice
+            self.tuned[key + ("ms",)] = times
+        return self._h if choice == "mixed" else self._h64
 
     def error_flag(self, reset=True):
         """Device error flag of the plan (set by a kernel whose bounded wait expired)."""
@@ -59,9 +107,13 @@ class SHTPlan:
 
     # ------------------------------------------------------------ workspace
     def workspace(self, batch, spin, adjoint):
-        n = ctypes.c_size_t()
-        _lib.call("ps_sht_workspace_bytes", self._h, int(batch), int(spin), int(adjoint), ctypes.byref(n))
-        need = int(n.value)
+        need = 0
+        for h in (self._h, self._h64):
+            if h is None:
+                continue
+            n = ctypes.c_size_t()
+            _lib.call("ps_sht_workspace_bytes", h, int(batch), int(spin), int(adjoint), ctypes.byref(n))
+            need = max(need, int(n.value))
         if self._ws is None or self._ws.numel() < need:
             self._ws = torch.empty(max(need, 256), dtype=torch.uint8, device=self.device)
         return self._ws, need
@@ -93,8 +145,11 @@ class SHTPlan:
         if B == 0:
             return out
         ws, nbytes = self.workspace(B, spin, 0)
-        _lib.call("ps_synthesis", self._h, ctypes.c_void_p(alm.data_ptr()), ctypes.c_void_p(out.data_ptr()),
-                  B, spin, ctypes.c_void_p(ws.data_ptr()), nbytes, self._stream())
+
+        def run(h):
+            _lib.call("ps_synthesis", h, ctypes.c_void_p(alm.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                      B, spin, ctypes.c_void_p(ws.data_ptr()), nbytes, self._stream())
+        run(self._pick(("synthesis", spin, self._bucket(B)), run))
         self.n_synthesis += B
         return out
 
@@ -116,7 +171,10 @@ class SHTPlan:
         if B == 0:
             return out
         ws, nbytes = self.workspace(B, spin, 1)
-        _lib.call("ps_adjoint", self._h, ctypes.c_void_p(map.data_ptr()), ctypes.c_void_p(out.data_ptr()),
-                  B, spin, float(scale), ctypes.c_void_p(ws.data_ptr()), nbytes, self._stream())
+
+        def run(h):
+            _lib.call("ps_adjoint", h, ctypes.c_void_p(map.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                      B, spin, float(scale), ctypes.c_void_p(ws.data_ptr()), nbytes, self._stream())
+        run(self._pick(("adjoint", spin, self._bucket(B)), run))
         self.n_adjoint += B
         return out

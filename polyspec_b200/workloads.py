@@ -143,3 +143,19 @@ def cg_fisher_setup(nside=1024, lmax=2048, n_holes=500, depth=30.0, fwhm_arcmin=
     noise = white_noise_cov(nside, depth, True)
     l_bins = np.linspace(2, lmax, nbins + 1).astype(int)
     return cl, cltot, beam, mask, noise, l_bins
+
+
+def anisotropic_noise_setup(nside, lmax, amp=3.0, depth=30.0, fwhm_arcmin=5.0, seed=0):
+    """Full-sky TEB workload with latitude-dependent white noise: the pixel noise
+    variance of the 30 uK' map is multiplied by 1 + amp z^2 (a deep equator, as a
+    scan strategy that crosses the poles less often would give).  Returns
+    (cl_raw, cl_tot, beam[3, lmax+1], mask[3, npix] (ones), noise_cov[3, npix])."""
+    cl = fiducial_cl(lmax, True)
+    b = gaussian_beam(lmax, fwhm_arcmin)
+    beam = np.stack([b, b, b])
+    nl = noise_cl(nside, lmax, depth, True)
+    cltot = total_cl(cl, beam, nl)
+    z, _ = pixel_z_phi(nside)
+    noise = white_noise_cov(nside, depth, True) * (1.0 + amp * z * z)[None, :]
+    mask = np.ones((3, 12 * nside * nside))
+    return cl, cltot, beam, mask, noise

@@ -96,8 +96,8 @@ def test_moments_and_apply_match_oracle(lmax):
     for got, want in ((C, 2 * Co), (G, 2 * Go), (T, 2 * To)):
         got = got.cpu().numpy()
         assert np.max(np.abs(got - want)) <= 1e-5 * np.max(np.abs(want))
-    Lm = g.normal(size=(nb, D, K)).astype(np.float32)
-    z = torch.einsum("abi,nbi->nai", d["sigma"], d["r"]).contiguous()
+    Lm = g.normal(size=(nb, OUT)).astype(np.float32)  # L (row-major D x K), then q
+    z = torch.einsum("abi,nbi->nai", d["sigma"].to(torch.complex128), d["r"]).contiguous()
     dLm = torch.as_tensor(Lm, device="cuda")
     _lib.call("ps_lbp_apply", Lr._vp(didx), Lr._vp(dnl), nb, Lr._vp(dLm), Lr._vp(d["sigma"]), Lr._vp(d["r"]),
               Lr._vp(z), B, nalm, Lr._stream())

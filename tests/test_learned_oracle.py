@@ -14,7 +14,7 @@ def _problem(n=7, F=6, H=5, D=6, K=2, seed=0):
     g = np.random.default_rng(seed)
     X = g.normal(size=(n, F))
     params = [g.normal(size=(H, F)) * 0.5, g.normal(size=H) * 0.1, g.normal(size=(H, H)) * 0.5, g.normal(size=H) * 0.1,
-              g.normal(size=(D * K, H)) * 0.3, g.normal(size=D * K) * 0.1]
+              g.normal(size=(D * K + 1, H)) * 0.3, g.normal(size=D * K + 1) * 0.1]
     U = g.normal(size=(n, 9, D))
     Tt = g.normal(size=(n, 9, D))
     C = np.einsum("nsd,nse->nde", U, U)
@@ -25,18 +25,19 @@ def _problem(n=7, F=6, H=5, D=6, K=2, seed=0):
 
 
 def test_loss_is_the_squared_error():
-    # J_b = Sum_s || L L^T u_s - t_s ||^2 for explicit samples
+    # J_b = Sum_s || (L L^T + d I) u_s - t_s ||^2 for explicit samples
     g = np.random.default_rng(1)
     D, K, S = 6, 2, 11
     L = g.normal(size=(1, D, K))
+    d = np.array([0.37])
     u = g.normal(size=(S, D))
     t = g.normal(size=(S, D))
     C = (u.T @ u)[None]
     Gr = u.T @ t
     G = (0.5 * (Gr + Gr.T))[None]
     T = np.array([np.sum(t * t)])
-    J, _ = O.block_loss(L, C, G, T)
-    P = L[0] @ L[0].T
+    J, _, _ = O.block_loss(L, d, C, G, T)
+    P = L[0] @ L[0].T + d[0] * np.eye(D)
     want = sum(np.sum((P @ u[s] - t[s]) ** 2) for s in range(S))
     assert abs(J[0] - want) <= 1e-10 * want
 
