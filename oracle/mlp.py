@@ -99,8 +99,8 @@ def apply(blocks, L, sigma, r, band_l):
                 sl = slice(i0, i0 + nl)
                 sq[f * band_l:f * band_l + nl] = np.sqrt(np.maximum(S[f, sl], 0.0))
                 u[f * band_l:f * band_l + nl] = r[n, f, sl]
-            Lb = L[b][:D * K].reshape(D, -1)
-            c = sq * (Lb @ (Lb.T @ (sq * u)) + 0.5 * np.tanh(L[b][D * K]) * (sq * u))
+            Lb = L[b][:-1].reshape(D, -1)
+            c = sq * (Lb @ (Lb.T @ (sq * u)) + 0.5 * np.tanh(L[b][-1]) * (sq * u))
             for f in range(3):
                 z[n, f, i0:i0 + nl] += c[f * band_l:f * band_l + nl]
     return z
