@@ -82,6 +82,25 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
 int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, int spin, double scale,
                void* workspace, size_t workspace_bytes, cudaStream_t stream);
 
+/* Legendre stages alone, in FP64 whatever the plan's precision (no reference
+ * counterpart; ducc0 exposes the same split as its leg2alm / alm2leg):
+ *   ps_legendre_synthesis  alm [batch][ncomp][nalm] -> phase [R][mmax+1][batch][ncomp]
+ *   ps_legendre_adjoint    phase -> alm (times scale), the exact adjoint
+ * where phase holds, for every ring and order m, the m-th Fourier coefficient
+ * of the ring (complex128; for spin s the pair Q, U).  Used on a ring-band plan
+ * (ps_plan_band) to build and apply the masked-band correction of the CG
+ * preconditioner.  ps_plan_band makes a plan over the nrings_north rings
+ * nearest the equator in each hemisphere (R = 2 nrings_north - 1 rings, the
+ * equator ring once), sharing the parent's tables: it must not outlive the
+ * parent and runs only the ps_legendre_* calls (ps_synthesis / ps_adjoint
+ * return PS_ERR_UNSUPPORTED on it). */
+int ps_plan_band(const ps_plan* full, int nrings_north, ps_plan** band);
+int ps_legendre_workspace_bytes(const ps_plan* plan, int batch, int spin, int adjoint, size_t* bytes);
+int ps_legendre_synthesis(const ps_plan* plan, const double* alm, double* phase, int batch, int spin,
+                          void* workspace, size_t workspace_bytes, cudaStream_t stream);
+int ps_legendre_adjoint(const ps_plan* plan, const double* phase, double* alm, int batch, int spin, double scale,
+                        void* workspace, size_t workspace_bytes, cudaStream_t stream);
+
 /* Allocation-free variant of ps_synthesis (no counterpart in the reference).
  * For callers that cannot allocate device memory at the point of the call (a
  * framework that owns all device memory through its own fixed allocator, a

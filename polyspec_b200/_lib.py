@@ -34,6 +34,12 @@ SIGNATURES = {
     "ps_adjoint": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_double, _c_void_p,
                             _c_size_t, _c_void_p]),
     "ps_synthesis_noalloc": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p]),
+    "ps_plan_band": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_void_p)]),
+    "ps_legendre_workspace_bytes": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, ctypes.POINTER(_c_size_t)]),
+    "ps_legendre_synthesis": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p, _c_size_t,
+                                       _c_void_p]),
+    "ps_legendre_adjoint": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_double, _c_void_p,
+                                     _c_size_t, _c_void_p]),
     "ps_pix_product": (_c_int, [_c_int, ctypes.POINTER(_c_void_p), _c_int, _c_void_p, _c_int64, _c_int, _c_double,
                                 _c_void_p]),
     "ps_pix_radial_sum_workspace_bytes": (_c_int, [_c_int, _c_int64, ctypes.POINTER(_c_size_t)]),

@@ -40,6 +40,9 @@ int launch_reduce_partials_f32(const float2* partial, double2* alm, int ntiles, 
 
 struct ps_plan {
   ps::Plan p;
+  // a ring-band plan (ps_plan_band) shares its parent's tables and runs the
+  // Legendre stages only
+  bool is_band = false;
   // FFT length classes: rings with the same work length share a launch
   std::vector<int> cls_len, cls_off, cls_cnt;
   int* d_ring_lists = nullptr;
@@ -292,6 +295,29 @@ int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_pl
   return PS_OK;
 }
 
+int ps_plan_band(const ps_plan* full, int nrings_north, ps_plan** out) {
+  if (!full || !out || full->is_band) return PS_ERR_INVALID;
+  const ps::Plan& F = full->p;
+  if (nrings_north < 1 || nrings_north > F.Rh || (F.R & 1) == 0) return PS_ERR_INVALID;
+  ps_plan* pl = new ps_plan();
+  pl->p = F;
+  pl->is_band = true;
+  // north rings [Rh - k, Rh) (the last one is the equator ring) and their mirrors
+  pl->p.d_rings = F.d_rings + (F.Rh - nrings_north);
+  pl->p.Rh = nrings_north;
+  pl->p.R = 2 * nrings_north - 1;
+  *out = pl;
+  return PS_OK;
+}
+
+static size_t leg_ws_bytes(const ps::Plan& P, int batch, int spin, int adjoint);
+
+int ps_legendre_workspace_bytes(const ps_plan* plan, int batch, int spin, int adjoint, size_t* bytes) {
+  if (!plan || !bytes || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  *bytes = leg_ws_bytes(plan->p, batch, spin, adjoint);
+  return PS_OK;
+}
+
 int ps_plan_destroy(ps_plan* plan) {
   if (!plan) return PS_ERR_INVALID;
   for (void* d : plan->owned) cudaFree(d);
@@ -331,6 +357,58 @@ static size_t sht_ws_bytes(const ps::Plan& P, int batch, int spin, int adjoint) 
   return phase + align256(size_t(ps::adjoint_tiles(P)) * P.nalm * nfc * sizeof(double2));
 }
 
+// FP64 Legendre stages alone (phase in and out in the caller's memory)
+static int fp64_adjoint_chunk(int batch, int spin) {
+  const int c = spin == 0 ? 8 : 4;
+  return batch < c ? batch : c;
+}
+
+static size_t leg_ws_bytes(const ps::Plan& P, int batch, int spin, int adjoint) {
+  const size_t ncomp = spin == 0 ? 1 : 2;
+  const size_t nf = size_t(batch) * ncomp;
+  if (!adjoint) return align256(size_t(P.nalm) * nf * sizeof(double2));
+  const size_t nfc = size_t(fp64_adjoint_chunk(batch, spin)) * ncomp;
+  return align256(size_t(ps::adjoint_tiles(P)) * P.nalm * nfc * sizeof(double2));
+}
+
+int ps_legendre_synthesis(const ps_plan* plan, const double* alm, double* phase, int batch, int spin,
+                          void* workspace, size_t workspace_bytes, cudaStream_t stream) {
+  if (!plan || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  if (batch == 0) return PS_OK;
+  if (!alm || !phase || !workspace) return PS_ERR_INVALID;
+  const ps::Plan& P = plan->p;
+  if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
+  if (workspace_bytes < leg_ws_bytes(P, batch, spin, 0)) return PS_ERR_WORKSPACE;
+  const int ncomp = spin == 0 ? 1 : 2;
+  double2* almT = static_cast<double2*>(workspace);
+  int rc = ps::launch_alm_to_T(reinterpret_cast<const double2*>(alm), almT, batch, ncomp, P.nalm, P.num_sms, stream);
+  if (rc) return rc;
+  return ps::launch_legendre_synth_f64(P, almT, reinterpret_cast<double2*>(phase), batch, spin, stream);
+}
+
+int ps_legendre_adjoint(const ps_plan* plan, const double* phase, double* alm, int batch, int spin, double scale,
+                        void* workspace, size_t workspace_bytes, cudaStream_t stream) {
+  if (!plan || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  if (batch == 0) return PS_OK;
+  if (!alm || !phase || !workspace) return PS_ERR_INVALID;
+  const ps::Plan& P = plan->p;
+  if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
+  if (workspace_bytes < leg_ws_bytes(P, batch, spin, 1)) return PS_ERR_WORKSPACE;
+  const int ncomp = spin == 0 ? 1 : 2;
+  double2* partial = static_cast<double2*>(workspace);
+  const int ch = fp64_adjoint_chunk(batch, spin);
+  for (int b0 = 0; b0 < batch; b0 += ch) {
+    const int bc = std::min(ch, batch - b0);
+    int rc = ps::launch_legendre_adjoint_f64(P, reinterpret_cast<const double2*>(phase), partial, batch, b0, bc,
+                                             spin, stream);
+    if (rc) return rc;
+    rc = ps::launch_reduce_partials(partial, reinterpret_cast<double2*>(alm), ps::adjoint_tiles(P), bc, ncomp,
+                                    P.nalm, scale, b0, P.num_sms, stream);
+    if (rc) return rc;
+  }
+  return PS_OK;
+}
+
 int ps_sht_workspace_bytes(const ps_plan* plan, int batch, int spin, int adjoint, size_t* bytes) {
   if (!plan || !bytes || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
   *bytes = sht_ws_bytes(plan->p, batch, spin, adjoint);
@@ -340,6 +418,7 @@ int ps_sht_workspace_bytes(const ps_plan* plan, int batch, int spin, int adjoint
 int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch, int spin, void* workspace,
                  size_t workspace_bytes, cudaStream_t stream) {
   if (!plan || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  if (plan->is_band) return PS_ERR_UNSUPPORTED;
   if (batch == 0) return PS_OK;
   if (!alm || !map || !workspace) return PS_ERR_INVALID;
   const ps::Plan& P = plan->p;
@@ -383,6 +462,7 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
 int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, int spin, double scale,
                void* workspace, size_t workspace_bytes, cudaStream_t stream) {
   if (!plan || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  if (plan->is_band) return PS_ERR_UNSUPPORTED;
   if (batch == 0) return PS_OK;
   if (!alm || !map || !workspace) return PS_ERR_INVALID;
   const ps::Plan& P = plan->p;

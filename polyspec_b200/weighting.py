@@ -123,9 +123,10 @@ class Weightings:
         d, as_torch = self.base._in(input_map, torch.float64)
         if hasattr(self, 'inpainting_mask'):
             d = self.inpaint_map(d)
-        if preconditioner == 'learned':
-            return self.base._out(self.batched_applySinv_optimal(d[None], preconditioner='learned', nstep=nstep,
-                                                                 thresh=thresh, verb=verb, lmax=lmax)[0], as_torch)
+        if preconditioner in ('learned', 'cut'):
+            return self.base._out(self.batched_applySinv_optimal(d[None], preconditioner=preconditioner,
+                                                                 nstep=nstep, thresh=thresh, verb=verb,
+                                                                 lmax=lmax)[0], as_torch)
         x0 = torch.einsum('abi,bi->ai', self.d_x0op, self.base.to_lm(d))
         cgd = CGD(self, d, x0=x0, preconditioner=preconditioner, verb=verb)
         cgd.run(nstep=nstep, thresh=thresh)
@@ -147,6 +148,13 @@ class Weightings:
         self.last_cgd = cgd
         lfilt = torch.as_tensor(self.base.l_arr <= lmax, device=self.base.device)
         return cgd.get_ivar_lm()[:, :, lfilt]
+
+    def cut_preconditioner(self):
+        """The masked-band preconditioner of this Weightings (built on first use)."""
+        if getattr(self, '_cut', None) is None:
+            from .cutprec import CutPreconditioner
+            self._cut = CutPreconditioner(self)
+        return self._cut
 
     def make_applySinv(self, kind='optimal', **kw):
         """A callable with the reference applySinv signature and a ``.batched``
@@ -207,6 +215,9 @@ class BatchedCGD:
             if self.learned is None or self.learned.L is None:
                 raise Exception("preconditioner='learned' needs a trained Weightings.learned")
             self.learned_max_steps = learned_max_steps
+        elif preconditioner == 'cut':
+            # masked-band preconditioner (polyspec_b200.cutprec), judged like 'learned'
+            self.cut = weightings.cut_preconditioner()
         b0 = self._get_b(d)
         self.x0 = x0
         b = b0 - self._apply_A(x0)
@@ -217,7 +228,7 @@ class BatchedCGD:
         z = self._apply_M(self.r, self.use_learned)
         self.rz = self.dot(self.r, z)
         self.rz0 = self.dot(b0, self._apply_M(b0, self.use_learned))
-        if preconditioner == 'learned':
+        if preconditioner in ('learned', 'cut'):
             self.judge0 = self.dot(b0, self._sigma(b0))
         self.p = z
         self.i = 0
@@ -230,7 +241,7 @@ class BatchedCGD:
 
     def _judge(self, r, rz, learned_mask, idx):
         """Stopping statistic: rz/rz0 of the plain CG (= r^T Sigma r / b^T Sigma b)."""
-        if self.preconditioner != 'learned':
+        if self.preconditioner not in ('learned', 'cut'):
             return rz / self.rz0[idx]
         return self.dot(r, self._sigma(r)) / self.judge0[idx]
 
@@ -252,6 +263,8 @@ class BatchedCGD:
 
     def _apply_M(self, ilm, learned_mask=None):
         Sig = self.W.d_Sigma
+        if self.preconditioner == 'cut':
+            return self.cut.apply(ilm)
         if self.preconditioner == 'learned':
             z = self.learned.apply(ilm)
             if learned_mask is not None and not bool(learned_mask.all()):

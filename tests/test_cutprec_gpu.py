@@ -1,0 +1,133 @@
+"""Band-restricted Legendre stages (ps_plan_band + ps_legendre_*) and the
+masked-band CG preconditioner built on them.
+
+* The band synthesis equals the m-th Fourier coefficients of the full FP64
+  synthesis on the band's rings (DFT of the ring pixels), 1e-11 relative.
+* The band adjoint is the exact adjoint of the band synthesis under plain complex
+  inner products, 1e-12 relative.
+* CG with the band preconditioner reaches the same tolerance as the plain
+  harmonic CG (same Sigma-norm stopping test) in fewer steps, and its solution
+  agrees with the plain CG's to the accuracy that tolerance allows."""
+import numpy as np
+import pytest
+
+
+def _band_rings(nside, k):
+    Rh = 2 * nside
+    north = np.arange(Rh - k, Rh)
+    south = 4 * nside - 2 - np.arange(Rh - 2, Rh - k - 1, -1)
+    return np.concatenate([north, south])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spin", [0, 2])
+def test_band_synthesis_matches_ring_dft(spin):
+    import torch
+    from polyspec_b200.sht import SHTPlan
+    from polyspec_b200.cutprec import ring_ranges
+    from polyspec_b200 import _lib
+    import ctypes
+    nside, lmax, k = 16, 40, 6
+    P = SHTPlan(nside, lmax)
+    g = torch.Generator(device="cuda").manual_seed(spin)
+    nc = 1 if spin == 0 else 2
+    alm = torch.randn((2, nc, P.nalm), dtype=torch.complex128, device="cuda", generator=g)
+    m_arr = np.concatenate([np.full(lmax + 1 - m, m) for m in range(lmax + 1)])
+    alm[:, :, torch.as_tensor(m_arr == 0, device="cuda")] = alm[:, :, torch.as_tensor(m_arr == 0, device="cuda")].real.to(torch.complex128)
+    full = P.synthesis(alm[:, 0] if spin == 0 else alm, spin)  # [2, npix] or [2, 2, npix]
+    h = ctypes.c_void_p()
+    _lib.call("ps_plan_band", P._h, k, ctypes.byref(h))
+    try:
+        Rb = 2 * k - 1
+        out = torch.empty((Rb, lmax + 1, 2, nc), dtype=torch.complex128, device="cuda")
+        n = ctypes.c_size_t()
+        _lib.call("ps_legendre_workspace_bytes", h, 2, spin, 0, ctypes.byref(n))
+        ws = torch.empty(max(int(n.value), 256), dtype=torch.uint8, device="cuda")
+        _lib.call("ps_legendre_synthesis", h, ctypes.c_void_p(alm.data_ptr()), ctypes.c_void_p(out.data_ptr()), 2,
+                  spin, ctypes.c_void_p(ws.data_ptr()), int(n.value),
+                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+    finally:
+        _lib.lib().ps_plan_destroy(h)
+    starts, counts = ring_ranges(nside)
+    fm = full.cpu().numpy().reshape(2, nc, -1)
+    ph = out.cpu().numpy()
+    from polyspec_b200.workloads import pixel_z_phi
+    _, phi = pixel_z_phi(nside)
+    err, scale = 0.0, 0.0
+    for bi, r in enumerate(_band_rings(nside, k)):
+        s, npr = int(starts[r]), int(counts[r])
+        for m in range(1, min(lmax, npr // 2 - 1) + 1):
+            e = np.exp(-1j * m * phi[s:s + npr])
+            c = (fm[:, :, s:s + npr] * e).sum(-1) / npr  # [2, nc]
+            err = max(err, float(np.abs(c - ph[bi, m]).max()))
+            scale = max(scale, float(np.abs(ph[bi, m]).max()))
+    assert err <= 1e-11 * scale, (err, scale)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spin", [0, 2])
+def test_band_adjoint_is_exact_adjoint(spin):
+    import torch
+    from polyspec_b200.sht import SHTPlan
+    from polyspec_b200 import _lib
+    import ctypes
+    nside, lmax, k = 16, 40, 5
+    P = SHTPlan(nside, lmax)
+    nc = 1 if spin == 0 else 2
+    g = torch.Generator(device="cuda").manual_seed(10 + spin)
+    x = torch.randn((3, nc, P.nalm), dtype=torch.complex128, device="cuda", generator=g)
+    Rb = 2 * k - 1
+    p = torch.randn((Rb, lmax + 1, 3, nc), dtype=torch.complex128, device="cuda", generator=g)
+    h = ctypes.c_void_p()
+    _lib.call("ps_plan_band", P._h, k, ctypes.byref(h))
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    try:
+        Lx = torch.empty_like(p)
+        n = ctypes.c_size_t()
+        _lib.call("ps_legendre_workspace_bytes", h, 3, spin, 0, ctypes.byref(n))
+        ws = torch.empty(max(int(n.value), 256), dtype=torch.uint8, device="cuda")
+        _lib.call("ps_legendre_synthesis", h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(Lx.data_ptr()), 3, spin,
+                  ctypes.c_void_p(ws.data_ptr()), int(n.value), st)
+        LHp = torch.empty_like(x)
+        _lib.call("ps_legendre_workspace_bytes", h, 3, spin, 1, ctypes.byref(n))
+        ws = torch.empty(max(int(n.value), 256), dtype=torch.uint8, device="cuda")
+        _lib.call("ps_legendre_adjoint", h, ctypes.c_void_p(p.data_ptr()), ctypes.c_void_p(LHp.data_ptr()), 3, spin,
+                  1.0, ctypes.c_void_p(ws.data_ptr()), int(n.value), st)
+        torch.cuda.synchronize()
+    finally:
+        _lib.lib().ps_plan_destroy(h)
+    lhs = complex(torch.sum(p.conj() * Lx))
+    rhs = complex(torch.sum(LHp.conj() * x))
+    assert abs(lhs - rhs) <= 1e-12 * (abs(lhs) + abs(rhs))
+
+
+@pytest.mark.gpu
+def test_cut_preconditioner_reduces_cg_steps():
+    import torch
+    from polyspec_b200 import PolySpec, Weightings
+    from polyspec_b200 import workloads as W
+    nside, lmax = 32, 64
+    cl, cltot, beam, mask, noise, lb = W.cg_fisher_setup(nside, lmax, n_holes=40)
+    base = PolySpec(nside, dict(cltot), beam=list(beam), pol=True, lmax=lmax)
+    wts = Weightings(base, mask, dict(cl), noise_cov=noise)
+    cut = wts.cut_preconditioner()
+    assert cut.enabled and cut.nband > 0 and cut.n_bad == 0
+    g = torch.Generator(device="cuda").manual_seed(0)
+    dmask = torch.as_tensor(mask, device="cuda")
+    maps = []
+    for i in range(6):
+        a = base.generate_data(seed=50 + i, output_type="harmonic", rng="device")
+        if i >= 3:  # B-mode-only skies: the slow systems of the Fisher estimator
+            a[0] = 0.0
+            a[1] = 0.0
+        maps.append(dmask * base.to_map(a))
+    maps = torch.stack(maps)
+    sol, its = {}, {}
+    for pre in ("harmonic", "cut"):
+        sol[pre] = wts.batched_applySinv_optimal(maps, preconditioner=pre, nstep=500, thresh=1e-8)
+        its[pre] = wts.last_cgd.iters.cpu().numpy()
+        assert bool((wts.last_cgd.err < 1e-8).all())
+    assert its["cut"].sum() < its["harmonic"].sum(), its
+    rel = float((sol["cut"] - sol["harmonic"]).abs().max() / sol["harmonic"].abs().max())
+    assert rel < 1e-3, rel
