@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     p.add_argument("--prec", default="mixed", choices=["fp64", "mixed"])
     p.add_argument("--unbatched", action="store_true", help="one CG solve at a time (reference structure)")
+    p.add_argument("--precond", default="cut", choices=["harmonic", "cut", "learned"],
+                   help="CG preconditioner of the CUDA arm (stopping test: the plain CG's r^T Sigma r / b^T Sigma b)")
     p.add_argument("--no-fp64-compare", action="store_true")
     p.add_argument("--nside", type=int, default=1024)
     p.add_argument("--lmax", type=int, default=2048)
@@ -64,9 +66,9 @@ def parse():
 
 
 def workload_config(a):
-    return {"workload": "PSpecBin TT/TE/EE/BB Fisher contribution, masked CG S^-1 (harmonic preconditioner, "
-                        "rz/rz0<1e-6), TEB Nside %d lmax %d, 8 linear bins, 30uK' white noise, 10%% cut + 500 holes"
-                        % (a.nside, a.lmax),
+    return {"workload": "PSpecBin TT/TE/EE/BB Fisher contribution, masked CG S^-1 to the reference's residual "
+                        "test (r^T Sigma r / b^T Sigma b < 1e-6, Sigma the harmonic preconditioner), TEB Nside %d "
+                        "lmax %d, 8 linear bins, 30uK' white noise, 10%% cut + 500 holes" % (a.nside, a.lmax),
             "nside": a.nside, "lmax": a.lmax, "fields": list(FIELDS), "n_bins": 8,
             "l2": "inputs larger than L2 (maps 3x%d MB, alm 3x%d MB per solve, batched working set several GB)"
                   % (12 * a.nside ** 2 * 8 // 2 ** 20, (a.lmax + 1) * (a.lmax + 2) // 2 * 16 // 2 ** 20)}
@@ -180,6 +182,16 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def psb_rows_maps(base, mask, l_bins, a_lm):
+    """The N_p + 1 masked maps whose S^-1 a Fisher contribution needs (training data)."""
+    import torch
+    from polyspec_b200 import PSpecBin
+    psb = PSpecBin(base, mask, None, l_bins, fields=list(FIELDS))
+    rows = psb._Q2_rows(base.applyAinv(a_lm, input_type='harmonic'))
+    alms = torch.stack([psb.d_beam * a_lm] + [psb.d_beam * r for r in rows])
+    return psb.d_mask[None] * base.to_map_batch(alms)
+
+
 # ---------------------------------------------------------------------- plain FP64 GPU + accuracy
 def fp64_compare(a, setup, seed):
     """One Fisher step of the plain FP64 GPU backend (same batched structure,
@@ -257,7 +269,24 @@ def run_cuda(a):
     cl, cltot, beam, mask, noise, l_bins = setup
     base = PolySpec(a.nside, dict(cltot), beam=list(beam), pol=True, lmax=a.lmax, prec=a.prec)
     wts = Weightings(base, mask, dict(cl), noise_cov=noise)
-    applySinv = wts.make_applySinv("optimal", preconditioner="harmonic", nstep=NSTEP, thresh=THRESH)
+    # one-time set-up of the preconditioner (per Weightings, outside the timed region)
+    torch.cuda.synchronize()
+    t_setup = time.time()
+    if a.precond == "cut":
+        wts.cut_preconditioner()
+    elif a.precond == "learned":
+        from polyspec_b200.learned import LearnedBandPreconditioner
+        lp = LearnedBandPreconditioner(wts)
+        tr = [base.generate_data(seed=900 + i, output_type="harmonic", deconvolve_beam=True, rng="device")
+              for i in range(2)]
+        for i, t_alm in enumerate(tr):
+            rows = psb_rows_maps(base, mask, l_bins, t_alm)
+            lp.collect(rows, nstep=NSTEP)
+        lp.train(epochs=400)
+        wts.learned = lp
+    torch.cuda.synchronize()
+    setup_s = time.time() - t_setup
+    applySinv = wts.make_applySinv("optimal", preconditioner=a.precond, nstep=NSTEP, thresh=THRESH)
     psb = PSpecBin(base, mask, applySinv, l_bins, fields=list(FIELDS))
 
     nsteps = a.warmup + 2 * a.steps
@@ -375,7 +404,9 @@ def run_cuda(a):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": t_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if a.prec == "fp64" else "f32+tf32", "data": "synthetic",
-            "config": dict(workload_config(a), parallelism="replicas x%d" % world, prec=a.prec),
+            "config": dict(workload_config(a), parallelism="replicas x%d" % world, prec=a.prec,
+                           preconditioner=a.precond, batched=not a.unbatched),
+            "preconditioner_setup_s": setup_s,
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clocks,
             "sht_teb_per_step": {"synthesis": rev / 2.0, "adjoint": fwd / 2.0},
             "cg_iters_per_solve": iters_per_solve,
