@@ -250,6 +250,21 @@ def fp64_compare(a, setup, seed):
     return plain, acc
 
 
+# ---------------------------------------------------------------------- replicas
+def replica_seeds(rank, nsteps):
+    """Seeds of one rank's Fisher simulations: disjoint across ranks (replicas, no collective)."""
+    return [rank * 100000 + i for i in range(nsteps)]
+
+
+def max_over_ranks(ms, device):
+    """The slowest rank's time (the job's time), from an all-reduce of one scalar."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t)
+
+
 # ---------------------------------------------------------------------- CUDA arm
 def run_cuda(a):
     import torch
@@ -290,7 +305,7 @@ def run_cuda(a):
     psb = PSpecBin(base, mask, applySinv, l_bins, fields=list(FIELDS))
 
     nsteps = a.warmup + 2 * a.steps
-    seeds = [rank * 100000 + i for i in range(nsteps)]
+    seeds = replica_seeds(rank, nsteps)
     a_dev = [base.generate_data(seed=s + int(1e7), output_type="harmonic", deconvolve_beam=True, rng="device")
              for s in seeds]
     torch.cuda.synchronize()
@@ -336,9 +351,7 @@ def run_cuda(a):
     fwd = (base.n_SHTs_forward - f0) / a.steps
     rev = (base.n_SHTs_reverse - r0) / a.steps
     if world > 1:
-        t = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t)
+        t_ms = max_over_ranks(t_ms, "cuda")
     value = world * a.steps / (t_ms / 1e3)
 
     # ---- end to end through the public API, host buffers
@@ -356,9 +369,7 @@ def run_cuda(a):
     e2e_ms = max(e0.elapsed_time(e1), (time.time() - t0) * 1e3)
     barrier()
     if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t)
+        e2e_ms = max_over_ranks(e2e_ms, "cuda")
     e2e = {"value": world * a.steps / (e2e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": int(host_a[0].numel() * host_a[0].element_size()),
            "d2h_bytes_per_step": int(fish.nbytes)}
@@ -413,7 +424,7 @@ def run_cuda(a):
             "cg_iters_of_each_solve": solve_iters[-1] if solve_iters else None,
             "kernel_ms": {k: round(v[1], 3) for k, v in stats.items() if v[0]}}
 
-    if a.prec != "fp64" and not a.no_fp64_compare:
+    if a.prec != "fp64" and not a.no_fp64_compare and world == 1:
         del psb, applySinv, wts, a_dev, base
         torch.cuda.empty_cache()
         line["plain_fp64_gpu"], line["accuracy"] = fp64_compare(a, setup, seeds[0])

