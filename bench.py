@@ -432,7 +432,8 @@ def run_cuda(a):
 
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         t_pair, cores = cpu_pair_time(a, setup, a.cpu_sample_pairs)
-        ips = iters_per_solve if np.isfinite(iters_per_solve) else PLAIN_CG_ITERS
+        # the reference's CPU path runs the plain harmonic CG: its step count, not this arm's
+        ips = PLAIN_CG_ITERS
         per_sim = pairs_per_sim(ips) * t_pair
         line["cpu_baseline"] = {
             "value": 1.0 / per_sim, "unit": UNIT, "cores": cores, "kind": "port",

@@ -6,8 +6,8 @@ masked-band CG preconditioner built on them.
 * The band adjoint is the exact adjoint of the band synthesis under plain complex
   inner products, 1e-12 relative.
 * CG with the band preconditioner reaches the same tolerance as the plain
-  harmonic CG (same Sigma-norm stopping test) in fewer steps, and its solution
-  agrees with the plain CG's to the accuracy that tolerance allows."""
+  harmonic CG (same Sigma-norm stopping test, checked on the recomputed true
+  residual b - A x) in fewer steps."""
 import numpy as np
 import pytest
 
@@ -126,11 +126,16 @@ def test_cut_preconditioner_reduces_cg_steps():
             a[1] = 0.0
         maps.append(dmask * base.to_map(a))
     maps = torch.stack(maps)
-    sol, its = {}, {}
+    its = {}
     for pre in ("harmonic", "cut"):
-        sol[pre] = wts.batched_applySinv_optimal(maps, preconditioner=pre, nstep=500, thresh=1e-8)
-        its[pre] = wts.last_cgd.iters.cpu().numpy()
-        assert bool((wts.last_cgd.err < 1e-8).all())
+        wts.batched_applySinv_optimal(maps, preconditioner=pre, nstep=500, thresh=1e-8)
+        cg = wts.last_cgd
+        its[pre] = cg.iters.cpu().numpy()
+        assert bool((cg.err < 1e-8).all())
+        # the true residual b - A x (recomputed, not the CG recurrence) meets the same test
+        b0 = cg._get_b(maps)
+        r = b0 - cg._apply_A(cg.x0 + cg.x)
+        sig = lambda v: torch.einsum('abi,nbi->nai', wts.d_Sigma, v)
+        true_err = cg.dot(r, sig(r)) / cg.dot(b0, sig(b0))
+        assert bool((true_err < 1e-7).all()), (pre, true_err)
     assert its["cut"].sum() < its["harmonic"].sum(), its
-    rel = float((sol["cut"] - sol["harmonic"]).abs().max() / sol["harmonic"].abs().max())
-    assert rel < 1e-3, rel
