@@ -9,8 +9,8 @@
  *    C++ exception crosses the ABI.  ps_error_string() names a code.
  *  - Every data pointer is a device pointer owned by the caller.  Plans own
  *    only their read-only tables (ring geometry, Legendre seeds, FFT tables);
- *    a plan is immutable after ps_plan_create and may be shared by callers
- *    on different streams.  Scratch memory is passed in explicitly
+ *    apart from its tile setting (ps_plan_set_tile) a plan is immutable after
+ *    ps_plan_create and may be shared by callers on different streams.  Scratch memory is passed in explicitly
  *    (ps_*_workspace_bytes gives the size), so no call allocates.
  *  - Work is enqueued on the given stream; nothing synchronises the host.
  *  - Layouts (as in the reference and ducc0): alm are complex128 (re, im
@@ -60,6 +60,15 @@ int ps_plan_info(const ps_plan* plan, int* nside, int* lmax, int64_t* npix, int6
  * (they then return without completing).  Reads it (synchronously, after the
  * device finishes its work) and optionally clears it.  No reference counterpart. */
 int ps_plan_error_flag(const ps_plan* plan, int* value, int reset);
+
+/* Tile setting of the Legendre stages (no reference counterpart): maps per CTA
+ * for direction 0 (synthesis) or 1 (adjoint) and one spin; 0 restores the
+ * library's choice by batch size.  Allowed: mixed synthesis spin 0 {8, 16, 32},
+ * spin s {4, 8}; mixed adjoint spin 0 {1, 8}, spin s {1, 4}; FP64 synthesis
+ * spin 0 {1, 4}, spin s {1, 2}; FP64 adjoint spin 0 {1, 4}, spin s {1}
+ * (PS_ERR_UNSUPPORTED otherwise).  Used by the autotuner; it changes the plan,
+ * so it must not run concurrently with transforms on the same plan. */
+int ps_plan_set_tile(ps_plan* plan, int direction, int spin, int tile);
 
 /* prec = PS_PREC_FP64: every stage in FP64.  prec = PS_PREC_MIXED: the
  * synthesis' Legendre stage runs on the tensor cores (tcgen05, TF32 split in

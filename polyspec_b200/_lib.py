@@ -35,6 +35,7 @@ SIGNATURES = {
                             _c_size_t, _c_void_p]),
     "ps_synthesis_noalloc": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p]),
     "ps_plan_band": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_void_p)]),
+    "ps_plan_set_tile": (_c_int, [_c_void_p, _c_int, _c_int, _c_int]),
     "ps_legendre_workspace_bytes": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_legendre_synthesis": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p, _c_size_t,
                                        _c_void_p]),

@@ -51,6 +51,9 @@ struct Plan {
   int n_bs_slots;
   int64_t bs_total;
   int num_sms;
+  // maps per CTA of the Legendre stages, [direction 0 synthesis / 1 adjoint][spin];
+  // 0 = the launcher's own choice (set by ps_plan_set_tile, e.g. from the autotuner)
+  int tile[2][4];
 };
 
 // ---------------------------------------------------------------------------

@@ -500,8 +500,9 @@ int launch_legendre_synth_f64(const Plan& P, const double2* almT, double2* phase
                               cudaStream_t st) {
   StatScope sc(PS_K_LEG_SYNTH, leg_flops(P, B, spin), leg_bytes(P, B, spin), st);
   dim3 grid((P.Rh + SYN_THREADS - 1) / SYN_THREADS, P.mmax + 1, 1);
+  const int t = P.tile[0][spin];
   if (spin == 0) {
-    if (B >= 4) {
+    if (t ? t == 4 : B >= 4) {
       grid.z = (B + 3) / 4;
       synth0_f64<4><<<grid, SYN_THREADS, 0, st>>>(P.d_rings, P.d_mnorm0, almT, phase, P.R, P.Rh, P.lmax, P.mmax, B);
     } else {
@@ -510,7 +511,7 @@ int launch_legendre_synth_f64(const Plan& P, const double2* almT, double2* phase
     }
   } else {
     if (!P.d_seed[spin]) return PS_ERR_INVALID;
-    if (B >= 2) {
+    if (t ? t == 2 : B >= 2) {
       grid.z = (B + 1) / 2;
       synthS_f64<2><<<grid, SYN_THREADS, 0, st>>>(P.d_rings, P.d_seed[spin], almT, phase, P.R, P.Rh, P.lmax,
                                                   P.mmax, B, spin);
@@ -531,8 +532,9 @@ int launch_legendre_adjoint_f64(const Plan& P, const double2* phase, double2* pa
                                 int spin, cudaStream_t st) {
   StatScope sc(PS_K_LEG_ADJOINT, leg_flops(P, Bc, spin), leg_bytes(P, Bc, spin), st);
   dim3 grid(adjoint_tiles(P), P.mmax + 1, 1);
+  const int t = P.tile[1][spin];
   if (spin == 0) {
-    if (Bc >= 4) {
+    if (t ? t == 4 : Bc >= 4) {
       grid.z = (Bc + 3) / 4;
       adj0_f64<4><<<grid, ADJ_THREADS, 0, st>>>(P.d_rings, P.d_mnorm0, phase, partial, P.R, P.Rh, P.lmax, P.mmax,
                                                 B, bofs, Bc, P.nalm);

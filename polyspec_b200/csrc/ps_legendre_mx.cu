@@ -340,8 +340,9 @@ int launch_legendre_adjoint_mx(const Plan& P, const float2* phase, float2* parti
   const double bytes = double(Bc) * (spin == 0 ? 1 : 2) * (8.0 * P.R * (P.mmax + 1) + 8.0 * P.nalm * mx_adjoint_tiles(P));
   StatScope sc(PS_K_LEG_ADJOINT, flops, bytes, st);
   dim3 grid(mx_adjoint_tiles(P), P.mmax + 1, 1);
+  const int t = P.tile[1][spin];
   if (spin == 0) {
-    if (Bc >= 8) {
+    if (t ? t == 8 : Bc >= 8) {
       grid.z = (Bc + 7) / 8;
       adj0_mx<8><<<grid, MX_THREADS, 0, st>>>(P.d_rings, P.d_mnorm0, phase, partial, P.R, P.Rh, P.lmax, P.mmax, B,
                                               bofs, Bc, P.nalm);
@@ -352,7 +353,7 @@ int launch_legendre_adjoint_mx(const Plan& P, const float2* phase, float2* parti
     }
   } else {
     if (!P.d_seed[spin]) return PS_ERR_INVALID;
-    if (Bc >= 4) {
+    if (t ? t == 4 : Bc >= 4) {
       grid.z = (Bc + 3) / 4;
       const int smem = int(sizeof(AdjSSmem<4>));
       // the opt-in attribute is per device: remember the devices it was set on

@@ -452,14 +452,17 @@ int launch_legendre_synth_tc(const Plan& P, const double2* almT, float2* phase, 
   const double flops = double(spin == 0 ? 4 : 16) * double(P.Rh) * double(P.nalm) * B;
   const double bytes = double(B) * (spin == 0 ? 1 : 2) * (16.0 * P.nalm + 8.0 * P.R * (P.mmax + 1));
   StatScope sc(PS_K_LEG_SYNTH, flops, bytes, st);
-  // BC (maps per CTA) bounded by the FP32 running sums a thread keeps: 4 BC (spin 0), 16 BC (spin s)
+  // BC (maps per CTA): the plan's tile setting if any, else by batch size
+  const int t = P.tile[0][spin];
   if (spin == 0) {
-    if (B > 16) return launch_synth_tc<1, 32>(P, almT, phase, B, 0, err_flag, st);
-    if (B > 8) return launch_synth_tc<1, 16>(P, almT, phase, B, 0, err_flag, st);
+    const int bc = t ? t : (B > 16 ? 32 : B > 8 ? 16 : 8);
+    if (bc == 32) return launch_synth_tc<1, 32>(P, almT, phase, B, 0, err_flag, st);
+    if (bc == 16) return launch_synth_tc<1, 16>(P, almT, phase, B, 0, err_flag, st);
     return launch_synth_tc<1, 8>(P, almT, phase, B, 0, err_flag, st);
   }
   if (!P.d_seed[spin]) return PS_ERR_INVALID;
-  if (B > 4) return launch_synth_tc<2, 8>(P, almT, phase, B, spin, err_flag, st);
+  const int bc = t ? t : (B > 4 ? 8 : 4);
+  if (bc == 8) return launch_synth_tc<2, 8>(P, almT, phase, B, spin, err_flag, st);
   return launch_synth_tc<2, 4>(P, almT, phase, B, spin, err_flag, st);
 }
 

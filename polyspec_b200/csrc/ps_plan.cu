@@ -145,6 +145,8 @@ int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_pl
   P.npix = 12 * int64_t(nside) * nside;
   P.nalm = int64_t(lmax + 1) * (lmax + 2) / 2;
   for (int s = 0; s < 4; ++s) P.d_seed[s] = nullptr;
+  for (int d = 0; d < 2; ++d)
+    for (int s = 0; s < 4; ++s) P.tile[d][s] = 0;
   if (ps_device_sm_count(&P.num_sms) != PS_OK) { delete pl; return PS_ERR_CUDA; }
   int err = PS_OK;
 
@@ -295,6 +297,25 @@ int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_pl
   return PS_OK;
 }
 
+// Allowed maps-per-CTA of the Legendre stages: {prec}{direction}{spin 0, spin s}
+static bool tile_allowed(int prec, int direction, int spin, int tile) {
+  if (tile == 0) return true;
+  const bool s0 = spin == 0;
+  if (prec == PS_PREC_MIXED) {
+    if (direction == 0) return s0 ? (tile == 8 || tile == 16 || tile == 32) : (tile == 4 || tile == 8);
+    return s0 ? (tile == 1 || tile == 8) : (tile == 1 || tile == 4);
+  }
+  if (direction == 0) return s0 ? (tile == 1 || tile == 4) : (tile == 1 || tile == 2);
+  return s0 ? (tile == 1 || tile == 4) : tile == 1;
+}
+
+int ps_plan_set_tile(ps_plan* plan, int direction, int spin, int tile) {
+  if (!plan || direction < 0 || direction > 1 || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  if (!tile_allowed(plan->p.prec, direction, spin, tile)) return PS_ERR_UNSUPPORTED;
+  plan->p.tile[direction][spin] = tile;
+  return PS_OK;
+}
+
 int ps_plan_band(const ps_plan* full, int nrings_north, ps_plan** out) {
   if (!full || !out || full->is_band) return PS_ERR_INVALID;
   const ps::Plan& F = full->p;
@@ -302,6 +323,8 @@ int ps_plan_band(const ps_plan* full, int nrings_north, ps_plan** out) {
   ps_plan* pl = new ps_plan();
   pl->p = F;
   pl->is_band = true;
+  for (int d = 0; d < 2; ++d)
+    for (int s = 0; s < 4; ++s) pl->p.tile[d][s] = 0;  // the band runs the FP64 kernels
   // north rings [Rh - k, Rh) (the last one is the equator ring) and their mirrors
   pl->p.d_rings = F.d_rings + (F.Rh - nrings_north);
   pl->p.Rh = nrings_north;

@@ -10,12 +10,12 @@ return CUDA tensors in the ducc0 layout used by the reference
 
 ``adjoint`` is ducc0's ``adjoint_synthesis`` times ``scale``.
 
-With ``prec='mixed'`` the plan also holds an FP64 plan and autotunes, per
-(direction, spin, batch size), which of the two pipelines runs: the first call
-of each kind times both (CUDA events, after one untimed run each) and keeps
-the faster one.  The tensor-core pipeline wins at large batches; for one or
-a few maps the FP64 CUDA-core kernels are faster (and exact to FP64).  The
-choices are visible in ``SHTPlan.tuned``.
+With ``autotune=True`` (default) the first call of each (direction, spin,
+batch bucket) times the candidate tile shapes of the Legendre kernels and, for
+``prec='mixed'``, the FP64 pipeline too (an FP64 plan is kept beside the mixed
+one) and keeps the fastest (polyspec_b200.autotune; choices cached in JSON).
+The tensor-core pipeline wins at large batches; for one or a few maps the FP64
+CUDA-core kernels are faster (and exact to FP64).
 """
 import ctypes
 
@@ -48,15 +48,21 @@ class SHTPlan:
                       _lib.PS_PREC_FP64 if prec == "fp64" else _lib.PS_PREC_MIXED, ctypes.byref(h))
         self._h = h
         self._ws = None
-        # mixed precision: an FP64 plan beside it for the autotuned small-batch path
+        # autotuning: tile shapes of this plan and, for mixed precision, an FP64 plan
+        # beside it for the small-batch path
         self._h64 = None
-        self.tuned = {}
-        if prec != "fp64" and autotune:
-            h64 = ctypes.c_void_p()
-            with torch.cuda.device(self.device):
-                _lib.call("ps_plan_create", self.nside, self.lmax, self.lmax, mask, _lib.PS_PREC_FP64,
-                          ctypes.byref(h64))
-            self._h64 = h64
+        self._tuner = None
+        if autotune:
+            from .autotune import Tuner
+            handles = {"fp64" if prec == "fp64" else "mixed": h}
+            if prec != "fp64":
+                h64 = ctypes.c_void_p()
+                with torch.cuda.device(self.device):
+                    _lib.call("ps_plan_create", self.nside, self.lmax, self.lmax, mask, _lib.PS_PREC_FP64,
+                              ctypes.byref(h64))
+                self._h64 = h64
+                handles["fp64"] = h64
+            self._tuner = Tuner(self.nside, self.lmax, handles, self.device)
         # counters of transforms issued through this plan
         self.n_synthesis = 0
         self.n_adjoint = 0
@@ -69,35 +75,14 @@ class SHTPlan:
                 setattr(self, name, None)
 
     # ------------------------------------------------------------ autotuning
-    @staticmethod
-    def _bucket(B):
-        if B <= 8:
-            return B
-        b = 16
-        while b < B:
-            b *= 2
-        return b
-
     def _pick(self, key, run):
-        """Plan handle for `key` = (direction, spin, batch bucket); `run(handle)` issues
-        the transform.  Times both pipelines on the first call of a key."""
-        if self._h64 is None:
+        """Plan handle for `key` = (direction, spin, batch); `run(handle)` issues the
+        transform.  With autotuning, the first call of a key times every pipeline and
+        tile shape (polyspec_b200.autotune)."""
+        if self._tuner is None:
             return self._h
-        choice = self.tuned.get(key)
-        if choice is None:
-            times = {}
-            for name, h in (("mixed", self._h), ("fp64", self._h64)):
-                run(h)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                run(h)
-                e1.record()
-                torch.cuda.synchronize()
-                times[name] = e0.elapsed_time(e1)
-            choice = min(times, key=times.get)
-            self.tuned[key] = choice
-            self.tuned[key + ("ms",)] = times
-        return self._h if choice == "mixed" else self._h64
+        direction, spin, B = key
+        return self._tuner.select(0 if direction == "synthesis" else 1, spin, B, run)
 
     def error_flag(self, reset=True):
         """Device error flag of the plan (set by a kernel whose bounded wait expired)."""
@@ -149,7 +134,7 @@ class SHTPlan:
         def run(h):
             _lib.call("ps_synthesis", h, ctypes.c_void_p(alm.data_ptr()), ctypes.c_void_p(out.data_ptr()),
                       B, spin, ctypes.c_void_p(ws.data_ptr()), nbytes, self._stream())
-        run(self._pick(("synthesis", spin, self._bucket(B)), run))
+        run(self._pick(("synthesis", spin, B), run))
         self.n_synthesis += B
         return out
 
@@ -175,6 +160,6 @@ class SHTPlan:
         def run(h):
             _lib.call("ps_adjoint", h, ctypes.c_void_p(map.data_ptr()), ctypes.c_void_p(out.data_ptr()),
                       B, spin, float(scale), ctypes.c_void_p(ws.data_ptr()), nbytes, self._stream())
-        run(self._pick(("adjoint", spin, self._bucket(B)), run))
+        run(self._pick(("adjoint", spin, B), run))
         self.n_adjoint += B
         return out
