@@ -60,7 +60,9 @@ class Tuner:
             gpu = torch.cuda.get_device_name(device)
         except Exception:
             gpu = "gpu"
-        self.prefix = "%s|nside%d|lmax%d" % (gpu, nside, lmax)
+        # the candidate set is part of the key: an FP64-only plan and a mixed plan (which
+        # may also run the FP64 pipeline) tune separately
+        self.prefix = "%s|nside%d|lmax%d|%s" % (gpu, nside, lmax, "+".join(sorted(self.handles)))
         self.choices = {}
         self.disk = _load()
 

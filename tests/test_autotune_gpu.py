@@ -33,7 +33,7 @@ def test_tiles_agree_and_choice_is_cached(tmp_path, monkeypatch):
     out = P.synthesis(alm, 2)
     assert float((out - want).abs().max() / want.abs().max()) < 1e-5
     d = json.loads(cache.read_text())
-    (key, choice), = [(k, v) for k, v in d.items() if "synthesis|spin2|b5" in k]
+    (key, choice), = [(k, v) for k, v in d.items() if "fp64+mixed|synthesis|spin2|b5" in k]
     assert choice["ms"]["%s/%d" % (choice["pipeline"], choice["tile"])] == min(choice["ms"].values())
     # a new plan reads the choice back without timing again
     P2 = SHTPlan(nside, lmax, prec="mixed")
