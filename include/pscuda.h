@@ -91,8 +91,9 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
 int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, int spin, double scale,
                void* workspace, size_t workspace_bytes, cudaStream_t stream);
 
-/* Legendre stages alone, in FP64 whatever the plan's precision (no reference
- * counterpart; ducc0 exposes the same split as its leg2alm / alm2leg):
+/* Legendre stages alone (no reference counterpart; ducc0 exposes the same split
+ * as its leg2alm / alm2leg), in the plan's precision (a mixed plan converts the
+ * phases to complex64 internally; inputs and outputs stay complex128):
  *   ps_legendre_synthesis  alm [batch][ncomp][nalm] -> phase [R][mmax+1][batch][ncomp]
  *   ps_legendre_adjoint    phase -> alm (times scale), the exact adjoint
  * where phase holds, for every ring and order m, the m-th Fourier coefficient

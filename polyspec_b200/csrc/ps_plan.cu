@@ -324,7 +324,7 @@ int ps_plan_band(const ps_plan* full, int nrings_north, ps_plan** out) {
   pl->p = F;
   pl->is_band = true;
   for (int d = 0; d < 2; ++d)
-    for (int s = 0; s < 4; ++s) pl->p.tile[d][s] = 0;  // the band runs the FP64 kernels
+    for (int s = 0; s < 4; ++s) pl->p.tile[d][s] = 0;  // the launchers' own choice on the band
   // north rings [Rh - k, Rh) (the last one is the equator ring) and their mirrors
   pl->p.d_rings = F.d_rings + (F.Rh - nrings_north);
   pl->p.Rh = nrings_north;
@@ -380,16 +380,43 @@ static size_t sht_ws_bytes(const ps::Plan& P, int batch, int spin, int adjoint) 
   return phase + align256(size_t(ps::adjoint_tiles(P)) * P.nalm * nfc * sizeof(double2));
 }
 
-// FP64 Legendre stages alone (phase in and out in the caller's memory)
+// Legendre stages alone (phase in and out in the caller's memory, complex128).
+// A mixed-precision plan runs its tensor-core synthesis / FP32 adjoint kernels
+// with the phases converted to complex64 in the workspace.
 static int fp64_adjoint_chunk(int batch, int spin) {
   const int c = spin == 0 ? 8 : 4;
   return batch < c ? batch : c;
 }
 
+namespace {
+__global__ void phase_f32_to_f64(const float2* __restrict__ in, double2* __restrict__ out, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const float2 v = in[i];
+    out[i] = make_double2(double(v.x), double(v.y));
+  }
+}
+__global__ void phase_f64_to_f32(const double2* __restrict__ in, float2* __restrict__ out, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const double2 v = in[i];
+    out[i] = make_float2(float(v.x), float(v.y));
+  }
+}
+int convert_grid(int64_t n, int sms) {
+  const int64_t need = (n + 255) / 256, cap = int64_t(sms) * 8;
+  return int(need < cap ? need : cap);
+}
+}  // namespace
+
 static size_t leg_ws_bytes(const ps::Plan& P, int batch, int spin, int adjoint) {
   const size_t ncomp = spin == 0 ? 1 : 2;
   const size_t nf = size_t(batch) * ncomp;
-  if (!adjoint) return align256(size_t(P.nalm) * nf * sizeof(double2));
+  const bool mixed = P.prec == PS_PREC_MIXED;
+  const size_t phase32 = mixed ? align256(size_t(P.R) * (P.mmax + 1) * nf * sizeof(float2)) : 0;
+  if (!adjoint) return align256(size_t(P.nalm) * nf * sizeof(double2)) + phase32;
+  if (mixed) {
+    const size_t nfc = size_t(adjoint_chunk(P, batch, spin)) * ncomp;
+    return phase32 + align256(size_t(ps::mx_adjoint_tiles(P)) * P.nalm * nfc * sizeof(float2));
+  }
   const size_t nfc = size_t(fp64_adjoint_chunk(batch, spin)) * ncomp;
   return align256(size_t(ps::adjoint_tiles(P)) * P.nalm * nfc * sizeof(double2));
 }
@@ -406,6 +433,16 @@ int ps_legendre_synthesis(const ps_plan* plan, const double* alm, double* phase,
   double2* almT = static_cast<double2*>(workspace);
   int rc = ps::launch_alm_to_T(reinterpret_cast<const double2*>(alm), almT, batch, ncomp, P.nalm, P.num_sms, stream);
   if (rc) return rc;
+  if (P.prec == PS_PREC_MIXED) {
+    float2* ph32 = reinterpret_cast<float2*>(static_cast<char*>(workspace) +
+                                             align256(size_t(P.nalm) * batch * ncomp * sizeof(double2)));
+    rc = ps::launch_legendre_synth_tc(P, almT, ph32, batch, spin, P.d_err, stream);
+    if (rc) return rc;
+    const int64_t n = int64_t(P.R) * (P.mmax + 1) * batch * ncomp;
+    phase_f32_to_f64<<<convert_grid(n, P.num_sms), 256, 0, stream>>>(ph32, reinterpret_cast<double2*>(phase), n);
+    PS_LAUNCH_CHECK();
+    return PS_OK;
+  }
   return ps::launch_legendre_synth_f64(P, almT, reinterpret_cast<double2*>(phase), batch, spin, stream);
 }
 
@@ -418,6 +455,23 @@ int ps_legendre_adjoint(const ps_plan* plan, const double* phase, double* alm, i
   if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
   if (workspace_bytes < leg_ws_bytes(P, batch, spin, 1)) return PS_ERR_WORKSPACE;
   const int ncomp = spin == 0 ? 1 : 2;
+  if (P.prec == PS_PREC_MIXED) {
+    const int64_t n = int64_t(P.R) * (P.mmax + 1) * batch * ncomp;
+    float2* ph32 = static_cast<float2*>(workspace);
+    float2* partial = reinterpret_cast<float2*>(static_cast<char*>(workspace) + align256(size_t(n) * sizeof(float2)));
+    phase_f64_to_f32<<<convert_grid(n, P.num_sms), 256, 0, stream>>>(reinterpret_cast<const double2*>(phase), ph32, n);
+    PS_LAUNCH_CHECK();
+    const int ch = adjoint_chunk(P, batch, spin);
+    for (int b0 = 0; b0 < batch; b0 += ch) {
+      const int bc = std::min(ch, batch - b0);
+      int rc = ps::launch_legendre_adjoint_mx(P, ph32, partial, batch, b0, bc, spin, stream);
+      if (rc) return rc;
+      rc = ps::launch_reduce_partials_f32(partial, reinterpret_cast<double2*>(alm), ps::mx_adjoint_tiles(P), bc, ncomp,
+                                          P.nalm, scale, b0, P.num_sms, stream);
+      if (rc) return rc;
+    }
+    return PS_OK;
+  }
   double2* partial = static_cast<double2*>(workspace);
   const int ch = fp64_adjoint_chunk(batch, spin);
   for (int b0 = 0; b0 < batch; b0 += ch) {

@@ -20,9 +20,10 @@ coefficient of each ring), L^H its exact adjoint, and Om = n_phi w on those ring
 (Y_c^H w Y_c = L^H Om L for one m).  K_m is 3 R x 3 R (T, Q, U on R band rings)
 for every m; it is built once, by applying the operator to unit vectors of the
 band's phase space (all m at once: the operator is diagonal in m), and inverted
-with a batched Cholesky factorisation.  Applying M costs a band-restricted
-Legendre synthesis and adjoint (R / (4 Nside) of a full transform's Legendre
-work) and one batched matrix product per CG step.  Holes outside the band and
+with a batched Cholesky factorisation (the band stages in FP64 for this).
+Applying M costs a band-restricted Legendre synthesis and adjoint in the plan's
+precision (R / (4 Nside) of a full transform's Legendre work) and one batched
+matrix product per CG step.  Holes outside the band and
 the quadrature error of the HEALPix grid are left to the CG.
 
 M is symmetric positive definite whenever the model is (K_m positive definite),
@@ -91,10 +92,22 @@ class CutPreconditioner:
         if not self.enabled:
             return
         P = base.plan(lmax)
-        h = ctypes.c_void_p()
-        _lib.call("ps_plan_band", P._h, k, ctypes.byref(h))
-        self._band = h
-        self._plan = P  # keeps the parent plan alive
+        self._plan = P  # keeps the parent plans alive
+        # the set-up runs the band stages in FP64 (K_m is ill-conditioned where the
+        # band matters most); the per-step application in the plan's precision
+        h_setup = P._h64 if P._h64 is not None else None
+        self._own64 = None
+        if h_setup is None and base.prec == "fp64":
+            h_setup = P._h
+        if h_setup is None:
+            h_setup = ctypes.c_void_p()
+            _lib.call("ps_plan_create", nside, lmax, lmax, 0b101, _lib.PS_PREC_FP64, ctypes.byref(h_setup))
+            self._own64 = h_setup
+        self._band64 = ctypes.c_void_p()
+        _lib.call("ps_plan_band", h_setup, k, ctypes.byref(self._band64))
+        self._band = ctypes.c_void_p()
+        _lib.call("ps_plan_band", P._h, k, ctypes.byref(self._band))
+        self._use = self._band64
         self.Rb = 2 * k - 1
         self.M = lmax + 1
         self.nalm = P.nalm
@@ -109,17 +122,19 @@ class CutPreconditioner:
         self.m0 = torch.as_tensor(base.m_arr == 0, device=dev)
         self.dtype = dtype
         self._build(chunk)
+        self._use = self._band
 
     def __del__(self):
-        h = getattr(self, "_band", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib.lib().ps_plan_destroy(h)
-            self._band = None
+        for name in ("_band", "_band64", "_own64"):
+            h = getattr(self, name, None)
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().ps_plan_destroy(h)
+                setattr(self, name, None)
 
     # ---------------------------------------------------------------- band Legendre stages
     def _ws(self, B, spin, adj):
         n = ctypes.c_size_t()
-        _lib.call("ps_legendre_workspace_bytes", self._band, B, spin, adj, ctypes.byref(n))
+        _lib.call("ps_legendre_workspace_bytes", self._use, B, spin, adj, ctypes.byref(n))
         return torch.empty(max(int(n.value), 256), dtype=torch.uint8, device=self.base.device), int(n.value)
 
     def synth(self, alm, spin):
@@ -127,7 +142,7 @@ class CutPreconditioner:
         B, nc = alm.shape[0], alm.shape[1]
         out = torch.empty((self.Rb, self.M, B, nc), dtype=torch.complex128, device=alm.device)
         ws, nb = self._ws(B, spin, 0)
-        _lib.call("ps_legendre_synthesis", self._band, _vp(alm.contiguous()), _vp(out), B, spin, _vp(ws), nb,
+        _lib.call("ps_legendre_synthesis", self._use, _vp(alm.contiguous()), _vp(out), B, spin, _vp(ws), nb,
                   _stream())
         return out
 
@@ -136,7 +151,7 @@ class CutPreconditioner:
         B, nc = phase.shape[2], phase.shape[3]
         out = torch.empty((B, nc, self.nalm), dtype=torch.complex128, device=phase.device)
         ws, nb = self._ws(B, spin, 1)
-        _lib.call("ps_legendre_adjoint", self._band, _vp(phase.contiguous()), _vp(out), B, spin, 1.0, _vp(ws), nb,
+        _lib.call("ps_legendre_adjoint", self._use, _vp(phase.contiguous()), _vp(out), B, spin, 1.0, _vp(ws), nb,
                   _stream())
         return out
 

@@ -227,9 +227,12 @@ class BatchedCGD:
         self.use_learned = torch.full((B,), preconditioner == 'learned', dtype=torch.bool, device=b.device)
         z = self._apply_M(self.r, self.use_learned)
         self.rz = self.dot(self.r, z)
-        self.rz0 = self.dot(b0, self._apply_M(b0, self.use_learned))
         if preconditioner in ('learned', 'cut'):
+            # the stopping test uses Sigma whatever M is (no M b0 needed)
             self.judge0 = self.dot(b0, self._sigma(b0))
+            self.rz0 = self.judge0
+        else:
+            self.rz0 = self.dot(b0, self._apply_M(b0, self.use_learned))
         self.p = z
         self.i = 0
         self.iters = torch.zeros(B, dtype=torch.int64, device=b.device)
