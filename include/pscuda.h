@@ -239,6 +239,18 @@ int ps_mlp_dense_backward(float* dY, const float* Y, const float* X, const void*
 int ps_mlp_adam(float* param, const float* grad, float* m, float* v, void* param_bf16, int n, float lr, float beta1,
                 float beta2, float eps, int step, cudaStream_t stream);
 
+/* ---------------------------------------------- CG vector kernels (harmonic)
+ * y[n][a][i] = post[a][i] Sum_b S[a][b][i] pre[b][i] x[n][b][i]: per-(l, m) real 3x3
+ * matrices S [3][3][nalm] float64 (Sigma, weighting.py:76-78; C^-1, :60-68) on
+ * complex128 vectors [batch][3][nalm]; pre / post [3][nalm] float64 or null (the
+ * beam).  ps_lm_dot: out[n] = Sum w[i] Re(x[n][a][i] conj(y[n][a][i])) with w the
+ * m weights [nalm] (the CG inner product, weighting.py:255), fixed-order sums. */
+int ps_lm_matvec3(const double* S, const double* pre, const double* post, const double* x, double* y, int batch,
+                  int64_t nalm, cudaStream_t stream);
+int ps_lm_dot_workspace_bytes(int batch, int64_t nalm, size_t* bytes);
+int ps_lm_dot(const double* x, const double* y, const double* w, int batch, int64_t nalm, double* out,
+              void* workspace, size_t workspace_bytes, cudaStream_t stream);
+
 /* ------------------------------------------------------------- launch statistics
  * No reference counterpart beyond its wall-clock SHT timer (polyspec/base.py:113-127,
  * polyspec/tspec_template.py:453-517): every kernel launch of the library is

@@ -67,6 +67,10 @@ SIGNATURES = {
                                        _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_size_t, _c_void_p]),
     "ps_mlp_adam": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, ctypes.c_float,
                              ctypes.c_float, ctypes.c_float, ctypes.c_float, _c_int, _c_void_p]),
+    "ps_lm_matvec3": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, _c_int64, _c_void_p]),
+    "ps_lm_dot_workspace_bytes": (_c_int, [_c_int, _c_int64, ctypes.POINTER(_c_size_t)]),
+    "ps_lm_dot": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int64, _c_void_p, _c_void_p, _c_size_t,
+                           _c_void_p]),
     "ps_stats_enable_timing": (_c_int, [_c_int]),
     "ps_stats_reset": (_c_int, []),
     "ps_stats_get": (_c_int, [_c_int, ctypes.POINTER(_c_int64), ctypes.POINTER(_c_double),

@@ -35,7 +35,7 @@ import ctypes
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, lmops
 
 
 def _vp(t):
@@ -118,7 +118,7 @@ class CutPreconditioner:
         om = np.concatenate([nphi * wbar[0], nphi * wbar[1], nphi * wbar[2]])
         self.om_half = torch.as_tensor(np.sqrt(om), device=dev)
         self.beam = base.dev('beam_lm')           # [3, nlm]
-        self.sigma = W.d_Sigma                     # [3, 3, nlm] complex
+        self.sigma_r = W.real3('Sigma')            # [3, 3, nlm] float64
         self.m0 = torch.as_tensor(base.m_arr == 0, device=dev)
         self.dtype = dtype
         self._build(chunk)
@@ -165,17 +165,17 @@ class CutPreconditioner:
         return y.permute(1, 0, 2).contiguous()
 
     def _from_band(self, y):
-        """(L B)^H: band vector [M, 3 Rb, B] (times Om^1/2) -> alm [B, 3, nalm]."""
+        """L^H: band vector [M, 3 Rb, B] (times Om^1/2) -> alm [B, 3, nalm] (before the beam)."""
         y = y.permute(1, 0, 2) * self.om_half[:, None, None]  # [3 Rb, M, B]
         Rb = self.Rb
         p0 = y[:Rb].unsqueeze(-1).contiguous()
         p2 = torch.stack([y[Rb:2 * Rb], y[2 * Rb:]], dim=-1).contiguous()
         a0 = self.adjoint(p0, 0)
         a2 = self.adjoint(p2, 2)
-        return torch.cat([a0, a2], dim=1) * self.beam[None]
+        return torch.cat([a0, a2], dim=1)  # the beam factor is applied by the caller
 
-    def _sigma(self, alm):
-        return torch.einsum('abi,nbi->nai', self.sigma, alm)
+    def _sigma(self, alm, pre=None):
+        return lmops.matvec3(self.sigma_r, alm, pre=pre)
 
     # ---------------------------------------------------------------- set-up
     def _build(self, chunk):
@@ -187,7 +187,7 @@ class CutPreconditioner:
             e = torch.zeros((self.M, n, nb), dtype=torch.complex128, device=dev)
             idx = torch.arange(nb, device=dev)
             e[:, j0 + idx, idx] = 1.0
-            col = self._to_band(self._sigma(self._from_band(e)))  # [M, n, nb]
+            col = self._to_band(self._sigma(self._from_band(e), pre=self.beam))  # [M, n, nb]
             G[:, :, j0:j0 + nb] = col
             del e, col
         # K_m = I - Herm(G_m), factorised and inverted in groups of orders (bounded memory)
@@ -215,6 +215,6 @@ class CutPreconditioner:
             return s
         y = self._to_band(s)                                   # [M, n, B]
         w = torch.bmm(self.Kinv, y.to(self.dtype)).to(torch.complex128)
-        c = self._sigma(self._from_band(w))
+        c = self._sigma(self._from_band(w), pre=self.beam)
         c[:, :, self.m0] = c[:, :, self.m0].real.to(torch.complex128)
         return s + c

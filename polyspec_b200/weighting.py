@@ -16,6 +16,8 @@ operators evaluated on the device.
 import numpy as np
 import torch
 
+from . import lmops
+
 
 def _per_lm(base, mat_l):
     """Per-l matrices [a, b, lmax+1] -> complex device tensor [a, b, nlm] (indexed by base.l_arr)."""
@@ -141,13 +143,21 @@ class Weightings:
         if lmax is None:
             lmax = self.base.lmax
         d = maps.to(device=self.base.device, dtype=torch.float64)
-        x0 = torch.einsum('abi,nbi->nai', self.d_x0op, self.base.to_lm_batch(d))
+        lm = self.base.to_lm_batch(d)
+        x0 = lmops.matvec3(self.real3('x0op'), lm) if self.pol else torch.einsum('abi,nbi->nai', self.d_x0op, lm)
         # the learned CG hands a system to the plain CG after half the step budget
         cgd = BatchedCGD(self, d, x0, preconditioner=preconditioner, learned_max_steps=max(1, nstep // 2))
         cgd.run(nstep=nstep, thresh=thresh, verb=verb)
         self.last_cgd = cgd
         lfilt = torch.as_tensor(self.base.l_arr <= lmax, device=self.base.device)
         return cgd.get_ivar_lm()[:, :, lfilt]
+
+    def real3(self, name):
+        """Float64 copy of the per-(l, m) 3x3 'Sigma', 'inv_Cl' or 'x0op' for the vector kernels."""
+        cache = self.__dict__.setdefault('_real3', {})
+        if name not in cache:
+            cache[name] = lmops.real3({'Sigma': self.d_Sigma, 'inv_Cl': self.d_inv_Cl, 'x0op': self.d_x0op}[name])
+        return cache[name]
 
     def cut_preconditioner(self):
         """The masked-band preconditioner of this Weightings (built on first use)."""
@@ -239,7 +249,12 @@ class BatchedCGD:
         self.active = torch.ones(B, dtype=torch.bool, device=b.device)
         self.err = self._judge(self.r, self.rz, self.use_learned, torch.arange(B, device=b.device))
 
+    def _pol(self, x):
+        return x.dim() == 3 and x.shape[1] == 3
+
     def _sigma(self, ilm):
+        if self._pol(ilm):
+            return lmops.matvec3(self.W.real3('Sigma'), ilm)
         return torch.einsum('abi,nbi->nai', self.W.d_Sigma, ilm)
 
     def _judge(self, r, rz, learned_mask, idx):
@@ -249,6 +264,8 @@ class BatchedCGD:
         return self.dot(r, self._sigma(r)) / self.judge0[idx]
 
     def dot(self, a, b):
+        if self._pol(a):
+            return lmops.dot(a, b, self.w)
         return torch.sum((a * b.conj()).real * self.w, dim=(-2, -1))
 
     def _get_b(self, d):
@@ -256,6 +273,8 @@ class BatchedCGD:
         return self.base.to_lm_batch(m * self.W.d_mask) * self.base.dev('beam_lm')
 
     def _apply_Cinv(self, ilm):
+        if self._pol(ilm):
+            return lmops.matvec3(self.W.real3('inv_Cl'), ilm)
         return torch.einsum('abi,nbi->nai', self.W.d_inv_Cl, ilm)
 
     def _apply_A(self, ilm):
@@ -275,7 +294,7 @@ class BatchedCGD:
                 z[plain] = torch.einsum('abi,nbi->nai', Sig, ilm[plain])
             return z
         if self.preconditioner == 'harmonic':
-            return torch.einsum('abi,nbi->nai', Sig, ilm)
+            return self._sigma(ilm)
         elif self.preconditioner == 'pseudo_inverse':
             beam = self.base.dev('beam_lm')
             Nl = torch.as_tensor(self.W.Nl_iso, device=self.base.device)[:, None]
