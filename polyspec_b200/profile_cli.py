@@ -11,6 +11,13 @@ ops: s0/a0 = spin-0 synthesis/adjoint, s2/a2 = spin-2 synthesis/adjoint.
 runs the pixel-product / radial-sum kernels on [nr, Npix] maps (config-3
 sizes by default) and prints each one's device time and achieved HBM GB/s
 (algorithmic bytes / CUDA-event time, best of --reps).
+
+    python -m polyspec_b200.profile_cli serve --n 256 [--reps 3] [--prec mixed]
+
+the mixed-size serving workload: n requests with Nside drawn uniformly from
+{256, 512, 1024, 2048}, lmax = 2 Nside, spin 0 or 2, half alm2map and half
+map2alm (seeded), grouped and replayed as one CUDA graph; prints maps/s
+(requests per second, both directions counted).
 """
 import argparse
 import sys
@@ -76,6 +83,33 @@ def pix(a):
               flush=True)
 
 
+def serve(a):
+    import numpy as np
+    from polyspec_b200.serve import SHTServer
+    rng = np.random.default_rng(0)
+    reqs = []
+    for i in range(a.n):
+        nside = int(rng.choice([256, 512, 1024, 2048]))
+        reqs.append(dict(nside=nside, lmax=2 * nside, spin=int(rng.choice([0, 2])),
+                         direction="alm2map" if i % 2 == 0 else "map2alm"))
+    srv = SHTServer(reqs, prec=a.prec)
+    for x in srv.inputs:
+        x.normal_()
+    best = None
+    for _ in range(a.reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        srv.run()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    groups = ", ".join("%d x (Nside %d, spin %d, %s)" % (len(idx), k[0], k[2], k[3]) for k, idx in srv.groups)
+    print("serve: %d requests in %d groups, graph replay %.1f ms -> %.1f maps/s" % (len(reqs), len(srv.groups), best,
+                                                                                  1e3 * len(reqs) / best))
+    print("groups:", groups)
+
+
 def main(argv=None):
     p = argparse.ArgumentParser()
     sub = p.add_subparsers(dest="cmd", required=True)
@@ -89,8 +123,14 @@ def main(argv=None):
     q.add_argument("--nside", type=int, default=512)
     q.add_argument("--nr", type=int, default=24)
     q.add_argument("--reps", type=int, default=3)
+    v = sub.add_parser("serve")
+    v.add_argument("--n", type=int, default=256)
+    v.add_argument("--reps", type=int, default=3)
+    v.add_argument("--prec", default="mixed")
     a = p.parse_args(argv)
-    if a.cmd == "sht":
+    if a.cmd == "serve":
+        serve(a)
+    elif a.cmd == "sht":
         sht(a)
     elif a.cmd == "pix":
         pix(a)
