@@ -3,9 +3,9 @@ counterpart; the reference's ducc0 picks its own blocking internally).
 
 For each (direction, spin, batch bucket) of a plan the first call times every
 candidate -- the mixed-precision pipeline with each allowed number of maps per
-CTA of its Legendre kernels, and the FP64 pipeline with each of its allowed
-tiles (ps_plan_set_tile) -- with CUDA events, after one untimed run, and keeps
-the fastest.  Results are kept per process and in a JSON cache keyed by GPU
+CTA of its Legendre kernels, and (for batches of up to 8 maps) the FP64
+pipeline with each of its allowed tiles (ps_plan_set_tile) -- with CUDA
+events, after one untimed run, and keeps the fastest.  Results are kept per process and in a JSON cache keyed by GPU
 model, Nside, lmax and the call's shape, so later processes reuse them; the
 cache file is $PS_TUNE_CACHE, default ~/.cache/polyspec_b200/tune.json.
 """
@@ -84,7 +84,9 @@ class Tuner:
         choice = self.choices.get(key) or self.disk.get(key)
         if choice is None or choice.get("pipeline") not in self.handles:
             times = {}
-            for pipeline in self.handles:
+            # the FP64 pipeline only competes for small batches (its workspace is twice the mixed one's)
+            cands = [pl for pl in self.handles if not (pl == "fp64" and len(self.handles) > 1 and B > 8)]
+            for pipeline in cands:
                 for tile in TILES[(pipeline, direction, spin > 0)]:
                     self._set(pipeline, direction, spin, tile)
                     h = self.handles[pipeline]

@@ -365,9 +365,15 @@ int ps_plan_info(const ps_plan* plan, int* nside, int* lmax, int64_t* npix, int6
 }
 
 // maps per Legendre-adjoint pass: the per-ring-tile partial sums of one pass
-// bound the adjoint's workspace independently of the batch size
+// bound the adjoint's workspace independently of the batch size (at most about
+// 4 GiB of partials per pass, at least one map)
 static int adjoint_chunk(const ps::Plan& P, int batch, int spin) {
-  const int c = (P.prec == PS_PREC_MIXED) ? (spin == 0 ? 16 : 8) : (spin == 0 ? 8 : 4);
+  int c = (P.prec == PS_PREC_MIXED) ? (spin == 0 ? 16 : 8) : (spin == 0 ? 8 : 4);
+  const int tiles = (P.prec == PS_PREC_MIXED) ? ps::mx_adjoint_tiles(P) : ps::adjoint_tiles(P);
+  const double per_map = double(tiles) * double(P.nalm) * (spin == 0 ? 1 : 2) *
+                         (P.prec == PS_PREC_MIXED ? sizeof(float2) : sizeof(double2));
+  const int cap = int(4294967296.0 / per_map);
+  if (c > cap) c = cap < 1 ? 1 : cap;
   return batch < c ? batch : c;
 }
 

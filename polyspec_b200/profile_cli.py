@@ -12,9 +12,10 @@ runs the pixel-product / radial-sum kernels on [nr, Npix] maps (config-3
 sizes by default) and prints each one's device time and achieved HBM GB/s
 (algorithmic bytes / CUDA-event time, best of --reps).
 
-    python -m polyspec_b200.profile_cli serve --n 256 [--reps 3] [--prec mixed]
+    python -m polyspec_b200.profile_cli serve --n 64 [--reps 3] [--prec mixed]
 
-the mixed-size serving workload: n requests with Nside drawn uniformly from
+the mixed-size serving workload (n = 64 keeps the FP64 maps and alm of all
+requests, about 15 GB per 16 requests, well inside HBM): n requests with Nside drawn uniformly from
 {256, 512, 1024, 2048}, lmax = 2 Nside, spin 0 or 2, half alm2map and half
 map2alm (seeded), grouped and replayed as one CUDA graph; prints maps/s
 (requests per second, both directions counted).
@@ -124,7 +125,7 @@ def main(argv=None):
     q.add_argument("--nr", type=int, default=24)
     q.add_argument("--reps", type=int, default=3)
     v = sub.add_parser("serve")
-    v.add_argument("--n", type=int, default=256)
+    v.add_argument("--n", type=int, default=64)
     v.add_argument("--reps", type=int, default=3)
     v.add_argument("--prec", default="mixed")
     a = p.parse_args(argv)

@@ -57,7 +57,7 @@ class SHTServer:
             self._gin.append(x)
             for j, i in enumerate(idx):
                 self.inputs[i] = x[j]
-            for h in (P._h, P._h64):
+            for h in (P._h, P._h64 if B <= 8 else None):  # the autotuner tries FP64 for small batches only
                 if h is None:
                     continue
                 n = ctypes.c_size_t()
