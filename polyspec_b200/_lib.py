@@ -11,6 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpscuda.so")
 
 PS_OK = 0
+PS_ERR_UNSUPPORTED = -2
 PS_ERR_NOT_CONVERGED = -6
 PS_PREC_FP64 = 0
 PS_PREC_MIXED = 1

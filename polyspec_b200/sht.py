@@ -58,10 +58,15 @@ class SHTPlan:
             if prec != "fp64":
                 h64 = ctypes.c_void_p()
                 with torch.cuda.device(self.device):
-                    _lib.call("ps_plan_create", self.nside, self.lmax, self.lmax, mask, _lib.PS_PREC_FP64,
-                              ctypes.byref(h64))
-                self._h64 = h64
-                handles["fp64"] = h64
+                    rc = _lib.lib().ps_plan_create(self.nside, self.lmax, self.lmax, mask, _lib.PS_PREC_FP64,
+                                                   ctypes.byref(h64))
+                # an FP64 plan may be unsupported where the mixed one is not (at Nside 2048 the
+                # FP64 Bluestein work arrays exceed shared memory): tune the mixed tiles only then
+                if rc == _lib.PS_OK:
+                    self._h64 = h64
+                    handles["fp64"] = h64
+                elif rc != _lib.PS_ERR_UNSUPPORTED:
+                    _lib.check("ps_plan_create", rc)
             self._tuner = Tuner(self.nside, self.lmax, handles, self.device)
         # counters of transforms issued through this plan
         self.n_synthesis = 0
