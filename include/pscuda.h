@@ -251,6 +251,42 @@ int ps_lm_dot_workspace_bytes(int batch, int64_t nalm, size_t* bytes);
 int ps_lm_dot(const double* x, const double* y, const double* w, int batch, int64_t nalm, double* out,
               void* workspace, size_t workspace_bytes, cudaStream_t stream);
 
+/* ------------------------------------------------------------- binned bispectrum (BSpecBin)
+ * Map sets are planar complex: map m is [2][npix] float64 (real plane, then
+ * imaginary plane) at maps + 2 m npix; npix must be even, pointers 16-byte aligned.
+ *
+ * ps_bispec_triplet_sums: out[o] (complex128) = Sum_pix Sum_{t = term_ptr[o]}^{term_ptr[o+1]-1}
+ *   M[terms[3t]] M[terms[3t+1]] M[terms[3t+2]] -- the per-triplet pixel sums of
+ *   polyspec/bspec_bin.py:339-364 (_analyze3, cubic term), :383-415 (_analyze1, the
+ *   linear term over simulations) and :733-755 (ideal numerator), all triplets in one
+ *   launch.  Fixed-order reductions (deterministic).  term_ptr [nout+1] and terms
+ *   [nterm][3] are int32 device arrays; indices outside [0, nmap) contribute nothing.
+ *   PS_ERR_UNSUPPORTED when a 32-pixel tile of all nmap maps exceeds shared memory
+ *   (nmap > 440).
+ * ps_bispec_pair_products: out[k] (planar [2][npix]) = Sum_{t = ptr[k]}^{ptr[k+1]-1}
+ *   s_t op_t(A[a_t]) B[b_t], prods[t] = {a_t, b_t, flags_t}: flags bit 0 conjugates A,
+ *   bit 1 negates the term -- the products of H maps whose spin-2 and spin-1
+ *   adjoint transforms make up compute_fisher_contribution's Q3 maps
+ *   (bspec_bin.py:496-518; there as to_lm_spin(P, M) with M = conj(P), whose
+ *   real-map inputs are (Re P, Im P)).  nout <= 65535.
+ * ps_bispec_assemble_q: out[r][u][lm] (complex128 [nrow][nfield][nlm]) =
+ *   scale[u][lm] Sum_c coef[c] V_c(lm) over the contributions c of row r
+ *   (row_ptr [nrow+1]; contrib [n][4] int32 = pair, field, l-bin, which) whose field
+ *   is u and with edges[bin] <= l_of_lm[lm] < edges[bin+1]; V = conj(G1) - conj(G2)
+ *   (which 0) or conj(C1) + conj(C2) (which 1), where A2, A1 [npair][2][nlm]
+ *   complex128 hold the (G, C) outputs of the pair's spin-2 and spin-1 adjoints.
+ *   The Q3 rows of bspec_bin.py:520-547 (both parities), times the m weights
+ *   (S^-1 weighting, :554) or the beam (input of the A^-1 branch, :552).  scale may
+ *   be NULL (1); nrow <= 65535. */
+int ps_bispec_triplet_sums_workspace_bytes(int nmap, int64_t npix, int nout, size_t* bytes);
+int ps_bispec_triplet_sums(const double* maps, int nmap, int64_t npix, const int* term_ptr, const int* terms,
+                           int nout, double* out, void* workspace, size_t workspace_bytes, cudaStream_t stream);
+int ps_bispec_pair_products(const double* A, int nA, const double* B, int nB, int64_t npix, const int* ptr,
+                            const int* prods, int nout, double* out, cudaStream_t stream);
+int ps_bispec_assemble_q(const double* A2, const double* A1, int npair, int64_t nlm, const int* l_of_lm,
+                         const int* edges, int nbins, const int* row_ptr, const int* contrib, const double* coef,
+                         int nrow, int nfield, const double* scale, double* out, cudaStream_t stream);
+
 /* ------------------------------------------------------------- launch statistics
  * No reference counterpart beyond its wall-clock SHT timer (polyspec/base.py:113-127,
  * polyspec/tspec_template.py:453-517): every kernel launch of the library is

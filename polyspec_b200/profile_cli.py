@@ -19,6 +19,12 @@ requests, about 15 GB per 16 requests, well inside HBM): n requests with Nside d
 {256, 512, 1024, 2048}, lmax = 2 Nside, spin 0 or 2, half alm2map and half
 map2alm (seeded), grouped and replayed as one CUDA graph; prints maps/s
 (requests per second, both directions counted).
+
+    python -m polyspec_b200.profile_cli bspec [--nside 256 --lmax 511 --nbins 10] [--precs fp64,mixed]
+
+one binned-bispectrum Fisher contribution (T+E, log bins, both parities, ideal
+S^-1 filter) per precision: device time, kernel time per kind, the numerator
+with two simulations, and the mixed-vs-FP64 Fisher difference.
 """
 import argparse
 import sys
@@ -111,6 +117,59 @@ def serve(a):
     print("groups:", groups)
 
 
+def bspec(a):
+    """Binned-bispectrum Fisher contributions (T+E, log bins, ideal filter) per second."""
+    import numpy as np
+    from polyspec_b200 import PolySpec, Weightings, _lib
+    from polyspec_b200 import workloads as W
+    from polyspec_b200.bspec_bin import BSpecBin
+    cltot, cl, beam, mask, l_bins, fields = W.bispec_setup(a.nside, a.lmax, a.nbins)
+    res = {}
+    for prec in a.precs.split(","):
+        base = PolySpec(a.nside, dict(cltot), beam=list(beam), pol=True, lmax=a.lmax, prec=prec)
+        wts = Weightings(base, np.stack([mask] * 3), dict(cl), noise_cov=W.white_noise_cov(a.nside))
+        bsb = BSpecBin(base, mask, wts.make_applySinv('ideal'), l_bins, fields=fields, parity='both')
+        bsb._compute_symmetry_factor()
+        a_lms = [base.generate_data(seed=11 + i, deconvolve_beam=True, output_type='harmonic', rng='device')
+                 for i in range(2)]
+        f = bsb.compute_fisher_contribution(0, a_lms=a_lms)  # warm-up (autotuning, lazy set-up)
+        torch.cuda.synchronize()
+        best = None
+        for _ in range(a.reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            f = bsb.compute_fisher_contribution(0, a_lms=a_lms)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        res[prec] = f
+        _lib.call("ps_stats_reset")
+        _lib.call("ps_stats_enable_timing", 1)
+        bsb.compute_fisher_contribution(0, a_lms=a_lms)
+        torch.cuda.synchronize()
+        _lib.call("ps_stats_enable_timing", 0)
+        st = {k: _lib.stats(k) for k in _lib.KERNEL_KINDS}
+        print("bspec %s kernel ms: %s" % (prec, ", ".join("%s %.1f" % (k, v[1]) for k, v in st.items() if v[0])))
+        data = base.to_map(base.generate_data(seed=3, output_type='harmonic', rng='device'))
+        bsb.generate_sims(2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        bsb.Bl_numerator(data)
+        e1.record()
+        torch.cuda.synchronize()
+        print("bspec %s: Nside %d lmax %d, %d bins, N_b %d, %d Q3 pairs: Fisher contribution %.1f ms -> %.3f sims/s;"
+              " numerator with 2 sims %.1f ms" % (prec, a.nside, a.lmax, len(l_bins) - 1, bsb.N_b,
+                                                  bsb._tables['npair'], best, 1e3 / best, e0.elapsed_time(e1)),
+              flush=True)
+        del bsb, wts, base
+        torch.cuda.empty_cache()
+    if "fp64" in res and "mixed" in res:
+        r = np.abs(res["mixed"] - res["fp64"]).max() / np.abs(res["fp64"]).max()
+        d = np.abs(np.diag(res["mixed"]) / np.diag(res["fp64"]) - 1).max()
+        print("bspec mixed vs fp64 Fisher: max rel (of max) %.2e, diagonal max rel %.2e" % (r, d))
+
+
 def main(argv=None):
     p = argparse.ArgumentParser()
     sub = p.add_subparsers(dest="cmd", required=True)
@@ -128,8 +187,16 @@ def main(argv=None):
     v.add_argument("--n", type=int, default=64)
     v.add_argument("--reps", type=int, default=3)
     v.add_argument("--prec", default="mixed")
+    b = sub.add_parser("bspec")
+    b.add_argument("--nside", type=int, default=256)
+    b.add_argument("--lmax", type=int, default=511)
+    b.add_argument("--nbins", type=int, default=10)
+    b.add_argument("--reps", type=int, default=2)
+    b.add_argument("--precs", default="fp64,mixed")
     a = p.parse_args(argv)
-    if a.cmd == "serve":
+    if a.cmd == "bspec":
+        bspec(a)
+    elif a.cmd == "serve":
         serve(a)
     elif a.cmd == "sht":
         sht(a)

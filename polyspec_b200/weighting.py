@@ -179,10 +179,23 @@ class Weightings:
 
             def batched(self, maps, lmax=None):
                 if kind == 'ideal':
-                    return torch.stack([W.applySinv_ideal(m, lmax=lmax) for m in maps])
+                    return W.batched_applySinv_ideal(maps, lmax=lmax)
                 return W.batched_applySinv_optimal(maps, lmax=lmax, **kw)
 
         return _ApplySinv()
+
+    def batched_applySinv_ideal(self, maps, lmax=None):
+        """applySinv_ideal on a leading batch axis: maps [B, nfield, Npix] (CUDA) ->
+        [B, nfield, nlm(lmax)], one batched adjoint transform per spin."""
+        if lmax is None:
+            lmax = self.base.lmax
+        if hasattr(self, 'inpainting_mask'):
+            maps = torch.stack([self.inpaint_map(m) for m in maps])
+        lfilt = torch.as_tensor(self.base.l_arr <= lmax, device=self.base.device)
+        icov = self.base.dev('inv_Cl_tot_lm_mat')
+        beam = self.base.dev('beam_lm')
+        lm = self.base.to_lm_batch(maps)
+        return beam[:, lfilt] * torch.einsum("abl,nbl->nal", icov[:, :, lfilt], lm[:, :, lfilt])
 
     def applySinv_ideal(self, input_map, input_type='map', lmax=None):
         """Ideal S^-1 = beam C_tot^-1 Y^dagger W (polyspec/weighting.py:186-214)."""

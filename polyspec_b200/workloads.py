@@ -159,3 +159,20 @@ def anisotropic_noise_setup(nside, lmax, amp=3.0, depth=30.0, fwhm_arcmin=5.0, s
     noise = white_noise_cov(nside, depth, True) * (1.0 + amp * z * z)[None, :]
     mask = np.ones((3, 12 * nside * nside))
     return cl, cltot, beam, mask, noise
+
+
+def bispec_setup(nside=256, lmax=511, nbins=10, fwhm_arcmin=30.0, pol=True):
+    """Binned-bispectrum workload: T and E (TTT, TTE, TEE, EEE), nbins log-spaced
+    l-bins in [2, lmax], fiducial spectra, Gaussian beam, the latitude mask
+    (|b| < 15 deg, 5 deg cosine taper) and the ideal S^-1 filter.  Returns
+    (Cl_tot, Cl_raw, beam rows, mask, l_bins, fields)."""
+    cl = fiducial_cl(lmax, pol)
+    b = gaussian_beam(lmax, fwhm_arcmin)
+    nf = 3 if pol else 1
+    beam = np.stack([b] * nf)
+    nl = noise_cl(nside, lmax, 30.0, pol)
+    cltot = total_cl(cl, beam, nl)
+    mask = latitude_mask(nside, 15.0, 5.0)
+    l_bins = np.unique(np.round(np.geomspace(2, lmax, nbins + 1)).astype(int))
+    fields = ['TTT', 'TTE', 'TEE', 'EEE'] if pol else ['TTT']
+    return cltot, cl, beam, mask, l_bins, fields
