@@ -183,7 +183,8 @@ int ps_pix_radial_sum(int kind, const double* r_weights, const double* tau, cons
                       cudaStream_t stream);
 
 /* out[r][lm] = weight Sum_X flX[l][X][r] h_lm[X][lm], l = ls[lm]  (complex128 h_lm
- * [npol][nlm], out [nr][nlm]; npol 1 or 2; tauNL_utils.pyx:80-98).  flX is
+ * [npol][nlm], out [nr][nlm]; npol 1, 2 or 3 -- as in the reference only X = T (npol 1)
+ * or X = T, E (npol 2, 3) enter the sum; tauNL_utils.pyx:80-98).  flX is
  * [lsize][npol][nr]; an lm whose l lies outside [0, lsize) gets zeros. */
 int ps_apply_fl_weights(const double* flX, int lsize, int npol, int nr, const double* h_lm, const int* ls,
                         int64_t nlm, double weight, double* out, cudaStream_t stream);
@@ -286,6 +287,20 @@ int ps_bispec_pair_products(const double* A, int nA, const double* B, int nB, in
 int ps_bispec_assemble_q(const double* A2, const double* A1, int npair, int64_t nlm, const int* l_of_lm,
                          const int* edges, int nbins, const int* row_ptr, const int* contrib, const double* coef,
                          int nrow, int nfield, const double* scale, double* out, cudaStream_t stream);
+
+/* ------------------------------------------------------------- k-space radial integrals (TSpecTemplate set-up)
+ * ps_kint_bessel_table: out[l - lmin][ix] = j_l(x[ix]) for l in [lmin, lmax] (polyspec/cython/
+ *   k_integrals.pyx:28-71: x = 0 -> delta_l0; x > 18000 + lmax -> sin(x - l pi/2)/x; zero above the
+ *   largest l whose small-x limit exceeds 1e-150).  x [nx] float64 device array.
+ * ps_kint_radial: out[l][X][r] += (-1)^l Sum_k (k_i - k_{i-1}) (f_{i-1} + f_i) for l in [lmin, lmax],
+ *   X < npol, r < nr, with f_i = kprod[i] T[X][l][i] j_{l+nshift}(k_i r[r]) and j linearly interpolated
+ *   from table (rows tab_lmin .. tab_lmin + tab_nl - 1, on the grid x, which must start at 0, increase,
+ *   and reach beyond every k r) -- q_integral and p_integral of k_integrals.pyx:262-353 (kprod = k^2/pi
+ *   for q, k^2 P_zeta(k)/pi for p).  T is [npol][nl_T][nk]; out is [*][npol_out][nr]. */
+int ps_kint_bessel_table(const double* x, int64_t nx, int lmin, int lmax, double* out, cudaStream_t stream);
+int ps_kint_radial(const double* table, const double* x, int64_t nx, int tab_lmin, int tab_nl, const double* k_arr,
+                   int nk, const double* kprod, const double* T, int npol, int nl_T, const double* r_arr, int nr,
+                   int lmin, int lmax, int nshift, int npol_out, double* out, cudaStream_t stream);
 
 /* ------------------------------------------------------------- launch statistics
  * No reference counterpart beyond its wall-clock SHT timer (polyspec/base.py:113-127,

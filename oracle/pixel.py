@@ -12,11 +12,15 @@ import numpy as np
 
 # ----------------------------------------------------------- tauNL_utils.pyx
 def apply_fl_weights(ls, flX, h_lm, weight):
-    """tauNL_utils.pyx:80-98: out[r, lm] = w Sum_X flX[l, X, r] h[X, lm]."""
+    """tauNL_utils.pyx:80-98: out[r, lm] = w Sum_X flX[l, X, r] h[X, lm] over X = T only
+    (npol 1) or X = T, E (npol 2 or 3: the reference ignores a third column)."""
     npol = flX.shape[1]
     nlm = h_lm.shape[1]
     f = flX[np.asarray(ls)[:nlm]]  # [nlm, npol, nr]
-    out = np.einsum("lxr,xl->rl", f, h_lm[:npol]) if npol > 1 else f[:, 0, :].T * h_lm[0][None, :]
+    if npol > 1:
+        out = np.einsum("lxr,xl->rl", f[:, :2], h_lm[:2])
+    else:
+        out = f[:, 0, :].T * h_lm[0][None, :]
     return out * weight
 
 

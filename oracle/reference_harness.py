@@ -31,3 +31,32 @@ def load(reference_root, modules=("base", "weighting", "pspec_bin")):
         spec.loader.exec_module(mod)
         out[name] = mod
     return out
+
+
+def load_cython(reference_root=None):
+    """Register the reference's Cython modules under ``refpolyspec.cython``: the
+    compiled tauNL_utils and ideal_fisher of oracle/_ref (built by
+    oracle/build_ref.sh from the reference sources) and the numpy k_integrals shim
+    (GSL, which the compiled module needs, is absent).  Call before loading
+    tspec_template."""
+    import importlib.machinery
+    if "refpolyspec" not in sys.modules:
+        raise RuntimeError("load() the reference package first")
+    cy = types.ModuleType("refpolyspec.cython")
+    cy.__path__ = []
+    sys.modules["refpolyspec.cython"] = cy
+    ref_dir = os.path.join(HERE, "_ref")
+    suffix = importlib.machinery.EXTENSION_SUFFIXES[0]
+    for name in ("tauNL_utils", "ideal_fisher"):
+        path = os.path.join(ref_dir, name + suffix)
+        if not os.path.exists(path):
+            raise RuntimeError("compiled reference module %s missing: run oracle/build_ref.sh" % path)
+        spec = importlib.util.spec_from_file_location("refpolyspec.cython." + name, path)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules["refpolyspec.cython." + name] = mod
+    shims = os.path.join(HERE, "shims")
+    spec = importlib.util.spec_from_file_location("refpolyspec.cython.k_integrals", os.path.join(shims, "k_integrals.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    sys.modules["refpolyspec.cython.k_integrals"] = mod

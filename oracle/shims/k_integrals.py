@@ -1,0 +1,101 @@
+"""ORACLE shim: numpy restatement of the reference's k-space integrals
+(polyspec/cython/k_integrals.pyx), standing in for the compiled module, which
+links GSL (absent here).  Test infrastructure only.
+
+Restated (same grids, branches and trapezium rule, vectorised):
+  * compute_bessel        k_integrals.pyx:28-71   j_l(x) table; GSL's Steed
+                          recurrence (gsl_sf_bessel_jl_steed_array, GSL version
+                          unpinned by the reference) is replaced by scipy's
+                          spherical_jn, with the reference's branches kept: x = 0,
+                          the large-x limit for x > 18000 + lmax, and zeros where
+                          the small-x limit falls below 1e-150;
+  * interpolate_jlkr      :84-110  linear interpolation of the table to k r;
+  * q_integral            :312-353 q_l^X(r) = (-1)^l Sum_k dk (f_k + f_k+1),
+                          f = (2/pi) k^2 / 2 T_l^X(k) j_l(kr);
+  * p_integral            :262-310 the same with P_zeta(k) in f and j_{l+n}.
+The other integrals (a, b, c, r, collider, F) raise NotImplementedError.
+"""
+import numpy as np
+from scipy.special import spherical_jn
+
+
+def _smallx(l, x):
+    """x << l limit of j_l(x) (k_integrals.pyx:73-75)."""
+    return (np.e * x / (2. * l + 1.)) ** (l + 0.5) / np.sqrt(4 * x * (l + 0.5))
+
+
+def compute_bessel(x_arr, lmin, lmax, jlx_arr, nthreads):
+    x_arr = np.asarray(x_arr, dtype=np.float64)
+    nx = len(x_arr)
+    tmp = np.zeros((nx, lmax + 1))
+    ls = np.arange(lmax + 1)
+    small = 1e-150
+    with np.errstate(over='ignore', under='ignore', divide='ignore', invalid='ignore'):
+        for ix in range(nx):
+            x = x_arr[ix]
+            if x == 0.:
+                tmp[ix, 0] = 1.
+            elif x > 18000 + lmax:
+                tmp[ix] = np.sin(x - ls * np.pi / 2.) / x
+            else:
+                if abs(_smallx(lmax, x)) > small:
+                    lt = lmax
+                else:
+                    lt = lmax
+                    for l in range(lmax, 0, -1):
+                        lt = l
+                        if abs(_smallx(l, x)) > small:
+                            break
+                    else:
+                        lt = 1  # the reference's loop variable ends at 1 when nothing breaks
+                tmp[ix, :lt + 1] = spherical_jn(np.arange(lt + 1), x)
+    jlx_arr[:, :] = tmp[:, lmin:lmax + 1].T
+
+
+def interpolate_jlkr(x_arr, k_arr, r_arr, jlx_arr, nthreads):
+    x_arr = np.asarray(x_arr)
+    kr = np.asarray(k_arr)[None, :] * np.asarray(r_arr)[:, None]          # [nr, nk]
+    ix = np.searchsorted(x_arr, kr) - 1
+    dx = x_arr[ix + 1] - x_arr[ix]
+    xp = (x_arr[ix + 1] - kr) / dx
+    xm = (kr - x_arr[ix]) / dx
+    jl = np.asarray(jlx_arr)
+    return jl[:, ix] * xp[None] + jl[:, ix + 1] * xm[None]               # [nl, nr, nk]
+
+
+def _trapz(kprod, T, jl, k_arr):
+    """Sum_k (k_{i} - k_{i-1}) (f_{i-1} + f_i), f = kprod T jl, over the last axis."""
+    f = kprod * T * jl
+    dk = np.diff(k_arr)
+    return np.sum(dk * (f[..., :-1] + f[..., 1:]), axis=-1)
+
+
+def q_integral(k_arr, Tl_arr, jlkr, lmin, lmax, nthreads, integs):
+    k_arr = np.asarray(k_arr)
+    kprod = 2. / np.pi * k_arr * k_arr / 2.
+    for il in range(lmax + 1 - lmin):
+        l = lmin + il
+        for X in range(len(Tl_arr)):
+            integs[l, X, :] += (-1.) ** l * _trapz(kprod, np.asarray(Tl_arr)[X, l][None], jlkr[il], k_arr)
+
+
+def p_integral(k_arr, Pzeta_arr, Tl_arr, jlkr_all, lmin, lmax, arr_lmin, arr_lmax, this_nmax, nthreads, integs):
+    k_arr = np.asarray(k_arr)
+    kprod = 2. / np.pi * k_arr * k_arr * np.asarray(Pzeta_arr) / 2.
+    nmax = len(integs) // 2
+    for n in range(-this_nmax, this_nmax + 1):
+        lshift1 = min(0, lmin - arr_lmin + n)
+        lshift2 = max(0, lmin - arr_lmin + n)
+        for il in range(lmax - lmin + lshift1 + 1):
+            l = lmin - lshift1 + il
+            for X in range(len(Tl_arr)):
+                integs[nmax + n, l, X, :] += (-1.) ** l * _trapz(kprod, np.asarray(Tl_arr)[X, l][None],
+                                                                 jlkr_all[lshift2 + il], k_arr)
+
+
+def _missing(*a, **k):
+    raise NotImplementedError("this k-space integral is outside the oracle's scope")
+
+
+compute_jl_prime = a_integral = b_integral = c_integral = r_integral = _missing
+collider_p_integral = compute_F_integral = compute_collider_F_integral = _missing

@@ -4,10 +4,15 @@
 //   adjoint    P_m   = sum_j map_j e^{-i m (phi0 + 2 pi j / nphi)},  m = 0..mmax
 // with the HEALPix m-aliasing (m folded modulo nphi).
 //
-// Two real fields share one complex FFT (their spectra are Hermitian): the
-// synthesis transforms conj(c_a) + i conj(c_b) and reads map_a, map_b from the
-// real and imaginary parts; the adjoint transforms x_a + i x_b and separates
-// X_a = (Z_k + Z*_{N-k})/2, X_b = (Z_k - Z*_{N-k})/(2i).  A CTA runs G such FFTs
+// The two real components of a spin-s map share one complex FFT (their spectra
+// are Hermitian): the synthesis transforms conj(c_a) + i conj(c_b) and reads
+// map_a, map_b from the real and imaginary parts; the adjoint transforms
+// x_a + i x_b and separates X_a = (Z_k + Z*_{N-k})/2, X_b = (Z_k - Z*_{N-k})/(2i).
+// Spin-0 maps get one FFT each (pack = 0): packing two independent maps would add
+// the rounding of the larger to the smaller (at the larger one's scale), which
+// shows when batch members differ by many orders of magnitude (the Fisher rows of
+// different templates do); the components of one spin map are mixed by the
+// Legendre stage anyway.  A CTA runs G such FFTs
 // at once (G = 256 / T threads per FFT), so small rings keep every thread busy.
 // FFTs are radix-2 with stages fused in pairs (one barrier and one shared-memory
 // round trip per two stages): decimation in frequency for power-of-two rings,
@@ -155,7 +160,8 @@ __device__ __forceinline__ RingDFTf make_dft(const RingInfo& g) {
 __global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list,
                                const float2* __restrict__ phase, double* __restrict__ map, int mmax, int nf,
                                int64_t npix, const float2* __restrict__ tw, int twlog,
-                               const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T) {
+                               const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T,
+                               int pack) {
   extern __shared__ float2 fbuf[];
   const int ir = ring_list[blockIdx.x];
   const RingInfo g = rings[ir];
@@ -163,9 +169,9 @@ __global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __
   const float2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
   const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
   const int G = blockDim.x / T;
-  const int pair = blockIdx.y * G + grp;
-  const int fa = 2 * pair, fb = 2 * pair + 1;
-  const bool va = fa < nf, vb = fb < nf;
+  const int unit = blockIdx.y * G + grp;
+  const int fa = pack ? 2 * unit : unit, fb = fa + 1;
+  const bool va = fa < nf, vb = pack && fb < nf;
   float2* buf = fbuf + size_t(grp) * d.M;
   const int N = d.N;
   const int64_t pden = g.phi_den;
@@ -208,7 +214,8 @@ __global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __
 __global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list,
                                  const double* __restrict__ map, float2* __restrict__ phase, int mmax, int nf,
                                  int64_t npix, const float2* __restrict__ tw, int twlog,
-                                 const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T) {
+                                 const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T,
+                               int pack) {
   extern __shared__ float2 fbuf[];
   const int ir = ring_list[blockIdx.x];
   const RingInfo g = rings[ir];
@@ -216,9 +223,9 @@ __global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* 
   const float2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
   const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
   const int G = blockDim.x / T;
-  const int pair = blockIdx.y * G + grp;
-  const int fa = 2 * pair, fb = 2 * pair + 1;
-  const bool va = fa < nf, vb = fb < nf;
+  const int unit = blockIdx.y * G + grp;
+  const int fa = pack ? 2 * unit : unit, fb = fa + 1;
+  const bool va = fa < nf, vb = pack && fb < nf;
   float2* buf = fbuf + size_t(grp) * d.M;
   const int N = d.N;
   const int64_t pden = g.phi_den;
@@ -244,19 +251,19 @@ __global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* 
   }
 }
 
-static void fft_shape(int work_len, int nf, int& T, int& G, int& gy) {
+static void fft_shape(int work_len, int nf, int pack, int& T, int& G, int& gy) {
   T = std::max(32, std::min(256, work_len / 4));
   G = std::max(1, 256 / T);
-  const int pairs = (nf + 1) / 2;
-  G = std::min(G, pairs);
-  gy = (pairs + G - 1) / G;
+  const int units = pack ? (nf + 1) / 2 : nf;
+  G = std::min(G, units);
+  gy = (units + G - 1) / G;
 }
 
 int launch_ring_synth_f32(const Plan& P, const int* d_list, int nrings, int work_len, const float2* phase,
-                          double* map, int nf, cudaStream_t st) {
+                          double* map, int nf, int pack, cudaStream_t st) {
   if (nrings == 0) return PS_OK;
   int T, G, gy;
-  fft_shape(work_len, nf, T, G, gy);
+  fft_shape(work_len, nf, pack, T, G, gy);
   const size_t smem = size_t(work_len) * G * sizeof(float2);
   if (smem > 48 * 1024) {
     if (cudaFuncSetAttribute(ring_synth_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -266,16 +273,16 @@ int launch_ring_synth_f32(const Plan& P, const int* d_list, int nrings, int work
   while ((1 << twlog) < P.max_fft) ++twlog;
   StatScope sc(PS_K_FFT_SYNTH, 0.0, 0.0, st);
   ring_synth_f32<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, phase, map, P.mmax, nf, P.npix,
-                                                         P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off, T);
+                                                         P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off, T, pack);
   PS_LAUNCH_CHECK();
   return PS_OK;
 }
 
 int launch_ring_adjoint_f32(const Plan& P, const int* d_list, int nrings, int work_len, const double* map,
-                            float2* phase, int nf, cudaStream_t st) {
+                            float2* phase, int nf, int pack, cudaStream_t st) {
   if (nrings == 0) return PS_OK;
   int T, G, gy;
-  fft_shape(work_len, nf, T, G, gy);
+  fft_shape(work_len, nf, pack, T, G, gy);
   const size_t smem = size_t(work_len) * G * sizeof(float2);
   if (smem > 48 * 1024) {
     if (cudaFuncSetAttribute(ring_adjoint_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -286,7 +293,7 @@ int launch_ring_adjoint_f32(const Plan& P, const int* d_list, int nrings, int wo
   while ((1 << twlog) < P.max_fft) ++twlog;
   StatScope sc(PS_K_FFT_ADJOINT, 0.0, 0.0, st);
   ring_adjoint_f32<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, map, phase, P.mmax, nf, P.npix,
-                                                           P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off, T);
+                                                           P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off, T, pack);
   PS_LAUNCH_CHECK();
   return PS_OK;
 }

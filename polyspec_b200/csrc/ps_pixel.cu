@@ -569,7 +569,7 @@ extern "C" int ps_pix_radial_sum(int kind, const double* r_weights, const double
 
 extern "C" int ps_apply_fl_weights(const double* flX, int lsize, int npol, int nr, const double* h_lm,
                                    const int* ls, int64_t nlm, double weight, double* out, cudaStream_t stream) {
-  if (!flX || !h_lm || !ls || !out || lsize <= 0 || nr <= 0 || nlm < 0 || (npol != 1 && npol != 2))
+  if (!flX || !h_lm || !ls || !out || lsize <= 0 || nr <= 0 || nlm < 0 || npol < 1 || npol > 3)
     return PS_ERR_INVALID;
   if (nlm == 0) return PS_OK;
   StatScope sc(PS_K_PIXEL, 0.0, 16.0 * nlm * (npol + nr) + 4.0 * nlm, stream);

@@ -22,13 +22,13 @@ int launch_alm_to_T(const double2* alm, double2* almT, int B, int ncomp, int64_t
 int launch_reduce_partials(const double2* partial, double2* alm, int ntiles, int B, int ncomp, int64_t nalm,
                            double scale, int bofs, int sms, cudaStream_t st);
 int launch_ring_synth_f64(const Plan& P, const int* d_list, int nrings, int work_len, const double2* phase,
-                          double* map, int nf, cudaStream_t st);
+                          double* map, int nf, int pack, cudaStream_t st);
 int launch_ring_adjoint_f64(const Plan& P, const int* d_list, int nrings, int work_len, const double* map,
-                            double2* phase, int nf, cudaStream_t st);
+                            double2* phase, int nf, int pack, cudaStream_t st);
 int launch_ring_synth_f32(const Plan& P, const int* d_list, int nrings, int work_len, const float2* phase,
-                          double* map, int nf, cudaStream_t st);
+                          double* map, int nf, int pack, cudaStream_t st);
 int launch_ring_adjoint_f32(const Plan& P, const int* d_list, int nrings, int work_len, const double* map,
-                            float2* phase, int nf, cudaStream_t st);
+                            float2* phase, int nf, int pack, cudaStream_t st);
 int launch_legendre_synth_tc(const Plan& P, const double2* almT, float2* phase, int B, int spin, int* err_flag,
                              cudaStream_t st);
 int launch_legendre_adjoint_mx(const Plan& P, const float2* phase, float2* partial, int B, int bofs, int Bc,
@@ -526,7 +526,7 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
     if (rc) return rc;
     for (size_t c = 0; c < plan->cls_len.size(); ++c) {
       rc = ps::launch_ring_synth_f32(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c], plan->cls_len[c],
-                                     phase, map, nf, stream);
+                                     phase, map, nf, spin > 0, stream);
       if (rc) return rc;
     }
     return PS_OK;
@@ -536,7 +536,7 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
   if (rc) return rc;
   for (size_t c = 0; c < plan->cls_len.size(); ++c) {
     rc = ps::launch_ring_synth_f64(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c], plan->cls_len[c],
-                                   phase, map, nf, stream);
+                                   phase, map, nf, spin > 0, stream);
     if (rc) return rc;
   }
   return PS_OK;
@@ -562,7 +562,7 @@ int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, i
     float2* partial = reinterpret_cast<float2*>(ws + phase_bytes);
     for (size_t c = 0; c < plan->cls_len.size(); ++c) {
       rc = ps::launch_ring_adjoint_f32(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c],
-                                       plan->cls_len[c], map, phase, nf, stream);
+                                       plan->cls_len[c], map, phase, nf, spin > 0, stream);
       if (rc) return rc;
     }
     const int ch = adjoint_chunk(P, batch, spin);
@@ -580,7 +580,7 @@ int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, i
   double2* partial = reinterpret_cast<double2*>(ws + phase_bytes);
   for (size_t c = 0; c < plan->cls_len.size(); ++c) {
     rc = ps::launch_ring_adjoint_f64(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c], plan->cls_len[c],
-                                     map, phase, nf, stream);
+                                     map, phase, nf, spin > 0, stream);
     if (rc) return rc;
   }
   const int ch = adjoint_chunk(P, batch, spin);

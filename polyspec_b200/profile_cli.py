@@ -170,6 +170,64 @@ def bspec(a):
         print("bspec mixed vs fp64 Fisher: max rel (of max) %.2e, diagonal max rel %.2e" % (r, d))
 
 
+def tspec(a):
+    """Template trispectrum (gNL-loc, lensing, point-source): set-up, numerator and one Fisher contribution."""
+    import time
+    import numpy as np
+    from polyspec_b200 import PolySpec, Weightings, _lib
+    from polyspec_b200 import workloads as W
+    from polyspec_b200.tspec_template import TSpecTemplate
+    w = W.tspec_setup(a.nside, a.lmax, a.nr)
+    res = {}
+    for prec in a.precs.split(","):
+        base = PolySpec(a.nside, dict(w['cltot']), beam=list(w['beam']), pol=True, prec=prec)
+        wts = Weightings(base, np.stack([w['mask']] * 3), dict(w['cl']), noise_cov=W.white_noise_cov(a.nside))
+        t0 = time.time()
+        tst = TSpecTemplate(base, w['mask'], wts.make_applySinv('ideal'), ['gNL-loc', 'lensing', 'point-source'],
+                            w['k_arr'], w['Tl_arr'], w['lmin'], w['lmax'], r_values=w['r_values'],
+                            r_weights=w['r_weights'], C_phi=w['C_phi'], C_lens_weight=w['C_lens_weight'])
+        torch.cuda.synchronize()
+        t_setup = time.time() - t0
+        a_lms = [base.generate_data(seed=21 + i, deconvolve_beam=True, output_type='harmonic', rng='device')
+                 for i in range(2)]
+        f = tst.compute_fisher_contribution(0, a_lms=a_lms)  # warm-up
+        best = None
+        for _ in range(a.reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            f = tst.compute_fisher_contribution(0, a_lms=a_lms)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        res[prec] = f
+        _lib.call("ps_stats_reset")
+        _lib.call("ps_stats_enable_timing", 1)
+        tst.compute_fisher_contribution(0, a_lms=a_lms)
+        torch.cuda.synchronize()
+        _lib.call("ps_stats_enable_timing", 0)
+        st = {k: _lib.stats(k) for k in _lib.KERNEL_KINDS}
+        data = base.to_map(base.generate_data(seed=3, output_type='harmonic', rng='device'))
+        tst.generate_sims(1)
+        tst.Tl_numerator(data)  # warm-up
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        num = tst.Tl_numerator(data)
+        e1.record()
+        torch.cuda.synchronize()
+        print("tspec %s: Nside %d lmax %d, N_r %d: set-up (k integrals) %.1f s; Fisher contribution %.1f ms"
+              " -> %.3f sims/s; numerator (1 sim pair) %.1f ms" % (prec, a.nside, a.lmax, a.nr, t_setup, best,
+                                                                  1e3 / best, e0.elapsed_time(e1)), flush=True)
+        print("tspec %s kernel ms: %s" % (prec, ", ".join("%s %.1f" % (k, v[1]) for k, v in st.items() if v[0])))
+        print("tspec %s numerator %s" % (prec, num))
+        del tst, wts, base
+        torch.cuda.empty_cache()
+    if "fp64" in res and "mixed" in res:
+        F, G = res["fp64"], res["mixed"]
+        d = np.sqrt(np.abs(np.outer(np.diag(F), np.diag(F))))
+        print("tspec mixed vs fp64 Fisher: max |dF| / sqrt(F_ii F_jj) %.2e" % (np.abs(G - F) / d).max())
+
+
 def main(argv=None):
     p = argparse.ArgumentParser()
     sub = p.add_subparsers(dest="cmd", required=True)
@@ -193,8 +251,16 @@ def main(argv=None):
     b.add_argument("--nbins", type=int, default=10)
     b.add_argument("--reps", type=int, default=2)
     b.add_argument("--precs", default="fp64,mixed")
+    t = sub.add_parser("tspec")
+    t.add_argument("--nside", type=int, default=512)
+    t.add_argument("--lmax", type=int, default=1000)
+    t.add_argument("--nr", type=int, default=24)
+    t.add_argument("--reps", type=int, default=2)
+    t.add_argument("--precs", default="fp64,mixed")
     a = p.parse_args(argv)
-    if a.cmd == "bspec":
+    if a.cmd == "tspec":
+        tspec(a)
+    elif a.cmd == "bspec":
         bspec(a)
     elif a.cmd == "serve":
         serve(a)

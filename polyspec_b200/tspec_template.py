@@ -1,0 +1,859 @@
+"""Template trispectrum estimator on the GPU (mirror of polyspec/tspec_template.py)
+for the gNL-loc, lensing and point-source templates.
+
+``TSpecTemplate(base, mask, applySinv, templates, k_arr, Tl_arr, lmin, lmax, ...)``
+keeps the reference constructor, its checks and attributes (l- and L-ranges and
+filters, ``to_compute``, ``p_inds``, ``qlXs``, ``plLXs``, ``timers``), the
+simulation handling (``generate_sims``, ``load_sims``) and the estimator methods
+(``Tl_numerator``, ``compute_fisher_contribution``, ``compute_fisher``,
+``Tl_unwindowed``, ``report_timings``, ``reset_timings``).  Other templates of the
+reference (gNL-con and the EFTI, tauNL and collider shapes) raise
+NotImplementedError, as does the radial-sampling optimiser.
+
+``applySinv`` receives and returns CUDA tensors (as for PSpecBin/BSpecBin here);
+one with a ``.batched`` method filters the 4 x n_templates Q rows of the Fisher
+contribution in one batch.  Returned numerators and Fisher matrices are numpy.
+
+Device mapping:
+* k-space integrals (polyspec/tspec_template.py:520-708): the j_l(x) table on the
+  reference's x grid and the q_l^X(r), p_l^X(r) trapezium sums run as the
+  ``ps_kint_*`` kernels (same grid, interpolation and summation order).
+* Filtered maps: ``ps_apply_fl_weights`` then one batched spin-0 synthesis over
+  the radial samples (P and Q maps); the lensing U and V maps are spin 0/1/2/3
+  syntheses; Phi_LM is the lens_phi_sum kernel plus one spin-1 adjoint.
+* Numerators: the radial pixel sums ``gnl_loc(_disc)_sum``; lensing and point
+  source sums are device reductions.
+* Fisher: the ``multiply(_asym)`` products, a batched adjoint over radial samples
+  and ``ps_radial_sum_lm`` for the gNL-loc Q derivatives; spin-1/2/3 adjoints for
+  lensing; the batched S^-1 weighting; ``ps_outer_product``.
+"""
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import _lib, pixel
+
+SUPPORTED = ['gNL-loc', 'lensing', 'point-source']
+
+
+def _vp(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class TSpecTemplate:
+    def __init__(self, base, mask, applySinv, templates, k_arr, Tl_arr, lmin, lmax,
+                 Lmin=None, Lmax=None, Lmin_lens=None, Lmax_lens=None, ns=0.96, As=2.1e-9, k_pivot=0.05,
+                 r_values=[], r_weights={}, rtau_values=[], rtau_weights={},
+                 C_phi=[], C_lens_weight={}, K_coll=0.1, k_coll=0.1, r_star=None, r_hor=None):
+        self.base = base
+        self.mask = mask
+        self.applySinv = applySinv
+        self.pol = self.base.pol
+        self.templates = templates
+        self.k_arr = k_arr
+        self.lmin = lmin
+        self.lmax = lmax
+        self.ns = ns
+        self.As = As
+        self.k_pivot = k_pivot
+        self.K_coll = K_coll
+        self.k_coll = k_coll
+
+        print("Primordial Spectrum: n_s = %.3f, A_s = %.3e, k_pivot = %.3f" % (self.ns, self.As, self.k_pivot))
+        self.Pzeta = lambda k: 2. * np.pi ** 2. / k ** 3 * self.As * (k / self.k_pivot) ** (self.ns - 1)
+
+        assert self.lmax <= base.lmax, "Maximum l can't be larger than HEALPix resolution!"
+        assert self.lmin >= 2, "Minimum l can't be less than 2"
+        if self.lmax > (base.lmax + 1) * 2 / 3:
+            print("## Caution: Maximum l is greater than (2/3)*HEALPix-lmax; this might cause boundary effects.")
+        self.Lmin = 1 if Lmin is None else Lmin
+        self.Lmax = min([base.lmax, 2 * self.lmax]) if Lmax is None else Lmax
+        assert self.Lmin >= 1, "Minimum L can't be less than 1"
+        assert self.Lmax <= 2 * self.lmax, "Lmax <= 2*lmax by the triangle conditions"
+        assert self.Lmax <= base.lmax, "Maximum L can't be larger than HEALPix resolution"
+
+        # lensing L ranges (polyspec/tspec_template.py:95-116)
+        if 'lensing' in self.templates:
+            gnl = np.any(['gNL' in t for t in self.templates])
+            tau = np.any(['tauNL' in t for t in self.templates])
+            if Lmin_lens is None:
+                self.Lmin_lens = 1 if (gnl or not tau) else self.Lmin
+            else:
+                self.Lmin_lens = Lmin_lens
+            if Lmax_lens is None:
+                self.Lmax_lens = min([base.lmax, 2 * self.lmax]) if (gnl or not tau) else self.Lmax
+            else:
+                self.Lmax_lens = Lmax_lens
+            assert self.Lmin_lens >= 1, "Minimum L_lens can't be less than 1"
+            assert self.Lmax_lens <= 2 * self.lmax, "Lmax_lens <= 2*lmax by the triangle conditions"
+            assert self.Lmax_lens <= base.lmax, "Maximum L can't be larger than HEALPix resolution"
+
+        self.lfilt = (self.base.l_arr >= self.lmin) & (self.base.l_arr <= self.lmax)
+        self.Lfilt = (self.base.l_arr >= self.Lmin) & (self.base.l_arr <= self.Lmax)
+        self.ls, self.ms = self.base.l_arr[self.lfilt], self.base.m_arr[self.lfilt]
+        if 'lensing' in self.templates:
+            self.Lfilt_lens = (self.base.l_arr >= self.Lmin_lens) & (self.base.l_arr <= self.Lmax_lens)
+        self.m_weight = np.asarray(self.base.m_weight[self.lfilt], order='C')
+        self.Cinv = np.asarray(self.base.inv_Cl_tot_lm_mat[:, :, self.lfilt], order='C')
+        self.beam_lm = np.asarray(self.base.beam_lm)[:, self.lfilt]
+
+        print("l-range: %s" % [self.lmin, self.lmax])
+        if 'lensing' in self.templates:
+            print("Lensing L-range: %s" % [self.Lmin_lens, self.Lmax_lens])
+        print("Polarizations: ['T', 'E']" if self.pol else "Polarizations: ['T']")
+
+        self._configure_templates(templates, C_phi, C_lens_weight)
+
+        if not type(mask) == float or type(mask) == int:
+            if len(mask) == 1 or len(mask) == 3:
+                assert len(mask[0]) == self.base.Npix, f'Mask has incorrect shape: {np.shape(mask)}'
+            else:
+                assert len(mask) == self.base.Npix, f'Mask has incorrect shape: {np.shape(mask)}'
+        if np.std(self.mask) < 1e-12 and np.abs(np.mean(self.mask) - 1) < 1e-12:
+            print("Mask: ones")
+            self.ones_mask = True
+        else:
+            print("Mask: spatially varying")
+            self.ones_mask = False
+
+        self.r_star = 13882.607764400758 if r_star is None else r_star
+        self.r_hor = 14163.032903769747 if r_hor is None else r_hor
+
+        if self.ints_1d:
+            self.Tl_arr = np.asarray(Tl_arr, dtype=np.float64, order='C')
+            if not self.pol:
+                assert len(self.Tl_arr) == 1, "Transfer function should contain only T components"
+            else:
+                assert len(self.Tl_arr) == 2, "Transfer function should contain both T and E components"
+            assert len(self.Tl_arr[0]) >= self.lmax + 1, "Transfer function must contain all ell modes of interest"
+            assert self.Tl_arr[0][:2].sum() == 0., "Transfer function should return zero for ell = 0, 1"
+            assert len(self.Tl_arr[0][0]) == len(k_arr), "Transfer function must be computed on the input k-grid"
+            if self.pol:
+                assert self.Tl_arr[1][:2].sum() == 0., "Transfer function should return zero for ell = 0, 1"
+
+        self.timers = {x: 0. for x in ['precomputation', 'numerator', 'fisher', 'optimization', 'analytic_fisher',
+                                       'fish_grfs', 'fish_outer', 'fish_weighting', 'fish_convolve', 'fish_deriv',
+                                       'fish_products', 'Sinv', 'Ainv', 'map_transforms', 'gNL_summation',
+                                       'tauNL_products', 'tauNL_summation', 'lensing_products',
+                                       'lensing_summation']}
+        self.base.time_sht = 0.
+
+        if len(r_values) == 0 and self.ints_1d:
+            print("# No input radial sampling points supplied; these can be computed with the "
+                  "optimize_radial_sampling_1d() function\n")
+            self.N_r = 0
+        elif self.ints_1d:
+            print("Reading in precomputed radial integration points")
+            assert len(r_values) > 0, "Must supply radial sampling points!"
+            for t in templates:
+                if t == 'gNL-loc':
+                    assert t in r_weights.keys(), "Must supply weight for template %s" % t
+            self.r_arr = np.asarray(r_values, dtype=np.float64)
+            self.N_r = len(self.r_arr)
+            self.r_weights = r_weights
+        else:
+            self.N_r = 0
+        self.N_rtau = 0
+
+        dev = base.device
+        self._dev = dev
+        self.d_lfilt = torch.as_tensor(np.nonzero(self.lfilt)[0], device=dev)
+        self.d_lminfilt = torch.as_tensor(np.nonzero(self.lminfilt)[0], device=dev)
+        self.d_beam_lm = torch.as_tensor(np.ascontiguousarray(self.beam_lm), device=dev)
+        self.d_m_weight = torch.as_tensor(self.m_weight, device=dev)
+        self.d_mask = torch.as_tensor(np.asarray(mask, dtype=np.float64), device=dev)
+        if self.d_mask.dim() == 1:
+            self.d_mask = self.d_mask[None]
+        if 'lensing' in self.templates:
+            self.d_Lminfilt_lens = torch.as_tensor(np.nonzero(self.Lminfilt_lens)[0], device=dev)
+        if self.N_r > 0:
+            t0 = time.time()
+            self._prepare_templates()
+            self.timers['precomputation'] += time.time() - t0
+
+    # ------------------------------------------------------------------ configuration
+    def _configure_templates(self, templates, C_phi, C_lens_weight):
+        """Template bookkeeping (polyspec/tspec_template.py:243-451) for the supported templates."""
+        self.all_templates_1d = ['gNL-loc', 'gNL-con', 'tauNL-loc', 'tauNL-direc', 'tauNL-even', 'tauNL-odd']
+        self.all_templates_2d = ['gNL-dotdot', 'gNL-dotdel', 'gNL-deldel']
+        self.all_templates_coll = ['tauNL-light', 'tauNL-heavy']
+        self.all_templates = self.all_templates_1d + self.all_templates_2d + self.all_templates_coll + \
+            ['lensing', 'point-source']
+        for t in templates:
+            known = t in self.all_templates or any(s in t for s in ('tauNL-direc', 'tauNL-even', 'tauNL-odd',
+                                                                     'tauNL-light', 'tauNL-heavy'))
+            assert known, "Unknown template %s supplied!" % t
+            if t not in SUPPORTED:
+                raise NotImplementedError("template %s is not implemented by the CUDA backend (supported: %s)"
+                                          % (t, SUPPORTED))
+        print("Templates: %s" % templates)
+        self.ints_1d, self.ints_2d, self.ints_coll = False, False, False
+        self.to_compute, self.n1n3n, self.coll_params = [], [], {}
+        if 'gNL-loc' in templates:
+            self.to_compute.append(['q'])
+            self.ints_1d = True
+        for t in templates:
+            if 'lensing' in t:
+                assert len(C_phi) > 0, "Must supply lensing power spectrum!"
+                assert len(C_phi) >= self.Lmax_lens + 1, "Must specify C^phi-phi(L) up to at least Lmax."
+                if not self.pol:
+                    assert 'TT' in C_lens_weight.keys(), "Must specify unlensed TT power spectrum!"
+                else:
+                    assert 'TE' in C_lens_weight.keys(), "Must specify unlensed TE power spectrum!"
+                    assert 'EE' in C_lens_weight.keys(), "Must specify unlensed EE power spectrum!"
+                    assert 'BB' in C_lens_weight.keys(), "Must specify unlensed BB power spectrum!"
+                    for k in C_lens_weight.keys():
+                        assert len(C_lens_weight[k]) >= self.lmax + 1, \
+                            "Must specify C_lens_weight(l) up to at least lmax."
+                self.C_phi = C_phi
+                self.C_lens_weight = {k: C_lens_weight[k][:self.lmax + 1] for k in C_lens_weight.keys()}
+                self.to_compute.append(['u', 'v'])
+            if 'point-source' in t:
+                self.to_compute.append(['u'])
+        self.n1n3n = np.zeros((0, 3), dtype=int)
+        self.to_compute = np.unique(np.concatenate(self.to_compute)) if self.to_compute else np.array([])
+        self.nmax = 0
+        self.nmax_coll = 0
+        self.nmax_coll_F = 0
+        self.p_inds = [0] if 'gNL-loc' in self.templates else []
+        self.nmax_F = 0
+        self.nLmax = self.Lmax
+        self.nLmin = self.Lmin
+        self.nLfilt = (self.base.l_arr >= self.nLmin) & (self.base.l_arr <= self.nLmax)
+        self.Ls, self.Ms = self.base.l_arr[self.nLfilt], self.base.m_arr[self.nLfilt]
+        self.nLminfilt = self.base.l_arr[self.base.l_arr <= self.nLmax] >= self.nLmin
+        self.Lminfilt = self.base.l_arr[self.base.l_arr <= self.Lmax] >= self.Lmin
+        if 'lensing' in self.templates:
+            self.Lminfilt_lens = self.base.l_arr[self.base.l_arr <= self.Lmax_lens] >= self.Lmin_lens
+        self.lminfilt = self.base.l_arr[self.base.l_arr <= self.lmax] >= self.lmin
+
+    def _prepare_templates(self, ints_1d=True, ints_2d=False, ints_coll=False):
+        """k-space integrals q_l^X(r) and p_l^X(r) on the GPU (polyspec/tspec_template.py:520-708)."""
+        dev = self._dev
+        print("N_k: %d" % len(self.k_arr))
+        print("N_r: %d" % self.N_r)
+        lmax = max([self.lmax + 1, self.lmax + self.nmax])
+        lmin = max([min([self.lmin - 1, self.lmin - self.nmax]), 0])
+        print("\nPrecomputing Bessel functions")
+        k_arr = np.asarray(self.k_arr, dtype=np.float64)
+        max_kr = max(k_arr) * max([0., max(self.r_arr)])
+        x_arr = list(np.arange(0, lmax * 2, 0.01)) + list(np.arange(lmax * 2, min(max_kr * 1.01, lmax * 100), 0.1))
+        if max_kr > 100 * lmax:
+            x_arr += list(np.linspace(lmax * 100, max_kr * 1.01, 1000))
+        x_arr = np.asarray(x_arr, dtype=np.float64)
+        assert np.max(x_arr) >= np.max(k_arr) * np.max(self.r_arr)
+        d_x = torch.as_tensor(x_arr, device=dev)
+        nl_tab = lmax - lmin + 1
+        table = torch.empty((nl_tab, len(x_arr)), dtype=torch.float64, device=dev)
+        _lib.call("ps_kint_bessel_table", _vp(d_x), len(x_arr), lmin, lmax, _vp(table), _stream())
+        if not bool(torch.isfinite(table).all()):
+            raise Exception("Spherical Bessel calculation failed!")
+        print("Interpolating Bessel functions")
+        npol = len(self.Tl_arr)
+        npol_out = 1 + 2 * self.pol
+        d_k = torch.as_tensor(k_arr, device=dev)
+        d_T = torch.as_tensor(np.ascontiguousarray(self.Tl_arr), device=dev)
+        d_r = torch.as_tensor(self.r_arr, device=dev)
+        nl_T = self.Tl_arr.shape[1]
+        if len(self.p_inds) > 0:
+            print("Computing p_lL^X(r) integrals")
+            kprod = torch.as_tensor(2. / np.pi * k_arr * k_arr * self.Pzeta(k_arr) / 2., device=dev)
+            plLXs = torch.zeros((2 * self.nmax + 1, lmax + 1, npol_out, self.N_r), dtype=torch.float64, device=dev)
+            for n in range(-max(self.p_inds), max(self.p_inds) + 1):
+                lshift1 = min(0, self.lmin - lmin + n)
+                _lib.call("ps_kint_radial", _vp(table), _vp(d_x), len(x_arr), lmin, nl_tab, _vp(d_k), len(k_arr),
+                          _vp(kprod), _vp(d_T), npol, nl_T, _vp(d_r), self.N_r, self.lmin - lshift1, self.lmax, n,
+                          npol_out, _vp(plLXs[self.nmax + n]), _stream())
+            self.d_plLXs = plLXs
+            self.plLXs = plLXs.cpu().numpy()
+        if 'q' in self.to_compute:
+            print("Computing q_l^X(r) integrals")
+            kprod = torch.as_tensor(2. / np.pi * k_arr * k_arr / 2., device=dev)
+            qlXs = torch.zeros((self.lmax + 1, npol_out, self.N_r), dtype=torch.float64, device=dev)
+            _lib.call("ps_kint_radial", _vp(table), _vp(d_x), len(x_arr), lmin, nl_tab, _vp(d_k), len(k_arr),
+                      _vp(kprod), _vp(d_T), npol, nl_T, _vp(d_r), self.N_r, self.lmin, self.lmax, 0, npol_out,
+                      _vp(qlXs), _stream())
+            self.d_qlXs = qlXs
+            self.qlXs = qlXs.cpu().numpy()
+        del table
+        self._make_utils()
+        print("Precomputation complete")
+
+    def set_radial_integrals(self, qlXs=None, plLXs=None):
+        """Install precomputed q_l^X(r) [lmax+1, 1+2 pol, N_r] and p_lL^X(r)
+        [1, lmax+2, 1+2 pol, N_r] arrays in place of the computed ones."""
+        if qlXs is not None:
+            self.qlXs = np.asarray(qlXs, dtype=np.float64)
+            self.d_qlXs = torch.as_tensor(self.qlXs, device=self._dev)
+        if plLXs is not None:
+            self.plLXs = np.asarray(plLXs, dtype=np.float64)
+            self.d_plLXs = torch.as_tensor(self.plLXs, device=self._dev)
+
+    def _make_utils(self):
+        self.utils = pixel.tauNL_utils(self.base.nthreads, self.N_r, self.base.l_arr.astype(np.int32),
+                                       self.base.m_arr.astype(np.int32), self.Lmin, self.Lmax,
+                                       self.ls.astype(np.int32), self.ms.astype(np.int32),
+                                       self.Ls.astype(np.int32), self.Ms.astype(np.int32), self.nmax_F)
+
+    # ------------------------------------------------------------------ timings
+    def report_timings(self):
+        """Timers (polyspec/tspec_template.py:453-497)."""
+        print("\n## Timings ##\n")
+        print("Precomputation: %.2fs" % self.timers['precomputation'])
+        for k, name in (('numerator', 'Numerator'), ('fisher', 'Fisher'), ('optimization', 'Optimization')):
+            if self.timers[k] != 0:
+                print("%s: %.2fs" % (name, self.timers[k]))
+        print("\n# Timing Breakdown")
+        if self.timers['Sinv'] != 0:
+            print("S^-1 filtering: %.2fs" % self.timers['Sinv'])
+        if self.timers['map_transforms'] != 0:
+            print("1-field transforms: %.2fs" % self.timers['map_transforms'])
+        if self.timers['numerator'] != 0:
+            if np.any([('gNL' in t) for t in self.templates]):
+                print("gNL -- 4-field summation: %.2fs" % self.timers['gNL_summation'])
+            if 'lensing' in self.templates:
+                print("Lensing -- 2-field transforms: %.2fs" % self.timers['lensing_products'])
+                print("Lensing -- 4-field summation: %.2fs" % self.timers['lensing_summation'])
+        if self.timers['fisher'] != 0:
+            if self.timers['fish_grfs'] != 0:
+                print("Fisher -- creating GRFs: %.2fs" % self.timers['fish_grfs'])
+            if self.timers['Ainv'] != 0:
+                print("Fisher -- A^-1 filtering: %.2fs" % self.timers['Ainv'])
+            print("Fisher -- 3-field derivatives: %.2fs" % self.timers['fish_deriv'])
+            print("Outer product: %.2fs" % self.timers['fish_outer'])
+        print("\n## Harmonic Transforms ##")
+        print("Forward: %d" % self.base.n_SHTs_forward)
+        print("Reverse: %d" % self.base.n_SHTs_reverse)
+        print("Time: %.2fs" % self.base.time_sht)
+        print("\n")
+
+    def reset_timings(self):
+        for f in self.timers.keys():
+            self.timers[f] = 0.
+        self.base.n_SHTs_forward = 0
+        self.base.n_SHTs_reverse = 0
+        self.base.time_sht = 0.
+
+    def _timed(self, key, t0):
+        torch.cuda.current_stream().synchronize()
+        self.timers[key] += time.time() - t0
+
+    # ------------------------------------------------------------------ filtered maps
+    def _full_lm(self, h_filt, lmax):
+        """Embed [..., nlm(l in [lmin, lmax])] into the full [..., nlm(lmax)] layout (zeros below lmin)."""
+        n = (lmax + 1) * (lmax + 2) // 2
+        out = torch.zeros(h_filt.shape[:-1] + (n,), dtype=torch.complex128, device=h_filt.device)
+        out[..., self.d_lminfilt] = h_filt
+        return out
+
+    def _compute_weighted_maps(self, h_lm_filt, flX_arr):
+        """[Sum_lm Y_lm(i) f_l^X(i) h_lm] maps for each radial sample (polyspec/tspec_template.py:799-815)."""
+        t0 = time.time()
+        summ = self._full_lm(self.utils.apply_fl_weights(flX_arr, h_lm_filt, 1.), self.lmax)
+        out = self.base.to_map_vec(summ, output_spin=0, lmax=self.lmax)
+        self._timed('map_transforms', t0)
+        return out
+
+    def _compute_weighted_gaunt_maps(self, h_lm_filt, flLX_arr_re, n, mu):
+        """n = mu = 0 case of polyspec/tspec_template.py:817-876 (the gNL-loc P maps)."""
+        assert n == 0 and mu == 0, "only n = 0 (gNL-loc) is implemented"
+        t0 = time.time()
+        nmax = len(flLX_arr_re) // 2
+        summ = self._full_lm(self.utils.apply_fl_weights(flLX_arr_re[nmax], h_lm_filt, 1. / np.sqrt(4. * np.pi)),
+                             self.lmax)
+        out = self.base.to_map_vec(summ, lmax=self.lmax)
+        self._timed('map_transforms', t0)
+        return out
+
+    def _compute_lensing_U_map(self, h_lm_filt):
+        """[U^T, U^E, U^B] (polyspec/tspec_template.py:878-910)."""
+        t0 = time.time()
+        b = self.base
+        U = torch.zeros((1 + 2 * self.pol, b.Npix), dtype=torch.complex128, device=self._dev)
+        inp = self._full_lm(h_lm_filt[0], self.lmax)
+        U[0] = b.to_map(inp[None], lmax=self.lmax)[0]
+        if 'lensing' in self.templates and self.pol:
+            for X in (1, 2):
+                inp = self._full_lm(h_lm_filt[X], self.lmax)
+                U[X] = b.to_map_spin(inp, inp, spin=2, lmax=self.lmax)[0]
+        self._timed('map_transforms', t0)
+        return U
+
+    def _compute_lensing_V_map(self, h_lm_filt):
+        """[V^T, V^{E,B}(+), V^{E,B}(-)] (polyspec/tspec_template.py:912-965)."""
+        t0 = time.time()
+        b = self.base
+        ls = torch.as_tensor(self.ls.astype(np.float64), device=self._dev)
+        lsi = torch.as_tensor(self.ls, device=self._dev)
+        C = {k: torch.as_tensor(np.asarray(v, dtype=np.float64), device=self._dev)[lsi]
+             for k, v in self.C_lens_weight.items()}
+        V = torch.zeros((1 + 2 * self.pol, b.Npix), dtype=torch.complex128, device=self._dev)
+        if not self.pol:
+            inp = self._full_lm(torch.sqrt(ls * (ls + 1.)) * C['TT'] * h_lm_filt[0], self.lmax)
+            V[0] = b.to_map_spin(-inp, inp, spin=1, lmax=self.lmax)[1]
+        else:
+            wienerT = C['TT'] * h_lm_filt[0] + C['TE'] * h_lm_filt[1]
+            inp = self._full_lm(torch.sqrt(ls * (ls + 1.)) * wienerT, self.lmax)
+            V[0] = b.to_map_spin(-inp, inp, spin=1, lmax=self.lmax)[1]
+            pref_p = torch.sqrt((ls + 2.) * (ls - 1.))
+            pref_m = torch.sqrt((ls - 2.) * (ls + 3.))
+            wienerE = C['TE'] * h_lm_filt[0] + C['EE'] * h_lm_filt[1]
+            wienerB = C['BB'] * h_lm_filt[2]
+            re = self._full_lm(pref_p * wienerE, self.lmax)
+            im = self._full_lm(1.0j * pref_p * wienerB, self.lmax)
+            V[1] = b.to_map_spin(re + im, -re + im, spin=1, lmax=self.lmax)[0]
+            re = self._full_lm(pref_m * wienerE, self.lmax)
+            im = self._full_lm(1.0j * pref_m * wienerB, self.lmax)
+            V[2] = b.to_map_spin(re + im, -re + im, spin=3, lmax=self.lmax)[0]
+        self._timed('map_transforms', t0)
+        return V
+
+    def _apply_all_filters(self, input_map):
+        """Filtered maps of one S^-1-weighted field (polyspec/tspec_template.py:1036-1096)."""
+        output = {}
+        if 0 in self.p_inds:
+            output['p00'] = self._compute_weighted_gaunt_maps(input_map, self.d_plLXs, 0, 0)
+        if 'q' in self.to_compute:
+            output['q'] = self._compute_weighted_maps(input_map, self.d_qlXs)
+        if 'u' in self.to_compute:
+            output['u'] = self._compute_lensing_U_map(input_map)
+        if 'v' in self.to_compute:
+            output['v'] = self._compute_lensing_V_map(input_map)
+        return output
+
+    def _filter_pair(self, input_maps, filtering='Q'):
+        """Filtered fields of a pair of inputs (polyspec/tspec_template.py:967-1034)."""
+        if filtering == 'P':
+            return {0: torch.stack([self._compute_weighted_gaunt_maps(m, self.d_plLXs, 0, 0)[None]
+                                    for m in input_maps])}
+        if filtering == 'Q':
+            return torch.stack([self._compute_weighted_maps(m, self.d_qlXs) for m in input_maps])
+        if filtering == 'U':
+            return torch.stack([self._compute_lensing_U_map(m) for m in input_maps])
+        if filtering == 'V':
+            return torch.stack([self._compute_lensing_V_map(m) for m in input_maps])
+        raise Exception("Filtering %s is not implemented!" % filtering)
+
+    def _compute_lensing_Phi(self, maps1, maps2, add_sym=False):
+        """Phi_LM of the lensing estimators (polyspec/tspec_template.py:1098-1108)."""
+        t0 = time.time()
+        if add_sym:
+            inp = pixel.lens_phi_sum_sym(maps1['u'], maps2['u'], maps1['v'], maps2['v'])
+        else:
+            inp = pixel.lens_phi_sum(maps1['u'], maps2['v'])
+        pm = self.base.to_lm_spin(inp, inp.conj(), spin=1, lmax=self.Lmax_lens)
+        out = (-0.25 * (pm[0] - pm[1]))[self.d_Lminfilt_lens]
+        self._timed('lensing_products', t0)
+        return out
+
+    def _lens_Ls(self):
+        filt = (self.base.l_arr >= self.Lmin_lens) * (self.base.l_arr <= self.Lmax_lens)
+        Ls = self.base.l_arr[filt]
+        Ms = self.base.m_arr[filt]
+        w = Ls * (Ls + 1.) * (1. + (Ms > 0)) * np.asarray(self.C_phi)[Ls]
+        return torch.as_tensor(w, device=self._dev)
+
+    # ------------------------------------------------------------------ simulations
+    def _sinv_filt(self, x, input_type='map'):
+        y = self.applySinv(x, input_type=input_type, lmax=self.lmax)
+        return y[:, self.d_lminfilt].contiguous()
+
+    def _process_sim(self, sim_pair, input_type='map'):
+        """Filtered maps of one simulation pair (polyspec/tspec_template.py:1110-1126)."""
+        t0 = time.time()
+        dt = torch.float64 if input_type == 'map' else torch.complex128
+        ha = self._sinv_filt(self.base._in(sim_pair[0], dt)[0], input_type)
+        hb = self._sinv_filt(self.base._in(sim_pair[1], dt)[0], input_type)
+        self._timed('Sinv', t0)
+        return self._apply_all_filters(ha), self._apply_all_filters(hb)
+
+    def load_sims(self, load_sim_pair, N_pairs, verb=False, preload=True, input_type='map'):
+        """Simulation pairs for the disconnected terms (polyspec/tspec_template.py:1128-1170)."""
+        self.N_it = N_pairs
+        print("Using %d pairs of Monte Carlo simulations" % self.N_it)
+        if preload:
+            self.preload = True
+            if self.ints_1d and (not hasattr(self, 'r_arr')):
+                raise Exception("Need to supply radial integration points or run optimize_radial_sampling_1d()!")
+            self.proc_a_maps, self.proc_b_maps = [], []
+            for ii in range(self.N_it):
+                if ii % 5 == 0 and verb:
+                    print("Processing bias simulation pair %d of %d" % (ii + 1, self.N_it))
+                a, b = self._process_sim(load_sim_pair(ii), input_type=input_type)
+                self.proc_a_maps.append(a)
+                self.proc_b_maps.append(b)
+        else:
+            self.preload = False
+            if verb:
+                print("No preloading; simulations will be loaded and accessed at runtime.")
+            self.load_sim_data = lambda ii: self._process_sim(load_sim_pair(ii), input_type=input_type)
+
+    def generate_sims(self, N_pairs, Cl_input=[], preload=True, verb=False):
+        """GRF simulation pairs for the disconnected terms (polyspec/tspec_template.py:1172-1229)."""
+        self.N_it = N_pairs
+        print("Using %d pairs of Monte Carlo simulations" % self.N_it)
+        if len(Cl_input) == 0:
+            Cl_input = self.base.Cl_tot
+        b = self.base
+
+        def pair(ii):
+            if self.ones_mask:
+                alpha = b.generate_data(int(1e5) + ii, Cl_input=Cl_input, output_type='harmonic', lmax=self.lmax,
+                                        deconvolve_beam=False)
+                beta = b.generate_data(int(2e5) + ii, Cl_input=Cl_input, output_type='harmonic', lmax=self.lmax,
+                                       deconvolve_beam=False)
+                return self._process_sim([alpha, beta], input_type='harmonic')
+            alpha = self.d_mask * b._in(b.generate_data(int(1e5) + ii, Cl_input=Cl_input, deconvolve_beam=False),
+                                        torch.float64)[0]
+            beta = self.d_mask * b._in(b.generate_data(int(2e5) + ii, Cl_input=Cl_input, deconvolve_beam=False),
+                                       torch.float64)[0]
+            return self._process_sim([alpha, beta])
+
+        if preload:
+            self.preload = True
+            if self.ints_1d and (not hasattr(self, 'r_arr')):
+                raise Exception("Need to supply radial integration points or run optimize_radial_sampling_1d()!")
+            self.proc_a_maps, self.proc_b_maps = [], []
+            for ii in range(self.N_it):
+                if ii % 5 == 0 and verb:
+                    print("Generating bias simulation pair %d of %d" % (ii + 1, self.N_it))
+                a, bb = pair(ii)
+                self.proc_a_maps.append(a)
+                self.proc_b_maps.append(bb)
+        else:
+            self.preload = False
+            if verb:
+                print("No preloading; simulations will be loaded and accessed at runtime.")
+            self.load_sim_data = pair
+
+    # ------------------------------------------------------------------ numerator
+    def Tl_numerator(self, data, include_disconnected_term=True, verb=False, input_type='map'):
+        """Numerator of the unwindowed trispectrum estimator (polyspec/tspec_template.py:1338-1955)."""
+        t_start = time.time()
+        if self.ints_1d and (not hasattr(self, 'r_arr')):
+            raise Exception("Need to supply radial integration points or run optimize_radial_sampling_1d()!")
+        if not hasattr(self, 'preload') and include_disconnected_term:
+            raise Exception("Need to generate or specify bias simulations!")
+        if self.pol:
+            assert len(data) == 3, "Data must contain T, Q, U components!"
+        else:
+            assert (len(data) == 1 and len(data[0]) == self.base.Npix) or len(data) == self.base.Npix, \
+                "Data must contain T only!"
+        if hasattr(self, 't0_num') and include_disconnected_term:
+            compute_t0 = False
+            if verb:
+                print("Using precomputed t0 term")
+        else:
+            compute_t0 = True
+        t0 = time.time()
+        d = self.base._in(data, torch.float64 if input_type == 'map' else torch.complex128)[0]
+        h_data_lm = self._sinv_filt(d, input_type)
+        self._timed('Sinv', t0)
+        proc_maps = self._apply_all_filters(h_data_lm)
+        A_pix = self.base.A_pix
+        t4_num = np.zeros(len(self.templates))
+        if not include_disconnected_term:
+            print("## No subtraction of (parity-conserving) disconnected terms performed!")
+        else:
+            t2_num = np.zeros(len(self.templates))
+            if compute_t0:
+                t0_num = np.zeros(len(self.templates))
+        if verb:
+            print("# Assembling trispectrum numerator (4-field term)")
+        Phi_dd = None
+        for ii, t in enumerate(self.templates):
+            if t == 'gNL-loc':
+                t0 = time.time()
+                t4_num[ii] = 9. / 100. * self.utils.gnl_loc_sum(self.r_weights[t], proc_maps['p00'], proc_maps['q']) \
+                    * 4. * A_pix * (4. * np.pi) ** 1.5
+                self._timed('gNL_summation', t0)
+            if t == 'lensing':
+                Phi_dd = self._compute_lensing_Phi(proc_maps, proc_maps)
+                w = self._lens_Ls()
+                t0 = time.time()
+                t4_num[ii] = 1. / 24. * float(torch.sum(w * (Phi_dd * Phi_dd.conj()).real)) * 12.
+                self._timed('lensing_summation', t0)
+            if t == 'point-source':
+                t0 = time.time()
+                t4_num[ii] = 1. / 24. * float(torch.sum(proc_maps['u'][0].real ** 4.)) * A_pix
+                self._timed('gNL_summation', t0)
+
+        if include_disconnected_term:
+            for isim in range(self.N_it):
+                if verb:
+                    print("# Assembling 2-field%s trispectrum numerator for simulation pair %d of %d"
+                          % ("" if not compute_t0 else " and 0-field", isim + 1, self.N_it))
+                if self.preload:
+                    pa, pb = self.proc_a_maps[isim], self.proc_b_maps[isim]
+                else:
+                    pa, pb = self.load_sim_data(isim)
+                for ii, t in enumerate(self.templates):
+                    if t == 'gNL-loc':
+                        t0 = time.time()
+                        w = self.r_weights[t]
+                        perm = lambda m12, m34: self.utils.gnl_loc_disc_sum(w, m12['p00'], m34['p00'], m12['q'],
+                                                                            m34['q'])
+                        summ = perm(proc_maps, pa) + perm(proc_maps, pb)
+                        t2_num[ii] += -54. / 100. * summ / self.N_it * A_pix * (4. * np.pi) ** 1.5
+                        if compute_t0:
+                            t0_num[ii] += 54. / 100. * perm(pa, pb) / self.N_it * A_pix * (4. * np.pi) ** 1.5
+                        self._timed('gNL_summation', t0)
+                    if t == 'lensing':
+                        w = self._lens_Ls()
+                        Phi_aa = self._compute_lensing_Phi(pa, pa)
+                        Phi_ad = self._compute_lensing_Phi(pa, proc_maps, add_sym=True)
+                        Phi_sum = 4. * Phi_aa * Phi_dd.conj() + 2. * Phi_ad * Phi_ad.conj()
+                        Phi_bb = self._compute_lensing_Phi(pb, pb)
+                        Phi_bd = self._compute_lensing_Phi(pb, proc_maps, add_sym=True)
+                        Phi_sum += 4. * Phi_bb * Phi_dd.conj() + 2. * Phi_bd * Phi_bd.conj()
+                        t0 = time.time()
+                        t2_num[ii] += -1. / 24. * float(torch.sum(w * Phi_sum).real) * 3. / self.N_it
+                        self._timed('lensing_summation', t0)
+                        if compute_t0:
+                            Phi_ab = self._compute_lensing_Phi(pa, pb, add_sym=True)
+                            Phi_sum = 4. * Phi_aa * Phi_bb.conj() + 2. * Phi_ab * Phi_ab.conj()
+                            t0 = time.time()
+                            t0_num[ii] += 1. / 24. * float(torch.sum(w * Phi_sum).real) * 3. / self.N_it
+                            self._timed('lensing_summation', t0)
+                    if t == 'point-source':
+                        t0 = time.time()
+                        perm = lambda m12, m34: float(torch.sum(m12['u'][0].real ** 2. * m34['u'][0].real ** 2.))
+                        summ = perm(proc_maps, pa) + perm(proc_maps, pb)
+                        t2_num[ii] += -3. / 24. * summ / self.N_it * A_pix
+                        if compute_t0:
+                            t0_num[ii] += 3. / 24. * perm(pa, pb) / self.N_it * A_pix
+                        self._timed('gNL_summation', t0)
+            if not compute_t0:
+                t0_num = self.t0_num
+            else:
+                self.t0_num = t0_num
+        self.timers['numerator'] += time.time() - t_start
+        if include_disconnected_term:
+            return t4_num + t2_num + t0_num
+        return t4_num
+
+    # ------------------------------------------------------------------ Fisher matrix
+    def _transform_maps(self, map123, flXs, weights):
+        """Sum_i w_i M_LM f^X_L(i) for real maps M [N_r, Npix] (polyspec/tspec_template.py:2575-2588, spin 0)."""
+        t0 = time.time()
+        lm_map = self.base.to_lm_vec(map123, lmax=self.lmax)[:, self.d_lminfilt].contiguous()
+        out = self.utils.radial_sum(lm_map, weights, flXs)
+        self._timed('fish_deriv', t0)
+        return out
+
+    def _weight_Q_maps(self, tmp_Q, weighting='Ainv'):
+        """S^-1 P weighting (A^-1 branch) or m weights (S^-1 branch) of Q rows
+        [R, 1+2 pol, nlm_filt] (polyspec/tspec_template.py:2556-2572), batched."""
+        if weighting == 'Sinv':
+            return tmp_Q * self.d_m_weight
+        t0 = time.time()
+        full = self._full_lm(self.d_beam_lm * tmp_Q, self.lmax)
+        R = len(full)
+        if self.ones_mask:
+            out = torch.stack([self.applySinv(full[r], input_type='harmonic', lmax=self.lmax) for r in range(R)])
+        else:
+            maps = torch.stack([self.base.to_map(full[r], lmax=self.lmax) for r in range(R)]) \
+                if full.shape[1] not in (1, 3) else self.base.to_map_batch(full, lmax=self.lmax)
+            maps = maps * self.d_mask[None]
+            if hasattr(self.applySinv, 'batched'):
+                out = self.applySinv.batched(maps, lmax=self.lmax)
+            else:
+                out = torch.stack([self.applySinv(m, lmax=self.lmax) for m in maps])
+        self._timed('Sinv', t0)
+        return out[:, :, self.d_lminfilt]
+
+    def _lensing_Q(self, U_maps, V_maps):
+        """Lensing Q derivatives [4, 1+2 pol, nlm_filt] (polyspec/tspec_template.py:2908-3014)."""
+        b = self.base
+        fields1 = {'u': U_maps[0], 'v': V_maps[0]}
+        fields2 = {'u': U_maps[1], 'v': V_maps[1]}
+        Ls = self.base.l_arr[(self.base.l_arr >= self.Lmin_lens) * (self.base.l_arr <= self.Lmax_lens)]
+        wL = torch.as_tensor(Ls * (Ls + 1.) * np.asarray(self.C_phi)[Ls], device=self._dev)
+        nL = (self.Lmax_lens + 1) * (self.Lmax_lens + 2) // 2
+
+        def W(m1, m2, add_sym=False):
+            tmp = torch.zeros(nL, dtype=torch.complex128, device=self._dev)
+            tmp[self.d_Lminfilt_lens] = wL * self._compute_lensing_Phi(m1, m2, add_sym=add_sym)
+            return b.to_map_spin(tmp, -tmp, spin=1, lmax=self.Lmax_lens)[0]
+
+        W_11 = W(fields1, fields1)
+        W_12sym = W(fields1, fields2, add_sym=True)
+        W_22 = W(fields2, fields2)
+        ls = torch.as_tensor(self.ls.astype(np.float64), device=self._dev)
+        lsi = torch.as_tensor(self.ls, device=self._dev)
+        Cl = {k: torch.as_tensor(np.asarray(v, dtype=np.float64), device=self._dev)[lsi]
+              for k, v in self.C_lens_weight.items()}
+        lpref0 = 0.5 * torch.sqrt(ls * (ls + 1.))
+        if self.pol:
+            lprefp1 = 0.25 * torch.sqrt((ls + 2.) * (ls - 1.))
+            lprefm1 = 0.25 * torch.sqrt((ls - 2.) * (ls + 3.))
+        f = self.d_lminfilt
+
+        def spin_lm(m, s):
+            pm = b.to_lm_spin(m, m.conj(), spin=s, lmax=self.lmax)
+            return pm[0][f], pm[1][f]
+
+        def get_Q(fields, Wm):
+            Q = torch.zeros((1 + 2 * self.pol, len(self.ls)), dtype=torch.complex128, device=self._dev)
+            m = torch.real(fields['v'][0] * Wm)
+            Q[0] = -b.to_lm(m[None], lmax=self.lmax)[0][f]
+            if self.pol:
+                m = fields['v'][1] * Wm - fields['v'][2] * Wm.conj()
+                p, mi = spin_lm(m, 2)
+                Q[1] = -0.25 * (p + mi)
+                Q[2] = 0.25j * (p - mi)
+            m = fields['u'][0] * Wm
+            p, mi = spin_lm(m, 1)
+            tp = p - mi
+            Q[0] += lpref0 * Cl['TT'] * tp
+            if self.pol:
+                Q[1] += lpref0 * Cl['TE'] * tp
+                for X, sgn_i in ((1, False), (2, True)):
+                    for s, lpref, conj in ((1, lprefp1, True), (3, lprefm1, False)):
+                        m = -fields['u'][X] * Wm.conj() if conj else fields['u'][X] * Wm
+                        p, mi = spin_lm(m, s)
+                        if not sgn_i:   # Z = E
+                            base_ = lpref * (p - mi)
+                            Q[0] += Cl['TE'] * base_
+                            Q[1] += Cl['EE'] * base_
+                            Q[2] += lpref * (-1.0j) * Cl['BB'] * (p + mi)
+                        else:           # Z = B
+                            base_ = lpref * 1.0j * (p + mi)
+                            Q[0] += Cl['TE'] * base_
+                            Q[1] += Cl['EE'] * base_
+                            Q[2] += lpref * Cl['BB'] * (p - mi)
+            return Q / 2.
+
+        out = torch.zeros((4, 1 + 2 * self.pol, len(self.ls)), dtype=torch.complex128, device=self._dev)
+        out[0] += 12 * get_Q(fields1, W_11)
+        out[1] += 12 * get_Q(fields2, W_22)
+        out[2] += 4 * get_Q(fields1, W_12sym)
+        out[2] += 4 * get_Q(fields2, W_11)
+        out[3] += 4 * get_Q(fields2, W_12sym)
+        out[3] += 4 * get_Q(fields1, W_22)
+        return out
+
+    def compute_fisher_contribution(self, seed, verb=False, a_lms=None):
+        """Fisher contribution of one pair of GRFs (polyspec/tspec_template.py:2590-3052).
+
+        ``a_lms`` (two beam-deconvolved harmonic fields) may replace the fields drawn
+        from ``seed``."""
+        t_start = time.time()
+        if self.ints_1d and (not hasattr(self, 'r_arr')):
+            raise Exception("Need to supply radial integration points or run optimize_radial_sampling_1d()!")
+        print("Computing Fisher matrix with seed %d" % seed)
+        b = self.base
+        nt = len(self.templates)
+        t0 = time.time()
+        if a_lms is None:
+            a_lms = []
+            for ii in range(2):
+                if self.ones_mask:
+                    a_lms.append(b.generate_data(seed=seed + int((1 + ii) * 1e9), output_type='harmonic',
+                                                 lmax=self.lmax, deconvolve_beam=True))
+                else:
+                    a_lms.append(b.generate_data(seed=seed + int((1 + ii) * 1e9), output_type='harmonic',
+                                                 deconvolve_beam=True))
+        a_lms = [b._in(a, torch.complex128)[0] for a in a_lms]
+        self._timed('fish_grfs', t0)
+
+        def compute_Q4(weighting):
+            t0 = time.time()
+            if weighting == 'Sinv':
+                if self.ones_mask:
+                    beam = b.dev('beam_lm', self.lmax)
+                    U = [self._sinv_filt(beam * a, 'harmonic') for a in a_lms]
+                else:
+                    U = [self._sinv_filt(self.d_mask * b.to_map(b.dev('beam_lm') * a)) for a in a_lms]
+                self._timed('Sinv', t0)
+            else:
+                if self.ones_mask:
+                    U = [b.applyAinv(a, input_type='harmonic', lmax=self.lmax)[:, self.d_lminfilt].contiguous()
+                         for a in a_lms]
+                else:
+                    U = [b.applyAinv(a, input_type='harmonic')[:, self.d_lfilt].contiguous() for a in a_lms]
+                self._timed('Ainv', t0)
+            if 'q' in self.to_compute:
+                Q_maps = self._filter_pair(U, 'Q')
+            if 'u' in self.to_compute:
+                U_maps = self._filter_pair(U, 'U')
+            if 'v' in self.to_compute:
+                V_maps = self._filter_pair(U, 'V')
+            if len(self.p_inds) > 0:
+                P_maps = self._filter_pair(U, 'P')
+            Qs = torch.zeros((4, nt, 1 + 2 * self.pol, len(self.ls)), dtype=torch.complex128, device=self._dev)
+            for ii, t in enumerate(self.templates):
+                if t == 'gNL-loc':
+                    w = self.r_weights[t]
+                    P0 = P_maps[0][:, 0] * np.sqrt(4. * np.pi)
+                    p = self.d_plLXs[self.nmax]
+                    q = self.d_qlXs
+                    u = self.utils
+                    Qs[0, ii] = 162. / 25. * self._transform_maps(u.multiply(P0[0], P0[0], Q_maps[0]), p, w)
+                    Qs[0, ii] += 54. / 25. * self._transform_maps(u.multiply(P0[0], P0[0], P0[0]), q, w)
+                    Qs[1, ii] = 162. / 25. * self._transform_maps(u.multiply(P0[1], P0[1], Q_maps[1]), p, w)
+                    Qs[1, ii] += 54. / 25. * self._transform_maps(u.multiply(P0[1], P0[1], P0[1]), q, w)
+                    Qs[2, ii] = 54. / 25. * self._transform_maps(u.multiply_asym(P0[0], P0[1], Q_maps[0], Q_maps[1]),
+                                                                 p, w)
+                    Qs[2, ii] += 54. / 25. * self._transform_maps(u.multiply(P0[0], P0[0], P0[1]), q, w)
+                    Qs[3, ii] = 54. / 25. * self._transform_maps(u.multiply_asym(P0[1], P0[0], Q_maps[1], Q_maps[0]),
+                                                                 p, w)
+                    Qs[3, ii] += 54. / 25. * self._transform_maps(u.multiply(P0[0], P0[1], P0[1]), q, w)
+                if t == 'lensing':
+                    Qs[:, ii] += self._lensing_Q(U_maps, V_maps)
+                if t == 'point-source':
+                    u0 = U_maps[:, 0]
+
+                    def psq(m):
+                        q = torch.zeros((1 + 2 * self.pol, len(self.ls)), dtype=torch.complex128, device=self._dev)
+                        q[0] = b.to_lm(m.real[None], lmax=self.lmax)[0, self.d_lminfilt]
+                        return q
+                    Qs[0, ii] = psq(u0[0] ** 3)
+                    Qs[1, ii] = psq(u0[1] ** 3)
+                    Qs[2, ii] = psq(u0[0] ** 2 * u0[1])
+                    Qs[3, ii] = psq(u0[1] ** 2 * u0[0])
+            flat = Qs.reshape(4 * nt, 1 + 2 * self.pol, len(self.ls))
+            flat = self._weight_Q_maps(flat, weighting)
+            return flat.reshape(4, nt, -1)
+
+        Q4_Sinv = compute_Q4('Sinv')
+        Q4_Ainv = compute_Q4('Ainv')
+        t0 = time.time()
+        fish = pixel.outer_product(Q4_Sinv, Q4_Ainv, self.base.nthreads, False)
+        self._timed('fish_outer', t0)
+        self.timers['fisher'] += time.time() - t_start
+        return fish.cpu().numpy()
+
+    def compute_fisher(self, N_it, verb=False):
+        """Monte Carlo Fisher matrix over seeds 0..N_it-1 (polyspec/tspec_template.py:3054-3072)."""
+        fish = np.zeros((len(self.templates), len(self.templates)))
+        for seed in range(N_it):
+            print("Computing Fisher contribution %d of %d" % (seed + 1, N_it))
+            fish += self.compute_fisher_contribution(seed, verb=verb * (seed == 0)) / N_it
+        self.fish = fish
+        self.inv_fish = np.linalg.inv(fish)
+        return fish
+
+    def Tl_unwindowed(self, data, fish=[], include_disconnected_term=True, verb=False, input_type='map'):
+        """inv(F) times the numerator, one entry per template (polyspec/tspec_template.py:3074-3108)."""
+        if len(fish) != 0:
+            self.fish = fish
+            self.inv_fish = np.linalg.inv(fish)
+        if not hasattr(self, 'inv_fish'):
+            raise Exception("Need to compute Fisher matrix first!")
+        Tl_num = self.Tl_numerator(data, verb=verb, include_disconnected_term=include_disconnected_term,
+                                   input_type=input_type)
+        Tl_out = np.matmul(self.inv_fish, Tl_num)
+        return {t: Tl_out[i] for i, t in enumerate(self.templates)}
+
+    def optimize_radial_sampling_1d(self, *args, **kwargs):
+        raise NotImplementedError("the radial-sampling optimiser is not implemented by the CUDA backend")
+
+    def optimize_radial_sampling_2d(self, *args, **kwargs):
+        raise NotImplementedError("the radial-sampling optimiser is not implemented by the CUDA backend")

@@ -176,3 +176,49 @@ def bispec_setup(nside=256, lmax=511, nbins=10, fwhm_arcmin=30.0, pol=True):
     l_bins = np.unique(np.round(np.geomspace(2, lmax, nbins + 1)).astype(int))
     fields = ['TTT', 'TTE', 'TEE', 'EEE'] if pol else ['TTT']
     return cltot, cl, beam, mask, l_bins, fields
+
+
+def smooth_transfer(npol, k_arr, lmax, seed=3):
+    """Seeded smooth stand-in transfer functions T_l^X(k) [npol, lmax+1, nk]: sums of
+    Gaussian bumps in (log k, l), zero at l = 0, 1."""
+    rng = np.random.default_rng(seed)
+    l = np.arange(lmax + 1)[:, None]
+    lk = np.log(k_arr)[None, :]
+    T = np.zeros((npol, lmax + 1, len(k_arr)))
+    for X in range(npol):
+        for _ in range(8):
+            a = rng.normal() * (0.3 if X else 1.0)
+            lc = rng.uniform(np.log(2e-4), np.log(0.08))
+            sl = rng.uniform(0.4, 1.2)
+            l0 = rng.uniform(0, lmax)
+            s0 = rng.uniform(0.05, 0.3) * lmax
+            T[X] += a * np.exp(-(lk - lc) ** 2 / (2 * sl ** 2) - (l - l0) ** 2 / (2 * s0 ** 2))
+    T[:, :2] = 0.
+    return T
+
+
+def tspec_setup(nside=512, lmax=1000, n_r=24, nk=400, fwhm_arcmin=10.0, pol=True, seed=0):
+    """Template-trispectrum workload (gNL-loc, lensing, point-source): seeded smooth
+    transfer functions on nk log-spaced k in [1e-4, 0.1], n_r radial samples around
+    recombination with seeded weights, C_phi = 1e-7 / (L (L+1))^2, the fiducial
+    spectra as lensing weights, Gaussian beam, latitude mask, ideal S^-1 filter.
+    Returns a dict of the TSpecTemplate arguments and the base's inputs."""
+    base_lmax = 3 * nside - 1
+    cl = fiducial_cl(base_lmax, pol)
+    b = gaussian_beam(base_lmax, fwhm_arcmin)
+    nf = 3 if pol else 1
+    beam = np.stack([b] * nf)
+    nl = noise_cl(nside, base_lmax, 30.0, pol)
+    cltot = total_cl(cl, beam, nl)
+    mask = latitude_mask(nside, 15.0, 5.0)
+    k_arr = np.geomspace(1e-4, 0.1, nk)
+    rng = np.random.default_rng(seed + 1)
+    r_values = np.linspace(13300., 14400., n_r)
+    weights = rng.uniform(0.5, 1.5, n_r) * (r_values[1] - r_values[0])
+    L = np.arange(base_lmax + 1, dtype=np.float64)
+    C_phi = np.zeros(base_lmax + 1)
+    C_phi[1:] = 1e-7 / (L[1:] * (L[1:] + 1.)) ** 2
+    C_lens = {k: cl[k].copy() for k in (['TT', 'TE', 'EE', 'BB'] if pol else ['TT'])}
+    return dict(cltot=cltot, cl=cl, beam=beam, mask=mask, k_arr=k_arr,
+                Tl_arr=smooth_transfer(2 if pol else 1, k_arr, lmax + 1, seed + 3), r_values=r_values,
+                r_weights={'gNL-loc': weights}, C_phi=C_phi, C_lens_weight=C_lens, lmin=2, lmax=lmax)

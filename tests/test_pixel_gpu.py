@@ -108,7 +108,7 @@ def test_lens_phi(npol, npix):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("npol", [1, 2])
+@pytest.mark.parametrize("npol", [1, 2, 3])
 @pytest.mark.parametrize("lmax,nr", [(12, 7), (100, 24)])
 def test_harmonic_weightings(npol, lmax, nr):
     from polyspec_b200 import pixel as P

@@ -65,7 +65,7 @@ def test_lens_phi_matches_reference(npol):
     assert close(O.lens_phi_sum_sym(U, U2, V, V2), F.lens_phi_sum_sym(U, U2, V, V2, 2), 1e-14)
 
 
-@pytest.mark.parametrize("npol", [1, 2])
+@pytest.mark.parametrize("npol", [1, 2, 3])
 def test_harmonic_weightings_match_reference(npol):
     T, _ = _ref()
     lmax, nr = 12, 7
