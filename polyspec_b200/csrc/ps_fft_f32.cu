@@ -8,11 +8,13 @@
 // are Hermitian): the synthesis transforms conj(c_a) + i conj(c_b) and reads
 // map_a, map_b from the real and imaginary parts; the adjoint transforms
 // x_a + i x_b and separates X_a = (Z_k + Z*_{N-k})/2, X_b = (Z_k - Z*_{N-k})/(2i).
-// Spin-0 maps get one FFT each (pack = 0): packing two independent maps would add
-// the rounding of the larger to the smaller (at the larger one's scale), which
-// shows when batch members differ by many orders of magnitude (the Fisher rows of
-// different templates do); the components of one spin map are mixed by the
-// Legendre stage anyway.  A CTA runs G such FFTs
+// A spin-0 map packs a ring with its mirror ring instead (pack = 0; same length
+// and phi0; the launch walks the north rings, the equator ring alone): packing two
+// different maps would add the rounding of the larger to the smaller at the larger
+// one's scale, which shows when batch members differ by many orders of magnitude
+// (the Fisher rows of different templates do), while the two rings of one map, or
+// the two components of one spin map (mixed by the Legendre stage anyway), share
+// their scale.  A CTA runs G such FFTs
 // at once (G = 256 / T threads per FFT), so small rings keep every thread busy.
 // FFTs are radix-2 with stages fused in pairs (one barrier and one shared-memory
 // round trip per two stages): decimation in frequency for power-of-two rings,
@@ -157,38 +159,43 @@ __device__ __forceinline__ RingDFTf make_dft(const RingInfo& g) {
 // ---------------------------------------------------------------------------
 // synthesis: phase [R][mmax+1][nf] (complex64) -> map [nf][npix] (float64)
 // grid (rings of the class, ceil(pairs / G)); block T*G threads; smem G*M float2
-__global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list,
+__global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list, int R,
                                const float2* __restrict__ phase, double* __restrict__ map, int mmax, int nf,
                                int64_t npix, const float2* __restrict__ tw, int twlog,
                                const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T,
                                int pack) {
   extern __shared__ float2 fbuf[];
   const int ir = ring_list[blockIdx.x];
+  // partner of a packed FFT: the other component of the same map (pack), else the
+  // same map on the mirror ring (same nphi and phi0; the list holds north rings)
+  const int irb = pack ? ir : R - 1 - ir;
   const RingInfo g = rings[ir];
+  const int64_t start_b = rings[irb].start;
   const RingDFTf d = make_dft(g);
   const float2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
   const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
   const int G = blockDim.x / T;
   const int unit = blockIdx.y * G + grp;
-  const int fa = pack ? 2 * unit : unit, fb = fa + 1;
-  const bool va = fa < nf, vb = pack && fb < nf;
+  const int fa = pack ? 2 * unit : unit, fb = pack ? fa + 1 : unit;
+  const bool va = fa < nf, vb = pack ? fb < nf : (va && irb != ir);
   float2* buf = fbuf + size_t(grp) * d.M;
   const int N = d.N;
   const int64_t pden = g.phi_den;
-  const float2* ph = phase + int64_t(ir) * (mmax + 1) * nf;
+  const float2* pha = phase + int64_t(ir) * (mmax + 1) * nf;
+  const float2* phb = phase + int64_t(irb) * (mmax + 1) * nf;
   // buf_k = conj(c_a,k) + i conj(c_b,k);  c_k = sum_{m=k mod N} F_m e^{i m phi0} + sum_{m=-k mod N, m>0} conj(...)
   for (int kk = u; kk < N; kk += T) {
     float2 ca = make_float2(0.f, 0.f), cb = ca;
     if (va) {
       for (int m = kk; m <= mmax; m += N) {
         const float2 e = expi_pi_ratio_f(int64_t(m) * g.phi_num, pden);
-        ca = fadd2(ca, fmul2(ph[int64_t(m) * nf + fa], e));
-        if (vb) cb = fadd2(cb, fmul2(ph[int64_t(m) * nf + fb], e));
+        ca = fadd2(ca, fmul2(pha[int64_t(m) * nf + fa], e));
+        if (vb) cb = fadd2(cb, fmul2(phb[int64_t(m) * nf + fb], e));
       }
       for (int m = (kk == 0) ? N : N - kk; m <= mmax; m += N) {
         const float2 e = expi_pi_ratio_f(int64_t(m) * g.phi_num, pden);
-        ca = fadd2(ca, fconj2(fmul2(ph[int64_t(m) * nf + fa], e)));
-        if (vb) cb = fadd2(cb, fconj2(fmul2(ph[int64_t(m) * nf + fb], e)));
+        ca = fadd2(ca, fconj2(fmul2(pha[int64_t(m) * nf + fa], e)));
+        if (vb) cb = fadd2(cb, fconj2(fmul2(phb[int64_t(m) * nf + fb], e)));
       }
     }
     // a real field keeps only Re(c_0) (F_0's imaginary part drops out of the
@@ -201,7 +208,7 @@ __global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __
   ring_dft_forward_f(buf, d, tw, twlog, bspec, u, T);
   if (va) {
     double* oa = map + int64_t(fa) * npix + g.start;
-    double* ob = map + int64_t(fb) * npix + g.start;
+    double* ob = map + int64_t(fb) * npix + start_b;
     for (int j = u; j < N; j += T) {
       const float2 y = dft_get_f(buf, d, j);
       oa[j] = double(y.x);
@@ -211,33 +218,38 @@ __global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __
 }
 
 // adjoint: map [nf][npix] (float64) -> phase [R][mmax+1][nf] (complex64)
-__global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list,
+__global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list, int R,
                                  const double* __restrict__ map, float2* __restrict__ phase, int mmax, int nf,
                                  int64_t npix, const float2* __restrict__ tw, int twlog,
                                  const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T,
                                int pack) {
   extern __shared__ float2 fbuf[];
   const int ir = ring_list[blockIdx.x];
+  // partner of a packed FFT: the other component of the same map (pack), else the
+  // same map on the mirror ring (same nphi and phi0; the list holds north rings)
+  const int irb = pack ? ir : R - 1 - ir;
   const RingInfo g = rings[ir];
+  const int64_t start_b = rings[irb].start;
   const RingDFTf d = make_dft(g);
   const float2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
   const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
   const int G = blockDim.x / T;
   const int unit = blockIdx.y * G + grp;
-  const int fa = pack ? 2 * unit : unit, fb = fa + 1;
-  const bool va = fa < nf, vb = pack && fb < nf;
+  const int fa = pack ? 2 * unit : unit, fb = pack ? fa + 1 : unit;
+  const bool va = fa < nf, vb = pack ? fb < nf : (va && irb != ir);
   float2* buf = fbuf + size_t(grp) * d.M;
   const int N = d.N;
   const int64_t pden = g.phi_den;
   {
     const double* ia = map + int64_t(va ? fa : 0) * npix + g.start;
-    const double* ib = map + int64_t(vb ? fb : 0) * npix + g.start;
+    const double* ib = map + int64_t(vb ? fb : 0) * npix + (vb ? start_b : g.start);
     for (int j = u; j < N; j += T) buf[j] = make_float2(va ? float(ia[j]) : 0.f, vb ? float(ib[j]) : 0.f);
   }
   __syncthreads();
   ring_dft_forward_f(buf, d, tw, twlog, bspec, u, T);
   if (va) {
-    float2* ph = phase + int64_t(ir) * (mmax + 1) * nf;
+    float2* pha = phase + int64_t(ir) * (mmax + 1) * nf;
+    float2* phb = phase + int64_t(irb) * (mmax + 1) * nf;
     for (int m = u; m <= mmax; m += T) {
       const int k = m % N, k2 = (N - k) % N;
       const float2 z = dft_get_f(buf, d, k), z2 = fconj2(dft_get_f(buf, d, k2));
@@ -245,8 +257,8 @@ __global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* 
       const float2 xa = make_float2(0.5f * (z.x + z2.x), 0.5f * (z.y + z2.y));
       // (z - z2) / (2i) = -i (z - z2) / 2
       const float2 xb = make_float2(0.5f * (z.y - z2.y), -0.5f * (z.x - z2.x));
-      ph[int64_t(m) * nf + fa] = fmul2(xa, e);
-      if (vb) ph[int64_t(m) * nf + fb] = fmul2(xb, e);
+      pha[int64_t(m) * nf + fa] = fmul2(xa, e);
+      if (vb) phb[int64_t(m) * nf + fb] = fmul2(xb, e);
     }
   }
 }
@@ -272,7 +284,7 @@ int launch_ring_synth_f32(const Plan& P, const int* d_list, int nrings, int work
   int twlog = 0;
   while ((1 << twlog) < P.max_fft) ++twlog;
   StatScope sc(PS_K_FFT_SYNTH, 0.0, 0.0, st);
-  ring_synth_f32<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, phase, map, P.mmax, nf, P.npix,
+  ring_synth_f32<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, P.R, phase, map, P.mmax, nf, P.npix,
                                                          P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off, T, pack);
   PS_LAUNCH_CHECK();
   return PS_OK;
@@ -292,7 +304,7 @@ int launch_ring_adjoint_f32(const Plan& P, const int* d_list, int nrings, int wo
   int twlog = 0;
   while ((1 << twlog) < P.max_fft) ++twlog;
   StatScope sc(PS_K_FFT_ADJOINT, 0.0, 0.0, st);
-  ring_adjoint_f32<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, map, phase, P.mmax, nf, P.npix,
+  ring_adjoint_f32<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, P.R, map, phase, P.mmax, nf, P.npix,
                                                            P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off, T, pack);
   PS_LAUNCH_CHECK();
   return PS_OK;

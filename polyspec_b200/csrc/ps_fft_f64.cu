@@ -7,11 +7,13 @@
 // are Hermitian): the synthesis transforms conj(c_a) + i conj(c_b) and reads
 // map_a, map_b from the real and imaginary parts; the adjoint transforms
 // x_a + i x_b and separates X_a = (Z_k + Z*_{N-k})/2, X_b = (Z_k - Z*_{N-k})/(2i).
-// Spin-0 maps get one FFT each (pack = 0): packing two independent maps would add
-// the rounding of the larger to the smaller (at the larger one's scale), which
-// shows when batch members differ by many orders of magnitude (the Fisher rows of
-// different templates do); the components of one spin map are mixed by the
-// Legendre stage anyway.  A CTA runs G such FFTs
+// A spin-0 map packs a ring with its mirror ring instead (pack = 0; same length
+// and phi0; the launch walks the north rings, the equator ring alone): packing two
+// different maps would add the rounding of the larger to the smaller at the larger
+// one's scale, which shows when batch members differ by many orders of magnitude
+// (the Fisher rows of different templates do), while the two rings of one map, or
+// the two components of one spin map (mixed by the Legendre stage anyway), share
+// their scale.  A CTA runs G such FFTs
 // at once (G = 256 / T threads per FFT); the grid is (rings of one work length,
 // groups of field pairs).  FFTs are radix-2 with stages fused in pairs (one
 // barrier and one shared-memory round trip per two stages): decimation in
@@ -154,24 +156,29 @@ __device__ __forceinline__ double2 dft_get(const double2* buf, const RingDFT& d,
 // ---------------------------------------------------------------------------
 // synthesis: phase [R][mmax+1][nf] -> map [nf][npix]
 // grid (rings of the class, ceil(pairs / G)); block T*G threads; smem G*M double2
-__global__ void ring_synth_f64(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list,
+__global__ void ring_synth_f64(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list, int R,
                                const double2* __restrict__ phase, double* __restrict__ map, int mmax, int nf,
                                int64_t npix, const double2* __restrict__ tw, int twlog,
                                const double2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T,
                                int pack) {
   extern __shared__ double2 dbuf[];
   const int ir = ring_list[blockIdx.x];
+  // partner of a packed FFT: the other component of the same map (pack), else the
+  // same map on the mirror ring (same nphi and phi0; the list holds north rings)
+  const int irb = pack ? ir : R - 1 - ir;
   const RingInfo g = rings[ir];
+  const int64_t start_b = rings[irb].start;
   const RingDFT d = make_dft_d(g);
   const double2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
   const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
   const int G = blockDim.x / T;
   const int unit = blockIdx.y * G + grp;
-  const int fa = pack ? 2 * unit : unit, fb = fa + 1;
-  const bool va = fa < nf, vb = pack && fb < nf;
+  const int fa = pack ? 2 * unit : unit, fb = pack ? fa + 1 : unit;
+  const bool va = fa < nf, vb = pack ? fb < nf : (va && irb != ir);
   double2* buf = dbuf + size_t(grp) * d.M;
   const int N = d.N;
-  const double2* ph = phase + int64_t(ir) * (mmax + 1) * nf;
+  const double2* pha = phase + int64_t(ir) * (mmax + 1) * nf;
+  const double2* phb = phase + int64_t(irb) * (mmax + 1) * nf;
   // buf_k = conj(c_a,k) + i conj(c_b,k);  c_k = sum_{m=k mod N} F_m e^{i m phi0} + sum_{m=-k mod N, m>0} conj(...)
   for (int kk = u; kk < N; kk += T) {
     double2 ca = make_double2(0.0, 0.0), cb = ca;
@@ -182,15 +189,15 @@ __global__ void ring_synth_f64(const RingInfo* __restrict__ rings, const int* __
       const double2 step = expi_pi_ratio(int64_t(N) * g.phi_num, g.phi_den);
       double2 e = e0;
       for (int m = kk; m <= mmax; m += N) {
-        ca = cadd(ca, cmul(ph[int64_t(m) * nf + fa], e));
-        if (vb) cb = cadd(cb, cmul(ph[int64_t(m) * nf + fb], e));
+        ca = cadd(ca, cmul(pha[int64_t(m) * nf + fa], e));
+        if (vb) cb = cadd(cb, cmul(phb[int64_t(m) * nf + fb], e));
         e = cmul(e, step);
       }
       // m = m0 + j N with m0 = N - kk (N for kk = 0): e^{i m0 phi0} = conj(e0) step
       e = cmul(cconj(e0), step);
       for (int m = (kk == 0) ? N : N - kk; m <= mmax; m += N) {
-        ca = cadd(ca, cconj(cmul(ph[int64_t(m) * nf + fa], e)));
-        if (vb) cb = cadd(cb, cconj(cmul(ph[int64_t(m) * nf + fb], e)));
+        ca = cadd(ca, cconj(cmul(pha[int64_t(m) * nf + fa], e)));
+        if (vb) cb = cadd(cb, cconj(cmul(phb[int64_t(m) * nf + fb], e)));
         e = cmul(e, step);
       }
     }
@@ -202,7 +209,7 @@ __global__ void ring_synth_f64(const RingInfo* __restrict__ rings, const int* __
   ring_dft_forward(buf, d, tw, twlog, bspec, u, T);
   if (va) {
     double* oa = map + int64_t(fa) * npix + g.start;
-    double* ob = map + int64_t(fb) * npix + g.start;
+    double* ob = map + int64_t(fb) * npix + start_b;
     for (int j = u; j < N; j += T) {
       const double2 y = dft_get(buf, d, j);
       oa[j] = y.x;
@@ -212,32 +219,37 @@ __global__ void ring_synth_f64(const RingInfo* __restrict__ rings, const int* __
 }
 
 // adjoint: map [nf][npix] -> phase [R][mmax+1][nf]
-__global__ void ring_adjoint_f64(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list,
+__global__ void ring_adjoint_f64(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list, int R,
                                  const double* __restrict__ map, double2* __restrict__ phase, int mmax, int nf,
                                  int64_t npix, const double2* __restrict__ tw, int twlog,
                                  const double2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T,
                                int pack) {
   extern __shared__ double2 dbuf[];
   const int ir = ring_list[blockIdx.x];
+  // partner of a packed FFT: the other component of the same map (pack), else the
+  // same map on the mirror ring (same nphi and phi0; the list holds north rings)
+  const int irb = pack ? ir : R - 1 - ir;
   const RingInfo g = rings[ir];
+  const int64_t start_b = rings[irb].start;
   const RingDFT d = make_dft_d(g);
   const double2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
   const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
   const int G = blockDim.x / T;
   const int unit = blockIdx.y * G + grp;
-  const int fa = pack ? 2 * unit : unit, fb = fa + 1;
-  const bool va = fa < nf, vb = pack && fb < nf;
+  const int fa = pack ? 2 * unit : unit, fb = pack ? fa + 1 : unit;
+  const bool va = fa < nf, vb = pack ? fb < nf : (va && irb != ir);
   double2* buf = dbuf + size_t(grp) * d.M;
   const int N = d.N;
   {
     const double* ia = map + int64_t(va ? fa : 0) * npix + g.start;
-    const double* ib = map + int64_t(vb ? fb : 0) * npix + g.start;
+    const double* ib = map + int64_t(vb ? fb : 0) * npix + (vb ? start_b : g.start);
     for (int j = u; j < N; j += T) buf[j] = make_double2(va ? ia[j] : 0.0, vb ? ib[j] : 0.0);
   }
   __syncthreads();
   ring_dft_forward(buf, d, tw, twlog, bspec, u, T);
   if (va) {
-    double2* ph = phase + int64_t(ir) * (mmax + 1) * nf;
+    double2* pha = phase + int64_t(ir) * (mmax + 1) * nf;
+    double2* phb = phase + int64_t(irb) * (mmax + 1) * nf;
     for (int k = u; k < N && k <= mmax; k += T) {
       const int k2 = (N - k) % N;
       const double2 z = dft_get(buf, d, k), z2 = cconj(dft_get(buf, d, k2));
@@ -247,8 +259,8 @@ __global__ void ring_adjoint_f64(const RingInfo* __restrict__ rings, const int* 
       double2 e = expi_pi_ratio(-int64_t(k) * g.phi_num, g.phi_den);
       const double2 step = expi_pi_ratio(-int64_t(N) * g.phi_num, g.phi_den);
       for (int m = k; m <= mmax; m += N) {
-        ph[int64_t(m) * nf + fa] = cmul(xa, e);
-        if (vb) ph[int64_t(m) * nf + fb] = cmul(xb, e);
+        pha[int64_t(m) * nf + fa] = cmul(xa, e);
+        if (vb) phb[int64_t(m) * nf + fb] = cmul(xb, e);
         e = cmul(e, step);
       }
     }
@@ -277,7 +289,7 @@ int launch_ring_synth_f64(const Plan& P, const int* d_list, int nrings, int work
   int twlog = 0;
   while ((1 << twlog) < P.max_fft) ++twlog;
   StatScope sc(PS_K_FFT_SYNTH, 0.0, 0.0, st);
-  ring_synth_f64<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, phase, map, P.mmax, nf, P.npix,
+  ring_synth_f64<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, P.R, phase, map, P.mmax, nf, P.npix,
                                                          P.d_twiddle, twlog, P.d_bs_spec, P.d_bs_off, T, pack);
   PS_LAUNCH_CHECK();
   return PS_OK;
@@ -298,7 +310,7 @@ int launch_ring_adjoint_f64(const Plan& P, const int* d_list, int nrings, int wo
   int twlog = 0;
   while ((1 << twlog) < P.max_fft) ++twlog;
   StatScope sc(PS_K_FFT_ADJOINT, 0.0, 0.0, st);
-  ring_adjoint_f64<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, map, phase, P.mmax, nf, P.npix,
+  ring_adjoint_f64<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, P.R, map, phase, P.mmax, nf, P.npix,
                                                            P.d_twiddle, twlog, P.d_bs_spec, P.d_bs_off, T, pack);
   PS_LAUNCH_CHECK();
   return PS_OK;

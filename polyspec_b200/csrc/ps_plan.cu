@@ -45,6 +45,7 @@ struct ps_plan {
   bool is_band = false;
   // FFT length classes: rings with the same work length share a launch
   std::vector<int> cls_len, cls_off, cls_cnt;
+  std::vector<int> cls_off_n, cls_cnt_n;  // the north rings (and the equator ring) of each class
   int* d_ring_lists = nullptr;
   std::vector<void*> owned;  // device allocations to free
 };
@@ -213,6 +214,13 @@ int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_pl
     pl->cls_cnt.push_back((int)kv.second.size());
     // largest rings first inside a class does not matter: all have equal work
     lists.insert(lists.end(), kv.second.begin(), kv.second.end());
+  }
+  for (auto& kv : classes) {
+    pl->cls_off_n.push_back((int)lists.size());
+    int n = 0;
+    for (int ir : kv.second)
+      if (ir <= P.R - 1 - ir) { lists.push_back(ir); ++n; }
+    pl->cls_cnt_n.push_back(n);
   }
   std::vector<double2> tw(max_fft / 2);
   for (int k = 0; k < max_fft / 2; ++k) {
@@ -525,8 +533,9 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
     rc = ps::launch_legendre_synth_tc(P, almT, phase, batch, spin, P.d_err, stream);
     if (rc) return rc;
     for (size_t c = 0; c < plan->cls_len.size(); ++c) {
-      rc = ps::launch_ring_synth_f32(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c], plan->cls_len[c],
-                                     phase, map, nf, spin > 0, stream);
+      rc = ps::launch_ring_synth_f32(P, plan->d_ring_lists + (spin ? plan->cls_off[c] : plan->cls_off_n[c]),
+                                     spin ? plan->cls_cnt[c] : plan->cls_cnt_n[c], plan->cls_len[c], phase, map, nf,
+                                     spin > 0, stream);
       if (rc) return rc;
     }
     return PS_OK;
@@ -535,8 +544,9 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
   rc = ps::launch_legendre_synth_f64(P, almT, phase, batch, spin, stream);
   if (rc) return rc;
   for (size_t c = 0; c < plan->cls_len.size(); ++c) {
-    rc = ps::launch_ring_synth_f64(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c], plan->cls_len[c],
-                                   phase, map, nf, spin > 0, stream);
+    rc = ps::launch_ring_synth_f64(P, plan->d_ring_lists + (spin ? plan->cls_off[c] : plan->cls_off_n[c]),
+                                   spin ? plan->cls_cnt[c] : plan->cls_cnt_n[c], plan->cls_len[c], phase, map, nf,
+                                   spin > 0, stream);
     if (rc) return rc;
   }
   return PS_OK;
@@ -561,8 +571,9 @@ int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, i
     float2* phase = reinterpret_cast<float2*>(ws);
     float2* partial = reinterpret_cast<float2*>(ws + phase_bytes);
     for (size_t c = 0; c < plan->cls_len.size(); ++c) {
-      rc = ps::launch_ring_adjoint_f32(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c],
-                                       plan->cls_len[c], map, phase, nf, spin > 0, stream);
+      rc = ps::launch_ring_adjoint_f32(P, plan->d_ring_lists + (spin ? plan->cls_off[c] : plan->cls_off_n[c]),
+                                       spin ? plan->cls_cnt[c] : plan->cls_cnt_n[c], plan->cls_len[c], map, phase,
+                                       nf, spin > 0, stream);
       if (rc) return rc;
     }
     const int ch = adjoint_chunk(P, batch, spin);
@@ -579,8 +590,9 @@ int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, i
   double2* phase = reinterpret_cast<double2*>(ws);
   double2* partial = reinterpret_cast<double2*>(ws + phase_bytes);
   for (size_t c = 0; c < plan->cls_len.size(); ++c) {
-    rc = ps::launch_ring_adjoint_f64(P, plan->d_ring_lists + plan->cls_off[c], plan->cls_cnt[c], plan->cls_len[c],
-                                     map, phase, nf, spin > 0, stream);
+    rc = ps::launch_ring_adjoint_f64(P, plan->d_ring_lists + (spin ? plan->cls_off[c] : plan->cls_off_n[c]),
+                                     spin ? plan->cls_cnt[c] : plan->cls_cnt_n[c], plan->cls_len[c], map, phase, nf,
+                                     spin > 0, stream);
     if (rc) return rc;
   }
   const int ch = adjoint_chunk(P, batch, spin);
