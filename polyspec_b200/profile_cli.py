@@ -130,6 +130,13 @@ def bspec(a):
         wts = Weightings(base, np.stack([mask] * 3), dict(cl), noise_cov=W.white_noise_cov(a.nside))
         bsb = BSpecBin(base, mask, wts.make_applySinv('ideal'), l_bins, fields=fields, parity='both')
         bsb._compute_symmetry_factor()
+        if a.numerator_only:
+            data = base.to_map(base.generate_data(seed=3, output_type='harmonic', rng='device'))
+            bsb.generate_sims(2)
+            bsb.Bl_numerator(data)
+            torch.cuda.synchronize()
+            print("bspec %s numerator done (N_b %d)" % (prec, bsb.N_b), flush=True)
+            continue
         a_lms = [base.generate_data(seed=11 + i, deconvolve_beam=True, output_type='harmonic', rng='device')
                  for i in range(2)]
         f = bsb.compute_fisher_contribution(0, a_lms=a_lms)  # warm-up (autotuning, lazy set-up)
@@ -251,6 +258,7 @@ def main(argv=None):
     b.add_argument("--nbins", type=int, default=10)
     b.add_argument("--reps", type=int, default=2)
     b.add_argument("--precs", default="fp64,mixed")
+    b.add_argument("--numerator-only", action="store_true", help="only Bl_numerator (for kernel captures)")
     t = sub.add_parser("tspec")
     t.add_argument("--nside", type=int, default=512)
     t.add_argument("--lmax", type=int, default=1000)
