@@ -14,9 +14,11 @@
 // (the Fisher rows of different templates do), while the two rings of one map, or
 // the two components of one spin map (mixed by the Legendre stage anyway), share
 // their scale.  A CTA runs G such FFTs
-// at once (G = 256 / T threads per FFT); the grid is (rings of one work length,
-// groups of field pairs).  FFTs are radix-2 with stages fused in pairs (one
-// barrier and one shared-memory round trip per two stages): decimation in
+// at once (G = 256 / T threads per FFT); the grid is (groups of fields, rings of
+// one work length), fields fastest, so that the CTAs of all maps of a ring run
+// together and share in L2 the sectors of the ring's phases (stored map-innermost).
+// FFTs are radix-2 with stages fused in pairs (one barrier and one shared-memory
+// round trip per two stages): decimation in
 // frequency for power-of-two rings, Bluestein's chirp-z convolution of
 // power-of-two length M >= 2 nphi - 1 for the others.
 //
@@ -155,14 +157,14 @@ __device__ __forceinline__ double2 dft_get(const double2* buf, const RingDFT& d,
 
 // ---------------------------------------------------------------------------
 // synthesis: phase [R][mmax+1][nf] -> map [nf][npix]
-// grid (rings of the class, ceil(pairs / G)); block T*G threads; smem G*M double2
+// grid (ceil(units / G), rings of the class); block T*G threads; smem G*M double2
 __global__ void ring_synth_f64(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list, int R,
                                const double2* __restrict__ phase, double* __restrict__ map, int mmax, int nf,
                                int64_t npix, const double2* __restrict__ tw, int twlog,
                                const double2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T,
                                int pack) {
   extern __shared__ double2 dbuf[];
-  const int ir = ring_list[blockIdx.x];
+  const int ir = ring_list[blockIdx.y];
   // partner of a packed FFT: the other component of the same map (pack), else the
   // same map on the mirror ring (same nphi and phi0; the list holds north rings)
   const int irb = pack ? ir : R - 1 - ir;
@@ -172,7 +174,7 @@ __global__ void ring_synth_f64(const RingInfo* __restrict__ rings, const int* __
   const double2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
   const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
   const int G = blockDim.x / T;
-  const int unit = blockIdx.y * G + grp;
+  const int unit = blockIdx.x * G + grp;
   const int fa = pack ? 2 * unit : unit, fb = pack ? fa + 1 : unit;
   const bool va = fa < nf, vb = pack ? fb < nf : (va && irb != ir);
   double2* buf = dbuf + size_t(grp) * d.M;
@@ -225,7 +227,7 @@ __global__ void ring_adjoint_f64(const RingInfo* __restrict__ rings, const int* 
                                  const double2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T,
                                int pack) {
   extern __shared__ double2 dbuf[];
-  const int ir = ring_list[blockIdx.x];
+  const int ir = ring_list[blockIdx.y];
   // partner of a packed FFT: the other component of the same map (pack), else the
   // same map on the mirror ring (same nphi and phi0; the list holds north rings)
   const int irb = pack ? ir : R - 1 - ir;
@@ -235,7 +237,7 @@ __global__ void ring_adjoint_f64(const RingInfo* __restrict__ rings, const int* 
   const double2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
   const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
   const int G = blockDim.x / T;
-  const int unit = blockIdx.y * G + grp;
+  const int unit = blockIdx.x * G + grp;
   const int fa = pack ? 2 * unit : unit, fb = pack ? fa + 1 : unit;
   const bool va = fa < nf, vb = pack ? fb < nf : (va && irb != ir);
   double2* buf = dbuf + size_t(grp) * d.M;
@@ -280,7 +282,7 @@ int launch_ring_synth_f64(const Plan& P, const int* d_list, int nrings, int work
   if (nrings == 0) return PS_OK;
   int T, G, gy;
   fft_shape_d(work_len, nf, pack, T, G, gy);
-  if (gy > 65535) return PS_ERR_INVALID;
+  if (nrings > 65535) return PS_ERR_INVALID;
   const size_t smem = size_t(work_len) * G * sizeof(double2);
   if (smem > 48 * 1024) {
     if (cudaFuncSetAttribute(ring_synth_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -289,7 +291,7 @@ int launch_ring_synth_f64(const Plan& P, const int* d_list, int nrings, int work
   int twlog = 0;
   while ((1 << twlog) < P.max_fft) ++twlog;
   StatScope sc(PS_K_FFT_SYNTH, 0.0, 0.0, st);
-  ring_synth_f64<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, P.R, phase, map, P.mmax, nf, P.npix,
+  ring_synth_f64<<<dim3(gy, nrings), T * G, smem, st>>>(P.d_rings, d_list, P.R, phase, map, P.mmax, nf, P.npix,
                                                          P.d_twiddle, twlog, P.d_bs_spec, P.d_bs_off, T, pack);
   PS_LAUNCH_CHECK();
   return PS_OK;
@@ -300,7 +302,7 @@ int launch_ring_adjoint_f64(const Plan& P, const int* d_list, int nrings, int wo
   if (nrings == 0) return PS_OK;
   int T, G, gy;
   fft_shape_d(work_len, nf, pack, T, G, gy);
-  if (gy > 65535) return PS_ERR_INVALID;
+  if (nrings > 65535) return PS_ERR_INVALID;
   const size_t smem = size_t(work_len) * G * sizeof(double2);
   if (smem > 48 * 1024) {
     if (cudaFuncSetAttribute(ring_adjoint_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -310,7 +312,7 @@ int launch_ring_adjoint_f64(const Plan& P, const int* d_list, int nrings, int wo
   int twlog = 0;
   while ((1 << twlog) < P.max_fft) ++twlog;
   StatScope sc(PS_K_FFT_ADJOINT, 0.0, 0.0, st);
-  ring_adjoint_f64<<<dim3(nrings, gy), T * G, smem, st>>>(P.d_rings, d_list, P.R, map, phase, P.mmax, nf, P.npix,
+  ring_adjoint_f64<<<dim3(gy, nrings), T * G, smem, st>>>(P.d_rings, d_list, P.R, map, phase, P.mmax, nf, P.npix,
                                                            P.d_twiddle, twlog, P.d_bs_spec, P.d_bs_off, T, pack);
   PS_LAUNCH_CHECK();
   return PS_OK;
