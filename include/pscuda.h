@@ -266,10 +266,12 @@ int ps_lm_dot(const double* x, const double* y, const double* w, int batch, int6
  *   (nmap > 440).
  * ps_bispec_pair_products: out[k] (planar [2][npix]) = Sum_{t = ptr[k]}^{ptr[k+1]-1}
  *   s_t op_t(A[a_t]) B[b_t], prods[t] = {a_t, b_t, flags_t}: flags bit 0 conjugates A,
- *   bit 1 negates the term -- the products of H maps whose spin-2 and spin-1
- *   adjoint transforms make up compute_fisher_contribution's Q3 maps
- *   (bspec_bin.py:496-518; there as to_lm_spin(P, M) with M = conj(P), whose
- *   real-map inputs are (Re P, Im P)).  nout <= 65535.
+ *   bit 1 negates the term, bits 2-7 hold its multiplicity (0 meaning 1) -- the
+ *   products of H maps whose spin-2 and spin-1 adjoint transforms make up
+ *   compute_fisher_contribution's Q3 maps (bspec_bin.py:496-518; there as
+ *   to_lm_spin(P, M) with M = conj(P), whose real-map inputs are (Re P, Im P)) and
+ *   the trispectrum's A and (H A) fields (tspec_bin.py:244-277, 685-730).
+ *   nout <= 65535.
  * ps_bispec_assemble_q: out[r][u][lm] (complex128 [nrow][nfield][nlm]) =
  *   scale[u][lm] Sum_c coef[c] V_c(lm) over the contributions c of row r
  *   (row_ptr [nrow+1]; contrib [n][4] int32 = pair, field, l-bin, which) whose field
@@ -278,7 +280,8 @@ int ps_lm_dot(const double* x, const double* y, const double* w, int batch, int6
  *   complex128 hold the (G, C) outputs of the pair's spin-2 and spin-1 adjoints.
  *   The Q3 rows of bspec_bin.py:520-547 (both parities), times the m weights
  *   (S^-1 weighting, :554) or the beam (input of the A^-1 branch, :552).  scale may
- *   be NULL (1); nrow <= 65535. */
+ *   be NULL (1); A2 may be NULL (V = conj(G1) or conj(C1): the Q4 rows of
+ *   tspec_bin.py:732-773); nrow <= 65535. */
 int ps_bispec_triplet_sums_workspace_bytes(int nmap, int64_t npix, int nout, size_t* bytes);
 int ps_bispec_triplet_sums(const double* maps, int nmap, int64_t npix, const int* term_ptr, const int* terms,
                            int nout, double* out, void* workspace, size_t workspace_bytes, cudaStream_t stream);

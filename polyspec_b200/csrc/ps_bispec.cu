@@ -10,7 +10,8 @@
 //    lanes own pixels, so shared-memory reads are conflict-free.  Per-CTA partials
 //    are added in a fixed order by a second kernel.
 //  * ps_bispec_pair_products: out[k] = Sum_t s_t op_t(A[a_t]) B[b_t] (op = identity
-//    or complex conjugate), written as planar [2][npix] real maps -- the inputs of
+//    or complex conjugate, s_t a signed small integer), written as planar [2][npix]
+//    real maps -- the inputs of
 //    the spin-2 and spin-1 adjoint transforms of the H-map products of
 //    compute_fisher_contribution (bspec_bin.py:496-518).
 //  * ps_bispec_assemble_q: the Q3 rows of compute_fisher_contribution
@@ -156,7 +157,8 @@ __global__ void pair_products_kernel(const double* __restrict__ A, int nA, const
       const double2 br = __ldg(reinterpret_cast<const double2*>(B + (2 * int64_t(b)) * npix) + q);
       const double2 bi = __ldg(reinterpret_cast<const double2*>(B + (2 * int64_t(b) + 1) * npix) + q);
       if (f & 1) { ai.x = -ai.x; ai.y = -ai.y; }
-      const double s = (f & 2) ? -1.0 : 1.0;
+      const int mult = (f >> 2) & 63;  // term multiplicity (0 means 1)
+      const double s = ((f & 2) ? -1.0 : 1.0) * double(mult ? mult : 1);
       re.x = fma(s, ar.x * br.x - ai.x * bi.x, re.x);
       re.y = fma(s, ar.y * br.y - ai.y * bi.y, re.y);
       im.x = fma(s, ar.x * bi.x + ai.x * br.x, im.x);
@@ -188,7 +190,7 @@ __global__ void assemble_q_kernel(const double2* __restrict__ A2, const double2*
         if (unsigned(b) >= unsigned(nbins) || unsigned(kk) >= unsigned(npair) || unsigned(which) > 1u) continue;
         if (l < __ldg(edges + b) || l >= __ldg(edges + b + 1)) continue;
         const int64_t k = kk;
-        const double2 v2 = __ldg(A2 + (2 * k + which) * nlm + i);
+        const double2 v2 = A2 ? __ldg(A2 + (2 * k + which) * nlm + i) : make_double2(0.0, 0.0);
         const double2 v1 = __ldg(A1 + (2 * k + which) * nlm + i);
         const double w = __ldg(coef + c);
         if (which == 0) {  // conj(G1) - conj(G2)
@@ -282,7 +284,7 @@ extern "C" int ps_bispec_assemble_q(const double* A2, const double* A1, int npai
                                     const int* contrib, const double* coef, int nrow, int nfield,
                                     const double* scale, double* out, cudaStream_t stream) {
   if (nrow == 0) return PS_OK;
-  if (!A2 || !A1 || !l_of_lm || !edges || !row_ptr || !contrib || !coef || !out || npair <= 0 || nlm <= 0 ||
+  if (!A1 || !l_of_lm || !edges || !row_ptr || !contrib || !coef || !out || npair <= 0 || nlm <= 0 ||
       nbins <= 0 || nrow < 0 || nfield < 1 || nfield > 3 || nrow > 65535)
     return PS_ERR_INVALID;
   StatScope sc(PS_K_VECTOR, 0.0, double(nrow) * nfield * 16.0 * nlm, stream);

@@ -142,8 +142,8 @@ class CutPreconditioner:
         B, nc = alm.shape[0], alm.shape[1]
         out = torch.empty((self.Rb, self.M, B, nc), dtype=torch.complex128, device=alm.device)
         ws, nb = self._ws(B, spin, 0)
-        _lib.call("ps_legendre_synthesis", self._use, _vp(alm.contiguous()), _vp(out), B, spin, _vp(ws), nb,
-                  _stream())
+        alm = alm.contiguous()  # held until the launch
+        _lib.call("ps_legendre_synthesis", self._use, _vp(alm), _vp(out), B, spin, _vp(ws), nb, _stream())
         return out
 
     def adjoint(self, phase, spin):
@@ -151,8 +151,8 @@ class CutPreconditioner:
         B, nc = phase.shape[2], phase.shape[3]
         out = torch.empty((B, nc, self.nalm), dtype=torch.complex128, device=phase.device)
         ws, nb = self._ws(B, spin, 1)
-        _lib.call("ps_legendre_adjoint", self._use, _vp(phase.contiguous()), _vp(out), B, spin, 1.0, _vp(ws), nb,
-                  _stream())
+        phase = phase.contiguous()  # held until the launch
+        _lib.call("ps_legendre_adjoint", self._use, _vp(phase), _vp(out), B, spin, 1.0, _vp(ws), nb, _stream())
         return out
 
     def _to_band(self, alm):
