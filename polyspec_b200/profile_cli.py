@@ -25,6 +25,12 @@ map2alm (seeded), grouped and replayed as one CUDA graph; prints maps/s
 one binned-bispectrum Fisher contribution (T+E, log bins, both parities, ideal
 S^-1 filter) per precision: device time, kernel time per kind, the numerator
 with two simulations, and the mixed-vs-FP64 Fisher difference.
+
+    python -m polyspec_b200.profile_cli tspecbin [--nside 128 --lmax 255 --nbins 6]
+    python -m polyspec_b200.profile_cli tspec [--nside 512 --lmax 1000 --nr 24]
+
+the binned trispectrum (T+E) and the template trispectrum (gNL-loc, lensing,
+point source): Fisher contribution and numerator times, FP64 and mixed.
 """
 import argparse
 import sys
@@ -235,6 +241,48 @@ def tspec(a):
         print("tspec mixed vs fp64 Fisher: max |dF| / sqrt(F_ii F_jj) %.2e" % (np.abs(G - F) / d).max())
 
 
+def tspecbin(a):
+    """Binned-trispectrum numerator and Fisher contribution (T+E, log bins, ideal filter)."""
+    import numpy as np
+    from polyspec_b200 import PolySpec, Weightings, _lib
+    from polyspec_b200 import workloads as W
+    from polyspec_b200.tspec_bin import TSpecBin
+    cltot, cl, beam, mask, l_bins, _ = W.bispec_setup(a.nside, a.lmax, a.nbins)
+    fields = ['TTTT', 'TTTE', 'TTEE', 'TETE', 'TEEE', 'EEEE']
+    res = {}
+    for prec in a.precs.split(","):
+        base = PolySpec(a.nside, dict(cltot), beam=list(beam), pol=True, lmax=a.lmax, prec=prec)
+        wts = Weightings(base, np.stack([mask] * 3), dict(cl), noise_cov=W.white_noise_cov(a.nside))
+        t = TSpecBin(base, mask, wts.make_applySinv('ideal'), l_bins, fields=fields, parity='both')
+        t._compute_symmetry_factor()
+        a_lms = [base.generate_data(seed=11 + i, deconvolve_beam=True, output_type='harmonic', rng='device')
+                 for i in range(2)]
+        t.compute_fisher_contribution(0, a_lms=a_lms)  # warm-up
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        f = t.compute_fisher_contribution(0, a_lms=a_lms)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_f = e0.elapsed_time(e1)
+        res[prec] = f
+        data = base.to_map(base.generate_data(seed=3, output_type='harmonic', rng='device'))
+        t.generate_sims(1)
+        t.Tl_numerator(data)
+        e0.record()
+        t.Tl_numerator(data)
+        e1.record()
+        torch.cuda.synchronize()
+        print("tspecbin %s: Nside %d lmax %d, %d bins, N_t %d, %d A pairs: Fisher contribution %.1f ms; numerator "
+              "(1 sim pair, t0 cached) %.1f ms" % (prec, a.nside, a.lmax, len(l_bins) - 1, t.N_t,
+                                                   t._tables['npair'], ms_f, e0.elapsed_time(e1)), flush=True)
+        del t, wts, base
+        torch.cuda.empty_cache()
+    if "fp64" in res and "mixed" in res:
+        F, G = res["fp64"], res["mixed"]
+        d = np.sqrt(np.abs(np.outer(np.diag(F), np.diag(F))))
+        print("tspecbin mixed vs fp64 Fisher: max |dF| / sqrt(F_ii F_jj) %.2e" % (np.abs(G - F) / d).max())
+
+
 def main(argv=None):
     p = argparse.ArgumentParser()
     sub = p.add_subparsers(dest="cmd", required=True)
@@ -265,8 +313,15 @@ def main(argv=None):
     t.add_argument("--nr", type=int, default=24)
     t.add_argument("--reps", type=int, default=2)
     t.add_argument("--precs", default="fp64,mixed")
+    tb = sub.add_parser("tspecbin")
+    tb.add_argument("--nside", type=int, default=128)
+    tb.add_argument("--lmax", type=int, default=255)
+    tb.add_argument("--nbins", type=int, default=6)
+    tb.add_argument("--precs", default="fp64,mixed")
     a = p.parse_args(argv)
-    if a.cmd == "tspec":
+    if a.cmd == "tspecbin":
+        tspecbin(a)
+    elif a.cmd == "tspec":
         tspec(a)
     elif a.cmd == "bspec":
         bspec(a)
