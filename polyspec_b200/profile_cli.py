@@ -265,6 +265,13 @@ def tspecbin(a):
         torch.cuda.synchronize()
         ms_f = e0.elapsed_time(e1)
         res[prec] = f
+        _lib.call("ps_stats_reset")
+        _lib.call("ps_stats_enable_timing", 1)
+        t.compute_fisher_contribution(0, a_lms=a_lms)
+        torch.cuda.synchronize()
+        _lib.call("ps_stats_enable_timing", 0)
+        st = {k: _lib.stats(k) for k in _lib.KERNEL_KINDS}
+        print("tspecbin %s kernel ms: %s" % (prec, ", ".join("%s %.1f" % (k, v[1]) for k, v in st.items() if v[0])))
         data = base.to_map(base.generate_data(seed=3, output_type='harmonic', rng='device'))
         t.generate_sims(1)
         t.Tl_numerator(data)

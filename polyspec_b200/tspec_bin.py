@@ -460,52 +460,24 @@ class TSpecBin:
             U = [b.applyAinv(a, input_type='harmonic') for a in a_lms]
         P1, P2 = self._P(U[0]), self._P(U[1])
         GC = [self._A(P1), self._A(P2), self._A(P1, P2)]  # A variants 11, 22, 12
-        q = T['quads']
-        nq, nH = len(q), T['nH']
-        hid = T['hid']
-        # (pair, L) combinations and their binned A maps: spin-2 synthesis of (G bin_L, -C bin_L)
-        pl_index = {}
-        for k in range(nq):
-            for pr in (T['pA'][k], T['pB'][k]):
-                pl_index.setdefault((int(pr), int(q[k, 8])), len(pl_index))
-        pls = sorted(pl_index.items(), key=lambda kv: kv[1])
-        npl = len(pls)
-        x = torch.empty((3 * npl, 2, P.nalm), dtype=torch.complex128, device=dev)
-        for (pr, L), i in pls:
-            for v in range(3):
-                x[3 * i + v, 0] = GC[v][pr, 0] * self.d_ell_bins[L]
-                x[3 * i + v, 1] = -GC[v][pr, 1] * self.d_ell_bins[L]
-        Ap = P.synthesis(x, 2)
+        F = self._fisher_tables()
+        nH, npl = T['nH'], F['npl']
+        # binned A maps of every (pair, L): spin-2 synthesis of (G bin_L, -C bin_L), variants 11, 22, 12
+        bl = self.d_ell_bins[F['pl_L']]                                  # [npl, nlm]
+        x = torch.empty((npl, 3, 2, P.nalm), dtype=torch.complex128, device=dev)
+        for v in range(3):
+            x[:, v, 0] = GC[v][F['pl_pair'], 0] * bl
+            x[:, v, 1] = -GC[v][F['pl_pair'], 1] * bl
+        Ap = P.synthesis(x.reshape(3 * npl, 2, P.nalm), 2)
         b.n_SHTs_reverse += 3 * npl
-        del x, GC
+        del x, GC, bl
         Hs = torch.cat([P1, P2]).contiguous()
         nf = len(self.d_beam)
         sc = self.d_mw[None].expand(nf, P.nalm).contiguous() if weighting == 'Sinv' else self.d_beam.contiguous()
         scale = np.pi / (3. * b.Nside ** 2)
         Q4 = []
         for tau in range(4):
-            keys, contrib, coef = {}, [], []
-            for ci, chi in enumerate(self.chi_arr):
-                for k in range(nq):
-                    u1, u2, u3, u4, b1, b2, b3, b4, L, p_u = (int(v) for v in q[k])
-                    row = ci * nq + k
-                    which = 0 if p_u * chi == 1 else 1
-                    c = 2.0 / self.sym_factor[row]
-                    for pr, f, bn, pu, pb in ((T['pA'][k], u3, b3, u4, b4), (T['pA'][k], u4, b4, u3, b3),
-                                              (T['pB'][k], u1, b1, u2, b2), (T['pB'][k], u2, b2, u1, b1)):
-                        key = (pl_index[(int(pr), L)], hid(pu, pb))
-                        if key not in keys:
-                            keys[key] = len(keys)
-                        contrib.append((keys[key], f, bn, which))
-                        coef.append(c)
-            prods, ptr = [], [0]
-            for (pli, item), _ in sorted(keys.items(), key=lambda kv: kv[1]):
-                for mult, hset, var in _Q_TERMS[tau]:
-                    prods.append((hset * nH + item, 3 * pli + var, 1 | 2 | (mult << 2)))  # -mult conj(P) A+
-                ptr.append(len(prods))
-            nkey = len(keys)
-            i32 = lambda a: torch.as_tensor(np.ascontiguousarray(np.asarray(a, dtype=np.int32)), device=dev)
-            d_ptr, d_prods = i32(ptr), i32(np.asarray(prods).reshape(-1, 3))
+            nkey, d_ptr, d_prods = F['nkey'], F['ptrs'][F['nterm'][tau]], F['prods'][tau]
             HA = torch.empty((nkey, 2, P.nalm), dtype=torch.complex128, device=dev)
             chunk = max(1, min(nkey, int(2 ** 31 // (16 * b.Npix))))
             for k0 in range(0, nkey, chunk):
@@ -513,19 +485,66 @@ class TSpecBin:
                 HA[k0:k0 + n] = P.adjoint(self._products(Hs, 2 * nH, Ap, 3 * npl, d_ptr, d_prods, n, k0), 1, scale)
             b.n_SHTs_forward += nkey
             Q = torch.empty((len(self.sym_factor), nf, P.nalm), dtype=torch.complex128, device=dev)
-            # the index tables must stay referenced until the launch (a temporary's memory could
-            # be handed to the next table before the kernel reads it)
-            d_rows = i32(4 * np.arange(len(self.sym_factor) + 1))
-            d_contrib = i32(np.asarray(contrib).reshape(-1, 4))
-            d_coef = torch.as_tensor(np.asarray(coef, dtype=np.float64), device=dev)
             _lib.call("ps_bispec_assemble_q", None, _vp(HA), nkey, P.nalm, _vp(T['l_of_lm']), _vp(T['edges']),
-                      self.Nl_squeeze, _vp(d_rows), _vp(d_contrib), _vp(d_coef), len(self.sym_factor), nf,
+                      self.Nl_squeeze, _vp(F['rows']), _vp(F['contrib']), _vp(F['coef']), len(self.sym_factor), nf,
                       _vp(sc), _vp(Q), _stream())
-            del HA, d_rows, d_contrib, d_coef
+            del HA
             if weighting == 'Ainv':
                 Q = self._filter_rows(Q)
             Q4.append(Q.reshape(len(self.sym_factor), -1))
         return torch.stack(Q4)
+
+    def _fisher_tables(self):
+        """Index tables of the Fisher contribution, which depend on the binning only: the
+        (pair, L) list of binned A maps, the (H A) fields (one per (pair, L) and partner
+        H map) with the pair-product terms of each Q type, and the four contributions of
+        every Q4 row (tspec_bin.py:641-773)."""
+        T = self._build_tables()
+        if 'fisher' in T:
+            return T['fisher']
+        dev = self.base.device
+        q = T['quads']
+        nq, nH, hid = len(q), T['nH'], T['hid']
+        pl_index = {}
+        for k in range(nq):
+            for pr in (T['pA'][k], T['pB'][k]):
+                pl_index.setdefault((int(pr), int(q[k, 8])), len(pl_index))
+        pls = sorted(pl_index.items(), key=lambda kv: kv[1])
+        keys, contrib, coef = {}, [], []
+        for ci, chi in enumerate(self.chi_arr):
+            for k in range(nq):
+                u1, u2, u3, u4, b1, b2, b3, b4, L, p_u = (int(v) for v in q[k])
+                row = ci * nq + k
+                which = 0 if p_u * chi == 1 else 1
+                c = 2.0 / self.sym_factor[row]
+                for pr, f, bn, pu, pb in ((T['pA'][k], u3, b3, u4, b4), (T['pA'][k], u4, b4, u3, b3),
+                                          (T['pB'][k], u1, b1, u2, b2), (T['pB'][k], u2, b2, u1, b1)):
+                    key = (pl_index[(int(pr), L)], hid(pu, pb))
+                    if key not in keys:
+                        keys[key] = len(keys)
+                    contrib.append((keys[key], f, bn, which))
+                    coef.append(c)
+        i32 = lambda a: torch.as_tensor(np.ascontiguousarray(np.asarray(a, dtype=np.int32)), device=dev)
+        ordered = sorted(keys.items(), key=lambda kv: kv[1])
+        prods = []
+        for tau in range(4):
+            pt = []
+            for (pli, item), _ in ordered:
+                for mult, hset, var in _Q_TERMS[tau]:
+                    pt.append((hset * nH + item, 3 * pli + var, 1 | 2 | (mult << 2)))  # -mult conj(P) A+
+            prods.append(i32(np.asarray(pt).reshape(-1, 3)))
+        nterm = [len(_Q_TERMS[tau]) for tau in range(4)]
+        F = dict(npl=len(pls), nkey=len(keys),
+                 pl_pair=torch.as_tensor([pr for (pr, L), _ in pls], device=dev),
+                 pl_L=torch.as_tensor([L for (pr, L), _ in pls], device=dev),
+                 prods=prods, rows=i32(4 * np.arange(len(self.sym_factor) + 1)),
+                 contrib=i32(np.asarray(contrib).reshape(-1, 4)),
+                 coef=torch.as_tensor(np.asarray(coef, dtype=np.float64), device=dev))
+        # term pointers per Q type (1 or 2 terms per (H A) field)
+        F['ptrs'] = {n: i32(n * np.arange(len(keys) + 1)) for n in set(nterm)}
+        F['nterm'] = nterm
+        T['fisher'] = F
+        return F
 
     def _filter_rows(self, Qb):
         """S^-1 P of beam-weighted rows [R, nfield, nlm] (tspec_bin.py:776-787)."""
