@@ -295,15 +295,18 @@ int ps_bispec_assemble_q(const double* A2, const double* A1, int npair, int64_t 
  * ps_kint_bessel_table: out[l - lmin][ix] = j_l(x[ix]) for l in [lmin, lmax] (polyspec/cython/
  *   k_integrals.pyx:28-71: x = 0 -> delta_l0; x > 18000 + lmax -> sin(x - l pi/2)/x; zero above the
  *   largest l whose small-x limit exceeds 1e-150).  x [nx] float64 device array.
- * ps_kint_radial: out[l][X][r] += (-1)^l Sum_k (k_i - k_{i-1}) (f_{i-1} + f_i) for l in [lmin, lmax],
- *   X < npol, r < nr, with f_i = kprod[i] T[X][l][i] j_{l+nshift}(k_i r[r]) and j linearly interpolated
- *   from table (rows tab_lmin .. tab_lmin + tab_nl - 1, on the grid x, which must start at 0, increase,
- *   and reach beyond every k r) -- q_integral and p_integral of k_integrals.pyx:262-353 (kprod = k^2/pi
- *   for q, k^2 P_zeta(k)/pi for p).  T is [npol][nl_T][nk]; out is [*][npol_out][nr]. */
+ * ps_kint_radial: out[l][X][r] += w_l Sum_k (k_i - k_{i-1}) (f_{i-1} + f_i) for l in [lmin, lmax],
+ *   X < npol, r < nr, with f_i = kprod[r kstride + i] T[X][l][i] J(k_i r[r]), w_l = (-1)^l (times
+ *   sqrt(l(l+1)) if lweight), J = j_{l+nshift} (deriv 0) or (l j_{l-1} - (l+1) j_{l+1})/(2l+1)
+ *   (deriv 1), each j linearly interpolated from table (rows tab_lmin .. tab_lmin + tab_nl - 1, on the
+ *   grid x, which must start at 0, increase, and reach beyond every k r) -- the q, p, r, a, b and c
+ *   integrals of k_integrals.pyx:112-396.  kstride is 0 (one kprod[nk] for all r) or nk (kprod[nr][nk]);
+ *   T is [npol][nl_T][nk]; out is [*][npol_out][nr]. */
 int ps_kint_bessel_table(const double* x, int64_t nx, int lmin, int lmax, double* out, cudaStream_t stream);
 int ps_kint_radial(const double* table, const double* x, int64_t nx, int tab_lmin, int tab_nl, const double* k_arr,
-                   int nk, const double* kprod, const double* T, int npol, int nl_T, const double* r_arr, int nr,
-                   int lmin, int lmax, int nshift, int npol_out, double* out, cudaStream_t stream);
+                   int nk, const double* kprod, int kstride, const double* T, int npol, int nl_T,
+                   const double* r_arr, int nr, int lmin, int lmax, int nshift, int deriv, int lweight, int npol_out,
+                   double* out, cudaStream_t stream);
 
 /* ------------------------------------------------------------- launch statistics
  * No reference counterpart beyond its wall-clock SHT timer (polyspec/base.py:113-127,

@@ -12,8 +12,14 @@ Restated (same grids, branches and trapezium rule, vectorised):
   * interpolate_jlkr      :84-110  linear interpolation of the table to k r;
   * q_integral            :312-353 q_l^X(r) = (-1)^l Sum_k dk (f_k + f_k+1),
                           f = (2/pi) k^2 / 2 T_l^X(k) j_l(kr);
-  * p_integral            :262-310 the same with P_zeta(k) in f and j_{l+n}.
-The other integrals (a, b, c, r, collider, F) raise NotImplementedError.
+  * p_integral            :262-310 the same with P_zeta(k) in f and j_{l+n};
+  * r_integral            :355-396 f = (2/pi) k^2 / 2 P_zeta(k)^(3/4) T_l^X(k) j_l(kr);
+  * compute_jl_prime      :112-124 j_l' = (l j_{l-1} - (l+1) j_{l+1}) / (2l+1);
+  * a_integral            :127-170 f = (2/pi) k^(13/4) P_zeta^(3/4) / 2 e^(k tau) T j_l(kr);
+  * b_integral            :172-215 f = (2/pi) k^(9/4) P_zeta^(3/4) / 2 (1 - k tau) e^(k tau) T j_l'(kr);
+  * c_integral            :217-260 f = (2/pi) k^(5/4) P_zeta^(3/4) / 2 (1 - k tau) e^(k tau) / r
+                          T j_l(kr), the sum weighted by sqrt(l (l+1)).
+The collider and F integrals raise NotImplementedError.
 """
 import numpy as np
 from scipy.special import spherical_jn
@@ -93,9 +99,59 @@ def p_integral(k_arr, Pzeta_arr, Tl_arr, jlkr_all, lmin, lmax, arr_lmin, arr_lma
                                                                  jlkr_all[lshift2 + il], k_arr)
 
 
+def r_integral(k_arr, Pzeta_arr, Tl_arr, jlkr, lmin, lmax, nthreads, integs):
+    k_arr = np.asarray(k_arr)
+    kprod = 2. / np.pi * k_arr * k_arr / 2. * np.asarray(Pzeta_arr) ** (3. / 4.)
+    for il in range(lmax + 1 - lmin):
+        l = lmin + il
+        for X in range(len(Tl_arr)):
+            integs[l, X, :] += (-1.) ** l * _trapz(kprod, np.asarray(Tl_arr)[X, l][None], jlkr[il], k_arr)
+
+
+def compute_jl_prime(lmin, lmax, lmin_base, lmax_base, jls, nthreads):
+    jls = np.asarray(jls)
+    out = np.zeros((lmax_base - lmin_base + 1,) + jls.shape[1:])
+    for l in range(lmin_base, lmax_base + 1):
+        out[l - lmin_base] = (l * jls[l - lmin - 1] - (l + 1.) * jls[l - lmin + 1]) / (2. * l + 1.)
+    return out
+
+
+def _ktau(k_arr, tau_arr, Pzeta_arr, kpow, damped, r_arr=None):
+    """[ntau, nk] k- and tau-dependent factor of the a, b, c integrands."""
+    k_arr, tau = np.asarray(k_arr), np.asarray(tau_arr)
+    kpref = 2. / np.pi * k_arr ** kpow * np.asarray(Pzeta_arr) ** (3. / 4.) / 2.
+    kt = k_arr[None, :] * tau[:, None]
+    out = kpref[None, :] * (1. - kt) * np.exp(kt) if damped else kpref[None, :] * np.exp(kt)
+    if r_arr is not None:
+        out = out / np.asarray(r_arr)[:, None]
+    return out
+
+
+def _rtau_integral(k_arr, ktauprod, Tl_arr, jl, lmin, lmax, integs, lweight):
+    for il in range(lmax + 1 - lmin):
+        l = lmin + il
+        pref = (-1.) ** l * (np.sqrt(l * (l + 1.)) if lweight else 1.)
+        for X in range(len(Tl_arr)):
+            integs[l, X, :] += pref * _trapz(ktauprod, np.asarray(Tl_arr)[X, l][None], jl[il], np.asarray(k_arr))
+
+
+def a_integral(k_arr, tau_arr, Pzeta_arr, Tl_arr, jlkrtau, lmin, lmax, nthreads, integs):
+    _rtau_integral(k_arr, _ktau(k_arr, tau_arr, Pzeta_arr, 13. / 4., False), Tl_arr, jlkrtau, lmin, lmax, integs,
+                   False)
+
+
+def b_integral(k_arr, tau_arr, Pzeta_arr, Tl_arr, jlkrtau_prime, lmin, lmax, nthreads, integs):
+    _rtau_integral(k_arr, _ktau(k_arr, tau_arr, Pzeta_arr, 9. / 4., True), Tl_arr, jlkrtau_prime, lmin, lmax,
+                   integs, False)
+
+
+def c_integral(k_arr, r_arr, tau_arr, Pzeta_arr, Tl_arr, jlkrtau, lmin, lmax, nthreads, integs):
+    _rtau_integral(k_arr, _ktau(k_arr, tau_arr, Pzeta_arr, 5. / 4., True, r_arr), Tl_arr, jlkrtau, lmin, lmax,
+                   integs, True)
+
+
 def _missing(*a, **k):
     raise NotImplementedError("this k-space integral is outside the oracle's scope")
 
 
-compute_jl_prime = a_integral = b_integral = c_integral = r_integral = _missing
 collider_p_integral = compute_F_integral = compute_collider_F_integral = _missing

@@ -72,8 +72,8 @@ SIGNATURES = {
     "ps_lm_dot_workspace_bytes": (_c_int, [_c_int, _c_int64, ctypes.POINTER(_c_size_t)]),
     "ps_kint_bessel_table": (_c_int, [_c_void_p, _c_int64, _c_int, _c_int, _c_void_p, _c_void_p]),
     "ps_kint_radial": (_c_int, [_c_void_p, _c_void_p, _c_int64, _c_int, _c_int, _c_void_p, _c_int, _c_void_p,
-                                _c_void_p, _c_int, _c_int, _c_void_p, _c_int, _c_int, _c_int, _c_int, _c_int,
-                                _c_void_p, _c_void_p]),
+                                _c_int, _c_void_p, _c_int, _c_int, _c_void_p, _c_int, _c_int, _c_int, _c_int, _c_int,
+                                _c_int, _c_int, _c_void_p, _c_void_p]),
     "ps_bispec_triplet_sums_workspace_bytes": (_c_int, [_c_int, _c_int64, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_bispec_triplet_sums": (_c_int, [_c_void_p, _c_int, _c_int64, _c_void_p, _c_void_p, _c_int, _c_void_p,
                                         _c_void_p, _c_size_t, _c_void_p]),

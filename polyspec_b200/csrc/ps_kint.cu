@@ -15,8 +15,12 @@
 //    f_i = kprod_i T_l^X(k_i) j_{l+n}(k_i r) with j interpolated linearly from the
 //    table at x = k r (the interval found by bisection: the largest grid point below
 //    k r, as numpy's searchsorted(...) - 1 in the reference) -- q_integral
-//    (:312-353, kprod = k^2/pi) and p_integral (:262-310, kprod = k^2 P_zeta(k)/pi).
-//    One thread per (l, X, r), k summed in order.
+//    (:312-353, kprod = k^2/pi), p_integral (:262-310, kprod = k^2 P_zeta(k)/pi) and
+//    r_integral (:355-396, kprod = k^2 P_zeta^(3/4)/pi); with a per-sample kprod[r][k]
+//    the (r, tau) integrals a (:127-170), b (:172-215, with j_l' = (l j_{l-1} -
+//    (l+1) j_{l+1})/(2l+1) of the interpolated values, as compute_jl_prime :112-124)
+//    and c (:217-260, weighted by sqrt(l(l+1))).  One thread per (l, X, r), k summed
+//    in order.
 #include "ps_common.cuh"
 #include "ps_stats.cuh"
 
@@ -122,19 +126,24 @@ __global__ void bessel_table_kernel(const double* __restrict__ xs, int64_t nx, i
 
 __global__ void kint_radial_kernel(const double* __restrict__ table, const double* __restrict__ xs, int64_t nx,
                                    int tab_lmin, int tab_nl, const double* __restrict__ k_arr, int nk,
-                                   const double* __restrict__ kprod, const double* __restrict__ T, int npol,
-                                   int nl_T, const double* __restrict__ r_arr, int nr, int lmin, int lmax,
-                                   int nshift, int npol_out, double* __restrict__ out) {
+                                   const double* __restrict__ kprod, int kstride, const double* __restrict__ T,
+                                   int npol, int nl_T, const double* __restrict__ r_arr, int nr, int lmin, int lmax,
+                                   int nshift, int deriv, int lweight, int npol_out, double* __restrict__ out) {
   const int64_t total = int64_t(lmax - lmin + 1) * npol * nr;
   for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
     const int ir = int(t % nr);
     const int X = int((t / nr) % npol);
     const int l = lmin + int(t / (int64_t(nr) * npol));
     const int row = l + nshift - tab_lmin;
-    if (row < 0 || row >= tab_nl || l >= nl_T) continue;
+    if (row < deriv || row + deriv >= tab_nl || l >= nl_T) continue;
     const double r = r_arr[ir];
     const double* jl = table + int64_t(row) * nx;
+    const double* jm = jl - nx;  // rows l - 1 and l + 1 (used for j_l')
+    const double* jp = jl + nx;
     const double* Tl = T + (int64_t(X) * nl_T + l) * nk;
+    const double* kp = kprod + int64_t(kstride) * ir;
+    double pref = (l & 1) ? -1.0 : 1.0;
+    if (lweight) pref *= sqrt(double(l) * (l + 1.0));
     double acc = 0.0, flow = 0.0;
     for (int ik = 0; ik < nk; ++ik) {
       const double kr = k_arr[ik] * r;
@@ -147,9 +156,15 @@ __global__ void kint_radial_kernel(const double* __restrict__ table, const doubl
       }
       const double dx = xs[lo + 1] - xs[lo];
       const double xp = (xs[lo + 1] - kr) / dx, xm = (kr - xs[lo]) / dx;
-      const double j = jl[lo] * xp + jl[lo + 1] * xm;
-      const double f = kprod[ik] * Tl[ik] * j;
-      if (ik > 0) acc += (l & 1 ? -1.0 : 1.0) * (k_arr[ik] - k_arr[ik - 1]) * (flow + f);
+      double j;
+      if (deriv) {  // j_l' = (l j_{l-1} - (l+1) j_{l+1}) / (2l+1) of the interpolated values
+        const double a = jm[lo] * xp + jm[lo + 1] * xm, b = jp[lo] * xp + jp[lo + 1] * xm;
+        j = (l * a - (l + 1.0) * b) / (2.0 * l + 1.0);
+      } else {
+        j = jl[lo] * xp + jl[lo + 1] * xm;
+      }
+      const double f = kp[ik] * Tl[ik] * j;
+      if (ik > 0) acc += pref * (k_arr[ik] - k_arr[ik - 1]) * (flow + f);
       flow = f;
     }
     out[(int64_t(l) * npol_out + X) * nr + ir] += acc;
@@ -173,18 +188,20 @@ extern "C" int ps_kint_bessel_table(const double* x, int64_t nx, int lmin, int l
 }
 
 extern "C" int ps_kint_radial(const double* table, const double* x, int64_t nx, int tab_lmin, int tab_nl,
-                              const double* k_arr, int nk, const double* kprod, const double* T, int npol, int nl_T,
-                              const double* r_arr, int nr, int lmin, int lmax, int nshift, int npol_out, double* out,
-                              cudaStream_t stream) {
+                              const double* k_arr, int nk, const double* kprod, int kstride, const double* T,
+                              int npol, int nl_T, const double* r_arr, int nr, int lmin, int lmax, int nshift,
+                              int deriv, int lweight, int npol_out, double* out, cudaStream_t stream) {
   if (!table || !x || !k_arr || !kprod || !T || !r_arr || !out || nx < 2 || tab_nl <= 0 || nk <= 0 || npol <= 0 ||
-      nr <= 0 || lmin < 0 || lmax < lmin || npol_out < npol || nl_T <= 0)
+      nr <= 0 || lmin < 0 || lmax < lmin || npol_out < npol || nl_T <= 0 || (kstride != 0 && kstride != nk) ||
+      deriv < 0 || deriv > 1)
     return PS_ERR_INVALID;
   const int64_t total = int64_t(lmax - lmin + 1) * npol * nr;
   StatScope sc(PS_K_VECTOR, 0.0, 8.0 * double(total) * nk, stream);
   int64_t g = (total + 127) / 128;
   if (g > 65535) g = 65535;
-  kint_radial_kernel<<<int(g), 128, 0, stream>>>(table, x, nx, tab_lmin, tab_nl, k_arr, nk, kprod, T, npol, nl_T,
-                                                 r_arr, nr, lmin, lmax, nshift, npol_out, out);
+  kint_radial_kernel<<<int(g), 128, 0, stream>>>(table, x, nx, tab_lmin, tab_nl, k_arr, nk, kprod, kstride, T,
+                                                 npol, nl_T, r_arr, nr, lmin, lmax, nshift, deriv, lweight,
+                                                 npol_out, out);
   PS_LAUNCH_CHECK();
   return PS_OK;
 }

@@ -1,14 +1,16 @@
 """Template trispectrum estimator on the GPU (mirror of polyspec/tspec_template.py)
-for the gNL-loc, lensing and point-source templates.
+for the gNL-loc, gNL-con, EFTI (gNL-dotdot, gNL-dotdel, gNL-deldel), lensing and
+point-source templates.
 
 ``TSpecTemplate(base, mask, applySinv, templates, k_arr, Tl_arr, lmin, lmax, ...)``
 keeps the reference constructor, its checks and attributes (l- and L-ranges and
-filters, ``to_compute``, ``p_inds``, ``qlXs``, ``plLXs``, ``timers``), the
+filters, ``to_compute``, ``p_inds``, ``qlXs``, ``plLXs``, ``rlXs``, ``alXs``,
+``blXs``, ``clXs``, ``timers``), the
 simulation handling (``generate_sims``, ``load_sims``) and the estimator methods
 (``Tl_numerator``, ``compute_fisher_contribution``, ``compute_fisher``,
-``Tl_unwindowed``, ``report_timings``, ``reset_timings``).  Other templates of the
-reference (gNL-con and the EFTI, tauNL and collider shapes) raise
-NotImplementedError, as does the radial-sampling optimiser.
+``Tl_unwindowed``, ``report_timings``, ``reset_timings``).  The reference's tauNL
+and collider templates raise NotImplementedError, as do the radial-sampling
+optimisers.
 
 ``applySinv`` receives and returns CUDA tensors (as for PSpecBin/BSpecBin here);
 one with a ``.batched`` method filters the 4 x n_templates Q rows of the Fisher
@@ -16,16 +18,18 @@ contribution in one batch.  Returned numerators and Fisher matrices are numpy.
 
 Device mapping:
 * k-space integrals (polyspec/tspec_template.py:520-708): the j_l(x) table on the
-  reference's x grid and the q_l^X(r), p_l^X(r) trapezium sums run as the
-  ``ps_kint_*`` kernels (same grid, interpolation and summation order).
+  reference's x grid and the q, p, r (radial) and a, b, c ((r, tau)) trapezium
+  sums run as the ``ps_kint_*`` kernels (same grid, interpolation and summation
+  order; b with j_l' from the interpolated j_{l-1}, j_{l+1}).
 * Filtered maps: ``ps_apply_fl_weights`` then one batched spin-0 synthesis over
-  the radial samples (P and Q maps); the lensing U and V maps are spin 0/1/2/3
-  syntheses; Phi_LM is the lens_phi_sum kernel plus one spin-1 adjoint.
-* Numerators: the radial pixel sums ``gnl_loc(_disc)_sum``; lensing and point
+  the radial samples (P, Q, R, A, B maps; C is spin 1); the lensing U and V maps
+  are spin 0/1/2/3 syntheses; Phi_LM is the lens_phi_sum kernel plus one spin-1
+  adjoint.
+* Numerators: the radial pixel sums ``gnl_*(_disc)_sum``; lensing and point
   source sums are device reductions.
-* Fisher: the ``multiply(_asym)`` products, a batched adjoint over radial samples
-  and ``ps_radial_sum_lm`` for the gNL-loc Q derivatives; spin-1/2/3 adjoints for
-  lensing; the batched S^-1 weighting; ``ps_outer_product``.
+* Fisher: the ``multiply*`` products, a batched spin-0 or spin-1 adjoint over the
+  samples and ``ps_radial_sum_lm`` for the gNL Q derivatives; spin-1/2/3 adjoints
+  for lensing; the batched S^-1 weighting; the Fisher outer product.
 """
 import ctypes
 import time
@@ -35,7 +39,7 @@ import torch
 
 from . import _lib, pixel
 
-SUPPORTED = ['gNL-loc', 'lensing', 'point-source']
+SUPPORTED = ['gNL-loc', 'gNL-con', 'gNL-dotdot', 'gNL-dotdel', 'gNL-deldel', 'lensing', 'point-source']
 
 
 def _vp(t):
@@ -125,7 +129,7 @@ class TSpecTemplate:
         self.r_star = 13882.607764400758 if r_star is None else r_star
         self.r_hor = 14163.032903769747 if r_hor is None else r_hor
 
-        if self.ints_1d:
+        if self.ints_1d or self.ints_2d:
             self.Tl_arr = np.asarray(Tl_arr, dtype=np.float64, order='C')
             if not self.pol:
                 assert len(self.Tl_arr) == 1, "Transfer function should contain only T components"
@@ -152,14 +156,31 @@ class TSpecTemplate:
             print("Reading in precomputed radial integration points")
             assert len(r_values) > 0, "Must supply radial sampling points!"
             for t in templates:
-                if t == 'gNL-loc':
+                if t in self.all_templates_1d:
                     assert t in r_weights.keys(), "Must supply weight for template %s" % t
             self.r_arr = np.asarray(r_values, dtype=np.float64)
             self.N_r = len(self.r_arr)
             self.r_weights = r_weights
         else:
             self.N_r = 0
-        self.N_rtau = 0
+        if len(rtau_values) == 0 and self.ints_2d:
+            print("# No input r/tau sampling points supplied; these can be computed with the "
+                  "optimize_radial_sampling_2d() function\n")
+            self.N_rtau = 0
+        elif self.ints_2d:
+            print("Reading in precomputed r/tau integration points")
+            assert len(rtau_values) > 0 and len(rtau_values[0]) == 2, \
+                "Must supply r/tau sampling points for 2d integrals shapes!"
+            for t in templates:
+                if t in self.all_templates_2d:
+                    assert t in rtau_weights.keys(), "Must supply weight for template %s" % t
+            self.rtau_arr = np.asarray(rtau_values, dtype=np.float64)
+            self.N_rtau = len(self.rtau_arr)
+            assert max(self.rtau_arr[:, 0]) >= 0, "r should be in range (0, inf)"
+            assert max(self.rtau_arr[:, 1]) <= 0, "tau should be in range (-inf, 0)"
+            self.rtau_weights = rtau_weights
+        else:
+            self.N_rtau = 0
 
         dev = base.device
         self._dev = dev
@@ -172,10 +193,12 @@ class TSpecTemplate:
             self.d_mask = self.d_mask[None]
         if 'lensing' in self.templates:
             self.d_Lminfilt_lens = torch.as_tensor(np.nonzero(self.Lminfilt_lens)[0], device=dev)
+        t0 = time.time()
         if self.N_r > 0:
-            t0 = time.time()
-            self._prepare_templates()
-            self.timers['precomputation'] += time.time() - t0
+            self._prepare_templates(self.ints_1d, False, False)
+        if self.N_rtau > 0:
+            self._prepare_templates(False, self.ints_2d, False)
+        self.timers['precomputation'] += time.time() - t0
 
     # ------------------------------------------------------------------ configuration
     def _configure_templates(self, templates, C_phi, C_lens_weight):
@@ -198,6 +221,18 @@ class TSpecTemplate:
         if 'gNL-loc' in templates:
             self.to_compute.append(['q'])
             self.ints_1d = True
+        if 'gNL-con' in templates:
+            self.to_compute.append(['r'])
+            self.ints_1d = True
+        if 'gNL-dotdot' in templates:
+            self.to_compute.append(['a'])
+            self.ints_2d = True
+        if 'gNL-dotdel' in templates:
+            self.to_compute.append(['a', 'b', 'c'])
+            self.ints_2d = True
+        if 'gNL-deldel' in templates:
+            self.to_compute.append(['b', 'c'])
+            self.ints_2d = True
         for t in templates:
             if 'lensing' in t:
                 assert len(C_phi) > 0, "Must supply lensing power spectrum!"
@@ -234,20 +269,29 @@ class TSpecTemplate:
         self.lminfilt = self.base.l_arr[self.base.l_arr <= self.lmax] >= self.lmin
 
     def _prepare_templates(self, ints_1d=True, ints_2d=False, ints_coll=False):
-        """k-space integrals q_l^X(r) and p_l^X(r) on the GPU (polyspec/tspec_template.py:520-708)."""
+        """k-space integrals on the GPU (polyspec/tspec_template.py:520-708): p and q (gNL-loc),
+        r (gNL-con) on the radial samples; a, b, c (the EFTI shapes) on the (r, tau) samples.
+        The j_l(x) table, its x grid, the interpolation to k r and the trapezium rule follow
+        the reference; ``ps_kint_bessel_table`` and ``ps_kint_radial`` do the work."""
         dev = self._dev
         print("N_k: %d" % len(self.k_arr))
-        print("N_r: %d" % self.N_r)
+        if ints_1d:
+            print("N_r: %d" % self.N_r)
+        if ints_2d:
+            print("N_rtau: %d" % self.N_rtau)
         lmax = max([self.lmax + 1, self.lmax + self.nmax])
         lmin = max([min([self.lmin - 1, self.lmin - self.nmax]), 0])
         print("\nPrecomputing Bessel functions")
         k_arr = np.asarray(self.k_arr, dtype=np.float64)
-        max_kr = max(k_arr) * max([0., max(self.r_arr)])
+        max_kr = 0.
+        if ints_1d:
+            max_kr = max(k_arr) * max([max_kr, max(self.r_arr)])
+        if ints_2d:
+            max_kr = max(k_arr) * max([max_kr, self.r_hor + 10000 + 5e6])
         x_arr = list(np.arange(0, lmax * 2, 0.01)) + list(np.arange(lmax * 2, min(max_kr * 1.01, lmax * 100), 0.1))
         if max_kr > 100 * lmax:
             x_arr += list(np.linspace(lmax * 100, max_kr * 1.01, 1000))
         x_arr = np.asarray(x_arr, dtype=np.float64)
-        assert np.max(x_arr) >= np.max(k_arr) * np.max(self.r_arr)
         d_x = torch.as_tensor(x_arr, device=dev)
         nl_tab = lmax - lmin + 1
         table = torch.empty((nl_tab, len(x_arr)), dtype=torch.float64, device=dev)
@@ -259,41 +303,74 @@ class TSpecTemplate:
         npol_out = 1 + 2 * self.pol
         d_k = torch.as_tensor(k_arr, device=dev)
         d_T = torch.as_tensor(np.ascontiguousarray(self.Tl_arr), device=dev)
-        d_r = torch.as_tensor(self.r_arr, device=dev)
         nl_T = self.Tl_arr.shape[1]
-        if len(self.p_inds) > 0:
-            print("Computing p_lL^X(r) integrals")
-            kprod = torch.as_tensor(2. / np.pi * k_arr * k_arr * self.Pzeta(k_arr) / 2., device=dev)
-            plLXs = torch.zeros((2 * self.nmax + 1, lmax + 1, npol_out, self.N_r), dtype=torch.float64, device=dev)
-            for n in range(-max(self.p_inds), max(self.p_inds) + 1):
-                lshift1 = min(0, self.lmin - lmin + n)
-                _lib.call("ps_kint_radial", _vp(table), _vp(d_x), len(x_arr), lmin, nl_tab, _vp(d_k), len(k_arr),
-                          _vp(kprod), _vp(d_T), npol, nl_T, _vp(d_r), self.N_r, self.lmin - lshift1, self.lmax, n,
-                          npol_out, _vp(plLXs[self.nmax + n]), _stream())
-            self.d_plLXs = plLXs
-            self.plLXs = plLXs.cpu().numpy()
-        if 'q' in self.to_compute:
-            print("Computing q_l^X(r) integrals")
-            kprod = torch.as_tensor(2. / np.pi * k_arr * k_arr / 2., device=dev)
-            qlXs = torch.zeros((self.lmax + 1, npol_out, self.N_r), dtype=torch.float64, device=dev)
+        Pz = self.Pzeta(k_arr)
+
+        def integral(kprod, r_arr, out, lo, hi, nshift=0, deriv=0, lweight=0):
+            kp = torch.as_tensor(np.ascontiguousarray(kprod, dtype=np.float64), device=dev)
+            d_r = torch.as_tensor(np.asarray(r_arr, dtype=np.float64), device=dev)
             _lib.call("ps_kint_radial", _vp(table), _vp(d_x), len(x_arr), lmin, nl_tab, _vp(d_k), len(k_arr),
-                      _vp(kprod), _vp(d_T), npol, nl_T, _vp(d_r), self.N_r, self.lmin, self.lmax, 0, npol_out,
-                      _vp(qlXs), _stream())
-            self.d_qlXs = qlXs
-            self.qlXs = qlXs.cpu().numpy()
+                      _vp(kp), 0 if kp.dim() == 1 else len(k_arr), _vp(d_T), npol, nl_T, _vp(d_r), len(r_arr),
+                      lo, hi, nshift, deriv, lweight, npol_out, _vp(out), _stream())
+            torch.cuda.current_stream().synchronize()  # kp, d_r are released on return
+
+        if ints_1d:
+            assert np.max(x_arr) >= np.max(k_arr) * np.max(self.r_arr)
+            if len(self.p_inds) > 0:
+                print("Computing p_lL^X(r) integrals")
+                plLXs = torch.zeros((2 * self.nmax + 1, lmax + 1, npol_out, self.N_r), dtype=torch.float64,
+                                    device=dev)
+                for n in range(-max(self.p_inds), max(self.p_inds) + 1):
+                    lshift1 = min(0, self.lmin - lmin + n)
+                    integral(2. / np.pi * k_arr * k_arr * Pz / 2., self.r_arr, plLXs[self.nmax + n],
+                             self.lmin - lshift1, self.lmax, nshift=n)
+                self.d_plLXs = plLXs
+                self.plLXs = plLXs.cpu().numpy()
+            if 'q' in self.to_compute:
+                print("Computing q_l^X(r) integrals")
+                qlXs = torch.zeros((self.lmax + 1, npol_out, self.N_r), dtype=torch.float64, device=dev)
+                integral(2. / np.pi * k_arr * k_arr / 2., self.r_arr, qlXs, self.lmin, self.lmax)
+                self.d_qlXs = qlXs
+                self.qlXs = qlXs.cpu().numpy()
+            if 'r' in self.to_compute:
+                print("Computing r_l^X(r) integrals")
+                rlXs = torch.zeros((self.lmax + 1, npol_out, self.N_r), dtype=torch.float64, device=dev)
+                integral(2. / np.pi * k_arr * k_arr / 2. * Pz ** (3. / 4.), self.r_arr, rlXs, self.lmin, self.lmax)
+                self.d_rlXs = rlXs
+                self.rlXs = rlXs.cpu().numpy()
+        if ints_2d:
+            assert np.max(x_arr) >= np.max(k_arr) * np.max(self.rtau_arr[:, 0])
+            r, tau = self.rtau_arr[:, 0], self.rtau_arr[:, 1]
+            ktau = k_arr[None, :] * tau[:, None]
+            for name, kpow, shape, deriv, lweight, per_r in (('a', 13. / 4., 0, 0, 0, False),
+                                                            ('b', 9. / 4., 1, 1, 0, False),
+                                                            ('c', 5. / 4., 1, 0, 1, True)):
+                if name not in self.to_compute:
+                    continue
+                print("Computing %s_l^X(r, tau) integrals" % name)
+                kpref = 2. / np.pi * k_arr ** kpow * Pz ** (3. / 4.) / 2.
+                kp = kpref[None, :] * (np.exp(ktau) if shape == 0 else (1. - ktau) * np.exp(ktau))
+                if per_r:
+                    kp = kp / r[:, None]
+                out = torch.zeros((self.lmax + 1, npol_out, self.N_rtau), dtype=torch.float64, device=dev)
+                integral(kp, r, out, self.lmin, self.lmax, deriv=deriv, lweight=lweight)
+                setattr(self, 'd_%slXs' % name, out)
+                setattr(self, '%slXs' % name, out.cpu().numpy())
         del table
         self._make_utils()
         print("Precomputation complete")
 
-    def set_radial_integrals(self, qlXs=None, plLXs=None):
-        """Install precomputed q_l^X(r) [lmax+1, 1+2 pol, N_r] and p_lL^X(r)
-        [1, lmax+2, 1+2 pol, N_r] arrays in place of the computed ones."""
-        if qlXs is not None:
-            self.qlXs = np.asarray(qlXs, dtype=np.float64)
-            self.d_qlXs = torch.as_tensor(self.qlXs, device=self._dev)
-        if plLXs is not None:
-            self.plLXs = np.asarray(plLXs, dtype=np.float64)
-            self.d_plLXs = torch.as_tensor(self.plLXs, device=self._dev)
+    def set_radial_integrals(self, qlXs=None, plLXs=None, **arrays):
+        """Install precomputed radial integrals in place of the computed ones: any of
+        qlXs, rlXs [lmax+1, 1+2 pol, N_r], plLXs [2 nmax+1, lmax+2, 1+2 pol, N_r], alXs,
+        blXs, clXs [lmax+1, 1+2 pol, N_rtau] (the reference's attribute names and layouts)."""
+        arrays.update(qlXs=qlXs, plLXs=plLXs)
+        for name, arr in arrays.items():
+            if arr is None:
+                continue
+            a = np.asarray(arr, dtype=np.float64)
+            setattr(self, name, a)
+            setattr(self, 'd_' + name, torch.as_tensor(a, device=self._dev))
 
     def _make_utils(self):
         self.utils = pixel.tauNL_utils(self.base.nthreads, self.N_r, self.base.l_arr.astype(np.int32),
@@ -352,11 +429,14 @@ class TSpecTemplate:
         out[..., self.d_lminfilt] = h_filt
         return out
 
-    def _compute_weighted_maps(self, h_lm_filt, flX_arr):
-        """[Sum_lm Y_lm(i) f_l^X(i) h_lm] maps for each radial sample (polyspec/tspec_template.py:799-815)."""
+    def _compute_weighted_maps(self, h_lm_filt, flX_arr, spin=0):
+        """[Sum_lm {}_sY_lm(i) f_l^X(i) h_lm] maps for each sampling point (polyspec/tspec_template.py:799-815);
+        for spin 1 the (+1) maps of the spin-1 transform of [-summ, 0]."""
         t0 = time.time()
         summ = self._full_lm(self.utils.apply_fl_weights(flX_arr, h_lm_filt, 1.), self.lmax)
-        out = self.base.to_map_vec(summ, output_spin=0, lmax=self.lmax)
+        out = self.base.to_map_vec(summ, output_spin=spin, lmax=self.lmax)
+        if spin != 0:
+            out = out[0]
         self._timed('map_transforms', t0)
         return out
 
@@ -417,10 +497,18 @@ class TSpecTemplate:
     def _apply_all_filters(self, input_map):
         """Filtered maps of one S^-1-weighted field (polyspec/tspec_template.py:1036-1096)."""
         output = {}
+        if 'a' in self.to_compute:
+            output['a'] = self._compute_weighted_maps(input_map, self.d_alXs)
+        if 'b' in self.to_compute:
+            output['b'] = self._compute_weighted_maps(input_map, self.d_blXs)
+        if 'c' in self.to_compute:
+            output['c'] = self._compute_weighted_maps(input_map, self.d_clXs, spin=1)
         if 0 in self.p_inds:
             output['p00'] = self._compute_weighted_gaunt_maps(input_map, self.d_plLXs, 0, 0)
         if 'q' in self.to_compute:
             output['q'] = self._compute_weighted_maps(input_map, self.d_qlXs)
+        if 'r' in self.to_compute:
+            output['r'] = self._compute_weighted_maps(input_map, self.d_rlXs)
         if 'u' in self.to_compute:
             output['u'] = self._compute_lensing_U_map(input_map)
         if 'v' in self.to_compute:
@@ -432,8 +520,11 @@ class TSpecTemplate:
         if filtering == 'P':
             return {0: torch.stack([self._compute_weighted_gaunt_maps(m, self.d_plLXs, 0, 0)[None]
                                     for m in input_maps])}
-        if filtering == 'Q':
-            return torch.stack([self._compute_weighted_maps(m, self.d_qlXs) for m in input_maps])
+        spin0 = {'Q': 'd_qlXs', 'R': 'd_rlXs', 'A': 'd_alXs', 'B': 'd_blXs'}
+        if filtering in spin0:
+            return torch.stack([self._compute_weighted_maps(m, getattr(self, spin0[filtering])) for m in input_maps])
+        if filtering == 'C':
+            return torch.stack([self._compute_weighted_maps(m, self.d_clXs, spin=1) for m in input_maps])
         if filtering == 'U':
             return torch.stack([self._compute_lensing_U_map(m) for m in input_maps])
         if filtering == 'V':
@@ -459,6 +550,12 @@ class TSpecTemplate:
         w = Ls * (Ls + 1.) * (1. + (Ms > 0)) * np.asarray(self.C_phi)[Ls]
         return torch.as_tensor(w, device=self._dev)
 
+    def _check_sampling(self):
+        if self.ints_1d and (not hasattr(self, 'r_arr')):
+            raise Exception("Need to supply radial integration points or run optimize_radial_sampling_1d()!")
+        if self.ints_2d and (not hasattr(self, 'rtau_arr')):
+            raise Exception("Need to supply radial/tau integration points or run optimize_radial_sampling_2d()!")
+
     # ------------------------------------------------------------------ simulations
     def _sinv_filt(self, x, input_type='map'):
         y = self.applySinv(x, input_type=input_type, lmax=self.lmax)
@@ -479,8 +576,7 @@ class TSpecTemplate:
         print("Using %d pairs of Monte Carlo simulations" % self.N_it)
         if preload:
             self.preload = True
-            if self.ints_1d and (not hasattr(self, 'r_arr')):
-                raise Exception("Need to supply radial integration points or run optimize_radial_sampling_1d()!")
+            self._check_sampling()
             self.proc_a_maps, self.proc_b_maps = [], []
             for ii in range(self.N_it):
                 if ii % 5 == 0 and verb:
@@ -517,8 +613,7 @@ class TSpecTemplate:
 
         if preload:
             self.preload = True
-            if self.ints_1d and (not hasattr(self, 'r_arr')):
-                raise Exception("Need to supply radial integration points or run optimize_radial_sampling_1d()!")
+            self._check_sampling()
             self.proc_a_maps, self.proc_b_maps = [], []
             for ii in range(self.N_it):
                 if ii % 5 == 0 and verb:
@@ -536,8 +631,7 @@ class TSpecTemplate:
     def Tl_numerator(self, data, include_disconnected_term=True, verb=False, input_type='map'):
         """Numerator of the unwindowed trispectrum estimator (polyspec/tspec_template.py:1338-1955)."""
         t_start = time.time()
-        if self.ints_1d and (not hasattr(self, 'r_arr')):
-            raise Exception("Need to supply radial integration points or run optimize_radial_sampling_1d()!")
+        self._check_sampling()
         if not hasattr(self, 'preload') and include_disconnected_term:
             raise Exception("Need to generate or specify bias simulations!")
         if self.pol:
@@ -573,6 +667,10 @@ class TSpecTemplate:
                 t4_num[ii] = 9. / 100. * self.utils.gnl_loc_sum(self.r_weights[t], proc_maps['p00'], proc_maps['q']) \
                     * 4. * A_pix * (4. * np.pi) ** 1.5
                 self._timed('gNL_summation', t0)
+            if t in ('gNL-con', 'gNL-dotdot', 'gNL-dotdel', 'gNL-deldel'):
+                t0 = time.time()
+                t4_num[ii] = self._gnl_shape_sum(t, proc_maps) * A_pix
+                self._timed('gNL_summation', t0)
             if t == 'lensing':
                 Phi_dd = self._compute_lensing_Phi(proc_maps, proc_maps)
                 w = self._lens_Ls()
@@ -603,6 +701,12 @@ class TSpecTemplate:
                         t2_num[ii] += -54. / 100. * summ / self.N_it * A_pix * (4. * np.pi) ** 1.5
                         if compute_t0:
                             t0_num[ii] += 54. / 100. * perm(pa, pb) / self.N_it * A_pix * (4. * np.pi) ** 1.5
+                        self._timed('gNL_summation', t0)
+                    if t in ('gNL-con', 'gNL-dotdot', 'gNL-dotdel', 'gNL-deldel'):
+                        t0 = time.time()
+                        t2_num[ii] += -self._gnl_shape_disc(t, proc_maps, pa, pb) / self.N_it * A_pix
+                        if compute_t0:
+                            t0_num[ii] += self._gnl_shape_disc(t, pb, pa) / self.N_it * A_pix
                         self._timed('gNL_summation', t0)
                     if t == 'lensing':
                         w = self._lens_Ls()
@@ -638,14 +742,100 @@ class TSpecTemplate:
             return t4_num + t2_num + t0_num
         return t4_num
 
+    def _gnl_shape_sum(self, t, m):
+        """4-field sums of gNL-con and the EFTI shapes without A_pix (polyspec/tspec_template.py:1394-1420)."""
+        u = self.utils
+        if t == 'gNL-con':
+            return 9. / 25. * u.gnl_con_sum(self.r_weights[t], m['r'])
+        w, tau = self.rtau_weights[t], self.rtau_arr[:, 1]
+        if t == 'gNL-dotdot':
+            return 384. / 25. * u.gnl_dotdot_sum(w, tau, m['a'])
+        if t == 'gNL-dotdel':
+            return 288. / 325. * u.gnl_dotdel_sum(w, tau, m['a'], m['b'], m['c']) * 12
+        return 1728. / 2575. * u.gnl_deldel_sum(w, m['b'], m['c']) * 6
+
+    def _gnl_shape_disc(self, t, d, a, b=None):
+        """Disconnected sums of gNL-con and the EFTI shapes without A_pix (polyspec/tspec_template.py:1582-1660):
+        with b, the 2-field sum over the pairs (d, a) and (d, b) (to be subtracted); without, the
+        0-field sum of the pair (d, a), called with d the second simulation and a the first."""
+        u = self.utils
+        pairs = [(d, a), (d, b)] if b is not None else [(d, a)]
+        summ = 0.
+        if t == 'gNL-con':
+            w = self.r_weights[t]
+            for x, y in pairs:
+                summ += u.gnl_con_disc_sum(w, x['r'], y['r'])
+            return 27. / 25. * summ
+        w, tau = self.rtau_weights[t], self.rtau_arr[:, 1]
+        if t == 'gNL-dotdot':
+            for x, y in pairs:
+                summ += u.gnl_dotdot_disc_sum(w, tau, x['a'], y['a'])
+            return 1152. / 25. * summ
+        if t == 'gNL-dotdel':
+            def perm(m1, m2, m3, m4):
+                return u.gnl_dotdel_disc_sum(w, tau, m1['a'], m2['a'], m3['b'], m4['b'], m3['c'], m4['c'])
+            for x, y in pairs:  # x is the data (or the first simulation), y the simulation
+                summ += 2 * perm(y, y, x, x) + 8 * perm(y, x, y, x) + 2 * perm(x, x, y, y)
+            return 864. / 325. * summ
+
+        def perm(m1, m2, m3, m4):
+            return u.gnl_deldel_disc_sum(w, m1['b'], m2['b'], m3['b'], m4['b'], m1['c'], m2['c'], m3['c'], m4['c'])
+        for x, y in pairs:
+            summ += 2 * perm(y, y, x, x) + 4 * perm(y, x, y, x)
+        return 5184. / 2575. * summ
+
     # ------------------------------------------------------------------ Fisher matrix
-    def _transform_maps(self, map123, flXs, weights):
-        """Sum_i w_i M_LM f^X_L(i) for real maps M [N_r, Npix] (polyspec/tspec_template.py:2575-2588, spin 0)."""
+    def _transform_maps(self, map123, flXs, weights, spin=0):
+        """Sum_i w_i M_LM f^X_L(i) for maps M [N, Npix] (polyspec/tspec_template.py:2575-2588): real maps
+        through a spin-0 adjoint; complex (+1) maps through the spin-1 adjoint of (M, conj M),
+        averaging the +1 and -1 harmonics."""
         t0 = time.time()
-        lm_map = self.base.to_lm_vec(map123, lmax=self.lmax)[:, self.d_lminfilt].contiguous()
-        out = self.utils.radial_sum(lm_map, weights, flXs)
+        if spin == 0:
+            lm_map = self.base.to_lm_vec(map123, lmax=self.lmax)[:, self.d_lminfilt].contiguous()
+            out = self.utils.radial_sum(lm_map, weights, flXs)
+        elif spin == 1:
+            lm_map = self.base.to_lm_vec(torch.stack([map123, map123.conj()]), spin=1, lmax=self.lmax)
+            out = self.utils.radial_sum_spin1(lm_map[:, :, self.d_lminfilt].contiguous(), weights, flXs)
+        else:
+            raise Exception(f"Wrong spin s = {spin}!")
         self._timed('fish_deriv', t0)
         return out
+
+    def _tau_pow(self, n):
+        """tau_i^n over the (r, tau) samples, shaped to scale an [l, X, i] integral array."""
+        return torch.as_tensor(self.rtau_arr[:, 1], device=self._dev)[None, None, :] ** n
+
+    def _dotdel_Q(self, A, B, C, w):
+        """Q-derivative rows (111, 222, 112, 122) of gNL-dotdel (polyspec/tspec_template.py:2768-2801)."""
+        u, tm = self.utils, self._transform_maps
+        t2 = self._tau_pow(2.)
+        fa, fb, fc = self.d_alXs * t2, self.d_blXs * t2, self.d_clXs * t2
+        Q = torch.zeros((4, 1 + 2 * self.pol, len(self.ls)), dtype=torch.complex128, device=self._dev)
+        for k, i in ((0, 0), (1, 1)):
+            Q[k] = 41472. / 325. * tm(u.multiplyCC(A[i], B[i], C[i]), fa, w)
+            Q[k] += 41472. / 325. * tm(u.multiply(A[i], A[i], B[i]), fb, w)
+            Q[k] += 41472. / 325. * tm(u.multiplyC(A[i], A[i], C[i]), fc, w, spin=1)
+        for k, (i, j) in ((2, (0, 1)), (3, (1, 0))):
+            Q[k] = 13824. / 325. * tm(u.multiplyCC_asym(A[i], A[j], B[i], B[j], C[i], C[j]), fa, w)
+            Q[k] += 13824. / 325. * tm(u.multiply_asym(A[i], A[j], B[i], B[j]), fb, w)
+            Q[k] += 13824. / 325. * tm(u.multiplyC_asym(A[i], A[j], C[i], C[j]), fc, w, spin=1)
+        return Q
+
+    def _deldel_Q(self, B, C, w):
+        """Q-derivative rows (111, 222, 112, 122) of gNL-deldel (polyspec/tspec_template.py:2803-2841)."""
+        u, tm = self.utils, self._transform_maps
+        fb, fc = self.d_blXs, self.d_clXs
+        quad = {(0, 0): u.multiply2(B[0], B[0], C[0], C[0]), (0, 1): u.multiply2(B[0], B[1], C[0], C[1]),
+                (1, 1): u.multiply2(B[1], B[1], C[1], C[1])}
+        Q = torch.zeros((4, 1 + 2 * self.pol, len(self.ls)), dtype=torch.complex128, device=self._dev)
+
+        def term(coef, i, q):
+            return coef * tm(u.multiply2R(B[i], q), fb, w) + coef * tm(u.multiply2C(C[i], q), fc, w, spin=1)
+        Q[0] = term(248772. / 2575., 0, quad[0, 0])
+        Q[1] = term(248772. / 2575., 1, quad[1, 1])
+        Q[2] = term(82944. / 2575., 1, quad[0, 0]) + term(165888. / 2575., 0, quad[0, 1])
+        Q[3] = term(82944. / 2575., 0, quad[1, 1]) + term(165888. / 2575., 1, quad[0, 1])
+        return Q
 
     def _weight_Q_maps(self, tmp_Q, weighting='Ainv'):
         """S^-1 P weighting (A^-1 branch) or m weights (S^-1 branch) of Q rows
@@ -745,8 +935,7 @@ class TSpecTemplate:
         ``a_lms`` (two beam-deconvolved harmonic fields) may replace the fields drawn
         from ``seed``."""
         t_start = time.time()
-        if self.ints_1d and (not hasattr(self, 'r_arr')):
-            raise Exception("Need to supply radial integration points or run optimize_radial_sampling_1d()!")
+        self._check_sampling()
         print("Computing Fisher matrix with seed %d" % seed)
         b = self.base
         nt = len(self.templates)
@@ -781,6 +970,14 @@ class TSpecTemplate:
                 self._timed('Ainv', t0)
             if 'q' in self.to_compute:
                 Q_maps = self._filter_pair(U, 'Q')
+            if 'r' in self.to_compute:
+                R_maps = self._filter_pair(U, 'R')
+            if 'a' in self.to_compute:
+                A_maps = self._filter_pair(U, 'A')
+            if 'b' in self.to_compute:
+                B_maps = self._filter_pair(U, 'B')
+            if 'c' in self.to_compute:
+                C_maps = self._filter_pair(U, 'C')
             if 'u' in self.to_compute:
                 U_maps = self._filter_pair(U, 'U')
             if 'v' in self.to_compute:
@@ -805,6 +1002,21 @@ class TSpecTemplate:
                     Qs[3, ii] = 54. / 25. * self._transform_maps(u.multiply_asym(P0[1], P0[0], Q_maps[1], Q_maps[0]),
                                                                  p, w)
                     Qs[3, ii] += 54. / 25. * self._transform_maps(u.multiply(P0[0], P0[1], P0[1]), q, w)
+                if t == 'gNL-con':
+                    w, f = self.r_weights[t], self.d_rlXs
+                    R = R_maps
+                    for k, (i, j, l) in enumerate(((0, 0, 0), (1, 1, 1), (0, 0, 1), (0, 1, 1))):
+                        Qs[k, ii] = 216. / 25. * self._transform_maps(self.utils.multiply(R[i], R[j], R[l]), f, w)
+                if t == 'gNL-dotdot':
+                    w = self.rtau_weights[t]
+                    f = self.d_alXs * self._tau_pow(4)
+                    A = A_maps
+                    for k, (i, j, l) in enumerate(((0, 0, 0), (1, 1, 1), (0, 0, 1), (0, 1, 1))):
+                        Qs[k, ii] = 9216. / 25. * self._transform_maps(self.utils.multiply(A[i], A[j], A[l]), f, w)
+                if t == 'gNL-dotdel':
+                    Qs[:, ii] = self._dotdel_Q(A_maps, B_maps, C_maps, self.rtau_weights[t])
+                if t == 'gNL-deldel':
+                    Qs[:, ii] = self._deldel_Q(B_maps, C_maps, self.rtau_weights[t])
                 if t == 'lensing':
                     Qs[:, ii] += self._lensing_Q(U_maps, V_maps)
                 if t == 'point-source':

@@ -115,8 +115,8 @@ def make(pol, ref):
     return out
 
 
-def main():
-    refroot = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+def load_reference(refroot):
+    """The reference's base, weighting and tspec_template modules over the oracle shims."""
     ref = reference_harness.load(refroot, modules=("base", "weighting"))
     reference_harness.load_cython()
     spec = importlib.util.spec_from_file_location("refpolyspec.tspec_template",
@@ -125,6 +125,12 @@ def main():
     sys.modules["refpolyspec.tspec_template"] = mod
     spec.loader.exec_module(mod)
     ref["tspec_template"] = mod
+    return ref
+
+
+def main():
+    refroot = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = load_reference(refroot)
     for pol in (False, True):
         d = make(pol, ref)
         path = os.path.join(HERE, "tspec_nside16_%s.npz" % ("teb" if pol else "t"))

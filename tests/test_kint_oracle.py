@@ -1,0 +1,60 @@
+"""The oracle's k-space integral restatement (oracle/shims/k_integrals.py) on the
+CPU: j_l' from the recurrence against scipy's derivative, and the (r, tau)
+integrals against the golden fixtures made through the reference."""
+import os
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_jl_prime_recurrence():
+    from scipy.special import spherical_jn
+    from oracle.shims import k_integrals as ki
+    x = np.linspace(0.5, 80., 41)
+    lmin, lmax = 1, 30
+    jl = np.stack([spherical_jn(l, x) for l in range(lmin, lmax + 1)])[:, None, :]   # [nl, 1, nx]
+    jp = ki.compute_jl_prime(lmin, lmax, 2, 29, jl, 1)
+    ref = np.stack([spherical_jn(l, x, derivative=True) for l in range(2, 30)])[:, None, :]
+    assert np.abs(jp - ref).max() < 1e-13
+
+
+@pytest.mark.parametrize("pol", [False, True])
+def test_rtau_integrals_match_fixture(pol):
+    """The shim's a, b, c and r integrals from the fixture's inputs, on the reference's x grid."""
+    from oracle.shims import k_integrals as ki
+    d = dict(np.load(os.path.join(GOLD, "tspec_efti_nside16_%s.npz" % ("teb" if pol else "t"))))
+    k, T = d["k_arr"], d["Tl_arr"]
+    lmin_t, lmax_t = int(d["lmin_t"]), int(d["lmax_t"])
+    lmax, lmin = lmax_t + 1, lmin_t - 1
+    Pz = 2. * np.pi ** 2. / k ** 3 * 2.1e-9 * (k / 0.05) ** (0.96 - 1)
+    npol_out = 3 if pol else 1
+
+    def xgrid(max_kr):
+        x = list(np.arange(0, lmax * 2, 0.01)) + list(np.arange(lmax * 2, min(max_kr * 1.01, lmax * 100), 0.1))
+        if max_kr > 100 * lmax:
+            x += list(np.linspace(lmax * 100, max_kr * 1.01, 1000))
+        return np.asarray(x)
+
+    x = xgrid(max(k) * max(d["r_values"]))
+    jlx = np.zeros((lmax - lmin + 1, len(x)))
+    ki.compute_bessel(x, lmin, lmax, jlx, 1)
+    jlkr = ki.interpolate_jlkr(x, k, d["r_values"], jlx, 1)[lmin_t - lmin:lmax_t - lmin + 1]
+    out = np.zeros((lmax_t + 1, npol_out, len(d["r_values"])))
+    ki.r_integral(k, Pz, T, jlkr, lmin_t, lmax_t, 1, out)
+    assert np.abs(out - d["rlXs"]).max() <= 1e-12 * np.abs(d["rlXs"]).max()
+
+    r, tau = d["rtau_values"][:, 0], d["rtau_values"][:, 1]
+    x = xgrid(max(k) * (14163.032903769747 + 10000 + 5e6))
+    jlx = np.zeros((lmax - lmin + 1, len(x)))
+    ki.compute_bessel(x, lmin, lmax, jlx, 1)
+    jall = ki.interpolate_jlkr(x, k, r, jlx, 1)
+    jprime = ki.compute_jl_prime(lmin, lmax, lmin_t, lmax_t, jall, 1)
+    j = jall[lmin_t - lmin:lmax_t - lmin + 1]
+    for name, fn, args in (("alXs", ki.a_integral, (k, tau, Pz, T, j)),
+                           ("blXs", ki.b_integral, (k, tau, Pz, T, jprime)),
+                           ("clXs", ki.c_integral, (k, r, tau, Pz, T, j))):
+        out = np.zeros((lmax_t + 1, npol_out, len(r)))
+        fn(*args, lmin_t, lmax_t, 1, out)
+        assert np.abs(out - d[name]).max() <= 1e-12 * np.abs(d[name]).max(), name
