@@ -147,13 +147,17 @@ int ps_synthesis_noalloc(const ps_plan* plan, const double* alm, double* map, in
  *   PS_PIX_R2C / PS_PIX_R2CSTAR re im                          C     ideal_fisher.pyx:18-38
  *   PS_PIX_LENS_PHI             U V ([npol][n] complex each)   C[n]  ideal_fisher.pyx:124-139
  *   PS_PIX_LENS_PHI_SYM         U1 U2 V1 V2                    C[n]  ideal_fisher.pyx:142-157
+ *   PS_PIX_PRODUCT_REAL1        A B          (fac)             R     ideal_fisher.pyx:177-190, :325-338
+ *   PS_PIX_PRODUCT_REAL2        A0 B0 A1 B1  (fac)             R     the same, two terms of equal weight
  * npol is 1 or 3 for the lensing sums and 1 otherwise; fac is used by the
- * *STAR products.  The reference's nthreads argument has no counterpart. */
+ * *STAR and PRODUCT_REAL products (the latter are compute_productP_real_all /
+ * compute_productQ_real_all for real F maps).  The reference's nthreads argument has no counterpart. */
 enum {
   PS_PIX_MULTIPLY = 0, PS_PIX_MULTIPLY_ASYM, PS_PIX_MULTIPLYC, PS_PIX_MULTIPLYC_ASYM, PS_PIX_MULTIPLYCC,
   PS_PIX_MULTIPLYCC_ASYM, PS_PIX_MULTIPLY2, PS_PIX_MULTIPLY2R, PS_PIX_MULTIPLY2C, PS_PIX_MULTIPLYRC,
   PS_PIX_MULTIPLYRCSTAR, PS_PIX_MULTIPLYRC_SYM, PS_PIX_MULTIPLYRCSTAR_SYM, PS_PIX_MULTIPLYRR,
-  PS_PIX_MULTIPLYRR_SYM, PS_PIX_R2C, PS_PIX_R2CSTAR, PS_PIX_LENS_PHI, PS_PIX_LENS_PHI_SYM, PS_PIX_NOPS
+  PS_PIX_MULTIPLYRR_SYM, PS_PIX_R2C, PS_PIX_R2CSTAR, PS_PIX_LENS_PHI, PS_PIX_LENS_PHI_SYM,
+  PS_PIX_PRODUCT_REAL1, PS_PIX_PRODUCT_REAL2, PS_PIX_NOPS
 };
 int ps_pix_product(int op, const void* const* inputs, int n_inputs, void* out, int64_t n, int npol, double fac,
                    cudaStream_t stream);
@@ -307,6 +311,25 @@ int ps_kint_radial(const double* table, const double* x, int64_t nx, int tab_lmi
                    int nk, const double* kprod, int kstride, const double* T, int npol, int nl_T,
                    const double* r_arr, int nr, int lmin, int lmax, int nshift, int deriv, int lweight, int npol_out,
                    double* out, cudaStream_t stream);
+
+/* ------------------------------------------------------------- local tauNL (TSpecTemplate 'tauNL-loc')
+ * ps_tau_F_integral: F[n + nmax_F][L][i][j] = F_{L,L+n}(r_i, r_j) for n in [-nmax_F, nmax_F], the closed
+ *   form of polyspec/cython/k_integrals.pyx:453-494 (compute_F_integral; reference pref argument, the
+ *   2^(ns-3) factor applied here) for L in [max(Lmin - nmax_F, 0), Lmax + nmax_F] with L, L + n >= 1;
+ *   other entries are left as they are.  F has (2 nmax_F + 1) * nL * nr * nr doubles, nL >= Lmax +
+ *   nmax_F + 1.  *err (device int) is set to 1 where a hypergeometric series did not converge.
+ * ps_tau_convolve_F: out[j][lm] = Sum_k F[L][j][k] w_k X[k][lm] / sqrt(4 pi) with L = lm_L[lm] (-1:
+ *   out = 0), the convolve_F_n000 of polyspec/cython/tauNL_utils.pyx:966-995 over a full lm list; X,
+ *   out complex [nr][nlm], F one n-slice [nL][nr][nr].  With dot != NULL (device double) also
+ *   *dot = Sum_{lm,j} lm_w[lm] w_j Re(A[j][lm] conj(out[j][lm])) -- tau_sum_n0 of
+ *   tauNL_utils.pyx:604-647 for (A, X) -- using a workspace of ps_tau_convolve_workspace_bytes; out
+ *   may then be NULL.  nr <= 384. */
+int ps_tau_F_integral(const double* r_arr, int nr, int Lmin, int Lmax, int nmax_F, int nL, double ns, double pref,
+                      double* F, int* err, cudaStream_t stream);
+int ps_tau_convolve_workspace_bytes(int64_t nlm, size_t* bytes);
+int ps_tau_convolve_F(const double* X, const double* A, const int* lm_L, const double* lm_w, const double* F,
+                      const double* r_weights, int nr, int64_t nlm, double* out, double* dot, void* workspace,
+                      size_t workspace_bytes, cudaStream_t stream);
 
 /* ------------------------------------------------------------- launch statistics
  * No reference counterpart beyond its wall-clock SHT timer (polyspec/base.py:113-127,

@@ -19,10 +19,13 @@ Restated (same grids, branches and trapezium rule, vectorised):
   * b_integral            :172-215 f = (2/pi) k^(9/4) P_zeta^(3/4) / 2 (1 - k tau) e^(k tau) T j_l'(kr);
   * c_integral            :217-260 f = (2/pi) k^(5/4) P_zeta^(3/4) / 2 (1 - k tau) e^(k tau) / r
                           T j_l(kr), the sum weighted by sqrt(l (l+1)).
-The collider and F integrals raise NotImplementedError.
+  * compute_F_integral    :453-494 F_{L,L+n}(r, r') in closed form; GSL's lngamma and
+                          hyperg_2F1 (GSL version unpinned by the reference) are
+                          replaced by scipy's gammaln and hyp2f1.
+The collider integrals raise NotImplementedError.
 """
 import numpy as np
-from scipy.special import spherical_jn
+from scipy.special import gammaln, hyp2f1, spherical_jn
 
 
 def _smallx(l, x):
@@ -150,8 +153,31 @@ def c_integral(k_arr, r_arr, tau_arr, Pzeta_arr, Tl_arr, jlkrtau, lmin, lmax, nt
                    integs, True)
 
 
+def compute_F_integral(r_arr, FLLs, Lmin, Lmax, nmax_F, ns, _pref, nthreads):
+    r_arr = np.asarray(r_arr, dtype=np.float64)
+    pref = 2. ** (ns - 3) * _pref
+    for n in range(-nmax_F, nmax_F + 1):
+        i2a, i2b = (ns - 2 - n) / 2., (ns - 2 + n) / 2.
+        lgam2a, lgam2b = gammaln(1. - i2a), gammaln(1. - i2b)
+        for L in range(max(Lmin - nmax_F, 0), Lmax + nmax_F + 1):
+            if L + n < 1 or L < 1 or L + n > Lmax + nmax_F:
+                continue
+            i1, i3a, i3b = L + (n - 1. + ns) / 2., L + 1.5, L + n + 1.5
+            lgam1 = gammaln(i1)
+            prefa = pref * np.exp(lgam1 - lgam2a - gammaln(i3a))
+            prefb = pref * np.exp(lgam1 - lgam2b - gammaln(i3b))
+            for ir, ri in enumerate(r_arr):
+                for jr, rj in enumerate(r_arr):
+                    if ri <= rj:
+                        FLLs[nmax_F + n, L, ir, jr] = prefa * hyp2f1(i1, i2a, i3a, ri * ri / (rj * rj)) \
+                            * (ri / rj) ** L * rj ** (1. - ns)
+                    else:
+                        FLLs[nmax_F + n, L, ir, jr] = prefb * hyp2f1(i1, i2b, i3b, rj * rj / (ri * ri)) \
+                            * (rj / ri) ** (L + n) * ri ** (1. - ns)
+
+
 def _missing(*a, **k):
     raise NotImplementedError("this k-space integral is outside the oracle's scope")
 
 
-collider_p_integral = compute_F_integral = compute_collider_F_integral = _missing
+collider_p_integral = compute_collider_F_integral = _missing

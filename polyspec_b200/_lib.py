@@ -74,6 +74,11 @@ SIGNATURES = {
     "ps_kint_radial": (_c_int, [_c_void_p, _c_void_p, _c_int64, _c_int, _c_int, _c_void_p, _c_int, _c_void_p,
                                 _c_int, _c_void_p, _c_int, _c_int, _c_void_p, _c_int, _c_int, _c_int, _c_int, _c_int,
                                 _c_int, _c_int, _c_void_p, _c_void_p]),
+    "ps_tau_F_integral": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, _c_int, _c_int, _c_double, _c_double,
+                                   _c_void_p, _c_void_p, _c_void_p]),
+    "ps_tau_convolve_workspace_bytes": (_c_int, [_c_int64, ctypes.POINTER(_c_size_t)]),
+    "ps_tau_convolve_F": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int,
+                                   _c_int64, _c_void_p, _c_void_p, _c_void_p, _c_size_t, _c_void_p]),
     "ps_bispec_triplet_sums_workspace_bytes": (_c_int, [_c_int, _c_int64, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_bispec_triplet_sums": (_c_int, [_c_void_p, _c_int, _c_int64, _c_void_p, _c_void_p, _c_int, _c_void_p,
                                         _c_void_p, _c_size_t, _c_void_p]),
@@ -93,7 +98,8 @@ SIGNATURES = {
 # pixel-product ops and radial-sum kinds (enums of include/pscuda.h, in order)
 PIX_OPS = ["multiply", "multiply_asym", "multiplyC", "multiplyC_asym", "multiplyCC", "multiplyCC_asym", "multiply2",
            "multiply2R", "multiply2C", "multiplyRC", "multiplyRCstar", "multiplyRC_sym", "multiplyRCstar_sym",
-           "multiplyRR", "multiplyRR_sym", "r2c", "r2cstar", "lens_phi_sum", "lens_phi_sum_sym"]
+           "multiplyRR", "multiplyRR_sym", "r2c", "r2cstar", "lens_phi_sum", "lens_phi_sum_sym",
+           "product_real1", "product_real2"]
 SUM_KINDS = ["gnl_loc_sum", "gnl_loc_disc_sum", "gnl_con_sum", "gnl_con_disc_sum", "gnl_dotdot_sum",
              "gnl_dotdot_disc_sum", "gnl_dotdel_sum", "gnl_dotdel_disc_sum", "gnl_deldel_sum", "gnl_deldel_disc_sum"]
 

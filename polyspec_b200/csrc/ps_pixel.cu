@@ -109,6 +109,11 @@ __device__ __forceinline__ void pix_elem(const PixIn& a, int64_t i) {
     static_cast<double2*>(a.out)[i] = make_double2(ldr(a.p[0], i), ldr(a.p[1], i));
   } else if constexpr (OP == PS_PIX_R2CSTAR) {  // :30-38  re - i im
     static_cast<double2*>(a.out)[i] = make_double2(ldr(a.p[0], i), -ldr(a.p[1], i));
+  } else if constexpr (OP == PS_PIX_PRODUCT_REAL1) {  // ideal_fisher.pyx:177-190, :325-338 (one term)  fac A B
+    static_cast<double*>(a.out)[i] = a.fac * ldr(a.p[0], i) * ldr(a.p[1], i);
+  } else if constexpr (OP == PS_PIX_PRODUCT_REAL2) {  // the same with two terms  fac A0 B0 + fac A1 B1
+    static_cast<double*>(a.out)[i] =
+        a.fac * ldr(a.p[0], i) * ldr(a.p[1], i) + a.fac * ldr(a.p[2], i) * ldr(a.p[3], i);
   } else if constexpr (OP == PS_PIX_LENS_PHI || OP == PS_PIX_LENS_PHI_SYM) {
     // ideal_fisher.pyx:124-157.  Spin 0: 2 U0 conj(V0).  With polarisation:
     //   2 U0 conj(V0) + (U1 conj(V1) - conj(U1) V2) + i (U2 conj(V1) + conj(U2) V2)
@@ -175,6 +180,8 @@ OpInfo op_info(int op, int npol) {
     case PS_PIX_R2CSTAR: return {2, 32};
     case PS_PIX_LENS_PHI: return {2, 16.0 + 32.0 * npol};
     case PS_PIX_LENS_PHI_SYM: return {4, 16.0 + 64.0 * npol};
+    case PS_PIX_PRODUCT_REAL1: return {2, 24};
+    case PS_PIX_PRODUCT_REAL2: return {4, 40};
     default: return {-1, 0};
   }
 }
@@ -516,6 +523,8 @@ extern "C" int ps_pix_product(int op, const void* const* inputs, int n_inputs, v
     case PS_PIX_R2CSTAR: launch_op<PS_PIX_R2CSTAR>(a, grid, stream); break;
     case PS_PIX_LENS_PHI: launch_op<PS_PIX_LENS_PHI>(a, grid, stream); break;
     case PS_PIX_LENS_PHI_SYM: launch_op<PS_PIX_LENS_PHI_SYM>(a, grid, stream); break;
+    case PS_PIX_PRODUCT_REAL1: launch_op<PS_PIX_PRODUCT_REAL1>(a, grid, stream); break;
+    case PS_PIX_PRODUCT_REAL2: launch_op<PS_PIX_PRODUCT_REAL2>(a, grid, stream); break;
     default: return PS_ERR_INVALID;
   }
   PS_LAUNCH_CHECK();

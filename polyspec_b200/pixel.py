@@ -258,6 +258,22 @@ def multiplyRR_sym(arr1, arr2, arr1b, arr2b, nthreads=0):
     return _product("multiplyRR_sym", (arr1, arr2, arr1b, arr2b), "rrrr", False)
 
 
+def compute_product_real_all(maps, F_maps, weights, pq_inds, F_inds, nthreads=0):
+    """out = Sum_i weights[i] maps[pq_inds[i]] F_maps[F_inds[i]] for real [N_r, Npix] maps, one or two terms
+    of equal weight: compute_productP_real_all / compute_productQ_real_all of ideal_fisher.pyx:177-190,
+    :325-338 with the F maps real (their n1 = 0 form)."""
+    w = [float(x) for x in weights]
+    if len(w) == 1:
+        return _product("product_real1", (maps[pq_inds[0]], F_maps[F_inds[0]]), "rr", False, fac=w[0])
+    if len(w) == 2 and w[0] == w[1]:
+        return _product("product_real2", (maps[pq_inds[0]], F_maps[F_inds[0]], maps[pq_inds[1]], F_maps[F_inds[1]]),
+                        "rrrr", False, fac=w[0])
+    raise ValueError("one term, or two terms of equal weight")
+
+
+compute_productP_real_all = compute_productQ_real_all = compute_product_real_all
+
+
 def lens_phi_sum(umap, vmap, nthreads=0):
     """Pixel sum of U and V maps of the lensing Phi estimator (ideal_fisher.pyx:124-139)."""
     npol, npix = np.shape(umap)[0], np.shape(umap)[1]

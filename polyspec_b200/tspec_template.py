@@ -1,6 +1,6 @@
 """Template trispectrum estimator on the GPU (mirror of polyspec/tspec_template.py)
-for the gNL-loc, gNL-con, EFTI (gNL-dotdot, gNL-dotdel, gNL-deldel), lensing and
-point-source templates.
+for the gNL-loc, gNL-con, EFTI (gNL-dotdot, gNL-dotdel, gNL-deldel), tauNL-loc,
+lensing and point-source templates.
 
 ``TSpecTemplate(base, mask, applySinv, templates, k_arr, Tl_arr, lmin, lmax, ...)``
 keeps the reference constructor, its checks and attributes (l- and L-ranges and
@@ -8,9 +8,9 @@ filters, ``to_compute``, ``p_inds``, ``qlXs``, ``plLXs``, ``rlXs``, ``alXs``,
 ``blXs``, ``clXs``, ``timers``), the
 simulation handling (``generate_sims``, ``load_sims``) and the estimator methods
 (``Tl_numerator``, ``compute_fisher_contribution``, ``compute_fisher``,
-``Tl_unwindowed``, ``report_timings``, ``reset_timings``).  The reference's tauNL
-and collider templates raise NotImplementedError, as do the radial-sampling
-optimisers.
+``Tl_unwindowed``, ``report_timings``, ``reset_timings``).  The reference's
+direction-dependent tauNL and collider templates raise NotImplementedError, as do
+the radial-sampling optimisers.
 
 ``applySinv`` receives and returns CUDA tensors (as for PSpecBin/BSpecBin here);
 one with a ``.batched`` method filters the 4 x n_templates Q rows of the Fisher
@@ -25,6 +25,10 @@ Device mapping:
   the radial samples (P, Q, R, A, B maps; C is spin 1); the lensing U and V maps
   are spin 0/1/2/3 syntheses; Phi_LM is the lens_phi_sum kernel plus one spin-1
   adjoint.
+* tauNL-loc: F_L(r, r') from ``ps_tau_F_integral`` (closed form, as the reference);
+  the (P Q)_LM maps are a product kernel plus a batched adjoint to Lmax; the sum
+  over (L, M, r, r') and the F-convolution of the Fisher derivative are
+  ``ps_tau_convolve_F``.
 * Numerators: the radial pixel sums ``gnl_*(_disc)_sum``; lensing and point
   source sums are device reductions.
 * Fisher: the ``multiply*`` products, a batched spin-0 or spin-1 adjoint over the
@@ -39,7 +43,8 @@ import torch
 
 from . import _lib, pixel
 
-SUPPORTED = ['gNL-loc', 'gNL-con', 'gNL-dotdot', 'gNL-dotdel', 'gNL-deldel', 'lensing', 'point-source']
+SUPPORTED = ['gNL-loc', 'gNL-con', 'gNL-dotdot', 'gNL-dotdel', 'gNL-deldel', 'tauNL-loc', 'lensing',
+             'point-source']
 
 
 def _vp(t):
@@ -233,6 +238,11 @@ class TSpecTemplate:
         if 'gNL-deldel' in templates:
             self.to_compute.append(['b', 'c'])
             self.ints_2d = True
+        n1n3n = []
+        if 'tauNL-loc' in templates:
+            self.to_compute.append(['q'])
+            n1n3n.append([0, 0, 0])
+            self.ints_1d = True
         for t in templates:
             if 'lensing' in t:
                 assert len(C_phi) > 0, "Must supply lensing power spectrum!"
@@ -251,15 +261,17 @@ class TSpecTemplate:
                 self.to_compute.append(['u', 'v'])
             if 'point-source' in t:
                 self.to_compute.append(['u'])
-        self.n1n3n = np.zeros((0, 3), dtype=int)
+        self.n1n3n = np.asarray(n1n3n, dtype=int).reshape(-1, 3)
         self.to_compute = np.unique(np.concatenate(self.to_compute)) if self.to_compute else np.array([])
-        self.nmax = 0
+        self.nmax = int(np.max(self.n1n3n[:, :2])) if len(self.n1n3n) > 0 else 0
         self.nmax_coll = 0
         self.nmax_coll_F = 0
         self.p_inds = [0] if 'gNL-loc' in self.templates else []
-        self.nmax_F = 0
-        self.nLmax = self.Lmax
-        self.nLmin = self.Lmin
+        if len(self.n1n3n) > 0:
+            self.p_inds = [int(x) for x in np.unique(self.p_inds + list(np.unique(self.n1n3n[:, :2])))]
+        self.nmax_F = int(np.max(self.n1n3n[:, 2])) if len(self.n1n3n) > 0 else 0
+        self.nLmax = self.Lmax + self.nmax_F
+        self.nLmin = self.Lmin - self.nmax_F
         self.nLfilt = (self.base.l_arr >= self.nLmin) & (self.base.l_arr <= self.nLmax)
         self.Ls, self.Ms = self.base.l_arr[self.nLfilt], self.base.m_arr[self.nLfilt]
         self.nLminfilt = self.base.l_arr[self.base.l_arr <= self.nLmax] >= self.nLmin
@@ -357,6 +369,19 @@ class TSpecTemplate:
                 setattr(self, 'd_%slXs' % name, out)
                 setattr(self, '%slXs' % name, out.cpu().numpy())
         del table
+        if ints_1d and len(self.n1n3n) > 0:
+            print("Computing F_LL'(r, r') integrals")
+            FLLs = torch.zeros((2 * self.nmax_F + 1, self.nLmax + 1, self.N_r, self.N_r), dtype=torch.float64,
+                               device=dev)
+            pref = 2. * np.pi ** 2 * self.As / self.k_pivot ** (self.ns - 1)
+            d_r = torch.as_tensor(np.asarray(self.r_arr, dtype=np.float64), device=dev)
+            err = torch.zeros(1, dtype=torch.int32, device=dev)
+            _lib.call("ps_tau_F_integral", _vp(d_r), self.N_r, self.Lmin, self.Lmax, self.nmax_F, self.nLmax + 1,
+                      float(self.ns), float(pref), _vp(FLLs), _vp(err), _stream())
+            if int(err.item()) != 0:
+                raise Exception("F_LL'(r, r') calculation failed: a hypergeometric series did not converge")
+            self.d_FLLs = FLLs
+            self.FLLs = FLLs.cpu().numpy()
         self._make_utils()
         print("Precomputation complete")
 
@@ -365,6 +390,8 @@ class TSpecTemplate:
         qlXs, rlXs [lmax+1, 1+2 pol, N_r], plLXs [2 nmax+1, lmax+2, 1+2 pol, N_r], alXs,
         blXs, clXs [lmax+1, 1+2 pol, N_rtau] (the reference's attribute names and layouts)."""
         arrays.update(qlXs=qlXs, plLXs=plLXs)
+        if arrays.get('FLLs') is not None:
+            arrays['FLLs'] = np.ascontiguousarray(arrays['FLLs'], dtype=np.float64)
         for name, arr in arrays.items():
             if arr is None:
                 continue
@@ -377,6 +404,15 @@ class TSpecTemplate:
                                        self.base.m_arr.astype(np.int32), self.Lmin, self.Lmax,
                                        self.ls.astype(np.int32), self.ms.astype(np.int32),
                                        self.Ls.astype(np.int32), self.Ms.astype(np.int32), self.nmax_F)
+        if len(self.n1n3n) > 0:
+            # per lm of the l <= nLmax list: L where Lmin <= L <= Lmax (else -1), and the m weight
+            sel = self.base.l_arr <= self.nLmax
+            L, M = self.base.l_arr[sel], self.base.m_arr[sel]
+            lm_L = np.where((L >= self.Lmin) & (L <= self.Lmax), L, -1).astype(np.int32)
+            self.d_tau_lm_L = torch.as_tensor(lm_L, device=self._dev)
+            self.d_tau_lm_w = torch.as_tensor(np.where(M == 0, 1., 2.), device=self._dev)
+            self.d_r_weights = {t: torch.as_tensor(np.asarray(self.r_weights[t], dtype=np.float64), device=self._dev)
+                                for t in self.templates if t in self.r_weights}
 
     # ------------------------------------------------------------------ timings
     def report_timings(self):
@@ -627,6 +663,90 @@ class TSpecTemplate:
                 print("No preloading; simulations will be loaded and accessed at runtime.")
             self.load_sim_data = pair
 
+    # ------------------------------------------------------------------ local tauNL
+    def _A_maps(self, map1, map2, n, add_sym=False):
+        """[P_00 Q]_LM for each radial sample (polyspec/tspec_template.py:1275-1300, n = 0), as
+        [1, N_r, nlm(nLmax)] over the full l <= nLmax list (entries with L < nLmin are unused);
+        optionally adding the map1 <-> map2 term."""
+        assert n == 0, "only n = 0 (tauNL-loc) is implemented"
+        t0 = time.time()
+        if add_sym:
+            prod = pixel.multiplyRR_sym(map2['q'], map1['p00'], map1['q'], map2['p00'])
+        else:
+            prod = pixel.multiplyRR(map2['q'], map1['p00'])
+        out = self.base.to_lm_vec(prod, lmax=self.nLmax)
+        self._timed('tauNL_summation', t0)
+        return out[None]
+
+    def _tau_convolve(self, X, weights, A=None):
+        """ps_tau_convolve_F over [N_r, nlm(nLmax)] harmonic maps: the F_L convolution of X
+        (polyspec/cython/tauNL_utils.pyx:966-995) or, with A, the tau sum of (A, X) (:604-647)."""
+        w = torch.as_tensor(np.asarray(weights, dtype=np.float64), device=self._dev)
+        X = X.contiguous()
+        nr, nlm = X.shape
+        F = self.d_FLLs[self.nmax_F].contiguous()
+        if A is None:
+            out = torch.empty_like(X)
+            _lib.call("ps_tau_convolve_F", _vp(X), None, _vp(self.d_tau_lm_L), None, _vp(F), _vp(w), nr, nlm,
+                      _vp(out), None, None, 0, _stream())
+            return out
+        A = A.contiguous()
+        nb = ctypes.c_size_t()
+        _lib.call("ps_tau_convolve_workspace_bytes", nlm, ctypes.byref(nb))
+        ws = torch.empty(max(int(nb.value), 8), dtype=torch.uint8, device=self._dev)
+        dot = torch.zeros(1, dtype=torch.float64, device=self._dev)
+        _lib.call("ps_tau_convolve_F", _vp(X), _vp(A), _vp(self.d_tau_lm_L), _vp(self.d_tau_lm_w), _vp(F), _vp(w),
+                  nr, nlm, None, _vp(dot), _vp(ws), int(nb.value), _stream())
+        return float(dot.item())
+
+    def _tau_sum(self, A, B, weights, n1, n3, n):
+        """Sum over (L, M, r, r') of the local tauNL estimator (polyspec/tspec_template.py:1231-1240, n = 0)."""
+        assert n == 0 and n1 == n3 == 0, "only n1 = n3 = n = 0 (tauNL-loc) is implemented"
+        t0 = time.time()
+        out = self._tau_convolve(B[n1][0], weights, A=A[n1][0])
+        self._timed('tauNL_summation', t0)
+        return out
+
+    def _compute_PQ_vecs(self, Pn3_maps, Q_maps, i, j, n3=0, add_sym=False):
+        """[P Q]_LM(r) of polyspec/tspec_template.py:1967-2010 for n3 = 0, [N_r, nlm(nLmax)]."""
+        assert n3 == 0
+        if add_sym:
+            prod = pixel.multiplyRR_sym(Q_maps[j], Pn3_maps[i, 0], Q_maps[i], Pn3_maps[j, 0])
+        else:
+            prod = pixel.multiplyRR(Q_maps[j], Pn3_maps[i, 0])
+        return self.base.to_lm_vec(prod, lmax=self.nLmax)
+
+    def _F_PQ(self, Pn3_maps, Q_maps, r_weights):
+        """F_L * [P Q]_LM maps for the (1, 1), (2, 2) and symmetrised (1, 2) pairs
+        (polyspec/tspec_template.py:2287-2306 and :2142-2163, n1 = n3 = n = 0): [3, N_r, Npix] real."""
+        out = []
+        for i1, i2 in ((0, 0), (1, 1), (0, 1)):
+            t0 = time.time()
+            PQ = self._compute_PQ_vecs(Pn3_maps, Q_maps, i1, i2, 0, add_sym=(i1 != i2))
+            conv = self._tau_convolve(PQ, r_weights)
+            out.append(self.base.to_map_vec(conv, lmax=self.nLmax))
+            self._timed('fish_convolve', t0)
+        return torch.stack(out)
+
+    def _Q4_contributions(self, P_maps, Q_maps, F_PQ, pq_inds, F_inds, r_weights, weights):
+        """One Q4 row of the local tauNL derivative (polyspec/tspec_template.py:2341-2405, n1 = 0):
+        q_l^X-weighted radial sum of [P F_PQ]_lm plus p_l^X-weighted radial sum of [Q F_PQ]_lm."""
+        t0 = time.time()
+        w = np.asarray(r_weights, dtype=np.float64)
+        prod = pixel.compute_productP_real_all(P_maps[:, 0], F_PQ, weights, pq_inds, F_inds)
+        lm = self.base.to_lm_vec(prod, lmax=self.lmax)[:, self.d_lminfilt].contiguous()
+        out = self.utils.radial_sum(lm, 0.5 * w, self.d_qlXs)
+        prod = pixel.compute_productQ_real_all(Q_maps, F_PQ, weights, pq_inds, F_inds)
+        lm = self.base.to_lm_vec(prod, lmax=self.lmax)[:, self.d_lminfilt].contiguous()
+        out = out + self.utils.radial_sum(lm, 0.5 * (w / np.sqrt(4. * np.pi)), self.d_plLXs[self.nmax])
+        self._timed('fish_deriv', t0)
+        return out
+
+    def _get_Q4_perms(self, P_maps, Q_maps, F_PQ, r_weights):
+        """The four Q4 rows (111, 222, 112, 122) of polyspec/tspec_template.py:2521-2554."""
+        rows = (([0], [0], [12.]), ([1], [1], [12.]), ([1, 0], [0, 2], [4., 4.]), ([0, 1], [1, 2], [4., 4.]))
+        return torch.stack([self._Q4_contributions(P_maps, Q_maps, F_PQ, p, f, r_weights, w) for p, f, w in rows])
+
     # ------------------------------------------------------------------ numerator
     def Tl_numerator(self, data, include_disconnected_term=True, verb=False, input_type='map'):
         """Numerator of the unwindowed trispectrum estimator (polyspec/tspec_template.py:1338-1955)."""
@@ -661,12 +781,18 @@ class TSpecTemplate:
         if verb:
             print("# Assembling trispectrum numerator (4-field term)")
         Phi_dd = None
+        A_dd = {}
         for ii, t in enumerate(self.templates):
             if t == 'gNL-loc':
                 t0 = time.time()
                 t4_num[ii] = 9. / 100. * self.utils.gnl_loc_sum(self.r_weights[t], proc_maps['p00'], proc_maps['q']) \
                     * 4. * A_pix * (4. * np.pi) ** 1.5
                 self._timed('gNL_summation', t0)
+            if t == 'tauNL-loc':
+                if 0 not in A_dd:
+                    A_dd[0] = self._A_maps(proc_maps, proc_maps, 0)
+                t4_num[ii] = 1. / 24. * self._tau_sum(A_dd, A_dd, self.r_weights[t], 0, 0, 0) * 12. \
+                    * (4. * np.pi) ** (3. / 2.)
             if t in ('gNL-con', 'gNL-dotdot', 'gNL-dotdel', 'gNL-deldel'):
                 t0 = time.time()
                 t4_num[ii] = self._gnl_shape_sum(t, proc_maps) * A_pix
@@ -691,7 +817,27 @@ class TSpecTemplate:
                     pa, pb = self.proc_a_maps[isim], self.proc_b_maps[isim]
                 else:
                     pa, pb = self.load_sim_data(isim)
+                A_aa, A_bb, A_ad, A_bd, A_ab = {}, {}, {}, {}, {}
                 for ii, t in enumerate(self.templates):
+                    if t == 'tauNL-loc':
+                        w = self.r_weights[t]
+                        if 0 not in A_aa:
+                            A_aa[0] = self._A_maps(pa, pa, 0)
+                            A_ad[0] = self._A_maps(pa, proc_maps, 0, add_sym=True)
+                        tau = 4 * self._tau_sum(A_aa, A_dd, w, 0, 0, 0)
+                        tau += 2 * self._tau_sum(A_ad, A_ad, w, 0, 0, 0)
+                        if 0 not in A_bb:
+                            A_bb[0] = self._A_maps(pb, pb, 0)
+                            A_bd[0] = self._A_maps(pb, proc_maps, 0, add_sym=True)
+                        tau += 4 * self._tau_sum(A_bb, A_dd, w, 0, 0, 0)
+                        tau += 2 * self._tau_sum(A_bd, A_bd, w, 0, 0, 0)
+                        t2_num[ii] += -1. / 24. * tau * 6 / self.N_it / 2. * (4. * np.pi) ** (3. / 2.)
+                        if compute_t0:
+                            if 0 not in A_ab:
+                                A_ab[0] = self._A_maps(pa, pb, 0, add_sym=True)
+                            tau = 4 * self._tau_sum(A_aa, A_bb, w, 0, 0, 0)
+                            tau += 2 * self._tau_sum(A_ab, A_ab, w, 0, 0, 0)
+                            t0_num[ii] += 1. / 24. * tau * 3 / self.N_it * (4. * np.pi) ** (3. / 2.)
                     if t == 'gNL-loc':
                         t0 = time.time()
                         w = self.r_weights[t]
@@ -1013,6 +1159,11 @@ class TSpecTemplate:
                     A = A_maps
                     for k, (i, j, l) in enumerate(((0, 0, 0), (1, 1, 1), (0, 0, 1), (0, 1, 1))):
                         Qs[k, ii] = 9216. / 25. * self._transform_maps(self.utils.multiply(A[i], A[j], A[l]), f, w)
+                if t == 'tauNL-loc':
+                    w = self.r_weights[t]
+                    F_vecs = self._F_PQ(P_maps[0], Q_maps, w)
+                    Qs[:, ii] += (4. * np.pi) ** 1.5 * self._get_Q4_perms(P_maps[0], Q_maps, F_vecs, w)
+                    del F_vecs
                 if t == 'gNL-dotdel':
                     Qs[:, ii] = self._dotdel_Q(A_maps, B_maps, C_maps, self.rtau_weights[t])
                 if t == 'gNL-deldel':

@@ -58,3 +58,26 @@ def test_rtau_integrals_match_fixture(pol):
         out = np.zeros((lmax_t + 1, npol_out, len(r)))
         fn(*args, lmin_t, lmax_t, 1, out)
         assert np.abs(out - d[name]).max() <= 1e-12 * np.abs(d[name]).max(), name
+
+
+def test_F_integral_hypergeometric_against_mpmath():
+    """The oracle's F_L(r, r') (scipy's 2F1) against the same closed form with mpmath's 2F1
+    at 40 digits, on the tauNL fixture's radial grid."""
+    import mpmath
+    from oracle.shims import k_integrals as ki
+    d = dict(np.load(os.path.join(GOLD, "tspec_tauloc_nside16_t.npz")))
+    r = d["r_values"]
+    ns, As, kp = 0.96, 2.1e-9, 0.05
+    pref = 2. * np.pi ** 2 * As / kp ** (ns - 1)
+    F = np.zeros_like(d["FLLs"])
+    ki.compute_F_integral(r, F, 1, F.shape[1] - 1, 0, ns, pref, 1)
+    assert np.abs(F - d["FLLs"]).max() <= 1e-14 * np.abs(d["FLLs"]).max()
+    mpmath.mp.dps = 40
+    for L in (1, 2, 7, 20, 47):
+        for i, j in ((0, 0), (0, 1), (2, 5), (4, 3)):
+            ri, rj = (r[i], r[j]) if r[i] <= r[j] else (r[j], r[i])
+            i1, i2, i3 = L + (ns - 1.) / 2., (ns - 2.) / 2., L + 1.5
+            pf = 2. ** (ns - 3) * pref * mpmath.exp(mpmath.loggamma(i1) - mpmath.loggamma(1 - i2) - mpmath.loggamma(i3))
+            exact = float(pf * mpmath.hyp2f1(i1, i2, i3, (mpmath.mpf(ri) / rj) ** 2) * (mpmath.mpf(ri) / rj) ** L
+                          * mpmath.mpf(rj) ** (1 - ns))
+            assert abs(F[0, L, i, j] - exact) <= 1e-11 * abs(exact), (L, i, j)
