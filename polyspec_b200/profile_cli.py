@@ -27,7 +27,7 @@ S^-1 filter) per precision: device time, kernel time per kind, the numerator
 with two simulations, and the mixed-vs-FP64 Fisher difference.
 
     python -m polyspec_b200.profile_cli tspecbin [--nside 128 --lmax 255 --nbins 6]
-    python -m polyspec_b200.profile_cli tspec [--nside 512 --lmax 1000 --nr 24]
+    python -m polyspec_b200.profile_cli tspec [--nside 512 --lmax 1000 --nr 24 --templates gNL-loc,...]
 
 the binned trispectrum (T+E) and the template trispectrum (gNL-loc, lensing,
 point source): Fisher contribution and numerator times, FP64 and mixed.
@@ -184,7 +184,8 @@ def bspec(a):
 
 
 def tspec(a):
-    """Template trispectrum (gNL-loc, lensing, point-source): set-up, numerator and one Fisher contribution."""
+    """Template trispectrum (--templates, default gNL-loc, lensing, point-source): set-up, numerator and one
+    Fisher contribution."""
     import time
     import numpy as np
     from polyspec_b200 import PolySpec, Weightings, _lib
@@ -196,9 +197,10 @@ def tspec(a):
         base = PolySpec(a.nside, dict(w['cltot']), beam=list(w['beam']), pol=True, prec=prec)
         wts = Weightings(base, np.stack([w['mask']] * 3), dict(w['cl']), noise_cov=W.white_noise_cov(a.nside))
         t0 = time.time()
-        tst = TSpecTemplate(base, w['mask'], wts.make_applySinv('ideal'), ['gNL-loc', 'lensing', 'point-source'],
+        tst = TSpecTemplate(base, w['mask'], wts.make_applySinv('ideal'), a.templates.split(","),
                             w['k_arr'], w['Tl_arr'], w['lmin'], w['lmax'], r_values=w['r_values'],
-                            r_weights=w['r_weights'], C_phi=w['C_phi'], C_lens_weight=w['C_lens_weight'])
+                            r_weights=w['r_weights'], rtau_values=w['rtau_values'], rtau_weights=w['rtau_weights'],
+                            C_phi=w['C_phi'], C_lens_weight=w['C_lens_weight'])
         torch.cuda.synchronize()
         t_setup = time.time() - t0
         a_lms = [base.generate_data(seed=21 + i, deconvolve_beam=True, output_type='harmonic', rng='device')
@@ -320,6 +322,7 @@ def main(argv=None):
     t.add_argument("--nr", type=int, default=24)
     t.add_argument("--reps", type=int, default=2)
     t.add_argument("--precs", default="fp64,mixed")
+    t.add_argument("--templates", default="gNL-loc,lensing,point-source")
     tb = sub.add_parser("tspecbin")
     tb.add_argument("--nside", type=int, default=128)
     tb.add_argument("--lmax", type=int, default=255)

@@ -197,12 +197,14 @@ def smooth_transfer(npol, k_arr, lmax, seed=3):
     return T
 
 
-def tspec_setup(nside=512, lmax=1000, n_r=24, nk=400, fwhm_arcmin=10.0, pol=True, seed=0):
-    """Template-trispectrum workload (gNL-loc, lensing, point-source): seeded smooth
-    transfer functions on nk log-spaced k in [1e-4, 0.1], n_r radial samples around
-    recombination with seeded weights, C_phi = 1e-7 / (L (L+1))^2, the fiducial
-    spectra as lensing weights, Gaussian beam, latitude mask, ideal S^-1 filter.
-    Returns a dict of the TSpecTemplate arguments and the base's inputs."""
+def tspec_setup(nside=512, lmax=1000, n_r=24, nk=400, fwhm_arcmin=10.0, pol=True, seed=0, n_rtau=(4, 4)):
+    """Template-trispectrum workload: seeded smooth transfer functions on nk log-spaced
+    k in [1e-4, 0.1], n_r radial samples around recombination with seeded weights (the
+    same weights for gNL-loc, gNL-con and tauNL-loc), an n_rtau[0] x n_rtau[1] grid of
+    (r, tau) samples (r in [13400, 14200] Mpc, tau in [-2000, -50] Mpc) with seeded
+    weights for the EFTI shapes, C_phi = 1e-7 / (L (L+1))^2, the fiducial spectra as
+    lensing weights, Gaussian beam, latitude mask, ideal S^-1 filter.  Returns a dict
+    of the TSpecTemplate arguments and the base's inputs."""
     base_lmax = 3 * nside - 1
     cl = fiducial_cl(base_lmax, pol)
     b = gaussian_beam(base_lmax, fwhm_arcmin)
@@ -219,6 +221,12 @@ def tspec_setup(nside=512, lmax=1000, n_r=24, nk=400, fwhm_arcmin=10.0, pol=True
     C_phi = np.zeros(base_lmax + 1)
     C_phi[1:] = 1e-7 / (L[1:] * (L[1:] + 1.)) ** 2
     C_lens = {k: cl[k].copy() for k in (['TT', 'TE', 'EE', 'BB'] if pol else ['TT'])}
+    rr, tt = np.meshgrid(np.linspace(13400., 14200., n_rtau[0]), -np.geomspace(50., 2000., n_rtau[1]),
+                         indexing='ij')
+    rtau_values = np.stack([rr.ravel(), tt.ravel()], axis=1)
+    rtau_w = rng.uniform(0.5, 1.5, len(rtau_values)) * 100.
     return dict(cltot=cltot, cl=cl, beam=beam, mask=mask, k_arr=k_arr,
                 Tl_arr=smooth_transfer(2 if pol else 1, k_arr, lmax + 1, seed + 3), r_values=r_values,
-                r_weights={'gNL-loc': weights}, C_phi=C_phi, C_lens_weight=C_lens, lmin=2, lmax=lmax)
+                r_weights={t: weights for t in ('gNL-loc', 'gNL-con', 'tauNL-loc')}, rtau_values=rtau_values,
+                rtau_weights={t: rtau_w for t in ('gNL-dotdot', 'gNL-dotdel', 'gNL-deldel')}, C_phi=C_phi,
+                C_lens_weight=C_lens, lmin=2, lmax=lmax)
