@@ -312,6 +312,20 @@ int ps_kint_radial(const double* table, const double* x, int64_t nx, int tab_lmi
                    const double* r_arr, int nr, int lmin, int lmax, int nshift, int deriv, int lweight, int npol_out,
                    double* out, cudaStream_t stream);
 
+/* ------------------------------------------------------------- inpainting (Weightings.inpaint_map)
+ * ps_healpix_neighbours: out[p][k] (int32 [12 nside^2][8]) = the RING neighbours of pixel p in the order
+ *   SW, W, NW, N, NE, E, SE, S, -1 where there are only 7 -- healpy.get_all_neighbours, which
+ *   polyspec/weighting.py:118, :138 calls.  tables (device int32 [2][9][12]): per 3 x 3 cell (cx + 3 cy,
+ *   cx/cy 0 below, 1 inside, 2 above the face's lattice) and face, the adjacent face (-1: none) and the
+ *   lattice symmetry bits (1 flip x, 2 flip y, 4 swap), as polyspec_b200/healpix.py derives them.
+ * ps_inpaint_average: dst[pix[i]] = the average of src over the 8 neighbours of pix[i] (nb from
+ *   ps_healpix_neighbours; -1 reads src[npix - 1]): the plain mean (weighted = 0, the smoothing passes of
+ *   weighting.py:135-141) or the mean weighted by (value != 1e-30) (weighted = 1, the fill passes of
+ *   :115-131).  dst must not alias src; entries of dst outside the list are left as they are. */
+int ps_healpix_neighbours(int nside, const int* tables, int* out, cudaStream_t stream);
+int ps_inpaint_average(const double* src, const int* pix, int64_t n, const int* nb, int64_t npix, int weighted,
+                       double* dst, cudaStream_t stream);
+
 /* ------------------------------------------------------------- local tauNL (TSpecTemplate 'tauNL-loc')
  * ps_tau_F_integral: F[n + nmax_F][L][i][j] = F_{L,L+n}(r_i, r_j) for n in [-nmax_F, nmax_F], the closed
  *   form of polyspec/cython/k_integrals.pyx:453-494 (compute_F_integral; reference pref argument, the

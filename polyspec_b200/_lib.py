@@ -74,6 +74,9 @@ SIGNATURES = {
     "ps_kint_radial": (_c_int, [_c_void_p, _c_void_p, _c_int64, _c_int, _c_int, _c_void_p, _c_int, _c_void_p,
                                 _c_int, _c_void_p, _c_int, _c_int, _c_void_p, _c_int, _c_int, _c_int, _c_int, _c_int,
                                 _c_int, _c_int, _c_void_p, _c_void_p]),
+    "ps_healpix_neighbours": (_c_int, [_c_int, _c_void_p, _c_void_p, _c_void_p]),
+    "ps_inpaint_average": (_c_int, [_c_void_p, _c_void_p, _c_int64, _c_void_p, _c_int64, _c_int, _c_void_p,
+                                    _c_void_p]),
     "ps_tau_F_integral": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, _c_int, _c_int, _c_double, _c_double,
                                    _c_void_p, _c_void_p, _c_void_p]),
     "ps_tau_convolve_workspace_bytes": (_c_int, [_c_int64, ctypes.POINTER(_c_size_t)]),

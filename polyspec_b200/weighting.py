@@ -13,10 +13,12 @@ give numpy outputs; CUDA-tensor inputs give CUDA-tensor outputs.
 (polyspec/weighting.py:217-367) with vectors, dot products and the A and M
 operators evaluated on the device.
 """
+import ctypes
+
 import numpy as np
 import torch
 
-from . import lmops
+from . import _lib, healpix, lmops
 
 
 def _per_lm(base, mat_l):
@@ -109,9 +111,55 @@ class Weightings:
 
     # ------------------------------------------------------------------
     def inpaint_map(self, input_map, n_average=50):
-        """Neighbour-average inpainting (polyspec/weighting.py:87-146) is not part
-        of this build's GPU path."""
-        raise NotImplementedError("inpainting is not implemented in the CUDA backend")
+        """Linear inpainting (polyspec/weighting.py:87-146): per field, zero the inpainting
+        region, then fill its zero pixels with the mean of their 8 neighbours pass by pass
+        (each pass over the pixels still zero, all reading the previous pass) until none is
+        left or a pass fills none, then smooth the region by n_average passes of the plain
+        neighbour mean.  The averages are ``ps_inpaint_average`` over the GPU neighbour table
+        of ``healpix.neighbours``; the pass bookkeeping (which pixels are still zero) is a
+        device compaction."""
+        assert hasattr(self, 'inpainting_mask'), "Must supply inpainting mask to use inpainting code!"
+        x, as_torch = self.base._in(input_map, torch.float64)
+        tmp = x.clone()
+        if not hasattr(self, 'd_inpaint_filt'):
+            self.d_inpaint_filt = torch.as_tensor(np.asarray(self.inpainting_mask) == 1, device=tmp.device)
+        filt = self.d_inpaint_filt
+        if int(filt.sum()) == 0:
+            return self.base._out(tmp, as_torch)
+        nb = healpix.neighbours(self.base.Nside, tmp.device)
+        npix = tmp.shape[-1]
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+        def average(src, pix, weighted, dst):  # pix: int32 list held by the caller
+            _lib.call("ps_inpaint_average", ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(pix.data_ptr()),
+                      pix.numel(), ctypes.c_void_p(nb.data_ptr()), npix, int(weighted),
+                      ctypes.c_void_p(dst.data_ptr()), st)
+
+        for field in range(1 + 2 * self.pol):
+            this = tmp[field].clone()
+            if float(torch.sum(this)) == 0:
+                continue
+            fm = filt[field]
+            this[fm] = 0
+            inpaint_pix = torch.nonzero((tmp[field] == 0) & fm).flatten().to(torch.int32)
+            while True:
+                nxt = this.clone()
+                average(this, inpaint_pix, True, nxt)
+                this = nxt
+                next_inpaint = torch.nonzero((this == 0) & fm).flatten().to(torch.int32)
+                if next_inpaint.numel() == 0:
+                    break
+                if next_inpaint.numel() == inpaint_pix.numel():
+                    print("# Inpainting field %d failed!" % field)
+                    break
+                inpaint_pix = next_inpaint
+            pix = torch.nonzero(fm).flatten().to(torch.int32)
+            other = this.clone()
+            for _ in range(n_average):
+                average(this, pix, False, other)
+                this, other = other, this
+            tmp[field] = this
+        return self.base._out(tmp, as_torch)
 
     def applySinv_optimal(self, input_map, preconditioner='pseudo_inverse', nstep=25, thresh=1e-4, verb=False,
                           input_type='map', lmax=None):
@@ -128,7 +176,7 @@ class Weightings:
         if preconditioner in ('learned', 'cut'):
             return self.base._out(self.batched_applySinv_optimal(d[None], preconditioner=preconditioner,
                                                                  nstep=nstep, thresh=thresh, verb=verb,
-                                                                 lmax=lmax)[0], as_torch)
+                                                                 lmax=lmax, _inpainted=True)[0], as_torch)
         x0 = torch.einsum('abi,bi->ai', self.d_x0op, self.base.to_lm(d))
         cgd = CGD(self, d, x0=x0, preconditioner=preconditioner, verb=verb)
         cgd.run(nstep=nstep, thresh=thresh)
@@ -137,12 +185,14 @@ class Weightings:
         return self.base._out(cgd.get_ivar_lm()[:, lfilt], as_torch)
 
     def batched_applySinv_optimal(self, maps, preconditioner='harmonic', nstep=25, thresh=1e-4, verb=False,
-                                  lmax=None):
+                                  lmax=None, _inpainted=False):
         """applySinv_optimal for a batch of maps [B, nfield, Npix] (CUDA tensor), solved
         as B lockstep CGs with batched SHTs; returns [B, nfield, nlm(lmax)]."""
         if lmax is None:
             lmax = self.base.lmax
         d = maps.to(device=self.base.device, dtype=torch.float64)
+        if hasattr(self, 'inpainting_mask') and not _inpainted:
+            d = torch.stack([self.inpaint_map(m) for m in d])
         lm = self.base.to_lm_batch(d)
         x0 = lmops.matvec3(self.real3('x0op'), lm) if self.pol else torch.einsum('abi,nbi->nai', self.d_x0op, lm)
         # the learned CG hands a system to the plain CG after half the step budget
