@@ -312,6 +312,22 @@ int ps_kint_radial(const double* table, const double* x, int64_t nx, int tab_lmi
                    const double* r_arr, int nr, int lmin, int lmax, int nshift, int deriv, int lweight, int npol_out,
                    double* out, cudaStream_t stream);
 
+/* ------------------------------------------------------------- ideal bispectrum Fisher (BSpecBin.compute_fisher_ideal)
+ * The 3j-symbol sums of polyspec/bspec_bin.py:699-827 as Gauss-Legendre quadratures of binned Wigner d-sums
+ * (the Gaunt identity Int d d d dx = 2 (3j)(3j)); no reference counterpart for the individual calls.
+ * ps_gl_nodes: n Gauss-Legendre nodes x and weights w on [-1, 1] (device arrays).
+ * ps_wigner_binned: Phi[g][b][q][par][k] = Sum_{l in [edges[b], edges[b+1])} H[g][l] s_par(l) d^l_{m_q n_q}(x[k])
+ *   for q = 0..3 <-> (m, n) = (-1,-1), (-1,2), (2,-1), (2,2), s_0 = 1, s_1 = (-1)^l; H [G][lmax+1], edges
+ *   [nbins+1] ascending with edges[nbins] = lmax + 1 (device arrays).
+ * ps_bispec_ideal_contract: out[t][par] = (1/18) Sum_k w[k] Sum_{X,Y} Prod_i Phi[g_i][b_i][(X_i, Y_i)][par][k] over
+ *   the m-vectors X, Y in {(-1,-1,2), (2,-1,-1), (-1,2,-1)}, for tasks[t] = (g0, b0, g1, b1, g2, b2) (int32
+ *   [ntask][6]); a task with an index out of range gets NaN. */
+int ps_gl_nodes(int n, double* x, double* w, cudaStream_t stream);
+int ps_wigner_binned(const double* x, int nk, int lmax, const int* edges, int nbins, const double* H, int G,
+                     double* Phi, cudaStream_t stream);
+int ps_bispec_ideal_contract(const double* Phi, const double* w, int nk, int G, int nbins, const int* tasks, int ntask,
+                             double* out, cudaStream_t stream);
+
 /* ------------------------------------------------------------- inpainting (Weightings.inpaint_map)
  * ps_healpix_neighbours: out[p][k] (int32 [12 nside^2][8]) = the RING neighbours of pixel p in the order
  *   SW, W, NW, N, NE, E, SE, S, -1 where there are only 7 -- healpy.get_all_neighbours, which

@@ -74,6 +74,11 @@ SIGNATURES = {
     "ps_kint_radial": (_c_int, [_c_void_p, _c_void_p, _c_int64, _c_int, _c_int, _c_void_p, _c_int, _c_void_p,
                                 _c_int, _c_void_p, _c_int, _c_int, _c_void_p, _c_int, _c_int, _c_int, _c_int, _c_int,
                                 _c_int, _c_int, _c_void_p, _c_void_p]),
+    "ps_gl_nodes": (_c_int, [_c_int, _c_void_p, _c_void_p, _c_void_p]),
+    "ps_wigner_binned": (_c_int, [_c_void_p, _c_int, _c_int, _c_void_p, _c_int, _c_void_p, _c_int, _c_void_p,
+                                  _c_void_p]),
+    "ps_bispec_ideal_contract": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_int, _c_void_p, _c_int,
+                                          _c_void_p, _c_void_p]),
     "ps_healpix_neighbours": (_c_int, [_c_int, _c_void_p, _c_void_p, _c_void_p]),
     "ps_inpaint_average": (_c_int, [_c_void_p, _c_void_p, _c_int64, _c_void_p, _c_int64, _c_int, _c_void_p,
                                     _c_void_p]),

@@ -5,7 +5,8 @@ include_partial_triangles=False, fields=[...], parity='both')`` keeps the
 reference interface, its bin list (``all_bins``, same order), symmetry factors,
 ``get_ells``, simulation handling (``generate_sims``, ``load_sims``) and
 estimator methods (``Bl_numerator``, ``compute_fisher_contribution``,
-``compute_fisher``, ``Bl_unwindowed``, ``Bl_numerator_ideal``).
+``compute_fisher``, ``Bl_unwindowed``, ``Bl_numerator_ideal``,
+``compute_fisher_ideal``, ``Bl_ideal``).
 ``applySinv`` receives and returns CUDA tensors (maps ``float64 [nfield, Npix]``,
 alm ``complex128 [nfield, nlm]``); an ``applySinv`` with a ``.batched`` method (a
 callable on a leading batch axis, e.g. ``Weightings.make_applySinv``) filters the
@@ -36,6 +37,8 @@ How the work maps to the device:
 * Fisher.  The four outer products of :577-582 equal one product of the
   differences, Re(conj(Q_S0 - Q_S1) (Q_A0 - Q_A1)^T) / 24, computed as one real
   GEMM over (Re, Im).
+* Ideal Fisher.  The 3j-symbol sums of :699-827 as Gauss-Legendre quadratures of
+  binned Wigner d-sums (see ``compute_fisher_ideal``).
 """
 import ctypes
 
@@ -547,11 +550,80 @@ class BSpecBin:
         out = self._reduce(self._triplet_sums(maps, T['cubic_ptr'], T['cubic']), chi_fixed=True)
         return out / np.mean(np.asarray(self.mask) ** 3)
 
+    _PERMS = ((0, 1, 2), (1, 2, 0), (2, 0, 1), (0, 2, 1), (1, 0, 2), (2, 1, 0))
+
     def compute_fisher_ideal(self, verb=False, N_cpus=1):
-        """Analytic ideal Fisher matrix (polyspec/bspec_bin.py:702-820): needs Wigner 3j
-        symbols, which this package does not compute."""
-        raise NotImplementedError("the ideal bispectrum Fisher matrix needs Wigner 3j symbols (pywigxjpf in the "
-                                  "reference); pass fish_ideal to Bl_ideal instead")
+        """Analytic ideal (unit-mask) Fisher matrix (polyspec/bspec_bin.py:699-827).
+
+        The reference sums fac tj^2 x beams x (2l+1)^3 / (4 pi) x the six-permutation
+        inverse-covariance product over every (l1, l2, l3) of each pair of bin triplets with
+        equal sorted bins, with 3j symbols from pywigxjpf.  Here each permutation's sum is a
+        product of three per-position factors h(l) = beam beam' Cinv (2l + 1), so it runs
+        as Gauss-Legendre quadratures of binned Wigner d-sums (``ps_wigner_binned``,
+        ``ps_bispec_ideal_contract``; the Gaunt identity Int d d d = 2 (3j)(3j)), split into
+        even and odd l1 + l2 + l3 by (-1)^l factors.  The pair enumeration, the parity
+        (real / imaginary part) selection and the symmetry-factor normalisation follow the
+        reference; ``N_cpus`` has no counterpart."""
+        if not hasattr(self, 'sym_factor'):
+            self._compute_symmetry_factor()
+        ab = np.asarray(self.all_bins)
+        lb = np.asarray(self.l_bins_squeeze, dtype=np.int64)
+        nbins, Lmax = len(lb) - 1, int(lb[-1]) - 1
+        groups = {}
+        for i, row in enumerate(ab):
+            groups.setdefault(tuple(sorted(int(b) for b in row[3:6])), []).append(i)
+        gid, tasks, task_entry, entries = {}, [], [], []
+        for idxs in groups.values():
+            for a, i in enumerate(idxs):
+                for j in idxs[a:]:
+                    u, b, up, bp = ab[i][:3], ab[i][3:6], ab[j][:3], ab[j][3:6]
+                    for sg in self._PERMS:
+                        if all(b[k] == bp[sg[k]] for k in range(3)):
+                            gs = [gid.setdefault((int(u[k]), int(up[k]), int(up[sg[k]])), len(gid)) for k in range(3)]
+                            tasks.append((gs[0], b[0], gs[1], b[1], gs[2], b[2]))
+                            task_entry.append(len(entries))
+                    entries.append((i, j))
+        dev = self.base.device
+        ls = np.arange(Lmax + 1, dtype=np.float64)
+        beam = np.asarray(self.beam, dtype=np.float64)
+        icov = np.asarray(self.base.inv_Cl_tot_mat, dtype=np.float64)
+        H = np.zeros((max(len(gid), 1), Lmax + 1))
+        for (a, b_, c), g in gid.items():
+            H[g] = beam[a][:Lmax + 1] * beam[b_][:Lmax + 1] * icov[a, c][:Lmax + 1] * (2. * ls + 1.)
+        nk = (3 * Lmax) // 2 + 2
+        x = torch.empty(nk, dtype=torch.float64, device=dev)
+        w = torch.empty_like(x)
+        _lib.call("ps_gl_nodes", nk, _vp(x), _vp(w), _stream())
+        d_H = torch.as_tensor(H, device=dev)
+        d_edges = torch.as_tensor(lb.astype(np.int32), device=dev)
+        G = H.shape[0]
+        Phi = torch.zeros((G, nbins, 4, 2, nk), dtype=torch.float64, device=dev)
+        _lib.call("ps_wigner_binned", _vp(x), nk, Lmax, _vp(d_edges), nbins, _vp(d_H), G, _vp(Phi), _stream())
+        d_tasks = torch.as_tensor(np.asarray(tasks, dtype=np.int32).reshape(-1, 6), device=dev)
+        S = torch.empty((len(tasks), 2), dtype=torch.float64, device=dev)
+        _lib.call("ps_bispec_ideal_contract", _vp(Phi), _vp(w), nk, G, nbins, _vp(d_tasks), len(tasks), _vp(S),
+                  _stream())
+        S = S.cpu().numpy()
+        value = np.zeros(len(entries), dtype=np.complex128)
+        np.add.at(value, np.asarray(task_entry, dtype=np.int64),
+                  ((S[:, 0] + S[:, 1]) / 2. + 1j * (S[:, 0] - S[:, 1]) / 2.) / (4. * np.pi))
+        NB = self.N_b
+        sym = np.asarray(self.sym_factor)
+        fish = np.zeros((NB, NB))
+        for e, (i, j) in enumerate(entries):
+            pu, pup = ab[i][6], ab[j][6]
+            for ci, chi in enumerate(self.chi_arr):
+                for cj, chip in enumerate(self.chi_arr):
+                    if pu * chi != pup * chip:
+                        continue
+                    out = value[e].real if pu * chi == 1 else value[e].imag
+                    fish[ci * NB // 2 + i, cj * NB // 2 + j] = out / sym[i] / sym[j]
+                    fish[cj * NB // 2 + j, ci * NB // 2 + i] = out / sym[i] / sym[j]
+        if verb:
+            print("Fisher matrix computation complete\n")
+        self.fish_ideal = fish
+        self.inv_fish_ideal = np.linalg.inv(self.fish_ideal)
+        return fish
 
     def Bl_ideal(self, data, fish_ideal=[], verb=False, N_cpus=1):
         """Ideal estimator with a supplied ideal Fisher matrix (polyspec/bspec_bin.py:822-861)."""

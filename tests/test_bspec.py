@@ -117,3 +117,14 @@ def test_fisher_contribution_unbatched_filter():
             return f(*a, **k)
     bsb.applySinv = Plain()
     assert rel(bsb.compute_fisher_contribution(1), d["fisher_seed1"]) < TOL_F
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pol", [False, True])
+def test_fisher_ideal(pol):
+    """The analytic ideal Fisher matrix against the reference's (exact 3j symbols,
+    tests/golden/make_golden_bspec_ideal.py): 1e-12 relative, max-norm."""
+    d = load(pol)
+    g = np.load(os.path.join(GOLD, "bspec_ideal_nside16_%s.npz" % ("teb" if pol else "t")))["fisher_ideal"]
+    _, bsb = _build(d, pol)
+    assert rel(bsb.compute_fisher_ideal(), g) < 1e-12
