@@ -128,3 +128,23 @@ def test_fisher_ideal(pol):
     g = np.load(os.path.join(GOLD, "bspec_ideal_nside16_%s.npz" % ("teb" if pol else "t")))["fisher_ideal"]
     _, bsb = _build(d, pol)
     assert rel(bsb.compute_fisher_ideal(), g) < 1e-12
+
+
+@pytest.mark.gpu
+def test_mc_fisher_converges_to_ideal():
+    """With a unit mask and the ideal filter the Monte Carlo Fisher matrix converges to
+    the analytic ideal one (the consistency check the reference's ideal estimators
+    provide): 160 seeds, diagonal within 5 %, every entry within 3 % of the largest."""
+    from polyspec_b200 import PolySpec, Weightings
+    from polyspec_b200.bspec_bin import BSpecBin
+    d = load(False)
+    cltot = {k[6:]: d[k] for k in d if k.startswith("cltot_")}
+    clraw = {k[6:]: d[k] for k in d if k.startswith("clraw_")}
+    base = PolySpec(int(d["nside"]), dict(cltot), beam=d["beam"][:1], pol=False, backend="cuda")
+    ones = np.ones_like(d["mask"])
+    wts = Weightings(base, ones, dict(clraw), noise_cov=d["noise"])
+    bsb = BSpecBin(base, ones[0], wts.make_applySinv('ideal'), d["l_bins"], fields=['TTT'], parity='even')
+    Fi = bsb.compute_fisher_ideal()
+    F = np.mean([bsb.compute_fisher_contribution(s) for s in range(160)], axis=0)
+    assert np.abs(np.diag(F) / np.diag(Fi) - 1.).max() < 0.05
+    assert np.abs(F - Fi).max() < 0.03 * np.abs(Fi).max()
