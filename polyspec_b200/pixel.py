@@ -274,6 +274,40 @@ def compute_product_real_all(maps, F_maps, weights, pq_inds, F_inds, nthreads=0)
 compute_productP_real_all = compute_productQ_real_all = compute_product_real_all
 
 
+def tau_convolve_F(X, lm_L, F, r_weights, A=None, lm_w=None):
+    """F_L convolution of harmonic maps X [N_r, nlm] (complex128, one lm list, CUDA):
+    out[j, lm] = Sum_k F[L(lm), j, k] w_k X[k, lm] / sqrt(4 pi) with L = lm_L[lm] (int32, -1: out = 0),
+    convolve_F_n000 of tauNL_utils.pyx:966-995 for F one n-slice [nL, N_r, N_r].  With A (and the m
+    weights lm_w) it returns instead the scalar Sum_{lm, j} lm_w w_j Re(A[j, lm] conj(out[j, lm])),
+    tau_sum_n0 (:604-647) of (A, X)."""
+    X = X.contiguous()
+    nr, nlm = X.shape
+    F = F.contiguous()
+    lm_L = lm_L.to(torch.int32).contiguous()
+    w = torch.as_tensor(np.asarray(r_weights, dtype=np.float64), device=X.device)
+    if F.shape[1:] != (nr, nr) or lm_L.numel() != nlm or w.numel() != nr:
+        raise ValueError("X, lm_L, F and r_weights do not match")
+    if A is None:
+        out = torch.empty_like(X)
+        _lib.call("ps_tau_convolve_F", ctypes.c_void_p(X.data_ptr()), None, ctypes.c_void_p(lm_L.data_ptr()), None,
+                  ctypes.c_void_p(F.data_ptr()), ctypes.c_void_p(w.data_ptr()), nr, nlm,
+                  ctypes.c_void_p(out.data_ptr()), None, None, 0, _stream())
+        return out
+    A = A.contiguous()
+    lm_w = lm_w.to(torch.float64).contiguous()
+    if A.shape != X.shape or lm_w.numel() != nlm:
+        raise ValueError("A, lm_w do not match X")
+    nb = ctypes.c_size_t()
+    _lib.call("ps_tau_convolve_workspace_bytes", nlm, ctypes.byref(nb))
+    ws = torch.empty(max(int(nb.value), 8), dtype=torch.uint8, device=X.device)
+    dot = torch.zeros(1, dtype=torch.float64, device=X.device)
+    _lib.call("ps_tau_convolve_F", ctypes.c_void_p(X.data_ptr()), ctypes.c_void_p(A.data_ptr()),
+              ctypes.c_void_p(lm_L.data_ptr()), ctypes.c_void_p(lm_w.data_ptr()), ctypes.c_void_p(F.data_ptr()),
+              ctypes.c_void_p(w.data_ptr()), nr, nlm, None, ctypes.c_void_p(dot.data_ptr()),
+              ctypes.c_void_p(ws.data_ptr()), int(nb.value), _stream())
+    return float(dot.item())
+
+
 def lens_phi_sum(umap, vmap, nthreads=0):
     """Pixel sum of U and V maps of the lensing Phi estimator (ideal_fisher.pyx:124-139)."""
     npol, npix = np.shape(umap)[0], np.shape(umap)[1]

@@ -679,25 +679,10 @@ class TSpecTemplate:
         return out[None]
 
     def _tau_convolve(self, X, weights, A=None):
-        """ps_tau_convolve_F over [N_r, nlm(nLmax)] harmonic maps: the F_L convolution of X
+        """pixel.tau_convolve_F over [N_r, nlm(nLmax)] harmonic maps: the F_L convolution of X
         (polyspec/cython/tauNL_utils.pyx:966-995) or, with A, the tau sum of (A, X) (:604-647)."""
-        w = torch.as_tensor(np.asarray(weights, dtype=np.float64), device=self._dev)
-        X = X.contiguous()
-        nr, nlm = X.shape
-        F = self.d_FLLs[self.nmax_F].contiguous()
-        if A is None:
-            out = torch.empty_like(X)
-            _lib.call("ps_tau_convolve_F", _vp(X), None, _vp(self.d_tau_lm_L), None, _vp(F), _vp(w), nr, nlm,
-                      _vp(out), None, None, 0, _stream())
-            return out
-        A = A.contiguous()
-        nb = ctypes.c_size_t()
-        _lib.call("ps_tau_convolve_workspace_bytes", nlm, ctypes.byref(nb))
-        ws = torch.empty(max(int(nb.value), 8), dtype=torch.uint8, device=self._dev)
-        dot = torch.zeros(1, dtype=torch.float64, device=self._dev)
-        _lib.call("ps_tau_convolve_F", _vp(X), _vp(A), _vp(self.d_tau_lm_L), _vp(self.d_tau_lm_w), _vp(F), _vp(w),
-                  nr, nlm, None, _vp(dot), _vp(ws), int(nb.value), _stream())
-        return float(dot.item())
+        return pixel.tau_convolve_F(X, self.d_tau_lm_L, self.d_FLLs[self.nmax_F], weights, A=A,
+                                    lm_w=self.d_tau_lm_w)
 
     def _tau_sum(self, A, B, weights, n1, n3, n):
         """Sum over (L, M, r, r') of the local tauNL estimator (polyspec/tspec_template.py:1231-1240, n = 0)."""

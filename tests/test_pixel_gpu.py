@@ -148,3 +148,51 @@ def test_outer_product(sym, na, nb, nin):
     _, F = _ref()
     if F is not None:
         assert close(got, F.outer_product(Qa, Qb, 2, sym), 1e-12)
+
+
+def _tau_case(nr, seed, zero_w=True):
+    """Random (L, M) maps, F_L(r, r') and radial weights (some zero) for the local-tauNL kernels."""
+    from pixel_cases import lm_setup
+    rng = np.random.default_rng(seed)
+    base_lmax, Lmin, Lmax = 20, 2, 12
+    l, m = lm_setup(base_lmax)
+    sel = l <= Lmax
+    Lfull, Mfull = l[sel], m[sel]
+    filt = Lfull >= Lmin
+    X = rng.normal(size=(nr, sel.sum())) + 1j * rng.normal(size=(nr, sel.sum()))
+    A = rng.normal(size=(nr, sel.sum())) + 1j * rng.normal(size=(nr, sel.sum()))
+    F = rng.normal(size=(1, Lmax + 1, nr, nr))
+    F = F + np.swapaxes(F, 2, 3)   # F_L(r, r') is symmetric for n = 0
+    w = rng.uniform(0.5, 2.0, nr)
+    if zero_w and nr > 2:
+        w[1] = 0.
+    lm_L = np.where(filt, Lfull, -1).astype(np.int32)
+    lm_w = np.where(Mfull == 0, 1., 2.)
+    args = (1, nr, l.astype(np.int32), m.astype(np.int32), Lmin, Lmax, l.astype(np.int32), m.astype(np.int32),
+            Lfull[filt].astype(np.int32), Mfull[filt].astype(np.int32), 0)
+    return X, A, F, w, lm_L, lm_w, filt, args
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nr,seed", [(1, 1), (6, 2), (24, 3), (97, 4)])
+def test_tau_convolve_and_sum(nr, seed):
+    """ps_tau_convolve_F against the compiled reference's convolve_F_n000 and tau_sum_n0
+    (zero radial weights included): 1e-13 of the largest magnitude."""
+    import torch
+    from polyspec_b200 import pixel as P
+    T, _ = _ref()
+    if T is None:
+        pytest.skip("oracle/_ref is not built")
+    X, A, F, w, lm_L, lm_w, filt, args = _tau_case(nr, seed)
+    dev = torch.device("cuda")
+    tX, tA, tF = (torch.as_tensor(v, device=dev) for v in (X, A, F[0]))
+    out = P.tau_convolve_F(tX, torch.as_tensor(lm_L, device=dev), tF, w).cpu().numpy()
+    ut = T.tauNL_utils(*args)
+    ref = np.zeros((len(filt), nr), dtype=np.complex128)
+    ut.convolve_F_n000(np.ascontiguousarray(X[:, filt].T), F, w, ref, 0, np.arange(nr, dtype=np.int32))
+    assert close(out.T, ref, 1e-13)
+    tau = P.tau_convolve_F(tX, torch.as_tensor(lm_L, device=dev), tF, w, A=tA,
+                           lm_w=torch.as_tensor(lm_w, device=dev))
+    tau_ref = ut.tau_sum_n0(np.ascontiguousarray(A[:, filt].T)[None], np.ascontiguousarray(X[:, filt].T)[None],
+                            F[0], w, 0)
+    assert abs(tau - tau_ref) <= 1e-12 * abs(tau_ref)
