@@ -348,16 +348,16 @@ int ps_inpaint_average(const double* src, const int* pix, int64_t n, const int* 
  *   2^(ns-3) factor applied here) for L in [max(Lmin - nmax_F, 0), Lmax + nmax_F] with L, L + n >= 1;
  *   other entries are left as they are.  F has (2 nmax_F + 1) * nL * nr * nr doubles, nL >= Lmax +
  *   nmax_F + 1.  *err (device int) is set to 1 where a hypergeometric series did not converge.
- * ps_tau_convolve_F: out[j][lm] = Sum_k F[L][j][k] w_k X[k][lm] / sqrt(4 pi) with L = lm_L[lm] (-1:
- *   out = 0), the convolve_F_n000 of polyspec/cython/tauNL_utils.pyx:966-995 over a full lm list; X,
- *   out complex [nr][nlm], F one n-slice [nL][nr][nr].  With dot != NULL (device double) also
+ * ps_tau_convolve_F: out[j][lm] = Sum_k F_L(r_j, r_k) w_k X[k][lm] / sqrt(4 pi) with L = lm_L[lm] (-1:
+ *   out = 0, else L < nL), the convolve_F_n000 of polyspec/cython/tauNL_utils.pyx:966-995 over a full lm
+ *   list; X, out complex [nr][nlm], F one n-slice stored transposed, [nr][nr][nL] (F[j][k][L]).  With dot != NULL (device double) also
  *   *dot = Sum_{lm,j} lm_w[lm] w_j Re(A[j][lm] conj(out[j][lm])) -- tau_sum_n0 of
  *   tauNL_utils.pyx:604-647 for (A, X) -- using a workspace of ps_tau_convolve_workspace_bytes; out
  *   may then be NULL.  nr <= 384. */
 int ps_tau_F_integral(const double* r_arr, int nr, int Lmin, int Lmax, int nmax_F, int nL, double ns, double pref,
                       double* F, int* err, cudaStream_t stream);
 int ps_tau_convolve_workspace_bytes(int64_t nlm, size_t* bytes);
-int ps_tau_convolve_F(const double* X, const double* A, const int* lm_L, const double* lm_w, const double* F,
+int ps_tau_convolve_F(const double* X, const double* A, const int* lm_L, const double* lm_w, const double* F, int nL,
                       const double* r_weights, int nr, int64_t nlm, double* out, double* dot, void* workspace,
                       size_t workspace_bytes, cudaStream_t stream);
 

@@ -85,8 +85,8 @@ SIGNATURES = {
     "ps_tau_F_integral": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, _c_int, _c_int, _c_double, _c_double,
                                    _c_void_p, _c_void_p, _c_void_p]),
     "ps_tau_convolve_workspace_bytes": (_c_int, [_c_int64, ctypes.POINTER(_c_size_t)]),
-    "ps_tau_convolve_F": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int,
-                                   _c_int64, _c_void_p, _c_void_p, _c_void_p, _c_size_t, _c_void_p]),
+    "ps_tau_convolve_F": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, _c_void_p,
+                                   _c_int, _c_int64, _c_void_p, _c_void_p, _c_void_p, _c_size_t, _c_void_p]),
     "ps_bispec_triplet_sums_workspace_bytes": (_c_int, [_c_int, _c_int64, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_bispec_triplet_sums": (_c_int, [_c_void_p, _c_int, _c_int64, _c_void_p, _c_void_p, _c_int, _c_void_p,
                                         _c_void_p, _c_size_t, _c_void_p]),

@@ -13,7 +13,9 @@
 //    formula (Abramowitz & Stegun 15.3.6, valid for non-integer c - a - b), and at
 //    z = 1 from Gauss's summation theorem.  One thread per (n, L, r, r').  A series that
 //    does not converge within its iteration limit sets an error flag.
-//  * ps_tau_convolve_F: out[j][lm] = Sum_k F_L(r_j, r_k) w_k X[k][lm] / sqrt(4 pi)
+//  * ps_tau_convolve_F: out[j][lm] = Sum_k F_L(r_j, r_k) w_k X[k][lm] / sqrt(4 pi), F stored
+//    [j][k][L] so that a warp's lanes (consecutive lm of one m: consecutive L) read
+//    consecutive words (an [L][j][k] layout left the kernel bound by L1 wavefronts)
 //    for lm with Lmin <= L <= Lmax (zero elsewhere), the n = n1 = n3 = 0 convolution
 //    tauNL_utils.pyx:966-995 (convolve_F_n000), skipping r_k with w_k = 0.  With A
 //    given it also returns
@@ -135,7 +137,7 @@ __global__ void tau_F_kernel(const double* __restrict__ r, int nr, int Lmin, int
 template <bool DOT>
 __global__ void __launch_bounds__(TAU_THREADS) tau_conv_kernel(
     const double2* __restrict__ X, const double2* __restrict__ A, const int* __restrict__ lm_L,
-    const double* __restrict__ lm_w, const double* __restrict__ F, const double* __restrict__ w, int nr,
+    const double* __restrict__ lm_w, const double* __restrict__ F, const double* __restrict__ w, int nr, int nL,
     int64_t nlm, double2* __restrict__ out, double* __restrict__ partial) {
   extern __shared__ double2 xs[];  // [nr][TAU_TILE]
   __shared__ double red[TAU_THREADS / 32];
@@ -151,11 +153,13 @@ __global__ void __launch_bounds__(TAU_THREADS) tau_conv_kernel(
   for (int j = ty; j < nr; j += TAU_JLANES) {
     double sx = 0.0, sy = 0.0;
     if (L >= 0) {
-      const double* Fr = F + (int64_t(L) * nr + j) * nr;
+      // F is stored [j][k][L]: the lanes of a warp (consecutive lm, mostly consecutive L) read
+      // consecutive words
+      const double* Fr = F + int64_t(j) * nr * nL + L;
       for (int k = 0; k < nr; ++k) {
         const double wk = __ldg(w + k);
         if (wk == 0.0) continue;
-        const double f = __ldg(Fr + k) * wk;
+        const double f = __ldg(Fr + int64_t(k) * nL) * wk;
         const double2 x = xs[k * TAU_TILE + tx];
         sx += f * x.x * inv_s4pi;
         sy += f * x.y * inv_s4pi;
@@ -221,9 +225,10 @@ extern "C" int ps_tau_convolve_workspace_bytes(int64_t nlm, size_t* bytes) {
 }
 
 extern "C" int ps_tau_convolve_F(const double* X, const double* A, const int* lm_L, const double* lm_w,
-                                 const double* F, const double* r_weights, int nr, int64_t nlm, double* out,
+                                 const double* F, int nL, const double* r_weights, int nr, int64_t nlm, double* out,
                                  double* dot, void* workspace, size_t workspace_bytes, cudaStream_t stream) {
-  if (!X || !lm_L || !F || !r_weights || nr <= 0 || nr > 384 || nlm <= 0 || (!out && !dot)) return PS_ERR_INVALID;
+  if (!X || !lm_L || !F || !r_weights || nr <= 0 || nr > 384 || nL <= 0 || nlm <= 0 || (!out && !dot))
+    return PS_ERR_INVALID;
   if (dot && (!A || !lm_w)) return PS_ERR_INVALID;
   const int64_t nblk = (nlm + TAU_TILE - 1) / TAU_TILE;
   if (nblk > 2147483647LL) return PS_ERR_INVALID;
@@ -236,14 +241,14 @@ extern "C" int ps_tau_convolve_F(const double* X, const double* A, const int* lm
       cudaFuncSetAttribute(tau_conv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     tau_conv_kernel<true><<<unsigned(nblk), TAU_THREADS, smem, stream>>>(
         reinterpret_cast<const double2*>(X), reinterpret_cast<const double2*>(A), lm_L, lm_w, F, r_weights, nr,
-        nlm, reinterpret_cast<double2*>(out), static_cast<double*>(workspace));
+        nL, nlm, reinterpret_cast<double2*>(out), static_cast<double*>(workspace));
     PS_LAUNCH_CHECK();
     tau_partial_sum<<<1, 256, 0, stream>>>(static_cast<double*>(workspace), nblk, dot);
   } else {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(tau_conv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     tau_conv_kernel<false><<<unsigned(nblk), TAU_THREADS, smem, stream>>>(
-        reinterpret_cast<const double2*>(X), nullptr, lm_L, nullptr, F, r_weights, nr, nlm,
+        reinterpret_cast<const double2*>(X), nullptr, lm_L, nullptr, F, r_weights, nr, nL, nlm,
         reinterpret_cast<double2*>(out), nullptr);
   }
   PS_LAUNCH_CHECK();

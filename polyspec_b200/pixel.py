@@ -282,15 +282,18 @@ def tau_convolve_F(X, lm_L, F, r_weights, A=None, lm_w=None):
     tau_sum_n0 (:604-647) of (A, X)."""
     X = X.contiguous()
     nr, nlm = X.shape
-    F = F.contiguous()
     lm_L = lm_L.to(torch.int32).contiguous()
     w = torch.as_tensor(np.asarray(r_weights, dtype=np.float64), device=X.device)
     if F.shape[1:] != (nr, nr) or lm_L.numel() != nlm or w.numel() != nr:
         raise ValueError("X, lm_L, F and r_weights do not match")
+    nL = F.shape[0]
+    if nlm and int(lm_L.max()) >= nL:
+        raise ValueError("lm_L holds an L beyond F")
+    FT = F.permute(1, 2, 0).contiguous()  # [j][k][L], the kernel's layout
     if A is None:
         out = torch.empty_like(X)
         _lib.call("ps_tau_convolve_F", ctypes.c_void_p(X.data_ptr()), None, ctypes.c_void_p(lm_L.data_ptr()), None,
-                  ctypes.c_void_p(F.data_ptr()), ctypes.c_void_p(w.data_ptr()), nr, nlm,
+                  ctypes.c_void_p(FT.data_ptr()), nL, ctypes.c_void_p(w.data_ptr()), nr, nlm,
                   ctypes.c_void_p(out.data_ptr()), None, None, 0, _stream())
         return out
     A = A.contiguous()
@@ -302,7 +305,7 @@ def tau_convolve_F(X, lm_L, F, r_weights, A=None, lm_w=None):
     ws = torch.empty(max(int(nb.value), 8), dtype=torch.uint8, device=X.device)
     dot = torch.zeros(1, dtype=torch.float64, device=X.device)
     _lib.call("ps_tau_convolve_F", ctypes.c_void_p(X.data_ptr()), ctypes.c_void_p(A.data_ptr()),
-              ctypes.c_void_p(lm_L.data_ptr()), ctypes.c_void_p(lm_w.data_ptr()), ctypes.c_void_p(F.data_ptr()),
+              ctypes.c_void_p(lm_L.data_ptr()), ctypes.c_void_p(lm_w.data_ptr()), ctypes.c_void_p(FT.data_ptr()), nL,
               ctypes.c_void_p(w.data_ptr()), nr, nlm, None, ctypes.c_void_p(dot.data_ptr()),
               ctypes.c_void_p(ws.data_ptr()), int(nb.value), _stream())
     return float(dot.item())
