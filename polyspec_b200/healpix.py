@@ -15,6 +15,7 @@ at Nside = 4 (a vertex is keyed exactly by its ring and azimuth index), and
 ``ps_healpix_neighbours`` applies them to every pixel, one thread per face pixel.
 """
 import ctypes
+from functools import lru_cache
 
 import numpy as np
 import torch
@@ -43,6 +44,7 @@ def _transform(n, bits, x, y):
     return x, y
 
 
+@lru_cache(maxsize=None)
 def face_tables(n0=4):
     """(face[9][12], bits[9][12]): for each 3 x 3 cell (cx + 3 cy, cx/cy = 0 below, 1 inside,
     2 above the face) and face, the adjacent face (-1: none) and the symmetry bits
