@@ -162,6 +162,48 @@ class tauNL_utils:
         """out[X, lm] = 1/2 Sum_r (lm_map[0, r, lm] - lm_map[1, r, lm]) flXs[l, X, r] w_r  (:240-255)."""
         return self._radial(lm_map, r_weights, flXs, True)
 
+    # ---------------------------------------------------------------- local tauNL contractions
+    def _tau_tables(self):
+        if not hasattr(self, '_d_tau_L'):
+            L = self.Ls.astype(np.int64)
+            lm_L = np.where((L >= self.Lmin) & (L <= self.Lmax), L, -1).astype(np.int32)
+            self._d_tau_L = torch.as_tensor(lm_L, device=_dev())
+            self._d_tau_w = torch.as_tensor(np.where(self.Ms == 0, 1., 2.), device=_dev())
+            # position of each Ls entry in the l <= max(Ls) list (L_indices of tauNL_utils.pyx:50-62)
+            nLmax, nLmin = int(self.Ls.max()), int(self.Ls.min())
+            full = self.l_arr[self.l_arr <= nLmax]
+            self._tau_pos = np.where(lm_L >= 0, np.nonzero(full >= nLmin)[0], -1)
+        return self._d_tau_L, self._d_tau_w, self._tau_pos
+
+    def tau_sum_n0(self, _arr1, _arr2, _FLLs, _r_weights, n1):
+        """Sum over mu, (L, M) with Lmin <= L <= Lmax and (r, r') of m_w F_L(r, r') w_r w_r' Re(arr1 conj(arr2))
+        / sqrt(4 pi) / sqrt(2 n1 + 1), arrays [n_mu, len(Ls), N_r] (tauNL_utils.pyx:604-647)."""
+        lm_L, lm_w, _ = self._tau_tables()
+        a1, _ = _prep(_arr1, torch.complex128)
+        a2, _ = _prep(_arr2, torch.complex128)
+        F, _ = _prep(_FLLs, torch.float64)
+        out = 0.
+        for mu in range(a1.shape[0]):
+            out += tau_convolve_F(a2[mu].T.contiguous(), lm_L, F, _r_weights, A=a1[mu].T.contiguous(), lm_w=lm_w)
+        return out / np.sqrt(2. * n1 + 1.)
+
+    def convolve_F_n000(self, PQ, FLLs, r_weights, out, nmax_F, inds):
+        """out[i, j] = Sum_k F_L(r_inds[j], r_inds[k]) w_k PQ[ip, k] / sqrt(4 pi) for the Ls entry ip at row i of
+        the l <= nLmax list, Lmin <= L <= Lmax (tauNL_utils.pyx:966-995); out is written in place."""
+        lm_L, _, pos = self._tau_tables()
+        inds = np.asarray(inds, dtype=np.int64)
+        F = FLLs[nmax_F] if isinstance(FLLs, torch.Tensor) else np.asarray(FLLs)[nmax_F]
+        F = F[:, inds][:, :, inds]
+        d_F, _ = _prep(F, torch.float64)
+        X, _ = _prep(PQ.T if isinstance(PQ, torch.Tensor) else np.asarray(PQ).T, torch.complex128)
+        conv = tau_convolve_F(X, lm_L, d_F, np.asarray(r_weights, dtype=np.float64)[:len(inds)])
+        rows = np.nonzero(pos >= 0)[0]
+        vals = conv.T[torch.as_tensor(rows, device=conv.device)]
+        if isinstance(out, torch.Tensor):
+            out[torch.as_tensor(pos[rows], device=out.device)] = vals.to(out.device)
+        else:
+            out[pos[rows]] = vals.cpu().numpy()
+
     # ---------------------------------------------------------------- map products
     def multiply(self, map1, map2, map3):
         return _product("multiply", (map1, map2, map3), "rrr", False)
@@ -271,7 +313,39 @@ def compute_product_real_all(maps, F_maps, weights, pq_inds, F_inds, nthreads=0)
     raise ValueError("one term, or two terms of equal weight")
 
 
-compute_productP_real_all = compute_productQ_real_all = compute_product_real_all
+def compute_productP_real_all(P_map, F_PQ, weights, pq_inds, F_inds, nthreads=0):
+    """ideal_fisher.pyx:177-190: Sum_i weights[i] P_map[pq_inds[i]] Re F_PQ[F_inds[i]] ([N_r, Npix] maps;
+    one term, or two of equal weight, as the local-tauNL derivative uses)."""
+    F = F_PQ.real if (isinstance(F_PQ, torch.Tensor) and F_PQ.is_complex()) or np.iscomplexobj(F_PQ) else F_PQ
+    return compute_product_real_all(P_map, F, weights, pq_inds, F_inds)
+
+
+def compute_productQ_real_all(Q_map, F_PQ, weights, pq_inds, F_inds, mu1_index, nthreads=0):
+    """ideal_fisher.pyx:325-338: Sum_i weights[i] Q_map[pq_inds[i]] Re F_PQ[F_inds[i], mu1_index]."""
+    F = F_PQ[:, mu1_index]
+    F = F.real if (isinstance(F, torch.Tensor) and F.is_complex()) or np.iscomplexobj(F) else F
+    return compute_product_real_all(Q_map, F, weights, pq_inds, F_inds)
+
+
+def integrate_pq(flXs, P_FPQ, ls, r_weights, out, inds, nthreads=0):
+    """ideal_fisher.pyx:361-375: out[X, lm] += Sum_i 0.5 w_i flXs[ls[lm], X, inds[i]] P_FPQ[lm, i], in place
+    (out numpy or CUDA tensor), as one ps_radial_sum_lm launch."""
+    inds = np.asarray(inds, dtype=np.int64)
+    f, _ = _prep(np.asarray(flXs)[:, :, inds] if not isinstance(flXs, torch.Tensor) else flXs[:, :, inds],
+                 torch.float64)
+    m, _ = _prep(P_FPQ.T if isinstance(P_FPQ, torch.Tensor) else np.asarray(P_FPQ).T, torch.complex128)
+    d_ls, _ = _prep(np.asarray(ls, dtype=np.int32), torch.int32)
+    w = torch.as_tensor(0.5 * np.asarray(r_weights, dtype=np.float64)[:len(inds)], device=m.device)
+    lsize, npol, nr = f.shape
+    nlm = m.shape[1]
+    res = torch.empty((npol, nlm), dtype=torch.complex128, device=m.device)
+    _lib.call("ps_radial_sum_lm", ctypes.c_void_p(m.data_ptr()), 0, ctypes.c_void_p(w.data_ptr()),
+              ctypes.c_void_p(f.data_ptr()), lsize, npol, nr, ctypes.c_void_p(d_ls.data_ptr()), nlm,
+              ctypes.c_void_p(res.data_ptr()), _stream())
+    if isinstance(out, torch.Tensor):
+        out[:npol] += res.to(out.device)
+    else:
+        out[:npol] += res.cpu().numpy()
 
 
 def tau_convolve_F(X, lm_L, F, r_weights, A=None, lm_w=None):

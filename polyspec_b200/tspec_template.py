@@ -718,10 +718,10 @@ class TSpecTemplate:
         q_l^X-weighted radial sum of [P F_PQ]_lm plus p_l^X-weighted radial sum of [Q F_PQ]_lm."""
         t0 = time.time()
         w = np.asarray(r_weights, dtype=np.float64)
-        prod = pixel.compute_productP_real_all(P_maps[:, 0], F_PQ, weights, pq_inds, F_inds)
+        prod = pixel.compute_product_real_all(P_maps[:, 0], F_PQ, weights, pq_inds, F_inds)
         lm = self.base.to_lm_vec(prod, lmax=self.lmax)[:, self.d_lminfilt].contiguous()
         out = self.utils.radial_sum(lm, 0.5 * w, self.d_qlXs)
-        prod = pixel.compute_productQ_real_all(Q_maps, F_PQ, weights, pq_inds, F_inds)
+        prod = pixel.compute_product_real_all(Q_maps, F_PQ, weights, pq_inds, F_inds)
         lm = self.base.to_lm_vec(prod, lmax=self.lmax)[:, self.d_lminfilt].contiguous()
         out = out + self.utils.radial_sum(lm, 0.5 * (w / np.sqrt(4. * np.pi)), self.d_plLXs[self.nmax])
         self._timed('fish_deriv', t0)

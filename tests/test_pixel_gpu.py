@@ -196,3 +196,48 @@ def test_tau_convolve_and_sum(nr, seed):
     tau_ref = ut.tau_sum_n0(np.ascontiguousarray(A[:, filt].T)[None], np.ascontiguousarray(X[:, filt].T)[None],
                             F[0], w, 0)
     assert abs(tau - tau_ref) <= 1e-12 * abs(tau_ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nr,seed", [(6, 5), (24, 6)])
+def test_tau_reference_signatures(nr, seed):
+    """The reference-signature tauNL_utils.tau_sum_n0 / convolve_F_n000 (with a subset of radial
+    indices) and the module functions compute_productP_real_all, compute_productQ_real_all and
+    integrate_pq against the compiled reference: 1e-13 of the largest magnitude."""
+    from polyspec_b200 import pixel as P
+    T, Fm = _ref()
+    if T is None:
+        pytest.skip("oracle/_ref is not built")
+    X, A, F, w, lm_L, lm_w, filt, args = _tau_case(nr, seed)
+    ut, mine = T.tauNL_utils(*args), P.tauNL_utils(*args)
+    a1 = np.ascontiguousarray(A[:, filt].T)[None]
+    a2 = np.ascontiguousarray(X[:, filt].T)[None]
+    t_ref, t = ut.tau_sum_n0(a1, a2, F[0], w, 0), mine.tau_sum_n0(a1, a2, F[0], w, 0)
+    assert abs(t - t_ref) <= 1e-12 * abs(t_ref)
+    inds = np.arange(nr, dtype=np.int32)[::2].copy()
+    PQ = np.ascontiguousarray(a2[0][:, inds])
+    out_ref = np.zeros((len(filt), len(inds)), dtype=np.complex128)
+    out = np.zeros_like(out_ref)
+    ut.convolve_F_n000(PQ, F, w[:len(inds)].copy(), out_ref, 0, inds)
+    mine.convolve_F_n000(PQ, F, w[:len(inds)].copy(), out, 0, inds)
+    assert close(out, out_ref, 1e-13)
+    rng = np.random.default_rng(seed)
+    npix = 768
+    Pm = rng.normal(size=(2, nr, npix))
+    Fq = rng.normal(size=(3, nr, npix)) + 1j * rng.normal(size=(3, nr, npix))
+    for wts, pq, fi in (([12.], [0], [0]), ([4., 4.], [1, 0], [0, 2])):
+        wts, pq, fi = np.asarray(wts), np.asarray(pq, dtype=np.int32), np.asarray(fi, dtype=np.int32)
+        assert close(P.compute_productP_real_all(Pm, Fq, wts, pq, fi, 1),
+                     Fm.compute_productP_real_all(Pm, Fq, wts, pq, fi, 1), 1e-14)
+        assert close(P.compute_productQ_real_all(Pm, Fq[:, None], wts, pq, fi, 0, 1),
+                     Fm.compute_productQ_real_all(Pm, np.ascontiguousarray(Fq[:, None]), wts, pq, fi, 0, 1), 1e-14)
+    lmax = 15
+    from pixel_cases import lm_setup
+    ls = lm_setup(lmax)[0].astype(np.int64)
+    flX = rng.normal(size=(lmax + 1, 2, nr))
+    Pf = rng.normal(size=(len(ls), len(inds))) + 1j * rng.normal(size=(len(ls), len(inds)))
+    o_ref = np.zeros((2, len(ls)), dtype=np.complex128)
+    o = np.zeros_like(o_ref)
+    Fm.integrate_pq(flX, Pf, ls, w[:len(inds)].copy(), o_ref, inds, 1)
+    P.integrate_pq(flX, Pf, ls, w[:len(inds)].copy(), o, inds, 1)
+    assert close(o, o_ref, 1e-13)
