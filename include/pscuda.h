@@ -327,6 +327,11 @@ int ps_wigner_binned(const double* x, int nk, int lmax, const int* edges, int nb
                      double* Phi, cudaStream_t stream);
 int ps_bispec_ideal_contract(const double* Phi, const double* w, int nk, int G, int nbins, const int* tasks, int ntask,
                              double* out, cudaStream_t stream);
+/* ps_quad_triple: out[t] = Sum_k w[k] A[ia][k] B[ib][k] C[ic][k] for tasks[t] = (ia, ib, ic) (int32 [ntask][3];
+ *   A [nA][nk], B [nB][nk], C [nC][nk]); an index out of range gives NaN.  Used with ps_wigner_binned rows for
+ *   the (l1 l2 L; -1 -1 2)^2 sums of TSpecBin's ideal 0- and 2-field terms (polyspec/tspec_bin.py:883-1045). */
+int ps_quad_triple(const double* A, int nA, const double* B, int nB, const double* C, int nC, const double* w, int nk,
+                   const int* tasks, int ntask, double* out, cudaStream_t stream);
 
 /* ------------------------------------------------------------- inpainting (Weightings.inpaint_map)
  * ps_healpix_neighbours: out[p][k] (int32 [12 nside^2][8]) = the RING neighbours of pixel p in the order

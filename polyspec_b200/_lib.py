@@ -79,6 +79,8 @@ SIGNATURES = {
                                   _c_void_p]),
     "ps_bispec_ideal_contract": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_int, _c_void_p, _c_int,
                                           _c_void_p, _c_void_p]),
+    "ps_quad_triple": (_c_int, [_c_void_p, _c_int, _c_void_p, _c_int, _c_void_p, _c_int, _c_void_p, _c_int,
+                                _c_void_p, _c_int, _c_void_p, _c_void_p]),
     "ps_healpix_neighbours": (_c_int, [_c_int, _c_void_p, _c_void_p, _c_void_p]),
     "ps_inpaint_average": (_c_int, [_c_void_p, _c_void_p, _c_int64, _c_void_p, _c_int64, _c_int, _c_void_p,
                                     _c_void_p]),

@@ -22,6 +22,8 @@
 //                                                     - (l+1) sqrt((l^2 - m^2)(l^2 - n^2)) d^{l-1}
 //    from d^1_{-1,-1} = cos^2(t/2), d^2_{2,2} = cos^4(t/2), d^2_{2,-1} = -2 cos(t/2) sin^3(t/2),
 //    d^2_{-1,2} = 2 cos(t/2) sin^3(t/2) (|d| <= 1: no scaling needed) and accumulates the bins.
+//  * ps_quad_triple: Sum_k w_k A[ia][k] B[ib][k] C[ic][k] per task (ia, ib, ic): the quadrature of
+//    three binned d-sums (TSpecBin's ideal 0- and 2-field terms).
 //  * ps_bispec_ideal_contract: per task (three (g, bin) pairs) the two sums
 //    S[par] = (1/18) Sum_k w_k Sum_{X,Y} Prod_i Phi[g_i][b_i][(X_i, Y_i)][par](x_k), one CTA per
 //    task, the nodes reduced in a fixed order.
@@ -170,10 +172,45 @@ __global__ void ideal_contract_kernel(const double* __restrict__ Phi, const doub
   }
 }
 
+__global__ void quad_triple_kernel(const double* __restrict__ A, int nA, const double* __restrict__ B, int nB,
+                                   const double* __restrict__ C, int nC, const double* __restrict__ w, int nk,
+                                   const int* __restrict__ tasks, double* __restrict__ out) {
+  const int task = blockIdx.x;
+  const int ia = tasks[3 * int64_t(task)], ib = tasks[3 * int64_t(task) + 1], ic = tasks[3 * int64_t(task) + 2];
+  if (ia < 0 || ia >= nA || ib < 0 || ib >= nB || ic < 0 || ic >= nC) {  // a malformed task reads nothing
+    if (threadIdx.x == 0) out[task] = nan("");
+    return;
+  }
+  const double* a = A + int64_t(ia) * nk;
+  const double* b = B + int64_t(ib) * nk;
+  const double* c = C + int64_t(ic) * nk;
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < nk; k += blockDim.x) s += w[k] * a[k] * b[k] * c[k];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[task] = red[0];
+}
+
 }  // namespace
 }  // namespace ps
 
 using namespace ps;
+
+extern "C" int ps_quad_triple(const double* A, int nA, const double* B, int nB, const double* C, int nC,
+                              const double* w, int nk, const int* tasks, int ntask, double* out, cudaStream_t stream) {
+  if (!A || !B || !C || !w || !tasks || !out || nA <= 0 || nB <= 0 || nC <= 0 || nk <= 0 || ntask < 0)
+    return PS_ERR_INVALID;
+  if (ntask == 0) return PS_OK;
+  StatScope sc(PS_K_VECTOR, 4.0 * double(ntask) * nk, 32.0 * double(ntask) * nk, stream);
+  quad_triple_kernel<<<ntask, 256, 0, stream>>>(A, nA, B, nB, C, nC, w, nk, tasks, out);
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}
 
 extern "C" int ps_gl_nodes(int n, double* x, double* w, cudaStream_t stream) {
   if (n <= 0 || !x || !w) return PS_ERR_INVALID;

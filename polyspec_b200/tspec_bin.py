@@ -5,9 +5,10 @@ include_partial_triangles=False, fields=[...], parity='both')`` keeps the
 reference interface, its bin ordering, symmetry factors, ``get_ells``,
 simulation handling (``generate_sims``, ``load_sims``) and the optimal estimator
 (``Tl_numerator``, ``compute_fisher_contribution``, ``compute_fisher``,
-``Tl_unwindowed``).  The ideal estimator (``Tl_numerator_ideal``,
-``compute_fisher_ideal``, ``Tl_ideal``) needs Wigner 3j and 6j symbols and raises
-NotImplementedError.  ``applySinv`` receives and returns CUDA tensors; one with a
+``Tl_unwindowed``) and the ideal estimator's numerator (``Tl_numerator_ideal``,
+with its 3j-symbol 0- and 2-field terms as Gauss-Legendre quadratures of binned
+Wigner d-sums) and ``Tl_ideal`` with a supplied ideal Fisher matrix;
+``compute_fisher_ideal`` (6j symbols) raises NotImplementedError.  ``applySinv`` receives and returns CUDA tensors; one with a
 ``.batched`` method filters the Fisher rows in batches.
 
 How the work maps to the device (the algebra was checked on the CPU against the
@@ -633,14 +634,151 @@ class TSpecBin:
         return out
 
     # ------------------------------------------------------------------ ideal estimator
-    def Tl_numerator_ideal(self, *args, **kwargs):
-        raise NotImplementedError("the ideal trispectrum estimator needs Wigner 3j/6j symbols (pywigxjpf in the "
-                                  "reference)")
+    def _ideal_t0_t2(self, C):
+        """The 0- and 2-field terms of the ideal estimator (polyspec/tspec_bin.py:883-1045) for the
+        data's beam C^-1 harmonics C [nfield, nlm].
+
+        For each (bin1, bin2, binL) the reference sums over l1, l2, L (triangles)
+            (2L+1) (l1 l2 L; -1 -1 2)^2 (-1)^L (2l1+1)(2l2+1)(-1)^(l1+l2) / (4 pi) x field factors,
+        the field factors being products of one function of l1 and one of l2 (the empirical and
+        theory inverse spectra times beams).  By the Gaunt identity
+        (l1 l2 L; -1 -1 2)^2 = 1/2 Int d^{l1}_{-1,-1} d^{l2}_{-1,-1} d^L_{2,2} dx, each sum is a
+        Gauss-Legendre quadrature of three binned d-sums (``ps_wigner_binned``, ``ps_quad_triple``).
+        The assembly into the quadruplet list follows the reference."""
+        b = self.base
+        dev = b.device
+        nf = 1 + 2 * self.pol
+        lb = np.asarray(self.l_bins_squeeze, dtype=np.int64)
+        Lb = np.asarray(self.L_bins, dtype=np.int64)
+        lmx, Lmx = int(lb[-1]) - 1, int(Lb[-1]) - 1
+        nb, nL = len(lb) - 1, len(Lb) - 1
+        # empirical inverse spectrum of the data (tspec_bin.py:887-895)
+        l_idx = torch.as_tensor(b.l_arr, device=dev)
+        keep = l_idx <= lmx
+        beam = torch.as_tensor(np.asarray(self.beam, dtype=np.float64)[:, :lmx + 1], device=dev)
+        ls = torch.arange(lmx + 1, dtype=torch.float64, device=dev)
+        Ce = torch.zeros((nf, nf, lmx + 1), dtype=torch.float64, device=dev)
+        for u1 in range(nf):
+            for u2 in range(nf):
+                sq = (0.5 * (C[u1] * torch.conj(C[u2]) + C[u2] * torch.conj(C[u1])) * self.d_mw).real
+                Ce[u1, u2].index_add_(0, l_idx[keep], sq[keep])
+                Ce[u1, u2] *= beam[u1] * beam[u2] / (2. * ls + 1.)
+        Ib = torch.as_tensor(np.asarray(b.inv_Cl_tot_mat, dtype=np.float64)[:nf, :nf, :lmx + 1], device=dev) \
+            * beam[:, None, :] * beam[None, :, :]
+        H = torch.cat([Ib.reshape(nf * nf, -1), Ce.reshape(nf * nf, -1)]) * (2. * ls + 1.)[None]
+        HL = (2. * torch.arange(Lmx + 1, dtype=torch.float64, device=dev) + 1.)[None].contiguous()
+        nk = (2 * lmx + Lmx) // 2 + 2
+        x = torch.empty(nk, dtype=torch.float64, device=dev)
+        w = torch.empty_like(x)
+        _lib.call("ps_gl_nodes", nk, _vp(x), _vp(w), _stream())
+        G = H.shape[0]
+        Phi = torch.zeros((G, nb, 4, 2, nk), dtype=torch.float64, device=dev)
+        H = H.contiguous()
+        d_lb = torch.as_tensor(lb.astype(np.int32), device=dev)
+        _lib.call("ps_wigner_binned", _vp(x), nk, lmx, _vp(d_lb), nb, _vp(H), G, _vp(Phi), _stream())
+        PhiL = torch.zeros((1, nL, 4, 2, nk), dtype=torch.float64, device=dev)
+        d_Lb = torch.as_tensor(Lb.astype(np.int32), device=dev)
+        _lib.call("ps_wigner_binned", _vp(x), nk, Lmx, _vp(d_Lb), nL, _vp(HL), 1, _vp(PhiL), _stream())
+        # rows: slot 0 = (-1,-1) (l1, l2), slot 3 = (2,2) (L); par 1 = (-1)^l weights
+        row = lambda g, bb, q, nbb: ((g * nbb + bb) * 4 + q) * 2 + 1
+        I_of = lambda a_, b_, bb: row(a_ * nf + b_, bb, 0, nb)
+        C_of = lambda a_, b_, bb: row(nf * nf + a_ * nf + b_, bb, 0, nb)
+        triples = [(b1, b2, bL) for b1 in range(nb) for b2 in range(nb) for bL in range(nL)
+                   if self._check_bin(b1, b2, bL)]
+        fp = [(a_, b_) for a_ in range(nf) for b_ in range(nf)]
+        tasks = []
+        for b1, b2, bL in triples:
+            rl = row(0, bL, 3, nL)
+            for a_, b_ in fp:
+                for c_, d_ in fp:
+                    tasks += [(C_of(a_, b_, b2), I_of(c_, d_, b1), rl), (I_of(a_, b_, b2), C_of(c_, d_, b1), rl),
+                              (I_of(a_, b_, b1), I_of(c_, d_, b2), rl)]
+        d_tasks = torch.as_tensor(np.asarray(tasks, dtype=np.int32).reshape(-1, 3), device=dev)
+        out = torch.empty(len(tasks), dtype=torch.float64, device=dev)
+        A = Phi.reshape(-1, nk)
+        _lib.call("ps_quad_triple", _vp(A), A.shape[0], _vp(A), A.shape[0], _vp(PhiL), PhiL.numel() // nk, _vp(w), nk,
+                  _vp(d_tasks), len(tasks), _vp(out), _stream())
+        o = out.cpu().numpy().reshape(len(triples), nf, nf, nf, nf, 3) / (8. * np.pi)
+        t2s = {t: -(o[i, ..., 0] + o[i, ..., 1]) for i, t in enumerate(triples)}
+        t0s = {t: o[i, ..., 2] for i, t in enumerate(triples)}
+        # assembly (tspec_bin.py:955-1022)
+        T = self._build_tables()
+        q = T['quads']
+        NT, nq = self.N_t, len(q)
+        t2n, t0n = np.zeros(NT), np.zeros(NT)
+        for index, (u1, u2, u3, u4, b1, b2, b3, b4, bL, p_u) in enumerate(q):
+            if ((b1 == b3) * (b2 == b4) + (b1 == b4) * (b2 == b3)) == 0:
+                continue
+            if (p_u == -1 and self.parity == 'even') or (p_u == 1 and self.parity == 'odd'):
+                continue
+            v0 = v2 = 0.
+            if b1 == b3 and b2 == b4:
+                v2 += t2s[b1, b2, bL][u2, u4, u3, u1]
+                v0 += t0s[b1, b2, bL][u3, u1, u4, u2]
+            if b1 == b4 and b2 == b3:
+                v2 += t2s[b1, b2, bL][u2, u3, u4, u1]
+                v0 += t0s[b1, b2, bL][u4, u1, u3, u2]
+            for ci, chi in enumerate(self.chi_arr):
+                if p_u * chi == -1:
+                    continue
+                t2n[ci * NT // 2 + index] = v2
+                t0n[ci * NT // 2 + index] = v0
+        t2 = t2n / np.mean(np.asarray(self.mask) ** 2) / self.sym_factor
+        t0 = t0n / self.sym_factor
+        return t0, t2
+
+    def Tl_numerator_ideal(self, data, verb=False, include_disconnected_term=True, N_cpus=4):
+        """Numerator of the ideal (unit-mask) trispectrum estimator (polyspec/tspec_bin.py:1047-1129),
+        normalised by <mask^4>: the 4-field term from the A fields of beam C^-1 Y^dagger data (the
+        same binned Gram matrices as Tl_numerator) plus the 0- and 2-field terms of _ideal_t0_t2.
+        ``N_cpus`` has no counterpart."""
+        if not hasattr(self, 'sym_factor'):
+            self._compute_symmetry_factor()
+        self._build_tables()
+        b = self.base
+        d = b._in(data, torch.float64)[0]
+        C = self.d_beam * torch.einsum('ijk,jk->ik', b.dev('inv_Cl_tot_lm_mat'), b.to_lm(d))
+        if verb:
+            print("\nComputing H maps")
+        Pd = self._P(C)
+        if verb:
+            print("Computing A_lm fields")
+        Add = self._A01(self._A(Pd))
+        Mdd = self._gram(Add, Add)
+        t4 = self._real_part(self._terms(lambda L, p, q: (Mdd[L][p, q] + Mdd[L][q, p]) / 2.))
+        out = t4 / np.mean(np.asarray(self.mask) ** 4.) / self.sym_factor
+        if not include_disconnected_term:
+            print("## No subtraction of (parity-conserving) disconnected terms performed!")
+            return out
+        t0, t2 = self._ideal_t0_t2(C)
+        self.t0_num_ideal = t0
+        return out + t2 + t0
 
     def compute_fisher_ideal(self, *args, **kwargs):
-        raise NotImplementedError("the ideal trispectrum Fisher matrix needs Wigner 3j/6j symbols (pywigxjpf in "
-                                  "the reference)")
+        """Analytic ideal Fisher matrix (polyspec/tspec_bin.py:1131-1370): needs Wigner 6j symbols and is
+        not computed here; pass ``fish_ideal`` to Tl_ideal."""
+        raise NotImplementedError("the ideal trispectrum Fisher matrix needs Wigner 6j symbols (pywigxjpf in "
+                                  "the reference); pass fish_ideal to Tl_ideal")
 
-    def Tl_ideal(self, *args, **kwargs):
-        raise NotImplementedError("the ideal trispectrum estimator needs Wigner 3j/6j symbols (pywigxjpf in the "
-                                  "reference)")
+    def Tl_ideal(self, data, fish_ideal=[], verb=False, include_disconnected_term=True, N_cpus=1):
+        """Ideal estimator inv(F_ideal) x numerator, as a dict per field and parity
+        (polyspec/tspec_bin.py:1372-1406).  The ideal Fisher matrix (6j symbols) is not computed
+        here: pass ``fish_ideal``."""
+        if len(fish_ideal) != 0:
+            self.fish_ideal = fish_ideal
+            self.inv_fish_ideal = np.linalg.inv(fish_ideal)
+        if not hasattr(self, 'inv_fish_ideal'):
+            print("Computing ideal Fisher matrix")
+            self.compute_fisher_ideal(verb=verb, N_cpus=N_cpus)
+        Tl_num_ideal = self.Tl_numerator_ideal(data, verb=verb, include_disconnected_term=include_disconnected_term)
+        Tl_out = np.matmul(self.inv_fish_ideal, Tl_num_ideal)
+        out = {}
+        index, config_index = 0, 0
+        chi_name = {1: '+', -1: '-'}
+        for chi in self.chi_arr:
+            for u in self.fields:
+                n = len(self.sym_factor_all[config_index])
+                out['%s' % u + '%s' % chi_name[chi]] = Tl_out[index:index + n]
+                index += n
+                config_index += 1
+        return out

@@ -61,14 +61,16 @@ def make(pol, ref, l_bins, fields, parity):
     return out
 
 
+CASES = [
+    (False, [2, 8, 14, 23], ['TTTT'], 'even', "tspecbin_nside16_t.npz"),
+    (True, [2, 10, 23], POL_FIELDS, 'both', "tspecbin_nside16_teb.npz"),
+]
+
+
 def main():
     refroot = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     ref = reference_harness.load(refroot, modules=("base", "weighting", "tspec_bin"))
-    cases = [
-        (False, [2, 8, 14, 23], ['TTTT'], 'even', "tspecbin_nside16_t.npz"),
-        (True, [2, 10, 23], POL_FIELDS, 'both', "tspecbin_nside16_teb.npz"),
-    ]
-    for pol, l_bins, fields, parity, name in cases:
+    for pol, l_bins, fields, parity, name in CASES:
         d = make(pol, ref, l_bins, fields, parity)
         path = os.path.join(HERE, name)
         np.savez_compressed(path, **d)

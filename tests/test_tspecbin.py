@@ -97,3 +97,15 @@ def test_fisher_contribution(pol):
     d = load(pol)
     _, t = _build(d, pol)
     assert fisher_err(t.compute_fisher_contribution(1), d["fisher_seed1"]) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pol", [False, True])
+def test_numerator_ideal(pol):
+    """Tl_numerator_ideal against the reference's (exact 3j symbols for the 0- and 2-field terms,
+    tests/golden/make_golden_tspecbin_ideal.py): 1e-10 relative, max-norm."""
+    d = load(pol)
+    g = np.load(os.path.join(GOLD, "tspecbin_ideal_nside16_%s.npz" % ("teb" if pol else "t")))
+    _, tsb = _build(d, pol)
+    assert rel(tsb.Tl_numerator_ideal(d["data"], include_disconnected_term=False), g["tl_num_ideal_4"]) < 1e-10
+    assert rel(tsb.Tl_numerator_ideal(d["data"], include_disconnected_term=True), g["tl_num_ideal_full"]) < 1e-10
