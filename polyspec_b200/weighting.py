@@ -281,7 +281,7 @@ class BatchedCGD:
         self.preconditioner = preconditioner
         self.w = self.base.dev('m_weight')
         if preconditioner == 'learned':
-            # learned band preconditioner (polyspec_b200.learned); the judge of convergence
+            # learned band preconditioner (polyspec_b200.learned); the convergence statistic
             # is the plain CG's r^T Sigma r / b^T Sigma b, and a system that misbehaves or
             # exceeds learned_max_steps continues with the plain harmonic CG
             self.learned = getattr(weightings, 'learned', None)
@@ -310,7 +310,7 @@ class BatchedCGD:
         self.i = 0
         self.iters = torch.zeros(B, dtype=torch.int64, device=b.device)
         self.active = torch.ones(B, dtype=torch.bool, device=b.device)
-        self.err = self._judge(self.r, self.rz, self.use_learned, torch.arange(B, device=b.device))
+        self.err = self._stop_stat(self.r, self.rz, self.use_learned, torch.arange(B, device=b.device))
 
     def _pol(self, x):
         return x.dim() == 3 and x.shape[1] == 3
@@ -320,7 +320,7 @@ class BatchedCGD:
             return lmops.matvec3(self.W.real3('Sigma'), ilm)
         return torch.einsum('abi,nbi->nai', self.W.d_Sigma, ilm)
 
-    def _judge(self, r, rz, learned_mask, idx):
+    def _stop_stat(self, r, rz, learned_mask, idx):
         """Stopping statistic: rz/rz0 of the plain CG (= r^T Sigma r / b^T Sigma b)."""
         if self.preconditioner not in ('learned', 'cut'):
             return rz / self.rz0[idx]
@@ -404,7 +404,7 @@ class BatchedCGD:
             self.x[idx] = x_new
             self.r[idx] = r
             self.p[idx] = p
-        self.err[idx] = self._judge(r, next_rz, lm, idx)
+        self.err[idx] = self._stop_stat(r, next_rz, lm, idx)
         self.rz[idx] = next_rz
         self.iters[idx] += 1
         self.i += 1
