@@ -289,7 +289,7 @@ class BatchedCGD:
                 raise Exception("preconditioner='learned' needs a trained Weightings.learned")
             self.learned_max_steps = learned_max_steps
         elif preconditioner == 'cut':
-            # masked-band preconditioner (polyspec_b200.cutprec), judged like 'learned'
+            # masked-band preconditioner (polyspec_b200.cutprec), stopped like 'learned'
             self.cut = weightings.cut_preconditioner()
         b0 = self._get_b(d)
         self.x0 = x0
@@ -302,8 +302,8 @@ class BatchedCGD:
         self.rz = self.dot(self.r, z)
         if preconditioner in ('learned', 'cut'):
             # the stopping test uses Sigma whatever M is (no M b0 needed)
-            self.judge0 = self.dot(b0, self._sigma(b0))
-            self.rz0 = self.judge0
+            self.stat0 = self.dot(b0, self._sigma(b0))
+            self.rz0 = self.stat0
         else:
             self.rz0 = self.dot(b0, self._apply_M(b0, self.use_learned))
         self.p = z
@@ -324,7 +324,7 @@ class BatchedCGD:
         """Stopping statistic: rz/rz0 of the plain CG (= r^T Sigma r / b^T Sigma b)."""
         if self.preconditioner not in ('learned', 'cut'):
             return rz / self.rz0[idx]
-        return self.dot(r, self._sigma(r)) / self.judge0[idx]
+        return self.dot(r, self._sigma(r)) / self.stat0[idx]
 
     def dot(self, a, b):
         if self._pol(a):
