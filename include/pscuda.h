@@ -333,6 +333,23 @@ int ps_bispec_ideal_contract(const double* Phi, const double* w, int nk, int G, 
 int ps_quad_triple(const double* A, int nA, const double* B, int nB, const double* C, int nC, const double* w, int nk,
                    const int* tasks, int ntask, double* out, cudaStream_t stream);
 
+/* ------------------------------------------------------------- small-momentum 3j / Gaunt coefficients
+ * ps_gaunt_table: out[i] = (l1 l2 n; m1 m2 m3) (gaunt = 0) or the Gaunt coefficient
+ *   sqrt((2l1+1)(2l2+1)(2n+1)/4pi) (l1 l2 n; 0 0 0)(l1 l2 n; m1 m2 m3) (gaunt = 1, the gaunt_symbol of
+ *   polyspec/cython/tauNL_utils.pyx:1716-1718) for args[i] = (l1, l2, n, m1, m2, m3) (int32 [n][6], device),
+ *   n a small momentum (the direction-dependent tauNL orders); evaluation by short-product Racah sums. */
+int ps_gaunt_table(const int* args, int n, int gaunt, double* out, cudaStream_t stream);
+/* ps_shift_weight_map_all: the Gaunt-weighted l-shifts of polyspec/cython/tauNL_utils.pyx:407-512 as a
+ *   gather.  flX [nshift = 2 nmax + 1][lsize][npol][nr] (the p_{l,l+n}^X(r) integrals), h [npol][nsrc] complex
+ *   harmonics of the source lm list (l = src_l[s]; src_of_lm maps the m-major index of l, m <= lmax_src to a
+ *   source or -1), targets (tL, tK) the m-major list of l <= lmax_src + n; Lre, Lim complex [nr][ntarget] are
+ *   accumulated in place; weight complex; 0 <= mu <= n <= nmax.  Workspace: ps_shift_weight_workspace_bytes. */
+int ps_shift_weight_workspace_bytes(int64_t ntarget, int n, size_t* bytes);
+int ps_shift_weight_map_all(const double* flX, int nshift, int lsize, int npol, int nr, const double* h, int64_t nsrc,
+                            const int* src_l, const int* src_of_lm, int lmax_src, const int* tL, const int* tK,
+                            int64_t ntarget, int n, int mu, double weight_re, double weight_im, int nmax, double* Lre,
+                            double* Lim, void* workspace, size_t workspace_bytes, cudaStream_t stream);
+
 /* ------------------------------------------------------------- inpainting (Weightings.inpaint_map)
  * ps_healpix_neighbours: out[p][k] (int32 [12 nside^2][8]) = the RING neighbours of pixel p in the order
  *   SW, W, NW, N, NE, E, SE, S, -1 where there are only 7 -- healpy.get_all_neighbours, which

@@ -79,6 +79,12 @@ SIGNATURES = {
                                   _c_void_p]),
     "ps_bispec_ideal_contract": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_int, _c_void_p, _c_int,
                                           _c_void_p, _c_void_p]),
+    "ps_gaunt_table": (_c_int, [_c_void_p, _c_int, _c_int, _c_void_p, _c_void_p]),
+    "ps_shift_weight_workspace_bytes": (_c_int, [_c_int64, _c_int, ctypes.POINTER(_c_size_t)]),
+    "ps_shift_weight_map_all": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, _c_int, _c_void_p, _c_int64, _c_void_p,
+                                         _c_void_p, _c_int, _c_void_p, _c_void_p, _c_int64, _c_int, _c_int,
+                                         _c_double, _c_double, _c_int, _c_void_p, _c_void_p, _c_void_p, _c_size_t,
+                                         _c_void_p]),
     "ps_quad_triple": (_c_int, [_c_void_p, _c_int, _c_void_p, _c_int, _c_void_p, _c_int, _c_void_p, _c_int,
                                 _c_void_p, _c_int, _c_void_p, _c_void_p]),
     "ps_healpix_neighbours": (_c_int, [_c_int, _c_void_p, _c_void_p, _c_void_p]),

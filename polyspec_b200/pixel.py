@@ -187,6 +187,52 @@ class tauNL_utils:
             out += tau_convolve_F(a2[mu].T.contiguous(), lm_L, F, _r_weights, A=a1[mu].T.contiguous(), lm_w=lm_w)
         return out / np.sqrt(2. * n1 + 1.)
 
+    def shift_and_weight_map_all(self, flX, h_lm, n, mu, weight, Larr_real, Larr_imag, nmax):
+        """Gaunt-weighted l-shifts of the transfer-weighted harmonics (tauNL_utils.pyx:407-512):
+        Larr_real/imag [N_r, nlm(lmax + n)] += Sum over shifts Delta of the (L = l + Delta, |mu -+ m|)
+        contributions, in place; two kernels (a coefficient table per (Delta, target), then a gather
+        per (target, radial sample)) in ps_shift_weight_map_all."""
+        f, _ = _prep(flX, torch.float64)
+        h, _ = _prep(h_lm, torch.complex128)
+        nshift, lsize, npol, nr = f.shape
+        nsrc = h.shape[1]
+        lmax_src = int(self.ls.max())
+        lmax_t = lmax_src + int(n)
+        if not hasattr(self, '_sw_tables') or self._sw_tables[0] != lmax_t:
+            full_l = np.concatenate([np.arange(m, lmax_src + 1) for m in range(lmax_src + 1)])
+            full_m = np.concatenate([np.full(lmax_src + 1 - m, m) for m in range(lmax_src + 1)])
+            src_of = -np.ones(len(full_l), dtype=np.int32)
+            pos = {(int(l), int(m)): i for i, (l, m) in enumerate(zip(full_l, full_m))}
+            for i, (l, m) in enumerate(zip(self.ls, self.ms)):
+                src_of[pos[(int(l), int(m))]] = i
+            tK = np.concatenate([np.full(lmax_t + 1 - m, m) for m in range(lmax_t + 1)]).astype(np.int32)
+            tL = np.concatenate([np.arange(m, lmax_t + 1) for m in range(lmax_t + 1)]).astype(np.int32)
+            d = _dev()
+            self._sw_tables = (lmax_t, torch.as_tensor(src_of, device=d), torch.as_tensor(tL, device=d),
+                               torch.as_tensor(tK, device=d), torch.as_tensor(self.ls.astype(np.int32), device=d))
+        _, d_src_of, d_tL, d_tK, d_src_l = self._sw_tables
+        ntarget = d_tL.numel()
+        Lre, re_torch = _prep(Larr_real, torch.complex128)
+        Lim, _ = _prep(Larr_imag, torch.complex128)
+        if Lre.shape != (nr, ntarget) or Lim.shape != (nr, ntarget):
+            raise ValueError("Larr arrays must be [N_r, nlm(lmax + n)]")
+        nb = ctypes.c_size_t()
+        _lib.call("ps_shift_weight_workspace_bytes", ntarget, int(n), ctypes.byref(nb))
+        ws = torch.empty(max(int(nb.value), 8), dtype=torch.uint8, device=Lre.device)
+        w = complex(weight)
+        _lib.call("ps_shift_weight_map_all", ctypes.c_void_p(f.data_ptr()), nshift, lsize, npol, nr,
+                  ctypes.c_void_p(h.data_ptr()), nsrc, ctypes.c_void_p(d_src_l.data_ptr()),
+                  ctypes.c_void_p(d_src_of.data_ptr()), lmax_src, ctypes.c_void_p(d_tL.data_ptr()),
+                  ctypes.c_void_p(d_tK.data_ptr()), ntarget, int(n), int(mu), w.real, w.imag, int(nmax),
+                  ctypes.c_void_p(Lre.data_ptr()), ctypes.c_void_p(Lim.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
+                  int(nb.value), _stream())
+        for dst, src in ((Larr_real, Lre), (Larr_imag, Lim)):
+            if isinstance(dst, torch.Tensor):
+                if dst.data_ptr() != src.data_ptr():
+                    dst.copy_(src)
+            else:
+                dst[...] = src.cpu().numpy()
+
     def convolve_F_n000(self, PQ, FLLs, r_weights, out, nmax_F, inds):
         """out[i, j] = Sum_k F_L(r_inds[j], r_inds[k]) w_k PQ[ip, k] / sqrt(4 pi) for the Ls entry ip at row i of
         the l <= nLmax list, Lmin <= L <= Lmax (tauNL_utils.pyx:966-995); out is written in place."""

@@ -241,3 +241,32 @@ def test_tau_reference_signatures(nr, seed):
     Fm.integrate_pq(flX, Pf, ls, w[:len(inds)].copy(), o_ref, inds, 1)
     P.integrate_pq(flX, Pf, ls, w[:len(inds)].copy(), o, inds, 1)
     assert close(o, o_ref, 1e-13)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,mu,npol,lmax", [(1, 0, 1, 12), (1, 1, 2, 12), (2, 0, 2, 12), (3, 2, 2, 12), (3, 3, 1, 12),
+                                             (2, 1, 2, 60), (5, 4, 2, 40)])
+def test_shift_and_weight_map_all(n, mu, npol, lmax):
+    """Gaunt-weighted l-shifts (ps_shift_weight_map_all) against the compiled reference's
+    shift_and_weight_map_all, accumulated into non-zero arrays: 1e-13 of the largest magnitude."""
+    from polyspec_b200 import pixel as P
+    from pixel_cases import lm_setup
+    T, _ = _ref()
+    if T is None:
+        pytest.skip("oracle/_ref is not built")
+    rng = np.random.default_rng(n * 100 + mu * 10 + npol + lmax)
+    base_lmax, lmin, nmax, nr = lmax + 6, 2, max(n, 3) + 1, 3
+    l, m = lm_setup(base_lmax)
+    sel = (l >= lmin) & (l <= lmax)
+    ls, ms = l[sel].astype(np.int32), m[sel].astype(np.int32)
+    flX = rng.normal(size=(2 * nmax + 1, base_lmax + 1, npol, nr))
+    h = rng.normal(size=(npol, len(ls))) + 1j * rng.normal(size=(npol, len(ls)))
+    weight = 0.7 - 0.3j
+    nt = (lmax + n + 1) * (lmax + n + 2) // 2
+    L0 = rng.normal(size=(nr, nt)) + 1j * rng.normal(size=(nr, nt))
+    Lr, Li = L0.copy(), 2. * L0
+    args = (1, nr, l.astype(np.int32), m.astype(np.int32), 1, 2 * lmax, ls, ms, ls, ms, nmax)
+    T.tauNL_utils(*args).shift_and_weight_map_all(flX, h, n, mu, weight, Lr, Li, nmax)
+    Gr, Gi = L0.copy(), 2. * L0
+    P.tauNL_utils(*args).shift_and_weight_map_all(flX, h, n, mu, weight, Gr, Gi, nmax)
+    assert close(Gr, Lr, 1e-13) and close(Gi, Li, 1e-13)
