@@ -477,13 +477,29 @@ class TSpecTemplate:
         return out
 
     def _compute_weighted_gaunt_maps(self, h_lm_filt, flLX_arr_re, n, mu):
-        """n = mu = 0 case of polyspec/tspec_template.py:817-876 (the gNL-loc P maps)."""
-        assert n == 0 and mu == 0, "only n = 0 (gNL-loc) is implemented"
+        """P_{n,mu} maps [N_r, Npix] of polyspec/tspec_template.py:817-876 (real p_lL^X integrals):
+        n = 0 is the transfer-weighted synthesis of h / sqrt(4 pi); n > 0 sums the Gaunt-weighted
+        shifts l -> l + Delta of conj(h) (``shift_and_weight_map_all``) into real- and imaginary-part
+        harmonics up to lmax + n and combines their syntheses as re - i im (complex maps)."""
+        assert mu <= n, "mu<=n is required!"
+        assert mu >= 0, "Negative mu can be obtained by conjugation properties"
         t0 = time.time()
         nmax = len(flLX_arr_re) // 2
-        summ = self._full_lm(self.utils.apply_fl_weights(flLX_arr_re[nmax], h_lm_filt, 1. / np.sqrt(4. * np.pi)),
-                             self.lmax)
-        out = self.base.to_map_vec(summ, lmax=self.lmax)
+        if n == 0:
+            summ = self._full_lm(self.utils.apply_fl_weights(flLX_arr_re[nmax], h_lm_filt,
+                                                             1. / np.sqrt(4. * np.pi)), self.lmax)
+            out = self.base.to_map_vec(summ, lmax=self.lmax)
+        else:
+            nr = flLX_arr_re.shape[3]
+            nt = int(np.sum(self.base.l_arr <= self.lmax + n))
+            Lr = torch.zeros((nr, nt), dtype=torch.complex128, device=self._dev)
+            Li = torch.zeros_like(Lr)
+            self.utils.shift_and_weight_map_all(flLX_arr_re, h_lm_filt, n, mu, 1.0, Lr, Li, nmax)
+            if bool((Li.imag != 0.).any()):
+                out = pixel.r2cstar(self.base.to_map_vec(Lr, lmax=self.lmax + n),
+                                    self.base.to_map_vec(1.0j * Li, lmax=self.lmax + n))
+            else:
+                out = self.base.to_map_vec(Lr, lmax=self.lmax + n)
         self._timed('map_transforms', t0)
         return out
 

@@ -87,3 +87,21 @@ def test_fisher_contribution(pol):
     d = load(pol)
     _, tst = _build(d, pol)
     assert fisher_err(tst.compute_fisher_contribution(1), d["fisher_seed1"]) < TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pol", [False, True])
+def test_gaunt_maps(pol):
+    """The direction-dependent P_{n,mu} maps (n = 1, 2) of _compute_weighted_gaunt_maps against the
+    reference's (tests/golden/make_golden_tspec_gaunt.py; its Gaunt coefficients from the compiled
+    wignerSymbols): 1e-12 of the largest magnitude."""
+    import torch
+    d = load(pol)
+    g = dict(np.load(os.path.join(GOLD, "tspec_gaunt_nside16_%s.npz" % ("teb" if pol else "t"))))
+    _, tst = _build(d, pol)
+    tst.set_radial_integrals(plLXs=g["plLXs"])
+    h = torch.as_tensor(g["h_filt"], device="cuda")
+    for n in (1, 2):
+        for mu in range(n + 1):
+            got = tst._compute_weighted_gaunt_maps(h, tst.d_plLXs, n, mu).cpu().numpy()
+            assert rel_max(got, g["p%d%d" % (n, mu)]) < 1e-12, (n, mu)
