@@ -344,6 +344,21 @@ int ps_gaunt_table(const int* args, int n, int gaunt, double* out, cudaStream_t 
  *   harmonics of the source lm list (l = src_l[s]; src_of_lm maps the m-major index of l, m <= lmax_src to a
  *   source or -1), targets (tL, tK) the m-major list of l <= lmax_src + n; Lre, Lim complex [nr][ntarget] are
  *   accumulated in place; weight complex; 0 <= mu <= n <= nmax.  Workspace: ps_shift_weight_workspace_bytes. */
+/* ps_pF_map_real: out[u][i] (complex [npol][nl]) += the Gaunt-weighted gather of compute_pF_map_real
+ *   (polyspec/cython/tauNL_utils.pyx:1531-1620): inputs plus/minus complex [nlm(lmax_in)][nin], p the p_lL^X
+ *   integrals [nshift = 2 nmax + 1][lsize][npol][nrp], radial weights w [nin] and sample indices inds [nin],
+ *   sources (ls, ms) [nl].
+ * ps_product_pnmu_sym: out[t] = Sum_k w_k [Re(P[pq_k][0][t] F[f_k][0][t]) + 2 Sum_{mu=1..n1} Re(P[pq_k][mu][t]
+ *   F[f_k][mu][t])] (compute_productPnmu_sym_all, polyspec/cython/ideal_fisher.pyx:195-212), complex P, F.
+ * ps_product_q_complex: out[t] = Sum_k w_k Q[pq_k][t] F[f_k][mu1][t] (compute_productQ_complex_all,
+ *   ideal_fisher.pyx:343-357), real Q, complex F [nF][nmu][ntot], complex out. */
+int ps_pF_map_real(const double* plus, const double* minus, int lmax_in, int nin, const double* p, int nshift, int lsize,
+                   int npol, int nrp, const double* w, const int* inds, const int* ls, const int* ms, int64_t nl, int n1,
+                   int mu1, int nmax, double* out, cudaStream_t stream);
+int ps_product_pnmu_sym(const double* P, const double* F, int n1, int64_t ntot, const double* wts, const int* pq,
+                        const int* fi, int nw, double* out, cudaStream_t stream);
+int ps_product_q_complex(const double* Q, const double* F, int nmu, int mu1, int64_t ntot, const double* wts,
+                         const int* pq, const int* fi, int nw, double* out, cudaStream_t stream);
 int ps_shift_weight_workspace_bytes(int64_t ntarget, int n, size_t* bytes);
 int ps_shift_weight_map_all(const double* flX, int nshift, int lsize, int npol, int nr, const double* h, int64_t nsrc,
                             const int* src_l, const int* src_of_lm, int lmax_src, const int* tL, const int* tK,

@@ -80,6 +80,13 @@ SIGNATURES = {
     "ps_bispec_ideal_contract": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_int, _c_void_p, _c_int,
                                           _c_void_p, _c_void_p]),
     "ps_gaunt_table": (_c_int, [_c_void_p, _c_int, _c_int, _c_void_p, _c_void_p]),
+    "ps_pF_map_real": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_void_p, _c_int, _c_int, _c_int, _c_int,
+                                _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int64, _c_int, _c_int, _c_int,
+                                _c_void_p, _c_void_p]),
+    "ps_product_pnmu_sym": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int64, _c_void_p, _c_void_p, _c_void_p, _c_int,
+                                     _c_void_p, _c_void_p]),
+    "ps_product_q_complex": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_int64, _c_void_p, _c_void_p,
+                                      _c_void_p, _c_int, _c_void_p, _c_void_p]),
     "ps_shift_weight_workspace_bytes": (_c_int, [_c_int64, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_shift_weight_map_all": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, _c_int, _c_void_p, _c_int64, _c_void_p,
                                          _c_void_p, _c_int, _c_void_p, _c_void_p, _c_int64, _c_int, _c_int,

@@ -194,3 +194,150 @@ extern "C" int ps_shift_weight_map_all(const double* flX, int nshift, int lsize,
   PS_LAUNCH_CHECK();
   return PS_OK;
 }
+
+// ---------------------------------------------------------------------------------
+// compute_pF_map_real (polyspec/cython/tauNL_utils.pyx:1531-1620): out[u][i] += Sum over
+// shifts Delta (parity of n1) of the Gaunt-weighted inputs at (l + Delta, m -+ mu1) times
+// p_{l,l+Delta}^u(r_j) w_j, summed over the radial samples; a gather per (source lm, u).
+// Inputs plus/minus are complex [nlm(lmax_in)][nin] with the radial index j reading column
+// j of the inputs and sample inds[j] of p.
+namespace ps {
+namespace {
+
+__global__ void pF_map_kernel(const double2* __restrict__ plus, const double2* __restrict__ minus, int lmax_in,
+                              int nin, const double* __restrict__ p, int nshift, int lsize, int npol, int nrp,
+                              const double* __restrict__ w, const int* __restrict__ inds, const int* __restrict__ ls,
+                              const int* __restrict__ ms, int64_t nl, int n1, int mu1, int nmax,
+                              double2* __restrict__ out) {
+  const int64_t total = nl * npol;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = t % nl;
+    const int u = int(t / nl);
+    const int l = ls[i], m = ms[i];
+    double2 acc = make_double2(0., 0.);
+    for (int Delta = -n1; Delta <= n1; Delta += 2) {
+      const int lp = l + Delta;
+      if (lp > lmax_in || lp < 0) continue;
+      // i^Delta
+      const int q = ((Delta % 4) + 4) % 4;
+      const double2 iD = q == 0 ? make_double2(1., 0.) : q == 1 ? make_double2(0., 1.)
+                       : q == 2 ? make_double2(-1., 0.) : make_double2(0., -1.);
+      const double* pp = p + ((int64_t(nmax + Delta) * lsize + l) * npol + u) * nrp;
+      for (int part = 0; part < 2; ++part) {
+        if (part == 1 && mu1 == 0) break;
+        const int mp = part == 0 ? m - mu1 : m + mu1;
+        if (abs(mp) > lp) continue;
+        const int64_t idx = int64_t(abs(mp)) * (2 * lmax_in + 1 - abs(mp)) / 2 + lp;
+        double G, sgn;
+        if (part == 0) {
+          G = gaunt_small(l, lp, n1, m, -mp, -mu1);
+          sgn = (m & 1) ? -0.5 : 0.5;
+        } else {
+          G = gaunt_small(l, lp, n1, m, -mp, mu1);
+          sgn = ((n1 + mu1 + m) & 1) ? -0.5 : 0.5;
+        }
+        if (G == 0.0) continue;
+        double2 gp = make_double2(iD.x * sgn * G, iD.y * sgn * G);
+        // part 0: mp >= 0 reads plus, mp < 0 reads conj(minus) times (-1)^mp; part 1 (mp > 0) reads minus
+        const bool conj_branch = part == 0 && mp < 0;
+        const double2* src = (part == 0 && !conj_branch) ? plus : minus;
+        if (conj_branch && (mp & 1)) gp = make_double2(-gp.x, -gp.y);
+        double2 s = make_double2(0., 0.);
+        for (int j = 0; j < nin; ++j) {
+          const double wj = w[j];
+          if (wj == 0.0) continue;
+          double2 v = src[idx * nin + j];
+          if (conj_branch) v.y = -v.y;
+          const double f = pp[inds[j]] * wj;
+          s.x += v.x * f;
+          s.y += v.y * f;
+        }
+        acc.x += gp.x * s.x - gp.y * s.y;
+        acc.y += gp.x * s.y + gp.y * s.x;
+      }
+    }
+    out[int64_t(u) * nl + i].x += acc.x;
+    out[int64_t(u) * nl + i].y += acc.y;
+  }
+}
+
+// out[r][pix] = Sum_i w_i [Re(P[pq_i][0] F[f_i][0]) + 2 Sum_{mu >= 1} Re(P[pq_i][mu] F[f_i][mu])]
+// (compute_productPnmu_sym_all, ideal_fisher.pyx:195-212); P [nP][n1+1][npix_tot], F [nF][n1+1][npix_tot]
+__global__ void pnmu_sym_kernel(const double2* __restrict__ P, const double2* __restrict__ F, int n1, int64_t ntot,
+                                const double* __restrict__ wts, const int* __restrict__ pq, const int* __restrict__ fi,
+                                int nw, double* __restrict__ out) {
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < ntot; t += int64_t(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < nw; ++k) {
+      const double2* p = P + int64_t(pq[k]) * (n1 + 1) * ntot + t;
+      const double2* f = F + int64_t(fi[k]) * (n1 + 1) * ntot + t;
+      double2 a = p[0], b = f[0];
+      s += wts[k] * (a.x * b.x - a.y * b.y);
+      for (int mu = 1; mu <= n1; ++mu) {
+        a = p[int64_t(mu) * ntot];
+        b = f[int64_t(mu) * ntot];
+        s += 2. * wts[k] * (a.x * b.x - a.y * b.y);
+      }
+    }
+    out[t] = s;
+  }
+}
+
+// out[r][pix] = Sum_i w_i Q[pq_i] F[f_i][mu1] (complex; compute_productQ_complex_all, ideal_fisher.pyx:343-357)
+__global__ void q_complex_kernel(const double* __restrict__ Q, const double2* __restrict__ F, int nmu, int mu1,
+                                 int64_t ntot, const double* __restrict__ wts, const int* __restrict__ pq,
+                                 const int* __restrict__ fi, int nw, double2* __restrict__ out) {
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < ntot; t += int64_t(gridDim.x) * blockDim.x) {
+    double2 s = make_double2(0., 0.);
+    for (int k = 0; k < nw; ++k) {
+      const double q = wts[k] * Q[int64_t(pq[k]) * ntot + t];
+      const double2 f = F[(int64_t(fi[k]) * nmu + mu1) * ntot + t];
+      s.x += q * f.x;
+      s.y += q * f.y;
+    }
+    out[t] = s;
+  }
+}
+
+}  // namespace
+}  // namespace ps
+
+extern "C" int ps_pF_map_real(const double* plus, const double* minus, int lmax_in, int nin, const double* p,
+                              int nshift, int lsize, int npol, int nrp, const double* w, const int* inds,
+                              const int* ls, const int* ms, int64_t nl, int n1, int mu1, int nmax, double* out,
+                              cudaStream_t stream) {
+  if (!plus || !minus || !p || !w || !inds || !ls || !ms || !out || lmax_in < 0 || nin <= 0 || nshift != 2 * nmax + 1 ||
+      n1 < 0 || n1 > 16 || n1 > nmax || mu1 < 0 || mu1 > n1 || npol <= 0 || nl <= 0 || nrp <= 0)
+    return PS_ERR_INVALID;
+  int64_t g = (nl * npol + 127) / 128;
+  if (g > 148 * 64) g = 148 * 64;
+  pF_map_kernel<<<int(g), 128, 0, stream>>>(reinterpret_cast<const double2*>(plus),
+                                            reinterpret_cast<const double2*>(minus), lmax_in, nin, p, nshift, lsize,
+                                            npol, nrp, w, inds, ls, ms, nl, n1, mu1, nmax,
+                                            reinterpret_cast<double2*>(out));
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}
+
+extern "C" int ps_product_pnmu_sym(const double* P, const double* F, int n1, int64_t ntot, const double* wts,
+                                   const int* pq, const int* fi, int nw, double* out, cudaStream_t stream) {
+  if (!P || !F || !wts || !pq || !fi || !out || n1 < 0 || ntot <= 0 || nw <= 0) return PS_ERR_INVALID;
+  int64_t g = (ntot + 255) / 256;
+  if (g > 148 * 16) g = 148 * 16;
+  pnmu_sym_kernel<<<int(g), 256, 0, stream>>>(reinterpret_cast<const double2*>(P), reinterpret_cast<const double2*>(F),
+                                              n1, ntot, wts, pq, fi, nw, out);
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}
+
+extern "C" int ps_product_q_complex(const double* Q, const double* F, int nmu, int mu1, int64_t ntot, const double* wts,
+                                    const int* pq, const int* fi, int nw, double* out, cudaStream_t stream) {
+  if (!Q || !F || !wts || !pq || !fi || !out || nmu <= 0 || mu1 < 0 || mu1 >= nmu || ntot <= 0 || nw <= 0)
+    return PS_ERR_INVALID;
+  int64_t g = (ntot + 255) / 256;
+  if (g > 148 * 16) g = 148 * 16;
+  q_complex_kernel<<<int(g), 256, 0, stream>>>(Q, reinterpret_cast<const double2*>(F), nmu, mu1, ntot, wts, pq, fi, nw,
+                                               reinterpret_cast<double2*>(out));
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}

@@ -187,6 +187,50 @@ class tauNL_utils:
             out += tau_convolve_F(a2[mu].T.contiguous(), lm_L, F, _r_weights, A=a1[mu].T.contiguous(), lm_w=lm_w)
         return out / np.sqrt(2. * n1 + 1.)
 
+    def convolve_F_n0(self, PQ, cPQ, FLLs, r_weights, out_real, out_imag, n1, mu1, nmax_F, inds):
+        """tauNL_utils.pyx:1026-1067 (n = 0, n1 > 0): with conv = the F_L convolution of convolve_F_n000,
+        out_real = p conv(PQ) + q conv(cPQ), out_imag = p conv(PQ) - q conv(cPQ), p = (-1)^(n1-mu1) / 2 / sqrt(2n1+1),
+        q = 1 / 2 / sqrt(2n1+1), written in place at the rows of the L range."""
+        def conv(X):
+            o = torch.zeros(tuple(out_real.shape), dtype=torch.complex128, device=_dev())
+            self.convolve_F_n000(X, FLLs, r_weights, o, nmax_F, inds)
+            return o
+        a, b = conv(PQ), conv(cPQ)
+        pp = (-1.) ** (n1 - mu1) / np.sqrt(2. * n1 + 1.) / 2.
+        pm = 1. / np.sqrt(2. * n1 + 1.) / 2.
+        rows = np.nonzero(self._tau_tables()[2] >= 0)[0]
+        pos = torch.as_tensor(self._tau_tables()[2][rows], device=_dev())
+        vr, vi = (pp * a + pm * b)[pos], (pp * a - pm * b)[pos]
+        for dst, v in ((out_real, vr), (out_imag, vi)):
+            if isinstance(dst, torch.Tensor):
+                dst[pos.to(dst.device)] = v.to(dst.device)
+            else:
+                dst[self._tau_tables()[2][rows]] = v.cpu().numpy()
+
+    def compute_pF_map_real(self, _input_plus, _input_minus, _plLXs, _r_weights, n1, mu1, nmax, lmax, _output, inds):
+        """tauNL_utils.pyx:1531-1620: _output [npol, len(ls)] += the Gaunt-weighted gather of the shifted inputs
+        ([nlm(lmax), len(inds)] complex) times p_{l,l+Delta}^X(r) w_r, in place (ps_pF_map_real)."""
+        plus, _ = _prep(_input_plus, torch.complex128)
+        minus, _ = _prep(_input_minus, torch.complex128)
+        pl, _ = _prep(_plLXs, torch.float64)
+        w = torch.as_tensor(np.asarray(_r_weights, dtype=np.float64), device=plus.device)
+        ind = _i32(inds)
+        if not hasattr(self, '_d_ms'):
+            self._d_ms = torch.as_tensor(self.ms, device=_dev())
+            self._d_ls32 = torch.as_tensor(self.ls, device=_dev())
+        nshift, lsize, npol, nrp = pl.shape
+        out, _ = _prep(_output, torch.complex128)
+        _lib.call("ps_pF_map_real", ctypes.c_void_p(plus.data_ptr()), ctypes.c_void_p(minus.data_ptr()), int(lmax),
+                  plus.shape[1], ctypes.c_void_p(pl.data_ptr()), nshift, lsize, npol, nrp,
+                  ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(ind.data_ptr()),
+                  ctypes.c_void_p(self._d_ls32.data_ptr()), ctypes.c_void_p(self._d_ms.data_ptr()), len(self.ls),
+                  int(n1), int(mu1), int(nmax), ctypes.c_void_p(out.data_ptr()), _stream())
+        if isinstance(_output, torch.Tensor):
+            if _output.data_ptr() != out.data_ptr():
+                _output.copy_(out)
+        else:
+            _output[...] = out.cpu().numpy()
+
     def shift_and_weight_map_all(self, flX, h_lm, n, mu, weight, Larr_real, Larr_imag, nmax):
         """Gaunt-weighted l-shifts of the transfer-weighted harmonics (tauNL_utils.pyx:407-512):
         Larr_real/imag [N_r, nlm(lmax + n)] += Sum over shifts Delta of the (L = l + Delta, |mu -+ m|)
@@ -371,6 +415,58 @@ def compute_productQ_real_all(Q_map, F_PQ, weights, pq_inds, F_inds, mu1_index, 
     F = F_PQ[:, mu1_index]
     F = F.real if (isinstance(F, torch.Tensor) and F.is_complex()) or np.iscomplexobj(F) else F
     return compute_product_real_all(Q_map, F, weights, pq_inds, F_inds)
+
+
+def _i32(x):
+    return torch.as_tensor(np.asarray(x, dtype=np.int32), device=_dev())
+
+
+def compute_productPnmu_sym_all(Pnmu_maps, F_PQ, weights, n1, pq_inds, F_inds, nthreads=0):
+    """ideal_fisher.pyx:195-212: Sum_i w_i [Re(P[pq_i, 0] F[F_i, 0]) + 2 Sum_{mu>=1} Re(P[pq_i, mu] F[F_i, mu])]
+    for complex P [nP, n1+1, N_r, Npix] and F [nF, n1+1, N_r, Npix]; real [N_r, Npix]."""
+    P, as_torch = _prep(Pnmu_maps, torch.complex128)
+    F, _ = _prep(F_PQ, torch.complex128)
+    ntot = P.shape[2] * P.shape[3]
+    out = torch.empty(P.shape[2:], dtype=torch.float64, device=P.device)
+    w = torch.as_tensor(np.asarray(weights, dtype=np.float64), device=P.device)
+    pq, fi = _i32(pq_inds), _i32(F_inds)
+    _lib.call("ps_product_pnmu_sym", ctypes.c_void_p(P.data_ptr()), ctypes.c_void_p(F.data_ptr()), int(n1), ntot,
+              ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(pq.data_ptr()), ctypes.c_void_p(fi.data_ptr()), len(w),
+              ctypes.c_void_p(out.data_ptr()), _stream())
+    torch.cuda.current_stream().synchronize()  # the index arrays are released on return
+    return _ret(out, as_torch)
+
+
+def compute_productQ_complex_all(Q_map, F_PQ, weights, pq_inds, F_inds, mu1_index, nthreads=0):
+    """ideal_fisher.pyx:343-357: Sum_i w_i Q[pq_i] F_PQ[F_i, mu1_index] (complex [N_r, Npix])."""
+    Q, as_torch = _prep(Q_map, torch.float64)
+    F, _ = _prep(F_PQ, torch.complex128)
+    ntot = Q.shape[1] * Q.shape[2]
+    out = torch.empty(Q.shape[1:], dtype=torch.complex128, device=Q.device)
+    w = torch.as_tensor(np.asarray(weights, dtype=np.float64), device=Q.device)
+    pq, fi = _i32(pq_inds), _i32(F_inds)
+    _lib.call("ps_product_q_complex", ctypes.c_void_p(Q.data_ptr()), ctypes.c_void_p(F.data_ptr()), F.shape[1],
+              int(mu1_index), ntot, ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(pq.data_ptr()),
+              ctypes.c_void_p(fi.data_ptr()), len(w), ctypes.c_void_p(out.data_ptr()), _stream())
+    torch.cuda.current_stream().synchronize()
+    return _ret(out, as_torch)
+
+
+def complex_to_complex(map1, map2, nthreads=0):
+    """ideal_fisher.pyx:274-286: out[0] = map1^T + i map2^T, out[1] = map1^T - i map2^T ([2, n1, n0])."""
+    a, as_torch = _prep(map1, torch.complex128)
+    b, _ = _prep(map2, torch.complex128)
+    out = torch.stack([(a + 1j * b).T, (a - 1j * b).T]).contiguous()
+    return _ret(out, as_torch)
+
+
+def r2cstar_inplace(re_arr, im_arr, out_arr, mu_index, nthreads=0):
+    """ideal_fisher.pyx:42-47: out_arr[mu_index] = re - i im, in place."""
+    v = r2cstar(re_arr, im_arr)
+    if isinstance(out_arr, torch.Tensor):
+        out_arr[mu_index] = torch.as_tensor(v, device=out_arr.device)
+    else:
+        out_arr[mu_index] = v.cpu().numpy() if isinstance(v, torch.Tensor) else v
 
 
 def integrate_pq(flXs, P_FPQ, ls, r_weights, out, inds, nthreads=0):

@@ -217,9 +217,10 @@ class TSpecTemplate:
             known = t in self.all_templates or any(s in t for s in ('tauNL-direc', 'tauNL-even', 'tauNL-odd',
                                                                      'tauNL-light', 'tauNL-heavy'))
             assert known, "Unknown template %s supplied!" % t
-            if t not in SUPPORTED:
-                raise NotImplementedError("template %s is not implemented by the CUDA backend (supported: %s)"
-                                          % (t, SUPPORTED))
+            direc0 = 'tauNL-direc' in t and int(t.split(':')[1].split(',')[2]) == 0
+            if t not in SUPPORTED and not direc0:
+                raise NotImplementedError("template %s is not implemented by the CUDA backend (supported: %s and "
+                                          "tauNL-direc:n1,n1,0)" % (t, SUPPORTED))
         print("Templates: %s" % templates)
         self.ints_1d, self.ints_2d, self.ints_coll = False, False, False
         self.to_compute, self.n1n3n, self.coll_params = [], [], {}
@@ -243,6 +244,20 @@ class TSpecTemplate:
             self.to_compute.append(['q'])
             n1n3n.append([0, 0, 0])
             self.ints_1d = True
+        for t in templates:
+            if 'tauNL-direc' in t:
+                n1, n3, n = np.asarray(t.split(':')[1].split(','), dtype=int)
+                if n1 == 0 and n3 == 0 and n == 0 and 'tauNL-loc' in self.templates:
+                    raise Exception("tauNL-loc and tauNL-direc:0,0,0 are fully degenerate!")
+                if ('tauNL-direc:%d,%d,%d' % (n3, n1, n) in self.templates) and (n1 < n3):
+                    raise Exception("tauNL-direc:%d,%d,%d and tauNL-direc:%d,%d,%d are fully degenerate!"
+                                    % (n1, n3, n, n3, n1, n))
+                assert (n >= abs(n1 - n3)) and (n <= n1 + n3), \
+                    "Direction-dependent indices %d,%d,%d do not satisfy triangle conditions" % (n1, n3, n)
+                assert (n1 <= 5) and (n3 <= 5) and (n <= 5), "n>5 has not yet been implemented!"
+                self.to_compute.append(['q'])
+                n1n3n.append([int(n1), int(n3), int(n)])
+                self.ints_1d = True
         for t in templates:
             if 'lensing' in t:
                 assert len(C_phi) > 0, "Must supply lensing power spectrum!"
@@ -404,6 +419,7 @@ class TSpecTemplate:
                                        self.base.m_arr.astype(np.int32), self.Lmin, self.Lmax,
                                        self.ls.astype(np.int32), self.ms.astype(np.int32),
                                        self.Ls.astype(np.int32), self.Ms.astype(np.int32), self.nmax_F)
+        self.d_nLminfilt_idx = torch.as_tensor(np.nonzero(self.nLminfilt)[0], device=self._dev)
         if len(self.n1n3n) > 0:
             # per lm of the l <= nLmax list: L where Lmin <= L <= Lmax (else -1), and the m weight
             sel = self.base.l_arr <= self.nLmax
@@ -555,8 +571,9 @@ class TSpecTemplate:
             output['b'] = self._compute_weighted_maps(input_map, self.d_blXs)
         if 'c' in self.to_compute:
             output['c'] = self._compute_weighted_maps(input_map, self.d_clXs, spin=1)
-        if 0 in self.p_inds:
-            output['p00'] = self._compute_weighted_gaunt_maps(input_map, self.d_plLXs, 0, 0)
+        for n in self.p_inds:
+            for mu in range(n + 1):
+                output['p%d%d' % (n, mu)] = self._compute_weighted_gaunt_maps(input_map, self.d_plLXs, n, mu)
         if 'q' in self.to_compute:
             output['q'] = self._compute_weighted_maps(input_map, self.d_qlXs)
         if 'r' in self.to_compute:
@@ -570,8 +587,11 @@ class TSpecTemplate:
     def _filter_pair(self, input_maps, filtering='Q'):
         """Filtered fields of a pair of inputs (polyspec/tspec_template.py:967-1034)."""
         if filtering == 'P':
-            return {0: torch.stack([self._compute_weighted_gaunt_maps(m, self.d_plLXs, 0, 0)[None]
-                                    for m in input_maps])}
+            out = {}
+            for n in self.p_inds:
+                out[n] = torch.stack([torch.stack([self._compute_weighted_gaunt_maps(m, self.d_plLXs, n, mu)
+                                                   for mu in range(n + 1)]) for m in input_maps])
+            return out
         spin0 = {'Q': 'd_qlXs', 'R': 'd_rlXs', 'A': 'd_alXs', 'B': 'd_blXs'}
         if filtering in spin0:
             return torch.stack([self._compute_weighted_maps(m, getattr(self, spin0[filtering])) for m in input_maps])
@@ -681,18 +701,38 @@ class TSpecTemplate:
 
     # ------------------------------------------------------------------ local tauNL
     def _A_maps(self, map1, map2, n, add_sym=False):
-        """[P_00 Q]_LM for each radial sample (polyspec/tspec_template.py:1275-1300, n = 0), as
-        [1, N_r, nlm(nLmax)] over the full l <= nLmax list (entries with L < nLmin are unused);
-        optionally adding the map1 <-> map2 term."""
-        assert n == 0, "only n = 0 (tauNL-loc) is implemented"
+        """[P_{n,mu} Q]_LM for mu = -n..n and each radial sample (polyspec/tspec_template.py:1275-1334), as
+        [2n+1, N_r, nlm(nLmax)] over the full l <= nLmax list (entries with L < nLmin are unused);
+        optionally adding the map1 <-> map2 term.  mu < 0 uses conjugation, (-1)^(n+mu) conj(P_{n,-mu})."""
         t0 = time.time()
-        if add_sym:
-            prod = pixel.multiplyRR_sym(map2['q'], map1['p00'], map1['q'], map2['p00'])
-        else:
-            prod = pixel.multiplyRR(map2['q'], map1['p00'])
-        out = self.base.to_lm_vec(prod, lmax=self.nLmax)
+        if n == 0:
+            if add_sym:
+                prod = pixel.multiplyRR_sym(map2['q'], map1['p00'], map1['q'], map2['p00'])
+            else:
+                prod = pixel.multiplyRR(map2['q'], map1['p00'])
+            out = self.base.to_lm_vec(prod, lmax=self.nLmax)[None]
+            self._timed('tauNL_summation', t0)
+            return out
+        output = []
+        for mu in range(-n, n + 1):
+            key = 'p%d%d' % (n, abs(mu))
+            if mu < 0:
+                fac = (-1.) ** (n + mu)
+                if add_sym:
+                    prod = pixel.multiplyRCstar_sym(map2['q'], map1[key], map1['q'], map2[key], fac)
+                else:
+                    prod = pixel.multiplyRCstar(map2['q'], map1[key], fac)
+            else:
+                if add_sym:
+                    prod = pixel.multiplyRC_sym(map2['q'], map1[key], map1['q'], map2[key])
+                else:
+                    prod = pixel.multiplyRC(map2['q'], map1[key])
+            out = self.base.to_lm_vec(prod.real.contiguous(), lmax=self.nLmax).to(torch.complex128)
+            if bool((prod[:, 0].imag != 0).any()):
+                out = out + 1j * self.base.to_lm_vec(prod.imag.contiguous(), lmax=self.nLmax)
+            output.append(out)
         self._timed('tauNL_summation', t0)
-        return out[None]
+        return torch.stack(output)
 
     def _tau_convolve(self, X, weights, A=None):
         """pixel.tau_convolve_F over [N_r, nlm(nLmax)] harmonic maps: the F_L convolution of X
@@ -701,12 +741,15 @@ class TSpecTemplate:
                                     lm_w=self.d_tau_lm_w)
 
     def _tau_sum(self, A, B, weights, n1, n3, n):
-        """Sum over (L, M, r, r') of the local tauNL estimator (polyspec/tspec_template.py:1231-1240, n = 0)."""
-        assert n == 0 and n1 == n3 == 0, "only n1 = n3 = n = 0 (tauNL-loc) is implemented"
+        """Sum over mu, (L, M), (r, r') of the tauNL estimators for n = 0 (polyspec/tspec_template.py:1231-1240
+        and tauNL_utils.pyx:604-647): Sum_mu tau(A[n1][mu], B[n1][mu]) / sqrt(2 n1 + 1)."""
+        assert n == 0 and n1 == n3, "only n = 0 (n1 = n3) is implemented"
         t0 = time.time()
-        out = self._tau_convolve(B[n1][0], weights, A=A[n1][0])
+        out = 0.
+        for mu in range(A[n1].shape[0]):
+            out += self._tau_convolve(B[n1][mu], weights, A=A[n1][mu])
         self._timed('tauNL_summation', t0)
-        return out
+        return out / np.sqrt(2. * n1 + 1.)
 
     def _compute_PQ_vecs(self, Pn3_maps, Q_maps, i, j, n3=0, add_sym=False):
         """[P Q]_LM(r) of polyspec/tspec_template.py:1967-2010 for n3 = 0, [N_r, nlm(nLmax)]."""
@@ -747,6 +790,91 @@ class TSpecTemplate:
         """The four Q4 rows (111, 222, 112, 122) of polyspec/tspec_template.py:2521-2554."""
         rows = (([0], [0], [12.]), ([1], [1], [12.]), ([1, 0], [0, 2], [4., 4.]), ([0, 1], [1, 2], [4., 4.]))
         return torch.stack([self._Q4_contributions(P_maps, Q_maps, F_PQ, p, f, r_weights, w) for p, f, w in rows])
+
+    def _compute_PQ_vecs_n(self, Pn3_maps, Q_maps, i, j, n3, add_sym=False):
+        """[P_{n3,mu3} Q]_LM for mu3 = -n3..n3 (polyspec/tspec_template.py:1967-2010, n3 > 0), in the
+        reference's layout [2 n3 + 1, len(Ls), N_r]."""
+        nl = int(np.sum(self.nLminfilt))
+        sel = self.d_nLminfilt_idx
+        PQ = torch.zeros((2 * n3 + 1, nl, Q_maps.shape[1]), dtype=torch.complex128, device=self._dev)
+        for mu3 in range(n3 + 1):
+            if add_sym:
+                prod = pixel.multiplyRC_sym(Q_maps[j], Pn3_maps[i, mu3], Q_maps[i], Pn3_maps[j, mu3])
+            else:
+                prod = pixel.multiplyRC(Q_maps[j], Pn3_maps[i, mu3])
+            lm = lambda x: self.base.to_lm_vec(x.contiguous(), lmax=self.nLmax)[:, sel].T
+            if mu3 == 0 and n3 % 2 == 0:
+                PQ[n3] = lm(prod.real)
+            elif mu3 == 0:
+                PQ[n3] = 1.0j * lm(prod.imag)
+            else:
+                pr, pi = lm(prod.real), 1.0j * lm(prod.imag)
+                PQ[n3 + mu3] = pr + pi
+                PQ[n3 - mu3] = (-1.) ** (n3 - mu3) * (pr - pi)
+        return PQ
+
+    def _convolve_F_n(self, PQ, r_weights, n1):
+        """F_L convolution of the [P Q] vectors for n = 0, n1 = n3 > 0 (polyspec/tspec_template.py:2142-2190 with
+        convolve_F_n0): [n1 + 1, N_r, Npix] complex maps, mu1 = 0..n1."""
+        nr = PQ.shape[2]
+        inds = np.arange(nr, dtype=np.int32)
+        out = torch.zeros((n1 + 1, nr, self.base.Npix), dtype=torch.complex128, device=self._dev)
+        nfull = len(self.nLminfilt)
+        for mu1 in range(n1 + 1):
+            o_re = torch.zeros((nfull, nr), dtype=torch.complex128, device=self._dev)
+            o_im = torch.zeros_like(o_re)
+            self.utils.convolve_F_n0(PQ[n1 - mu1], PQ[n1 + mu1], self.d_FLLs, r_weights, o_re, o_im, n1, mu1,
+                                     self.nmax_F, inds)
+            if bool((o_im != 0.).any()):
+                out[mu1] = pixel.r2cstar(self.base.to_map_vec(o_re.T.contiguous(), lmax=self.nLmax),
+                                         self.base.to_map_vec((1.0j * o_im).T.contiguous(), lmax=self.nLmax))
+            else:
+                out[mu1] = self.base.to_map_vec(o_re.T.contiguous(), lmax=self.nLmax)
+        return out
+
+    def _F_PQ_n(self, Pn3_maps, Q_maps, r_weights, n1):
+        """F_L * [P_{n1,mu} Q] maps of the (1, 1), (2, 2) and symmetrised (1, 2) pairs for n = 0, n1 = n3 > 0
+        (polyspec/tspec_template.py:2287-2306): [3, n1 + 1, N_r, Npix] complex."""
+        out = []
+        for i1, i2 in ((0, 0), (1, 1), (0, 1)):
+            t0 = time.time()
+            PQ = self._compute_PQ_vecs_n(Pn3_maps, Q_maps, i1, i2, n1, add_sym=(i1 != i2))
+            out.append(self._convolve_F_n(PQ, r_weights, n1))
+            self._timed('fish_convolve', t0)
+        return torch.stack(out)
+
+    def _Q4_contributions_n(self, Pn1_maps, Q_maps, F_PQ, pq_inds, F_inds, r_weights, weights, n1):
+        """One Q4 row for n1 > 0 (polyspec/tspec_template.py:2405-2505): the q_l^X radial sum of
+        [Sum_mu P_{n1,mu} F_PQ]_lm plus, per mu1, the Gaunt-weighted p_lL^X sums of the shifted [Q F_PQ]_lm."""
+        t0 = time.time()
+        b = self.base
+        w = np.asarray(r_weights, dtype=np.float64)
+        nr = Q_maps.shape[1]
+        inds = np.arange(nr, dtype=np.int32)
+        out = torch.zeros((1 + 2 * self.pol, len(self.ls)), dtype=torch.complex128, device=self._dev)
+        prod = pixel.compute_productPnmu_sym_all(Pn1_maps, F_PQ, weights, n1, pq_inds, F_inds)
+        P_FPQ = b.to_lm_vec(prod, lmax=self.lmax)[:, self.d_lminfilt]
+        pixel.integrate_pq(self.d_qlXs, P_FPQ.T, self.ls, w, out, inds)
+        lmx = min(self.lmax + n1, b.lmax)
+        for mu1 in range(n1 + 1):
+            if bool((F_PQ[F_inds[0], mu1, :, 0].imag != 0).any()):
+                prod = pixel.compute_productQ_complex_all(Q_maps, F_PQ, weights, pq_inds, F_inds, mu1)
+                pm = pixel.complex_to_complex(b.to_lm_vec(prod.real.contiguous(), lmax=lmx),
+                                              b.to_lm_vec(prod.imag.contiguous(), lmax=lmx))
+                plus, minus = pm[0], pm[1]
+            else:
+                prod = pixel.compute_productQ_real_all(Q_maps, F_PQ, weights, pq_inds, F_inds, mu1)
+                plus = b.to_lm_vec(prod, lmax=lmx).T.contiguous()
+                minus = plus
+            self.utils.compute_pF_map_real(plus, minus, self.d_plLXs, w, n1, mu1, self.nmax, lmx, out, inds)
+        self._timed('fish_deriv', t0)
+        return out
+
+    def _get_Q4_perms_n(self, P_maps, Q_maps, F_PQ, r_weights, n1):
+        """The four Q4 rows (111, 222, 112, 122) for n1 > 0 (polyspec/tspec_template.py:2521-2554)."""
+        rows = (([0], [0], [12.]), ([1], [1], [12.]), ([1, 0], [0, 2], [4., 4.]), ([0, 1], [1, 2], [4., 4.]))
+        return torch.stack([self._Q4_contributions_n(P_maps, Q_maps, F_PQ, p, f, r_weights, w, n1)
+                            for p, f, w in rows])
 
     # ------------------------------------------------------------------ numerator
     def Tl_numerator(self, data, include_disconnected_term=True, verb=False, input_type='map'):
@@ -794,6 +922,12 @@ class TSpecTemplate:
                     A_dd[0] = self._A_maps(proc_maps, proc_maps, 0)
                 t4_num[ii] = 1. / 24. * self._tau_sum(A_dd, A_dd, self.r_weights[t], 0, 0, 0) * 12. \
                     * (4. * np.pi) ** (3. / 2.)
+            if 'tauNL-direc' in t:
+                n1, n3, n = np.asarray(t.split(':')[1].split(','), dtype=int)
+                for nn in (n1, n3):
+                    if nn not in A_dd:
+                        A_dd[nn] = self._A_maps(proc_maps, proc_maps, nn)
+                t4_num[ii] = self._tau_sum(A_dd, A_dd, self.r_weights[t], n1, n3, n) / 48. * 24.
             if t in ('gNL-con', 'gNL-dotdot', 'gNL-dotdel', 'gNL-deldel'):
                 t0 = time.time()
                 t4_num[ii] = self._gnl_shape_sum(t, proc_maps) * A_pix
@@ -820,6 +954,32 @@ class TSpecTemplate:
                     pa, pb = self.load_sim_data(isim)
                 A_aa, A_bb, A_ad, A_bd, A_ab = {}, {}, {}, {}, {}
                 for ii, t in enumerate(self.templates):
+                    if 'tauNL-direc' in t:
+                        n1, n3, n = np.asarray(t.split(':')[1].split(','), dtype=int)
+                        w = self.r_weights[t]
+                        tmp = 0.
+                        for A_xx, A_xd, px in ((A_aa, A_ad, pa), (A_bb, A_bd, pb)):
+                            for nn in np.unique([n1, n3]):
+                                if nn not in A_xx:
+                                    A_xx[nn] = self._A_maps(px, px, nn)
+                                    A_xd[nn] = self._A_maps(px, proc_maps, nn, add_sym=True)
+                            if n1 == n3:
+                                tmp += 2 * self._tau_sum(A_xx, A_dd, w, n1, n3, n)
+                            else:
+                                tmp += self._tau_sum(A_xx, A_dd, w, n1, n3, n) + self._tau_sum(A_dd, A_xx, w, n1, n3, n)
+                            tmp += self._tau_sum(A_xd, A_xd, w, n1, n3, n)
+                        t2_num[ii] += -1. / 48. * tmp * 6. / self.N_it / 2. * 4.
+                        if compute_t0:
+                            tmp = 0.
+                            for nn in np.unique([n1, n3]):
+                                if nn not in A_ab:
+                                    A_ab[nn] = self._A_maps(pa, pb, nn, add_sym=True)
+                            if n1 == n3:
+                                tmp += 2 * self._tau_sum(A_aa, A_bb, w, n1, n3, n)
+                            else:
+                                tmp += self._tau_sum(A_aa, A_bb, w, n1, n3, n) + self._tau_sum(A_bb, A_aa, w, n1, n3, n)
+                            tmp += self._tau_sum(A_ab, A_ab, w, n1, n3, n)
+                            t0_num[ii] += 1. / 48. * tmp * 3 / self.N_it * 4.
                     if t == 'tauNL-loc':
                         w = self.r_weights[t]
                         if 0 not in A_aa:
@@ -1164,6 +1324,16 @@ class TSpecTemplate:
                     w = self.r_weights[t]
                     F_vecs = self._F_PQ(P_maps[0], Q_maps, w)
                     Qs[:, ii] += (4. * np.pi) ** 1.5 * self._get_Q4_perms(P_maps[0], Q_maps, F_vecs, w)
+                    del F_vecs
+                if 'tauNL-direc' in t:
+                    n1, n3, n = np.asarray(t.split(':')[1].split(','), dtype=int)
+                    w = self.r_weights[t]
+                    if n1 == 0:
+                        F_vecs = self._F_PQ(P_maps[0], Q_maps, w)
+                        Qs[:, ii] += self._get_Q4_perms(P_maps[0], Q_maps, F_vecs, w)
+                    else:
+                        F_vecs = self._F_PQ_n(P_maps[n3], Q_maps, w, n1)
+                        Qs[:, ii] += self._get_Q4_perms_n(P_maps[n1], Q_maps, F_vecs, w, n1)
                     del F_vecs
                 if t == 'gNL-dotdel':
                     Qs[:, ii] = self._dotdel_Q(A_maps, B_maps, C_maps, self.rtau_weights[t])

@@ -1,5 +1,6 @@
-"""Generate the P_{n,mu} map fixtures (the direction-dependent tauNL filtered maps) of
-tests/golden from the UNMODIFIED reference.
+"""Generate the direction-dependent tauNL fixtures (P_{n,mu} maps; the tauNL-direc:1,1,0 and
+tauNL-direc:2,2,0 numerators and Fisher contribution) of tests/golden from the
+UNMODIFIED reference.
 
     python tests/golden/make_golden_tspec_gaunt.py [/path/to/reference]
 
@@ -8,7 +9,9 @@ tauNL-direc:1,1,0 and tauNL-direc:2,2,0 over the oracle shims of make_golden_tsp
 (so p_lL^X(r) is computed for the shifts -2..2) and saves its p_lL^X(r) integrals
 and the filtered maps P_{n,mu} (n = 1, 2; 0 <= mu <= n) of the S^-1-filtered data
 (_compute_weighted_gaunt_maps, whose Gaunt coefficients come from the reference's
-compiled wignerSymbols), for T only and for T, E, B.
+compiled wignerSymbols), the q_l^X(r) and F_L(r, r') integrals, the numerator with and
+without the disconnected terms (one simulation pair) and compute_fisher_contribution(1),
+for T only and for T, E, B.
 """
 import os
 import sys
@@ -42,10 +45,17 @@ def make(pol, ref):
                                r_weights=r_weights)
     data = base.to_map(base.generate_data(seed=5, output_type="harmonic"))
     h = np.asarray(tst.applySinv(data, input_type='map', lmax=tst.lmax)[:, tst.lminfilt], order='C')
-    out = {"plLXs": tst.plLXs, "h_filt": h}
+    out = {"plLXs": tst.plLXs, "h_filt": h, "qlXs": tst.qlXs, "FLLs": tst.FLLs, "data": data,
+           "r_values": r_values, "k_arr": k_arr, "Tl_arr": Tl, "templates": np.asarray(TEMPLATES)}
+    for t, w in r_weights.items():
+        out["r_weights_" + t] = w
     for n in (1, 2):
         for mu in range(n + 1):
             out["p%d%d" % (n, mu)] = tst._compute_weighted_gaunt_maps(h, tst.plLXs, n, mu)
+    tst.generate_sims(1)
+    out["tl_num_4"] = tst.Tl_numerator(data, include_disconnected_term=False)
+    out["tl_num_full"] = tst.Tl_numerator(data, include_disconnected_term=True)
+    out["fisher_seed1"] = tst.compute_fisher_contribution(1)
     return out
 
 
