@@ -1,6 +1,6 @@
 """Template trispectrum estimator on the GPU (mirror of polyspec/tspec_template.py)
 for the gNL-loc, gNL-con, EFTI (gNL-dotdot, gNL-dotdel, gNL-deldel), tauNL-loc,
-lensing and point-source templates.
+direction-dependent tauNL-direc:n1,n1,0, lensing and point-source templates.
 
 ``TSpecTemplate(base, mask, applySinv, templates, k_arr, Tl_arr, lmin, lmax, ...)``
 keeps the reference constructor, its checks and attributes (l- and L-ranges and
@@ -9,8 +9,8 @@ filters, ``to_compute``, ``p_inds``, ``qlXs``, ``plLXs``, ``rlXs``, ``alXs``,
 simulation handling (``generate_sims``, ``load_sims``) and the estimator methods
 (``Tl_numerator``, ``compute_fisher_contribution``, ``compute_fisher``,
 ``Tl_unwindowed``, ``report_timings``, ``reset_timings``).  The reference's
-direction-dependent tauNL and collider templates raise NotImplementedError, as do
-the radial-sampling optimisers.
+direction-dependent tauNL templates with n > 0 and its collider templates raise
+NotImplementedError, as do the radial-sampling optimisers.
 
 ``applySinv`` receives and returns CUDA tensors (as for PSpecBin/BSpecBin here);
 one with a ``.batched`` method filters the 4 x n_templates Q rows of the Fisher
