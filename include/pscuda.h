@@ -359,6 +359,22 @@ int ps_product_pnmu_sym(const double* P, const double* F, int n1, int64_t ntot, 
                         const int* fi, int nw, double* out, cudaStream_t stream);
 int ps_product_q_complex(const double* Q, const double* F, int nmu, int mu1, int64_t ntot, const double* wts,
                          const int* pq, const int* fi, int nw, double* out, cudaStream_t stream);
+/* ps_tau_sum_general: *out = tau_sum_general of polyspec/cython/tauNL_utils.pyx:650-715 for A [2n1+1][nrow][nr],
+ *   B [2n3+1][nrow][nr] (complex, rows (rowL, rowM) of the L-list, row_of_full mapping the m-major index of (L, |M|),
+ *   L <= nLmax, to a row or -1), F [2 nmax_F + 1][nLF][nr][nr], radial weights w [nr].  Workspace:
+ *   ps_tau_general_workspace_bytes.
+ * ps_convolve_F_general: convolve_F_general of tauNL_utils.pyx:1069-1180 for one mu1: out_re/out_im complex
+ *   [len(l <= nLmax)][nr] += plus +- minus at full_of_row[row] for rows with Lmin <= L <= Lmax; PQ [2n3+1][nrow][nr],
+ *   F [2 nmax_F + 1][nLF][nrF][nrF] read at the radial indices inds [nr]. */
+int ps_tau_general_workspace_bytes(int nrow, int nr, size_t* bytes);
+int ps_tau_sum_general(const double* A, const double* B, const int* row_of_full, const int* rowL, const int* rowM,
+                       int nrow, int nLmax, int Lmin, int Lmax, const double* F, int nLF, int nmax_F, const double* w,
+                       int nr, int n1, int n3, int n, double* out, void* workspace, size_t workspace_bytes,
+                       cudaStream_t stream);
+int ps_convolve_F_general(const double* PQ, const int* row_of_full, const int* rowL, const int* rowM,
+                          const int* full_of_row, int nrow, int nLmax, int Lmin, int Lmax, const double* F, int nLF,
+                          int nrF, int nmax_F, const double* w, const int* inds, int nr, int n1, int n3, int n, int mu1,
+                          double* out_re, double* out_im, cudaStream_t stream);
 int ps_shift_weight_workspace_bytes(int64_t ntarget, int n, size_t* bytes);
 int ps_shift_weight_map_all(const double* flX, int nshift, int lsize, int npol, int nr, const double* h, int64_t nsrc,
                             const int* src_l, const int* src_of_lm, int lmax_src, const int* tL, const int* tK,

@@ -341,3 +341,219 @@ extern "C" int ps_product_q_complex(const double* Q, const double* F, int nmu, i
   PS_LAUNCH_CHECK();
   return PS_OK;
 }
+
+// ---------------------------------------------------------------------------------
+// The n > 0 contractions of the direction-dependent tauNL estimators:
+//  * tau_sum_general (polyspec/cython/tauNL_utils.pyx:650-715): Sum over (Delta, mu), (L, M),
+//    mu1 and (r_j, r_k) of Re(pref * B[..][(L+Delta, -M-mu)][k] w_k A[n1+mu1][(L, M)][j]) F w_j with
+//    pref = (2 if M != 0) i^Delta Gaunt(L, L+Delta, n; M, -M-mu, mu) (n1 n3 n; mu1 mu3 mu) and the
+//    conjugate, sign-flipped B where -M-mu < 0; one thread per ((L, M), r_j), per-CTA partials
+//    summed in a fixed order.
+//  * convolve_F_general (:1069-1180): per ((L, M), r_j) the two Gaunt-weighted F convolutions
+//    of the shifted [P Q] vectors (M -> M - mu and -M - mu), accumulated as plus + minus and
+//    plus - minus at the row of (L, M) in the l <= nLmax list.
+// Arrays are [mu][row][r] over a list of (L, M) rows (rowL, rowM); row_of_full maps the m-major
+// index of (L, |M|), L <= nLmax, to its row (-1: absent).
+namespace ps {
+namespace {
+
+__device__ __forceinline__ double2 ipow(int d) {
+  const int q = ((d % 4) + 4) % 4;
+  return q == 0 ? make_double2(1., 0.) : q == 1 ? make_double2(0., 1.) : q == 2 ? make_double2(-1., 0.)
+                                                                              : make_double2(0., -1.);
+}
+__device__ __forceinline__ double2 cm(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ int64_t lm_full(int L, int M, int lmax) {
+  return int64_t(M) * (2 * lmax + 1 - M) / 2 + L;
+}
+
+__global__ void tau_general_kernel(const double2* __restrict__ A, const double2* __restrict__ B,
+                                   const int* __restrict__ row_of_full, const int* __restrict__ rowL,
+                                   const int* __restrict__ rowM, int nrow, int nLmax, int Lmin, int Lmax,
+                                   const double* __restrict__ F, int nLF, int nmax_F, const double* __restrict__ w,
+                                   int nr, int n1, int n3, int n, double* __restrict__ partial) {
+  __shared__ double red[128];
+  double acc = 0.0;
+  const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (t < int64_t(nrow) * nr) {
+    const int i = int(t / nr), j = int(t % nr);
+    const int L = rowL[i], M = rowM[i];
+    const double wj = w[j];
+    if (L >= Lmin && L <= Lmax && wj != 0.0) {
+      for (int Delta = -n; Delta <= n; ++Delta) {
+        if ((Delta + n) & 1) continue;  // the Gaunt coefficient vanishes
+        const int Lp = L + Delta;
+        if (Lp < Lmin || Lp > Lmax) continue;
+        const double* Fr = F + ((int64_t(nmax_F + Delta) * nLF + L) * nr + j) * nr;
+        for (int mu = -n; mu <= n; ++mu) {
+          const int Mp = -M - mu;
+          if (abs(Mp) > Lp) continue;
+          const double G = gaunt_small(L, Lp, n, M, -M - mu, mu);
+          if (G == 0.0) continue;
+          const double2 p1 = cm(ipow(Delta), make_double2((M != 0 ? 2.0 : 1.0) * G, 0.));
+          const int rowp = row_of_full[lm_full(Lp, abs(Mp), nLmax)];
+          if (rowp < 0) continue;
+          for (int mu1 = -n1; mu1 <= n1; ++mu1) {
+            const int mu3 = -mu1 - mu;
+            if (abs(mu3) > n3) continue;
+            double t3 = threej_small(n1, n3, n, mu1, mu3, mu);
+            if (t3 == 0.0) continue;
+            if (Mp < 0 && ((Mp + n3 + mu3) & 1)) t3 = -t3;
+            const double2* src = Mp >= 0 ? B + (int64_t(n3 + mu3) * nrow + rowp) * nr
+                                         : B + (int64_t(n3 - mu3) * nrow + rowp) * nr;
+            double2 s = make_double2(0., 0.);
+            for (int k = 0; k < nr; ++k) {
+              const double wk = w[k];
+              if (wk == 0.0) continue;
+              double2 v = src[k];
+              if (Mp < 0) v.y = -v.y;
+              const double f = Fr[k] * wk;
+              s.x += v.x * f;
+              s.y += v.y * f;
+            }
+            const double2 v = cm(make_double2(p1.x * t3, p1.y * t3), s);
+            const double2 a = A[(int64_t(n1 + mu1) * nrow + i) * nr + j];
+            acc += (v.x * a.x - v.y * a.y) * wj;
+          }
+        }
+      }
+    }
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+__global__ void sum_partials(const double* __restrict__ partial, int64_t n, double* __restrict__ out) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (int(threadIdx.x) < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0];
+}
+
+__global__ void conv_general_kernel(const double2* __restrict__ PQ, const int* __restrict__ row_of_full,
+                                    const int* __restrict__ rowL, const int* __restrict__ rowM,
+                                    const int* __restrict__ full_of_row, int nrow, int nLmax, int Lmin, int Lmax,
+                                    const double* __restrict__ F, int nLF, int nrF, int nmax_F,
+                                    const double* __restrict__ w, const int* __restrict__ inds, int nr, int n1,
+                                    int n3, int n, int mu1, double2* __restrict__ out_re,
+                                    double2* __restrict__ out_im) {
+  const int64_t total = int64_t(nrow) * nr;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+    const int i = int(t / nr), j = int(t % nr);
+    const int L = rowL[i], M = rowM[i];
+    if (L < Lmin || L > Lmax || full_of_row[i] < 0) continue;
+    double2 plus = make_double2(0., 0.), minus = plus;
+    for (int Delta = -n; Delta <= n; ++Delta) {
+      if ((Delta + n) & 1) continue;
+      const int Lp = L + Delta;
+      if (Lp < Lmin || Lp > Lmax) continue;
+      const double* Fr = F + ((int64_t(nmax_F + Delta) * nLF + L) * nrF + inds[j]) * nrF;
+      for (int mu = -n; mu <= n; ++mu) {
+        const int mu3 = -mu1 - mu;
+        if (abs(mu3) > n3) continue;
+        const double t3 = threej_small(n1, n3, n, mu1, mu3, mu);
+        if (t3 == 0.0) continue;
+        const double2 pref = make_double2(ipow(Delta).x * t3, ipow(Delta).y * t3);
+        for (int part = 0; part < 2; ++part) {
+          if (part == 1 && M == 0) break;
+          const int Mp = part == 0 ? M - mu : -M - mu;
+          if (abs(Mp) > Lp) continue;
+          double G = part == 0 ? gaunt_small(L, Lp, n, -M, M - mu, mu) : gaunt_small(L, Lp, n, M, -M - mu, mu);
+          if (G == 0.0) continue;
+          double2 g;
+          if (part == 0) {
+            const int e = Mp >= 0 ? M : (M + Mp + n3 + mu3);
+            if (e & 1) G = -G;
+            if (M != 0) G *= 0.5;
+            g = make_double2(pref.x * G, pref.y * G);
+          } else {
+            if (Mp < 0 && ((Mp + n3 + mu3) & 1)) G = -G;
+            G *= 0.5;
+            g = make_double2(pref.x * G, -pref.y * G);  // conj(pref)
+          }
+          const int rowp = row_of_full[lm_full(Lp, abs(Mp), nLmax)];
+          if (rowp < 0) continue;
+          // plus part reads PQ[n3+mu3] (Mp >= 0) or conj(PQ[n3-mu3]); minus part the conjugates of those
+          const bool conj_src = (part == 0) ? (Mp < 0) : (Mp >= 0);
+          const double2* src = (Mp >= 0 ? PQ + (int64_t(n3 + mu3) * nrow + rowp) * nr
+                                        : PQ + (int64_t(n3 - mu3) * nrow + rowp) * nr);
+          double2 s = make_double2(0., 0.);
+          for (int k = 0; k < nr; ++k) {
+            const double wk = w[k];
+            if (wk == 0.0) continue;
+            double2 v = src[k];
+            if (conj_src) v.y = -v.y;
+            const double f = Fr[inds[k]] * wk;
+            s.x += v.x * f;
+            s.y += v.y * f;
+          }
+          const double2 c = cm(s, g);
+          if (part == 0) { plus.x += c.x; plus.y += c.y; } else { minus.x += c.x; minus.y += c.y; }
+        }
+      }
+    }
+    const int64_t o = int64_t(full_of_row[i]) * nr + j;
+    out_re[o].x += plus.x + minus.x;
+    out_re[o].y += plus.y + minus.y;
+    out_im[o].x += plus.x - minus.x;
+    out_im[o].y += plus.y - minus.y;
+  }
+}
+
+}  // namespace
+}  // namespace ps
+
+extern "C" int ps_tau_general_workspace_bytes(int nrow, int nr, size_t* bytes) {
+  if (!bytes || nrow <= 0 || nr <= 0) return PS_ERR_INVALID;
+  *bytes = sizeof(double) * size_t((int64_t(nrow) * nr + 127) / 128);
+  return PS_OK;
+}
+
+extern "C" int ps_tau_sum_general(const double* A, const double* B, const int* row_of_full, const int* rowL,
+                                  const int* rowM, int nrow, int nLmax, int Lmin, int Lmax, const double* F, int nLF,
+                                  int nmax_F, const double* w, int nr, int n1, int n3, int n, double* out,
+                                  void* workspace, size_t workspace_bytes, cudaStream_t stream) {
+  if (!A || !B || !row_of_full || !rowL || !rowM || !F || !w || !out || nrow <= 0 || nr <= 0 || n < 0 || n > 16 ||
+      n1 < 0 || n1 > 16 || n3 < 0 || n3 > 16 || n > nmax_F || Lmax >= nLF || Lmax > nLmax)
+    return PS_ERR_INVALID;
+  const int64_t nblk = (int64_t(nrow) * nr + 127) / 128;
+  if (!workspace || workspace_bytes < sizeof(double) * size_t(nblk)) return PS_ERR_WORKSPACE;
+  tau_general_kernel<<<unsigned(nblk), 128, 0, stream>>>(
+      reinterpret_cast<const double2*>(A), reinterpret_cast<const double2*>(B), row_of_full, rowL, rowM, nrow, nLmax,
+      Lmin, Lmax, F, nLF, nmax_F, w, nr, n1, n3, n, static_cast<double*>(workspace));
+  PS_LAUNCH_CHECK();
+  sum_partials<<<1, 256, 0, stream>>>(static_cast<double*>(workspace), nblk, out);
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}
+
+extern "C" int ps_convolve_F_general(const double* PQ, const int* row_of_full, const int* rowL, const int* rowM,
+                                     const int* full_of_row, int nrow, int nLmax, int Lmin, int Lmax, const double* F,
+                                     int nLF, int nrF, int nmax_F, const double* w, const int* inds, int nr, int n1,
+                                     int n3, int n, int mu1, double* out_re, double* out_im, cudaStream_t stream) {
+  if (!PQ || !row_of_full || !rowL || !rowM || !full_of_row || !F || !w || !inds || !out_re || !out_im || nrow <= 0 ||
+      nr <= 0 || nrF < nr || n < 0 || n > 16 || n1 < 0 || n1 > 16 || n3 < 0 || n3 > 16 || abs(mu1) > n1 ||
+      n > nmax_F || Lmax >= nLF || Lmax > nLmax)
+    return PS_ERR_INVALID;
+  int64_t g = (int64_t(nrow) * nr + 127) / 128;
+  if (g > 148 * 64) g = 148 * 64;
+  conv_general_kernel<<<int(g), 128, 0, stream>>>(reinterpret_cast<const double2*>(PQ), row_of_full, rowL, rowM,
+                                                  full_of_row, nrow, nLmax, Lmin, Lmax, F, nLF, nrF, nmax_F, w, inds,
+                                                  nr, n1, n3, n, mu1, reinterpret_cast<double2*>(out_re),
+                                                  reinterpret_cast<double2*>(out_im));
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}

@@ -187,6 +187,77 @@ class tauNL_utils:
             out += tau_convolve_F(a2[mu].T.contiguous(), lm_L, F, _r_weights, A=a1[mu].T.contiguous(), lm_w=lm_w)
         return out / np.sqrt(2. * n1 + 1.)
 
+    def _row_tables(self):
+        if not hasattr(self, '_d_rows'):
+            d = _dev()
+            nLmax, nLmin = int(self.Ls.max()), int(self.Ls.min())
+            full_l = self.l_arr[self.l_arr <= nLmax]
+            row_of_full = -np.ones(len(full_l), dtype=np.int32)
+            row_of_full[np.nonzero(full_l >= nLmin)[0]] = np.arange(len(self.Ls), dtype=np.int32)
+            self._d_rows = (nLmax, torch.as_tensor(row_of_full, device=d),
+                            torch.as_tensor(self.Ls.astype(np.int32), device=d),
+                            torch.as_tensor(self.Ms.astype(np.int32), device=d),
+                            torch.as_tensor(self._tau_tables()[2].astype(np.int32), device=d))
+        return self._d_rows
+
+    def tau_sum_general(self, _arr1, _arr2, _FLLs, _r_weights, n1, n3, n):
+        """tauNL_utils.pyx:650-715: the (Delta, mu), (L, M), mu1, (r, r') sum of the direction-dependent tauNL
+        estimator for arrays [2n+1, len(Ls), N_r] (ps_tau_sum_general)."""
+        nLmax, row_of_full, rowL, rowM, _ = self._row_tables()
+        a1, _ = _prep(_arr1, torch.complex128)
+        a2, _ = _prep(_arr2, torch.complex128)
+        F, _ = _prep(_FLLs, torch.float64)
+        w = torch.as_tensor(np.asarray(_r_weights, dtype=np.float64), device=a1.device)
+        nrow, nr = len(self.Ls), a1.shape[-1]
+        if (tuple(a1.shape) != (2 * n1 + 1, nrow, nr) or tuple(a2.shape) != (2 * n3 + 1, nrow, nr)
+                or F.dim() != 4 or F.shape[0] % 2 != 1 or tuple(F.shape[2:]) != (nr, nr) or w.numel() != nr
+                or not 0 <= self.Lmin <= self.Lmax < F.shape[1]):
+            raise ValueError("tau_sum_general: arrays must be [2n1+1 / 2n3+1, len(Ls), N_r], FLLs "
+                             "[2 nmax_F + 1, > Lmax, N_r, N_r], r_weights [N_r]")
+        nb = ctypes.c_size_t()
+        _lib.call("ps_tau_general_workspace_bytes", nrow, nr, ctypes.byref(nb))
+        ws = torch.empty(max(int(nb.value), 8), dtype=torch.uint8, device=a1.device)
+        out = torch.zeros(1, dtype=torch.float64, device=a1.device)
+        _lib.call("ps_tau_sum_general", ctypes.c_void_p(a1.data_ptr()), ctypes.c_void_p(a2.data_ptr()),
+                  ctypes.c_void_p(row_of_full.data_ptr()), ctypes.c_void_p(rowL.data_ptr()),
+                  ctypes.c_void_p(rowM.data_ptr()), nrow, nLmax, self.Lmin, self.Lmax, ctypes.c_void_p(F.data_ptr()),
+                  F.shape[1], (F.shape[0] - 1) // 2, ctypes.c_void_p(w.data_ptr()), nr, int(n1), int(n3), int(n),
+                  ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), int(nb.value), _stream())
+        return float(out.item())
+
+    def convolve_F_general(self, _PQ, _FLLs, _r_weights, out_real, out_imag, n1, n3, n, mu1, inds):
+        """tauNL_utils.pyx:1069-1180: the Gaunt-weighted F convolutions for one mu1, accumulated in place into
+        out_real / out_imag [len(l <= nLmax), len(inds)] (ps_convolve_F_general)."""
+        nLmax, row_of_full, rowL, rowM, full_of_row = self._row_tables()
+        PQ, _ = _prep(_PQ, torch.complex128)
+        F, _ = _prep(_FLLs, torch.float64)
+        w = torch.as_tensor(np.asarray(_r_weights, dtype=np.float64), device=PQ.device)
+        ind = _i32(inds)
+        o_re, _ = _prep(out_real, torch.complex128)
+        o_im, _ = _prep(out_imag, torch.complex128)
+        nr, nfull = len(inds), int(np.sum(self.l_arr <= nLmax))
+        ia = np.asarray(inds)
+        if (tuple(PQ.shape) != (2 * n3 + 1, len(self.Ls), nr) or F.dim() != 4 or F.shape[0] % 2 != 1
+                or F.shape[2] != F.shape[3] or (nr and (ia.min() < 0 or ia.max() >= F.shape[2]))
+                or w.numel() < nr or tuple(o_re.shape) != (nfull, nr) or tuple(o_im.shape) != (nfull, nr)
+                or not 0 <= self.Lmin <= self.Lmax < F.shape[1] or abs(mu1) > n1):
+            raise ValueError("convolve_F_general: PQ [2n3+1, len(Ls), len(inds)], FLLs [2 nmax_F + 1, > Lmax, "
+                             "N_r, N_r] with inds < N_r, outputs [len(l <= max(Ls)), len(inds)], |mu1| <= n1")
+        if nr == 0:
+            return
+        _lib.call("ps_convolve_F_general", ctypes.c_void_p(PQ.data_ptr()), ctypes.c_void_p(row_of_full.data_ptr()),
+                  ctypes.c_void_p(rowL.data_ptr()), ctypes.c_void_p(rowM.data_ptr()),
+                  ctypes.c_void_p(full_of_row.data_ptr()), PQ.shape[1], nLmax, self.Lmin, self.Lmax,
+                  ctypes.c_void_p(F.data_ptr()), F.shape[1], F.shape[2], (F.shape[0] - 1) // 2,
+                  ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(ind.data_ptr()), len(inds), int(n1), int(n3), int(n),
+                  int(mu1), ctypes.c_void_p(o_re.data_ptr()), ctypes.c_void_p(o_im.data_ptr()), _stream())
+        for dst, src in ((out_real, o_re), (out_imag, o_im)):
+            if isinstance(dst, torch.Tensor):
+                if dst.data_ptr() != src.data_ptr():
+                    dst.copy_(src)
+            else:
+                dst[...] = src.cpu().numpy()
+
     def convolve_F_n0(self, PQ, cPQ, FLLs, r_weights, out_real, out_imag, n1, mu1, nmax_F, inds):
         """tauNL_utils.pyx:1026-1067 (n = 0, n1 > 0): with conv = the F_L convolution of convolve_F_n000,
         out_real = p conv(PQ) + q conv(cPQ), out_imag = p conv(PQ) - q conv(cPQ), p = (-1)^(n1-mu1) / 2 / sqrt(2n1+1),

@@ -1,6 +1,6 @@
 """Template trispectrum estimator on the GPU (mirror of polyspec/tspec_template.py)
 for the gNL-loc, gNL-con, EFTI (gNL-dotdot, gNL-dotdel, gNL-deldel), tauNL-loc,
-direction-dependent tauNL-direc:n1,n1,0, lensing and point-source templates.
+direction-dependent tauNL-direc:n1,n3,n, lensing and point-source templates.
 
 ``TSpecTemplate(base, mask, applySinv, templates, k_arr, Tl_arr, lmin, lmax, ...)``
 keeps the reference constructor, its checks and attributes (l- and L-ranges and
@@ -9,8 +9,8 @@ filters, ``to_compute``, ``p_inds``, ``qlXs``, ``plLXs``, ``rlXs``, ``alXs``,
 simulation handling (``generate_sims``, ``load_sims``) and the estimator methods
 (``Tl_numerator``, ``compute_fisher_contribution``, ``compute_fisher``,
 ``Tl_unwindowed``, ``report_timings``, ``reset_timings``).  The reference's
-direction-dependent tauNL templates with n > 0 and its collider templates raise
-NotImplementedError, as do the radial-sampling optimisers.
+tauNL-even/odd combinations and its collider templates raise NotImplementedError,
+as do the radial-sampling optimisers.
 
 ``applySinv`` receives and returns CUDA tensors (as for PSpecBin/BSpecBin here);
 one with a ``.batched`` method filters the 4 x n_templates Q rows of the Fisher
@@ -217,10 +217,9 @@ class TSpecTemplate:
             known = t in self.all_templates or any(s in t for s in ('tauNL-direc', 'tauNL-even', 'tauNL-odd',
                                                                      'tauNL-light', 'tauNL-heavy'))
             assert known, "Unknown template %s supplied!" % t
-            direc0 = 'tauNL-direc' in t and int(t.split(':')[1].split(',')[2]) == 0
-            if t not in SUPPORTED and not direc0:
+            if t not in SUPPORTED and 'tauNL-direc' not in t:
                 raise NotImplementedError("template %s is not implemented by the CUDA backend (supported: %s and "
-                                          "tauNL-direc:n1,n1,0)" % (t, SUPPORTED))
+                                          "tauNL-direc:n1,n3,n)" % (t, SUPPORTED))
         print("Templates: %s" % templates)
         self.ints_1d, self.ints_2d, self.ints_coll = False, False, False
         self.to_compute, self.n1n3n, self.coll_params = [], [], {}
@@ -741,15 +740,23 @@ class TSpecTemplate:
                                     lm_w=self.d_tau_lm_w)
 
     def _tau_sum(self, A, B, weights, n1, n3, n):
-        """Sum over mu, (L, M), (r, r') of the tauNL estimators for n = 0 (polyspec/tspec_template.py:1231-1240
-        and tauNL_utils.pyx:604-647): Sum_mu tau(A[n1][mu], B[n1][mu]) / sqrt(2 n1 + 1)."""
-        assert n == 0 and n1 == n3, "only n = 0 (n1 = n3) is implemented"
+        """Sum over mu1, mu3, mu, (L, M), (L', M'), (r, r') of the tauNL estimators
+        (polyspec/tspec_template.py:1231-1240).  n = 0 (n1 = n3): Sum_mu tau(A[n1][mu], B[n1][mu]) / sqrt(2 n1 + 1)
+        (tauNL_utils.pyx:604-647); n > 0: the Gaunt- and 3j-weighted sum of tauNL_utils.pyx:650-715 over the
+        A[n1], B[n3] maps in the reference's [2n+1, len(Ls), N_r] layout."""
         t0 = time.time()
-        out = 0.
-        for mu in range(A[n1].shape[0]):
-            out += self._tau_convolve(B[n1][mu], weights, A=A[n1][mu])
+        if n == 0:
+            assert n1 == n3
+            out = 0.
+            for mu in range(A[n1].shape[0]):
+                out += self._tau_convolve(B[n1][mu], weights, A=A[n1][mu])
+            out /= np.sqrt(2. * n1 + 1.)
+        else:
+            def rows(X):
+                return X[:, :, self.d_nLminfilt_idx].permute(0, 2, 1).contiguous()
+            out = self.utils.tau_sum_general(rows(A[n1]), rows(B[n3]), self.d_FLLs, weights, n1, n3, n)
         self._timed('tauNL_summation', t0)
-        return out / np.sqrt(2. * n1 + 1.)
+        return out
 
     def _compute_PQ_vecs(self, Pn3_maps, Q_maps, i, j, n3=0, add_sym=False):
         """[P Q]_LM(r) of polyspec/tspec_template.py:1967-2010 for n3 = 0, [N_r, nlm(nLmax)]."""
@@ -796,6 +803,12 @@ class TSpecTemplate:
         reference's layout [2 n3 + 1, len(Ls), N_r]."""
         nl = int(np.sum(self.nLminfilt))
         sel = self.d_nLminfilt_idx
+        if n3 == 0:
+            if add_sym:
+                prod = pixel.multiplyRR_sym(Q_maps[j], Pn3_maps[i, 0], Q_maps[i], Pn3_maps[j, 0])
+            else:
+                prod = pixel.multiplyRR(Q_maps[j], Pn3_maps[i, 0])
+            return self.base.to_lm_vec(prod, lmax=self.nLmax)[:, sel].T[None].contiguous()
         PQ = torch.zeros((2 * n3 + 1, nl, Q_maps.shape[1]), dtype=torch.complex128, device=self._dev)
         for mu3 in range(n3 + 1):
             if add_sym:
@@ -813,9 +826,10 @@ class TSpecTemplate:
                 PQ[n3 - mu3] = (-1.) ** (n3 - mu3) * (pr - pi)
         return PQ
 
-    def _convolve_F_n(self, PQ, r_weights, n1):
-        """F_L convolution of the [P Q] vectors for n = 0, n1 = n3 > 0 (polyspec/tspec_template.py:2142-2190 with
-        convolve_F_n0): [n1 + 1, N_r, Npix] complex maps, mu1 = 0..n1."""
+    def _convolve_F_n(self, PQ, r_weights, n1, n3=None, n=0):
+        """F convolution of the [P_{n3} Q] vectors (polyspec/tspec_template.py:2142-2190): convolve_F_n0 for n = 0
+        (n1 = n3), convolve_F_general otherwise; [n1 + 1, N_r, Npix] complex maps, mu1 = 0..n1."""
+        n3 = n1 if n3 is None else n3
         nr = PQ.shape[2]
         inds = np.arange(nr, dtype=np.int32)
         out = torch.zeros((n1 + 1, nr, self.base.Npix), dtype=torch.complex128, device=self._dev)
@@ -823,8 +837,11 @@ class TSpecTemplate:
         for mu1 in range(n1 + 1):
             o_re = torch.zeros((nfull, nr), dtype=torch.complex128, device=self._dev)
             o_im = torch.zeros_like(o_re)
-            self.utils.convolve_F_n0(PQ[n1 - mu1], PQ[n1 + mu1], self.d_FLLs, r_weights, o_re, o_im, n1, mu1,
-                                     self.nmax_F, inds)
+            if n == 0:
+                self.utils.convolve_F_n0(PQ[n1 - mu1], PQ[n1 + mu1], self.d_FLLs, r_weights, o_re, o_im, n1, mu1,
+                                         self.nmax_F, inds)
+            else:
+                self.utils.convolve_F_general(PQ, self.d_FLLs, r_weights, o_re, o_im, n1, n3, n, mu1, inds)
             if bool((o_im != 0.).any()):
                 out[mu1] = pixel.r2cstar(self.base.to_map_vec(o_re.T.contiguous(), lmax=self.nLmax),
                                          self.base.to_map_vec((1.0j * o_im).T.contiguous(), lmax=self.nLmax))
@@ -832,14 +849,15 @@ class TSpecTemplate:
                 out[mu1] = self.base.to_map_vec(o_re.T.contiguous(), lmax=self.nLmax)
         return out
 
-    def _F_PQ_n(self, Pn3_maps, Q_maps, r_weights, n1):
-        """F_L * [P_{n1,mu} Q] maps of the (1, 1), (2, 2) and symmetrised (1, 2) pairs for n = 0, n1 = n3 > 0
-        (polyspec/tspec_template.py:2287-2306): [3, n1 + 1, N_r, Npix] complex."""
+    def _F_PQ_n(self, Pn3_maps, Q_maps, r_weights, n1, n3=None, n=0):
+        """F * [P_{n3,mu} Q] maps of the (1, 1), (2, 2) and symmetrised (1, 2) pairs for (n1, n3, n) other than
+        (0, 0, 0) (polyspec/tspec_template.py:2287-2306): [3, n1 + 1, N_r, Npix] complex."""
+        n3 = n1 if n3 is None else n3
         out = []
         for i1, i2 in ((0, 0), (1, 1), (0, 1)):
             t0 = time.time()
-            PQ = self._compute_PQ_vecs_n(Pn3_maps, Q_maps, i1, i2, n1, add_sym=(i1 != i2))
-            out.append(self._convolve_F_n(PQ, r_weights, n1))
+            PQ = self._compute_PQ_vecs_n(Pn3_maps, Q_maps, i1, i2, n3, add_sym=(i1 != i2))
+            out.append(self._convolve_F_n(PQ, r_weights, n1, n3, n))
             self._timed('fish_convolve', t0)
         return torch.stack(out)
 
@@ -1328,13 +1346,20 @@ class TSpecTemplate:
                 if 'tauNL-direc' in t:
                     n1, n3, n = np.asarray(t.split(':')[1].split(','), dtype=int)
                     w = self.r_weights[t]
-                    if n1 == 0:
-                        F_vecs = self._F_PQ(P_maps[0], Q_maps, w)
-                        Qs[:, ii] += self._get_Q4_perms(P_maps[0], Q_maps, F_vecs, w)
-                    else:
-                        F_vecs = self._F_PQ_n(P_maps[n3], Q_maps, w, n1)
-                        Qs[:, ii] += self._get_Q4_perms_n(P_maps[n1], Q_maps, F_vecs, w, n1)
-                    del F_vecs
+                    # polyspec/tspec_template.py:2850-2862: n1 != n3 adds both orderings, symmetrised
+                    parts = [(n1, n3, 1.)] if n1 == n3 else [(n1, n3, 0.5), (n3, n1, 0.5 * (-1.) ** (n1 + n3))]
+                    for a, c, wt in parts:
+                        if a == 0 and c == 0:
+                            F_vecs = self._F_PQ(P_maps[0], Q_maps, w)
+                            Qs[:, ii] += wt * self._get_Q4_perms(P_maps[0], Q_maps, F_vecs, w)
+                        elif a == 0:
+                            # the n1 = 0 rows read the real part of the mu1 = 0 F maps (ideal_fisher.pyx:177, :325)
+                            F_vecs = self._F_PQ_n(P_maps[c], Q_maps, w, a, c, n)
+                            Qs[:, ii] += wt * self._get_Q4_perms(P_maps[0], Q_maps, F_vecs[:, 0].real.contiguous(), w)
+                        else:
+                            F_vecs = self._F_PQ_n(P_maps[c], Q_maps, w, a, c, n)
+                            Qs[:, ii] += wt * self._get_Q4_perms_n(P_maps[a], Q_maps, F_vecs, w, a)
+                        del F_vecs
                 if t == 'gNL-dotdel':
                     Qs[:, ii] = self._dotdel_Q(A_maps, B_maps, C_maps, self.rtau_weights[t])
                 if t == 'gNL-deldel':

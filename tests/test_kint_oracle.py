@@ -81,3 +81,32 @@ def test_F_integral_hypergeometric_against_mpmath():
             exact = float(pf * mpmath.hyp2f1(i1, i2, i3, (mpmath.mpf(ri) / rj) ** 2) * (mpmath.mpf(ri) / rj) ** L
                           * mpmath.mpf(rj) ** (1 - ns))
             assert abs(F[0, L, i, j] - exact) <= 1e-11 * abs(exact), (L, i, j)
+
+
+def test_F_integral_shifted_against_mpmath():
+    """The oracle's F_{L,L+n}(r, r') for n = -2..2 (nmax_F = 2, the direction-dependent tauNL
+    fixture's radial grid and L range) against its closed form with mpmath's 2F1 at 40 digits,
+    for r <= r' (argument r^2/r'^2, power L) and r > r' (argument r'^2/r^2, power L + n)."""
+    import mpmath
+    from oracle.shims import k_integrals as ki
+    d = dict(np.load(os.path.join(GOLD, "tspec_direc_nside16_t.npz")))
+    r = d["r_values"]
+    ns, As, kp = 0.96, 2.1e-9, 0.05
+    pref = 2. * np.pi ** 2 * As / kp ** (ns - 1)
+    F = np.zeros_like(d["FLLs"])
+    ki.compute_F_integral(r, F, 2, 40, 2, ns, pref, 1)
+    assert np.abs(F - d["FLLs"]).max() <= 1e-14 * np.abs(d["FLLs"]).max()
+    mpmath.mp.dps = 40
+    for n in (-2, -1, 1, 2):
+        for L in (3, 9, 33):  # the reference leaves F = 0 where L + n < 1
+            for i, j in ((0, 0), (0, 3), (4, 1)):
+                ri, rj = mpmath.mpf(r[i]), mpmath.mpf(r[j])
+                i1 = L + (n - 1. + ns) / 2.
+                if ri <= rj:
+                    i2, i3, x, pw, big = (ns - 2 - n) / 2., L + 1.5, (ri / rj) ** 2, (ri / rj) ** L, rj
+                else:
+                    i2, i3, x, pw, big = (ns - 2 + n) / 2., L + n + 1.5, (rj / ri) ** 2, (rj / ri) ** (L + n), ri
+                pf = 2. ** (ns - 3) * pref * mpmath.exp(mpmath.loggamma(i1) - mpmath.loggamma(1 - i2)
+                                                        - mpmath.loggamma(i3))
+                exact = float(pf * mpmath.hyp2f1(i1, i2, i3, x) * pw * big ** (1 - ns))
+                assert abs(F[2 + n, L, i, j] - exact) <= 1e-11 * abs(exact), (n, L, i, j)

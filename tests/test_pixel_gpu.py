@@ -270,3 +270,46 @@ def test_shift_and_weight_map_all(n, mu, npol, lmax):
     Gr, Gi = L0.copy(), 2. * L0
     P.tauNL_utils(*args).shift_and_weight_map_all(flX, h, n, mu, weight, Gr, Gi, nmax)
     assert close(Gr, Lr, 1e-13) and close(Gi, Li, 1e-13)
+
+
+def _general_case(nr, nmax_F, seed, lmax_L=11, Lmin=2, Lmax=9):
+    from pixel_cases import lm_setup
+    rng = np.random.default_rng(seed)
+    l, m = lm_setup(lmax_L + 4)
+    sel = (l >= 1) & (l <= lmax_L)
+    Ls, Ms = l[sel].astype(np.int32), m[sel].astype(np.int32)
+    F = rng.normal(size=(2 * nmax_F + 1, Lmax + 3, nr, nr))
+    w = rng.uniform(0.5, 1.5, size=nr)
+    w[nr // 2] = 0.
+    args = (1, nr, l.astype(np.int32), m.astype(np.int32), Lmin, Lmax, Ls, Ms, Ls, Ms, nmax_F)
+    return rng, Ls, F, w, args, int(np.sum(l <= lmax_L))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n1,n3,n", [(1, 1, 0), (1, 1, 2), (1, 2, 1), (2, 1, 3), (2, 2, 2), (3, 2, 1)])
+def test_tau_general(n1, n3, n):
+    """tauNL_utils.tau_sum_general and convolve_F_general (every mu1, a subset of radial indices,
+    accumulated into non-zero outputs) against the compiled reference: 1e-12 relative for the sum,
+    1e-13 of the largest magnitude for the convolutions."""
+    from polyspec_b200 import pixel as P
+    T, _ = _ref()
+    if T is None:
+        pytest.skip("oracle/_ref is not built")
+    nr = 5
+    rng, Ls, F, w, args, nfull = _general_case(nr, max(n, 3), 100 * n1 + 10 * n3 + n)
+    ut, mine = T.tauNL_utils(*args), P.tauNL_utils(*args)
+
+    def cplx(*shape):
+        return rng.normal(size=shape) + 1j * rng.normal(size=shape)
+
+    a1, a2 = cplx(2 * n1 + 1, len(Ls), nr), cplx(2 * n3 + 1, len(Ls), nr)
+    t_ref, t = ut.tau_sum_general(a1, a2, F, w, n1, n3, n), mine.tau_sum_general(a1, a2, F, w, n1, n3, n)
+    assert abs(t - t_ref) <= 1e-12 * max(abs(t_ref), 1e-300), (t, t_ref)
+    inds = np.array([0, 2, 3, 4], dtype=np.int32)
+    PQ = cplx(2 * n3 + 1, len(Ls), len(inds))
+    for mu1 in range(-n1, n1 + 1):
+        o0r, o0i = cplx(nfull, len(inds)), cplx(nfull, len(inds))
+        rr, ri, gr, gi = o0r.copy(), o0i.copy(), o0r.copy(), o0i.copy()
+        ut.convolve_F_general(PQ, F, w[:len(inds)].copy(), rr, ri, n1, n3, n, mu1, inds)
+        mine.convolve_F_general(PQ, F, w[:len(inds)].copy(), gr, gi, n1, n3, n, mu1, inds)
+        assert close(gr - o0r, rr - o0r, 1e-13) and close(gi - o0i, ri - o0i, 1e-13)

@@ -1,9 +1,10 @@
-"""TSpecTemplate for the direction-dependent tauNL templates with n = 0
-(tauNL-direc:1,1,0 and tauNL-direc:2,2,0, together) against golden fixtures made by
-the unmodified reference (tests/golden/make_golden_tspec_gaunt.py; its Gaunt and 3j
-symbols from the compiled wignerSymbols).  The k-space and F integrals are injected
-from the fixture.  Numerators and Fisher entries to 1e-9, relative per entry (a
-Fisher entry is compared with sqrt(F_ii F_jj))."""
+"""TSpecTemplate for the direction-dependent tauNL templates against golden fixtures made
+by the unmodified reference (its Gaunt and 3j symbols from the compiled wignerSymbols):
+n = 0 (tauNL-direc:1,1,0 and tauNL-direc:2,2,0 together, make_golden_tspec_gaunt.py) and
+general (n1, n3, n) (tauNL-direc:1,1,2, tauNL-direc:1,2,1 and tauNL-direc:0,1,1 together,
+L in [2, 40], make_golden_tspec_direc.py).  The k-space and F integrals are injected from
+the fixture.  Numerators and Fisher entries to 1e-9, relative per entry (a Fisher entry is
+compared with sqrt(F_ii F_jj))."""
 import os
 
 import numpy as np
@@ -15,15 +16,18 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 TOL = 1e-9
 
 
-def load(pol):
-    return dict(np.load(os.path.join(GOLD, "tspec_gaunt_nside16_%s.npz" % ("teb" if pol else "t"))))
+FIXTURES = {"n0": ("tspec_gaunt", {}), "general": ("tspec_direc", {"Lmin": 2, "Lmax": 40})}
 
 
-def _build(pol):
+def load(pol, kind="n0"):
+    return dict(np.load(os.path.join(GOLD, "%s_nside16_%s.npz" % (FIXTURES[kind][0], "teb" if pol else "t"))))
+
+
+def _build(pol, kind="n0"):
     import torch
     from polyspec_b200 import PolySpec, Weightings
     from polyspec_b200.tspec_template import TSpecTemplate
-    d = load(pol)
+    d = load(pol, kind)
     base_d = dict(np.load(os.path.join(GOLD, "tspec_tauloc_nside16_%s.npz" % ("teb" if pol else "t"))))
     cltot = {k[6:]: base_d[k] for k in base_d if k.startswith("cltot_")}
     clraw = {k[6:]: base_d[k] for k in base_d if k.startswith("clraw_")}
@@ -42,31 +46,71 @@ def _build(pol):
     templates = [str(t) for t in d["templates"]]
     r_weights = {t: d["r_weights_" + t] for t in templates}
     tst = TSpecTemplate(base, base_d["mask"], Ideal(), templates, d["k_arr"], d["Tl_arr"], int(base_d["lmin_t"]),
-                        int(base_d["lmax_t"]), r_values=d["r_values"], r_weights=r_weights)
+                        int(base_d["lmax_t"]), r_values=d["r_values"], r_weights=r_weights, **FIXTURES[kind][1])
     tst.set_radial_integrals(d["qlXs"], d["plLXs"], FLLs=d["FLLs"])
     return d, tst
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["n0", "general"])
 @pytest.mark.parametrize("pol", [False, True])
-def test_numerator(pol):
-    d, tst = _build(pol)
+def test_numerator(pol, kind):
+    d, tst = _build(pol, kind)
     tst.generate_sims(1)
     assert rel_each(tst.Tl_numerator(d["data"], include_disconnected_term=False), d["tl_num_4"]) < TOL
     assert rel_each(tst.Tl_numerator(d["data"], include_disconnected_term=True), d["tl_num_full"]) < TOL
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["n0", "general"])
 @pytest.mark.parametrize("pol", [False, True])
-def test_fisher_contribution(pol):
-    d, tst = _build(pol)
+def test_fisher_contribution(pol, kind):
+    d, tst = _build(pol, kind)
     assert fisher_err(tst.compute_fisher_contribution(1), d["fisher_seed1"]) < TOL
 
 
-def test_unsupported_direc_raises():
-    """Direction-dependent templates with n > 0 are refused while the templates are parsed."""
+def _configured(templates):
     from polyspec_b200.tspec_template import TSpecTemplate
     t = TSpecTemplate.__new__(TSpecTemplate)
-    t.templates = ['tauNL-direc:1,1,1']
+    t.templates = list(templates)
+    t.Lmin, t.Lmax, t.lmin, t.lmax = 2, 40, 2, 30
+
+    class _Base:
+        l_arr = np.concatenate([np.arange(m, 48) for m in range(48)])
+        m_arr = np.concatenate([np.full(48 - m, m) for m in range(48)])
+    t.base = _Base()
+    t._configure_templates(t.templates, [], {})
+    return t
+
+
+def test_direc_configuration():
+    """General (n1, n3, n) parse as the reference does: P_{n} maps for n1 and n3, the triangle
+    condition and the n1 <-> n3 degeneracy check; tauNL-even/odd are refused."""
+    t = _configured(['tauNL-direc:1,2,1', 'tauNL-direc:0,1,1'])
+    assert [list(x) for x in t.n1n3n] == [[1, 2, 1], [0, 1, 1]] and t.p_inds == [0, 1, 2]
+    with pytest.raises(AssertionError):
+        _configured(['tauNL-direc:1,1,3'])
+    with pytest.raises(Exception, match="degenerate"):
+        _configured(['tauNL-direc:1,2,1', 'tauNL-direc:2,1,1'])
     with pytest.raises(NotImplementedError):
-        t._configure_templates(t.templates, [], {})
+        _configured(['tauNL-even:1'])
+
+
+@pytest.mark.gpu
+def test_F_integrals_shifted():
+    """F_{L,L+n}(r, r') for n = -2..2 computed on the GPU (ps_tau_F_integral, not injected)
+    against the fixture's: 1e-11 of the largest magnitude."""
+    import torch
+    from polyspec_b200 import PolySpec
+    from polyspec_b200.tspec_template import TSpecTemplate
+    d = load(False, "general")
+    base_d = dict(np.load(os.path.join(GOLD, "tspec_tauloc_nside16_t.npz")))
+    base = PolySpec(int(base_d["nside"]), {k[6:]: base_d[k] for k in base_d if k.startswith("cltot_")},
+                    beam=base_d["beam"][:1], pol=False, backend="cuda")
+    templates = [str(t) for t in d["templates"]]
+    tst = TSpecTemplate(base, base_d["mask"], lambda x, input_type='map', lmax=None: x, templates, d["k_arr"],
+                        d["Tl_arr"], int(base_d["lmin_t"]), int(base_d["lmax_t"]), r_values=d["r_values"],
+                        r_weights={t: d["r_weights_" + t] for t in templates}, Lmin=2, Lmax=40)
+    assert tst.FLLs.shape == d["FLLs"].shape
+    assert np.abs(tst.FLLs - d["FLLs"]).max() <= 1e-11 * np.abs(d["FLLs"]).max()
+    del torch
