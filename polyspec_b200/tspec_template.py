@@ -47,6 +47,49 @@ SUPPORTED = ['gNL-loc', 'gNL-con', 'gNL-dotdot', 'gNL-dotdel', 'gNL-deldel', 'ta
              'point-source']
 
 
+def _is_direc(t):
+    """Direction-dependent tauNL templates: tauNL-direc:n1,n3,n, tauNL-even:n and tauNL-odd:n."""
+    return any(s in t for s in ('tauNL-direc', 'tauNL-even', 'tauNL-odd'))
+
+
+def _fact_ratio(num, den):
+    """prod(num)! / prod(den)! as a float, from exact integers."""
+    from math import factorial
+    a, b = 1, 1
+    for x in num:
+        a *= factorial(x)
+    for x in den:
+        b *= factorial(x)
+    return a / b
+
+
+def wig3zero(l1, l2, l3):
+    """Wigner 3j symbol (l1 l2 l3; 0 0 0) for small integer l (the closed form of Edmonds 1957, eq. 3.7.17)."""
+    L = l1 + l2 + l3
+    if L % 2 or l3 < abs(l1 - l2) or l3 > l1 + l2 or min(l1, l2, l3) < 0:
+        return 0.
+    g = L // 2
+    r = np.sqrt(_fact_ratio((L - 2 * l1, L - 2 * l2, L - 2 * l3), (L + 1,)))
+    return (-1.) ** g * r * _fact_ratio((g,), (g - l1, g - l2, g - l3))
+
+
+def wig6(j1, j2, j3, j4, j5, j6):
+    """Wigner 6j symbol {j1 j2 j3; j4 j5 j6} for small integer j (Racah's single sum, Edmonds 1957, eq. 6.3.7)."""
+    triads = ((j1, j2, j3), (j1, j5, j6), (j4, j2, j6), (j4, j5, j3))
+    for a, b, c in triads:
+        if c < abs(a - b) or c > a + b or min(a, b, c) < 0:
+            return 0.
+    delta = 1.
+    for a, b, c in triads:
+        delta *= np.sqrt(_fact_ratio((a + b - c, a - b + c, -a + b + c), (a + b + c + 1,)))
+    A = [a + b + c for a, b, c in triads]
+    B = (j1 + j2 + j4 + j5, j2 + j3 + j5 + j6, j3 + j1 + j6 + j4)
+    total = 0.
+    for t in range(max(A), min(B) + 1):
+        total += (-1.) ** t * _fact_ratio((t + 1,), [t - a for a in A] + [b - t for b in B])
+    return delta * total
+
+
 def _vp(t):
     return ctypes.c_void_p(t.data_ptr())
 
@@ -161,7 +204,7 @@ class TSpecTemplate:
             print("Reading in precomputed radial integration points")
             assert len(r_values) > 0, "Must supply radial sampling points!"
             for t in templates:
-                if t in self.all_templates_1d:
+                if t in self.all_templates_1d or _is_direc(t):
                     assert t in r_weights.keys(), "Must supply weight for template %s" % t
             self.r_arr = np.asarray(r_values, dtype=np.float64)
             self.N_r = len(self.r_arr)
@@ -217,9 +260,9 @@ class TSpecTemplate:
             known = t in self.all_templates or any(s in t for s in ('tauNL-direc', 'tauNL-even', 'tauNL-odd',
                                                                      'tauNL-light', 'tauNL-heavy'))
             assert known, "Unknown template %s supplied!" % t
-            if t not in SUPPORTED and 'tauNL-direc' not in t:
-                raise NotImplementedError("template %s is not implemented by the CUDA backend (supported: %s and "
-                                          "tauNL-direc:n1,n3,n)" % (t, SUPPORTED))
+            if t not in SUPPORTED and not _is_direc(t):
+                raise NotImplementedError("template %s is not implemented by the CUDA backend (supported: %s, "
+                                          "tauNL-direc:n1,n3,n, tauNL-even:n, tauNL-odd:n)" % (t, SUPPORTED))
         print("Templates: %s" % templates)
         self.ints_1d, self.ints_2d, self.ints_coll = False, False, False
         self.to_compute, self.n1n3n, self.coll_params = [], [], {}
@@ -256,6 +299,30 @@ class TSpecTemplate:
                 assert (n1 <= 5) and (n3 <= 5) and (n <= 5), "n>5 has not yet been implemented!"
                 self.to_compute.append(['q'])
                 n1n3n.append([int(n1), int(n3), int(n)])
+                self.ints_1d = True
+            if 'tauNL-even' in t:
+                n = int(t.split(':')[1])
+                if n == 0 and 'tauNL-loc' in self.templates:
+                    raise Exception("tauNL-even:0 and tauNL-loc are fully degenerate!")
+                if n == 0 and 'tauNL-direc:0,0,0' in self.templates:
+                    raise Exception("tauNL-even:0 and tauNL-direc:0,0,0 are fully degenerate!")
+                if ('tauNL-direc:%d,%d,%d' % (0, n, n) in self.templates) and \
+                        ('tauNL-direc:%d,%d,%d' % (n, n, 0) in self.templates):
+                    raise Exception("tauNL-even:%d is fully degenerate with tauNL-direc:%d,%d,%d and "
+                                    "tauNL-direc:%d,%d,%d" % (n, 0, n, n, n, n, 0))
+                self.to_compute.append(['q'])
+                n1n3n += [[0, n, n], [n, n, 0]]
+                self.ints_1d = True
+            if 'tauNL-odd' in t:
+                n = int(t.split(':')[1])
+                if n == 0 and 'tauNL-direc:1,1,1' in self.templates:
+                    raise Exception("tauNL-odd:0 and tauNL-direc:1,1,1 are fully degenerate!")
+                # (n1, n3, n) pieces that satisfy the triangle conditions (polyspec/tspec_template.py:329-345)
+                cands = [[n - 1, n - 1, 1], [n - 1, n + 1, 1], [n + 1, n - 1, 1], [n + 1, n + 1, 1],
+                         [n - 1, 1, n - 1], [n - 1, 1, n + 1], [n + 1, 1, n - 1], [n + 1, 1, n + 1],
+                         [1, n - 1, n - 1], [1, n - 1, n + 1], [1, n + 1, n - 1], [1, n + 1, n + 1]]
+                n1n3n += [c for c in cands if abs(c[0] - c[1]) <= c[2] <= c[0] + c[1] and min(c) >= 0]
+                self.to_compute.append(['q'])
                 self.ints_1d = True
         for t in templates:
             if 'lensing' in t:
@@ -699,6 +766,55 @@ class TSpecTemplate:
             self.load_sim_data = pair
 
     # ------------------------------------------------------------------ local tauNL
+    def _decompose_tauNL_even(self, n):
+        """(n1, n3, n) pieces of tauNL-even:n and their weights (polyspec/tspec_template.py:754-760)."""
+        pref = (-1.) ** n / 3. * (4. * np.pi) ** 1.5 / np.sqrt(2. * n + 1.)
+        if n == 0:
+            return [[0, 0, 0]], [3 * pref]
+        return [[n, n, 0], [0, n, n]], [pref, 2 * pref]
+
+    def _decompose_tauNL_odd(self, n):
+        """(n1, n3, n) pieces of tauNL-odd:n and their weights (polyspec/tspec_template.py:762-796): for N, N' in
+        |n-1|..n+1, weight (-1)^n sqrt(2)/3 (4 pi)^(3/2) sqrt((2N+1)(2N'+1)) (N 1 n; 0 0 0)(N' 1 n; 0 0 0)
+        {N 1 N'; 1 n 1} on (min, max, 1) (with (-1)^(N+N') when N > N') and, times 1 + (-1)^(n+N+1), on
+        (1, N, N'); equal pieces summed, in sorted order."""
+        pref = (-1.) ** n * np.sqrt(2.) / 3. * (4. * np.pi) ** 1.5
+        parts, weights = [], []
+        for N in range(abs(n - 1), n + 2):
+            f1 = wig3zero(N, 1, n)
+            if f1 == 0:
+                continue
+            for Np in range(abs(n - 1), n + 2):
+                f12 = f1 * wig3zero(Np, 1, n)
+                if f12 == 0:
+                    continue
+                f12 *= wig6(N, 1, Np, 1, n, 1)
+                if f12 == 0:
+                    continue
+                w = pref * np.sqrt(2. * N + 1.) * np.sqrt(2. * Np + 1.) * f12
+                if Np >= N:
+                    parts.append([N, Np, 1])
+                    weights.append(w)
+                else:
+                    parts.append([Np, N, 1])
+                    weights.append((-1) ** (Np + N) * w)
+                parts.append([1, N, Np])
+                weights.append(w * (1. + (-1) ** (n + N + 1)))
+        uniq = [list(u) for u in np.unique(parts, axis=0)] if parts else []
+        return uniq, [float(np.sum([weights[i] for i in range(len(parts)) if parts[i] == u])) for u in uniq]
+
+    def _direc_parts(self, t):
+        """[(n1, n3, n, weight)] of a direction-dependent template: tauNL-direc:n1,n3,n alone, or the
+        decomposition of tauNL-even:n / tauNL-odd:n.  Its 4-, 2- and 0-field numerator terms and its Fisher
+        derivative are the weighted sums of the tauNL-direc ones (polyspec/tspec_template.py:1433-1487,
+        :1689-1815, :2850-2893)."""
+        if 'tauNL-direc' in t:
+            n1, n3, n = (int(x) for x in t.split(':')[1].split(','))
+            return [(n1, n3, n, 1.)]
+        n = int(t.split(':')[1])
+        parts, weights = (self._decompose_tauNL_even(n) if 'tauNL-even' in t else self._decompose_tauNL_odd(n))
+        return [(int(a), int(b), int(c), float(w)) for (a, b, c), w in zip(parts, weights)]
+
     def _A_maps(self, map1, map2, n, add_sym=False):
         """[P_{n,mu} Q]_LM for mu = -n..n and each radial sample (polyspec/tspec_template.py:1275-1334), as
         [2n+1, N_r, nlm(nLmax)] over the full l <= nLmax list (entries with L < nLmin are unused);
@@ -940,12 +1056,14 @@ class TSpecTemplate:
                     A_dd[0] = self._A_maps(proc_maps, proc_maps, 0)
                 t4_num[ii] = 1. / 24. * self._tau_sum(A_dd, A_dd, self.r_weights[t], 0, 0, 0) * 12. \
                     * (4. * np.pi) ** (3. / 2.)
-            if 'tauNL-direc' in t:
-                n1, n3, n = np.asarray(t.split(':')[1].split(','), dtype=int)
-                for nn in (n1, n3):
-                    if nn not in A_dd:
-                        A_dd[nn] = self._A_maps(proc_maps, proc_maps, nn)
-                t4_num[ii] = self._tau_sum(A_dd, A_dd, self.r_weights[t], n1, n3, n) / 48. * 24.
+            if _is_direc(t):
+                tau = 0.
+                for n1, n3, n, wt in self._direc_parts(t):
+                    for nn in (n1, n3):
+                        if nn not in A_dd:
+                            A_dd[nn] = self._A_maps(proc_maps, proc_maps, nn)
+                    tau += wt * self._tau_sum(A_dd, A_dd, self.r_weights[t], n1, n3, n)
+                t4_num[ii] = tau / 48. * 24.
             if t in ('gNL-con', 'gNL-dotdot', 'gNL-dotdel', 'gNL-deldel'):
                 t0 = time.time()
                 t4_num[ii] = self._gnl_shape_sum(t, proc_maps) * A_pix
@@ -972,32 +1090,38 @@ class TSpecTemplate:
                     pa, pb = self.load_sim_data(isim)
                 A_aa, A_bb, A_ad, A_bd, A_ab = {}, {}, {}, {}, {}
                 for ii, t in enumerate(self.templates):
-                    if 'tauNL-direc' in t:
-                        n1, n3, n = np.asarray(t.split(':')[1].split(','), dtype=int)
+                    if _is_direc(t):
                         w = self.r_weights[t]
-                        tmp = 0.
-                        for A_xx, A_xd, px in ((A_aa, A_ad, pa), (A_bb, A_bd, pb)):
-                            for nn in np.unique([n1, n3]):
-                                if nn not in A_xx:
-                                    A_xx[nn] = self._A_maps(px, px, nn)
-                                    A_xd[nn] = self._A_maps(px, proc_maps, nn, add_sym=True)
-                            if n1 == n3:
-                                tmp += 2 * self._tau_sum(A_xx, A_dd, w, n1, n3, n)
-                            else:
-                                tmp += self._tau_sum(A_xx, A_dd, w, n1, n3, n) + self._tau_sum(A_dd, A_xx, w, n1, n3, n)
-                            tmp += self._tau_sum(A_xd, A_xd, w, n1, n3, n)
-                        t2_num[ii] += -1. / 48. * tmp * 6. / self.N_it / 2. * 4.
-                        if compute_t0:
+                        t2, t0s = 0., 0.
+                        for n1, n3, n, wt in self._direc_parts(t):
                             tmp = 0.
-                            for nn in np.unique([n1, n3]):
-                                if nn not in A_ab:
-                                    A_ab[nn] = self._A_maps(pa, pb, nn, add_sym=True)
-                            if n1 == n3:
-                                tmp += 2 * self._tau_sum(A_aa, A_bb, w, n1, n3, n)
-                            else:
-                                tmp += self._tau_sum(A_aa, A_bb, w, n1, n3, n) + self._tau_sum(A_bb, A_aa, w, n1, n3, n)
-                            tmp += self._tau_sum(A_ab, A_ab, w, n1, n3, n)
-                            t0_num[ii] += 1. / 48. * tmp * 3 / self.N_it * 4.
+                            for A_xx, A_xd, px in ((A_aa, A_ad, pa), (A_bb, A_bd, pb)):
+                                for nn in np.unique([n1, n3]):
+                                    if nn not in A_xx:
+                                        A_xx[nn] = self._A_maps(px, px, nn)
+                                        A_xd[nn] = self._A_maps(px, proc_maps, nn, add_sym=True)
+                                if n1 == n3:
+                                    tmp += 2 * self._tau_sum(A_xx, A_dd, w, n1, n3, n)
+                                else:
+                                    tmp += self._tau_sum(A_xx, A_dd, w, n1, n3, n) \
+                                        + self._tau_sum(A_dd, A_xx, w, n1, n3, n)
+                                tmp += self._tau_sum(A_xd, A_xd, w, n1, n3, n)
+                            t2 += wt * tmp
+                            if compute_t0:
+                                tmp = 0.
+                                for nn in np.unique([n1, n3]):
+                                    if nn not in A_ab:
+                                        A_ab[nn] = self._A_maps(pa, pb, nn, add_sym=True)
+                                if n1 == n3:
+                                    tmp += 2 * self._tau_sum(A_aa, A_bb, w, n1, n3, n)
+                                else:
+                                    tmp += self._tau_sum(A_aa, A_bb, w, n1, n3, n) \
+                                        + self._tau_sum(A_bb, A_aa, w, n1, n3, n)
+                                tmp += self._tau_sum(A_ab, A_ab, w, n1, n3, n)
+                                t0s += wt * tmp
+                        t2_num[ii] += -1. / 48. * t2 * 6. / self.N_it / 2. * 4.
+                        if compute_t0:
+                            t0_num[ii] += 1. / 48. * t0s * 3 / self.N_it * 4.
                     if t == 'tauNL-loc':
                         w = self.r_weights[t]
                         if 0 not in A_aa:
@@ -1343,12 +1467,14 @@ class TSpecTemplate:
                     F_vecs = self._F_PQ(P_maps[0], Q_maps, w)
                     Qs[:, ii] += (4. * np.pi) ** 1.5 * self._get_Q4_perms(P_maps[0], Q_maps, F_vecs, w)
                     del F_vecs
-                if 'tauNL-direc' in t:
-                    n1, n3, n = np.asarray(t.split(':')[1].split(','), dtype=int)
+                if _is_direc(t):
                     w = self.r_weights[t]
-                    # polyspec/tspec_template.py:2850-2862: n1 != n3 adds both orderings, symmetrised
-                    parts = [(n1, n3, 1.)] if n1 == n3 else [(n1, n3, 0.5), (n3, n1, 0.5 * (-1.) ** (n1 + n3))]
-                    for a, c, wt in parts:
+                    # polyspec/tspec_template.py:2850-2893: n1 != n3 adds both orderings, symmetrised
+                    parts = []
+                    for n1, n3, n, wp in self._direc_parts(t):
+                        parts += ([(n1, n3, n, wp)] if n1 == n3 else
+                                  [(n1, n3, n, 0.5 * wp), (n3, n1, n, 0.5 * (-1.) ** (n1 + n3) * wp)])
+                    for a, c, n, wt in parts:
                         if a == 0 and c == 0:
                             F_vecs = self._F_PQ(P_maps[0], Q_maps, w)
                             Qs[:, ii] += wt * self._get_Q4_perms(P_maps[0], Q_maps, F_vecs, w)

@@ -1,11 +1,12 @@
-"""Generate the general direction-dependent tauNL fixtures (n > 0 or n1 != n3) of tests/golden
-from the UNMODIFIED reference.
+"""Generate the general direction-dependent tauNL fixtures (n > 0 or n1 != n3, and the
+tauNL-even / tauNL-odd combinations) of tests/golden from the UNMODIFIED reference.
 
     python tests/golden/make_golden_tspec_direc.py [/path/to/reference]
 
-Builds polyspec/tspec_template.py's TSpecTemplate as-is with the templates
-tauNL-direc:1,1,2, tauNL-direc:1,2,1 and tauNL-direc:0,1,1 over the oracle shims of
-make_golden_tspec.py (with 2 <= L <= 40) and saves its q_l^X(r), p_lL^X(r) and F_{L,L+Delta}(r, r') integrals,
+Builds polyspec/tspec_template.py's TSpecTemplate as-is, once with the templates
+tauNL-direc:1,1,2, tauNL-direc:1,2,1 and tauNL-direc:0,1,1 (tspec_direc_*) and once with
+tauNL-even:0, tauNL-even:1 and tauNL-odd:1 (tspec_evenodd_*; the odd weights use the shim's
+exact 6j symbols), over the oracle shims of make_golden_tspec.py (with 2 <= L <= 40) and saves its q_l^X(r), p_lL^X(r) and F_{L,L+Delta}(r, r') integrals,
 the numerator with and without the disconnected terms (one simulation pair) and
 compute_fisher_contribution(1), for T only and for T, E, B.  These exercise the reference's
 tau_sum_general and convolve_F_general (tauNL_utils.pyx:650-715, :1069-1190), the n1 != n3
@@ -22,13 +23,14 @@ sys.path.insert(0, HERE)
 import make_golden_tspec as mgt  # noqa: E402  (installs the numpy / scipy aliases)
 from make_golden import inputs, NSIDE  # noqa: E402
 
-TEMPLATES = ['tauNL-direc:1,1,2', 'tauNL-direc:1,2,1', 'tauNL-direc:0,1,1']
+TEMPLATE_SETS = {"direc": ['tauNL-direc:1,1,2', 'tauNL-direc:1,2,1', 'tauNL-direc:0,1,1'],
+                 "evenodd": ['tauNL-even:0', 'tauNL-even:1', 'tauNL-odd:1']}
 LMIN, LMAX = mgt.LMIN, mgt.LMAX
 # L range of the exchanged momentum: L_MAX + max(n) must stay within the maps' lmax (3 Nside - 1)
 L_MIN, L_MAX = 2, 40
 
 
-def make(pol, ref):
+def make(pol, ref, TEMPLATES):
     base_mod, wt_mod, ts_mod = ref["base"], ref["weighting"], ref["tspec_template"]
     lmax, cl, beam, cltot, mask, noise = inputs(pol)
     base = base_mod.PolySpec(NSIDE, dict(cltot), beam=list(beam) if pol else beam[:1], pol=pol, backend="ducc",
@@ -58,11 +60,12 @@ def make(pol, ref):
 def main():
     refroot = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     ref = mgt.load_reference(refroot)
-    for pol in (False, True):
-        d = make(pol, ref)
-        path = os.path.join(HERE, "tspec_direc_nside16_%s.npz" % ("teb" if pol else "t"))
-        np.savez_compressed(path, **d)
-        print("wrote", path, os.path.getsize(path), "bytes")
+    for name, templates in TEMPLATE_SETS.items():
+        for pol in (False, True):
+            d = make(pol, ref, templates)
+            path = os.path.join(HERE, "tspec_%s_nside16_%s.npz" % (name, "teb" if pol else "t"))
+            np.savez_compressed(path, **d)
+            print("wrote", path, os.path.getsize(path), "bytes")
 
 
 if __name__ == "__main__":

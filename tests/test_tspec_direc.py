@@ -2,7 +2,8 @@
 by the unmodified reference (its Gaunt and 3j symbols from the compiled wignerSymbols):
 n = 0 (tauNL-direc:1,1,0 and tauNL-direc:2,2,0 together, make_golden_tspec_gaunt.py) and
 general (n1, n3, n) (tauNL-direc:1,1,2, tauNL-direc:1,2,1 and tauNL-direc:0,1,1 together,
-L in [2, 40], make_golden_tspec_direc.py).  The k-space and F integrals are injected from
+L in [2, 40]) and the tauNL-even:0, tauNL-even:1 and tauNL-odd:1 combinations
+(make_golden_tspec_direc.py).  The k-space and F integrals are injected from
 the fixture.  Numerators and Fisher entries to 1e-9, relative per entry (a Fisher entry is
 compared with sqrt(F_ii F_jj))."""
 import os
@@ -16,7 +17,8 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 TOL = 1e-9
 
 
-FIXTURES = {"n0": ("tspec_gaunt", {}), "general": ("tspec_direc", {"Lmin": 2, "Lmax": 40})}
+FIXTURES = {"n0": ("tspec_gaunt", {}), "general": ("tspec_direc", {"Lmin": 2, "Lmax": 40}),
+            "evenodd": ("tspec_evenodd", {"Lmin": 2, "Lmax": 40})}
 
 
 def load(pol, kind="n0"):
@@ -52,7 +54,7 @@ def _build(pol, kind="n0"):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", ["n0", "general"])
+@pytest.mark.parametrize("kind", ["n0", "general", "evenodd"])
 @pytest.mark.parametrize("pol", [False, True])
 def test_numerator(pol, kind):
     d, tst = _build(pol, kind)
@@ -62,7 +64,7 @@ def test_numerator(pol, kind):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", ["n0", "general"])
+@pytest.mark.parametrize("kind", ["n0", "general", "evenodd"])
 @pytest.mark.parametrize("pol", [False, True])
 def test_fisher_contribution(pol, kind):
     d, tst = _build(pol, kind)
@@ -85,7 +87,7 @@ def _configured(templates):
 
 def test_direc_configuration():
     """General (n1, n3, n) parse as the reference does: P_{n} maps for n1 and n3, the triangle
-    condition and the n1 <-> n3 degeneracy check; tauNL-even/odd are refused."""
+    condition and the n1 <-> n3 degeneracy check; the collider templates are refused."""
     t = _configured(['tauNL-direc:1,2,1', 'tauNL-direc:0,1,1'])
     assert [list(x) for x in t.n1n3n] == [[1, 2, 1], [0, 1, 1]] and t.p_inds == [0, 1, 2]
     with pytest.raises(AssertionError):
@@ -93,7 +95,7 @@ def test_direc_configuration():
     with pytest.raises(Exception, match="degenerate"):
         _configured(['tauNL-direc:1,2,1', 'tauNL-direc:2,1,1'])
     with pytest.raises(NotImplementedError):
-        _configured(['tauNL-even:1'])
+        _configured(['tauNL-light:1,1.5'])
 
 
 @pytest.mark.gpu
@@ -114,3 +116,33 @@ def test_F_integrals_shifted():
     assert tst.FLLs.shape == d["FLLs"].shape
     assert np.abs(tst.FLLs - d["FLLs"]).max() <= 1e-11 * np.abs(d["FLLs"]).max()
     del torch
+
+
+def test_small_wigner_symbols():
+    """The package's wig3zero / wig6 (host-side, for the tauNL-odd weights) and the oracle shim's
+    wig6jj against sympy's exact symbols: 1e-14 relative."""
+    from sympy.physics.wigner import wigner_3j, wigner_6j
+    from polyspec_b200.tspec_template import wig3zero, wig6
+    from oracle.shims import pywigxjpf as pw
+    for l1 in range(7):
+        for l2 in range(7):
+            for l3 in range(9):
+                e = float(wigner_3j(l1, l2, l3, 0, 0, 0))
+                assert abs(wig3zero(l1, l2, l3) - e) <= 1e-14 * abs(e)
+    for js in [(1, 1, 1, 1, 1, 1), (2, 1, 2, 1, 3, 1), (0, 1, 1, 1, 1, 1), (3, 1, 4, 1, 3, 1), (2, 1, 1, 1, 2, 1),
+               (4, 1, 4, 1, 5, 1), (5, 1, 6, 1, 5, 1), (1, 2, 3, 2, 1, 2), (3, 3, 3, 3, 3, 3), (2, 1, 4, 1, 3, 1)]:
+        e = float(wigner_6j(*js))
+        assert abs(wig6(*js) - e) <= 1e-14 * max(abs(e), 1e-300), js
+        assert abs(pw.wig6jj(*(2 * j for j in js)) - e) <= 1e-14 * max(abs(e), 1e-300), js
+
+
+def test_odd_even_decompositions():
+    """tauNL-even/odd decompositions: the pieces satisfy the triangle conditions and appear in the
+    parsed (n1, n3, n) list, and the even weights are (-1)^n (4 pi)^(3/2) / (3 sqrt(2n+1)) times 1, 2."""
+    t = _configured(['tauNL-even:2', 'tauNL-odd:1'])
+    got = {tuple(x) for x in t.n1n3n}
+    for tt in ('tauNL-even:2', 'tauNL-odd:1'):
+        for n1, n3, n, w in t._direc_parts(tt):
+            assert (n1, n3, n) in got and abs(n1 - n3) <= n <= n1 + n3 and np.isfinite(w)
+    pe = (4. * np.pi) ** 1.5 / 3. / np.sqrt(5.)
+    assert np.allclose([w for *_, w in t._direc_parts('tauNL-even:2')], [pe, 2 * pe], rtol=1e-15)
