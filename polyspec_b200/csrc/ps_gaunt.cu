@@ -2,6 +2,7 @@
 // ps_gaunt.cuh (used by the parity tests of the direction-dependent contractions).
 #include "ps_common.cuh"
 #include "ps_gaunt.cuh"
+#include "ps_stats.cuh"
 
 namespace ps {
 namespace {
@@ -347,9 +348,8 @@ extern "C" int ps_product_q_complex(const double* Q, const double* F, int nmu, i
 //  * tau_sum_general (polyspec/cython/tauNL_utils.pyx:650-715): Sum over (Delta, mu), (L, M),
 //    mu1 and (r_j, r_k) of Re(pref * B[..][(L+Delta, -M-mu)][k] w_k A[n1+mu1][(L, M)][j]) F w_j with
 //    pref = (2 if M != 0) i^Delta Gaunt(L, L+Delta, n; M, -M-mu, mu) (n1 n3 n; mu1 mu3 mu) and the
-//    conjugate, sign-flipped B where -M-mu < 0; one thread per ((L, M), r_j), per-CTA partials
-//    summed in a fixed order.
-//  * convolve_F_general (:1069-1180): per ((L, M), r_j) the two Gaunt-weighted F convolutions
+//    conjugate, sign-flipped B where -M-mu < 0; per-CTA partials summed in a fixed order.
+//  * convolve_F_general (:1069-1180): for each ((L, M), r_j) the two Gaunt-weighted F convolutions
 //    of the shifted [P Q] vectors (M -> M - mu and -M - mu), accumulated as plus + minus and
 //    plus - minus at the row of (L, M) in the l <= nLmax list.
 // Arrays are [mu][row][r] over a list of (L, M) rows (rowL, rowM); row_of_full maps the m-major
@@ -369,55 +369,177 @@ __device__ __forceinline__ int64_t lm_full(int L, int M, int lmax) {
   return int64_t(M) * (2 * lmax + 1 - M) / 2 + L;
 }
 
-__global__ void tau_general_kernel(const double2* __restrict__ A, const double2* __restrict__ B,
-                                   const int* __restrict__ row_of_full, const int* __restrict__ rowL,
-                                   const int* __restrict__ rowM, int nrow, int nLmax, int Lmin, int Lmax,
-                                   const double* __restrict__ F, int nLF, int nmax_F, const double* __restrict__ w,
-                                   int nr, int n1, int n3, int n, double* __restrict__ partial) {
-  __shared__ double red[128];
+// Both kernels give one warp to each (L, M) row.  A row's coupling terms, (Delta, mu, mu1) for the
+// tau sum and (Delta, mu, part) for the convolution, are built 32 at a time, one per lane (its
+// Gaunt and 3j coefficients, the (L+Delta, -M-mu) or (L+Delta, M-mu) row and which [P Q] plane,
+// conjugated or not, it reads) and kept in shared memory; then lane j takes radial sample j and runs
+// the r' sum of every term of the batch.  The coefficients are thus computed once per row, not
+// once per (row, r), and the terms are visited in (Delta, mu, mu1 / part) order.
+constexpr int kRowWarps = 4;
+
+struct RowTerm {
+  double2 g;   // complex coefficient
+  int rowp;    // source row (-1: the term vanishes)
+  int plane;   // source [P Q] / B plane
+  int conj;    // read the conjugate of the source
+  int dF;      // Delta (F plane nmax_F + Delta)
+  int extra;   // tau sum: A plane n1 + mu1; convolution: 0 plus part, 1 minus part
+};
+
+// Source vectors of up to kStage terms, radial samples k0 .. k0 + kn - 1, staged in shared memory
+// (conjugated where the term says so) by coalesced loads that are all in flight together; the r'
+// sums then read them as broadcasts.
+constexpr int kStage = 8;
+
+__device__ __forceinline__ void stage_sources(const double2* __restrict__ src, const RowTerm* terms, int qn, int nrow,
+                                              int nr, int k0, int kn, int lane, double2 (*vs)[32]) {
+#pragma unroll
+  for (int qq = 0; qq < kStage; ++qq) {
+    if (qq < qn && terms[qq].rowp >= 0 && lane < kn) {
+      double2 v = src[(int64_t(terms[qq].plane) * nrow + terms[qq].rowp) * nr + k0 + lane];
+      if (terms[qq].conj) v.y = -v.y;
+      vs[qq][lane] = v;
+    }
+  }
+}
+
+// s += Sum_k v[k] F_j(r'_k) w_k over kn samples (F read at inds[k] when given), skipping zero weights
+// as the reference does, in the order of k.
+__device__ __forceinline__ void radial_sum(const double2* v, const double* __restrict__ Fr,
+                                           const int* __restrict__ inds, const double* __restrict__ w, int kn,
+                                           double2& s) {
+  for (int k = 0; k < kn; ++k) {
+    const double wk = w[k];
+    if (wk == 0.0) continue;
+    const double2 x = v[k];
+    const double f = Fr[inds ? inds[k] : k] * wk;
+    s.x += x.x * f;
+    s.y += x.y * f;
+  }
+}
+
+// The coupling term t of row (L, M), built out of line so that its Gaunt and 3j evaluation does not
+// raise the register count of the r' loops.
+__device__ __noinline__ RowTerm tau_term(int t, int nT, int L, int M, const int* __restrict__ row_of_full, int nLmax,
+                                         int Lmin, int Lmax, int n1, int n3, int n) {
+  RowTerm c;
+  c.rowp = -1;
+  if (t >= nT) return c;
+  const int nmu = 2 * n + 1, nmu1 = 2 * n1 + 1;
+  const int mu1 = t % nmu1 - n1;
+  const int mu = (t / nmu1) % nmu - n;
+  const int Delta = 2 * (t / (nmu1 * nmu)) - n;
+  const int Lp = L + Delta, Mp = -M - mu, mu3 = -mu1 - mu;
+  if (Lp < Lmin || Lp > Lmax || abs(Mp) > Lp || abs(mu3) > n3) return c;
+  const double G = gaunt_small(L, Lp, n, M, -M - mu, mu);
+  double t3 = G != 0.0 ? threej_small(n1, n3, n, mu1, mu3, mu) : 0.0;
+  const int rowp = row_of_full[lm_full(Lp, abs(Mp), nLmax)];
+  if (t3 == 0.0 || rowp < 0) return c;
+  if (Mp < 0 && ((Mp + n3 + mu3) & 1)) t3 = -t3;
+  const double2 p1 = cm(ipow(Delta), make_double2((M != 0 ? 2.0 : 1.0) * G, 0.));
+  c.g = make_double2(p1.x * t3, p1.y * t3);
+  c.rowp = rowp;
+  c.plane = Mp >= 0 ? n3 + mu3 : n3 - mu3;
+  c.conj = Mp < 0;
+  c.dF = Delta;
+  c.extra = n1 + mu1;
+  return c;
+}
+
+__device__ __noinline__ RowTerm conv_term(int t, int nT, int L, int M, const int* __restrict__ row_of_full, int nLmax,
+                                          int Lmin, int Lmax, int n1, int n3, int n, int mu1) {
+  RowTerm c;
+  c.rowp = -1;
+  if (t >= nT) return c;
+  const int nmu = 2 * n + 1;
+  const int part = t & 1;
+  const int mu = (t >> 1) % nmu - n;
+  const int Delta = 2 * ((t >> 1) / nmu) - n;
+  const int Lp = L + Delta, mu3 = -mu1 - mu;
+  const int Mp = part == 0 ? M - mu : -M - mu;
+  if (Lp < Lmin || Lp > Lmax || abs(mu3) > n3 || (part == 1 && M == 0) || abs(Mp) > Lp) return c;
+  const double t3 = threej_small(n1, n3, n, mu1, mu3, mu);
+  double G = t3 != 0.0 ? (part == 0 ? gaunt_small(L, Lp, n, -M, M - mu, mu) : gaunt_small(L, Lp, n, M, -M - mu, mu))
+                       : 0.0;
+  const int rowp = row_of_full[lm_full(Lp, abs(Mp), nLmax)];
+  if (G == 0.0 || rowp < 0) return c;
+  const double2 pref = make_double2(ipow(Delta).x * t3, ipow(Delta).y * t3);
+  if (part == 0) {
+    const int e = Mp >= 0 ? M : (M + Mp + n3 + mu3);
+    if (e & 1) G = -G;
+    if (M != 0) G *= 0.5;
+    c.g = make_double2(pref.x * G, pref.y * G);
+  } else {
+    if (Mp < 0 && ((Mp + n3 + mu3) & 1)) G = -G;
+    G *= 0.5;
+    c.g = make_double2(pref.x * G, -pref.y * G);  // conj(pref)
+  }
+  c.rowp = rowp;
+  c.plane = Mp >= 0 ? n3 + mu3 : n3 - mu3;
+  // plus part reads PQ[n3+mu3] (Mp >= 0) or conj(PQ[n3-mu3]); minus part the conjugates of those
+  c.conj = (part == 0) ? (Mp < 0) : (Mp >= 0);
+  c.dF = Delta;
+  c.extra = part;
+  return c;
+}
+
+__global__ void __launch_bounds__(32 * kRowWarps)
+tau_general_kernel(const double2* __restrict__ A, const double2* __restrict__ B, const int* __restrict__ row_of_full,
+                   const int* __restrict__ rowL, const int* __restrict__ rowM, int nrow, int nLmax, int Lmin,
+                   int Lmax, const double* __restrict__ F, int nLF, int nmax_F, const double* __restrict__ w, int nr,
+                   int n1, int n3, int n, double* __restrict__ partial) {
+  __shared__ RowTerm sh[kRowWarps][32];
+  __shared__ double2 vsh[kRowWarps][kStage][32];
+  __shared__ double red[32 * kRowWarps];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  RowTerm* terms = sh[wid];
+  const int nmu = 2 * n + 1, nmu1 = 2 * n1 + 1;
+  const int nT = (n + 1) * nmu * nmu1;  // Delta = -n, -n + 2, ..., n (odd Delta + n: no Gaunt coupling)
   double acc = 0.0;
-  const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (t < int64_t(nrow) * nr) {
-    const int i = int(t / nr), j = int(t % nr);
+  for (int64_t i = blockIdx.x * int64_t(kRowWarps) + wid; i < nrow; i += int64_t(gridDim.x) * kRowWarps) {
     const int L = rowL[i], M = rowM[i];
-    const double wj = w[j];
-    if (L >= Lmin && L <= Lmax && wj != 0.0) {
-      for (int Delta = -n; Delta <= n; ++Delta) {
-        if ((Delta + n) & 1) continue;  // the Gaunt coefficient vanishes
-        const int Lp = L + Delta;
-        if (Lp < Lmin || Lp > Lmax) continue;
-        const double* Fr = F + ((int64_t(nmax_F + Delta) * nLF + L) * nr + j) * nr;
-        for (int mu = -n; mu <= n; ++mu) {
-          const int Mp = -M - mu;
-          if (abs(Mp) > Lp) continue;
-          const double G = gaunt_small(L, Lp, n, M, -M - mu, mu);
-          if (G == 0.0) continue;
-          const double2 p1 = cm(ipow(Delta), make_double2((M != 0 ? 2.0 : 1.0) * G, 0.));
-          const int rowp = row_of_full[lm_full(Lp, abs(Mp), nLmax)];
-          if (rowp < 0) continue;
-          for (int mu1 = -n1; mu1 <= n1; ++mu1) {
-            const int mu3 = -mu1 - mu;
-            if (abs(mu3) > n3) continue;
-            double t3 = threej_small(n1, n3, n, mu1, mu3, mu);
-            if (t3 == 0.0) continue;
-            if (Mp < 0 && ((Mp + n3 + mu3) & 1)) t3 = -t3;
-            const double2* src = Mp >= 0 ? B + (int64_t(n3 + mu3) * nrow + rowp) * nr
-                                         : B + (int64_t(n3 - mu3) * nrow + rowp) * nr;
-            double2 s = make_double2(0., 0.);
-            for (int k = 0; k < nr; ++k) {
-              const double wk = w[k];
-              if (wk == 0.0) continue;
-              double2 v = src[k];
-              if (Mp < 0) v.y = -v.y;
-              const double f = Fr[k] * wk;
-              s.x += v.x * f;
-              s.y += v.y * f;
+    if (L < Lmin || L > Lmax) continue;  // warp-uniform
+    for (int j0 = 0; j0 < nr; j0 += 32) {
+      const int j = j0 + lane;
+      const double wj = j < nr ? w[j] : 0.0;
+      for (int t0 = 0; t0 < nT; t0 += 32) {
+        const RowTerm c = tau_term(t0 + lane, nT, L, M, row_of_full, nLmax, Lmin, Lmax, n1, n3, n);
+        terms[lane] = c;
+        __syncwarp();
+        const int nt = min(32, nT - t0);
+        for (int q0 = 0; q0 < nt; q0 += kStage) {
+          const int qn = min(kStage, nt - q0);
+          double2 sacc[kStage];
+#pragma unroll
+          for (int qq = 0; qq < kStage; ++qq) sacc[qq] = make_double2(0., 0.);
+          for (int k0 = 0; k0 < nr; k0 += 32) {
+            const int kn = min(32, nr - k0);
+            stage_sources(B, terms + q0, qn, nrow, nr, k0, kn, lane, vsh[wid]);
+            __syncwarp();
+            if (wj != 0.0) {
+#pragma unroll
+              for (int qq = 0; qq < kStage; ++qq) {
+                if (qq < qn && terms[q0 + qq].rowp >= 0) {
+                  const double* Fr = F + ((int64_t(nmax_F + terms[q0 + qq].dF) * nLF + L) * nr + j) * nr + k0;
+                  radial_sum(vsh[wid][qq], Fr, nullptr, w + k0, kn, sacc[qq]);
+                }
+              }
             }
-            const double2 v = cm(make_double2(p1.x * t3, p1.y * t3), s);
-            const double2 a = A[(int64_t(n1 + mu1) * nrow + i) * nr + j];
-            acc += (v.x * a.x - v.y * a.y) * wj;
+            __syncwarp();
+          }
+          if (wj != 0.0) {
+#pragma unroll
+            for (int qq = 0; qq < kStage; ++qq) {
+              if (qq < qn && terms[q0 + qq].rowp >= 0) {
+                const RowTerm& tm = terms[q0 + qq];
+                const double2 v = cm(tm.g, sacc[qq]);
+                const double2 a = A[(int64_t(tm.extra) * nrow + i) * nr + j];
+                acc += (v.x * a.x - v.y * a.y) * wj;
+              }
+            }
           }
         }
+        __syncwarp();
       }
     }
   }
@@ -443,82 +565,91 @@ __global__ void sum_partials(const double* __restrict__ partial, int64_t n, doub
   if (threadIdx.x == 0) out[0] = red[0];
 }
 
-__global__ void conv_general_kernel(const double2* __restrict__ PQ, const int* __restrict__ row_of_full,
-                                    const int* __restrict__ rowL, const int* __restrict__ rowM,
-                                    const int* __restrict__ full_of_row, int nrow, int nLmax, int Lmin, int Lmax,
-                                    const double* __restrict__ F, int nLF, int nrF, int nmax_F,
-                                    const double* __restrict__ w, const int* __restrict__ inds, int nr, int n1,
-                                    int n3, int n, int mu1, double2* __restrict__ out_re,
-                                    double2* __restrict__ out_im) {
-  const int64_t total = int64_t(nrow) * nr;
-  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
-    const int i = int(t / nr), j = int(t % nr);
-    const int L = rowL[i], M = rowM[i];
-    if (L < Lmin || L > Lmax || full_of_row[i] < 0) continue;
-    double2 plus = make_double2(0., 0.), minus = plus;
-    for (int Delta = -n; Delta <= n; ++Delta) {
-      if ((Delta + n) & 1) continue;
-      const int Lp = L + Delta;
-      if (Lp < Lmin || Lp > Lmax) continue;
-      const double* Fr = F + ((int64_t(nmax_F + Delta) * nLF + L) * nrF + inds[j]) * nrF;
-      for (int mu = -n; mu <= n; ++mu) {
-        const int mu3 = -mu1 - mu;
-        if (abs(mu3) > n3) continue;
-        const double t3 = threej_small(n1, n3, n, mu1, mu3, mu);
-        if (t3 == 0.0) continue;
-        const double2 pref = make_double2(ipow(Delta).x * t3, ipow(Delta).y * t3);
-        for (int part = 0; part < 2; ++part) {
-          if (part == 1 && M == 0) break;
-          const int Mp = part == 0 ? M - mu : -M - mu;
-          if (abs(Mp) > Lp) continue;
-          double G = part == 0 ? gaunt_small(L, Lp, n, -M, M - mu, mu) : gaunt_small(L, Lp, n, M, -M - mu, mu);
-          if (G == 0.0) continue;
-          double2 g;
-          if (part == 0) {
-            const int e = Mp >= 0 ? M : (M + Mp + n3 + mu3);
-            if (e & 1) G = -G;
-            if (M != 0) G *= 0.5;
-            g = make_double2(pref.x * G, pref.y * G);
-          } else {
-            if (Mp < 0 && ((Mp + n3 + mu3) & 1)) G = -G;
-            G *= 0.5;
-            g = make_double2(pref.x * G, -pref.y * G);  // conj(pref)
+__global__ void __launch_bounds__(32 * kRowWarps)
+conv_general_kernel(const double2* __restrict__ PQ, const int* __restrict__ row_of_full, const int* __restrict__ rowL,
+                    const int* __restrict__ rowM, const int* __restrict__ full_of_row, int nrow, int nLmax, int Lmin,
+                    int Lmax, const double* __restrict__ F, int nLF, int nrF, int nmax_F, const double* __restrict__ w,
+                    const int* __restrict__ inds, int nr, int n1, int n3, int n, int mu1, double2* __restrict__ out_re,
+                    double2* __restrict__ out_im) {
+  __shared__ RowTerm sh[kRowWarps][32];
+  __shared__ double2 vsh[kRowWarps][kStage][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  RowTerm* terms = sh[wid];
+  const int nmu = 2 * n + 1;
+  const int nT = (n + 1) * nmu * 2;  // (Delta, mu, part), part 0: M -> M - mu, part 1: M -> -M - mu
+  for (int64_t i = blockIdx.x * int64_t(kRowWarps) + wid; i < nrow; i += int64_t(gridDim.x) * kRowWarps) {
+    const int L = rowL[i], M = rowM[i], fo = full_of_row[i];
+    if (L < Lmin || L > Lmax || fo < 0) continue;  // warp-uniform
+    for (int j0 = 0; j0 < nr; j0 += 32) {
+      const int j = j0 + lane;
+      const bool active = j < nr;
+      const int ij = active ? inds[j] : 0;
+      double2 plus = make_double2(0., 0.), minus = plus;
+      for (int t0 = 0; t0 < nT; t0 += 32) {
+        const RowTerm c = conv_term(t0 + lane, nT, L, M, row_of_full, nLmax, Lmin, Lmax, n1, n3, n, mu1);
+        terms[lane] = c;
+        __syncwarp();
+        const int nt = min(32, nT - t0);
+        for (int q0 = 0; q0 < nt; q0 += kStage) {
+          const int qn = min(kStage, nt - q0);
+          double2 sacc[kStage];
+#pragma unroll
+          for (int qq = 0; qq < kStage; ++qq) sacc[qq] = make_double2(0., 0.);
+          for (int k0 = 0; k0 < nr; k0 += 32) {
+            const int kn = min(32, nr - k0);
+            stage_sources(PQ, terms + q0, qn, nrow, nr, k0, kn, lane, vsh[wid]);
+            __syncwarp();
+            if (active) {
+#pragma unroll
+              for (int qq = 0; qq < kStage; ++qq) {
+                if (qq < qn && terms[q0 + qq].rowp >= 0) {
+                  const double* Fr = F + ((int64_t(nmax_F + terms[q0 + qq].dF) * nLF + L) * nrF + ij) * nrF;
+                  radial_sum(vsh[wid][qq], Fr, inds + k0, w + k0, kn, sacc[qq]);
+                }
+              }
+            }
+            __syncwarp();
           }
-          const int rowp = row_of_full[lm_full(Lp, abs(Mp), nLmax)];
-          if (rowp < 0) continue;
-          // plus part reads PQ[n3+mu3] (Mp >= 0) or conj(PQ[n3-mu3]); minus part the conjugates of those
-          const bool conj_src = (part == 0) ? (Mp < 0) : (Mp >= 0);
-          const double2* src = (Mp >= 0 ? PQ + (int64_t(n3 + mu3) * nrow + rowp) * nr
-                                        : PQ + (int64_t(n3 - mu3) * nrow + rowp) * nr);
-          double2 s = make_double2(0., 0.);
-          for (int k = 0; k < nr; ++k) {
-            const double wk = w[k];
-            if (wk == 0.0) continue;
-            double2 v = src[k];
-            if (conj_src) v.y = -v.y;
-            const double f = Fr[inds[k]] * wk;
-            s.x += v.x * f;
-            s.y += v.y * f;
+          if (active) {
+#pragma unroll
+            for (int qq = 0; qq < kStage; ++qq) {
+              if (qq < qn && terms[q0 + qq].rowp >= 0) {
+                const double2 r = cm(sacc[qq], terms[q0 + qq].g);
+                if (terms[q0 + qq].extra == 0) {
+                  plus.x += r.x;
+                  plus.y += r.y;
+                } else {
+                  minus.x += r.x;
+                  minus.y += r.y;
+                }
+              }
+            }
           }
-          const double2 c = cm(s, g);
-          if (part == 0) { plus.x += c.x; plus.y += c.y; } else { minus.x += c.x; minus.y += c.y; }
         }
+        __syncwarp();
+      }
+      if (active) {
+        const int64_t o = int64_t(fo) * nr + j;
+        out_re[o].x += plus.x + minus.x;
+        out_re[o].y += plus.y + minus.y;
+        out_im[o].x += plus.x - minus.x;
+        out_im[o].y += plus.y - minus.y;
       }
     }
-    const int64_t o = int64_t(full_of_row[i]) * nr + j;
-    out_re[o].x += plus.x + minus.x;
-    out_re[o].y += plus.y + minus.y;
-    out_im[o].x += plus.x - minus.x;
-    out_im[o].y += plus.y - minus.y;
   }
 }
 
 }  // namespace
 }  // namespace ps
 
+static int64_t row_grid(int nrow) {
+  int64_t g = (int64_t(nrow) + kRowWarps - 1) / kRowWarps;
+  return g > 148 * 16 ? 148 * 16 : g;
+}
+
 extern "C" int ps_tau_general_workspace_bytes(int nrow, int nr, size_t* bytes) {
   if (!bytes || nrow <= 0 || nr <= 0) return PS_ERR_INVALID;
-  *bytes = sizeof(double) * size_t((int64_t(nrow) * nr + 127) / 128);
+  *bytes = sizeof(double) * size_t(row_grid(nrow));
   return PS_OK;
 }
 
@@ -529,9 +660,10 @@ extern "C" int ps_tau_sum_general(const double* A, const double* B, const int* r
   if (!A || !B || !row_of_full || !rowL || !rowM || !F || !w || !out || nrow <= 0 || nr <= 0 || n < 0 || n > 16 ||
       n1 < 0 || n1 > 16 || n3 < 0 || n3 > 16 || n > nmax_F || Lmax >= nLF || Lmax > nLmax)
     return PS_ERR_INVALID;
-  const int64_t nblk = (int64_t(nrow) * nr + 127) / 128;
+  const int64_t nblk = row_grid(nrow);
   if (!workspace || workspace_bytes < sizeof(double) * size_t(nblk)) return PS_ERR_WORKSPACE;
-  tau_general_kernel<<<unsigned(nblk), 128, 0, stream>>>(
+  StatScope sc(PS_K_PIXEL, 0.0, 16.0 * double(nrow) * nr * (2 * n1 + 2 * n3 + 2), stream);
+  tau_general_kernel<<<unsigned(nblk), 32 * kRowWarps, 0, stream>>>(
       reinterpret_cast<const double2*>(A), reinterpret_cast<const double2*>(B), row_of_full, rowL, rowM, nrow, nLmax,
       Lmin, Lmax, F, nLF, nmax_F, w, nr, n1, n3, n, static_cast<double*>(workspace));
   PS_LAUNCH_CHECK();
@@ -548,9 +680,8 @@ extern "C" int ps_convolve_F_general(const double* PQ, const int* row_of_full, c
       nr <= 0 || nrF < nr || n < 0 || n > 16 || n1 < 0 || n1 > 16 || n3 < 0 || n3 > 16 || abs(mu1) > n1 ||
       n > nmax_F || Lmax >= nLF || Lmax > nLmax)
     return PS_ERR_INVALID;
-  int64_t g = (int64_t(nrow) * nr + 127) / 128;
-  if (g > 148 * 64) g = 148 * 64;
-  conv_general_kernel<<<int(g), 128, 0, stream>>>(reinterpret_cast<const double2*>(PQ), row_of_full, rowL, rowM,
+  StatScope sc(PS_K_PIXEL, 0.0, 16.0 * double(nrow) * nr * (2 * n3 + 3), stream);
+  conv_general_kernel<<<int(row_grid(nrow)), 32 * kRowWarps, 0, stream>>>(reinterpret_cast<const double2*>(PQ), row_of_full, rowL, rowM,
                                                   full_of_row, nrow, nLmax, Lmin, Lmax, F, nLF, nrF, nmax_F, w, inds,
                                                   nr, n1, n3, n, mu1, reinterpret_cast<double2*>(out_re),
                                                   reinterpret_cast<double2*>(out_im));

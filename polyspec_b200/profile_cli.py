@@ -39,6 +39,7 @@ neighbour rings, fill passes plus 50 smoothing passes; prints the neighbour-tabl
 build time and the inpaint_map time.
 """
 import argparse
+import re
 import sys
 
 import torch
@@ -242,10 +243,14 @@ def tspec(a):
         base = PolySpec(a.nside, dict(w['cltot']), beam=list(w['beam']), pol=True, prec=prec)
         wts = Weightings(base, np.stack([w['mask']] * 3), dict(w['cl']), noise_cov=W.white_noise_cov(a.nside))
         t0 = time.time()
-        tst = TSpecTemplate(base, w['mask'], wts.make_applySinv('ideal'), a.templates.split(","),
+        templates = re.split(r",(?=[A-Za-z])", a.templates)  # tauNL-direc:1,1,2 keeps its commas
+        r_weights = dict(w['r_weights'])
+        for t in templates:  # direction-dependent templates take the tauNL-loc radial weights
+            r_weights.setdefault(t, w['r_weights']['tauNL-loc'])
+        tst = TSpecTemplate(base, w['mask'], wts.make_applySinv('ideal'), templates,
                             w['k_arr'], w['Tl_arr'], w['lmin'], w['lmax'], r_values=w['r_values'],
-                            r_weights=w['r_weights'], rtau_values=w['rtau_values'], rtau_weights=w['rtau_weights'],
-                            C_phi=w['C_phi'], C_lens_weight=w['C_lens_weight'])
+                            r_weights=r_weights, rtau_values=w['rtau_values'], rtau_weights=w['rtau_weights'],
+                            C_phi=w['C_phi'], C_lens_weight=w['C_lens_weight'], Lmax=a.Lmax)
         torch.cuda.synchronize()
         t_setup = time.time() - t0
         a_lms = [base.generate_data(seed=21 + i, deconvolve_beam=True, output_type='harmonic', rng='device')
@@ -371,6 +376,9 @@ def main(argv=None):
     t.add_argument("--nr", type=int, default=24)
     t.add_argument("--reps", type=int, default=2)
     t.add_argument("--precs", default="fp64,mixed")
+    t.add_argument("--Lmax", type=int, default=None,
+                   help="exchange-momentum L range top (default min(3 Nside - 1, 2 lmax); templates with n > 0 "
+                        "need Lmax + n <= 3 Nside - 1)")
     t.add_argument("--templates", default="gNL-loc,lensing,point-source")
     tb = sub.add_parser("tspecbin")
     tb.add_argument("--nside", type=int, default=128)

@@ -353,6 +353,9 @@ class TSpecTemplate:
         self.nmax_F = int(np.max(self.n1n3n[:, 2])) if len(self.n1n3n) > 0 else 0
         self.nLmax = self.Lmax + self.nmax_F
         self.nLmin = self.Lmin - self.nmax_F
+        # (the reference fails later, indexing past the maps' harmonics, when this does not hold)
+        assert self.nLmax <= int(np.max(self.base.l_arr)), \
+            "Lmax + max(n) = %d exceeds the maps' lmax %d: lower Lmax" % (self.nLmax, int(np.max(self.base.l_arr)))
         self.nLfilt = (self.base.l_arr >= self.nLmin) & (self.base.l_arr <= self.nLmax)
         self.Ls, self.Ms = self.base.l_arr[self.nLfilt], self.base.m_arr[self.nLfilt]
         self.nLminfilt = self.base.l_arr[self.base.l_arr <= self.nLmax] >= self.nLmin

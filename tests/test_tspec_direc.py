@@ -146,3 +146,18 @@ def test_odd_even_decompositions():
             assert (n1, n3, n) in got and abs(n1 - n3) <= n <= n1 + n3 and np.isfinite(w)
     pe = (4. * np.pi) ** 1.5 / 3. / np.sqrt(5.)
     assert np.allclose([w for *_, w in t._direc_parts('tauNL-even:2')], [pe, 2 * pe], rtol=1e-15)
+
+
+def test_lmax_too_large_for_shifts():
+    """Lmax + n beyond the maps' lmax is refused while the templates are parsed."""
+    from polyspec_b200.tspec_template import TSpecTemplate
+    t = TSpecTemplate.__new__(TSpecTemplate)
+    t.templates = ['tauNL-direc:1,1,2']
+    t.Lmin, t.Lmax, t.lmin, t.lmax = 2, 47, 2, 30
+
+    class _Base:
+        l_arr = np.concatenate([np.arange(m, 48) for m in range(48)])
+        m_arr = np.concatenate([np.full(48 - m, m) for m in range(48)])
+    t.base = _Base()
+    with pytest.raises(AssertionError, match="Lmax"):
+        t._configure_templates(t.templates, [], {})
