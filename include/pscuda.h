@@ -366,15 +366,20 @@ int ps_product_q_complex(const double* Q, const double* F, int nmu, int mu1, int
  * ps_convolve_F_general: convolve_F_general of tauNL_utils.pyx:1069-1180 for one mu1: out_re/out_im complex
  *   [len(l <= nLmax)][nr] += plus +- minus at full_of_row[row] for rows with Lmin <= L <= Lmax; PQ [2n3+1][nrow][nr],
  *   F [2 nmax_F + 1][nLF][nrF][nrF] read at the radial indices inds [nr]. */
+/* ps_gaunt_row_table: gtab [nrow][n + 1][2n + 1][2], the Gaunt coefficients of every row for Delta = -n, -n+2, .., n,
+ *   mu = -n..n: part 0 Gaunt(L, L+Delta, n; -M, M-mu, mu), part 1 Gaunt(L, L+Delta, n; M, -M-mu, mu) (0 outside
+ *   Lmin <= L, L+Delta <= Lmax or |M'| > L+Delta); computed once per n and passed to the two contractions. */
+int ps_gaunt_row_table(const int* rowL, const int* rowM, int nrow, int Lmin, int Lmax, int n, double* gtab,
+                       cudaStream_t stream);
 int ps_tau_general_workspace_bytes(int nrow, int nr, size_t* bytes);
 int ps_tau_sum_general(const double* A, const double* B, const int* row_of_full, const int* rowL, const int* rowM,
                        int nrow, int nLmax, int Lmin, int Lmax, const double* F, int nLF, int nmax_F, const double* w,
-                       int nr, int n1, int n3, int n, double* out, void* workspace, size_t workspace_bytes,
-                       cudaStream_t stream);
+                       int nr, int n1, int n3, int n, const double* gtab, double* out, void* workspace,
+                       size_t workspace_bytes, cudaStream_t stream);
 int ps_convolve_F_general(const double* PQ, const int* row_of_full, const int* rowL, const int* rowM,
                           const int* full_of_row, int nrow, int nLmax, int Lmin, int Lmax, const double* F, int nLF,
                           int nrF, int nmax_F, const double* w, const int* inds, int nr, int n1, int n3, int n, int mu1,
-                          double* out_re, double* out_im, cudaStream_t stream);
+                          const double* gtab, double* out_re, double* out_im, cudaStream_t stream);
 int ps_shift_weight_workspace_bytes(int64_t ntarget, int n, size_t* bytes);
 int ps_shift_weight_map_all(const double* flX, int nshift, int lsize, int npol, int nr, const double* h, int64_t nsrc,
                             const int* src_l, const int* src_of_lm, int lmax_src, const int* tL, const int* tK,

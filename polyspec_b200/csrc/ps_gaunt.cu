@@ -376,6 +376,27 @@ __device__ __forceinline__ int64_t lm_full(int L, int M, int lmax) {
 // the r' sum of every term of the batch.  The coefficients are thus computed once per row, not
 // once per (row, r), and the terms are visited in (Delta, mu, mu1 / part) order.
 constexpr int kRowWarps = 4;
+constexpr int kMaxT3 = 33 * 33;  // (2 n1 + 1)(2 n + 1) for n1, n <= 16
+
+// Gaunt coefficients of every (L, M) row: gtab[row][(Delta + n) / 2][mu + n][part] with
+// part 0 = Gaunt(L, L+Delta, n; -M, M-mu, mu), part 1 = Gaunt(L, L+Delta, n; M, -M-mu, mu), 0 where
+// L+Delta lies outside [Lmin, Lmax] or the M' index outside L+Delta.  They depend on neither mu1,
+// the maps nor the weights, so one table serves every contraction of a given n.
+__global__ void gaunt_row_table_kernel(const int* __restrict__ rowL, const int* __restrict__ rowM, int nrow, int Lmin,
+                                       int Lmax, int n, double* __restrict__ out) {
+  const int nmu = 2 * n + 1, per = (n + 1) * nmu * 2;
+  const int64_t total = int64_t(nrow) * per;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = t / per;
+    const int r = int(t % per), part = r & 1, mu = (r >> 1) % nmu - n, Delta = 2 * ((r >> 1) / nmu) - n;
+    const int L = rowL[i], M = rowM[i], Lp = L + Delta;
+    const int Mp = part == 0 ? M - mu : -M - mu;
+    double G = 0.0;
+    if (L >= Lmin && L <= Lmax && Lp >= Lmin && Lp <= Lmax && abs(Mp) <= Lp)
+      G = part == 0 ? gaunt_small(L, Lp, n, -M, M - mu, mu) : gaunt_small(L, Lp, n, M, -M - mu, mu);
+    out[t] = G;
+  }
+}
 
 struct RowTerm {
   double2 g;   // complex coefficient
@@ -421,7 +442,8 @@ __device__ __forceinline__ void radial_sum(const double2* v, const double* __res
 // The coupling term t of row (L, M), built out of line so that its Gaunt and 3j evaluation does not
 // raise the register count of the r' loops.
 __device__ __noinline__ RowTerm tau_term(int t, int nT, int L, int M, const int* __restrict__ row_of_full, int nLmax,
-                                         int Lmin, int Lmax, int n1, int n3, int n) {
+                                         int Lmin, int Lmax, int n1, int n3, int n, const double* __restrict__ grow,
+                                         const double* t3tab) {
   RowTerm c;
   c.rowp = -1;
   if (t >= nT) return c;
@@ -431,8 +453,8 @@ __device__ __noinline__ RowTerm tau_term(int t, int nT, int L, int M, const int*
   const int Delta = 2 * (t / (nmu1 * nmu)) - n;
   const int Lp = L + Delta, Mp = -M - mu, mu3 = -mu1 - mu;
   if (Lp < Lmin || Lp > Lmax || abs(Mp) > Lp || abs(mu3) > n3) return c;
-  const double G = gaunt_small(L, Lp, n, M, -M - mu, mu);
-  double t3 = G != 0.0 ? threej_small(n1, n3, n, mu1, mu3, mu) : 0.0;
+  const double G = grow[(((Delta + n) / 2) * nmu + mu + n) * 2 + 1];
+  double t3 = G != 0.0 ? t3tab[(mu1 + n1) * nmu + mu + n] : 0.0;
   const int rowp = row_of_full[lm_full(Lp, abs(Mp), nLmax)];
   if (t3 == 0.0 || rowp < 0) return c;
   if (Mp < 0 && ((Mp + n3 + mu3) & 1)) t3 = -t3;
@@ -447,7 +469,8 @@ __device__ __noinline__ RowTerm tau_term(int t, int nT, int L, int M, const int*
 }
 
 __device__ __noinline__ RowTerm conv_term(int t, int nT, int L, int M, const int* __restrict__ row_of_full, int nLmax,
-                                          int Lmin, int Lmax, int n1, int n3, int n, int mu1) {
+                                          int Lmin, int Lmax, int n1, int n3, int n, int mu1,
+                                          const double* __restrict__ grow, const double* t3tab) {
   RowTerm c;
   c.rowp = -1;
   if (t >= nT) return c;
@@ -458,9 +481,8 @@ __device__ __noinline__ RowTerm conv_term(int t, int nT, int L, int M, const int
   const int Lp = L + Delta, mu3 = -mu1 - mu;
   const int Mp = part == 0 ? M - mu : -M - mu;
   if (Lp < Lmin || Lp > Lmax || abs(mu3) > n3 || (part == 1 && M == 0) || abs(Mp) > Lp) return c;
-  const double t3 = threej_small(n1, n3, n, mu1, mu3, mu);
-  double G = t3 != 0.0 ? (part == 0 ? gaunt_small(L, Lp, n, -M, M - mu, mu) : gaunt_small(L, Lp, n, M, -M - mu, mu))
-                       : 0.0;
+  const double t3 = t3tab[(mu1 + n1) * nmu + mu + n];
+  double G = t3 != 0.0 ? grow[(((Delta + n) / 2) * nmu + mu + n) * 2 + part] : 0.0;
   const int rowp = row_of_full[lm_full(Lp, abs(Mp), nLmax)];
   if (G == 0.0 || rowp < 0) return c;
   const double2 pref = make_double2(ipow(Delta).x * t3, ipow(Delta).y * t3);
@@ -487,7 +509,7 @@ __global__ void __launch_bounds__(32 * kRowWarps)
 tau_general_kernel(const double2* __restrict__ A, const double2* __restrict__ B, const int* __restrict__ row_of_full,
                    const int* __restrict__ rowL, const int* __restrict__ rowM, int nrow, int nLmax, int Lmin,
                    int Lmax, const double* __restrict__ F, int nLF, int nmax_F, const double* __restrict__ w, int nr,
-                   int n1, int n3, int n, double* __restrict__ partial) {
+                   int n1, int n3, int n, const double* __restrict__ gtab, double* __restrict__ partial) {
   __shared__ RowTerm sh[kRowWarps][32];
   __shared__ double2 vsh[kRowWarps][kStage][32];
   __shared__ double red[32 * kRowWarps];
@@ -495,6 +517,10 @@ tau_general_kernel(const double2* __restrict__ A, const double2* __restrict__ B,
   RowTerm* terms = sh[wid];
   const int nmu = 2 * n + 1, nmu1 = 2 * n1 + 1;
   const int nT = (n + 1) * nmu * nmu1;  // Delta = -n, -n + 2, ..., n (odd Delta + n: no Gaunt coupling)
+  __shared__ double t3tab[kMaxT3];
+  for (int q = threadIdx.x; q < nmu1 * nmu; q += blockDim.x)
+    t3tab[q] = threej_small(n1, n3, n, q / nmu - n1, -(q / nmu - n1) - (q % nmu - n), q % nmu - n);
+  __syncthreads();
   double acc = 0.0;
   for (int64_t i = blockIdx.x * int64_t(kRowWarps) + wid; i < nrow; i += int64_t(gridDim.x) * kRowWarps) {
     const int L = rowL[i], M = rowM[i];
@@ -503,7 +529,8 @@ tau_general_kernel(const double2* __restrict__ A, const double2* __restrict__ B,
       const int j = j0 + lane;
       const double wj = j < nr ? w[j] : 0.0;
       for (int t0 = 0; t0 < nT; t0 += 32) {
-        const RowTerm c = tau_term(t0 + lane, nT, L, M, row_of_full, nLmax, Lmin, Lmax, n1, n3, n);
+        const RowTerm c = tau_term(t0 + lane, nT, L, M, row_of_full, nLmax, Lmin, Lmax, n1, n3, n,
+                                   gtab + i * int64_t((n + 1) * nmu * 2), t3tab);
         terms[lane] = c;
         __syncwarp();
         const int nt = min(32, nT - t0);
@@ -569,14 +596,18 @@ __global__ void __launch_bounds__(32 * kRowWarps)
 conv_general_kernel(const double2* __restrict__ PQ, const int* __restrict__ row_of_full, const int* __restrict__ rowL,
                     const int* __restrict__ rowM, const int* __restrict__ full_of_row, int nrow, int nLmax, int Lmin,
                     int Lmax, const double* __restrict__ F, int nLF, int nrF, int nmax_F, const double* __restrict__ w,
-                    const int* __restrict__ inds, int nr, int n1, int n3, int n, int mu1, double2* __restrict__ out_re,
-                    double2* __restrict__ out_im) {
+                    const int* __restrict__ inds, int nr, int n1, int n3, int n, int mu1,
+                    const double* __restrict__ gtab, double2* __restrict__ out_re, double2* __restrict__ out_im) {
   __shared__ RowTerm sh[kRowWarps][32];
   __shared__ double2 vsh[kRowWarps][kStage][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   RowTerm* terms = sh[wid];
   const int nmu = 2 * n + 1;
   const int nT = (n + 1) * nmu * 2;  // (Delta, mu, part), part 0: M -> M - mu, part 1: M -> -M - mu
+  __shared__ double t3tab[kMaxT3];
+  for (int q = threadIdx.x; q < (2 * n1 + 1) * nmu; q += blockDim.x)
+    t3tab[q] = threej_small(n1, n3, n, q / nmu - n1, -(q / nmu - n1) - (q % nmu - n), q % nmu - n);
+  __syncthreads();
   for (int64_t i = blockIdx.x * int64_t(kRowWarps) + wid; i < nrow; i += int64_t(gridDim.x) * kRowWarps) {
     const int L = rowL[i], M = rowM[i], fo = full_of_row[i];
     if (L < Lmin || L > Lmax || fo < 0) continue;  // warp-uniform
@@ -586,7 +617,8 @@ conv_general_kernel(const double2* __restrict__ PQ, const int* __restrict__ row_
       const int ij = active ? inds[j] : 0;
       double2 plus = make_double2(0., 0.), minus = plus;
       for (int t0 = 0; t0 < nT; t0 += 32) {
-        const RowTerm c = conv_term(t0 + lane, nT, L, M, row_of_full, nLmax, Lmin, Lmax, n1, n3, n, mu1);
+        const RowTerm c = conv_term(t0 + lane, nT, L, M, row_of_full, nLmax, Lmin, Lmax, n1, n3, n, mu1,
+                                    gtab + i * int64_t(nT), t3tab);
         terms[lane] = c;
         __syncwarp();
         const int nt = min(32, nT - t0);
@@ -653,11 +685,23 @@ extern "C" int ps_tau_general_workspace_bytes(int nrow, int nr, size_t* bytes) {
   return PS_OK;
 }
 
+extern "C" int ps_gaunt_row_table(const int* rowL, const int* rowM, int nrow, int Lmin, int Lmax, int n, double* out,
+                                  cudaStream_t stream) {
+  if (!rowL || !rowM || !out || nrow <= 0 || n < 0 || n > 16) return PS_ERR_INVALID;
+  const int64_t total = int64_t(nrow) * (n + 1) * (2 * n + 1) * 2;
+  int64_t g = (total + 255) / 256;
+  if (g > 148 * 32) g = 148 * 32;
+  gaunt_row_table_kernel<<<int(g), 256, 0, stream>>>(rowL, rowM, nrow, Lmin, Lmax, n, out);
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}
+
 extern "C" int ps_tau_sum_general(const double* A, const double* B, const int* row_of_full, const int* rowL,
                                   const int* rowM, int nrow, int nLmax, int Lmin, int Lmax, const double* F, int nLF,
-                                  int nmax_F, const double* w, int nr, int n1, int n3, int n, double* out,
-                                  void* workspace, size_t workspace_bytes, cudaStream_t stream) {
-  if (!A || !B || !row_of_full || !rowL || !rowM || !F || !w || !out || nrow <= 0 || nr <= 0 || n < 0 || n > 16 ||
+                                  int nmax_F, const double* w, int nr, int n1, int n3, int n, const double* gtab,
+                                  double* out, void* workspace, size_t workspace_bytes, cudaStream_t stream) {
+  if (!A || !B || !row_of_full || !rowL || !rowM || !F || !w || !gtab || !out || nrow <= 0 || nr <= 0 || n < 0 ||
+      n > 16 ||
       n1 < 0 || n1 > 16 || n3 < 0 || n3 > 16 || n > nmax_F || Lmax >= nLF || Lmax > nLmax)
     return PS_ERR_INVALID;
   const int64_t nblk = row_grid(nrow);
@@ -665,7 +709,7 @@ extern "C" int ps_tau_sum_general(const double* A, const double* B, const int* r
   StatScope sc(PS_K_PIXEL, 0.0, 16.0 * double(nrow) * nr * (2 * n1 + 2 * n3 + 2), stream);
   tau_general_kernel<<<unsigned(nblk), 32 * kRowWarps, 0, stream>>>(
       reinterpret_cast<const double2*>(A), reinterpret_cast<const double2*>(B), row_of_full, rowL, rowM, nrow, nLmax,
-      Lmin, Lmax, F, nLF, nmax_F, w, nr, n1, n3, n, static_cast<double*>(workspace));
+      Lmin, Lmax, F, nLF, nmax_F, w, nr, n1, n3, n, gtab, static_cast<double*>(workspace));
   PS_LAUNCH_CHECK();
   sum_partials<<<1, 256, 0, stream>>>(static_cast<double*>(workspace), nblk, out);
   PS_LAUNCH_CHECK();
@@ -675,15 +719,17 @@ extern "C" int ps_tau_sum_general(const double* A, const double* B, const int* r
 extern "C" int ps_convolve_F_general(const double* PQ, const int* row_of_full, const int* rowL, const int* rowM,
                                      const int* full_of_row, int nrow, int nLmax, int Lmin, int Lmax, const double* F,
                                      int nLF, int nrF, int nmax_F, const double* w, const int* inds, int nr, int n1,
-                                     int n3, int n, int mu1, double* out_re, double* out_im, cudaStream_t stream) {
-  if (!PQ || !row_of_full || !rowL || !rowM || !full_of_row || !F || !w || !inds || !out_re || !out_im || nrow <= 0 ||
+                                     int n3, int n, int mu1, const double* gtab, double* out_re, double* out_im,
+                                     cudaStream_t stream) {
+  if (!PQ || !row_of_full || !rowL || !rowM || !full_of_row || !F || !w || !inds || !gtab || !out_re || !out_im ||
+      nrow <= 0 ||
       nr <= 0 || nrF < nr || n < 0 || n > 16 || n1 < 0 || n1 > 16 || n3 < 0 || n3 > 16 || abs(mu1) > n1 ||
       n > nmax_F || Lmax >= nLF || Lmax > nLmax)
     return PS_ERR_INVALID;
   StatScope sc(PS_K_PIXEL, 0.0, 16.0 * double(nrow) * nr * (2 * n3 + 3), stream);
   conv_general_kernel<<<int(row_grid(nrow)), 32 * kRowWarps, 0, stream>>>(reinterpret_cast<const double2*>(PQ), row_of_full, rowL, rowM,
                                                   full_of_row, nrow, nLmax, Lmin, Lmax, F, nLF, nrF, nmax_F, w, inds,
-                                                  nr, n1, n3, n, mu1, reinterpret_cast<double2*>(out_re),
+                                                  nr, n1, n3, n, mu1, gtab, reinterpret_cast<double2*>(out_re),
                                                   reinterpret_cast<double2*>(out_im));
   PS_LAUNCH_CHECK();
   return PS_OK;

@@ -200,6 +200,18 @@ class tauNL_utils:
                             torch.as_tensor(self._tau_tables()[2].astype(np.int32), device=d))
         return self._d_rows
 
+    def _gaunt_rows(self, n):
+        """Device table of the rows' Gaunt coefficients for momentum n (ps_gaunt_row_table), kept per n."""
+        if not hasattr(self, '_d_gtab'):
+            self._d_gtab = {}
+        if n not in self._d_gtab:
+            _, _, rowL, rowM, _ = self._row_tables()
+            t = torch.empty(len(self.Ls) * (n + 1) * (2 * n + 1) * 2, dtype=torch.float64, device=rowL.device)
+            _lib.call("ps_gaunt_row_table", ctypes.c_void_p(rowL.data_ptr()), ctypes.c_void_p(rowM.data_ptr()),
+                      len(self.Ls), self.Lmin, self.Lmax, int(n), ctypes.c_void_p(t.data_ptr()), _stream())
+            self._d_gtab[n] = t
+        return self._d_gtab[n]
+
     def tau_sum_general(self, _arr1, _arr2, _FLLs, _r_weights, n1, n3, n):
         """tauNL_utils.pyx:650-715: the (Delta, mu), (L, M), mu1, (r, r') sum of the direction-dependent tauNL
         estimator for arrays [2n+1, len(Ls), N_r] (ps_tau_sum_general)."""
@@ -222,7 +234,8 @@ class tauNL_utils:
                   ctypes.c_void_p(row_of_full.data_ptr()), ctypes.c_void_p(rowL.data_ptr()),
                   ctypes.c_void_p(rowM.data_ptr()), nrow, nLmax, self.Lmin, self.Lmax, ctypes.c_void_p(F.data_ptr()),
                   F.shape[1], (F.shape[0] - 1) // 2, ctypes.c_void_p(w.data_ptr()), nr, int(n1), int(n3), int(n),
-                  ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), int(nb.value), _stream())
+                  ctypes.c_void_p(self._gaunt_rows(int(n)).data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                  ctypes.c_void_p(ws.data_ptr()), int(nb.value), _stream())
         return float(out.item())
 
     def convolve_F_general(self, _PQ, _FLLs, _r_weights, out_real, out_imag, n1, n3, n, mu1, inds):
@@ -250,7 +263,8 @@ class tauNL_utils:
                   ctypes.c_void_p(full_of_row.data_ptr()), PQ.shape[1], nLmax, self.Lmin, self.Lmax,
                   ctypes.c_void_p(F.data_ptr()), F.shape[1], F.shape[2], (F.shape[0] - 1) // 2,
                   ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(ind.data_ptr()), len(inds), int(n1), int(n3), int(n),
-                  int(mu1), ctypes.c_void_p(o_re.data_ptr()), ctypes.c_void_p(o_im.data_ptr()), _stream())
+                  int(mu1), ctypes.c_void_p(self._gaunt_rows(int(n)).data_ptr()), ctypes.c_void_p(o_re.data_ptr()),
+                  ctypes.c_void_p(o_im.data_ptr()), _stream())
         for dst, src in ((out_real, o_re), (out_imag, o_im)):
             if isinstance(dst, torch.Tensor):
                 if dst.data_ptr() != src.data_ptr():
