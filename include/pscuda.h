@@ -361,11 +361,12 @@ int ps_product_q_complex(const double* Q, const double* F, int nmu, int mu1, int
                          const int* pq, const int* fi, int nw, double* out, cudaStream_t stream);
 /* ps_tau_sum_general: *out = tau_sum_general of polyspec/cython/tauNL_utils.pyx:650-715 for A [2n1+1][nrow][nr],
  *   B [2n3+1][nrow][nr] (complex, rows (rowL, rowM) of the L-list, row_of_full mapping the m-major index of (L, |M|),
- *   L <= nLmax, to a row or -1), F [2 nmax_F + 1][nLF][nr][nr], radial weights w [nr].  Workspace:
+ *   L <= nLmax, to a row or -1), FT [2 nmax_F + 1][nLF][nr][nr] = the reference's FLLs with its two radial axes
+ *   swapped (FT[..][k][j] = F_{L,L+Delta}(r_j, r'_k)), radial weights w [nr].  Workspace:
  *   ps_tau_general_workspace_bytes.
  * ps_convolve_F_general: convolve_F_general of tauNL_utils.pyx:1069-1180 for one mu1: out_re/out_im complex
  *   [len(l <= nLmax)][nr] += plus +- minus at full_of_row[row] for rows with Lmin <= L <= Lmax; PQ [2n3+1][nrow][nr],
- *   F [2 nmax_F + 1][nLF][nrF][nrF] read at the radial indices inds [nr]. */
+ *   FT [2 nmax_F + 1][nLF][nrF][nrF] (radial axes swapped as above) read at the radial indices inds [nr]. */
 /* ps_gaunt_row_table: gtab [nrow][n + 1][2n + 1][2], the Gaunt coefficients of every row for Delta = -n, -n+2, .., n,
  *   mu = -n..n: part 0 Gaunt(L, L+Delta, n; -M, M-mu, mu), part 1 Gaunt(L, L+Delta, n; M, -M-mu, mu) (0 outside
  *   Lmin <= L, L+Delta <= Lmax or |M'| > L+Delta); computed once per n and passed to the two contractions. */

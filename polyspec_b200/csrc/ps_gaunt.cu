@@ -353,7 +353,8 @@ extern "C" int ps_product_q_complex(const double* Q, const double* F, int nmu, i
 //    of the shifted [P Q] vectors (M -> M - mu and -M - mu), accumulated as plus + minus and
 //    plus - minus at the row of (L, M) in the l <= nLmax list.
 // Arrays are [mu][row][r] over a list of (L, M) rows (rowL, rowM); row_of_full maps the m-major
-// index of (L, |M|), L <= nLmax, to its row (-1: absent).
+// index of (L, |M|), L <= nLmax, to its row (-1: absent).  F comes transposed, [Delta][L][r'][r], so that
+// the lanes of a warp (one radial sample r each) read consecutive addresses.
 namespace ps {
 namespace {
 
@@ -425,15 +426,52 @@ __device__ __forceinline__ void stage_sources(const double2* __restrict__ src, c
 }
 
 // s += Sum_k v[k] F_j(r'_k) w_k over kn samples (F read at inds[k] when given), skipping zero weights
-// as the reference does, in the order of k.
-__device__ __forceinline__ void radial_sum(const double2* v, const double* __restrict__ Fr,
+// as the reference does, in the order of k; Fp, ld, jc as for radial_sum_list.
+__device__ __forceinline__ void radial_sum(const double2* v, const double* __restrict__ Fp, int64_t ld, int jc,
                                            const int* __restrict__ inds, const double* __restrict__ w, int kn,
                                            double2& s) {
   for (int k = 0; k < kn; ++k) {
     const double wk = w[k];
     if (wk == 0.0) continue;
     const double2 x = v[k];
-    const double f = Fr[inds ? inds[k] : k] * wk;
+    const double f = Fp[(inds ? inds[k] : k) * ld + jc] * wk;
+    s.x += x.x * f;
+    s.y += x.y * f;
+  }
+}
+
+// The radial samples with non-zero weight, in order, for N_r <= 32 (one staging chunk): their
+// index k, weight and F column (inds[k], or k); built once per block.
+struct RadialList {
+  int nk;
+  int k[32];
+  int col[32];
+  double w[32];
+};
+
+__device__ __forceinline__ void build_radial_list(RadialList& rl, const double* __restrict__ w,
+                                                  const int* __restrict__ inds, int nr) {
+  if (threadIdx.x == 0) {
+    int c = 0;
+    for (int k = 0; k < nr && k < 32; ++k) {
+      if (w[k] == 0.0) continue;
+      rl.k[c] = k;
+      rl.col[c] = inds ? inds[k] : k;
+      rl.w[c] = w[k];
+      ++c;
+    }
+    rl.nk = c;
+  }
+}
+
+// s += Sum over the listed samples of v[k] F_j(col) w, the same terms in the same order as radial_sum.
+// Fp is the (Delta, L) plane of the transposed F, [r'][r] with row stride ld, jc the lane's column.
+__device__ __forceinline__ void radial_sum_list(const double2* v, const double* __restrict__ Fp, int64_t ld, int jc,
+                                                const RadialList& rl, double2& s) {
+  const int nk = rl.nk;
+  for (int q = 0; q < nk; ++q) {
+    const double2 x = v[rl.k[q]];
+    const double f = Fp[rl.col[q] * ld + jc] * rl.w[q];
     s.x += x.x * f;
     s.y += x.y * f;
   }
@@ -518,8 +556,10 @@ tau_general_kernel(const double2* __restrict__ A, const double2* __restrict__ B,
   const int nmu = 2 * n + 1, nmu1 = 2 * n1 + 1;
   const int nT = (n + 1) * nmu * nmu1;  // Delta = -n, -n + 2, ..., n (odd Delta + n: no Gaunt coupling)
   __shared__ double t3tab[kMaxT3];
+  __shared__ RadialList rl;
   for (int q = threadIdx.x; q < nmu1 * nmu; q += blockDim.x)
     t3tab[q] = threej_small(n1, n3, n, q / nmu - n1, -(q / nmu - n1) - (q % nmu - n), q % nmu - n);
+  build_radial_list(rl, w, nullptr, nr);
   __syncthreads();
   double acc = 0.0;
   for (int64_t i = blockIdx.x * int64_t(kRowWarps) + wid; i < nrow; i += int64_t(gridDim.x) * kRowWarps) {
@@ -547,8 +587,11 @@ tau_general_kernel(const double2* __restrict__ A, const double2* __restrict__ B,
 #pragma unroll
               for (int qq = 0; qq < kStage; ++qq) {
                 if (qq < qn && terms[q0 + qq].rowp >= 0) {
-                  const double* Fr = F + ((int64_t(nmax_F + terms[q0 + qq].dF) * nLF + L) * nr + j) * nr + k0;
-                  radial_sum(vsh[wid][qq], Fr, nullptr, w + k0, kn, sacc[qq]);
+                  const double* Fp = F + (int64_t(nmax_F + terms[q0 + qq].dF) * nLF + L) * nr * nr;
+                  if (nr <= 32)
+                    radial_sum_list(vsh[wid][qq], Fp, nr, j, rl, sacc[qq]);
+                  else
+                    radial_sum(vsh[wid][qq], Fp + int64_t(k0) * nr, nr, j, nullptr, w + k0, kn, sacc[qq]);
                 }
               }
             }
@@ -605,8 +648,10 @@ conv_general_kernel(const double2* __restrict__ PQ, const int* __restrict__ row_
   const int nmu = 2 * n + 1;
   const int nT = (n + 1) * nmu * 2;  // (Delta, mu, part), part 0: M -> M - mu, part 1: M -> -M - mu
   __shared__ double t3tab[kMaxT3];
+  __shared__ RadialList rl;
   for (int q = threadIdx.x; q < (2 * n1 + 1) * nmu; q += blockDim.x)
     t3tab[q] = threej_small(n1, n3, n, q / nmu - n1, -(q / nmu - n1) - (q % nmu - n), q % nmu - n);
+  build_radial_list(rl, w, inds, nr);
   __syncthreads();
   for (int64_t i = blockIdx.x * int64_t(kRowWarps) + wid; i < nrow; i += int64_t(gridDim.x) * kRowWarps) {
     const int L = rowL[i], M = rowM[i], fo = full_of_row[i];
@@ -635,8 +680,11 @@ conv_general_kernel(const double2* __restrict__ PQ, const int* __restrict__ row_
 #pragma unroll
               for (int qq = 0; qq < kStage; ++qq) {
                 if (qq < qn && terms[q0 + qq].rowp >= 0) {
-                  const double* Fr = F + ((int64_t(nmax_F + terms[q0 + qq].dF) * nLF + L) * nrF + ij) * nrF;
-                  radial_sum(vsh[wid][qq], Fr, inds + k0, w + k0, kn, sacc[qq]);
+                  const double* Fp = F + (int64_t(nmax_F + terms[q0 + qq].dF) * nLF + L) * nrF * nrF;
+                  if (nr <= 32)
+                    radial_sum_list(vsh[wid][qq], Fp, nrF, ij, rl, sacc[qq]);
+                  else
+                    radial_sum(vsh[wid][qq], Fp, nrF, ij, inds + k0, w + k0, kn, sacc[qq]);
                 }
               }
             }

@@ -230,6 +230,7 @@ class tauNL_utils:
         _lib.call("ps_tau_general_workspace_bytes", nrow, nr, ctypes.byref(nb))
         ws = torch.empty(max(int(nb.value), 8), dtype=torch.uint8, device=a1.device)
         out = torch.zeros(1, dtype=torch.float64, device=a1.device)
+        F = F.transpose(2, 3).contiguous()  # the kernels read F_{L,L+Delta}(r, r') as [r'][r]
         _lib.call("ps_tau_sum_general", ctypes.c_void_p(a1.data_ptr()), ctypes.c_void_p(a2.data_ptr()),
                   ctypes.c_void_p(row_of_full.data_ptr()), ctypes.c_void_p(rowL.data_ptr()),
                   ctypes.c_void_p(rowM.data_ptr()), nrow, nLmax, self.Lmin, self.Lmax, ctypes.c_void_p(F.data_ptr()),
@@ -258,6 +259,7 @@ class tauNL_utils:
                              "N_r, N_r] with inds < N_r, outputs [len(l <= max(Ls)), len(inds)], |mu1| <= n1")
         if nr == 0:
             return
+        F = F.transpose(2, 3).contiguous()  # the kernels read F_{L,L+Delta}(r, r') as [r'][r]
         _lib.call("ps_convolve_F_general", ctypes.c_void_p(PQ.data_ptr()), ctypes.c_void_p(row_of_full.data_ptr()),
                   ctypes.c_void_p(rowL.data_ptr()), ctypes.c_void_p(rowM.data_ptr()),
                   ctypes.c_void_p(full_of_row.data_ptr()), PQ.shape[1], nLmax, self.Lmin, self.Lmax,
