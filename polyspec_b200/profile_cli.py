@@ -37,6 +37,12 @@ point source): Fisher contribution and numerator times, FP64 and mixed.
 inpainting of a T, Q, U map: --holes seeded point-source holes grown by --layers
 neighbour rings, fill passes plus 50 smoothing passes; prints the neighbour-table
 build time and the inpaint_map time.
+
+    python -m polyspec_b200.profile_cli tauconv [--Lmax 600 --nr 24 --n1 1 --n3 2 --n 2 --launches 4]
+
+one direction-dependent tauNL F convolution (tauNL_utils.convolve_F_general, mu1 = 0) over the
+(L, M) rows with L <= Lmax + 2 and random [P Q] vectors and F: --launches calls, the last timed
+with CUDA events (the first three are warm-ups).
 """
 import argparse
 import re
@@ -342,6 +348,35 @@ def tspecbin(a):
         print("tspecbin mixed vs fp64 Fisher: max |dF| / sqrt(F_ii F_jj) %.2e" % (np.abs(G - F) / d).max())
 
 
+def tauconv(a):
+    """The general F convolution alone (ps_convolve_F_general) on seeded random inputs."""
+    import numpy as np
+    from polyspec_b200 import pixel as P
+    nmax_F, top = max(a.n, 2), a.Lmax + 2
+    l = np.concatenate([np.arange(m, top + 1) for m in range(top + 1)]).astype(np.int32)
+    m = np.concatenate([np.full(top + 1 - mm, mm) for mm in range(top + 1)]).astype(np.int32)
+    ut = P.tauNL_utils(1, a.nr, l, m, 2, a.Lmax, l, m, l, m, nmax_F)
+    rng = np.random.default_rng(1)
+    dev = torch.device("cuda")
+    F = torch.as_tensor(rng.normal(size=(2 * nmax_F + 1, top + 1, a.nr, a.nr)), device=dev)
+    g = torch.Generator(device=dev).manual_seed(2)
+    PQ = torch.randn((2 * a.n3 + 1, len(l), a.nr), dtype=torch.complex128, device=dev, generator=g)
+    w = rng.uniform(0.5, 1.5, a.nr)
+    inds = np.arange(a.nr, dtype=np.int32)
+    o_re = torch.zeros((len(l), a.nr), dtype=torch.complex128, device=dev)
+    o_im = torch.zeros_like(o_re)
+    for _ in range(a.launches - 1):
+        ut.convolve_F_general(PQ, F, w, o_re, o_im, a.n1, a.n3, a.n, 0, inds)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ut.convolve_F_general(PQ, F, w, o_re, o_im, a.n1, a.n3, a.n, 0, inds)
+    e1.record()
+    torch.cuda.synchronize()
+    print("tauconv: %d rows, N_r %d, (n1, n3, n) = (%d, %d, %d): %.3f ms" % (len(l), a.nr, a.n1, a.n3, a.n,
+                                                                          e0.elapsed_time(e1)))
+
+
 def main(argv=None):
     p = argparse.ArgumentParser()
     sub = p.add_subparsers(dest="cmd", required=True)
@@ -370,6 +405,13 @@ def main(argv=None):
     b.add_argument("--reps", type=int, default=2)
     b.add_argument("--precs", default="fp64,mixed")
     b.add_argument("--numerator-only", action="store_true", help="only Bl_numerator (for kernel captures)")
+    c = sub.add_parser("tauconv")
+    c.add_argument("--Lmax", type=int, default=600)
+    c.add_argument("--nr", type=int, default=24)
+    c.add_argument("--n1", type=int, default=1)
+    c.add_argument("--n3", type=int, default=2)
+    c.add_argument("--n", type=int, default=2)
+    c.add_argument("--launches", type=int, default=4)
     t = sub.add_parser("tspec")
     t.add_argument("--nside", type=int, default=512)
     t.add_argument("--lmax", type=int, default=1000)
@@ -400,6 +442,8 @@ def main(argv=None):
         sht(a)
     elif a.cmd == "pix":
         pix(a)
+    elif a.cmd == "tauconv":
+        tauconv(a)
 
 
 if __name__ == "__main__":
