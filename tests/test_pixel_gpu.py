@@ -313,3 +313,35 @@ def test_tau_general(n1, n3, n):
         ut.convolve_F_general(PQ, F, w[:len(inds)].copy(), rr, ri, n1, n3, n, mu1, inds)
         mine.convolve_F_general(PQ, F, w[:len(inds)].copy(), gr, gi, n1, n3, n, mu1, inds)
         assert close(gr - o0r, rr - o0r, 1e-13) and close(gi - o0i, ri - o0i, 1e-13)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n1,n3,n", [(1, 2, 1), (2, 2, 2)])
+def test_tau_general_many_radii(n1, n3, n):
+    """tau_sum_general and convolve_F_general with more than 32 radial samples (the kernels' chunked
+    r' path: N_r 37, a 35-sample subset with a zero weight for the convolution) against the compiled
+    reference: 1e-12 relative for the sum, 1e-13 of the largest magnitude for the convolutions."""
+    from polyspec_b200 import pixel as P
+    T, _ = _ref()
+    if T is None:
+        pytest.skip("oracle/_ref is not built")
+    nr = 37
+    rng, Ls, F, w, args, nfull = _general_case(nr, max(n, 2), 7 + 100 * n1 + 10 * n3 + n, lmax_L=7, Lmax=5)
+    ut, mine = T.tauNL_utils(*args), P.tauNL_utils(*args)
+
+    def cplx(*shape):
+        return rng.normal(size=shape) + 1j * rng.normal(size=shape)
+
+    a1, a2 = cplx(2 * n1 + 1, len(Ls), nr), cplx(2 * n3 + 1, len(Ls), nr)
+    t_ref, t = ut.tau_sum_general(a1, a2, F, w, n1, n3, n), mine.tau_sum_general(a1, a2, F, w, n1, n3, n)
+    assert abs(t - t_ref) <= 1e-12 * max(abs(t_ref), 1e-300), (t, t_ref)
+    inds = np.concatenate([np.arange(0, 20), np.arange(22, 37)]).astype(np.int32)
+    PQ = cplx(2 * n3 + 1, len(Ls), len(inds))
+    wi = w[:len(inds)].copy()
+    wi[3] = 0.
+    for mu1 in range(-n1, n1 + 1):
+        o0r, o0i = cplx(nfull, len(inds)), cplx(nfull, len(inds))
+        rr, ri, gr, gi = o0r.copy(), o0i.copy(), o0r.copy(), o0i.copy()
+        ut.convolve_F_general(PQ, F, wi, rr, ri, n1, n3, n, mu1, inds)
+        mine.convolve_F_general(PQ, F, wi, gr, gi, n1, n3, n, mu1, inds)
+        assert close(gr - o0r, rr - o0r, 1e-13) and close(gi - o0i, ri - o0i, 1e-13)
