@@ -369,7 +369,11 @@ int ps_product_q_complex(const double* Q, const double* F, int nmu, int mu1, int
  *   FT [2 nmax_F + 1][nLF][nrF][nrF] (radial axes swapped as above) read at the radial indices inds [nr]. */
 /* ps_gaunt_row_table: gtab [nrow][n + 1][2n + 1][2], the Gaunt coefficients of every row for Delta = -n, -n+2, .., n,
  *   mu = -n..n: part 0 Gaunt(L, L+Delta, n; -M, M-mu, mu), part 1 Gaunt(L, L+Delta, n; M, -M-mu, mu) (0 outside
- *   Lmin <= L, L+Delta <= Lmax or |M'| > L+Delta); computed once per n and passed to the two contractions. */
+ *   Lmin <= L, L+Delta <= Lmax or |M'| > L+Delta); computed once per n and passed to the two contractions.
+ *   The gtab given to ps_tau_sum_general / ps_convolve_F_general must come from this function called with the
+ *   same (rowL, rowM, nrow, Lmin, Lmax, n) as the contraction: nothing checks this, and a table built for other
+ *   rows or another L range silently drops or keeps the wrong coupling terms.  The workspace of
+ *   ps_tau_sum_general depends on the current device's SM count: query it on the device that runs the call. */
 int ps_gaunt_row_table(const int* rowL, const int* rowM, int nrow, int Lmin, int Lmax, int n, double* gtab,
                        cudaStream_t stream);
 int ps_tau_general_workspace_bytes(int nrow, int nr, size_t* bytes);

@@ -7,7 +7,8 @@
 # Flags follow the reference's setup.py (-fopenmp -O3 -ffast-math
 # -march=broadwell); its GSL link libraries are dropped (ideal_fisher uses none).
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:-${PS_REFERENCE_ROOT:-}}
+[ -n "$REF" ] || { echo "usage: build_ref.sh <reference checkout> (or set PS_REFERENCE_ROOT)"; exit 1; }
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 SRC="$REF/polyspec/cython"

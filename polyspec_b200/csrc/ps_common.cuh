@@ -109,6 +109,20 @@ __host__ __device__ __forceinline__ void to_kscale(Scaled s, double& v, int& k) 
   v = ldexp(s.v, e);
 }
 
+// Streaming-multiprocessor count of the current device (read once per device and
+// kept), for grid caps that a workspace query and its launch must agree on.
+inline int device_sms() {
+  static int cached[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 148;
+    cached[dev] = n;
+  }
+  return cached[dev];
+}
+
 }  // namespace ps
 
 // launch-error helper for the C-ABI layer

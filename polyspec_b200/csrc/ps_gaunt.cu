@@ -722,9 +722,13 @@ conv_general_kernel(const double2* __restrict__ PQ, const int* __restrict__ row_
 }  // namespace
 }  // namespace ps
 
+// CTAs of the per-row contraction kernels: one per kRowWarps rows, at most 16 per SM of
+// the current device.  ps_tau_general_workspace_bytes and the launches both size by this
+// one function (one partial sum per CTA).
 static int64_t row_grid(int nrow) {
+  const int64_t cap = int64_t(ps::device_sms()) * 16;
   int64_t g = (int64_t(nrow) + kRowWarps - 1) / kRowWarps;
-  return g > 148 * 16 ? 148 * 16 : g;
+  return g > cap ? cap : g;
 }
 
 extern "C" int ps_tau_general_workspace_bytes(int nrow, int nr, size_t* bytes) {

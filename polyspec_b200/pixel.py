@@ -212,6 +212,20 @@ class tauNL_utils:
             self._d_gtab[n] = t
         return self._d_gtab[n]
 
+    def _F_rprime_major(self, src, F):
+        """F_{L,L+Delta}(r, r') as the general contractions read it, [r'][r] innermost.  The
+        estimator passes the same device FLLs for every mu1 and (n1, n3, n), so the transposed
+        copy of a CUDA tensor is kept and reused while that tensor is unchanged (same storage,
+        shape and version counter); numpy inputs are transposed per call."""
+        if not isinstance(src, torch.Tensor) or not src.is_cuda:
+            return F.transpose(2, 3).contiguous()
+        key = (src.data_ptr(), tuple(src.shape), tuple(src.stride()), src._version, src.dtype)
+        cache = self.__dict__.setdefault('_F_T_cache', {})
+        if cache.get('src') is not src or cache.get('key') != key:
+            cache['src'], cache['key'] = src, key
+            cache['F'] = F.transpose(2, 3).contiguous()
+        return cache['F']
+
     def tau_sum_general(self, _arr1, _arr2, _FLLs, _r_weights, n1, n3, n):
         """tauNL_utils.pyx:650-715: the (Delta, mu), (L, M), mu1, (r, r') sum of the direction-dependent tauNL
         estimator for arrays [2n+1, len(Ls), N_r] (ps_tau_sum_general)."""
@@ -230,7 +244,7 @@ class tauNL_utils:
         _lib.call("ps_tau_general_workspace_bytes", nrow, nr, ctypes.byref(nb))
         ws = torch.empty(max(int(nb.value), 8), dtype=torch.uint8, device=a1.device)
         out = torch.zeros(1, dtype=torch.float64, device=a1.device)
-        F = F.transpose(2, 3).contiguous()  # the kernels read F_{L,L+Delta}(r, r') as [r'][r]
+        F = self._F_rprime_major(_FLLs, F)
         _lib.call("ps_tau_sum_general", ctypes.c_void_p(a1.data_ptr()), ctypes.c_void_p(a2.data_ptr()),
                   ctypes.c_void_p(row_of_full.data_ptr()), ctypes.c_void_p(rowL.data_ptr()),
                   ctypes.c_void_p(rowM.data_ptr()), nrow, nLmax, self.Lmin, self.Lmax, ctypes.c_void_p(F.data_ptr()),
@@ -259,7 +273,7 @@ class tauNL_utils:
                              "N_r, N_r] with inds < N_r, outputs [len(l <= max(Ls)), len(inds)], |mu1| <= n1")
         if nr == 0:
             return
-        F = F.transpose(2, 3).contiguous()  # the kernels read F_{L,L+Delta}(r, r') as [r'][r]
+        F = self._F_rprime_major(_FLLs, F)
         _lib.call("ps_convolve_F_general", ctypes.c_void_p(PQ.data_ptr()), ctypes.c_void_p(row_of_full.data_ptr()),
                   ctypes.c_void_p(rowL.data_ptr()), ctypes.c_void_p(rowM.data_ptr()),
                   ctypes.c_void_p(full_of_row.data_ptr()), PQ.shape[1], nLmax, self.Lmin, self.Lmax,

@@ -353,9 +353,14 @@ class TSpecTemplate:
         self.nmax_F = int(np.max(self.n1n3n[:, 2])) if len(self.n1n3n) > 0 else 0
         self.nLmax = self.Lmax + self.nmax_F
         self.nLmin = self.Lmin - self.nmax_F
-        # (the reference fails later, indexing past the maps' harmonics, when this does not hold)
-        assert self.nLmax <= int(np.max(self.base.l_arr)), \
-            "Lmax + max(n) = %d exceeds the maps' lmax %d: lower Lmax" % (self.nLmax, int(np.max(self.base.l_arr)))
+        # The reference fails later when this does not hold: its default Lmax = min(base.lmax, 2 lmax)
+        # (polyspec/tspec_template.py:87-88) plus n > 0 asks to_lm_vec for L beyond base.lmax
+        # (:1302), whose output then no longer matches the l <= base.lmax filters (:443-447).
+        # Here the configuration is refused at construction, also under python -O.
+        if self.nLmax > int(np.max(self.base.l_arr)):
+            raise ValueError("Lmax + max(n) = %d exceeds the maps' lmax %d: pass Lmax <= %d"
+                             % (self.nLmax, int(np.max(self.base.l_arr)),
+                                int(np.max(self.base.l_arr)) - self.nmax_F))
         self.nLfilt = (self.base.l_arr >= self.nLmin) & (self.base.l_arr <= self.nLmax)
         self.Ls, self.Ms = self.base.l_arr[self.nLfilt], self.base.m_arr[self.nLfilt]
         self.nLminfilt = self.base.l_arr[self.base.l_arr <= self.nLmax] >= self.nLmin

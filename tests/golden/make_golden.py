@@ -127,7 +127,9 @@ def make(pol, ref):
 
 
 def main():
-    refroot = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    refroot = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PS_REFERENCE_ROOT", "")
+    if not refroot:
+        sys.exit("usage: %s <reference checkout> (or set PS_REFERENCE_ROOT)" % sys.argv[0])
     ref = reference_harness.load(refroot)
     for pol in (False, True):
         d = make(pol, ref)

@@ -73,7 +73,9 @@ def make(pol, ref, l_bins, fields, parity):
 
 
 def main():
-    refroot = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    refroot = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PS_REFERENCE_ROOT", "")
+    if not refroot:
+        sys.exit("usage: %s <reference checkout> (or set PS_REFERENCE_ROOT)" % sys.argv[0])
     ref = reference_harness.load(refroot, modules=("base", "weighting", "bspec_bin"))
     cases = [
         (False, [2, 6, 10, 16, 23], ['TTT'], 'even', "bspec_nside16_t.npz"),

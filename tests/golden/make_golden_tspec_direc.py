@@ -58,7 +58,9 @@ def make(pol, ref, TEMPLATES):
 
 
 def main():
-    refroot = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    refroot = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PS_REFERENCE_ROOT", "")
+    if not refroot:
+        sys.exit("usage: %s <reference checkout> (or set PS_REFERENCE_ROOT)" % sys.argv[0])
     ref = mgt.load_reference(refroot)
     for name, templates in TEMPLATE_SETS.items():
         for pol in (False, True):

@@ -68,7 +68,9 @@ CASES = [
 
 
 def main():
-    refroot = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    refroot = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PS_REFERENCE_ROOT", "")
+    if not refroot:
+        sys.exit("usage: %s <reference checkout> (or set PS_REFERENCE_ROOT)" % sys.argv[0])
     ref = reference_harness.load(refroot, modules=("base", "weighting", "tspec_bin"))
     for pol, l_bins, fields, parity, name in CASES:
         d = make(pol, ref, l_bins, fields, parity)

@@ -44,6 +44,40 @@ def test_noalloc_synthesis_matches_workspace_entry_point():
 
 
 @pytest.mark.gpu
+def test_noalloc_mixed_precision_matches_workspace_entry_point():
+    """The mixed-precision plan puts FP32 ring phases and the tensor-core Legendre stage's
+    inputs in the same static scratch: compare with ps_synthesis on the same plan handle and a
+    workspace the caller allocates (same kernels, so the results agree to rounding)."""
+    import torch
+    from polyspec_b200 import _lib
+    from polyspec_b200.sht import SHTPlan
+
+    L = _lib.lib()
+    plan = SHTPlan(32, 95, prec="mixed", autotune=False)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for call in range(2):
+        for spin, batch in ((0, 8), (2, 4), (3, 1)):
+            need = ctypes.c_size_t()
+            _lib.call("ps_sht_workspace_bytes", plan._h, batch, spin, 0, ctypes.byref(need))
+            assert need.value <= 16 * 1024 * 1024
+            g = torch.Generator(device="cuda").manual_seed(1000 + 100 * call + 10 * spin + batch)
+            shape = (batch, plan.nalm) if spin == 0 else (batch, 2, plan.nalm)
+            alm = torch.randn(shape, dtype=torch.complex128, device="cuda", generator=g)
+            npix_shape = (batch, plan.npix) if spin == 0 else (batch, 2, plan.npix)
+            ref = torch.empty(npix_shape, dtype=torch.float64, device="cuda")
+            ws = torch.empty(max(need.value, 256), dtype=torch.uint8, device="cuda")
+            _lib.call("ps_synthesis", plan._h, ctypes.c_void_p(alm.data_ptr()), ctypes.c_void_p(ref.data_ptr()),
+                      batch, spin, ctypes.c_void_p(ws.data_ptr()), need.value, stream)
+            out = torch.full_like(ref, float("nan"))
+            rc = L.ps_synthesis_noalloc(plan._h, ctypes.c_void_p(alm.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                        batch, spin, stream)
+            assert rc == 0, _lib.lib().ps_error_string(rc)
+            torch.cuda.synchronize()
+            assert plan.error_flag() == 0
+            assert _rel(out, ref) < TOL, (call, spin, batch)
+
+
+@pytest.mark.gpu
 def test_noalloc_rejects_requests_beyond_its_scratch():
     import torch
     from polyspec_b200 import _lib
