@@ -159,5 +159,5 @@ def test_lmax_too_large_for_shifts():
         l_arr = np.concatenate([np.arange(m, 48) for m in range(48)])
         m_arr = np.concatenate([np.full(48 - m, m) for m in range(48)])
     t.base = _Base()
-    with pytest.raises(AssertionError, match="Lmax"):
+    with pytest.raises(ValueError, match="Lmax"):
         t._configure_templates(t.templates, [], {})
