@@ -74,7 +74,26 @@ int ps_plan_set_tile(ps_plan* plan, int direction, int spin, int tile);
  * synthesis' Legendre stage runs on the tensor cores (tcgen05, TF32 split in
  * three products, FP32 accumulation) from FP64 recurrences; the adjoint's
  * Legendre stage contracts FP32-rounded FP64 recurrences with FP32 FMAs; the
- * ring transforms run in FP32; inputs and outputs stay FP64 in both cases. */
+ * ring transforms run in FP32; inputs and outputs stay FP64 in both cases.
+ *
+ * Legendre tables (mixed plans only; no reference counterpart -- ducc0 always
+ * recomputes the recurrences).  ps_plan_build_table computes the FP32 Legendre
+ * values of one spin once (FP64 recurrence, as the on-the-fly kernels) into a
+ * table the plan owns (ps_plan_table_bytes: Rh * nalm * 4 bytes for spin 0,
+ * twice that for spin s, Rh = 2 nside rounded up to 128; 17.7 GB and 35.4 GB
+ * at nside 1024, lmax 2048).  From then on both Legendre stages of that spin
+ * -- on the plan and on its band plans -- are streaming tensor-core GEMMs over
+ * the table (TF32 split in three products, FP32 sums), and the adjoint writes
+ * alm without per-ring-tile partial sums (its workspace shrinks: query
+ * ps_sht_workspace_bytes after building).  The build allocates (cudaMalloc)
+ * and enqueues on `stream`; it returns PS_ERR_NOMEM when the table does not
+ * fit, PS_ERR_UNSUPPORTED on FP64 or band plans.  ps_plan_drop_tables frees
+ * them (after synchronising the device); ps_plan_has_table tells whether a
+ * spin's transforms use one. */
+int ps_plan_table_bytes(const ps_plan* plan, int spin, size_t* bytes);
+int ps_plan_build_table(ps_plan* plan, int spin, cudaStream_t stream);
+int ps_plan_has_table(const ps_plan* plan, int spin, int* has);
+int ps_plan_drop_tables(ps_plan* plan);
 
 /* Scratch bytes needed by ps_synthesis / ps_adjoint for `batch` maps of `spin`. */
 int ps_sht_workspace_bytes(const ps_plan* plan, int batch, int spin, int adjoint, size_t* bytes);
@@ -90,6 +109,24 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
  * polyspec/base.py:147-151 (to_lm), :193 and :206 (to_lm_vec), :253 (to_lm_spin). */
 int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, int spin, double scale,
                void* workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/* Fused weighted round trip of the masked CG operator (no single reference call;
+ * replaces, per spin, the pair to_map -> pixel weight -> to_lm inside
+ * CGD._apply_A at polyspec/weighting.py:297-299):
+ *   alm_out[b] = scale * lscale * Y^H W Y (lscale * alm_in[b])
+ * with Y this plan's synthesis of `spin`, W = weight [ncomp][npix] (float64;
+ * spin 0: one component; spin s: Q and U), lscale [ncomp][nalm] (float64, e.g.
+ * the beam per lm; NULL = 1).  alm element (b, c, idx) is at
+ * alm[b * alm_stride + c * nalm + idx] (complex128; alm_stride >= ncomp * nalm
+ * complex elements, so T and (E, B) of a [batch][3][nalm] array are used in
+ * place).  Needs a mixed plan holding the Legendre table of `spin`
+ * (ps_plan_build_table); PS_ERR_UNSUPPORTED otherwise.  The maps are never
+ * written to memory: each ring is synthesised, weighted and transformed back
+ * in shared memory.  alm_in and alm_out must not overlap. */
+int ps_roundtrip_workspace_bytes(const ps_plan* plan, int batch, int spin, size_t* bytes);
+int ps_sht_weighted_roundtrip(const ps_plan* plan, const double* alm_in, double* alm_out, int64_t alm_stride,
+                              int batch, int spin, const double* weight, const double* lscale, double scale,
+                              void* workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* Legendre stages alone (no reference counterpart; ducc0 exposes the same split
  * as its leg2alm / alm2leg), in the plan's precision (a mixed plan converts the

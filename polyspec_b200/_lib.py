@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "libpscuda.so")
 
 PS_OK = 0
 PS_ERR_UNSUPPORTED = -2
+PS_ERR_NOMEM = -3
 PS_ERR_NOT_CONVERGED = -6
 PS_PREC_FP64 = 0
 PS_PREC_MIXED = 1
@@ -37,6 +38,13 @@ SIGNATURES = {
     "ps_synthesis_noalloc": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p]),
     "ps_plan_band": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_void_p)]),
     "ps_plan_set_tile": (_c_int, [_c_void_p, _c_int, _c_int, _c_int]),
+    "ps_plan_table_bytes": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_size_t)]),
+    "ps_plan_build_table": (_c_int, [_c_void_p, _c_int, _c_void_p]),
+    "ps_plan_has_table": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_int)]),
+    "ps_plan_drop_tables": (_c_int, [_c_void_p]),
+    "ps_roundtrip_workspace_bytes": (_c_int, [_c_void_p, _c_int, _c_int, ctypes.POINTER(_c_size_t)]),
+    "ps_sht_weighted_roundtrip": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int64, _c_int, _c_int, _c_void_p,
+                                           _c_void_p, _c_double, _c_void_p, _c_size_t, _c_void_p]),
     "ps_legendre_workspace_bytes": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_legendre_synthesis": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p, _c_size_t,
                                        _c_void_p]),

@@ -46,6 +46,11 @@ struct Plan {
   double2* d_bs_spec;       // Bluestein spectra (FP64)
   float2* d_twiddle_f;      // FP32 copies for the mixed-precision ring transforms
   float2* d_bs_spec_f;
+  // mixed plans: e^{i m phi0} of every north ring (the mirror ring has the same phi0),
+  // [Rh][mmax+1], and the Bluestein chirps e^{-i pi j^2 / N}, j < N, of every slot
+  float2* d_rot_f;
+  float2* d_chirp_f;
+  int64_t* d_chirp_off;
   int* d_err;               // device error flag raised by kernels whose bounded waits expired
   int64_t* d_bs_off;        // [nslots]
   int n_bs_slots;
@@ -54,6 +59,13 @@ struct Plan {
   // maps per CTA of the Legendre stages, [direction 0 synthesis / 1 adjoint][spin];
   // 0 = the launcher's own choice (set by ps_plan_set_tile, e.g. from the autotuner)
   int tile[2][4];
+  // Legendre tables of a mixed-precision plan (ps_plan_build_table), per spin; null when
+  // not built.  d_tab_off [mmax+2]: first table block of each order; d_tab_work: the
+  // (m, first block) list of the table adjoint's CTAs.
+  float* d_tab[4];
+  int64_t* d_tab_off;
+  int2* d_tab_work;
+  int tab_nwork;
 };
 
 // ---------------------------------------------------------------------------

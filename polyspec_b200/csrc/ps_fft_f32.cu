@@ -22,7 +22,9 @@
 // FFTs are radix-2 with stages fused in pairs (one barrier and one shared-memory
 // round trip per two stages): decimation in frequency for power-of-two rings,
 // Bluestein's chirp-z convolution of power-of-two length M >= 2 nphi - 1 for the
-// others.  Rings are launched in classes of equal work length.
+// others.  Rings are launched in classes of equal work length.  The ring rotations
+// e^{i m phi0} and the Bluestein chirps come from tables of the plan (computed in FP64
+// on the host), so no kernel evaluates a sine or cosine.
 #include "ps_common.cuh"
 #include "ps_stats.cuh"
 
@@ -38,14 +40,6 @@ __device__ __forceinline__ float2 fconj2(float2 a) { return make_float2(a.x, -a.
 __device__ __forceinline__ int bitrev_f(int i, int logn) { return (int)(__brev((unsigned)i) >> (32 - logn)); }
 __device__ __forceinline__ int ilog2_f(int n) { return 31 - __clz(n); }
 
-// e^{i pi q / den} for integer q (exact argument reduction modulo 2 den)
-__device__ __forceinline__ float2 expi_pi_ratio_f(int64_t q, int64_t den) {
-  q %= 2 * den;
-  if (q < 0) q += 2 * den;
-  float s, c;
-  sincospif(float(double(q) / double(den)), &s, &c);
-  return make_float2(c, s);
-}
 
 // twiddle e^{sign 2 pi i j / 2^s} from tw[k] = e^{-2 pi i k / 2^twlog}
 __device__ __forceinline__ float2 twid(const float2* __restrict__ tw, int j, int s, int twlog, int sign) {
@@ -121,12 +115,8 @@ __device__ void fft_dit_f(float2* a, int logn, int sign, const float2* __restric
 struct RingDFTf {
   int N, M, logM;
   bool bluestein;
+  const float2* chirp;  // e^{-i pi j^2 / N}, j < N (the plan's table of this ring length)
 };
-
-__device__ __forceinline__ float2 chirp_f(int j, int N) {
-  const int64_t q = (int64_t(j) * j) % (2 * int64_t(N));
-  return expi_pi_ratio_f(-q, N);
-}
 
 // In-place forward DFT (sign -1) of buf[0..N); read results with dft_get_f.
 __device__ void ring_dft_forward_f(float2* buf, const RingDFTf& d, const float2* __restrict__ tw, int twlog,
@@ -135,7 +125,7 @@ __device__ void ring_dft_forward_f(float2* buf, const RingDFTf& d, const float2*
     fft_dif_f(buf, d.logM, -1, tw, twlog, u, T);
     return;
   }
-  for (int j = u; j < d.M; j += T) buf[j] = (j < d.N) ? fmul2(buf[j], chirp_f(j, d.N)) : make_float2(0.f, 0.f);
+  for (int j = u; j < d.M; j += T) buf[j] = (j < d.N) ? fmul2(buf[j], d.chirp[j]) : make_float2(0.f, 0.f);
   __syncthreads();
   fft_dif_f(buf, d.logM, -1, tw, twlog, u, T);
   for (int p = u; p < d.M; p += T) buf[p] = fmul2(buf[p], bspec[p]);
@@ -145,17 +135,19 @@ __device__ void ring_dft_forward_f(float2* buf, const RingDFTf& d, const float2*
 
 __device__ __forceinline__ float2 dft_get_f(const float2* buf, const RingDFTf& d, int k) {
   if (!d.bluestein) return buf[bitrev_f(k, d.logM)];
-  const float2 v = fmul2(buf[k], chirp_f(k, d.N));
+  const float2 v = fmul2(buf[k], d.chirp[k]);
   const float s = 1.0f / float(d.M);
   return make_float2(v.x * s, v.y * s);
 }
 
-__device__ __forceinline__ RingDFTf make_dft(const RingInfo& g) {
+__device__ __forceinline__ RingDFTf make_dft(const RingInfo& g, const float2* __restrict__ chirp,
+                                             const int64_t* __restrict__ chirp_off) {
   RingDFTf d;
   d.N = g.nphi;
   d.bluestein = g.bs_slot >= 0;
   d.M = d.bluestein ? g.bs_m : d.N;
   d.logM = ilog2_f(d.M);
+  d.chirp = d.bluestein ? chirp + chirp_off[g.bs_slot] : nullptr;
   return d;
 }
 
@@ -165,8 +157,9 @@ __device__ __forceinline__ RingDFTf make_dft(const RingInfo& g) {
 __global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list, int R,
                                const float2* __restrict__ phase, double* __restrict__ map, int mmax, int nf,
                                int64_t npix, const float2* __restrict__ tw, int twlog,
-                               const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T,
-                               int pack) {
+                               const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off,
+                               const float2* __restrict__ rot, const float2* __restrict__ chirp,
+                               const int64_t* __restrict__ chirp_off, int T, int pack) {
   extern __shared__ float2 fbuf[];
   const int ir = ring_list[blockIdx.y];
   // partner of a packed FFT: the other component of the same map (pack), else the
@@ -174,7 +167,8 @@ __global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __
   const int irb = pack ? ir : R - 1 - ir;
   const RingInfo g = rings[ir];
   const int64_t start_b = rings[irb].start;
-  const RingDFTf d = make_dft(g);
+  const RingDFTf d = make_dft(g, chirp, chirp_off);
+  const float2* rotr = rot + int64_t(min(ir, R - 1 - ir)) * (mmax + 1);  // e^{i m phi0} of this ring
   const float2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
   const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
   const int G = blockDim.x / T;
@@ -183,7 +177,6 @@ __global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __
   const bool va = fa < nf, vb = pack ? fb < nf : (va && irb != ir);
   float2* buf = fbuf + size_t(grp) * d.M;
   const int N = d.N;
-  const int64_t pden = g.phi_den;
   const float2* pha = phase + int64_t(ir) * (mmax + 1) * nf;
   const float2* phb = phase + int64_t(irb) * (mmax + 1) * nf;
   // buf_k = conj(c_a,k) + i conj(c_b,k);  c_k = sum_{m=k mod N} F_m e^{i m phi0} + sum_{m=-k mod N, m>0} conj(...)
@@ -191,12 +184,12 @@ __global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __
     float2 ca = make_float2(0.f, 0.f), cb = ca;
     if (va) {
       for (int m = kk; m <= mmax; m += N) {
-        const float2 e = expi_pi_ratio_f(int64_t(m) * g.phi_num, pden);
+        const float2 e = rotr[m];
         ca = fadd2(ca, fmul2(pha[int64_t(m) * nf + fa], e));
         if (vb) cb = fadd2(cb, fmul2(phb[int64_t(m) * nf + fb], e));
       }
       for (int m = (kk == 0) ? N : N - kk; m <= mmax; m += N) {
-        const float2 e = expi_pi_ratio_f(int64_t(m) * g.phi_num, pden);
+        const float2 e = rotr[m];
         ca = fadd2(ca, fconj2(fmul2(pha[int64_t(m) * nf + fa], e)));
         if (vb) cb = fadd2(cb, fconj2(fmul2(phb[int64_t(m) * nf + fb], e)));
       }
@@ -224,8 +217,9 @@ __global__ void ring_synth_f32(const RingInfo* __restrict__ rings, const int* __
 __global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list, int R,
                                  const double* __restrict__ map, float2* __restrict__ phase, int mmax, int nf,
                                  int64_t npix, const float2* __restrict__ tw, int twlog,
-                                 const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off, int T,
-                               int pack) {
+                                 const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off,
+                               const float2* __restrict__ rot, const float2* __restrict__ chirp,
+                               const int64_t* __restrict__ chirp_off, int T, int pack) {
   extern __shared__ float2 fbuf[];
   const int ir = ring_list[blockIdx.y];
   // partner of a packed FFT: the other component of the same map (pack), else the
@@ -233,7 +227,8 @@ __global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* 
   const int irb = pack ? ir : R - 1 - ir;
   const RingInfo g = rings[ir];
   const int64_t start_b = rings[irb].start;
-  const RingDFTf d = make_dft(g);
+  const RingDFTf d = make_dft(g, chirp, chirp_off);
+  const float2* rotr = rot + int64_t(min(ir, R - 1 - ir)) * (mmax + 1);  // e^{i m phi0} of this ring
   const float2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
   const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
   const int G = blockDim.x / T;
@@ -242,7 +237,6 @@ __global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* 
   const bool va = fa < nf, vb = pack ? fb < nf : (va && irb != ir);
   float2* buf = fbuf + size_t(grp) * d.M;
   const int N = d.N;
-  const int64_t pden = g.phi_den;
   {
     const double* ia = map + int64_t(va ? fa : 0) * npix + g.start;
     const double* ib = map + int64_t(vb ? fb : 0) * npix + (vb ? start_b : g.start);
@@ -256,9 +250,95 @@ __global__ void ring_adjoint_f32(const RingInfo* __restrict__ rings, const int* 
     for (int m = u; m <= mmax; m += T) {
       const int k = m % N, k2 = (N - k) % N;
       const float2 z = dft_get_f(buf, d, k), z2 = fconj2(dft_get_f(buf, d, k2));
-      const float2 e = expi_pi_ratio_f(-int64_t(m) * g.phi_num, pden);
+      const float2 e = fconj2(rotr[m]);
       const float2 xa = make_float2(0.5f * (z.x + z2.x), 0.5f * (z.y + z2.y));
       // (z - z2) / (2i) = -i (z - z2) / 2
+      const float2 xb = make_float2(0.5f * (z.y - z2.y), -0.5f * (z.x - z2.x));
+      pha[int64_t(m) * nf + fa] = fmul2(xa, e);
+      if (vb) phb[int64_t(m) * nf + fb] = fmul2(xb, e);
+    }
+  }
+}
+
+// synthesis -> pixel weights -> adjoint of the same rings, in place on the phases:
+//   phase [R][mmax+1][nf] (complex64)  ->  P'_m = sum_j w_j map_j e^{-i m (phi0 + 2 pi j / nphi)}
+// with map = the ring's synthesis of the phases and w the per-pixel weight of each field
+// (weight [ncw][npix]: field a reads component 0, field b component 1 for a spin map, or
+// component 0 on the mirror ring for spin 0).  The map never leaves shared memory: between the
+// two DFTs each thread weights the pixels it owns (natural order for the second DFT: the
+// bit-reversal of the first undone in place, in pairs).  The block reads every phase it writes
+// before the first barrier, so in place is safe.
+__global__ void ring_roundtrip_f32(const RingInfo* __restrict__ rings, const int* __restrict__ ring_list, int R,
+                                   float2* __restrict__ phase, int mmax, int nf, const double* __restrict__ weight,
+                                   int64_t npix, const float2* __restrict__ tw, int twlog,
+                                   const float2* __restrict__ bs_spec, const int64_t* __restrict__ bs_off,
+                                   const float2* __restrict__ rot, const float2* __restrict__ chirp,
+                                   const int64_t* __restrict__ chirp_off, int T, int pack) {
+  extern __shared__ float2 fbuf[];
+  const int ir = ring_list[blockIdx.y];
+  const int irb = pack ? ir : R - 1 - ir;
+  const RingInfo g = rings[ir];
+  const int64_t start_b = rings[irb].start;
+  const RingDFTf d = make_dft(g, chirp, chirp_off);
+  const float2* rotr = rot + int64_t(min(ir, R - 1 - ir)) * (mmax + 1);  // e^{i m phi0} of this ring
+  const float2* bspec = d.bluestein ? bs_spec + bs_off[g.bs_slot] : nullptr;
+  const int grp = threadIdx.x / T, u = threadIdx.x - grp * T;
+  const int G = blockDim.x / T;
+  const int unit = blockIdx.x * G + grp;
+  const int fa = pack ? 2 * unit : unit, fb = pack ? fa + 1 : unit;
+  const bool va = fa < nf, vb = pack ? fb < nf : (va && irb != ir);
+  float2* buf = fbuf + size_t(grp) * d.M;
+  const int N = d.N;
+  float2* pha = phase + int64_t(ir) * (mmax + 1) * nf;
+  float2* phb = phase + int64_t(irb) * (mmax + 1) * nf;
+  for (int kk = u; kk < N; kk += T) {
+    float2 ca = make_float2(0.f, 0.f), cb = ca;
+    if (va) {
+      for (int m = kk; m <= mmax; m += N) {
+        const float2 e = rotr[m];
+        ca = fadd2(ca, fmul2(pha[int64_t(m) * nf + fa], e));
+        if (vb) cb = fadd2(cb, fmul2(phb[int64_t(m) * nf + fb], e));
+      }
+      for (int m = (kk == 0) ? N : N - kk; m <= mmax; m += N) {
+        const float2 e = rotr[m];
+        ca = fadd2(ca, fconj2(fmul2(pha[int64_t(m) * nf + fa], e)));
+        if (vb) cb = fadd2(cb, fconj2(fmul2(phb[int64_t(m) * nf + fb], e)));
+      }
+    }
+    if (kk == 0) { ca.y = 0.f; cb.y = 0.f; }
+    buf[kk] = make_float2(ca.x + cb.y, -ca.y + cb.x);
+  }
+  __syncthreads();
+  ring_dft_forward_f(buf, d, tw, twlog, bspec, u, T);
+  // pixel j of field a is Re y_j, of field b Im y_j (y_j = dft_get_f(buf, d, j)); weight them
+  const double* wa = weight + g.start;
+  const double* wb = weight + (pack ? npix : 0) + start_b;
+  if (!d.bluestein) {
+    for (int j = u; j < N; j += T) {
+      const int jr = bitrev_f(j, d.logM);
+      if (j < jr) {
+        const float2 yj = buf[jr], yr = buf[j];
+        buf[j] = make_float2(va ? float(wa[j]) * yj.x : 0.f, vb ? float(wb[j]) * yj.y : 0.f);
+        buf[jr] = make_float2(va ? float(wa[jr]) * yr.x : 0.f, vb ? float(wb[jr]) * yr.y : 0.f);
+      } else if (j == jr) {
+        const float2 yj = buf[j];
+        buf[j] = make_float2(va ? float(wa[j]) * yj.x : 0.f, vb ? float(wb[j]) * yj.y : 0.f);
+      }
+    }
+  } else {
+    for (int j = u; j < N; j += T) {
+      const float2 yj = dft_get_f(buf, d, j);
+      buf[j] = make_float2(va ? float(wa[j]) * yj.x : 0.f, vb ? float(wb[j]) * yj.y : 0.f);
+    }
+  }
+  __syncthreads();
+  ring_dft_forward_f(buf, d, tw, twlog, bspec, u, T);
+  if (va) {
+    for (int m = u; m <= mmax; m += T) {
+      const int k = m % N, k2 = (N - k) % N;
+      const float2 z = dft_get_f(buf, d, k), z2 = fconj2(dft_get_f(buf, d, k2));
+      const float2 e = fconj2(rotr[m]);
+      const float2 xa = make_float2(0.5f * (z.x + z2.x), 0.5f * (z.y + z2.y));
       const float2 xb = make_float2(0.5f * (z.y - z2.y), -0.5f * (z.x - z2.x));
       pha[int64_t(m) * nf + fa] = fmul2(xa, e);
       if (vb) phb[int64_t(m) * nf + fb] = fmul2(xb, e);
@@ -289,7 +369,8 @@ int launch_ring_synth_f32(const Plan& P, const int* d_list, int nrings, int work
   while ((1 << twlog) < P.max_fft) ++twlog;
   StatScope sc(PS_K_FFT_SYNTH, 0.0, 0.0, st);
   ring_synth_f32<<<dim3(gy, nrings), T * G, smem, st>>>(P.d_rings, d_list, P.R, phase, map, P.mmax, nf, P.npix,
-                                                         P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off, T, pack);
+                                                         P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off,
+                                                         P.d_rot_f, P.d_chirp_f, P.d_chirp_off, T, pack);
   PS_LAUNCH_CHECK();
   return PS_OK;
 }
@@ -310,7 +391,32 @@ int launch_ring_adjoint_f32(const Plan& P, const int* d_list, int nrings, int wo
   while ((1 << twlog) < P.max_fft) ++twlog;
   StatScope sc(PS_K_FFT_ADJOINT, 0.0, 0.0, st);
   ring_adjoint_f32<<<dim3(gy, nrings), T * G, smem, st>>>(P.d_rings, d_list, P.R, map, phase, P.mmax, nf, P.npix,
-                                                           P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off, T, pack);
+                                                           P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off,
+                                                         P.d_rot_f, P.d_chirp_f, P.d_chirp_off, T, pack);
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}
+
+int launch_ring_roundtrip_f32(const Plan& P, const int* d_list, int nrings, int work_len, float2* phase,
+                              const double* weight, int nf, int pack, cudaStream_t st) {
+  if (nrings == 0) return PS_OK;
+  int T, G, gy;
+  fft_shape(work_len, nf, pack, T, G, gy);
+  if (nrings > 65535) return PS_ERR_INVALID;
+  const size_t smem = size_t(work_len) * G * sizeof(float2);
+  if (smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(ring_roundtrip_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return PS_ERR_CUDA;
+  }
+  int twlog = 0;
+  while ((1 << twlog) < P.max_fft) ++twlog;
+  // the pixel weights and the phases, read and written once
+  const double bytes = double(P.npix) * 8.0 * (pack ? 2.0 : 1.0) + 2.0 * 8.0 * P.R * (P.mmax + 1) * nf;
+  StatScope sc(PS_K_FFT_SYNTH, 0.0, bytes * double(nrings) / double(P.R), st);
+  ring_roundtrip_f32<<<dim3(gy, nrings), T * G, smem, st>>>(P.d_rings, d_list, P.R, phase, P.mmax, nf, weight,
+                                                             P.npix, P.d_twiddle_f, twlog, P.d_bs_spec_f, P.d_bs_off,
+                                                             P.d_rot_f, P.d_chirp_f, P.d_chirp_off, T, pack);
   PS_LAUNCH_CHECK();
   return PS_OK;
 }

@@ -36,13 +36,27 @@ int launch_legendre_adjoint_mx(const Plan& P, const float2* phase, float2* parti
 int mx_adjoint_tiles(const Plan& P);
 int launch_reduce_partials_f32(const float2* partial, double2* alm, int ntiles, int B, int ncomp, int64_t nalm,
                                double scale, int bofs, int sms, cudaStream_t st);
+size_t tab_bytes(int Rh, int lmax, int mmax, int spin);
+void tab_blockoff(int lmax, int mmax, std::vector<int64_t>& off);
+void tab_adj_work(int lmax, int mmax, std::vector<int2>& work);
+int launch_tab_gen(const Plan& P, int spin, const int64_t* d_blockoff, float* table, cudaStream_t st);
+int launch_tab_synth(const Plan& P, const float* table, const int64_t* d_blockoff, int Rh_table, int toff,
+                     const double2* almT, float2* phase, int B, int spin, int* err_flag, cudaStream_t st);
+int launch_tab_adj(const Plan& P, const float* table, const int64_t* d_blockoff, const int2* d_work, int nwork,
+                   int Rh_table, int toff, const float2* phase, double2* alm, int B, int spin, double scale,
+                   int64_t out_stride, const double* lscale, int* err_flag, cudaStream_t st);
 }  // namespace ps
 
 struct ps_plan {
   ps::Plan p;
   // a ring-band plan (ps_plan_band) shares its parent's tables and runs the
-  // Legendre stages only
+  // Legendre stages only; it reads the parent's Legendre tables (built before or
+  // after the band plan) through `parent`
   bool is_band = false;
+  const ps_plan* parent = nullptr;
+  // Legendre tables owned by this plan (ps_plan_build_table), per spin
+  void* tab_alloc[4] = {nullptr, nullptr, nullptr, nullptr};
+  void* tab_meta = nullptr;  // d_tab_off and d_tab_work in one allocation
   // FFT length classes: rings with the same work length share a launch
   std::vector<int> cls_len, cls_off, cls_cnt;
   std::vector<int> cls_off_n, cls_cnt_n;  // the north rings (and the equator ring) of each class
@@ -105,6 +119,26 @@ ps::Scaled ssqrt(ps::Scaled s) {
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// The Legendre table a mixed-precision plan's transforms of `spin` read, if any: the
+// plan's own, or for a band plan its parent's at the band's ring offset.
+struct TabRef {
+  const float* tab;
+  const int64_t* off;
+  const int2* work;
+  int nwork, Rh_table, toff;
+};
+bool table_for(const ps_plan* plan, int spin, TabRef& t) {
+  const ps_plan* owner = plan->is_band ? plan->parent : plan;
+  if (!owner || plan->p.prec != PS_PREC_MIXED || !owner->p.d_tab[spin]) return false;
+  t.tab = owner->p.d_tab[spin];
+  t.off = owner->p.d_tab_off;
+  t.work = owner->p.d_tab_work;
+  t.nwork = owner->p.tab_nwork;
+  t.Rh_table = owner->p.Rh;
+  t.toff = owner->p.Rh - plan->p.Rh;
+  return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -145,7 +179,10 @@ int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_pl
   P.R = 4 * nside - 1; P.Rh = 2 * nside;
   P.npix = 12 * int64_t(nside) * nside;
   P.nalm = int64_t(lmax + 1) * (lmax + 2) / 2;
-  for (int s = 0; s < 4; ++s) P.d_seed[s] = nullptr;
+  for (int s = 0; s < 4; ++s) { P.d_seed[s] = nullptr; P.d_tab[s] = nullptr; }
+  P.d_tab_off = nullptr;
+  P.d_tab_work = nullptr;
+  P.tab_nwork = 0;
   for (int d = 0; d < 2; ++d)
     for (int s = 0; s < 4; ++s) P.tile[d][s] = 0;
   if (ps_device_sm_count(&P.num_sms) != PS_OK) { delete pl; return PS_ERR_CUDA; }
@@ -299,6 +336,35 @@ int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_pl
     P.d_err = dev_upload(pl, zero, err);
   }
   P.d_bs_off = dev_upload(pl, bs_off, err);
+  P.d_rot_f = nullptr;
+  P.d_chirp_f = nullptr;
+  P.d_chirp_off = nullptr;
+  if (prec == PS_PREC_MIXED) {
+    // ring rotations and Bluestein chirps of the FP32 ring transforms, from exact integer
+    // argument reduction in FP64 (so the kernels evaluate no sincos)
+    std::vector<float2> rot(size_t(P.Rh) * (mmax + 1));
+    for (int rp = 0; rp < P.Rh; ++rp) {
+      const int64_t num = rings[rp].phi_num, den = rings[rp].phi_den;
+      for (int m = 0; m <= mmax; ++m) {
+        const int64_t q = (int64_t(m) * num) % (2 * den);
+        const double a = M_PI * double(q) / double(den);
+        rot[size_t(rp) * (mmax + 1) + m] = make_float2(float(std::cos(a)), float(std::sin(a)));
+      }
+    }
+    std::vector<float2> chirp;
+    std::vector<int64_t> chirp_off;
+    for (int N : bs_n) {
+      chirp_off.push_back((int64_t)chirp.size());
+      for (int j = 0; j < N; ++j) {
+        const int64_t q = (int64_t(j) * j) % (2 * int64_t(N));
+        const double a = -M_PI * double(q) / double(N);
+        chirp.push_back(make_float2(float(std::cos(a)), float(std::sin(a))));
+      }
+    }
+    P.d_rot_f = dev_upload(pl, rot, err);
+    P.d_chirp_f = dev_upload(pl, chirp, err);
+    P.d_chirp_off = dev_upload(pl, chirp_off, err);
+  }
   pl->d_ring_lists = dev_upload(pl, lists, err);
   if (err != PS_OK) { ps_plan_destroy(pl); return err; }
   *out = pl;
@@ -331,6 +397,7 @@ int ps_plan_band(const ps_plan* full, int nrings_north, ps_plan** out) {
   ps_plan* pl = new ps_plan();
   pl->p = F;
   pl->is_band = true;
+  pl->parent = full;
   for (int d = 0; d < 2; ++d)
     for (int s = 0; s < 4; ++s) pl->p.tile[d][s] = 0;  // the launchers' own choice on the band
   // north rings [Rh - k, Rh) (the last one is the equator ring) and their mirrors
@@ -341,18 +408,88 @@ int ps_plan_band(const ps_plan* full, int nrings_north, ps_plan** out) {
   return PS_OK;
 }
 
-static size_t leg_ws_bytes(const ps::Plan& P, int batch, int spin, int adjoint);
+static size_t leg_ws_bytes(const ps_plan* plan, int batch, int spin, int adjoint);
 
 int ps_legendre_workspace_bytes(const ps_plan* plan, int batch, int spin, int adjoint, size_t* bytes) {
   if (!plan || !bytes || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
-  *bytes = leg_ws_bytes(plan->p, batch, spin, adjoint);
+  *bytes = leg_ws_bytes(plan, batch, spin, adjoint);
   return PS_OK;
 }
 
 int ps_plan_destroy(ps_plan* plan) {
   if (!plan) return PS_ERR_INVALID;
-  for (void* d : plan->owned) cudaFree(d);
+  if (!plan->is_band) {
+    for (void* d : plan->owned) cudaFree(d);
+    for (void* d : plan->tab_alloc) if (d) cudaFree(d);
+    if (plan->tab_meta) cudaFree(plan->tab_meta);
+  }
   delete plan;
+  return PS_OK;
+}
+
+int ps_plan_table_bytes(const ps_plan* plan, int spin, size_t* bytes) {
+  if (!plan || !bytes || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  const ps::Plan& P = plan->p;
+  *bytes = ps::tab_bytes(P.Rh, P.lmax, P.mmax, spin);
+  return PS_OK;
+}
+
+int ps_plan_has_table(const ps_plan* plan, int spin, int* has) {
+  if (!plan || !has || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  const ps_plan* owner = plan->is_band ? plan->parent : plan;
+  *has = owner && owner->p.d_tab[spin] != nullptr;
+  return PS_OK;
+}
+
+int ps_plan_build_table(ps_plan* plan, int spin, cudaStream_t stream) {
+  if (!plan || spin < 0 || spin > 3) return PS_ERR_INVALID;
+  if (plan->is_band || plan->p.prec != PS_PREC_MIXED) return PS_ERR_UNSUPPORTED;
+  ps::Plan& P = plan->p;
+  if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
+  if (P.d_tab[spin]) return PS_OK;
+  if (!plan->tab_meta) {
+    std::vector<int64_t> off;
+    std::vector<int2> work;
+    ps::tab_blockoff(P.lmax, P.mmax, off);
+    ps::tab_adj_work(P.lmax, P.mmax, work);
+    const size_t off_bytes = align256(off.size() * sizeof(int64_t));
+    void* d = nullptr;
+    if (cudaMalloc(&d, off_bytes + work.size() * sizeof(int2)) != cudaSuccess) {
+      cudaGetLastError();
+      return PS_ERR_NOMEM;
+    }
+    if (cudaMemcpy(d, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(static_cast<char*>(d) + off_bytes, work.data(), work.size() * sizeof(int2),
+                   cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaFree(d);
+      return PS_ERR_CUDA;
+    }
+    plan->tab_meta = d;
+    P.d_tab_off = static_cast<int64_t*>(d);
+    P.d_tab_work = reinterpret_cast<int2*>(static_cast<char*>(d) + off_bytes);
+    P.tab_nwork = int(work.size());
+  }
+  void* t = nullptr;
+  if (cudaMalloc(&t, ps::tab_bytes(P.Rh, P.lmax, P.mmax, spin)) != cudaSuccess) {
+    cudaGetLastError();
+    return PS_ERR_NOMEM;
+  }
+  const int rc = ps::launch_tab_gen(P, spin, P.d_tab_off, static_cast<float*>(t), stream);
+  if (rc != PS_OK) { cudaFree(t); return rc; }
+  plan->tab_alloc[spin] = t;
+  P.d_tab[spin] = static_cast<float*>(t);
+  return PS_OK;
+}
+
+int ps_plan_drop_tables(ps_plan* plan) {
+  if (!plan) return PS_ERR_INVALID;
+  if (plan->is_band) return PS_ERR_UNSUPPORTED;
+  if (cudaDeviceSynchronize() != cudaSuccess) return PS_ERR_CUDA;
+  for (int s = 0; s < 4; ++s) {
+    if (plan->tab_alloc[s]) cudaFree(plan->tab_alloc[s]);
+    plan->tab_alloc[s] = nullptr;
+    plan->p.d_tab[s] = nullptr;
+  }
   return PS_OK;
 }
 
@@ -385,11 +522,14 @@ static int adjoint_chunk(const ps::Plan& P, int batch, int spin) {
   return batch < c ? batch : c;
 }
 
-static size_t sht_ws_bytes(const ps::Plan& P, int batch, int spin, int adjoint) {
+static size_t sht_ws_bytes(const ps_plan* plan, int batch, int spin, int adjoint) {
+  const ps::Plan& P = plan->p;
   const size_t ncomp = spin == 0 ? 1 : 2;
   const size_t nf = size_t(batch) * ncomp;
   const size_t phase = align256(size_t(P.R) * (P.mmax + 1) * nf * sizeof(double2));
   if (!adjoint) return align256(size_t(P.nalm) * nf * sizeof(double2)) + phase;
+  TabRef tr;
+  if (table_for(plan, spin, tr)) return phase;  // the table adjoint writes alm directly
   const size_t nfc = size_t(adjoint_chunk(P, batch, spin)) * ncomp;
   return phase + align256(size_t(ps::adjoint_tiles(P)) * P.nalm * nfc * sizeof(double2));
 }
@@ -421,12 +561,15 @@ int convert_grid(int64_t n, int sms) {
 }
 }  // namespace
 
-static size_t leg_ws_bytes(const ps::Plan& P, int batch, int spin, int adjoint) {
+static size_t leg_ws_bytes(const ps_plan* plan, int batch, int spin, int adjoint) {
+  const ps::Plan& P = plan->p;
   const size_t ncomp = spin == 0 ? 1 : 2;
   const size_t nf = size_t(batch) * ncomp;
   const bool mixed = P.prec == PS_PREC_MIXED;
   const size_t phase32 = mixed ? align256(size_t(P.R) * (P.mmax + 1) * nf * sizeof(float2)) : 0;
   if (!adjoint) return align256(size_t(P.nalm) * nf * sizeof(double2)) + phase32;
+  TabRef tr;
+  if (table_for(plan, spin, tr)) return phase32;
   if (mixed) {
     const size_t nfc = size_t(adjoint_chunk(P, batch, spin)) * ncomp;
     return phase32 + align256(size_t(ps::mx_adjoint_tiles(P)) * P.nalm * nfc * sizeof(float2));
@@ -442,7 +585,7 @@ int ps_legendre_synthesis(const ps_plan* plan, const double* alm, double* phase,
   if (!alm || !phase || !workspace) return PS_ERR_INVALID;
   const ps::Plan& P = plan->p;
   if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
-  if (workspace_bytes < leg_ws_bytes(P, batch, spin, 0)) return PS_ERR_WORKSPACE;
+  if (workspace_bytes < leg_ws_bytes(plan, batch, spin, 0)) return PS_ERR_WORKSPACE;
   const int ncomp = spin == 0 ? 1 : 2;
   double2* almT = static_cast<double2*>(workspace);
   int rc = ps::launch_alm_to_T(reinterpret_cast<const double2*>(alm), almT, batch, ncomp, P.nalm, P.num_sms, stream);
@@ -450,7 +593,11 @@ int ps_legendre_synthesis(const ps_plan* plan, const double* alm, double* phase,
   if (P.prec == PS_PREC_MIXED) {
     float2* ph32 = reinterpret_cast<float2*>(static_cast<char*>(workspace) +
                                              align256(size_t(P.nalm) * batch * ncomp * sizeof(double2)));
-    rc = ps::launch_legendre_synth_tc(P, almT, ph32, batch, spin, P.d_err, stream);
+    TabRef tr;
+    if (table_for(plan, spin, tr))
+      rc = ps::launch_tab_synth(P, tr.tab, tr.off, tr.Rh_table, tr.toff, almT, ph32, batch, spin, P.d_err, stream);
+    else
+      rc = ps::launch_legendre_synth_tc(P, almT, ph32, batch, spin, P.d_err, stream);
     if (rc) return rc;
     const int64_t n = int64_t(P.R) * (P.mmax + 1) * batch * ncomp;
     phase_f32_to_f64<<<convert_grid(n, P.num_sms), 256, 0, stream>>>(ph32, reinterpret_cast<double2*>(phase), n);
@@ -467,7 +614,7 @@ int ps_legendre_adjoint(const ps_plan* plan, const double* phase, double* alm, i
   if (!alm || !phase || !workspace) return PS_ERR_INVALID;
   const ps::Plan& P = plan->p;
   if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
-  if (workspace_bytes < leg_ws_bytes(P, batch, spin, 1)) return PS_ERR_WORKSPACE;
+  if (workspace_bytes < leg_ws_bytes(plan, batch, spin, 1)) return PS_ERR_WORKSPACE;
   const int ncomp = spin == 0 ? 1 : 2;
   if (P.prec == PS_PREC_MIXED) {
     const int64_t n = int64_t(P.R) * (P.mmax + 1) * batch * ncomp;
@@ -475,6 +622,11 @@ int ps_legendre_adjoint(const ps_plan* plan, const double* phase, double* alm, i
     float2* partial = reinterpret_cast<float2*>(static_cast<char*>(workspace) + align256(size_t(n) * sizeof(float2)));
     phase_f64_to_f32<<<convert_grid(n, P.num_sms), 256, 0, stream>>>(reinterpret_cast<const double2*>(phase), ph32, n);
     PS_LAUNCH_CHECK();
+    TabRef tr;
+    if (table_for(plan, spin, tr))
+      return ps::launch_tab_adj(P, tr.tab, tr.off, tr.work, tr.nwork, tr.Rh_table, tr.toff, ph32,
+                                reinterpret_cast<double2*>(alm), batch, spin, scale, int64_t(ncomp) * P.nalm, nullptr,
+                                P.d_err, stream);
     const int ch = adjoint_chunk(P, batch, spin);
     for (int b0 = 0; b0 < batch; b0 += ch) {
       const int bc = std::min(ch, batch - b0);
@@ -502,7 +654,7 @@ int ps_legendre_adjoint(const ps_plan* plan, const double* phase, double* alm, i
 
 int ps_sht_workspace_bytes(const ps_plan* plan, int batch, int spin, int adjoint, size_t* bytes) {
   if (!plan || !bytes || batch < 0 || spin < 0 || spin > 3) return PS_ERR_INVALID;
-  *bytes = sht_ws_bytes(plan->p, batch, spin, adjoint);
+  *bytes = sht_ws_bytes(plan, batch, spin, adjoint);
   return PS_OK;
 }
 
@@ -514,7 +666,7 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
   if (!alm || !map || !workspace) return PS_ERR_INVALID;
   const ps::Plan& P = plan->p;
   if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
-  if (workspace_bytes < sht_ws_bytes(P, batch, spin, 0)) return PS_ERR_WORKSPACE;
+  if (workspace_bytes < sht_ws_bytes(plan, batch, spin, 0)) return PS_ERR_WORKSPACE;
   const int ncomp = spin == 0 ? 1 : 2;
   const int nf = batch * ncomp;
   char* ws = static_cast<char*>(workspace);
@@ -530,7 +682,11 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
   if (P.prec == PS_PREC_MIXED) {
     // tensor-core Legendre stage (TF32 x3, FP32 accumulation) and FP32 ring transforms
     float2* phase = reinterpret_cast<float2*>(phase_ptr);
-    rc = ps::launch_legendre_synth_tc(P, almT, phase, batch, spin, P.d_err, stream);
+    TabRef tr;
+    if (table_for(plan, spin, tr))
+      rc = ps::launch_tab_synth(P, tr.tab, tr.off, tr.Rh_table, tr.toff, almT, phase, batch, spin, P.d_err, stream);
+    else
+      rc = ps::launch_legendre_synth_tc(P, almT, phase, batch, spin, P.d_err, stream);
     if (rc) return rc;
     for (size_t c = 0; c < plan->cls_len.size(); ++c) {
       rc = ps::launch_ring_synth_f32(P, plan->d_ring_lists + (spin ? plan->cls_off[c] : plan->cls_off_n[c]),
@@ -560,7 +716,7 @@ int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, i
   if (!alm || !map || !workspace) return PS_ERR_INVALID;
   const ps::Plan& P = plan->p;
   if (spin > 0 && !P.d_seed[spin]) return PS_ERR_INVALID;
-  if (workspace_bytes < sht_ws_bytes(P, batch, spin, 1)) return PS_ERR_WORKSPACE;
+  if (workspace_bytes < sht_ws_bytes(plan, batch, spin, 1)) return PS_ERR_WORKSPACE;
   const int ncomp = spin == 0 ? 1 : 2;
   const int nf = batch * ncomp;
   char* ws = static_cast<char*>(workspace);
@@ -576,6 +732,11 @@ int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, i
                                        nf, spin > 0, stream);
       if (rc) return rc;
     }
+    TabRef tr;
+    if (table_for(plan, spin, tr))
+      return ps::launch_tab_adj(P, tr.tab, tr.off, tr.work, tr.nwork, tr.Rh_table, tr.toff, phase,
+                                reinterpret_cast<double2*>(alm), batch, spin, scale, int64_t(ncomp) * P.nalm, nullptr,
+                                P.d_err, stream);
     const int ch = adjoint_chunk(P, batch, spin);
     for (int b0 = 0; b0 < batch; b0 += ch) {
       const int bc = std::min(ch, batch - b0);
@@ -608,3 +769,42 @@ int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, i
 }
 
 }  // extern "C"
+
+namespace ps {
+// The pieces of a full mixed-precision plan with the Legendre table of `spin` that the fused
+// round trip (ps_roundtrip.cu) needs; PS_ERR_UNSUPPORTED for FP64 or band plans and for spins
+// without a table.
+struct RoundtripView {
+  const Plan* P;
+  const float* tab;
+  const int64_t* off;
+  const int2* work;
+  int nwork;
+  const int* ring_lists;
+  const int* cls_len;
+  const int* cls_off;
+  const int* cls_cnt;
+  const int* cls_off_n;
+  const int* cls_cnt_n;
+  int ncls;
+};
+int roundtrip_view(const ps_plan* plan, int spin, RoundtripView& v) {
+  if (plan->is_band || plan->p.prec != PS_PREC_MIXED) return PS_ERR_UNSUPPORTED;
+  if (spin > 0 && !plan->p.d_seed[spin]) return PS_ERR_INVALID;
+  TabRef tr;
+  if (!table_for(plan, spin, tr)) return PS_ERR_UNSUPPORTED;
+  v.P = &plan->p;
+  v.tab = tr.tab;
+  v.off = tr.off;
+  v.work = tr.work;
+  v.nwork = tr.nwork;
+  v.ring_lists = plan->d_ring_lists;
+  v.cls_len = plan->cls_len.data();
+  v.cls_off = plan->cls_off.data();
+  v.cls_cnt = plan->cls_cnt.data();
+  v.cls_off_n = plan->cls_off_n.data();
+  v.cls_cnt_n = plan->cls_cnt_n.data();
+  v.ncls = int(plan->cls_len.size());
+  return PS_OK;
+}
+}  // namespace ps
