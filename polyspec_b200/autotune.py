@@ -78,16 +78,20 @@ class Tuner:
     def _set(self, pipeline, direction, spin, tile):
         _lib.call("ps_plan_set_tile", self.handles[pipeline], direction, spin, tile)
 
-    def select(self, direction, spin, B, run):
-        """Handle to run the transform with (its tile already set); `run(handle)` issues it."""
-        key = "%s|%s|spin%d|b%d" % (self.prefix, ("synthesis", "adjoint")[direction], spin, self.bucket(B))
+    def select(self, direction, spin, B, run, table=False):
+        """Handle to run the transform with (its tile already set); `run(handle)` issues it.
+        With `table` the mixed plan streams its Legendre table (ps_plan_build_table): its
+        on-the-fly tile shapes do not apply, and the choice is cached under its own key."""
+        key = "%s|%s|spin%d|b%d%s" % (self.prefix, ("synthesis", "adjoint")[direction], spin, self.bucket(B),
+                                      "|tab" if table else "")
         choice = self.choices.get(key) or self.disk.get(key)
         if choice is None or choice.get("pipeline") not in self.handles:
             times = {}
             # the FP64 pipeline only competes for small batches (its workspace is twice the mixed one's)
             cands = [pl for pl in self.handles if not (pl == "fp64" and len(self.handles) > 1 and B > 8)]
             for pipeline in cands:
-                for tile in TILES[(pipeline, direction, spin > 0)]:
+                tiles = (0,) if (table and pipeline == "mixed") else TILES[(pipeline, direction, spin > 0)]
+                for tile in tiles:
                     self._set(pipeline, direction, spin, tile)
                     h = self.handles[pipeline]
                     run(h)

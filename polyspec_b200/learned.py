@@ -138,9 +138,19 @@ class MLP:
 
 
 class LearnedBandPreconditioner:
-    def __init__(self, weightings, seed=0):
+    """``base='harmonic'``: M = Sigma + S^1/2 (L L^T + d I) S^1/2 on band blocks, trained on the
+    plain CG's (r, e) pairs.  ``base='cut'``: the same correction on top of the masked-band
+    preconditioner, M = M_cut + S^1/2 (L L^T + d I) S^1/2 (M_cut >= Sigma, so M stays SPD),
+    trained on the pairs of the cut-preconditioned CG with targets e - M_cut r: the network
+    only has to learn what M_cut leaves."""
+
+    def __init__(self, weightings, seed=0, base='harmonic'):
         self.W = weightings
         self.base = weightings.base
+        if base not in ('harmonic', 'cut'):
+            raise ValueError("base must be 'harmonic' or 'cut'")
+        self.base_prec = base
+        self.cut = weightings.cut_preconditioner() if base == 'cut' else None
         if not self.base.pol:
             raise ValueError("the learned band preconditioner works on T, E, B (pol=True)")
         dev = self.base.device
@@ -192,11 +202,14 @@ class LearnedBandPreconditioner:
         from .weighting import BatchedCGD
         W = self.W
         x0 = torch.einsum('abi,nbi->nai', W.d_x0op, self.base.to_lm_batch(maps))
-        cg = BatchedCGD(W, maps, x0, preconditioner='harmonic')
+        cg = BatchedCGD(W, maps, x0, preconditioner=self.base_prec)
         cg.run(nstep=nstep, thresh=thresh_solve)
         xstar = cg.x.clone()
-        cg = BatchedCGD(W, maps, x0, preconditioner='harmonic')
-        self.add_pairs(cg.r, xstar - cg.x)
+        cg = BatchedCGD(W, maps, x0, preconditioner=self.base_prec)
+
+        def target(r, e):  # what the learned correction has to supply on top of the base operator
+            return e if self.cut is None else e - self.cut.apply(r)
+        self.add_pairs(cg.r, target(cg.r, xstar - cg.x))
         for _ in range(nstep):
             if not bool(cg.active.any()):
                 break
@@ -204,7 +217,8 @@ class LearnedBandPreconditioner:
             cg.step()
             cg.active &= ~(cg.err < thresh_collect)
             idx = torch.nonzero(act).flatten()
-            self.add_pairs(cg.r[idx], xstar[idx] - cg.x[idx])
+            if idx.numel():
+                self.add_pairs(cg.r[idx], target(cg.r[idx], xstar[idx] - cg.x[idx]))
         return cg
 
     # ---------------------------------------------------------------- training
@@ -238,7 +252,10 @@ class LearnedBandPreconditioner:
     # ---------------------------------------------------------------- application
     def apply(self, r):
         """M r for r complex128 [B, 3, nlm]."""
-        z = torch.einsum('abi,nbi->nai', self.sigma_c, r).contiguous()
+        if self.cut is not None:
+            z = self.cut.apply(r).contiguous()
+        else:
+            z = torch.einsum('abi,nbi->nai', self.sigma_c, r).contiguous()
         if self.L is None:
             return z
         r = r.contiguous()

@@ -1,10 +1,11 @@
 """Small fixed workloads for profiling the kernels under ncu.
 
-    python -m polyspec_b200.profile_cli sht --nside 1024 --lmax 2048 --ops s0,a0,s2,a2 [--batch 1]
+    python -m polyspec_b200.profile_cli sht --nside 1024 --lmax 2048 --ops s0,a0,s2,a2 [--batch 1] [--tables on]
 
 Each op runs once (no warm-up) so that a launch list or an ncu capture of
 ``-k <kernel> -c 1`` sees exactly one launch per transform stage.
-ops: s0/a0 = spin-0 synthesis/adjoint, s2/a2 = spin-2 synthesis/adjoint.
+ops: s0/a0 = spin-0 synthesis/adjoint, s2/a2 = spin-2 synthesis/adjoint; only the
+spins of the ops are planned (and, for a mixed plan, tabulated).
 
     python -m polyspec_b200.profile_cli pix --nside 512 --nr 24 [--reps 3]
 
@@ -92,13 +93,18 @@ def inpaint(a):
 
 def sht(a):
     from polyspec_b200.sht import SHTPlan
-    P = SHTPlan(a.nside, a.lmax, prec=a.prec, autotune=False)
+    ops = a.ops.split(",")
+    spins = sorted({0} | {int(op[1]) for op in ops if op[1:].isdigit()})
+    P = SHTPlan(a.nside, a.lmax, spins=spins, prec=a.prec, autotune=False,
+                tables={"auto": "auto", "on": True, "off": False}[a.tables])
     B = a.batch
-    alm0 = torch.randn(B, P.nalm, dtype=torch.complex128, device="cuda")
-    map0 = torch.randn(B, P.npix, dtype=torch.float64, device="cuda")
-    alm2 = torch.randn(B, 2, P.nalm, dtype=torch.complex128, device="cuda")
-    map2 = torch.randn(B, 2, P.npix, dtype=torch.float64, device="cuda")
-    for op in a.ops.split(","):
+    need0 = any(op in ("s0", "a0") for op in ops)
+    need2 = any(op in ("s2", "a2") for op in ops)
+    alm0 = torch.randn(B, P.nalm, dtype=torch.complex128, device="cuda") if need0 else None
+    map0 = torch.randn(B, P.npix, dtype=torch.float64, device="cuda") if need0 else None
+    alm2 = torch.randn(B, 2, P.nalm, dtype=torch.complex128, device="cuda") if need2 else None
+    map2 = torch.randn(B, 2, P.npix, dtype=torch.float64, device="cuda") if need2 else None
+    for op in ops:
         if op == "s0":
             P.synthesis(alm0, 0)
         elif op == "a0":
@@ -110,7 +116,7 @@ def sht(a):
         else:
             raise SystemExit("unknown op " + op)
     torch.cuda.synchronize()
-    print("done", a.ops)
+    print("done", a.ops, "tables", {s: P.has_table(s) for s in spins} if a.prec != "fp64" else None)
 
 
 def pix(a):
@@ -386,6 +392,8 @@ def main(argv=None):
     s.add_argument("--batch", type=int, default=1)
     s.add_argument("--prec", default="fp64")
     s.add_argument("--ops", default="s0,a0,s2,a2")
+    s.add_argument("--tables", default="auto", choices=["auto", "on", "off"],
+                   help="Legendre tables of a mixed plan (built before the first transform of each spin)")
     ip = sub.add_parser("inpaint")
     ip.add_argument("--nside", type=int, default=1024)
     ip.add_argument("--holes", type=int, default=2000)

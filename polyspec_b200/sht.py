@@ -16,8 +16,18 @@ batch bucket) times the candidate tile shapes of the Legendre kernels and, for
 one) and keeps the fastest (polyspec_b200.autotune; choices cached in JSON).
 The tensor-core pipeline wins at large batches; for one or a few maps the FP64
 CUDA-core kernels are faster (and exact to FP64).
+
+Legendre tables (``tables='auto'``, mixed precision only): the first transform
+of a spin builds the plan's FP32 Legendre table of that spin
+(``ps_plan_build_table``) when it fits in ``table_fraction`` of the free device
+memory (default 0.45, or the environment variable PS_TABLE_MEM_FRACTION); the
+Legendre stages of that spin then stream the table through tensor-core GEMMs.
+Where it does not fit (Nside 2048 at lmax 4096 needs 137 GB for spin 0) the
+on-the-fly kernels run.  ``tables=True`` builds regardless of the budget (and
+raises if the allocation fails), ``tables=False`` never builds.
 """
 import ctypes
+import os
 
 import torch
 
@@ -29,7 +39,8 @@ def nalm(lmax):
 
 
 class SHTPlan:
-    def __init__(self, nside, lmax=None, spins=(0, 1, 2, 3), prec="fp64", device=None, autotune=True):
+    def __init__(self, nside, lmax=None, spins=(0, 1, 2, 3), prec="fp64", device=None, autotune=True,
+                 tables="auto", table_fraction=None):
         if not torch.cuda.is_available():
             raise RuntimeError("the CUDA backend needs a GPU (no CPU fallback)")
         self.nside = int(nside)
@@ -71,6 +82,57 @@ class SHTPlan:
         # counters of transforms issued through this plan
         self.n_synthesis = 0
         self.n_adjoint = 0
+        # Legendre tables: spins already tried (built or refused)
+        self.tables = tables if prec != "fp64" else False
+        self.table_fraction = float(table_fraction if table_fraction is not None
+                                    else os.environ.get("PS_TABLE_MEM_FRACTION", 0.45))
+        self._tab_tried = set()
+
+    # ------------------------------------------------------------ Legendre tables
+    def table_bytes(self, spin):
+        n = ctypes.c_size_t()
+        _lib.call("ps_plan_table_bytes", self._h, int(spin), ctypes.byref(n))
+        return int(n.value)
+
+    def has_table(self, spin):
+        v = ctypes.c_int()
+        _lib.call("ps_plan_has_table", self._h, int(spin), ctypes.byref(v))
+        return bool(v.value)
+
+    def build_table(self, spin, force=False):
+        """Build the FP32 Legendre table of `spin` (mixed plans).  Without `force`, only when
+        it fits in table_fraction of the free device memory; returns whether the plan has it."""
+        spin = int(spin)
+        if self.prec == "fp64":
+            return False
+        if self.has_table(spin):
+            return True
+        need = self.table_bytes(spin)
+        with torch.cuda.device(self.device):
+            free, _ = torch.cuda.mem_get_info()
+            if not force and need > self.table_fraction * free:
+                torch.cuda.empty_cache()
+                free, _ = torch.cuda.mem_get_info()
+                if need > self.table_fraction * free:
+                    return False
+            rc = _lib.lib().ps_plan_build_table(self._h, spin, self._stream())
+            if rc == _lib.PS_ERR_NOMEM:
+                torch.cuda.empty_cache()
+                rc = _lib.lib().ps_plan_build_table(self._h, spin, self._stream())
+            if rc == _lib.PS_ERR_NOMEM and not force:
+                return False
+            _lib.check("ps_plan_build_table", rc)
+        return True
+
+    def drop_tables(self):
+        _lib.call("ps_plan_drop_tables", self._h)
+        self._tab_tried.clear()
+
+    def _maybe_table(self, spin):
+        if self.tables is False or spin in self._tab_tried:
+            return
+        self._tab_tried.add(spin)
+        self.build_table(spin, force=self.tables is True)
 
     def __del__(self):
         for name in ("_h", "_h64"):
@@ -87,7 +149,8 @@ class SHTPlan:
         if self._tuner is None:
             return self._h
         direction, spin, B = key
-        return self._tuner.select(0 if direction == "synthesis" else 1, spin, B, run)
+        table = self.prec != "fp64" and self.has_table(spin)
+        return self._tuner.select(0 if direction == "synthesis" else 1, spin, B, run, table=table)
 
     def error_flag(self, reset=True):
         """Device error flag of the plan (set by a kernel whose bounded wait expired)."""
@@ -134,6 +197,7 @@ class SHTPlan:
         out = torch.empty(shape, dtype=torch.float64, device=alm.device)
         if B == 0:
             return out
+        self._maybe_table(spin)
         ws, nbytes = self.workspace(B, spin, 0)
 
         def run(h):
@@ -141,6 +205,40 @@ class SHTPlan:
                       B, spin, ctypes.c_void_p(ws.data_ptr()), nbytes, self._stream())
         run(self._pick(("synthesis", spin, B), run))
         self.n_synthesis += B
+        return out
+
+    def weighted_roundtrip(self, alm, weight, lscale=None, scale=1.0, out=None):
+        """Fused  out = scale * lscale * Y^H W Y (lscale * alm)  for every field of alm [B, nf, nalm]
+        (nf = 1: T, spin 0; nf = 3: T spin 0 and (E, B) spin 2), weight [nf, npix] float64,
+        lscale [nf, nalm] float64 or None (ps_sht_weighted_roundtrip: the maps stay in shared
+        memory).  Returns None when a spin lacks its Legendre table (the caller composes
+        synthesis, weight and adjoint instead)."""
+        if self.prec == "fp64" or alm.dim() != 3 or alm.shape[1] not in (1, 3):
+            return None
+        B, nf = alm.shape[0], alm.shape[1]
+        spins = [(0, 0)] if nf == 1 else [(0, 0), (2, 1)]
+        for spin, _ in spins:
+            self._maybe_table(spin)
+            if not self.has_table(spin):
+                return None
+        alm = alm.contiguous()
+        if out is None:
+            out = torch.empty_like(alm)
+        w = weight.contiguous()
+        ls = lscale.contiguous() if lscale is not None else None
+        for spin, c0 in spins:
+            n = ctypes.c_size_t()
+            _lib.call("ps_roundtrip_workspace_bytes", self._h, B, spin, ctypes.byref(n))
+            if self._ws is None or self._ws.numel() < n.value:
+                self._ws = torch.empty(max(n.value, 256), dtype=torch.uint8, device=self.device)
+            off = c0 * self.nalm * 16
+            _lib.call("ps_sht_weighted_roundtrip", self._h, ctypes.c_void_p(alm.data_ptr() + off),
+                      ctypes.c_void_p(out.data_ptr() + off), nf * self.nalm, B, spin,
+                      ctypes.c_void_p(w.data_ptr() + c0 * self.npix * 8),
+                      ctypes.c_void_p(ls.data_ptr() + c0 * self.nalm * 8) if ls is not None else ctypes.c_void_p(0),
+                      float(scale), ctypes.c_void_p(self._ws.data_ptr()), self._ws.numel(), self._stream())
+        self.n_synthesis += B * len(spins)
+        self.n_adjoint += B * len(spins)
         return out
 
     def adjoint(self, map, spin=0, scale=1.0):
@@ -160,6 +258,7 @@ class SHTPlan:
         out = torch.empty(shape, dtype=torch.complex128, device=map.device)
         if B == 0:
             return out
+        self._maybe_table(spin)
         ws, nbytes = self.workspace(B, spin, 1)
 
         def run(h):

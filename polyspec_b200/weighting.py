@@ -14,6 +14,7 @@ give numpy outputs; CUDA-tensor inputs give CUDA-tensor outputs.
 operators evaluated on the device.
 """
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -209,6 +210,17 @@ class Weightings:
             cache[name] = lmops.real3({'Sigma': self.d_Sigma, 'inv_Cl': self.d_inv_Cl, 'x0op': self.d_x0op}[name])
         return cache[name]
 
+    def roundtrip_operands(self):
+        """(pixel weight W N^-1 W / A_pix [nf, npix], beam [nf, nlm]) as float64 device arrays for the
+        fused CG operator, or None (FP64 plans, no noise covariance, or PS_FUSED_A=0)."""
+        if self.base.prec == 'fp64' or not hasattr(self, 'd_WNW') or os.environ.get("PS_FUSED_A", "1") == "0":
+            return None
+        if getattr(self, '_rt_ops', None) is None:
+            w = (self.d_WNW / self.pixel_area).expand(1 + 2 * self.pol, -1).contiguous()
+            beam = self.base.dev('beam_lm').real.to(torch.float64).contiguous()
+            self._rt_ops = (w, beam)
+        return self._rt_ops
+
     def cut_preconditioner(self):
         """The masked-band preconditioner of this Weightings (built on first use)."""
         if getattr(self, '_cut', None) is None:
@@ -341,10 +353,26 @@ class BatchedCGD:
         return torch.einsum('abi,nbi->nai', self.W.d_inv_Cl, ilm)
 
     def _apply_A(self, ilm):
+        # mixed plans with Legendre tables: B Y^H (W N^-1 W / A_pix) Y B in one fused call per spin
+        # (ps_sht_weighted_roundtrip; the maps stay in shared memory)
+        rt = self.W.roundtrip_operands()
+        if rt is not None:
+            out = self.base.plan().weighted_roundtrip(ilm, rt[0], rt[1], np.pi / (3. * self.base.Nside ** 2))
+            if out is not None:
+                B, nf = ilm.shape[0], ilm.shape[1]
+                self.base.n_SHTs_reverse += B * (1 + (nf == 3))
+                self.base.n_SHTs_forward += B * (1 + (nf == 3))
+                return self._apply_Cinv(ilm) + out
         beam = self.base.dev('beam_lm')
         m = self.base.to_map_batch(ilm * beam)
         m = m * (self.W.d_WNW / self.W.pixel_area)
         return self._apply_Cinv(ilm) + self.base.to_lm_batch(m) * beam
+
+    def _fallback_M(self, r):
+        """Preconditioner of a system the learned CG hands back: the learned operator's own base
+        (the masked-band preconditioner when it sits on that one, else the harmonic Sigma)."""
+        cut = getattr(self.learned, 'cut', None) if hasattr(self, 'learned') else None
+        return cut.apply(r) if cut is not None else self._sigma(r)
 
     def _apply_M(self, ilm, learned_mask=None):
         Sig = self.W.d_Sigma
@@ -354,7 +382,7 @@ class BatchedCGD:
             z = self.learned.apply(ilm)
             if learned_mask is not None and not bool(learned_mask.all()):
                 plain = ~learned_mask
-                z[plain] = torch.einsum('abi,nbi->nai', Sig, ilm[plain])
+                z[plain] = self._fallback_M(ilm[plain])
             return z
         if self.preconditioner == 'harmonic':
             return self._sigma(ilm)
@@ -393,7 +421,7 @@ class BatchedCGD:
             if self.learned_max_steps is not None:
                 bad |= lm & (self.iters[idx] + 1 >= self.learned_max_steps)
             if bool(bad.any()):
-                zs = self._sigma(r[bad])
+                zs = self._fallback_M(r[bad])
                 p[bad] = zs
                 next_rz[bad] = self.dot(r[bad], zs)
                 lm = lm & ~bad
