@@ -74,6 +74,9 @@ def parse():
     p.add_argument("--nside", type=int, default=1024)
     p.add_argument("--lmax", type=int, default=2048)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="fisher-teb", choices=["fisher-teb", "pspec-t64"],
+                   help="fisher-teb: the headline (default); pspec-t64: PSpecBin T at Nside 64, lmax 128, ideal "
+                        "S^-1 of the latitude-masked map, Fisher from seeds 1-10, beside the CPU oracle port")
     return p.parse_args()
 
 
@@ -516,8 +519,66 @@ def run_cuda(a):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------- PSpecBin T at Nside 64
+def pspec_t64(a):
+    """PSpecBin plain, T only: Nside 64, lmax 128, 8 bins of 16 from l = 2, C_l = 1000/(l+10)^2,
+    30' beam, |lat| < 15 deg cut with a 5 deg cosine taper, applySinv = ideal S^-1 of the masked
+    map; one step = the Fisher contributions of seeds 1-10 (polyspec/pspec_bin.py:94-164) and the
+    numerator of the seed-0 GRF.  FP64 on the GPU and, on the host, the oracle restatement."""
+    import torch
+    from polyspec_b200 import PolySpec, Weightings, PSpecBin
+    from polyspec_b200 import workloads as Wl
+    nside, lmax = 64, 128
+    cl = Wl.fiducial_cl(lmax, False)
+    b = Wl.gaussian_beam(lmax, 30.0)
+    cltot = {'TT': cl['TT'] * b ** 2}
+    mask = Wl.latitude_mask(nside, 15.0, 5.0)
+    l_bins = 2 + 16 * np.arange(9)
+    seeds = list(range(1, 11))
+    line = {"metric": "PSpecBin Fisher sims/s (T, Nside 64)", "unit": "sims/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "PSpecBin T, Nside 64, lmax 128, 8 bins of 16 from l=2, 30' beam, |lat|<15 deg "
+                                   "cut + 5 deg taper, ideal S^-1, Fisher seeds 1-10 per step"}}
+    base = PolySpec(nside, dict(cltot), beam=[b], pol=False, lmax=lmax, prec="fp64")
+    wts = Weightings(base, mask[None], {'TT': cl['TT']})
+    psb = PSpecBin(base, mask, wts.make_applySinv('ideal'), l_bins, fields=["TT"])
+    data = base.generate_data(seed=0, output_type='map')
+    for _ in range(a.warmup):
+        for s in seeds:
+            psb.compute_fisher_contribution(s)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    for _ in range(a.steps):
+        fish = np.mean([psb.compute_fisher_contribution(s) for s in seeds], axis=0)
+        num = psb.Cl_numerator(data)
+    torch.cuda.synchronize()
+    t_gpu = (time.time() - t0) / a.steps
+    line["value"] = len(seeds) / t_gpu
+    line["ms_per_step"] = 1e3 * t_gpu
+    line["e2e"] = {"value": line["value"], "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                   "note": "numpy in, numpy out through the reference API (GRF drawn by numpy on the host)"}
+    if not a.no_cpu_baseline:
+        from oracle import polyspec_port as P
+        from oracle import sht as osht
+        pb = P.PortBase(nside, cltot, np.asarray([b]), pol=False, lmax=lmax)
+        pw = P.PortWeightings(pb, mask[None], {'TT': cl['TT']}, np.ones((1, 12 * nside ** 2)))
+        pp = P.PortPSpecBin(pb, mask, pw.applySinv_ideal, l_bins, ["TT"])
+        t0 = time.time()
+        fcpu = np.mean([pp.compute_fisher_contribution(a_lm=np.asarray(base.generate_data(
+            seed=s + int(1e7), output_type='harmonic', deconvolve_beam=True))) for s in seeds], axis=0)
+        t_cpu = time.time() - t0
+        line["cpu_baseline"] = {"value": len(seeds) / t_cpu, "unit": "sims/s", "cores": osht.default_threads(),
+                                "kind": "port", "sample": "the same 10 Fisher contributions on the oracle "
+                                                          "restatement (FP64, all host threads)"}
+        line["fisher_gpu_vs_cpu_max_rel"] = float(np.abs(fish - fcpu).max() / np.abs(fcpu).max())
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
+    if a.workload == "pspec-t64":
+        pspec_t64(a)
+        return
     if a.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return
