@@ -260,24 +260,27 @@ __device__ __forceinline__ void tab_issue(uint32_t sbase, uint32_t tmem, uint32_
   }
 }
 
-// S += D for this thread's TMEM lane (first stage: S = D), columns [0, n) of both accumulators
+// S += D for this thread's TMEM lane (first stage: S = D), columns [0, n) of both accumulators;
+// the four loads of a column chunk (D and S of both accumulators) share one wait
 __device__ __forceinline__ void tab_drain(uint32_t lane_addr, int n, bool first) {
 #pragma unroll 1
-  for (int acc = 0; acc < 2; ++acc) {
-#pragma unroll 1
-    for (int cb = 0; cb < n; cb += 16) {
-      float v[16], s[16];
-      const uint32_t dcol = lane_addr + uint32_t(acc * TB_NMAX + cb);
-      const uint32_t scol = lane_addr + uint32_t(2 * TB_NMAX + acc * TB_NMAX + cb);
-      tc::tmem_ld16(dcol, v);
-      if (!first) tc::tmem_ld16(scol, s);
-      tc::tmem_ld_wait();
-      if (!first) {
-#pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] += s[q];
-      }
-      tmem_st16(scol, v);
+  for (int cb = 0; cb < n; cb += 16) {
+    float d0[16], d1[16], s0[16], s1[16];
+    const uint32_t dc0 = lane_addr + uint32_t(cb), dc1 = lane_addr + uint32_t(TB_NMAX + cb);
+    const uint32_t sc0 = lane_addr + uint32_t(2 * TB_NMAX + cb), sc1 = lane_addr + uint32_t(3 * TB_NMAX + cb);
+    tc::tmem_ld16(dc0, d0);
+    tc::tmem_ld16(dc1, d1);
+    if (!first) {
+      tc::tmem_ld16(sc0, s0);
+      tc::tmem_ld16(sc1, s1);
     }
+    tc::tmem_ld_wait();
+    if (!first) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) { d0[q] += s0[q]; d1[q] += s1[q]; }
+    }
+    tmem_st16(sc0, d0);
+    tmem_st16(sc1, d1);
   }
   tmem_st_wait();
 }
@@ -308,10 +311,8 @@ __device__ __forceinline__ TabCta tab_begin(uint8_t* smem_raw) {
   return c;
 }
 
-// issue the stage's MMAs (thread 0) after every thread's operand stores, wait for them and
-// drain D into S; returns false (and raises the error flag) when the wait expires
-__device__ __forceinline__ bool tab_stage(const TabCta& c, uint32_t idesc, int n, bool first, uint32_t& phase,
-                                          int* err_flag) {
+// issue the stage's MMAs (thread 0) once every thread's operand stores are in shared memory
+__device__ __forceinline__ void tab_issue_stage(const TabCta& c, uint32_t idesc) {
   tc::fence_proxy_async();
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -319,6 +320,12 @@ __device__ __forceinline__ bool tab_stage(const TabCta& c, uint32_t idesc, int n
     tab_issue(c.sbase, c.tmem, idesc);
     tc::mma_commit(tc::smem_u32(c.mbar));
   }
+}
+
+// wait for the stage's MMAs and drain D into S; returns false (and raises the error flag) when
+// the wait expires.  After it returns true the operand tiles may be overwritten.
+__device__ __forceinline__ bool tab_finish_stage(const TabCta& c, int n, bool first, uint32_t& phase,
+                                                 int* err_flag) {
   const bool ok = __syncthreads_and(tc::mbar_wait_bounded(tc::smem_u32(c.mbar), phase, TB_WAIT_LIMIT));
   if (!ok) {
     if (threadIdx.x == 0) atomicExch(err_flag, 1);
@@ -379,96 +386,120 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_synth_kernel(const float* _
   const int nb = tab_nblocks(m, lmax);
   const int64_t base = alm_index(m, m, lmax);
   const int nhalf = NOPS == 1 ? 1 : 2;  // stages per table block
-  uint32_t phase_bit = 0;
-  bool ok = true;
-  for (int b = 0; b < nb && ok; ++b) {
+  const int nst = nb * nhalf;
+  // Raw operands of one stage, held in registers from the global loads to the split and the
+  // shared-memory stores, so that stage s + 1 is in flight while the MMAs of stage s run.
+  // A: 4 tasks of a 4 (ring) x 4 (K) block (lane = quad, task t = warp + 4 it).
+  // B: spin 0: 4 tasks (map lane, acc, k4) x 4 l of a_lm; spin s: 2 tasks (map lane & 15) x 4 l x (G, C).
+  float4 va[4][4];
+  float2 ab[4][4];  // rounded to FP32 at the load (the operand is FP32 before its TF32 split anyway)
+  auto a_task = [&](int t, int h, int& acc, int& kk, int& pos0, int& comp) {
+    if (NOPS == 1) {
+      acc = t >> 3; kk = 4 * (t & 7); pos0 = acc * 32 + kk; comp = 0;
+    } else {
+      comp = t >> 3;
+      const int par = (t >> 2) & 1, g4 = t & 3;
+      acc = comp == 0 ? par : 1 - par;
+      kk = 16 * comp + 4 * g4;
+      pos0 = par * 32 + 16 * h + 4 * g4;
+    }
+  };
+  auto load = [&](int st) {
+    const int b = st / nhalf, h = st % nhalf;
     const float* unit0 = table + ((blockoff[m] + b) * int64_t(nquads) + q0) * UNIT;
-    for (int h = 0; h < nhalf && ok; ++h) {
-      // ---- A: 512 tasks of a 4 (ring) x 4 (K) block; lane = quad, warp + 4 it = task t
+    const bool qv = (q0 + lane) < nquads;
 #pragma unroll
-      for (int it = 0; it < 4; ++it) {
-        const int t = warp + 4 * it;
-        int acc, kk, pos0, comp;
-        if (NOPS == 1) {
-          acc = t >> 3; kk = 4 * (t & 7); pos0 = acc * 32 + kk; comp = 0;
-        } else {
-          comp = t >> 3;
-          const int par = (t >> 2) & 1, g4 = t & 3;
-          acc = comp == 0 ? par : 1 - par;
-          kk = 16 * comp + 4 * g4;
-          pos0 = par * 32 + 16 * h + 4 * g4;
-        }
-        float4 v[4];
-        const bool qv = (q0 + lane) < nquads;
-        const float* u = unit0 + int64_t(lane) * UNIT + (comp * TB_LB + pos0) * 4;
+    for (int it = 0; it < 4; ++it) {
+      int acc, kk, pos0, comp;
+      a_task(warp + 4 * it, h, acc, kk, pos0, comp);
+      const float* u = unit0 + int64_t(lane) * UNIT + (comp * TB_LB + pos0) * 4;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-          v[i] = qv ? __ldg(reinterpret_cast<const float4*>(u) + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const int ks = kk >> 3, kc = (kk >> 2) & 1;
-        const uint32_t oh = TabSmem::a(acc, ks, 0), ol = TabSmem::a(acc, ks, 1);
-        // ring 4 lane + i of the tile -> A row 32 i + lane; rings outside [toff, toff + nrp) are zero
-        const int rg0 = 4 * (q0 + lane);
+      for (int i = 0; i < 4; ++i)
+        va[it][i] = qv ? __ldg(reinterpret_cast<const float4*>(u) + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (NOPS == 1) {
+      const int j = lane;
+#pragma unroll
+      for (int i2 = 0; i2 < 4; ++i2) {
+        const int t = warp + 4 * i2, acc = t >> 3, k4 = t & 7;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          const int rt = rg0 + i;
-          const bool in = rt >= toff && rt < toff + nrp;
-          float4 w;
-          w.x = in ? (i == 0 ? v[0].x : i == 1 ? v[0].y : i == 2 ? v[0].z : v[0].w) : 0.f;
-          w.y = in ? (i == 0 ? v[1].x : i == 1 ? v[1].y : i == 2 ? v[1].z : v[1].w) : 0.f;
-          w.z = in ? (i == 0 ? v[2].x : i == 1 ? v[2].y : i == 2 ? v[2].z : v[2].w) : 0.f;
-          w.w = in ? (i == 0 ? v[3].x : i == 1 ? v[3].y : i == 2 ? v[3].z : v[3].w) : 0.f;
-          const uint32_t co = kcore_off(32 * i + lane, kc);
-          st_split(c.smem, oh + co, ol + co, w);
+          const int l = tab_l(m, b, acc * 32 + 4 * k4 + i);
+          const double2 a = (j < gs && l <= lmax) ? almT[(base + (l - m)) * B + b0 + j] : make_double2(0.0, 0.0);
+          ab[i2][i] = make_float2(float(a.x), float(a.y));
         }
       }
-      // ---- B: rows = columns (part, map), K chunks of 4 positions
-      if (NOPS == 1) {
-        // task (map j = lane, acc, k4): 2 chunks (re, im)
-        for (int t = warp; t < 16; t += 4) {
-          const int acc = t >> 3, k4 = t & 7;
-          const int j = lane;
-          if (j < gs) {
-            float4 re, im;
-            float* pr = &re.x;
-            float* pi = &im.x;
+    } else {
+      const int j = lane & 15;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              const int l = tab_l(m, b, acc * 32 + 4 * k4 + i);
-              double2 a = make_double2(0.0, 0.0);
-              if (l <= lmax) a = almT[(base + (l - m)) * B + b0 + j];
-              pr[i] = float(a.x);
-              pi[i] = float(a.y);
-            }
-            const int ks = k4 >> 1, kc = k4 & 1;
-            st_split(c.smem, TabSmem::b(acc, ks, 0) + kcore_off(j, kc), TabSmem::b(acc, ks, 1) + kcore_off(j, kc), re);
-            st_split(c.smem, TabSmem::b(acc, ks, 0) + kcore_off(gs + j, kc),
-                     TabSmem::b(acc, ks, 1) + kcore_off(gs + j, kc), im);
-          }
+      for (int i2 = 0; i2 < 2; ++i2) {
+        const int t = warp * 2 + (lane >> 4) + 8 * i2, acc = t >> 3, k4 = t & 7;
+        const int comp = k4 >> 2, g4 = k4 & 3, par = comp == 0 ? acc : 1 - acc;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int l = tab_l(m, b, par * 32 + 16 * h + 4 * g4 + i);
+          const bool v = j < gs && l <= lmax;
+          const int64_t o = ((base + (l - m)) * B + b0 + j) * 2;
+          const double2 G = v ? almT[o] : make_double2(0.0, 0.0), C = v ? almT[o + 1] : make_double2(0.0, 0.0);
+          ab[2 * i2][i] = make_float2(float(G.x), float(G.y));
+          ab[2 * i2 + 1][i] = make_float2(float(C.x), float(C.y));
         }
-      } else {
-        // task (map j = lane & 15, acc, k4): K chunk k = 4 k4 .. 4 k4 + 3, operand comp = k4 >> 2;
-        // 4 chunks (parts Q.re, Q.im, U.re, U.im)
-        const int j = lane & 15;
-        for (int t = warp * 2 + (lane >> 4); t < 16; t += 8) {
-          const int acc = t >> 3, k4 = t & 7;
-          if (j >= gs) continue;
-          const int comp = k4 >> 2, g4 = k4 & 3;
-          const int par = comp == 0 ? acc : 1 - acc;
-          // F+ rows take X = -(G, C) (even spin) or Y; F- rows the other one
+      }
+    }
+  };
+  auto store = [&](int st) {
+    const int h = st % nhalf;
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      int acc, kk, pos0, comp;
+      a_task(warp + 4 * it, h, acc, kk, pos0, comp);
+      const int ks = kk >> 3, kc = (kk >> 2) & 1;
+      const uint32_t oh = TabSmem::a(acc, ks, 0), ol = TabSmem::a(acc, ks, 1);
+      // ring 4 lane + i of the tile -> A row 32 i + lane; rings outside [toff, toff + nrp) are zero
+      const int rg0 = 4 * (q0 + lane);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int rt = rg0 + i;
+        const bool in = rt >= toff && rt < toff + nrp;
+        float4 w;
+        w.x = in ? (&va[it][0].x)[i] : 0.f;
+        w.y = in ? (&va[it][1].x)[i] : 0.f;
+        w.z = in ? (&va[it][2].x)[i] : 0.f;
+        w.w = in ? (&va[it][3].x)[i] : 0.f;
+        const uint32_t co = kcore_off(32 * i + lane, kc);
+        st_split(c.smem, oh + co, ol + co, w);
+      }
+    }
+    if (NOPS == 1) {
+      const int j = lane;
+      if (j < gs) {
+#pragma unroll
+        for (int i2 = 0; i2 < 4; ++i2) {
+          const int t = warp + 4 * i2, acc = t >> 3, k4 = t & 7;
+          const float4 re = make_float4(ab[i2][0].x, ab[i2][1].x, ab[i2][2].x, ab[i2][3].x);
+          const float4 im = make_float4(ab[i2][0].y, ab[i2][1].y, ab[i2][2].y, ab[i2][3].y);
+          const int ks = k4 >> 1, kc = k4 & 1;
+          st_split(c.smem, TabSmem::b(acc, ks, 0) + kcore_off(j, kc), TabSmem::b(acc, ks, 1) + kcore_off(j, kc), re);
+          st_split(c.smem, TabSmem::b(acc, ks, 0) + kcore_off(gs + j, kc),
+                   TabSmem::b(acc, ks, 1) + kcore_off(gs + j, kc), im);
+        }
+      }
+    } else {
+      // F+ rows take X = -(G, C) (even spin) or Y = (C.im, -C.re, -G.im, G.re); F- rows the other one
+      const int j = lane & 15;
+      if (j < gs) {
+#pragma unroll
+        for (int i2 = 0; i2 < 2; ++i2) {
+          const int t = warp * 2 + (lane >> 4) + 8 * i2, acc = t >> 3, k4 = t & 7;
+          const int comp = k4 >> 2;
           const bool use_x = (comp == 0) != (spin_odd != 0);
           float4 pt[4];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            const int l = tab_l(m, b, par * 32 + 16 * h + 4 * g4 + i);
-            double2 G = make_double2(0.0, 0.0), C = G;
-            if (l <= lmax) {
-              const int64_t o = ((base + (l - m)) * B + b0 + j) * 2;
-              G = almT[o];
-              C = almT[o + 1];
-            }
+            const float2 G = ab[2 * i2][i], C = ab[2 * i2 + 1][i];
             float p0, p1, p2, p3;
-            if (use_x) { p0 = float(-G.x); p1 = float(-G.y); p2 = float(-C.x); p3 = float(-C.y); }
-            else { p0 = float(C.y); p1 = float(-C.x); p2 = float(-G.y); p3 = float(G.x); }
+            if (use_x) { p0 = -G.x; p1 = -G.y; p2 = -C.x; p3 = -C.y; }
+            else { p0 = C.y; p1 = -C.x; p2 = -G.y; p3 = G.x; }
             (&pt[0].x)[i] = p0; (&pt[1].x)[i] = p1; (&pt[2].x)[i] = p2; (&pt[3].x)[i] = p3;
           }
           const int kk = 4 * k4, ks = kk >> 3, kc = (kk >> 2) & 1;
@@ -480,8 +511,17 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_synth_kernel(const float* _
           }
         }
       }
-      ok = tab_stage(c, idesc, n, b == 0 && h == 0, phase_bit, err_flag);
     }
+  };
+  uint32_t phase_bit = 0;
+  bool ok = true;
+  load(0);
+  for (int st = 0; st < nst; ++st) {
+    store(st);
+    tab_issue_stage(c, idesc);
+    if (st + 1 < nst) load(st + 1);
+    ok = tab_finish_stage(c, n, st == 0, phase_bit, err_flag);
+    if (!ok) break;
   }
   if (ok) {
     // epilogue: TMEM lane 32 w + q <-> ring 4 q + w of the tile
@@ -548,21 +588,28 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
   const int R = 2 * nrp - 1;
   const int rt_begin = toff & ~3, rt_end = toff + nrp;
   const int nstages = (rt_end - rt_begin + RSTAGE - 1) / RSTAGE;
-  uint32_t phase_bit = 0;
-  bool ok = true;
-  for (int st = 0; st < nstages && ok; ++st) {
+  // Raw operands of one stage in registers (loaded while the previous stage's MMAs run).
+  // A: NT (acc, blk, comp, quad) combinations, lane = position j, one float4 each (task t = warp + 4 i).
+  // B: tasks (map j, quad qd) t = tid + 128 i: the north and south phases of 4 rings.
+  constexpr int NQ = RSTAGE / 4;
+  constexpr int NT = 2 * 4 * NOPS * NQ;  // (acc, blk, comp, quad) combinations
+  constexpr int NA = NT / 4;
+  constexpr int BT = NOPS == 1 ? 2 : 1;  // tasks per thread: NQ * gs <= 256 (spin 0) or 64 (spin s)
+  float4 va[NA];
+  float2 pn[BT][4][NCOMP], pv[BT][4][NCOMP];
+  auto a_task = [&](int t, int& qd, int& comp, int& blk, int& acc) {
+    qd = t % NQ;
+    int r = t / NQ;
+    comp = r % NOPS; r /= NOPS;
+    blk = r % 4;
+    acc = r / 4;
+  };
+  auto load = [&](int st) {
     const int rs0 = rt_begin + st * RSTAGE;  // first table ring of the stage (quad aligned)
-    // ---- A: rows = 32 positions x 4 blocks, K = rings; chunk = float4 (4 rings at one position)
-    // task: lane = position j within the parity half, warp + 4 it -> (acc, blk, comp, quad)
-    constexpr int NQ = RSTAGE / 4;
-    constexpr int NT = 2 * 4 * NOPS * NQ;  // (acc, blk, comp, quad) combinations
-#pragma unroll 4
-    for (int t = warp; t < NT; t += 4) {
-      const int qd = t % NQ;
-      int r = t / NQ;
-      const int comp = r % NOPS; r /= NOPS;
-      const int blk = r % 4;
-      const int acc = r / 4;
+#pragma unroll
+    for (int i = 0; i < NA; ++i) {
+      int qd, comp, blk, acc;
+      a_task(warp + 4 * i, qd, comp, blk, acc);
       const int b = bb + blk;
       const int qg = rs0 / 4 + qd;
       float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -578,39 +625,57 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
           if (r0 + 3 < toff || r0 + 3 >= rt_end) v.w = 0.f;
         }
       }
-      const int kk = comp * 16 + 4 * qd;  // K index of the chunk (spin 0: comp = 0, qd < 8)
-      const int ks = kk >> 3, kc = (kk >> 2) & 1;
-      const int row = blk * 32 + lane;
-      st_split(c.smem, TabSmem::a(acc, ks, 0) + kcore_off(row, kc), TabSmem::a(acc, ks, 1) + kcore_off(row, kc), v);
+      va[i] = v;
     }
-    // ---- B: rows = columns (part, map), K = rings; task (map j, quad qd)
-    for (int t = tid; t < NQ * gs; t += TB_THREADS) {
-      const int j = t % gs, qd = t / gs;
-      // ring sums (combo 0: N + S) and differences (combo 1: N - S) of 4 rings, per component
-      float4 cre[2][NCOMP], cim[2][NCOMP];
+#pragma unroll
+    for (int bi = 0; bi < BT; ++bi) {
+      const int t = tid + TB_THREADS * bi;
+      const bool tv = t < NQ * gs;
+      const int j = tv ? t % gs : 0, qd = tv ? t / gs : 0;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int rt = rs0 + 4 * qd + i;
         const int ip = rt - toff;
-        float2 nv[NCOMP], sv[NCOMP];
-#pragma unroll
-        for (int cc = 0; cc < NCOMP; ++cc) { nv[cc] = make_float2(0.f, 0.f); sv[cc] = nv[cc]; }
-        if (rt >= toff && ip < nrp) {
-          const int rsth = R - 1 - ip;
-#pragma unroll
-          for (int cc = 0; cc < NCOMP; ++cc) {
-            nv[cc] = phase[((int64_t(ip) * (mmax + 1) + m) * B + b0 + j) * NCOMP + cc];
-            if (rsth != ip) sv[cc] = phase[((int64_t(rsth) * (mmax + 1) + m) * B + b0 + j) * NCOMP + cc];
-          }
-        }
+        const bool in = tv && rt >= toff && ip < nrp;
+        const int rsth = R - 1 - ip;
 #pragma unroll
         for (int cc = 0; cc < NCOMP; ++cc) {
-          (&cre[0][cc].x)[i] = nv[cc].x + sv[cc].x;
-          (&cim[0][cc].x)[i] = nv[cc].y + sv[cc].y;
-          (&cre[1][cc].x)[i] = nv[cc].x - sv[cc].x;
-          (&cim[1][cc].x)[i] = nv[cc].y - sv[cc].y;
+          pn[bi][i][cc] = in ? phase[((int64_t(ip) * (mmax + 1) + m) * B + b0 + j) * NCOMP + cc]
+                             : make_float2(0.f, 0.f);
+          pv[bi][i][cc] = (in && rsth != ip) ? phase[((int64_t(rsth) * (mmax + 1) + m) * B + b0 + j) * NCOMP + cc]
+                                             : make_float2(0.f, 0.f);
         }
       }
+    }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int i = 0; i < NA; ++i) {
+      int qd, comp, blk, acc;
+      a_task(warp + 4 * i, qd, comp, blk, acc);
+      const int kk = comp * 16 + 4 * qd;  // K index of the chunk (spin 0: comp = 0, qd < 8)
+      const int ks = kk >> 3, kc = (kk >> 2) & 1;
+      const int row = blk * 32 + lane;
+      st_split(c.smem, TabSmem::a(acc, ks, 0) + kcore_off(row, kc), TabSmem::a(acc, ks, 1) + kcore_off(row, kc),
+               va[i]);
+    }
+#pragma unroll
+    for (int bi = 0; bi < BT; ++bi) {
+      const int t = tid + TB_THREADS * bi;
+      if (t >= NQ * gs) continue;
+      const int j = t % gs, qd = t / gs;
+      // ring sums (combo 0: N + S) and differences (combo 1: N - S) of 4 rings, per component
+      float4 cre[2][NCOMP], cim[2][NCOMP];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int cc = 0; cc < NCOMP; ++cc) {
+          const float2 nv = pn[bi][i][cc], sv = pv[bi][i][cc];
+          (&cre[0][cc].x)[i] = nv.x + sv.x;
+          (&cim[0][cc].x)[i] = nv.y + sv.y;
+          (&cre[1][cc].x)[i] = nv.x - sv.x;
+          (&cim[1][cc].x)[i] = nv.y - sv.y;
+        }
       if (NOPS == 1) {
         const int kk = 4 * qd, ks = kk >> 3, kc = (kk >> 2) & 1;
 #pragma unroll
@@ -630,7 +695,7 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
           for (int comp = 0; comp < 2; ++comp) {
             const int k = comp == 0 ? acc : 1 - acc;
             const bool use_x = (comp == 0) != (spin_odd != 0);
-            const float4 qr = cre[k][0], qi = cim[k][0], ur = cre[k][1], ui = cim[k][1];
+            const float4 qr = cre[k][0], qi = cim[k][0], ur = cre[k][NCOMP - 1], ui = cim[k][NCOMP - 1];
             float4 p[4];
             if (use_x) {
               p[0] = make_float4(-qr.x, -qr.y, -qr.z, -qr.w);
@@ -654,7 +719,16 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
         }
       }
     }
-    ok = tab_stage(c, idesc, n, st == 0, phase_bit, err_flag);
+  };
+  uint32_t phase_bit = 0;
+  bool ok = true;
+  load(0);
+  for (int st = 0; st < nstages; ++st) {
+    store();
+    tab_issue_stage(c, idesc);
+    if (st + 1 < nstages) load(st + 1);
+    ok = tab_finish_stage(c, n, st == 0, phase_bit, err_flag);
+    if (!ok) break;
   }
   if (ok) {
     // epilogue: TMEM lane = A row = blk * 32 + j; accumulator acc is l = tab_l(m, bb + blk, acc * 32 + j)
