@@ -63,10 +63,8 @@ namespace ps {
 
 constexpr int TB_LB = 64;        // l per table block
 constexpr int TB_TILE = 128;     // ring pairs per synthesis tile (MMA M)
-constexpr int TB_NMAX = 64;      // D columns per accumulator
 constexpr int TB_THREADS = 128;
 constexpr uint32_t TB_WAIT_LIMIT = 1u << 24;
-constexpr uint32_t TB_TMEM_COLS = 256;
 
 // ------------------------------------------------------------------ table geometry
 // number of table blocks of order m
@@ -232,27 +230,70 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
 }
 __device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// shared-memory plan of both GEMMs: A[acc][kstep][hi/lo] 4 KB each, B[acc][kstep][hi/lo] NMAX x 32 B each
+// Shared-memory plan of both GEMMs (offsets from a 1024-byte aligned base):
+//   A[acc][kstep][hi/lo]   4 KB each (128 rows x 8 K)          64 KB
+//   B[acc][kstep][hi/lo]   NMAX x 32 B each                    16 NMAX x 32 B
+//   STG[2]                 raw table tiles of the next stages, filled by bulk copies
+//   MISC                   mbarriers (MMA done, staging buffer full x 2), TMEM slot
+template <int NMAX, uint32_t STG_BYTES>
 struct TabSmem {
   static constexpr int KS = 4;  // K steps (of 8) per accumulator and stage
   static constexpr uint32_t A_TILE = TB_TILE * 32;
-  static constexpr uint32_t B_TILE = TB_NMAX * 32;
+  static constexpr uint32_t B_TILE = NMAX * 32;
   static constexpr uint32_t B_OFF = 2 * KS * 2 * A_TILE;
-  static constexpr uint32_t MISC_OFF = B_OFF + 2 * KS * 2 * B_TILE;
+  static constexpr uint32_t STG_OFF = B_OFF + 2 * KS * 2 * B_TILE;
+  static constexpr uint32_t MISC_OFF = STG_OFF + 2 * STG_BYTES;
   static constexpr uint32_t DYN = MISC_OFF + 64 + 1024;
+  static constexpr uint32_t TMEM_COLS = 4 * NMAX;  // D[2][NMAX], S[2][NMAX]
   __device__ static uint32_t a(int acc, int ks, int hl) { return ((acc * KS + ks) * 2 + hl) * A_TILE; }
   __device__ static uint32_t b(int acc, int ks, int hl) { return B_OFF + ((acc * KS + ks) * 2 + hl) * B_TILE; }
+  __device__ static uint32_t stg(int buf) { return STG_OFF + uint32_t(buf) * STG_BYTES; }
 };
 
+// CTA state shared by both GEMMs
+struct TabCta {
+  uint8_t* smem;
+  uint32_t sbase;
+  uint32_t mbar_mma;   // MMAs of the current stage complete
+  uint32_t mbar_full;  // + 8 * buf: staging buffer buf filled
+  uint32_t tmem;
+};
+
+template <class S>
+__device__ __forceinline__ TabCta tab_begin(uint8_t* smem_raw) {
+  TabCta c;
+  c.smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  c.sbase = tc::smem_u32(c.smem);
+  c.mbar_mma = c.sbase + S::MISC_OFF;
+  c.mbar_full = c.sbase + S::MISC_OFF + 8;
+  uint32_t* slot = reinterpret_cast<uint32_t*>(c.smem + S::MISC_OFF + 32);
+  if ((threadIdx.x >> 5) == 0) {
+    tc::tmem_alloc(tc::smem_u32(slot), S::TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  if (threadIdx.x == 0) {
+    tc::mbar_init(c.mbar_mma, 1);
+    tc::mbar_init(c.mbar_full, 1);
+    tc::mbar_init(c.mbar_full + 8, 1);
+    tc::fence_mbar_init();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  c.tmem = *slot;
+  return c;
+}
+
 // one stage's MMAs: 2 accumulators x 4 K steps x (hi.hi + hi.lo + lo.hi), D fresh per stage
+template <class S, int NMAX>
 __device__ __forceinline__ void tab_issue(uint32_t sbase, uint32_t tmem, uint32_t idesc) {
 #pragma unroll
   for (int acc = 0; acc < 2; ++acc) {
-    const uint32_t d = tmem + uint32_t(acc * TB_NMAX);
+    const uint32_t d = tmem + uint32_t(acc * NMAX);
 #pragma unroll
-    for (int ks = 0; ks < TabSmem::KS; ++ks) {
-      const uint64_t ah = kdesc(sbase + TabSmem::a(acc, ks, 0)), al = kdesc(sbase + TabSmem::a(acc, ks, 1));
-      const uint64_t bh = kdesc(sbase + TabSmem::b(acc, ks, 0)), bl = kdesc(sbase + TabSmem::b(acc, ks, 1));
+    for (int ks = 0; ks < S::KS; ++ks) {
+      const uint64_t ah = kdesc(sbase + S::a(acc, ks, 0)), al = kdesc(sbase + S::a(acc, ks, 1));
+      const uint64_t bh = kdesc(sbase + S::b(acc, ks, 0)), bl = kdesc(sbase + S::b(acc, ks, 1));
       tc::mma_tf32(d, ah, bh, idesc, ks > 0 ? 1u : 0u);
       tc::mma_tf32(d, ah, bl, idesc, 1u);
       tc::mma_tf32(d, al, bh, idesc, 1u);
@@ -262,12 +303,13 @@ __device__ __forceinline__ void tab_issue(uint32_t sbase, uint32_t tmem, uint32_
 
 // S += D for this thread's TMEM lane (first stage: S = D), columns [0, n) of both accumulators;
 // the four loads of a column chunk (D and S of both accumulators) share one wait
+template <int NMAX>
 __device__ __forceinline__ void tab_drain(uint32_t lane_addr, int n, bool first) {
 #pragma unroll 1
   for (int cb = 0; cb < n; cb += 16) {
     float d0[16], d1[16], s0[16], s1[16];
-    const uint32_t dc0 = lane_addr + uint32_t(cb), dc1 = lane_addr + uint32_t(TB_NMAX + cb);
-    const uint32_t sc0 = lane_addr + uint32_t(2 * TB_NMAX + cb), sc1 = lane_addr + uint32_t(3 * TB_NMAX + cb);
+    const uint32_t dc0 = lane_addr + uint32_t(cb), dc1 = lane_addr + uint32_t(NMAX + cb);
+    const uint32_t sc0 = lane_addr + uint32_t(2 * NMAX + cb), sc1 = lane_addr + uint32_t(3 * NMAX + cb);
     tc::tmem_ld16(dc0, d0);
     tc::tmem_ld16(dc1, d1);
     if (!first) {
@@ -285,91 +327,85 @@ __device__ __forceinline__ void tab_drain(uint32_t lane_addr, int n, bool first)
   tmem_st_wait();
 }
 
-// CTA prologue / epilogue shared by both GEMMs
-struct TabCta {
-  uint8_t* smem;
-  uint32_t sbase;
-  uint64_t* mbar;
-  uint32_t tmem;
-};
-
-__device__ __forceinline__ TabCta tab_begin(uint8_t* smem_raw) {
-  TabCta c;
-  c.smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  c.sbase = tc::smem_u32(c.smem);
-  c.mbar = reinterpret_cast<uint64_t*>(c.smem + TabSmem::MISC_OFF);
-  uint32_t* slot = reinterpret_cast<uint32_t*>(c.smem + TabSmem::MISC_OFF + 16);
-  if ((threadIdx.x >> 5) == 0) {
-    tc::tmem_alloc(tc::smem_u32(slot), TB_TMEM_COLS);
-    tc::tmem_relinquish();
-  }
-  if (threadIdx.x == 0) tc::mbar_init(tc::smem_u32(c.mbar), 1);
-  tc::fence_before_sync();
-  __syncthreads();
-  tc::fence_after_sync();
-  c.tmem = *slot;
-  return c;
+// bounded wait of every thread on an mbarrier phase; on expiry raise the flag
+__device__ __forceinline__ bool tab_wait(uint32_t mbar, uint32_t parity, int* err_flag) {
+  const bool ok = __syncthreads_and(tc::mbar_wait_bounded(mbar, parity, TB_WAIT_LIMIT));
+  if (!ok && threadIdx.x == 0) atomicExch(err_flag, 1);
+  return ok;
 }
 
-// issue the stage's MMAs (thread 0) once every thread's operand stores are in shared memory
+// make every thread's operand stores visible to the tensor core, then (thread 0) issue the MMAs
+template <class S, int NMAX>
 __device__ __forceinline__ void tab_issue_stage(const TabCta& c, uint32_t idesc) {
   tc::fence_proxy_async();
   __syncthreads();
   if (threadIdx.x == 0) {
     tc::fence_after_sync();
-    tab_issue(c.sbase, c.tmem, idesc);
-    tc::mma_commit(tc::smem_u32(c.mbar));
+    tab_issue<S, NMAX>(c.sbase, c.tmem, idesc);
+    tc::mma_commit(c.mbar_mma);
   }
 }
 
-// wait for the stage's MMAs and drain D into S; returns false (and raises the error flag) when
-// the wait expires.  After it returns true the operand tiles may be overwritten.
+// wait for the stage's MMAs and drain D into S; false (flag raised) when the wait expires
+template <int NMAX>
 __device__ __forceinline__ bool tab_finish_stage(const TabCta& c, int n, bool first, uint32_t& phase,
                                                  int* err_flag) {
-  const bool ok = __syncthreads_and(tc::mbar_wait_bounded(tc::smem_u32(c.mbar), phase, TB_WAIT_LIMIT));
-  if (!ok) {
-    if (threadIdx.x == 0) atomicExch(err_flag, 1);
-    tc::mbar_wait_bounded(tc::smem_u32(c.mbar), phase, TB_WAIT_LIMIT);
+  if (!tab_wait(c.mbar_mma, phase, err_flag)) {
+    tc::mbar_wait_bounded(c.mbar_mma, phase, TB_WAIT_LIMIT);  // once more, for the issued MMAs
     return false;
   }
   phase ^= 1u;
   tc::fence_after_sync();
   const uint32_t lane_addr = c.tmem + (uint32_t((threadIdx.x >> 5) * 32) << 16);
-  tab_drain(lane_addr, n, first);
+  tab_drain<NMAX>(lane_addr, n, first);
   tc::fence_before_sync();
   __syncthreads();
   return true;
 }
 
+template <class S>
 __device__ __forceinline__ void tab_end(const TabCta& c) {
   tc::fence_before_sync();
   __syncthreads();
-  if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(c.tmem, TB_TMEM_COLS);
+  if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(c.tmem, S::TMEM_COLS);
 }
 
 // the S columns [cb, cb + 16) of accumulator acc of this thread's lane
+template <int NMAX>
 __device__ __forceinline__ void tab_read_sum(const TabCta& c, int acc, int cb, float* v) {
   const uint32_t lane_addr = c.tmem + (uint32_t((threadIdx.x >> 5) * 32) << 16);
-  tc::tmem_ld16(lane_addr + uint32_t(2 * TB_NMAX + acc * TB_NMAX + cb), v);
+  tc::tmem_ld16(lane_addr + uint32_t(2 * NMAX + acc * NMAX + cb), v);
   tc::tmem_ld_wait();
 }
 
 __device__ __forceinline__ int round16(int x) { return (x + 15) & ~15; }
 
-// ------------------------------------------------------------------ synthesis
-// almT [nalm][B][NCOMP] complex128 -> phase [R][mmax+1][B][NCOMP] complex64 of the ring pairs
-// [0, nrp) (table rings toff + i; north row i, south row R - 1 - i, R = 2 nrp - 1).
-// grid.x = map group + G * (ring tile + T * m)
+// raw table tile of the synthesis: the 32 units (quads) of one block and ring tile, each unit at a
+// padded stride (unit + 16 bytes) so that lanes reading different units hit different banks
 template <int NOPS>
-__global__ void __launch_bounds__(TB_THREADS, 2) tab_synth_kernel(const float* __restrict__ table,
+struct SynthStg {
+  static constexpr int UNIT = NOPS * TB_LB * 4;  // floats
+  static constexpr int USTR = UNIT + 4;
+  static constexpr uint32_t BYTES = 32u * USTR * 4u;
+};
+
+// ------------------------------------------------------------------ synthesis
+// almT [nalm][B][NOPS] complex128 -> phase [R][mmax+1][B][NOPS] complex64 of the ring pairs
+// [0, nrp) (table rings toff + i; north row i, south row R - 1 - i, R = 2 nrp - 1).
+// grid.x = map group + G * (ring tile + T * m).  One CTA per SM: the table tiles of the next two
+// blocks are in flight (bulk copies into the staging buffers) while a stage is split and multiplied.
+template <int NOPS, int NMAX>
+__global__ void __launch_bounds__(TB_THREADS, 1) tab_synth_kernel(const float* __restrict__ table,
                                                                    const int64_t* __restrict__ blockoff, int nquads,
                                                                    int toff, int nrp, int lmax, int mmax,
                                                                    const double2* __restrict__ almT,
                                                                    float2* __restrict__ phase, int B, int gsize,
                                                                    int ngroups, int ntiles, int spin_odd,
                                                                    int* __restrict__ err_flag) {
+  using G = SynthStg<NOPS>;
+  using S = TabSmem<NMAX, G::BYTES>;
   constexpr int NCOMP = NOPS;
-  constexpr int UNIT = NOPS * TB_LB * 4;
+  constexpr int UNIT = G::UNIT;
   extern __shared__ uint8_t tab_smem_raw[];
   int bid = blockIdx.x;
   const int grp = bid % ngroups; bid /= ngroups;
@@ -381,51 +417,42 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_synth_kernel(const float* _
   const int n = round16(ncols);
   const uint32_t idesc = tc::idesc_tf32(128, n, 0, 0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  TabCta c = tab_begin(tab_smem_raw);
+  TabCta c = tab_begin<S>(tab_smem_raw);
   const int q0 = toff / 4 + tile * 32;  // first table quad of the tile
   const int nb = tab_nblocks(m, lmax);
   const int64_t base = alm_index(m, m, lmax);
   const int nhalf = NOPS == 1 ? 1 : 2;  // stages per table block
   const int nst = nb * nhalf;
-  // Raw operands of one stage, held in registers from the global loads to the split and the
-  // shared-memory stores, so that stage s + 1 is in flight while the MMAs of stage s run.
-  // A: 4 tasks of a 4 (ring) x 4 (K) block (lane = quad, task t = warp + 4 it).
-  // B: spin 0: 4 tasks (map lane, acc, k4) x 4 l of a_lm; spin s: 2 tasks (map lane & 15) x 4 l x (G, C).
-  float4 va[4][4];
-  float2 ab[4][4];  // rounded to FP32 at the load (the operand is FP32 before its TF32 split anyway)
-  auto a_task = [&](int t, int h, int& acc, int& kk, int& pos0, int& comp) {
-    if (NOPS == 1) {
-      acc = t >> 3; kk = 4 * (t & 7); pos0 = acc * 32 + kk; comp = 0;
-    } else {
-      comp = t >> 3;
-      const int par = (t >> 2) & 1, g4 = t & 3;
-      acc = comp == 0 ? par : 1 - par;
-      kk = 16 * comp + 4 * g4;
-      pos0 = par * 32 + 16 * h + 4 * g4;
-    }
+  const int nvq = max(0, min(32, nquads - q0));  // units of the tile inside the table
+  // bulk copies of block b's tile into staging buffer b & 1 (thread 0)
+  int issued = 0, waited = 0;  // blocks whose copies were issued / whose buffer wait completed (all threads)
+  auto issue_block = [&](int b) {
+    if (b >= nb) return;
+    issued = b + 1;
+    if (threadIdx.x != 0) return;
+    const uint32_t bar = c.mbar_full + 8u * uint32_t(b & 1);
+    tc::mbar_arrive_expect_tx(bar, uint32_t(nvq) * UNIT * 4u);
+    const float* src = table + ((blockoff[m] + b) * int64_t(nquads) + q0) * UNIT;
+    const uint32_t dst = c.sbase + S::stg(b & 1);
+    for (int q = 0; q < nvq; ++q) tc::bulk_g2s(dst + uint32_t(q) * G::USTR * 4u, src + int64_t(q) * UNIT, UNIT * 4u, bar);
   };
-  auto load = [&](int st) {
+  // alm of one stage in registers (FP32), loaded a stage ahead.  spin 0: tasks t = tid + 128 i2
+  // (map j = t % gs, (acc, k4) = t / gs; 16 gs <= 8 NMAX tasks) x 4 l; spin s: 2 tasks (map
+  // lane & 15) x 4 l x (G, C)
+  constexpr int BTS = NOPS == 1 ? (NMAX / 2) * 16 / TB_THREADS : 4;
+  float2 ab[BTS][4];
+  auto load_alm = [&](int st) {
     const int b = st / nhalf, h = st % nhalf;
-    const float* unit0 = table + ((blockoff[m] + b) * int64_t(nquads) + q0) * UNIT;
-    const bool qv = (q0 + lane) < nquads;
-#pragma unroll
-    for (int it = 0; it < 4; ++it) {
-      int acc, kk, pos0, comp;
-      a_task(warp + 4 * it, h, acc, kk, pos0, comp);
-      const float* u = unit0 + int64_t(lane) * UNIT + (comp * TB_LB + pos0) * 4;
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        va[it][i] = qv ? __ldg(reinterpret_cast<const float4*>(u) + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
     if (NOPS == 1) {
-      const int j = lane;
 #pragma unroll
-      for (int i2 = 0; i2 < 4; ++i2) {
-        const int t = warp + 4 * i2, acc = t >> 3, k4 = t & 7;
+      for (int i2 = 0; i2 < BTS; ++i2) {
+        const int t = tid + TB_THREADS * i2;
+        const bool tv = t < 16 * gs;
+        const int j = tv ? t % gs : 0, ak = tv ? t / gs : 0, acc = ak >> 3, k4 = ak & 7;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const int l = tab_l(m, b, acc * 32 + 4 * k4 + i);
-          const double2 a = (j < gs && l <= lmax) ? almT[(base + (l - m)) * B + b0 + j] : make_double2(0.0, 0.0);
+          const double2 a = (tv && l <= lmax) ? almT[(base + (l - m)) * B + b0 + j] : make_double2(0.0, 0.0);
           ab[i2][i] = make_float2(float(a.x), float(a.y));
         }
       }
@@ -440,49 +467,63 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_synth_kernel(const float* _
           const int l = tab_l(m, b, par * 32 + 16 * h + 4 * g4 + i);
           const bool v = j < gs && l <= lmax;
           const int64_t o = ((base + (l - m)) * B + b0 + j) * 2;
-          const double2 G = v ? almT[o] : make_double2(0.0, 0.0), C = v ? almT[o + 1] : make_double2(0.0, 0.0);
-          ab[2 * i2][i] = make_float2(float(G.x), float(G.y));
-          ab[2 * i2 + 1][i] = make_float2(float(C.x), float(C.y));
+          const double2 Gv = v ? almT[o] : make_double2(0.0, 0.0), Cv = v ? almT[o + 1] : make_double2(0.0, 0.0);
+          ab[2 * i2][i] = make_float2(float(Gv.x), float(Gv.y));
+          ab[2 * i2 + 1][i] = make_float2(float(Cv.x), float(Cv.y));
         }
       }
     }
   };
+  // split and store the operands of stage st: A from the staged table tile, B from the registers
   auto store = [&](int st) {
-    const int h = st % nhalf;
+    const int b = st / nhalf, h = st % nhalf;
+    const float* stg = reinterpret_cast<const float*>(c.smem + S::stg(b & 1));
 #pragma unroll
     for (int it = 0; it < 4; ++it) {
+      const int t = warp + 4 * it;
       int acc, kk, pos0, comp;
-      a_task(warp + 4 * it, h, acc, kk, pos0, comp);
+      if (NOPS == 1) {
+        acc = t >> 3; kk = 4 * (t & 7); pos0 = acc * 32 + kk; comp = 0;
+      } else {
+        comp = t >> 3;
+        const int par = (t >> 2) & 1, g4 = t & 3;
+        acc = comp == 0 ? par : 1 - par;
+        kk = 16 * comp + 4 * g4;
+        pos0 = par * 32 + 16 * h + 4 * g4;
+      }
+      const float* u = stg + lane * G::USTR + (comp * TB_LB + pos0) * 4;
+      float4 v[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) v[i] = reinterpret_cast<const float4*>(u)[i];
       const int ks = kk >> 3, kc = (kk >> 2) & 1;
-      const uint32_t oh = TabSmem::a(acc, ks, 0), ol = TabSmem::a(acc, ks, 1);
-      // ring 4 lane + i of the tile -> A row 32 i + lane; rings outside [toff, toff + nrp) are zero
+      const uint32_t oh = S::a(acc, ks, 0), ol = S::a(acc, ks, 1);
+      // ring 4 lane + i of the tile -> A row 32 i + lane; rings outside [toff, toff + nrp) (and units
+      // beyond the table) are zero
       const int rg0 = 4 * (q0 + lane);
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int rt = rg0 + i;
-        const bool in = rt >= toff && rt < toff + nrp;
+        const bool in = rt >= toff && rt < toff + nrp && lane < nvq;
         float4 w;
-        w.x = in ? (&va[it][0].x)[i] : 0.f;
-        w.y = in ? (&va[it][1].x)[i] : 0.f;
-        w.z = in ? (&va[it][2].x)[i] : 0.f;
-        w.w = in ? (&va[it][3].x)[i] : 0.f;
+        w.x = in ? (&v[0].x)[i] : 0.f;
+        w.y = in ? (&v[1].x)[i] : 0.f;
+        w.z = in ? (&v[2].x)[i] : 0.f;
+        w.w = in ? (&v[3].x)[i] : 0.f;
         const uint32_t co = kcore_off(32 * i + lane, kc);
         st_split(c.smem, oh + co, ol + co, w);
       }
     }
     if (NOPS == 1) {
-      const int j = lane;
-      if (j < gs) {
 #pragma unroll
-        for (int i2 = 0; i2 < 4; ++i2) {
-          const int t = warp + 4 * i2, acc = t >> 3, k4 = t & 7;
-          const float4 re = make_float4(ab[i2][0].x, ab[i2][1].x, ab[i2][2].x, ab[i2][3].x);
-          const float4 im = make_float4(ab[i2][0].y, ab[i2][1].y, ab[i2][2].y, ab[i2][3].y);
-          const int ks = k4 >> 1, kc = k4 & 1;
-          st_split(c.smem, TabSmem::b(acc, ks, 0) + kcore_off(j, kc), TabSmem::b(acc, ks, 1) + kcore_off(j, kc), re);
-          st_split(c.smem, TabSmem::b(acc, ks, 0) + kcore_off(gs + j, kc),
-                   TabSmem::b(acc, ks, 1) + kcore_off(gs + j, kc), im);
-        }
+      for (int i2 = 0; i2 < BTS; ++i2) {
+        const int t = tid + TB_THREADS * i2;
+        if (t >= 16 * gs) continue;
+        const int j = t % gs, ak = t / gs, acc = ak >> 3, k4 = ak & 7;
+        const float4 re = make_float4(ab[i2][0].x, ab[i2][1].x, ab[i2][2].x, ab[i2][3].x);
+        const float4 im = make_float4(ab[i2][0].y, ab[i2][1].y, ab[i2][2].y, ab[i2][3].y);
+        const int ks = k4 >> 1, kc = k4 & 1;
+        st_split(c.smem, S::b(acc, ks, 0) + kcore_off(j, kc), S::b(acc, ks, 1) + kcore_off(j, kc), re);
+        st_split(c.smem, S::b(acc, ks, 0) + kcore_off(gs + j, kc), S::b(acc, ks, 1) + kcore_off(gs + j, kc), im);
       }
     } else {
       // F+ rows take X = -(G, C) (even spin) or Y = (C.im, -C.re, -G.im, G.re); F- rows the other one
@@ -496,31 +537,42 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_synth_kernel(const float* _
           float4 pt[4];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            const float2 G = ab[2 * i2][i], C = ab[2 * i2 + 1][i];
+            const float2 Gv = ab[2 * i2][i], Cv = ab[2 * i2 + 1][i];
             float p0, p1, p2, p3;
-            if (use_x) { p0 = -G.x; p1 = -G.y; p2 = -C.x; p3 = -C.y; }
-            else { p0 = C.y; p1 = -C.x; p2 = -G.y; p3 = G.x; }
+            if (use_x) { p0 = -Gv.x; p1 = -Gv.y; p2 = -Cv.x; p3 = -Cv.y; }
+            else { p0 = Cv.y; p1 = -Cv.x; p2 = -Gv.y; p3 = Gv.x; }
             (&pt[0].x)[i] = p0; (&pt[1].x)[i] = p1; (&pt[2].x)[i] = p2; (&pt[3].x)[i] = p3;
           }
           const int kk = 4 * k4, ks = kk >> 3, kc = (kk >> 2) & 1;
 #pragma unroll
           for (int part = 0; part < 4; ++part) {
             const int row = part * gs + j;
-            st_split(c.smem, TabSmem::b(acc, ks, 0) + kcore_off(row, kc), TabSmem::b(acc, ks, 1) + kcore_off(row, kc),
-                     pt[part]);
+            st_split(c.smem, S::b(acc, ks, 0) + kcore_off(row, kc), S::b(acc, ks, 1) + kcore_off(row, kc), pt[part]);
           }
         }
       }
     }
   };
-  uint32_t phase_bit = 0;
+  uint32_t ph_mma = 0;
   bool ok = true;
-  load(0);
+  issue_block(0);
+  issue_block(1);
+  load_alm(0);
   for (int st = 0; st < nst; ++st) {
+    const int b = st / nhalf, h = st % nhalf;
+    if (h == 0) {
+      if (!tab_wait(c.mbar_full + 8u * uint32_t(b & 1), uint32_t(b >> 1) & 1u, err_flag)) {
+        ok = false;
+        break;
+      }
+      waited = b + 1;
+    }
     store(st);
-    tab_issue_stage(c, idesc);
-    if (st + 1 < nst) load(st + 1);
-    ok = tab_finish_stage(c, n, st == 0, phase_bit, err_flag);
+    tab_issue_stage<S, NMAX>(c, idesc);
+    // the staged tile of block b has been read (barrier inside tab_issue_stage): refill its buffer
+    if (h == nhalf - 1) issue_block(b + 2);
+    if (st + 1 < nst) load_alm(st + 1);
+    ok = tab_finish_stage<NMAX>(c, n, st == 0, ph_mma, err_flag);
     if (!ok) break;
   }
   if (ok) {
@@ -533,8 +585,8 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_synth_kernel(const float* _
 #pragma unroll 1
     for (int cb = 0; cb < n; cb += 16) {
       float s0[16], s1[16];
-      tab_read_sum(c, 0, cb, s0);
-      tab_read_sum(c, 1, cb, s1);
+      tab_read_sum<NMAX>(c, 0, cb, s0);
+      tab_read_sum<NMAX>(c, 1, cb, s1);
       if (!in) continue;
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
@@ -550,16 +602,29 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_synth_kernel(const float* _
         }
       }
     }
+  } else if (threadIdx.x == 0) {
+    // bulk copies still in flight land in this CTA's shared memory: wait for them (bounded) before exit
+    for (int k = waited; k < issued; ++k)
+      tc::mbar_wait_bounded(c.mbar_full + 8u * uint32_t(k & 1), uint32_t(k >> 1) & 1u, TB_WAIT_LIMIT);
   }
-  tab_end(c);
+  tab_end<S>(c);
 }
 
-// ------------------------------------------------------------------ adjoint
-// phase [R][mmax+1][B][NCOMP] complex64 of ring pairs [0, nrp) -> alm of map b at alm + b * out_stride
-// ([NCOMP][nalm] complex128, times scale and lscale[comp][idx] when given), for the maps [b0, b0 + gs)
-// of each group.  grid.x = map group + G * (entry of the (m, first block) work list)
+// raw table tile of one adjoint stage: for each of the 4 blocks, the RSTAGE / 4 consecutive units
 template <int NOPS>
-__global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __restrict__ table,
+struct AdjStg {
+  static constexpr int UNIT = NOPS * TB_LB * 4;
+  static constexpr int NQ = NOPS == 1 ? 8 : 4;  // quads per stage
+  static constexpr uint32_t BLK_BYTES = uint32_t(NQ) * UNIT * 4u;
+  static constexpr uint32_t BYTES = 4u * BLK_BYTES;
+};
+
+// ------------------------------------------------------------------ adjoint
+// phase [R][mmax+1][B][NOPS] complex64 of ring pairs [0, nrp) -> alm of map b at alm + b * out_stride
+// ([NOPS][nalm] complex128, times scale and lscale[comp][idx] when given), for the maps [b0, b0 + gs)
+// of each group.  grid.x = map group + G * (entry of the (m, first block) work list)
+template <int NOPS, int NMAX>
+__global__ void __launch_bounds__(TB_THREADS, 1) tab_adj_kernel(const float* __restrict__ table,
                                                                  const int64_t* __restrict__ blockoff, int nquads,
                                                                  int toff, int nrp, int lmax, int mmax,
                                                                  const float2* __restrict__ phase,
@@ -569,9 +634,12 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
                                                                  int64_t out_stride,
                                                                  const double* __restrict__ lscale,
                                                                  int* __restrict__ err_flag) {
+  using G = AdjStg<NOPS>;
+  using S = TabSmem<NMAX, G::BYTES>;
   constexpr int NCOMP = NOPS;
-  constexpr int UNIT = NOPS * TB_LB * 4;
-  constexpr int RSTAGE = NOPS == 1 ? 32 : 16;  // table rings per stage
+  constexpr int UNIT = G::UNIT;
+  constexpr int RSTAGE = 4 * G::NQ;  // table rings per stage
+  constexpr int NQ = G::NQ;
   extern __shared__ uint8_t tab_smem_raw[];
   int bid = blockIdx.x;
   const int grp = bid % ngroups; bid /= ngroups;
@@ -583,50 +651,36 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
   const int n = round16(ncols);
   const uint32_t idesc = tc::idesc_tf32(128, n, 0, 0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  TabCta c = tab_begin(tab_smem_raw);
+  TabCta c = tab_begin<S>(tab_smem_raw);
   const int nb = tab_nblocks(m, lmax);
   const int R = 2 * nrp - 1;
   const int rt_begin = toff & ~3, rt_end = toff + nrp;
   const int nstages = (rt_end - rt_begin + RSTAGE - 1) / RSTAGE;
-  // Raw operands of one stage in registers (loaded while the previous stage's MMAs run).
-  // A: NT (acc, blk, comp, quad) combinations, lane = position j, one float4 each (task t = warp + 4 i).
-  // B: tasks (map j, quad qd) t = tid + 128 i: the north and south phases of 4 rings.
-  constexpr int NQ = RSTAGE / 4;
-  constexpr int NT = 2 * 4 * NOPS * NQ;  // (acc, blk, comp, quad) combinations
-  constexpr int NA = NT / 4;
-  constexpr int BT = NOPS == 1 ? 2 : 1;  // tasks per thread: NQ * gs <= 256 (spin 0) or 64 (spin s)
-  float4 va[NA];
-  float2 pn[BT][4][NCOMP], pv[BT][4][NCOMP];
-  auto a_task = [&](int t, int& qd, int& comp, int& blk, int& acc) {
-    qd = t % NQ;
-    int r = t / NQ;
-    comp = r % NOPS; r /= NOPS;
-    blk = r % 4;
-    acc = r / 4;
-  };
-  auto load = [&](int st) {
-    const int rs0 = rt_begin + st * RSTAGE;  // first table ring of the stage (quad aligned)
-#pragma unroll
-    for (int i = 0; i < NA; ++i) {
-      int qd, comp, blk, acc;
-      a_task(warp + 4 * i, qd, comp, blk, acc);
-      const int b = bb + blk;
-      const int qg = rs0 / 4 + qd;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (b < nb && qg < nquads) {
-        v = __ldg(reinterpret_cast<const float4*>(table + ((blockoff[m] + b) * int64_t(nquads) + qg) * UNIT +
-                                                  (comp * TB_LB + acc * 32 + lane) * 4));
-        // rings outside [toff, toff + nrp) contribute nothing
-        const int r0 = 4 * qg;
-        if (r0 < toff || r0 + 3 >= rt_end) {
-          if (r0 + 0 < toff || r0 + 0 >= rt_end) v.x = 0.f;
-          if (r0 + 1 < toff || r0 + 1 >= rt_end) v.y = 0.f;
-          if (r0 + 2 < toff || r0 + 2 >= rt_end) v.z = 0.f;
-          if (r0 + 3 < toff || r0 + 3 >= rt_end) v.w = 0.f;
-        }
-      }
-      va[i] = v;
+  // bulk copies of stage st's units into staging buffer st & 1 (thread 0)
+  int issued = 0, waited = 0;  // stages whose copies were issued / whose buffer wait completed (all threads)
+  auto issue_stage_copy = [&](int st) {
+    if (st >= nstages) return;
+    issued = st + 1;
+    if (threadIdx.x != 0) return;
+    const int qs = (rt_begin + st * RSTAGE) / 4;
+    const int nvq = max(0, min(NQ, nquads - qs));
+    int nblk = 0;
+    for (int blk = 0; blk < 4; ++blk) nblk += (bb + blk < nb);
+    const uint32_t bar = c.mbar_full + 8u * uint32_t(st & 1);
+    tc::mbar_arrive_expect_tx(bar, uint32_t(nblk * nvq) * UNIT * 4u);
+    const uint32_t dst = c.sbase + S::stg(st & 1);
+    for (int blk = 0; blk < 4; ++blk) {
+      if (bb + blk >= nb || nvq == 0) continue;
+      const float* src = table + ((blockoff[m] + bb + blk) * int64_t(nquads) + qs) * UNIT;
+      tc::bulk_g2s(dst + uint32_t(blk) * G::BLK_BYTES, src, uint32_t(nvq) * UNIT * 4u, bar);
     }
+  };
+  // phases of one stage in registers, loaded a stage ahead: tasks (map j, quad qd) t = tid + 128 i
+  // tasks per thread: NQ quads x up to NMAX / 2 (spin 0) or NMAX / 4 (spin s) maps
+  constexpr int BT = (NQ * (NOPS == 1 ? NMAX / 2 : NMAX / 4) + TB_THREADS - 1) / TB_THREADS;
+  float2 pn[BT][4][NCOMP], pv[BT][4][NCOMP];
+  auto load_phase = [&](int st) {
+    const int rs0 = rt_begin + st * RSTAGE;
 #pragma unroll
     for (int bi = 0; bi < BT; ++bi) {
       const int t = tid + TB_THREADS * bi;
@@ -648,16 +702,38 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
       }
     }
   };
-  auto store = [&]() {
-#pragma unroll
-    for (int i = 0; i < NA; ++i) {
-      int qd, comp, blk, acc;
-      a_task(warp + 4 * i, qd, comp, blk, acc);
+  auto store = [&](int st) {
+    const int rs0 = rt_begin + st * RSTAGE;
+    const float* stg = reinterpret_cast<const float*>(c.smem + S::stg(st & 1));
+    // A: rows = 32 positions x 4 blocks, K = rings; chunk = float4 (4 rings at one position);
+    // task t = warp + 4 i -> (quad, comp, block, acc), lane = position within the parity half
+    constexpr int NT = 2 * 4 * NOPS * NQ;
+#pragma unroll 4
+    for (int t = warp; t < NT; t += 4) {
+      const int qd = t % NQ;
+      int r = t / NQ;
+      const int comp = r % NOPS; r /= NOPS;
+      const int blk = r % 4;
+      const int acc = r / 4;
+      const int b = bb + blk;
+      const int qg = rs0 / 4 + qd;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (b < nb && qg < nquads) {
+        v = *reinterpret_cast<const float4*>(stg + blk * (G::BLK_BYTES / 4) + qd * UNIT +
+                                             (comp * TB_LB + acc * 32 + lane) * 4);
+        // rings outside [toff, toff + nrp) contribute nothing
+        const int r0 = 4 * qg;
+        if (r0 < toff || r0 + 3 >= rt_end) {
+          if (r0 + 0 < toff || r0 + 0 >= rt_end) v.x = 0.f;
+          if (r0 + 1 < toff || r0 + 1 >= rt_end) v.y = 0.f;
+          if (r0 + 2 < toff || r0 + 2 >= rt_end) v.z = 0.f;
+          if (r0 + 3 < toff || r0 + 3 >= rt_end) v.w = 0.f;
+        }
+      }
       const int kk = comp * 16 + 4 * qd;  // K index of the chunk (spin 0: comp = 0, qd < 8)
       const int ks = kk >> 3, kc = (kk >> 2) & 1;
       const int row = blk * 32 + lane;
-      st_split(c.smem, TabSmem::a(acc, ks, 0) + kcore_off(row, kc), TabSmem::a(acc, ks, 1) + kcore_off(row, kc),
-               va[i]);
+      st_split(c.smem, S::a(acc, ks, 0) + kcore_off(row, kc), S::a(acc, ks, 1) + kcore_off(row, kc), v);
     }
 #pragma unroll
     for (int bi = 0; bi < BT; ++bi) {
@@ -680,10 +756,9 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
         const int kk = 4 * qd, ks = kk >> 3, kc = (kk >> 2) & 1;
 #pragma unroll
         for (int acc = 0; acc < 2; ++acc) {
-          st_split(c.smem, TabSmem::b(acc, ks, 0) + kcore_off(j, kc), TabSmem::b(acc, ks, 1) + kcore_off(j, kc),
-                   cre[acc][0]);
-          st_split(c.smem, TabSmem::b(acc, ks, 0) + kcore_off(gs + j, kc),
-                   TabSmem::b(acc, ks, 1) + kcore_off(gs + j, kc), cim[acc][0]);
+          st_split(c.smem, S::b(acc, ks, 0) + kcore_off(j, kc), S::b(acc, ks, 1) + kcore_off(j, kc), cre[acc][0]);
+          st_split(c.smem, S::b(acc, ks, 0) + kcore_off(gs + j, kc), S::b(acc, ks, 1) + kcore_off(gs + j, kc),
+                   cim[acc][0]);
         }
       } else {
         // columns (G.re, G.im, C.re, C.im); combo k: Q = (cre[k][0], cim[k][0]), U = (cre[k][1], cim[k][1])
@@ -712,22 +787,30 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
 #pragma unroll
             for (int part = 0; part < 4; ++part) {
               const int row = part * gs + j;
-              st_split(c.smem, TabSmem::b(acc, ks, 0) + kcore_off(row, kc),
-                       TabSmem::b(acc, ks, 1) + kcore_off(row, kc), p[part]);
+              st_split(c.smem, S::b(acc, ks, 0) + kcore_off(row, kc), S::b(acc, ks, 1) + kcore_off(row, kc),
+                       p[part]);
             }
           }
         }
       }
     }
   };
-  uint32_t phase_bit = 0;
+  uint32_t ph_mma = 0;
   bool ok = true;
-  load(0);
+  issue_stage_copy(0);
+  issue_stage_copy(1);
+  load_phase(0);
   for (int st = 0; st < nstages; ++st) {
-    store();
-    tab_issue_stage(c, idesc);
-    if (st + 1 < nstages) load(st + 1);
-    ok = tab_finish_stage(c, n, st == 0, phase_bit, err_flag);
+    if (!tab_wait(c.mbar_full + 8u * uint32_t(st & 1), uint32_t(st >> 1) & 1u, err_flag)) {
+      ok = false;
+      break;
+    }
+    waited = st + 1;
+    store(st);
+    tab_issue_stage<S, NMAX>(c, idesc);
+    issue_stage_copy(st + 2);  // staging buffer st & 1 has been read (barrier inside tab_issue_stage)
+    if (st + 1 < nstages) load_phase(st + 1);
+    ok = tab_finish_stage<NMAX>(c, n, st == 0, ph_mma, err_flag);
     if (!ok) break;
   }
   if (ok) {
@@ -742,7 +825,7 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
 #pragma unroll 1
       for (int cb = 0; cb < n; cb += 16) {
         float s[16];
-        tab_read_sum(c, acc, cb, s);
+        tab_read_sum<NMAX>(c, acc, cb, s);
         if (!in) continue;
         // columns come in (re, im) pairs of one complex value only when gs is even; write parts one by one
 #pragma unroll
@@ -758,8 +841,11 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tab_adj_kernel(const float* __r
         }
       }
     }
+  } else if (threadIdx.x == 0) {
+    for (int k = waited; k < issued; ++k)
+      tc::mbar_wait_bounded(c.mbar_full + 8u * uint32_t(k & 1), uint32_t(k >> 1) & 1u, TB_WAIT_LIMIT);
   }
-  tab_end(c);
+  tab_end<S>(c);
 }
 
 // ------------------------------------------------------------------ host side
@@ -811,9 +897,9 @@ int launch_tab_gen(const Plan& P, int spin, const int64_t* d_blockoff, float* ta
   return PS_OK;
 }
 
-// maps per group: as many as fit the 64 columns, spread evenly over the groups
-static int tab_group_size(int B, int spin, int& ngroups) {
-  const int cap = spin == 0 ? TB_NMAX / 2 : TB_NMAX / 4;
+// maps per group: as many as fit the nmax columns of an accumulator, spread evenly over the groups
+static int tab_group_size(int B, int spin, int nmax, int& ngroups) {
+  const int cap = spin == 0 ? nmax / 2 : nmax / 4;
   ngroups = (B + cap - 1) / cap;
   return (B + ngroups - 1) / ngroups;
 }
@@ -826,23 +912,27 @@ int launch_tab_synth(const Plan& P, const float* table, const int64_t* d_blockof
   const double bytes = double(tab_bytes(Rh_table, P.lmax, P.mmax, spin)) * double(P.Rh) / double(Rh_table) +
                        double(B) * (spin == 0 ? 1 : 2) * (16.0 * P.nalm + 8.0 * P.R * (P.mmax + 1));
   StatScope sc(PS_K_LEG_SYNTH, flops, bytes, st);
+  // 128 columns per accumulator for spin 0 (up to 64 maps per pass over the table), 64 for spin s
+  // (16 maps; its staged tiles are twice as large, which leaves shared memory for no more)
+  const int nmax = spin == 0 ? 128 : 64;
   int ngroups = 1;
-  const int gsize = tab_group_size(B, spin, ngroups);
+  const int gsize = tab_group_size(B, spin, nmax, ngroups);
   const int ntiles = ((toff & 3) + P.Rh + TB_TILE - 1) / TB_TILE;
   const int nquads = tab_quads(Rh_table);
   const int64_t nblk = int64_t(ngroups) * ntiles * (P.mmax + 1);
   if (nblk > 0x7fffffff) return PS_ERR_UNSUPPORTED;
-  const int smem = int(TabSmem::DYN);
   if (spin == 0) {
-    if (set_smem_attr((const void*)tab_synth_kernel<1>, smem)) return PS_ERR_CUDA;
-    tab_synth_kernel<1><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
-                                                                  P.mmax, almT, phase, B, gsize, ngroups, ntiles, 0,
-                                                                  err_flag);
+    const int smem = int(TabSmem<128, SynthStg<1>::BYTES>::DYN);
+    if (set_smem_attr((const void*)tab_synth_kernel<1, 128>, smem)) return PS_ERR_CUDA;
+    tab_synth_kernel<1, 128><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+                                                                       P.mmax, almT, phase, B, gsize, ngroups, ntiles,
+                                                                       0, err_flag);
   } else {
-    if (set_smem_attr((const void*)tab_synth_kernel<2>, smem)) return PS_ERR_CUDA;
-    tab_synth_kernel<2><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
-                                                                  P.mmax, almT, phase, B, gsize, ngroups, ntiles,
-                                                                  spin & 1, err_flag);
+    const int smem = int(TabSmem<64, SynthStg<2>::BYTES>::DYN);
+    if (set_smem_attr((const void*)tab_synth_kernel<2, 64>, smem)) return PS_ERR_CUDA;
+    tab_synth_kernel<2, 64><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+                                                                      P.mmax, almT, phase, B, gsize, ngroups, ntiles,
+                                                                      spin & 1, err_flag);
   }
   PS_LAUNCH_CHECK();
   return PS_OK;
@@ -864,23 +954,26 @@ int launch_tab_adj(const Plan& P, const float* table, const int64_t* d_blockoff,
   const double bytes = double(tab_bytes(Rh_table, P.lmax, P.mmax, spin)) * double(P.Rh) / double(Rh_table) +
                        double(B) * (spin == 0 ? 1 : 2) * (16.0 * P.nalm + 8.0 * P.R * (P.mmax + 1));
   StatScope sc(PS_K_LEG_ADJOINT, flops, bytes, st);
+  // 128 columns per accumulator: up to 64 maps of spin 0 or 32 of spin s per pass over the table
+  constexpr int nmax = 128;
   int ngroups = 1;
-  const int gsize = tab_group_size(B, spin, ngroups);
+  const int gsize = tab_group_size(B, spin, nmax, ngroups);
   const int nquads = tab_quads(Rh_table);
   const int64_t nblk = int64_t(ngroups) * nwork;
   if (nblk > 0x7fffffff) return PS_ERR_UNSUPPORTED;
-  const int smem = int(TabSmem::DYN);
   if (spin == 0) {
-    if (set_smem_attr((const void*)tab_adj_kernel<1>, smem)) return PS_ERR_CUDA;
-    tab_adj_kernel<1><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
-                                                                P.mmax, phase, alm, B, gsize, ngroups, d_work,
-                                                                P.nalm, scale, 0, out_stride, lscale, err_flag);
+    const int smem = int(TabSmem<nmax, AdjStg<1>::BYTES>::DYN);
+    if (set_smem_attr((const void*)tab_adj_kernel<1, nmax>, smem)) return PS_ERR_CUDA;
+    tab_adj_kernel<1, nmax><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+                                                                      P.mmax, phase, alm, B, gsize, ngroups, d_work,
+                                                                      P.nalm, scale, 0, out_stride, lscale, err_flag);
   } else {
-    if (set_smem_attr((const void*)tab_adj_kernel<2>, smem)) return PS_ERR_CUDA;
-    tab_adj_kernel<2><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
-                                                                P.mmax, phase, alm, B, gsize, ngroups, d_work,
-                                                                P.nalm, scale, spin & 1, out_stride, lscale,
-                                                                err_flag);
+    const int smem = int(TabSmem<nmax, AdjStg<2>::BYTES>::DYN);
+    if (set_smem_attr((const void*)tab_adj_kernel<2, nmax>, smem)) return PS_ERR_CUDA;
+    tab_adj_kernel<2, nmax><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+                                                                      P.mmax, phase, alm, B, gsize, ngroups, d_work,
+                                                                      P.nalm, scale, spin & 1, out_stride, lscale,
+                                                                      err_flag);
   }
   PS_LAUNCH_CHECK();
   return PS_OK;

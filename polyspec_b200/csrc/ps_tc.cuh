@@ -33,6 +33,20 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 __device__ __forceinline__ void mbar_init(uint32_t saddr, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr), "r"(count));
 }
+// make mbarrier initialisations visible to the async proxy (bulk copies complete on them)
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// one arrival that also announces `bytes` of bulk-copy transactions on the barrier
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t saddr, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr), "r"(bytes) : "memory");
+}
+// bulk copy global -> this CTA's shared memory (addresses 16-byte aligned, bytes a multiple of 16),
+// completing `bytes` transactions on the mbarrier
+__device__ __forceinline__ void bulk_g2s(uint32_t dst_saddr, const void* src, uint32_t bytes, uint32_t mbar_saddr) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_saddr),
+      "l"(src), "r"(bytes), "r"(mbar_saddr)
+      : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint32_t saddr, uint32_t parity) {
   uint32_t ok;
   asm volatile(
