@@ -7,8 +7,8 @@
 // the order in which the two GEMMs below consume them.  Each transform then
 // streams the table instead of re-running the recurrence for every group of
 // maps: at Nside 1024, lmax 2048 the spin-0 table is 17.7 GB and the spin-s
-// table (F+ and F-) 35.4 GB, read once per transform of up to 32 (spin 0) or
-// 16 (spin s) maps per map group.
+// table (F+ and F-) 35.4 GB, read once per map group of a transform (up to
+// 64 maps of spin 0, 16 (synthesis) or 32 (adjoint) of spin s).
 //
 // Table layout.  For each order m the l range [m, lmax] is cut into blocks of
 // 64 consecutive l; inside a block the 64 positions are sorted by parity of
@@ -25,12 +25,20 @@
 // per K step (hi.hi + hi.lo + lo.hi).  The tensor core's FP32 accumulation
 // truncates, so the accumulator D is restarted for every stage of 32 K values
 // and added into a running sum S that also lives in TMEM (round-to-nearest
-// FP32 adds by the four epilogue warps).  TMEM: D[2 accumulators][64 columns]
-// and S[2][64], 256 columns per CTA, two CTAs per SM.
+// FP32 adds by the drain warps).  TMEM: D[2 accumulators][128 columns] and
+// S[2][128], all 512 columns of the SM: one CTA of 16 warps per SM, the four
+// warps that share a TMEM lane quarter splitting the columns between them.
 //
 // Columns of D are (part, map) with the part index outermost: spin 0
 // (re, im) of the complex value, spin s four real parts; map group g of up
-// to 32 (spin 0) or 16 (spin s) maps.  N = the used columns rounded up to 16.
+// to 64 (spin 0) or 16 / 32 (spin s synthesis / adjoint) maps.  N = the used
+// columns rounded up to 16.
+//
+// Staging.  The table tiles of the next two stages (and, in the spin-s
+// adjoint, the phase rows of the stage's rings) are fetched by bulk copies
+// (cp.async.bulk with mbarrier transaction counts) into two shared buffers
+// while the current stage is split and multiplied; the a_lm (synthesis) and
+// spin-0 phases (adjoint) of the next stage are loaded into registers.
 //
 // Synthesis (alm -> ring phases), CTA = (map group, ring tile of 128 ring
 // pairs, m): M = ring pairs, K = l, two accumulators.  Spin 0: accumulator p
@@ -63,7 +71,8 @@ namespace ps {
 
 constexpr int TB_LB = 64;        // l per table block
 constexpr int TB_TILE = 128;     // ring pairs per synthesis tile (MMA M)
-constexpr int TB_THREADS = 128;
+constexpr int TB_THREADS = 128;  // table generation
+constexpr int TM_THREADS = 512;  // the two GEMMs: 16 warps, 4 per TMEM lane quarter
 constexpr uint32_t TB_WAIT_LIMIT = 1u << 24;
 
 // ------------------------------------------------------------------ table geometry
@@ -301,28 +310,25 @@ __device__ __forceinline__ void tab_issue(uint32_t sbase, uint32_t tmem, uint32_
   }
 }
 
-// S += D for this thread's TMEM lane (first stage: S = D), columns [0, n) of both accumulators;
-// the four loads of a column chunk (D and S of both accumulators) share one wait
+// S += D for this thread's TMEM lane (first stage: S = D), columns [0, n) of both accumulators.
+// Unit u = (16-column chunk u >> 1, accumulator u & 1); the TM_THREADS / 128 warps that share a TMEM
+// lane quarter take every fourth unit; the loads of D and S of a unit share one wait
 template <int NMAX>
 __device__ __forceinline__ void tab_drain(uint32_t lane_addr, int n, bool first) {
+  const int nu = n >> 3;
 #pragma unroll 1
-  for (int cb = 0; cb < n; cb += 16) {
-    float d0[16], d1[16], s0[16], s1[16];
-    const uint32_t dc0 = lane_addr + uint32_t(cb), dc1 = lane_addr + uint32_t(NMAX + cb);
-    const uint32_t sc0 = lane_addr + uint32_t(2 * NMAX + cb), sc1 = lane_addr + uint32_t(3 * NMAX + cb);
-    tc::tmem_ld16(dc0, d0);
-    tc::tmem_ld16(dc1, d1);
-    if (!first) {
-      tc::tmem_ld16(sc0, s0);
-      tc::tmem_ld16(sc1, s1);
-    }
+  for (int u = int(threadIdx.x >> 7); u < nu; u += TM_THREADS / 128) {
+    float d[16], s[16];
+    const uint32_t dc = lane_addr + uint32_t((u & 1) * NMAX + 16 * (u >> 1));
+    const uint32_t sc = dc + uint32_t(2 * NMAX);
+    tc::tmem_ld16(dc, d);
+    if (!first) tc::tmem_ld16(sc, s);
     tc::tmem_ld_wait();
     if (!first) {
 #pragma unroll
-      for (int q = 0; q < 16; ++q) { d0[q] += s0[q]; d1[q] += s1[q]; }
+      for (int q = 0; q < 16; ++q) d[q] += s[q];
     }
-    tmem_st16(sc0, d0);
-    tmem_st16(sc1, d1);
+    tmem_st16(sc, d);
   }
   tmem_st_wait();
 }
@@ -356,7 +362,7 @@ __device__ __forceinline__ bool tab_finish_stage(const TabCta& c, int n, bool fi
   }
   phase ^= 1u;
   tc::fence_after_sync();
-  const uint32_t lane_addr = c.tmem + (uint32_t((threadIdx.x >> 5) * 32) << 16);
+  const uint32_t lane_addr = c.tmem + (uint32_t(((threadIdx.x >> 5) & 3) * 32) << 16);
   tab_drain<NMAX>(lane_addr, n, first);
   tc::fence_before_sync();
   __syncthreads();
@@ -373,7 +379,7 @@ __device__ __forceinline__ void tab_end(const TabCta& c) {
 // the S columns [cb, cb + 16) of accumulator acc of this thread's lane
 template <int NMAX>
 __device__ __forceinline__ void tab_read_sum(const TabCta& c, int acc, int cb, float* v) {
-  const uint32_t lane_addr = c.tmem + (uint32_t((threadIdx.x >> 5) * 32) << 16);
+  const uint32_t lane_addr = c.tmem + (uint32_t(((threadIdx.x >> 5) & 3) * 32) << 16);
   tc::tmem_ld16(lane_addr + uint32_t(2 * NMAX + acc * NMAX + cb), v);
   tc::tmem_ld_wait();
 }
@@ -392,10 +398,11 @@ struct SynthStg {
 // ------------------------------------------------------------------ synthesis
 // almT [nalm][B][NOPS] complex128 -> phase [R][mmax+1][B][NOPS] complex64 of the ring pairs
 // [0, nrp) (table rings toff + i; north row i, south row R - 1 - i, R = 2 nrp - 1).
-// grid.x = map group + G * (ring tile + T * m).  One CTA per SM: the table tiles of the next two
-// blocks are in flight (bulk copies into the staging buffers) while a stage is split and multiplied.
+// grid.x = map group + G * (ring tile + T * m).  One CTA of 16 warps per SM: the table tiles of
+// the next two blocks are in flight (bulk copies into the staging buffers) while a stage is split
+// and multiplied; every thread has one operand task per stage.
 template <int NOPS, int NMAX>
-__global__ void __launch_bounds__(TB_THREADS, 1) tab_synth_kernel(const float* __restrict__ table,
+__global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* __restrict__ table,
                                                                    const int64_t* __restrict__ blockoff, int nquads,
                                                                    int toff, int nrp, int lmax, int mmax,
                                                                    const double2* __restrict__ almT,
@@ -424,52 +431,81 @@ __global__ void __launch_bounds__(TB_THREADS, 1) tab_synth_kernel(const float* _
   const int nhalf = NOPS == 1 ? 1 : 2;  // stages per table block
   const int nst = nb * nhalf;
   const int nvq = max(0, min(32, nquads - q0));  // units of the tile inside the table
-  // bulk copies of block b's tile into staging buffer b & 1 (thread 0)
   int issued = 0, waited = 0;  // blocks whose copies were issued / whose buffer wait completed (all threads)
+  // bulk copies of block b's tile into staging buffer b & 1 (warp 0: lane q copies unit q)
   auto issue_block = [&](int b) {
     if (b >= nb) return;
     issued = b + 1;
-    if (threadIdx.x != 0) return;
+    if (warp != 0) return;
     const uint32_t bar = c.mbar_full + 8u * uint32_t(b & 1);
-    tc::mbar_arrive_expect_tx(bar, uint32_t(nvq) * UNIT * 4u);
-    const float* src = table + ((blockoff[m] + b) * int64_t(nquads) + q0) * UNIT;
-    const uint32_t dst = c.sbase + S::stg(b & 1);
-    for (int q = 0; q < nvq; ++q) tc::bulk_g2s(dst + uint32_t(q) * G::USTR * 4u, src + int64_t(q) * UNIT, UNIT * 4u, bar);
+    if (lane == 0) tc::mbar_arrive_expect_tx(bar, uint32_t(nvq) * UNIT * 4u);
+    __syncwarp();  // the transaction count is expected before any unit lands
+    if (lane < nvq) {
+      const float* src = table + ((blockoff[m] + b) * int64_t(nquads) + q0 + lane) * UNIT;
+      tc::bulk_g2s(c.sbase + S::stg(b & 1) + uint32_t(lane) * G::USTR * 4u, src, UNIT * 4u, bar);
+    }
   };
-  // alm of one stage in registers (FP32), loaded a stage ahead.  spin 0: tasks t = tid + 128 i2
-  // (map j = t % gs, (acc, k4) = t / gs; 16 gs <= 8 NMAX tasks) x 4 l; spin s: 2 tasks (map
-  // lane & 15) x 4 l x (G, C)
-  constexpr int BTS = NOPS == 1 ? (NMAX / 2) * 16 / TB_THREADS : 4;
-  float2 ab[BTS][4];
+  // ---- this thread's A task (the same every stage): warp = task (K chunk and accumulator), lane = quad
+  int a_acc, a_pos0, a_comp;
+  {
+    const int t = warp;
+    if (NOPS == 1) {
+      a_acc = t >> 3; a_pos0 = a_acc * 32 + 4 * (t & 7); a_comp = 0;
+    } else {
+      a_comp = t >> 3;
+      const int par = (t >> 2) & 1, g4 = t & 3;
+      a_acc = a_comp == 0 ? par : 1 - par;
+      a_pos0 = par * 32 + 4 * g4;  // + 16 h
+    }
+  }
+  const int a_kk = NOPS == 1 ? 4 * (warp & 7) : 16 * (warp >> 3) + 4 * (warp & 3);
+  const uint32_t a_oh = S::a(a_acc, a_kk >> 3, 0), a_ol = S::a(a_acc, a_kk >> 3, 1);
+  const int a_kc = (a_kk >> 2) & 1;
+  bool a_in[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int rt = 4 * (q0 + lane) + i;
+    a_in[i] = rt >= toff && rt < toff + nrp && lane < nvq;
+  }
+  // ---- this thread's B tasks: spin 0: t = tid + 512 i (map j = t % gs, (acc, k4) = t / gs), 16 gs <= 1024;
+  // spin s: t = tid < 256 (map j = t & 15, (acc, k4) = t >> 4)
+  constexpr int BTS = NOPS == 1 ? 2 : 1;
+  int b_j[BTS], b_acc[BTS], b_k4[BTS], b_lofs[BTS];
+  bool b_v[BTS];
+#pragma unroll
+  for (int i2 = 0; i2 < BTS; ++i2) {
+    const int t = tid + TM_THREADS * i2;
+    if (NOPS == 1) {
+      b_v[i2] = t < 16 * gs;
+      const int j = b_v[i2] ? t % gs : 0, ak = b_v[i2] ? t / gs : 0;
+      b_j[i2] = j; b_acc[i2] = ak >> 3; b_k4[i2] = ak & 7;
+      b_lofs[i2] = 8 * b_k4[i2] + b_acc[i2];  // l = m + 64 b + b_lofs + 2 i
+    } else {
+      const int j = t & 15, ak = (t >> 4) & 15;
+      b_v[i2] = t < 256 && j < gs;
+      b_j[i2] = j; b_acc[i2] = ak >> 3; b_k4[i2] = ak & 7;
+      const int comp = b_k4[i2] >> 2, g4 = b_k4[i2] & 3, par = comp == 0 ? b_acc[i2] : 1 - b_acc[i2];
+      b_lofs[i2] = 2 * 4 * g4 + par;  // l = m + 64 b + 32 h + b_lofs + 2 i
+    }
+  }
+  // alm of one stage in registers (FP32), loaded a stage ahead: spin 0 (re, im) of 4 l per task,
+  // spin s G and C of 4 l
+  float2 ab[BTS][2][4];
   auto load_alm = [&](int st) {
     const int b = st / nhalf, h = st % nhalf;
-    if (NOPS == 1) {
 #pragma unroll
-      for (int i2 = 0; i2 < BTS; ++i2) {
-        const int t = tid + TB_THREADS * i2;
-        const bool tv = t < 16 * gs;
-        const int j = tv ? t % gs : 0, ak = tv ? t / gs : 0, acc = ak >> 3, k4 = ak & 7;
+    for (int i2 = 0; i2 < BTS; ++i2) {
+      const int l0 = m + TB_LB * b + 32 * h + b_lofs[i2];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int l = tab_l(m, b, acc * 32 + 4 * k4 + i);
-          const double2 a = (tv && l <= lmax) ? almT[(base + (l - m)) * B + b0 + j] : make_double2(0.0, 0.0);
-          ab[i2][i] = make_float2(float(a.x), float(a.y));
-        }
-      }
-    } else {
-      const int j = lane & 15;
-#pragma unroll
-      for (int i2 = 0; i2 < 2; ++i2) {
-        const int t = warp * 2 + (lane >> 4) + 8 * i2, acc = t >> 3, k4 = t & 7;
-        const int comp = k4 >> 2, g4 = k4 & 3, par = comp == 0 ? acc : 1 - acc;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int l = tab_l(m, b, par * 32 + 16 * h + 4 * g4 + i);
-          const bool v = j < gs && l <= lmax;
-          const int64_t o = ((base + (l - m)) * B + b0 + j) * 2;
-          const double2 Gv = v ? almT[o] : make_double2(0.0, 0.0), Cv = v ? almT[o + 1] : make_double2(0.0, 0.0);
-          ab[2 * i2][i] = make_float2(float(Gv.x), float(Gv.y));
-          ab[2 * i2 + 1][i] = make_float2(float(Cv.x), float(Cv.y));
+      for (int i = 0; i < 4; ++i) {
+        const int l = l0 + 2 * i;
+        const bool v = b_v[i2] && l <= lmax;
+        const int64_t o = ((base + (l - m)) * B + b0 + b_j[i2]) * NCOMP;
+        const double2 x0 = v ? almT[o] : make_double2(0.0, 0.0);
+        ab[i2][0][i] = make_float2(float(x0.x), float(x0.y));
+        if (NOPS == 2) {
+          const double2 x1 = v ? almT[o + 1] : make_double2(0.0, 0.0);
+          ab[i2][1][i] = make_float2(float(x1.x), float(x1.y));
         }
       }
     }
@@ -477,78 +513,51 @@ __global__ void __launch_bounds__(TB_THREADS, 1) tab_synth_kernel(const float* _
   // split and store the operands of stage st: A from the staged table tile, B from the registers
   auto store = [&](int st) {
     const int b = st / nhalf, h = st % nhalf;
-    const float* stg = reinterpret_cast<const float*>(c.smem + S::stg(b & 1));
-#pragma unroll
-    for (int it = 0; it < 4; ++it) {
-      const int t = warp + 4 * it;
-      int acc, kk, pos0, comp;
-      if (NOPS == 1) {
-        acc = t >> 3; kk = 4 * (t & 7); pos0 = acc * 32 + kk; comp = 0;
-      } else {
-        comp = t >> 3;
-        const int par = (t >> 2) & 1, g4 = t & 3;
-        acc = comp == 0 ? par : 1 - par;
-        kk = 16 * comp + 4 * g4;
-        pos0 = par * 32 + 16 * h + 4 * g4;
-      }
-      const float* u = stg + lane * G::USTR + (comp * TB_LB + pos0) * 4;
+    {
+      const float* stg = reinterpret_cast<const float*>(c.smem + S::stg(b & 1));
+      const float* u = stg + lane * G::USTR + (a_comp * TB_LB + a_pos0 + 16 * h) * 4;
       float4 v[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) v[i] = reinterpret_cast<const float4*>(u)[i];
-      const int ks = kk >> 3, kc = (kk >> 2) & 1;
-      const uint32_t oh = S::a(acc, ks, 0), ol = S::a(acc, ks, 1);
-      // ring 4 lane + i of the tile -> A row 32 i + lane; rings outside [toff, toff + nrp) (and units
-      // beyond the table) are zero
-      const int rg0 = 4 * (q0 + lane);
+      // ring 4 lane + i of the tile -> A row 32 i + lane; rings outside [toff, toff + nrp) are zero
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        const int rt = rg0 + i;
-        const bool in = rt >= toff && rt < toff + nrp && lane < nvq;
         float4 w;
-        w.x = in ? (&v[0].x)[i] : 0.f;
-        w.y = in ? (&v[1].x)[i] : 0.f;
-        w.z = in ? (&v[2].x)[i] : 0.f;
-        w.w = in ? (&v[3].x)[i] : 0.f;
-        const uint32_t co = kcore_off(32 * i + lane, kc);
-        st_split(c.smem, oh + co, ol + co, w);
+        w.x = a_in[i] ? (&v[0].x)[i] : 0.f;
+        w.y = a_in[i] ? (&v[1].x)[i] : 0.f;
+        w.z = a_in[i] ? (&v[2].x)[i] : 0.f;
+        w.w = a_in[i] ? (&v[3].x)[i] : 0.f;
+        const uint32_t co = kcore_off(32 * i + lane, a_kc);
+        st_split(c.smem, a_oh + co, a_ol + co, w);
       }
     }
-    if (NOPS == 1) {
 #pragma unroll
-      for (int i2 = 0; i2 < BTS; ++i2) {
-        const int t = tid + TB_THREADS * i2;
-        if (t >= 16 * gs) continue;
-        const int j = t % gs, ak = t / gs, acc = ak >> 3, k4 = ak & 7;
-        const float4 re = make_float4(ab[i2][0].x, ab[i2][1].x, ab[i2][2].x, ab[i2][3].x);
-        const float4 im = make_float4(ab[i2][0].y, ab[i2][1].y, ab[i2][2].y, ab[i2][3].y);
-        const int ks = k4 >> 1, kc = k4 & 1;
+    for (int i2 = 0; i2 < BTS; ++i2) {
+      if (!b_v[i2]) continue;
+      const int j = b_j[i2], acc = b_acc[i2], k4 = b_k4[i2];
+      const int ks = k4 >> 1, kc = k4 & 1;
+      if (NOPS == 1) {
+        const float4 re = make_float4(ab[i2][0][0].x, ab[i2][0][1].x, ab[i2][0][2].x, ab[i2][0][3].x);
+        const float4 im = make_float4(ab[i2][0][0].y, ab[i2][0][1].y, ab[i2][0][2].y, ab[i2][0][3].y);
         st_split(c.smem, S::b(acc, ks, 0) + kcore_off(j, kc), S::b(acc, ks, 1) + kcore_off(j, kc), re);
         st_split(c.smem, S::b(acc, ks, 0) + kcore_off(gs + j, kc), S::b(acc, ks, 1) + kcore_off(gs + j, kc), im);
-      }
-    } else {
-      // F+ rows take X = -(G, C) (even spin) or Y = (C.im, -C.re, -G.im, G.re); F- rows the other one
-      const int j = lane & 15;
-      if (j < gs) {
+      } else {
+        // F+ rows take X = -(G, C) (even spin) or Y = (C.im, -C.re, -G.im, G.re); F- rows the other one
+        const int comp = k4 >> 2;
+        const bool use_x = (comp == 0) != (spin_odd != 0);
+        float4 pt[4];
 #pragma unroll
-        for (int i2 = 0; i2 < 2; ++i2) {
-          const int t = warp * 2 + (lane >> 4) + 8 * i2, acc = t >> 3, k4 = t & 7;
-          const int comp = k4 >> 2;
-          const bool use_x = (comp == 0) != (spin_odd != 0);
-          float4 pt[4];
+        for (int i = 0; i < 4; ++i) {
+          const float2 Gv = ab[i2][0][i], Cv = ab[i2][1][i];
+          float p0, p1, p2, p3;
+          if (use_x) { p0 = -Gv.x; p1 = -Gv.y; p2 = -Cv.x; p3 = -Cv.y; }
+          else { p0 = Cv.y; p1 = -Cv.x; p2 = -Gv.y; p3 = Gv.x; }
+          (&pt[0].x)[i] = p0; (&pt[1].x)[i] = p1; (&pt[2].x)[i] = p2; (&pt[3].x)[i] = p3;
+        }
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const float2 Gv = ab[2 * i2][i], Cv = ab[2 * i2 + 1][i];
-            float p0, p1, p2, p3;
-            if (use_x) { p0 = -Gv.x; p1 = -Gv.y; p2 = -Cv.x; p3 = -Cv.y; }
-            else { p0 = Cv.y; p1 = -Cv.x; p2 = -Gv.y; p3 = Gv.x; }
-            (&pt[0].x)[i] = p0; (&pt[1].x)[i] = p1; (&pt[2].x)[i] = p2; (&pt[3].x)[i] = p3;
-          }
-          const int kk = 4 * k4, ks = kk >> 3, kc = (kk >> 2) & 1;
-#pragma unroll
-          for (int part = 0; part < 4; ++part) {
-            const int row = part * gs + j;
-            st_split(c.smem, S::b(acc, ks, 0) + kcore_off(row, kc), S::b(acc, ks, 1) + kcore_off(row, kc), pt[part]);
-          }
+        for (int part = 0; part < 4; ++part) {
+          const int row = part * gs + j;
+          st_split(c.smem, S::b(acc, ks, 0) + kcore_off(row, kc), S::b(acc, ks, 1) + kcore_off(row, kc), pt[part]);
         }
       }
     }
@@ -576,31 +585,42 @@ __global__ void __launch_bounds__(TB_THREADS, 1) tab_synth_kernel(const float* _
     if (!ok) break;
   }
   if (ok) {
-    // epilogue: TMEM lane 32 w + q <-> ring 4 q + w of the tile
-    const int rt = 4 * (q0 + lane) + warp;  // table ring
-    const int i = rt - toff;                // ring pair of the plan
-    const bool in = rt >= toff && i < nrp;
-    const int R = 2 * nrp - 1;
-    const int rs = R - 1 - i;
+    // epilogue.  TMEM lane tl = 32 lq + q <-> ring 4 q + lq of the tile (lq = warp & 3).  The sums go
+    // through shared memory (free now: every MMA and copy has completed) as rows [north/south][tl]
+    // [map][part], then every ring's row of gs maps is written with coalesced stores
+    constexpr int RS = NMAX + 1;  // row stride (floats): consecutive lanes in consecutive banks
+    static_assert(2 * 128 * RS * 4 <= int(S::MISC_OFF), "epilogue rows exceed the free shared memory");
+    float* rows = reinterpret_cast<float*>(c.smem);
+    const int lq = warp & 3, cs = warp >> 2;
+    const int tl = 32 * lq + lane;
 #pragma unroll 1
-    for (int cb = 0; cb < n; cb += 16) {
+    for (int cb = 16 * cs; cb < n; cb += 64) {
       float s0[16], s1[16];
       tab_read_sum<NMAX>(c, 0, cb, s0);
       tab_read_sum<NMAX>(c, 1, cb, s1);
-      if (!in) continue;
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         const int col = cb + q;
         if (col >= ncols) break;
         const int part = col / gs, j = col % gs;
-        const float nv = s0[q] + s1[q], sv = s0[q] - s1[q];
-        float* pn = reinterpret_cast<float*>(phase + ((int64_t(i) * (mmax + 1) + m) * B + b0 + j) * NCOMP) + part;
-        *pn = nv;
-        if (rs != i) {
-          float* ps_ = reinterpret_cast<float*>(phase + ((int64_t(rs) * (mmax + 1) + m) * B + b0 + j) * NCOMP) + part;
-          *ps_ = sv;
-        }
+        const int pos = j * 2 * NCOMP + part;
+        rows[tl * RS + pos] = s0[q] + s1[q];
+        rows[(128 + tl) * RS + pos] = s0[q] - s1[q];
       }
+    }
+    __syncthreads();
+    const int R = 2 * nrp - 1;
+#pragma unroll 1
+    for (int row = warp; row < 256; row += TM_THREADS / 32) {
+      const int ns = row >> 7, t = row & 127;
+      const int rt = 4 * q0 + 4 * (t & 31) + (t >> 5);  // table ring of TMEM lane t
+      const int i = rt - toff;                          // ring pair of the plan
+      if (rt < toff || i >= nrp) continue;
+      const int ring = ns == 0 ? i : R - 1 - i;
+      if (ns == 1 && ring == i) continue;  // the equator has no south ring
+      float* dst = reinterpret_cast<float*>(phase + ((int64_t(ring) * (mmax + 1) + m) * B + b0) * NCOMP);
+      const float* src = rows + row * RS;
+      for (int pos = lane; pos < ncols; pos += 32) dst[pos] = src[pos];
     }
   } else if (threadIdx.x == 0) {
     // bulk copies still in flight land in this CTA's shared memory: wait for them (bounded) before exit
@@ -611,12 +631,17 @@ __global__ void __launch_bounds__(TB_THREADS, 1) tab_synth_kernel(const float* _
 }
 
 // raw table tile of one adjoint stage: for each of the 4 blocks, the RSTAGE / 4 consecutive units
+// (spin s: followed by the phases of the stage's rings, [north/south][ring][map] complex64 pairs
+// with a row stride of PH_MAPS maps)
 template <int NOPS>
 struct AdjStg {
   static constexpr int UNIT = NOPS * TB_LB * 4;
   static constexpr int NQ = NOPS == 1 ? 8 : 4;  // quads per stage
   static constexpr uint32_t BLK_BYTES = uint32_t(NQ) * UNIT * 4u;
-  static constexpr uint32_t BYTES = 4u * BLK_BYTES;
+  static constexpr uint32_t TAB_BYTES = 4u * BLK_BYTES;
+  static constexpr int PH_MAPS = 32;  // maps per group (spin s)
+  static constexpr uint32_t PH_BYTES = NOPS == 2 ? 2u * 4u * NQ * PH_MAPS * 16u : 0u;
+  static constexpr uint32_t BYTES = TAB_BYTES + PH_BYTES;
 };
 
 // ------------------------------------------------------------------ adjoint
@@ -624,7 +649,7 @@ struct AdjStg {
 // ([NOPS][nalm] complex128, times scale and lscale[comp][idx] when given), for the maps [b0, b0 + gs)
 // of each group.  grid.x = map group + G * (entry of the (m, first block) work list)
 template <int NOPS, int NMAX>
-__global__ void __launch_bounds__(TB_THREADS, 1) tab_adj_kernel(const float* __restrict__ table,
+__global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __restrict__ table,
                                                                  const int64_t* __restrict__ blockoff, int nquads,
                                                                  int toff, int nrp, int lmax, int mmax,
                                                                  const float2* __restrict__ phase,
@@ -656,60 +681,81 @@ __global__ void __launch_bounds__(TB_THREADS, 1) tab_adj_kernel(const float* __r
   const int R = 2 * nrp - 1;
   const int rt_begin = toff & ~3, rt_end = toff + nrp;
   const int nstages = (rt_end - rt_begin + RSTAGE - 1) / RSTAGE;
-  // bulk copies of stage st's units into staging buffer st & 1 (thread 0)
   int issued = 0, waited = 0;  // stages whose copies were issued / whose buffer wait completed (all threads)
+  // bulk copies of stage st's units into staging buffer st & 1 (thread 0)
+  // bulk copies of stage st's units (and, spin s, of its phase rows) into staging buffer st & 1
+  // (warp 0: lane 0 the table units, lane r the phase rows of ring r of the stage)
   auto issue_stage_copy = [&](int st) {
     if (st >= nstages) return;
     issued = st + 1;
-    if (threadIdx.x != 0) return;
-    const int qs = (rt_begin + st * RSTAGE) / 4;
+    if (warp != 0) return;
+    const int rs0 = rt_begin + st * RSTAGE;
+    const int qs = rs0 / 4;
     const int nvq = max(0, min(NQ, nquads - qs));
     int nblk = 0;
     for (int blk = 0; blk < 4; ++blk) nblk += (bb + blk < nb);
+    uint32_t tx = uint32_t(nblk * nvq) * UNIT * 4u;
+    // spin s: ring rs0 + r (r = lane < RSTAGE) has a north row when it is a ring of the plan, and a
+    // south row unless it is the equator
+    const int ip = rs0 + lane - toff;
+    const bool ph_n = NOPS == 2 && lane < RSTAGE && ip >= 0 && ip < nrp;
+    const bool ph_s = ph_n && R - 1 - ip != ip;
+    const uint32_t row_bytes = uint32_t(gs) * 16u;
+    if (NOPS == 2) {
+      uint32_t rows = uint32_t(ph_n) + uint32_t(ph_s);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) rows += __shfl_xor_sync(0xffffffffu, rows, o);
+      tx += rows * row_bytes;
+    }
     const uint32_t bar = c.mbar_full + 8u * uint32_t(st & 1);
-    tc::mbar_arrive_expect_tx(bar, uint32_t(nblk * nvq) * UNIT * 4u);
     const uint32_t dst = c.sbase + S::stg(st & 1);
-    for (int blk = 0; blk < 4; ++blk) {
-      if (bb + blk >= nb || nvq == 0) continue;
-      const float* src = table + ((blockoff[m] + bb + blk) * int64_t(nquads) + qs) * UNIT;
-      tc::bulk_g2s(dst + uint32_t(blk) * G::BLK_BYTES, src, uint32_t(nvq) * UNIT * 4u, bar);
+    if (lane == 0) {
+      tc::mbar_arrive_expect_tx(bar, tx);
+      for (int blk = 0; blk < 4; ++blk) {
+        if (bb + blk >= nb || nvq == 0) continue;
+        const float* src = table + ((blockoff[m] + bb + blk) * int64_t(nquads) + qs) * UNIT;
+        tc::bulk_g2s(dst + uint32_t(blk) * G::BLK_BYTES, src, uint32_t(nvq) * UNIT * 4u, bar);
+      }
+    }
+    if (NOPS == 2) {
+      __syncwarp();  // the transaction count is expected before any phase row lands
+      const uint32_t pd = dst + G::TAB_BYTES + uint32_t(lane) * G::PH_MAPS * 16u;
+      if (ph_n)
+        tc::bulk_g2s(pd, phase + ((int64_t(ip) * (mmax + 1) + m) * B + b0) * NCOMP, row_bytes, bar);
+      if (ph_s)
+        tc::bulk_g2s(pd + uint32_t(RSTAGE) * G::PH_MAPS * 16u,
+                     phase + ((int64_t(R - 1 - ip) * (mmax + 1) + m) * B + b0) * NCOMP, row_bytes, bar);
     }
   };
-  // phases of one stage in registers, loaded a stage ahead: tasks (map j, quad qd) t = tid + 128 i
-  // tasks per thread: NQ quads x up to NMAX / 2 (spin 0) or NMAX / 4 (spin s) maps
-  constexpr int BT = (NQ * (NOPS == 1 ? NMAX / 2 : NMAX / 4) + TB_THREADS - 1) / TB_THREADS;
-  float2 pn[BT][4][NCOMP], pv[BT][4][NCOMP];
+  // ---- A tasks: combination t = warp + 16 it (quad, comp, block, acc), lane = position in the parity half
+  constexpr int NT = 2 * 4 * NOPS * NQ;  // 64
+  constexpr int NA = NT / (TM_THREADS / 32);
+  // ---- B tasks.  spin 0: t = tid (map j = t % gs, quad qd = t / gs), NQ gs <= 512, phases loaded to
+  // registers a stage ahead.  spin s: t = tid (sub = t & 3 -> (acc, comp), map j = (t >> 2) % gs,
+  // quad qd = (t >> 2) / gs), NQ gs <= 128, phases read from the staged rows
+  const int p_t = NOPS == 1 ? tid : tid >> 2;
+  const bool p_v = p_t < NQ * gs;
+  const int p_j = p_v ? p_t % gs : 0, p_qd = p_v ? p_t / gs : 0;
+  float2 pn[4], pv[4];
   auto load_phase = [&](int st) {
+    if (NOPS != 1) return;
     const int rs0 = rt_begin + st * RSTAGE;
 #pragma unroll
-    for (int bi = 0; bi < BT; ++bi) {
-      const int t = tid + TB_THREADS * bi;
-      const bool tv = t < NQ * gs;
-      const int j = tv ? t % gs : 0, qd = tv ? t / gs : 0;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int rt = rs0 + 4 * qd + i;
-        const int ip = rt - toff;
-        const bool in = tv && rt >= toff && ip < nrp;
-        const int rsth = R - 1 - ip;
-#pragma unroll
-        for (int cc = 0; cc < NCOMP; ++cc) {
-          pn[bi][i][cc] = in ? phase[((int64_t(ip) * (mmax + 1) + m) * B + b0 + j) * NCOMP + cc]
-                             : make_float2(0.f, 0.f);
-          pv[bi][i][cc] = (in && rsth != ip) ? phase[((int64_t(rsth) * (mmax + 1) + m) * B + b0 + j) * NCOMP + cc]
-                                             : make_float2(0.f, 0.f);
-        }
-      }
+    for (int i = 0; i < 4; ++i) {
+      const int rt = rs0 + 4 * p_qd + i;
+      const int ip = rt - toff;
+      const bool in = p_v && rt >= toff && ip < nrp;
+      const int rsth = R - 1 - ip;
+      pn[i] = in ? phase[(int64_t(ip) * (mmax + 1) + m) * B + b0 + p_j] : make_float2(0.f, 0.f);
+      pv[i] = (in && rsth != ip) ? phase[(int64_t(rsth) * (mmax + 1) + m) * B + b0 + p_j] : make_float2(0.f, 0.f);
     }
   };
   auto store = [&](int st) {
     const int rs0 = rt_begin + st * RSTAGE;
     const float* stg = reinterpret_cast<const float*>(c.smem + S::stg(st & 1));
-    // A: rows = 32 positions x 4 blocks, K = rings; chunk = float4 (4 rings at one position);
-    // task t = warp + 4 i -> (quad, comp, block, acc), lane = position within the parity half
-    constexpr int NT = 2 * 4 * NOPS * NQ;
-#pragma unroll 4
-    for (int t = warp; t < NT; t += 4) {
+#pragma unroll
+    for (int it = 0; it < NA; ++it) {
+      const int t = warp + (TM_THREADS / 32) * it;
       const int qd = t % NQ;
       int r = t / NQ;
       const int comp = r % NOPS; r /= NOPS;
@@ -735,63 +781,57 @@ __global__ void __launch_bounds__(TB_THREADS, 1) tab_adj_kernel(const float* __r
       const int row = blk * 32 + lane;
       st_split(c.smem, S::a(acc, ks, 0) + kcore_off(row, kc), S::a(acc, ks, 1) + kcore_off(row, kc), v);
     }
+    if (p_v && NOPS == 1) {
+      const int j = p_j, qd = p_qd;
+      // ring sums (combo 0: N + S) and differences (combo 1: N - S) of 4 rings
+      float4 cre[2], cim[2];
 #pragma unroll
-    for (int bi = 0; bi < BT; ++bi) {
-      const int t = tid + TB_THREADS * bi;
-      if (t >= NQ * gs) continue;
-      const int j = t % gs, qd = t / gs;
-      // ring sums (combo 0: N + S) and differences (combo 1: N - S) of 4 rings, per component
-      float4 cre[2][NCOMP], cim[2][NCOMP];
+      for (int i = 0; i < 4; ++i) {
+        (&cre[0].x)[i] = pn[i].x + pv[i].x;
+        (&cim[0].x)[i] = pn[i].y + pv[i].y;
+        (&cre[1].x)[i] = pn[i].x - pv[i].x;
+        (&cim[1].x)[i] = pn[i].y - pv[i].y;
+      }
+      const int kk = 4 * qd, ks = kk >> 3, kc = (kk >> 2) & 1;
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int acc = 0; acc < 2; ++acc) {
+        st_split(c.smem, S::b(acc, ks, 0) + kcore_off(j, kc), S::b(acc, ks, 1) + kcore_off(j, kc), cre[acc]);
+        st_split(c.smem, S::b(acc, ks, 0) + kcore_off(gs + j, kc), S::b(acc, ks, 1) + kcore_off(gs + j, kc),
+                 cim[acc]);
+      }
+    } else if (p_v) {
+      // columns (G.re, G.im, C.re, C.im); combo k (0: N + S, 1: N - S) of the rings' (Q, U):
+      // Xa(k) = (-Q.re, -Q.im, -U.re, -U.im), Ya(k) = (U.im, -U.re, -Q.im, Q.re)
+      // even spin: F+ rows Xa(acc), F- rows Ya(1 - acc); odd spin: F+ rows Ya(acc), F- rows Xa(1 - acc)
+      const int j = p_j, qd = p_qd;
+      const int acc = (tid >> 1) & 1, comp = tid & 1;
+      const int k = comp == 0 ? acc : 1 - acc;
+      const bool use_x = (comp == 0) != (spin_odd != 0);
+      const float4* ph = reinterpret_cast<const float4*>(c.smem + S::stg(st & 1) + G::TAB_BYTES);
+      float4 p[4];
 #pragma unroll
-        for (int cc = 0; cc < NCOMP; ++cc) {
-          const float2 nv = pn[bi][i][cc], sv = pv[bi][i][cc];
-          (&cre[0][cc].x)[i] = nv.x + sv.x;
-          (&cim[0][cc].x)[i] = nv.y + sv.y;
-          (&cre[1][cc].x)[i] = nv.x - sv.x;
-          (&cim[1][cc].x)[i] = nv.y - sv.y;
+      for (int i = 0; i < 4; ++i) {
+        const int r = 4 * qd + i;  // ring of the stage
+        const int ip = rs0 + r - toff;
+        const bool in = ip >= 0 && ip < nrp;
+        const bool hs = in && R - 1 - ip != ip;
+        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 nv = in ? ph[r * G::PH_MAPS + j] : z;
+        const float4 sv = hs ? ph[(RSTAGE + r) * G::PH_MAPS + j] : z;
+        const float4 cv = k == 0 ? make_float4(nv.x + sv.x, nv.y + sv.y, nv.z + sv.z, nv.w + sv.w)
+                                 : make_float4(nv.x - sv.x, nv.y - sv.y, nv.z - sv.z, nv.w - sv.w);
+        // cv = (Q.re, Q.im, U.re, U.im) of ring i
+        if (use_x) {
+          (&p[0].x)[i] = -cv.x; (&p[1].x)[i] = -cv.y; (&p[2].x)[i] = -cv.z; (&p[3].x)[i] = -cv.w;
+        } else {
+          (&p[0].x)[i] = cv.w; (&p[1].x)[i] = -cv.z; (&p[2].x)[i] = -cv.y; (&p[3].x)[i] = cv.x;
         }
-      if (NOPS == 1) {
-        const int kk = 4 * qd, ks = kk >> 3, kc = (kk >> 2) & 1;
+      }
+      const int kk = comp * 16 + 4 * qd, ks = kk >> 3, kc = (kk >> 2) & 1;
 #pragma unroll
-        for (int acc = 0; acc < 2; ++acc) {
-          st_split(c.smem, S::b(acc, ks, 0) + kcore_off(j, kc), S::b(acc, ks, 1) + kcore_off(j, kc), cre[acc][0]);
-          st_split(c.smem, S::b(acc, ks, 0) + kcore_off(gs + j, kc), S::b(acc, ks, 1) + kcore_off(gs + j, kc),
-                   cim[acc][0]);
-        }
-      } else {
-        // columns (G.re, G.im, C.re, C.im); combo k: Q = (cre[k][0], cim[k][0]), U = (cre[k][1], cim[k][1])
-        // Xa(k) = (-Q.re, -Q.im, -U.re, -U.im), Ya(k) = (U.im, -U.re, -Q.im, Q.re)
-        // even spin: F+ rows Xa(acc), F- rows Ya(1 - acc); odd spin: F+ rows Ya(acc), F- rows Xa(1 - acc)
-#pragma unroll
-        for (int acc = 0; acc < 2; ++acc) {
-#pragma unroll
-          for (int comp = 0; comp < 2; ++comp) {
-            const int k = comp == 0 ? acc : 1 - acc;
-            const bool use_x = (comp == 0) != (spin_odd != 0);
-            const float4 qr = cre[k][0], qi = cim[k][0], ur = cre[k][NCOMP - 1], ui = cim[k][NCOMP - 1];
-            float4 p[4];
-            if (use_x) {
-              p[0] = make_float4(-qr.x, -qr.y, -qr.z, -qr.w);
-              p[1] = make_float4(-qi.x, -qi.y, -qi.z, -qi.w);
-              p[2] = make_float4(-ur.x, -ur.y, -ur.z, -ur.w);
-              p[3] = make_float4(-ui.x, -ui.y, -ui.z, -ui.w);
-            } else {
-              p[0] = ui;
-              p[1] = make_float4(-ur.x, -ur.y, -ur.z, -ur.w);
-              p[2] = make_float4(-qi.x, -qi.y, -qi.z, -qi.w);
-              p[3] = qr;
-            }
-            const int kk = comp * 16 + 4 * qd, ks = kk >> 3, kc = (kk >> 2) & 1;
-#pragma unroll
-            for (int part = 0; part < 4; ++part) {
-              const int row = part * gs + j;
-              st_split(c.smem, S::b(acc, ks, 0) + kcore_off(row, kc), S::b(acc, ks, 1) + kcore_off(row, kc),
-                       p[part]);
-            }
-          }
-        }
+      for (int part = 0; part < 4; ++part) {
+        const int row = part * gs + j;
+        st_split(c.smem, S::b(acc, ks, 0) + kcore_off(row, kc), S::b(acc, ks, 1) + kcore_off(row, kc), p[part]);
       }
     }
   };
@@ -814,8 +854,9 @@ __global__ void __launch_bounds__(TB_THREADS, 1) tab_adj_kernel(const float* __r
     if (!ok) break;
   }
   if (ok) {
-    // epilogue: TMEM lane = A row = blk * 32 + j; accumulator acc is l = tab_l(m, bb + blk, acc * 32 + j)
-    const int blk = warp, j = lane;
+    // epilogue: TMEM lane = A row = blk * 32 + j (blk = warp & 3); accumulator acc is
+    // l = tab_l(m, bb + blk, acc * 32 + j); the four warps of a lane quarter take every fourth column chunk
+    const int blk = warp & 3, cs = warp >> 2, j = lane;
     const int b = bb + blk;
 #pragma unroll 1
     for (int acc = 0; acc < 2; ++acc) {
@@ -823,7 +864,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1) tab_adj_kernel(const float* __r
       const bool in = b < nb && l <= lmax;
       const int64_t idx = alm_index(l, m, lmax);
 #pragma unroll 1
-      for (int cb = 0; cb < n; cb += 16) {
+      for (int cb = 16 * cs; cb < n; cb += 64) {
         float s[16];
         tab_read_sum<NMAX>(c, acc, cb, s);
         if (!in) continue;
@@ -924,13 +965,13 @@ int launch_tab_synth(const Plan& P, const float* table, const int64_t* d_blockof
   if (spin == 0) {
     const int smem = int(TabSmem<128, SynthStg<1>::BYTES>::DYN);
     if (set_smem_attr((const void*)tab_synth_kernel<1, 128>, smem)) return PS_ERR_CUDA;
-    tab_synth_kernel<1, 128><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+    tab_synth_kernel<1, 128><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
                                                                        P.mmax, almT, phase, B, gsize, ngroups, ntiles,
                                                                        0, err_flag);
   } else {
     const int smem = int(TabSmem<64, SynthStg<2>::BYTES>::DYN);
     if (set_smem_attr((const void*)tab_synth_kernel<2, 64>, smem)) return PS_ERR_CUDA;
-    tab_synth_kernel<2, 64><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+    tab_synth_kernel<2, 64><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
                                                                       P.mmax, almT, phase, B, gsize, ngroups, ntiles,
                                                                       spin & 1, err_flag);
   }
@@ -961,16 +1002,18 @@ int launch_tab_adj(const Plan& P, const float* table, const int64_t* d_blockoff,
   const int nquads = tab_quads(Rh_table);
   const int64_t nblk = int64_t(ngroups) * nwork;
   if (nblk > 0x7fffffff) return PS_ERR_UNSUPPORTED;
+  // spin s phase rows are staged by bulk copies, which start on 16-byte boundaries
+  if (spin != 0 && (reinterpret_cast<uintptr_t>(phase) & 15u)) return PS_ERR_INVALID;
   if (spin == 0) {
     const int smem = int(TabSmem<nmax, AdjStg<1>::BYTES>::DYN);
     if (set_smem_attr((const void*)tab_adj_kernel<1, nmax>, smem)) return PS_ERR_CUDA;
-    tab_adj_kernel<1, nmax><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+    tab_adj_kernel<1, nmax><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
                                                                       P.mmax, phase, alm, B, gsize, ngroups, d_work,
                                                                       P.nalm, scale, 0, out_stride, lscale, err_flag);
   } else {
     const int smem = int(TabSmem<nmax, AdjStg<2>::BYTES>::DYN);
     if (set_smem_attr((const void*)tab_adj_kernel<2, nmax>, smem)) return PS_ERR_CUDA;
-    tab_adj_kernel<2, nmax><<<unsigned(nblk), TB_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+    tab_adj_kernel<2, nmax><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
                                                                       P.mmax, phase, alm, B, gsize, ngroups, d_work,
                                                                       P.nalm, scale, spin & 1, out_stride, lscale,
                                                                       err_flag);
