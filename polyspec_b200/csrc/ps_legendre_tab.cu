@@ -8,36 +8,38 @@
 // streams the table instead of re-running the recurrence for every group of
 // maps: at Nside 1024, lmax 2048 the spin-0 table is 17.7 GB and the spin-s
 // table (F+ and F-) 35.4 GB, read once per map group of a transform (up to
-// 64 maps of spin 0, 16 (synthesis) or 32 (adjoint) of spin s).
+// 40 maps of spin 0 or 20 of spin s).
 //
 // Table layout.  For each order m the l range [m, lmax] is cut into blocks of
-// 64 consecutive l; inside a block the 64 positions are sorted by parity of
-// l - m: position j < 32 holds l = m + 64b + 2j, position 32 + j holds
-// l = m + 64b + 2j + 1 (zero beyond lmax).  Ring pairs (north ring and its
-// mirror, the equator last) are grouped in quads of 4; one unit
-// (m, block b, quad q) is [ncomp][64 positions][4 rings] FP32 (ncomp 1 for
-// spin 0, 2 for spin s: F+ then F-), and units are stored in the order
-// (m, b, q).  A float4 of a unit is four consecutive rings at one l, which is
-// one 16-byte row of a K-major core matrix of the adjoint's A operand (K =
+// 64 consecutive l.  Position j (0..31) of parity p of block b is
+// l = m + 64b + 2j + p (zero beyond lmax); each block has two halves h, the
+// positions 16h..16h+15 of both parities.  Ring pairs (north ring and its
+// mirror, the equator last) are grouped in quads of 4.  One unit
+// (m, b, h, quad q) is [ncomp][parity][16 positions][4 rings] FP32 (ncomp 1
+// for spin 0, 2 for spin s: F+ then F-), and units are stored in the order
+// (m, b, h, q), so that a synthesis stage (one half block of a 128-ring tile)
+// is 32 runs of one unit.  A float4 of a unit is four consecutive rings at one
+// l: a 16-byte row of a K-major core matrix of the adjoint's A operand (K =
 // rings); the synthesis (K = l) transposes 4 x 4 blocks in registers.
 //
 // Both GEMMs split every FP32 operand into TF32 hi + lo and issue three MMAs
-// per K step (hi.hi + hi.lo + lo.hi).  The tensor core's FP32 accumulation
-// truncates, so the accumulator D is restarted for every stage of 32 K values
-// and added into a running sum S that also lives in TMEM (round-to-nearest
-// FP32 adds by the drain warps).  TMEM: D[2 accumulators][128 columns] and
-// S[2][128], all 512 columns of the SM: one CTA of 16 warps per SM, the four
-// warps that share a TMEM lane quarter splitting the columns between them.
+// per K step (hi.hi + hi.lo + lo.hi).  A stage is 16 K values per
+// accumulator; operand tiles are double-buffered so that the MMAs of a stage
+// run while the next stage is split.  The tensor core's FP32 accumulation
+// truncates, so the accumulator D is restarted every two stages (32 K
+// values) and added into a running sum S in TMEM (round-to-nearest FP32 adds
+// by all 16 warps, the four warps of a TMEM lane quarter splitting the
+// columns).  TMEM: D[2 buffers][2 accumulators][80] and S[2][80], so that the
+// drain of one D overlaps the MMAs into the other.  One CTA of 16 warps per
+// SM; one barrier per stage.
 //
 // Columns of D are (part, map) with the part index outermost: spin 0
 // (re, im) of the complex value, spin s four real parts; map group g of up
-// to 64 (spin 0) or 16 / 32 (spin s synthesis / adjoint) maps.  N = the used
-// columns rounded up to 16.
+// to 40 (spin 0) or 20 (spin s) maps.  N = the used columns rounded up to 16.
 //
-// Staging.  The table tiles of the next two stages (and, in the spin-s
-// adjoint, the phase rows of the stage's rings) are fetched by bulk copies
-// (cp.async.bulk with mbarrier transaction counts) into two shared buffers
-// while the current stage is split and multiplied; the a_lm (synthesis) and
+// Staging.  The table tiles (and, in the spin-s adjoint, the phase rows of
+// the stage's rings) of up to four stages ahead are fetched by bulk copies
+// (cp.async.bulk with mbarrier transaction counts); the a_lm (synthesis) and
 // spin-0 phases (adjoint) of the next stage are loaded into registers.
 //
 // Synthesis (alm -> ring phases), CTA = (map group, ring tile of 128 ring
@@ -45,13 +47,12 @@
 // sums the l of parity p; north ring = S0 + S1, south = S0 - S1.  Spin s:
 // W = sum_even F+ u + sum_odd F- v and V = sum_odd F+ u + sum_even F- v (u, v
 // the (Q, U) contributions of (G, C) through F+ and F-); north = W + V,
-// south = W - V.  The A row of ring 4q + i of the tile is 32 i + q, so that
-// the 16-byte stores of eight consecutive lanes (consecutive q) fall into
-// eight different bank groups.
+// south = W - V.  A stage of spin s is 8 positions of F+ (K 0..7) and of F-
+// (K 8..15).
 //
 // Adjoint (ring phases -> alm), CTA = (map group, group of 4 l blocks, m):
 // M = 128 l of one parity (32 positions of each of the 4 blocks), K = rings
-// (32 per stage for spin 0; for spin s 16 rings as F+ rows and the same 16 as
+// (16 per stage for spin 0; for spin s 8 rings as F+ rows and the same 8 as
 // F- rows), two accumulators (parity 0 and 1) against the ring sums N + S
 // and differences N - S.  The output is written straight into the caller's
 // alm (FP64, times scale and an optional per-lm factor): there are no
@@ -78,9 +79,13 @@ constexpr uint32_t TB_WAIT_LIMIT = 1u << 24;
 // ------------------------------------------------------------------ table geometry
 // number of table blocks of order m
 __host__ __device__ __forceinline__ int tab_nblocks(int m, int lmax) { return (lmax - m) / TB_LB + 1; }
-// l of position pos of block b (may exceed lmax)
-__host__ __device__ __forceinline__ int tab_l(int m, int b, int pos) {
-  return m + TB_LB * b + 2 * (pos & 31) + (pos >> 5);
+// l of position j (0..31) of parity par of block b (may exceed lmax)
+__host__ __device__ __forceinline__ int tab_l(int m, int b, int j, int par) { return m + TB_LB * b + 2 * j + par; }
+// floats per unit (m, b, h, q): [ncomp][2 parities][16 positions][4 rings]
+__host__ __device__ constexpr int tab_unit_floats(int ncomp) { return ncomp * 2 * 16 * 4; }
+// unit index of (global block gb = blockoff[m] + b, half h, quad q)
+__host__ __device__ __forceinline__ int64_t tab_unit_index(int64_t gb, int h, int nquads, int q) {
+  return (gb * 2 + h) * int64_t(nquads) + q;
 }
 
 // ------------------------------------------------------------------ recurrence (as the FP64 kernels)
@@ -117,17 +122,17 @@ __device__ __forceinline__ void tab_seedS(int m, int s, const RingInfo& g, SeedN
 }
 
 // One CTA = 128 ring pairs of one order m; thread = ring pair.  Block by block the
-// values go to a padded shared stage [32 quads][unit + 4 floats] and then out to
-// the table as 32 contiguous units.
+// values go to a padded shared stage [2 halves][32 quads][unit + 4 floats] and then
+// out to the table as two runs of 32 contiguous units.
 template <int NOPS>
 __global__ void __launch_bounds__(TB_THREADS) tab_gen_kernel(const RingInfo* __restrict__ rings,
                                                              const double* __restrict__ mnorm,
                                                              const SeedNorm* __restrict__ seednorm, int Rh, int lmax,
                                                              int spin, const int64_t* __restrict__ blockoff,
                                                              int nquads, float* __restrict__ table) {
-  constexpr int UNIT = NOPS * TB_LB * 4;  // floats per unit
-  constexpr int USTR = UNIT + 4;          // padded stride in the stage
-  extern __shared__ __align__(16) float tg_stage[];  // [32][USTR]
+  constexpr int UNIT = tab_unit_floats(NOPS);  // floats per unit
+  constexpr int USTR = UNIT + 4;                // padded stride in the stage
+  extern __shared__ __align__(16) float tg_stage[];  // [2][32][USTR]
   __shared__ double s_c0[TB_LB], s_c1[TB_LB], s_c2[TB_LB];
   const int m = blockIdx.y, tile = blockIdx.x, tid = threadIdx.x;
   const int rp = tile * TB_TILE + tid;
@@ -170,7 +175,9 @@ __global__ void __launch_bounds__(TB_THREADS) tab_gen_kernel(const RingInfo* __r
     __syncthreads();
     for (int j = 0; j < TB_LB; ++j) {
       const int l = l0 + j;
-      const int pos = ((j & 1) << 5) | (j >> 1);
+      // l = l0 + 2 jp + par: half jp >> 4, element ((comp * 2 + par) * 16 + (jp & 15)) * 4 of the unit
+      const int jp = j >> 1, par = j & 1;
+      const int pos = (jp >> 4) * 32 * USTR / 4 + par * 16 + (jp & 15);
       if (NOPS == 1) {
         my[pos * 4] = (k == 0 && l <= lmax) ? float(f) : 0.f;
         const double nxt = s_c0[j] * x * f - s_c1[j] * fp;
@@ -181,7 +188,7 @@ __global__ void __launch_bounds__(TB_THREADS) tab_gen_kernel(const RingInfo* __r
         if (l == lmin) { f = sf; gg = sg; fp = 0.0; gp = 0.0; }
         const bool use = (k == 0) && (l <= lmax);
         my[pos * 4] = use ? float(0.5 * (f + gg)) : 0.f;
-        my[(TB_LB + pos) * 4] = use ? float(0.5 * (f - gg)) : 0.f;
+        my[(32 + pos) * 4] = use ? float(0.5 * (f - gg)) : 0.f;
         const double ax = s_c0[j] * x;
         const double fn = (ax + s_c1[j]) * f - s_c2[j] * fp;
         const double gn = (ax - s_c1[j]) * gg - s_c2[j] * gp;
@@ -192,17 +199,23 @@ __global__ void __launch_bounds__(TB_THREADS) tab_gen_kernel(const RingInfo* __r
       }
     }
     __syncthreads();
-    // 32 units of this tile are contiguous in the table
-    float4* dst = reinterpret_cast<float4*>(table + ((blockoff[m] + b) * int64_t(nquads) + int64_t(tile) * 32) * UNIT);
-    for (int i = tid; i < 32 * UNIT / 4; i += TB_THREADS) {
-      const int q = i / (UNIT / 4), w = i % (UNIT / 4);
-      dst[i] = *reinterpret_cast<const float4*>(tg_stage + q * USTR + 4 * w);
+    // the 32 units of this tile are contiguous in the table, for each half
+    for (int h = 0; h < 2; ++h) {
+      float4* dst = reinterpret_cast<float4*>(table + tab_unit_index(blockoff[m] + b, h, nquads, tile * 32) * UNIT);
+      for (int i = tid; i < 32 * UNIT / 4; i += TB_THREADS) {
+        const int q = i / (UNIT / 4), w = i % (UNIT / 4);
+        dst[i] = *reinterpret_cast<const float4*>(tg_stage + (h * 32 + q) * USTR + 4 * w);
+      }
     }
     __syncthreads();
   }
 }
 
 // ------------------------------------------------------------------ MMA helpers
+constexpr int TB_NMAX = 80;  // columns per accumulator (MMA N at most)
+
+// K-major core matrices without swizzle: 8 rows x 16 bytes each, the two core matrices of an
+// 8-wide K step 128 bytes apart, 8-row groups 256 bytes apart
 __device__ __forceinline__ uint32_t kcore_off(int row, int kc) {
   return uint32_t(((row >> 3) * 2 + kc) * 128 + (row & 7) * 16);
 }
@@ -238,33 +251,45 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
       : "memory");
 }
 __device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ int round16(int x) { return (x + 15) & ~15; }
 
-// Shared-memory plan of both GEMMs (offsets from a 1024-byte aligned base):
-//   A[acc][kstep][hi/lo]   4 KB each (128 rows x 8 K)          64 KB
-//   B[acc][kstep][hi/lo]   NMAX x 32 B each                    16 NMAX x 32 B
-//   STG[2]                 raw table tiles of the next stages, filled by bulk copies
-//   MISC                   mbarriers (MMA done, staging buffer full x 2), TMEM slot
-template <int NMAX, uint32_t STG_BYTES>
+// Shared memory of one GEMM CTA.  Operand tiles, double-buffered by stage parity:
+// A [buf][acc][ks][hi/lo] 4 KB each (128 rows x 8 K), B [buf][acc][ks][hi/lo] TB_NMAX x 32 B each;
+// then NR staging buffers of RAW bytes for the bulk copies, then the barriers:
+// mbar_mma[2] (MMAs of the stages of that parity complete), mbar_full[NR] (staging buffer filled).
+template <uint32_t RAW, int NR_>
 struct TabSmem {
-  static constexpr int KS = 4;  // K steps (of 8) per accumulator and stage
-  static constexpr uint32_t A_TILE = TB_TILE * 32;
-  static constexpr uint32_t B_TILE = NMAX * 32;
-  static constexpr uint32_t B_OFF = 2 * KS * 2 * A_TILE;
-  static constexpr uint32_t STG_OFF = B_OFF + 2 * KS * 2 * B_TILE;
-  static constexpr uint32_t MISC_OFF = STG_OFF + 2 * STG_BYTES;
-  static constexpr uint32_t DYN = MISC_OFF + 64 + 1024;
-  static constexpr uint32_t TMEM_COLS = 4 * NMAX;  // D[2][NMAX], S[2][NMAX]
-  __device__ static uint32_t a(int acc, int ks, int hl) { return ((acc * KS + ks) * 2 + hl) * A_TILE; }
-  __device__ static uint32_t b(int acc, int ks, int hl) { return B_OFF + ((acc * KS + ks) * 2 + hl) * B_TILE; }
-  __device__ static uint32_t stg(int buf) { return STG_OFF + uint32_t(buf) * STG_BYTES; }
+  static constexpr int NR = NR_;
+  static constexpr uint32_t RAW_BYTES = RAW;
+  static constexpr uint32_t A_TILE = 128 * 32;
+  static constexpr uint32_t B_TILE = TB_NMAX * 32;
+  static constexpr uint32_t A_BUF = 8 * A_TILE;
+  static constexpr uint32_t B_BUF = 8 * B_TILE;
+  static constexpr uint32_t B_OFF = 2 * A_BUF;
+  static constexpr uint32_t RAW_OFF = B_OFF + 2 * B_BUF;
+  static constexpr uint32_t MISC_OFF = RAW_OFF + NR * RAW;
+  static constexpr uint32_t DYN = MISC_OFF + 128 + 1024;  // + alignment of the base to 1 KB
+  static constexpr uint32_t TMEM_COLS = 512;              // D[2][2][TB_NMAX], S[2][TB_NMAX]
+  static_assert(RAW % 16 == 0 && NR <= 4, "staging buffers");
+  __device__ static uint32_t a(int buf, int acc, int ks, int hl) {
+    return uint32_t(buf) * A_BUF + uint32_t((acc * 2 + ks) * 2 + hl) * A_TILE;
+  }
+  __device__ static uint32_t b(int buf, int acc, int ks, int hl) {
+    return B_OFF + uint32_t(buf) * B_BUF + uint32_t((acc * 2 + ks) * 2 + hl) * B_TILE;
+  }
+  __device__ static uint32_t raw(int i) { return RAW_OFF + uint32_t(i) * RAW; }
 };
+
+// TMEM columns: D[dbuf][acc] at (2 dbuf + acc) TB_NMAX, S[acc] at (4 + acc) TB_NMAX
+__device__ __forceinline__ uint32_t tcol_d(int dbuf, int acc) { return uint32_t((2 * dbuf + acc) * TB_NMAX); }
+__device__ __forceinline__ uint32_t tcol_s(int acc) { return uint32_t((4 + acc) * TB_NMAX); }
 
 // CTA state shared by both GEMMs
 struct TabCta {
   uint8_t* smem;
   uint32_t sbase;
-  uint32_t mbar_mma;   // MMAs of the current stage complete
-  uint32_t mbar_full;  // + 8 * buf: staging buffer buf filled
+  uint32_t mbar_mma;   // + 8 * (stage & 1)
+  uint32_t mbar_full;  // + 8 * staging buffer
   uint32_t tmem;
 };
 
@@ -274,16 +299,16 @@ __device__ __forceinline__ TabCta tab_begin(uint8_t* smem_raw) {
   c.smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   c.sbase = tc::smem_u32(c.smem);
   c.mbar_mma = c.sbase + S::MISC_OFF;
-  c.mbar_full = c.sbase + S::MISC_OFF + 8;
-  uint32_t* slot = reinterpret_cast<uint32_t*>(c.smem + S::MISC_OFF + 32);
+  c.mbar_full = c.sbase + S::MISC_OFF + 16;
+  uint32_t* slot = reinterpret_cast<uint32_t*>(c.smem + S::MISC_OFF + 96);
   if ((threadIdx.x >> 5) == 0) {
     tc::tmem_alloc(tc::smem_u32(slot), S::TMEM_COLS);
     tc::tmem_relinquish();
   }
   if (threadIdx.x == 0) {
     tc::mbar_init(c.mbar_mma, 1);
-    tc::mbar_init(c.mbar_full, 1);
-    tc::mbar_init(c.mbar_full + 8, 1);
+    tc::mbar_init(c.mbar_mma + 8, 1);
+    for (int i = 0; i < S::NR; ++i) tc::mbar_init(c.mbar_full + 8u * uint32_t(i), 1);
     tc::fence_mbar_init();
   }
   tc::fence_before_sync();
@@ -293,82 +318,6 @@ __device__ __forceinline__ TabCta tab_begin(uint8_t* smem_raw) {
   return c;
 }
 
-// one stage's MMAs: 2 accumulators x 4 K steps x (hi.hi + hi.lo + lo.hi), D fresh per stage
-template <class S, int NMAX>
-__device__ __forceinline__ void tab_issue(uint32_t sbase, uint32_t tmem, uint32_t idesc) {
-#pragma unroll
-  for (int acc = 0; acc < 2; ++acc) {
-    const uint32_t d = tmem + uint32_t(acc * NMAX);
-#pragma unroll
-    for (int ks = 0; ks < S::KS; ++ks) {
-      const uint64_t ah = kdesc(sbase + S::a(acc, ks, 0)), al = kdesc(sbase + S::a(acc, ks, 1));
-      const uint64_t bh = kdesc(sbase + S::b(acc, ks, 0)), bl = kdesc(sbase + S::b(acc, ks, 1));
-      tc::mma_tf32(d, ah, bh, idesc, ks > 0 ? 1u : 0u);
-      tc::mma_tf32(d, ah, bl, idesc, 1u);
-      tc::mma_tf32(d, al, bh, idesc, 1u);
-    }
-  }
-}
-
-// S += D for this thread's TMEM lane (first stage: S = D), columns [0, n) of both accumulators.
-// Unit u = (16-column chunk u >> 1, accumulator u & 1); the TM_THREADS / 128 warps that share a TMEM
-// lane quarter take every fourth unit; the loads of D and S of a unit share one wait
-template <int NMAX>
-__device__ __forceinline__ void tab_drain(uint32_t lane_addr, int n, bool first) {
-  const int nu = n >> 3;
-#pragma unroll 1
-  for (int u = int(threadIdx.x >> 7); u < nu; u += TM_THREADS / 128) {
-    float d[16], s[16];
-    const uint32_t dc = lane_addr + uint32_t((u & 1) * NMAX + 16 * (u >> 1));
-    const uint32_t sc = dc + uint32_t(2 * NMAX);
-    tc::tmem_ld16(dc, d);
-    if (!first) tc::tmem_ld16(sc, s);
-    tc::tmem_ld_wait();
-    if (!first) {
-#pragma unroll
-      for (int q = 0; q < 16; ++q) d[q] += s[q];
-    }
-    tmem_st16(sc, d);
-  }
-  tmem_st_wait();
-}
-
-// bounded wait of every thread on an mbarrier phase; on expiry raise the flag
-__device__ __forceinline__ bool tab_wait(uint32_t mbar, uint32_t parity, int* err_flag) {
-  const bool ok = __syncthreads_and(tc::mbar_wait_bounded(mbar, parity, TB_WAIT_LIMIT));
-  if (!ok && threadIdx.x == 0) atomicExch(err_flag, 1);
-  return ok;
-}
-
-// make every thread's operand stores visible to the tensor core, then (thread 0) issue the MMAs
-template <class S, int NMAX>
-__device__ __forceinline__ void tab_issue_stage(const TabCta& c, uint32_t idesc) {
-  tc::fence_proxy_async();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    tc::fence_after_sync();
-    tab_issue<S, NMAX>(c.sbase, c.tmem, idesc);
-    tc::mma_commit(c.mbar_mma);
-  }
-}
-
-// wait for the stage's MMAs and drain D into S; false (flag raised) when the wait expires
-template <int NMAX>
-__device__ __forceinline__ bool tab_finish_stage(const TabCta& c, int n, bool first, uint32_t& phase,
-                                                 int* err_flag) {
-  if (!tab_wait(c.mbar_mma, phase, err_flag)) {
-    tc::mbar_wait_bounded(c.mbar_mma, phase, TB_WAIT_LIMIT);  // once more, for the issued MMAs
-    return false;
-  }
-  phase ^= 1u;
-  tc::fence_after_sync();
-  const uint32_t lane_addr = c.tmem + (uint32_t(((threadIdx.x >> 5) & 3) * 32) << 16);
-  tab_drain<NMAX>(lane_addr, n, first);
-  tc::fence_before_sync();
-  __syncthreads();
-  return true;
-}
-
 template <class S>
 __device__ __forceinline__ void tab_end(const TabCta& c) {
   tc::fence_before_sync();
@@ -376,32 +325,86 @@ __device__ __forceinline__ void tab_end(const TabCta& c) {
   if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(c.tmem, S::TMEM_COLS);
 }
 
+// one stage's MMAs (thread 0): 2 accumulators x 2 K steps x (hi.hi + hi.lo + lo.hi) from operand
+// buffer buf into D[dbuf]; restart: the first stage of a D period overwrites D.  Both operands
+// K-major.  The tensor core's FP32 accumulator add truncates, with an error relative to the
+// accumulator's magnitude: the small cross terms (hi.lo, lo.hi) go in first, while the accumulator
+// is small, and the hi.hi products last, so that only those adds truncate at full magnitude.
+template <class S>
+__device__ __forceinline__ void tab_mma(const TabCta& c, int buf, int dbuf, bool restart, uint32_t idesc) {
+#pragma unroll
+  for (int acc = 0; acc < 2; ++acc) {
+    const uint32_t d = c.tmem + tcol_d(dbuf, acc);
+    uint64_t ah[2], al[2], bh[2], bl[2];
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) {
+      ah[ks] = kdesc(c.sbase + S::a(buf, acc, ks, 0));
+      al[ks] = kdesc(c.sbase + S::a(buf, acc, ks, 1));
+      bh[ks] = kdesc(c.sbase + S::b(buf, acc, ks, 0));
+      bl[ks] = kdesc(c.sbase + S::b(buf, acc, ks, 1));
+    }
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) tc::mma_tf32(d, ah[ks], bl[ks], idesc, (restart && ks == 0) ? 0u : 1u);
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) tc::mma_tf32(d, al[ks], bh[ks], idesc, 1u);
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) tc::mma_tf32(d, ah[ks], bh[ks], idesc, 1u);
+  }
+}
+
+// S += D[dbuf] (first D period: S = D) for this thread's TMEM lane, columns [0, n) of both
+// accumulators.  Unit u = (16-column chunk u >> 1, accumulator u & 1); the four warps that share
+// a TMEM lane quarter take every fourth unit
+__device__ __forceinline__ void tab_drain(const TabCta& c, int dbuf, int n, bool first) {
+  const uint32_t lane_addr = c.tmem + (uint32_t(((threadIdx.x >> 5) & 3) * 32) << 16);
+  const int nu = n >> 3;
+#pragma unroll 1
+  for (int u = int(threadIdx.x >> 7); u < nu; u += TM_THREADS / 128) {
+    float d[16], sm[16];
+    const int acc = u & 1, cb = 16 * (u >> 1);
+    const uint32_t dc = lane_addr + tcol_d(dbuf, acc) + uint32_t(cb);
+    const uint32_t sc = lane_addr + tcol_s(acc) + uint32_t(cb);
+    tc::tmem_ld16(dc, d);
+    if (!first) tc::tmem_ld16(sc, sm);
+    tc::tmem_ld_wait();
+    if (!first) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) d[q] += sm[q];
+    }
+    tmem_st16(sc, d);
+  }
+  tmem_st_wait();
+}
+
 // the S columns [cb, cb + 16) of accumulator acc of this thread's lane
-template <int NMAX>
 __device__ __forceinline__ void tab_read_sum(const TabCta& c, int acc, int cb, float* v) {
   const uint32_t lane_addr = c.tmem + (uint32_t(((threadIdx.x >> 5) & 3) * 32) << 16);
-  tc::tmem_ld16(lane_addr + uint32_t(2 * NMAX + acc * NMAX + cb), v);
+  tc::tmem_ld16(lane_addr + tcol_s(acc) + uint32_t(cb), v);
   tc::tmem_ld_wait();
 }
 
-__device__ __forceinline__ int round16(int x) { return (x + 15) & ~15; }
-
-// raw table tile of the synthesis: the 32 units (quads) of one block and ring tile, each unit at a
-// padded stride (unit + 16 bytes) so that lanes reading different units hit different banks
-template <int NOPS>
-struct SynthStg {
-  static constexpr int UNIT = NOPS * TB_LB * 4;  // floats
-  static constexpr int USTR = UNIT + 4;
-  static constexpr uint32_t BYTES = 32u * USTR * 4u;
-};
+// bounded wait, uniform over the warp (false: the limit was reached by some lane)
+__device__ __forceinline__ bool tab_wait(uint32_t mbar, uint32_t parity) {
+  return __all_sync(0xffffffffu, tc::mbar_wait_bounded(mbar, parity, TB_WAIT_LIMIT)) != 0;
+}
 
 // ------------------------------------------------------------------ synthesis
+// staging of the synthesis: one half block (32 units) of a 128-ring tile per buffer, each unit at a
+// padded stride (unit + 16 bytes) so that lanes reading different units hit different banks; a
+// spin-s half block feeds two stages (8 positions each)
+template <int NOPS>
+struct SynthCfg {
+  static constexpr int UNIT = tab_unit_floats(NOPS);
+  static constexpr int USTR = UNIT + 4;
+  static constexpr uint32_t RAW = 32u * USTR * 4u;
+  static constexpr int NR = NOPS == 1 ? 4 : 3;
+  static constexpr int SPT = NOPS == 1 ? 1 : 2;  // stages per staged half block
+};
+
 // almT [nalm][B][NOPS] complex128 -> phase [R][mmax+1][B][NOPS] complex64 of the ring pairs
 // [0, nrp) (table rings toff + i; north row i, south row R - 1 - i, R = 2 nrp - 1).
-// grid.x = map group + G * (ring tile + T * m).  One CTA of 16 warps per SM: the table tiles of
-// the next two blocks are in flight (bulk copies into the staging buffers) while a stage is split
-// and multiplied; every thread has one operand task per stage.
-template <int NOPS, int NMAX>
+// grid.x = map group + G * (ring tile + T * m).
+template <int NOPS>
 __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* __restrict__ table,
                                                                    const int64_t* __restrict__ blockoff, int nquads,
                                                                    int toff, int nrp, int lmax, int mmax,
@@ -409,10 +412,12 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
                                                                    float2* __restrict__ phase, int B, int gsize,
                                                                    int ngroups, int ntiles, int spin_odd,
                                                                    int* __restrict__ err_flag) {
-  using G = SynthStg<NOPS>;
-  using S = TabSmem<NMAX, G::BYTES>;
+  using G = SynthCfg<NOPS>;
+  using S = TabSmem<G::RAW, G::NR>;
   constexpr int NCOMP = NOPS;
   constexpr int UNIT = G::UNIT;
+  constexpr int SPT = G::SPT;
+  constexpr int NR = G::NR;
   extern __shared__ uint8_t tab_smem_raw[];
   int bid = blockIdx.x;
   const int grp = bid % ngroups; bid /= ngroups;
@@ -426,169 +431,162 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   TabCta c = tab_begin<S>(tab_smem_raw);
   const int q0 = toff / 4 + tile * 32;  // first table quad of the tile
+  const int nvq = max(0, min(32, nquads - q0));
   const int nb = tab_nblocks(m, lmax);
+  const int nraw = 2 * nb;  // staged half blocks
+  const int nst = nraw * SPT;
   const int64_t base = alm_index(m, m, lmax);
-  const int nhalf = NOPS == 1 ? 1 : 2;  // stages per table block
-  const int nst = nb * nhalf;
-  const int nvq = max(0, min(32, nquads - q0));  // units of the tile inside the table
-  int issued = 0, waited = 0;  // blocks whose copies were issued / whose buffer wait completed (all threads)
-  // bulk copies of block b's tile into staging buffer b & 1 (warp 0: lane q copies unit q)
-  auto issue_block = [&](int b) {
-    if (b >= nb) return;
-    issued = b + 1;
+  const int64_t gb0 = blockoff[m];
+  int raw_issued = 0, raw_waited = 0;  // half blocks whose copies were issued / waited for (uniform)
+  // bulk copies of half block r (block r >> 1, half r & 1) of the tile into staging buffer r % NR
+  // (warp 0: lane q copies unit q)
+  auto issue_raw = [&](int r) {
+    if (r >= nraw) return;
+    raw_issued = r + 1;
     if (warp != 0) return;
-    const uint32_t bar = c.mbar_full + 8u * uint32_t(b & 1);
+    const uint32_t bar = c.mbar_full + 8u * uint32_t(r % NR);
     if (lane == 0) tc::mbar_arrive_expect_tx(bar, uint32_t(nvq) * UNIT * 4u);
     __syncwarp();  // the transaction count is expected before any unit lands
-    if (lane < nvq) {
-      const float* src = table + ((blockoff[m] + b) * int64_t(nquads) + q0 + lane) * UNIT;
-      tc::bulk_g2s(c.sbase + S::stg(b & 1) + uint32_t(lane) * G::USTR * 4u, src, UNIT * 4u, bar);
-    }
+    if (lane < nvq)
+      tc::bulk_g2s(c.sbase + S::raw(r % NR) + uint32_t(lane * G::USTR) * 4u,
+                   table + tab_unit_index(gb0 + (r >> 1), r & 1, nquads, q0 + lane) * UNIT, UNIT * 4u, bar);
   };
-  // ---- this thread's A task (the same every stage): warp = task (K chunk and accumulator), lane = quad
-  int a_acc, a_pos0, a_comp;
+  // ---- A: task t = tid < 256 (quad q = t & 31, r = t >> 5) loads 4 positions x 4 rings of quad q and
+  // stores them transposed: ring 4 q + i of the tile is A row 32 i + q (the 16-byte stores of eight
+  // consecutive lanes fall into eight different bank groups), K = 4 consecutive positions.
+  // spin 0: (parity p, group g) = (r >> 2, r & 3), positions 4 g + i -> A(acc p, ks g >> 1, kc g & 1);
+  // spin s (stage half qq): (comp cc, parity p, group g) = (r >> 2, (r >> 1) & 1, r & 1) at positions
+  // 8 qq + 4 g + i -> A(acc = p for F+, 1 - p for F-; ks cc, kc g)
+  const bool a_v = tid < 256;
+  int a_src;
+  uint32_t a_dst;
   {
-    const int t = warp;
+    const int q = tid & 31, r = (tid >> 5) & 7;
+    int p, g, acc, ks, cc;
     if (NOPS == 1) {
-      a_acc = t >> 3; a_pos0 = a_acc * 32 + 4 * (t & 7); a_comp = 0;
+      cc = 0; p = r >> 2; g = r & 3; acc = p; ks = g >> 1;
     } else {
-      a_comp = t >> 3;
-      const int par = (t >> 2) & 1, g4 = t & 3;
-      a_acc = a_comp == 0 ? par : 1 - par;
-      a_pos0 = par * 32 + 4 * g4;  // + 16 h
+      cc = r >> 2; p = (r >> 1) & 1; g = r & 1; acc = cc == 0 ? p : 1 - p; ks = cc;
     }
+    a_src = q * G::USTR + ((cc * 2 + p) * 16 + 4 * g) * 4;  // spin s: + 32 qq
+    a_dst = uint32_t(((acc * 2 + ks) * 2) * S::A_TILE) + kcore_off(q, g & 1);  // row 32 i + q: + 1024 i
   }
-  const int a_kk = NOPS == 1 ? 4 * (warp & 7) : 16 * (warp >> 3) + 4 * (warp & 3);
-  const uint32_t a_oh = S::a(a_acc, a_kk >> 3, 0), a_ol = S::a(a_acc, a_kk >> 3, 1);
-  const int a_kc = (a_kk >> 2) & 1;
-  bool a_in[4];
+  // ---- B: task t = 511 - tid < 8 gs (map j = t % gs, (acc, k4) = t / gs), 4 K values of 2 (spin 0) or
+  // 4 (spin s) rows.  K index 4 k4 + i of acc: spin 0 position 16 h + 4 k4 + i of parity acc;
+  // spin s comp cc = k4 >> 1 at position 16 h + 8 qq + 4 (k4 & 1) + i, parity acc (F+) or 1 - acc (F-)
+  const int b_t = TM_THREADS - 1 - tid;  // from the top, away from the A tasks
+  const bool b_v = b_t < 8 * gs;
+  const int b_j = b_v ? b_t % gs : 0, b_ak = b_v ? b_t / gs : 0;
+  const int b_acc = b_ak >> 2, b_k4 = b_ak & 3;
+  const int b_cc = NOPS == 1 ? 0 : b_k4 >> 1;
+  const int b_lofs = NOPS == 1 ? 8 * b_k4 + b_acc : 8 * (b_k4 & 1) + (b_cc == 0 ? b_acc : 1 - b_acc);
+  const int b_ks = b_k4 >> 1, b_kc = b_k4 & 1;
+  float2 ab[NCOMP][4];
+  auto load_alm = [&](int s) {
+    const int r = s / SPT, qq = s % SPT, b = r >> 1, h = r & 1;
+    const int l0 = m + TB_LB * b + 32 * h + 16 * qq + b_lofs;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int rt = 4 * (q0 + lane) + i;
-    a_in[i] = rt >= toff && rt < toff + nrp && lane < nvq;
-  }
-  // ---- this thread's B tasks: spin 0: t = tid + 512 i (map j = t % gs, (acc, k4) = t / gs), 16 gs <= 1024;
-  // spin s: t = tid < 256 (map j = t & 15, (acc, k4) = t >> 4)
-  constexpr int BTS = NOPS == 1 ? 2 : 1;
-  int b_j[BTS], b_acc[BTS], b_k4[BTS], b_lofs[BTS];
-  bool b_v[BTS];
+    for (int i = 0; i < 4; ++i) {
+      const int l = l0 + 2 * i;
+      const bool v = b_v && l <= lmax;
+      const int64_t o = ((base + (l - m)) * B + b0 + b_j) * NCOMP;
 #pragma unroll
-  for (int i2 = 0; i2 < BTS; ++i2) {
-    const int t = tid + TM_THREADS * i2;
-    if (NOPS == 1) {
-      b_v[i2] = t < 16 * gs;
-      const int j = b_v[i2] ? t % gs : 0, ak = b_v[i2] ? t / gs : 0;
-      b_j[i2] = j; b_acc[i2] = ak >> 3; b_k4[i2] = ak & 7;
-      b_lofs[i2] = 8 * b_k4[i2] + b_acc[i2];  // l = m + 64 b + b_lofs + 2 i
-    } else {
-      const int j = t & 15, ak = (t >> 4) & 15;
-      b_v[i2] = t < 256 && j < gs;
-      b_j[i2] = j; b_acc[i2] = ak >> 3; b_k4[i2] = ak & 7;
-      const int comp = b_k4[i2] >> 2, g4 = b_k4[i2] & 3, par = comp == 0 ? b_acc[i2] : 1 - b_acc[i2];
-      b_lofs[i2] = 2 * 4 * g4 + par;  // l = m + 64 b + 32 h + b_lofs + 2 i
-    }
-  }
-  // alm of one stage in registers (FP32), loaded a stage ahead: spin 0 (re, im) of 4 l per task,
-  // spin s G and C of 4 l
-  float2 ab[BTS][2][4];
-  auto load_alm = [&](int st) {
-    const int b = st / nhalf, h = st % nhalf;
-#pragma unroll
-    for (int i2 = 0; i2 < BTS; ++i2) {
-      const int l0 = m + TB_LB * b + 32 * h + b_lofs[i2];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int l = l0 + 2 * i;
-        const bool v = b_v[i2] && l <= lmax;
-        const int64_t o = ((base + (l - m)) * B + b0 + b_j[i2]) * NCOMP;
-        const double2 x0 = v ? almT[o] : make_double2(0.0, 0.0);
-        ab[i2][0][i] = make_float2(float(x0.x), float(x0.y));
-        if (NOPS == 2) {
-          const double2 x1 = v ? almT[o + 1] : make_double2(0.0, 0.0);
-          ab[i2][1][i] = make_float2(float(x1.x), float(x1.y));
-        }
+      for (int cc = 0; cc < NCOMP; ++cc) {
+        const double2 x = v ? almT[o + cc] : make_double2(0.0, 0.0);
+        ab[cc][i] = make_float2(float(x.x), float(x.y));
       }
     }
   };
-  // split and store the operands of stage st: A from the staged table tile, B from the registers
-  auto store = [&](int st) {
-    const int b = st / nhalf, h = st % nhalf;
-    {
-      const float* stg = reinterpret_cast<const float*>(c.smem + S::stg(b & 1));
-      const float* u = stg + lane * G::USTR + (a_comp * TB_LB + a_pos0 + 16 * h) * 4;
+  // split and store the operands of stage s into buffer s & 1
+  auto store = [&](int s) {
+    const int buf = s & 1, qq = s % SPT;
+    if (a_v) {
+      const float* u = reinterpret_cast<const float*>(c.smem + S::raw((s / SPT) % NR)) + a_src + 32 * qq;
       float4 v[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) v[i] = reinterpret_cast<const float4*>(u)[i];
-      // ring 4 lane + i of the tile -> A row 32 i + lane; rings outside [toff, toff + nrp) are zero
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        float4 w;
-        w.x = a_in[i] ? (&v[0].x)[i] : 0.f;
-        w.y = a_in[i] ? (&v[1].x)[i] : 0.f;
-        w.z = a_in[i] ? (&v[2].x)[i] : 0.f;
-        w.w = a_in[i] ? (&v[3].x)[i] : 0.f;
-        const uint32_t co = kcore_off(32 * i + lane, a_kc);
-        st_split(c.smem, a_oh + co, a_ol + co, w);
+        // ring i of the quad: its values at the 4 positions
+        const float4 w = make_float4((&v[0].x)[i], (&v[1].x)[i], (&v[2].x)[i], (&v[3].x)[i]);
+        const uint32_t d = S::a(buf, 0, 0, 0) + a_dst + uint32_t(i) * kcore_off(32, 0);
+        st_split(c.smem, d, d + S::A_TILE, w);
       }
     }
+    if (!b_v) return;
+    const uint32_t bh = S::b(buf, b_acc, b_ks, 0), bl = S::b(buf, b_acc, b_ks, 1);
+    if (NOPS == 1) {
+      const float4 re = make_float4(ab[0][0].x, ab[0][1].x, ab[0][2].x, ab[0][3].x);
+      const float4 im = make_float4(ab[0][0].y, ab[0][1].y, ab[0][2].y, ab[0][3].y);
+      st_split(c.smem, bh + kcore_off(b_j, b_kc), bl + kcore_off(b_j, b_kc), re);
+      st_split(c.smem, bh + kcore_off(gs + b_j, b_kc), bl + kcore_off(gs + b_j, b_kc), im);
+    } else {
+      // F+ rows take X = -(G, C) (even spin) or Y = (C.im, -C.re, -G.im, G.re); F- rows the other one
+      const bool use_x = (b_cc == 0) != (spin_odd != 0);
+      float4 pt[4];
 #pragma unroll
-    for (int i2 = 0; i2 < BTS; ++i2) {
-      if (!b_v[i2]) continue;
-      const int j = b_j[i2], acc = b_acc[i2], k4 = b_k4[i2];
-      const int ks = k4 >> 1, kc = k4 & 1;
-      if (NOPS == 1) {
-        const float4 re = make_float4(ab[i2][0][0].x, ab[i2][0][1].x, ab[i2][0][2].x, ab[i2][0][3].x);
-        const float4 im = make_float4(ab[i2][0][0].y, ab[i2][0][1].y, ab[i2][0][2].y, ab[i2][0][3].y);
-        st_split(c.smem, S::b(acc, ks, 0) + kcore_off(j, kc), S::b(acc, ks, 1) + kcore_off(j, kc), re);
-        st_split(c.smem, S::b(acc, ks, 0) + kcore_off(gs + j, kc), S::b(acc, ks, 1) + kcore_off(gs + j, kc), im);
-      } else {
-        // F+ rows take X = -(G, C) (even spin) or Y = (C.im, -C.re, -G.im, G.re); F- rows the other one
-        const int comp = k4 >> 2;
-        const bool use_x = (comp == 0) != (spin_odd != 0);
-        float4 pt[4];
+      for (int i = 0; i < 4; ++i) {
+        const float2 Gv = ab[0][i], Cv = ab[NCOMP - 1][i];
+        float p0, p1, p2, p3;
+        if (use_x) { p0 = -Gv.x; p1 = -Gv.y; p2 = -Cv.x; p3 = -Cv.y; }
+        else { p0 = Cv.y; p1 = -Cv.x; p2 = -Gv.y; p3 = Gv.x; }
+        (&pt[0].x)[i] = p0; (&pt[1].x)[i] = p1; (&pt[2].x)[i] = p2; (&pt[3].x)[i] = p3;
+      }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float2 Gv = ab[i2][0][i], Cv = ab[i2][1][i];
-          float p0, p1, p2, p3;
-          if (use_x) { p0 = -Gv.x; p1 = -Gv.y; p2 = -Cv.x; p3 = -Cv.y; }
-          else { p0 = Cv.y; p1 = -Cv.x; p2 = -Gv.y; p3 = Gv.x; }
-          (&pt[0].x)[i] = p0; (&pt[1].x)[i] = p1; (&pt[2].x)[i] = p2; (&pt[3].x)[i] = p3;
-        }
-#pragma unroll
-        for (int part = 0; part < 4; ++part) {
-          const int row = part * gs + j;
-          st_split(c.smem, S::b(acc, ks, 0) + kcore_off(row, kc), S::b(acc, ks, 1) + kcore_off(row, kc), pt[part]);
-        }
+      for (int part = 0; part < 4; ++part) {
+        const int row = part * gs + b_j;
+        st_split(c.smem, bh + kcore_off(row, b_kc), bl + kcore_off(row, b_kc), pt[part]);
       }
     }
   };
-  uint32_t ph_mma = 0;
-  bool ok = true;
-  issue_block(0);
-  issue_block(1);
+  for (int r = 0; r < NR; ++r) issue_raw(r);
   load_alm(0);
-  for (int st = 0; st < nst; ++st) {
-    const int b = st / nhalf, h = st % nhalf;
-    if (h == 0) {
-      if (!tab_wait(c.mbar_full + 8u * uint32_t(b & 1), uint32_t(b >> 1) & 1u, err_flag)) {
-        ok = false;
-        break;
-      }
-      waited = b + 1;
+  bool ok = true, failed = false;
+  int mma_issued = 0;
+  for (int s = 0; s < nst; ++s) {
+    const int r = s / SPT, qq = s % SPT;
+    if (qq == 0) {
+      ok = ok && tab_wait(c.mbar_full + 8u * uint32_t(r % NR), uint32_t(r / NR) & 1u);
+      if (ok) raw_waited = r + 1;
     }
-    store(st);
-    tab_issue_stage<S, NMAX>(c, idesc);
-    // the staged tile of block b has been read (barrier inside tab_issue_stage): refill its buffer
-    if (h == nhalf - 1) issue_block(b + 2);
-    if (st + 1 < nst) load_alm(st + 1);
-    ok = tab_finish_stage<NMAX>(c, n, st == 0, ph_mma, err_flag);
-    if (!ok) break;
+    if (ok) store(s);
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    if (__syncthreads_or(!ok)) { failed = true; break; }
+    tc::fence_after_sync();
+    if (tid == 0) {
+      tab_mma<S>(c, s & 1, (s >> 1) & 1, (s & 1) == 0, idesc);
+      tc::mma_commit(c.mbar_mma + 8u * uint32_t(s & 1));
+    }
+    mma_issued = s + 1;
+    if (qq == SPT - 1) issue_raw(r + NR);  // half block r has been split (barrier above): refill its buffer
+    if (s + 1 < nst) load_alm(s + 1);
+    if (s >= 1) {
+      // MMAs of stage s - 1 complete: its operand buffer is free; drain D after the second stage of a period
+      const int sp = s - 1;
+      ok = ok && tab_wait(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u);
+      if (ok && (sp & 1)) {
+        tc::fence_after_sync();
+        tab_drain(c, (sp >> 1) & 1, n, sp == 1);
+      }
+    }
   }
-  if (ok) {
+  if (!failed) {
+    const int sp = nst - 1;
+    ok = ok && tab_wait(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u);
+    if (ok) {
+      tc::fence_after_sync();
+      tab_drain(c, (sp >> 1) & 1, n, (sp >> 1) == 0);
+    }
+    tc::fence_before_sync();
+    if (__syncthreads_or(!ok)) failed = true;
+    tc::fence_after_sync();
+  }
+  if (!failed) {
     // epilogue.  TMEM lane tl = 32 lq + q <-> ring 4 q + lq of the tile (lq = warp & 3).  The sums go
-    // through shared memory (free now: every MMA and copy has completed) as rows [north/south][tl]
-    // [map][part], then every ring's row of gs maps is written with coalesced stores
-    constexpr int RS = NMAX + 1;  // row stride (floats): consecutive lanes in consecutive banks
+    // through shared memory (free now) as rows [north/south][lane][map][part], then each ring's row of
+    // gs maps is written with coalesced stores
+    constexpr int RS = TB_NMAX + 1;  // row stride (floats): consecutive lanes in consecutive banks
     static_assert(2 * 128 * RS * 4 <= int(S::MISC_OFF), "epilogue rows exceed the free shared memory");
     float* rows = reinterpret_cast<float*>(c.smem);
     const int lq = warp & 3, cs = warp >> 2;
@@ -596,8 +594,8 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
 #pragma unroll 1
     for (int cb = 16 * cs; cb < n; cb += 64) {
       float s0[16], s1[16];
-      tab_read_sum<NMAX>(c, 0, cb, s0);
-      tab_read_sum<NMAX>(c, 1, cb, s1);
+      tab_read_sum(c, 0, cb, s0);
+      tab_read_sum(c, 1, cb, s1);
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         const int col = cb + q;
@@ -614,7 +612,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
     for (int row = warp; row < 256; row += TM_THREADS / 32) {
       const int ns = row >> 7, t = row & 127;
       const int rt = 4 * q0 + 4 * (t & 31) + (t >> 5);  // table ring of TMEM lane t
-      const int i = rt - toff;                          // ring pair of the plan
+      const int i = rt - toff;    // ring pair of the plan
       if (rt < toff || i >= nrp) continue;
       const int ring = ns == 0 ? i : R - 1 - i;
       if (ns == 1 && ring == i) continue;  // the equator has no south ring
@@ -622,33 +620,39 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
       const float* src = rows + row * RS;
       for (int pos = lane; pos < ncols; pos += 32) dst[pos] = src[pos];
     }
-  } else if (threadIdx.x == 0) {
-    // bulk copies still in flight land in this CTA's shared memory: wait for them (bounded) before exit
-    for (int k = waited; k < issued; ++k)
-      tc::mbar_wait_bounded(c.mbar_full + 8u * uint32_t(k & 1), uint32_t(k >> 1) & 1u, TB_WAIT_LIMIT);
+  } else if (tid == 0) {
+    atomicExch(err_flag, 1);
+    // MMAs and bulk copies still in flight touch this CTA's memory: wait for them (bounded) before exit
+    if (mma_issued > 0) {
+      const int sp = mma_issued - 1;
+      tc::mbar_wait_bounded(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u, TB_WAIT_LIMIT);
+    }
+    for (int k = raw_waited; k < raw_issued; ++k)
+      tc::mbar_wait_bounded(c.mbar_full + 8u * uint32_t(k % NR), uint32_t(k / NR) & 1u, TB_WAIT_LIMIT);
   }
   tab_end<S>(c);
 }
 
-// raw table tile of one adjoint stage: for each of the 4 blocks, the RSTAGE / 4 consecutive units
-// (spin s: followed by the phases of the stage's rings, [north/south][ring][map] complex64 pairs
-// with a row stride of PH_MAPS maps)
+// ------------------------------------------------------------------ adjoint
+// staging of one adjoint stage: for each of the 4 blocks and both halves, the NQ units of the
+// stage's rings, [block][half][quad][unit]; spin s: then the north and south phase rows of the
+// stage's rings, [north/south][ring][PH_MAPS maps] complex64 pairs
 template <int NOPS>
-struct AdjStg {
-  static constexpr int UNIT = NOPS * TB_LB * 4;
-  static constexpr int NQ = NOPS == 1 ? 8 : 4;  // quads per stage
-  static constexpr uint32_t BLK_BYTES = uint32_t(NQ) * UNIT * 4u;
-  static constexpr uint32_t TAB_BYTES = 4u * BLK_BYTES;
-  static constexpr int PH_MAPS = 32;  // maps per group (spin s)
-  static constexpr uint32_t PH_BYTES = NOPS == 2 ? 2u * 4u * NQ * PH_MAPS * 16u : 0u;
-  static constexpr uint32_t BYTES = TAB_BYTES + PH_BYTES;
+struct AdjCfg {
+  static constexpr int UNIT = tab_unit_floats(NOPS);
+  static constexpr int NQ = NOPS == 1 ? 4 : 2;  // quads per stage
+  static constexpr int RSTAGE = 4 * NQ;         // rings per stage
+  static constexpr uint32_t TAB_BYTES = 8u * NQ * UNIT * 4u;
+  static constexpr int PH_MAPS = TB_NMAX / 4;   // maps per group (spin s)
+  static constexpr uint32_t PH_BYTES = NOPS == 2 ? 2u * RSTAGE * PH_MAPS * 16u : 0u;
+  static constexpr uint32_t RAW = TAB_BYTES + PH_BYTES;
+  static constexpr int NR = 4;
 };
 
-// ------------------------------------------------------------------ adjoint
 // phase [R][mmax+1][B][NOPS] complex64 of ring pairs [0, nrp) -> alm of map b at alm + b * out_stride
 // ([NOPS][nalm] complex128, times scale and lscale[comp][idx] when given), for the maps [b0, b0 + gs)
 // of each group.  grid.x = map group + G * (entry of the (m, first block) work list)
-template <int NOPS, int NMAX>
+template <int NOPS>
 __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __restrict__ table,
                                                                  const int64_t* __restrict__ blockoff, int nquads,
                                                                  int toff, int nrp, int lmax, int mmax,
@@ -659,12 +663,13 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
                                                                  int64_t out_stride,
                                                                  const double* __restrict__ lscale,
                                                                  int* __restrict__ err_flag) {
-  using G = AdjStg<NOPS>;
-  using S = TabSmem<NMAX, G::BYTES>;
+  using G = AdjCfg<NOPS>;
+  using S = TabSmem<G::RAW, G::NR>;
   constexpr int NCOMP = NOPS;
   constexpr int UNIT = G::UNIT;
-  constexpr int RSTAGE = 4 * G::NQ;  // table rings per stage
   constexpr int NQ = G::NQ;
+  constexpr int RSTAGE = G::RSTAGE;
+  constexpr int NR = G::NR;
   extern __shared__ uint8_t tab_smem_raw[];
   int bid = blockIdx.x;
   const int grp = bid % ngroups; bid /= ngroups;
@@ -678,61 +683,62 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   TabCta c = tab_begin<S>(tab_smem_raw);
   const int nb = tab_nblocks(m, lmax);
+  const int nblk = min(4, nb - bb);
   const int R = 2 * nrp - 1;
   const int rt_begin = toff & ~3, rt_end = toff + nrp;
-  const int nstages = (rt_end - rt_begin + RSTAGE - 1) / RSTAGE;
-  int issued = 0, waited = 0;  // stages whose copies were issued / whose buffer wait completed (all threads)
-  // bulk copies of stage st's units into staging buffer st & 1 (thread 0)
-  // bulk copies of stage st's units (and, spin s, of its phase rows) into staging buffer st & 1
-  // (warp 0: lane 0 the table units, lane r the phase rows of ring r of the stage)
-  auto issue_stage_copy = [&](int st) {
-    if (st >= nstages) return;
-    issued = st + 1;
+  const int nst = (rt_end - rt_begin + RSTAGE - 1) / RSTAGE;
+  const int64_t gb0 = blockoff[m] + bb;
+  int raw_issued = 0, raw_waited = 0;  // stages whose copies were issued / waited for (uniform)
+  // bulk copies of stage st into staging buffer st % NR (warp 0: lane 2 blk + h the units of block
+  // blk, half h; spin s: lane r < RSTAGE the phase rows of ring r of the stage)
+  auto issue_raw = [&](int st) {
+    if (st >= nst) return;
+    raw_issued = st + 1;
     if (warp != 0) return;
     const int rs0 = rt_begin + st * RSTAGE;
     const int qs = rs0 / 4;
     const int nvq = max(0, min(NQ, nquads - qs));
-    int nblk = 0;
-    for (int blk = 0; blk < 4; ++blk) nblk += (bb + blk < nb);
-    uint32_t tx = uint32_t(nblk * nvq) * UNIT * 4u;
-    // spin s: ring rs0 + r (r = lane < RSTAGE) has a north row when it is a ring of the plan, and a
-    // south row unless it is the equator
+    uint32_t tx = uint32_t(nblk * 2 * nvq) * UNIT * 4u;
     const int ip = rs0 + lane - toff;
     const bool ph_n = NOPS == 2 && lane < RSTAGE && ip >= 0 && ip < nrp;
     const bool ph_s = ph_n && R - 1 - ip != ip;
     const uint32_t row_bytes = uint32_t(gs) * 16u;
+    if (NOPS == 2)
+      tx += uint32_t(__popc(__ballot_sync(0xffffffffu, ph_n)) + __popc(__ballot_sync(0xffffffffu, ph_s))) * row_bytes;
+    const uint32_t bar = c.mbar_full + 8u * uint32_t(st % NR);
+    const uint32_t dst = c.sbase + S::raw(st % NR);
+    if (lane == 0) tc::mbar_arrive_expect_tx(bar, tx);
+    __syncwarp();  // the transaction count is expected before any copy lands
+    if (lane < 8 && (lane >> 1) < nblk && nvq > 0)
+      tc::bulk_g2s(dst + uint32_t(lane * NQ * UNIT) * 4u,
+                   table + tab_unit_index(gb0 + (lane >> 1), lane & 1, nquads, qs) * UNIT, uint32_t(nvq) * UNIT * 4u,
+                   bar);
     if (NOPS == 2) {
-      uint32_t rows = uint32_t(ph_n) + uint32_t(ph_s);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) rows += __shfl_xor_sync(0xffffffffu, rows, o);
-      tx += rows * row_bytes;
-    }
-    const uint32_t bar = c.mbar_full + 8u * uint32_t(st & 1);
-    const uint32_t dst = c.sbase + S::stg(st & 1);
-    if (lane == 0) {
-      tc::mbar_arrive_expect_tx(bar, tx);
-      for (int blk = 0; blk < 4; ++blk) {
-        if (bb + blk >= nb || nvq == 0) continue;
-        const float* src = table + ((blockoff[m] + bb + blk) * int64_t(nquads) + qs) * UNIT;
-        tc::bulk_g2s(dst + uint32_t(blk) * G::BLK_BYTES, src, uint32_t(nvq) * UNIT * 4u, bar);
-      }
-    }
-    if (NOPS == 2) {
-      __syncwarp();  // the transaction count is expected before any phase row lands
       const uint32_t pd = dst + G::TAB_BYTES + uint32_t(lane) * G::PH_MAPS * 16u;
-      if (ph_n)
-        tc::bulk_g2s(pd, phase + ((int64_t(ip) * (mmax + 1) + m) * B + b0) * NCOMP, row_bytes, bar);
+      if (ph_n) tc::bulk_g2s(pd, phase + ((int64_t(ip) * (mmax + 1) + m) * B + b0) * NCOMP, row_bytes, bar);
       if (ph_s)
         tc::bulk_g2s(pd + uint32_t(RSTAGE) * G::PH_MAPS * 16u,
                      phase + ((int64_t(R - 1 - ip) * (mmax + 1) + m) * B + b0) * NCOMP, row_bytes, bar);
     }
   };
-  // ---- A tasks: combination t = warp + 16 it (quad, comp, block, acc), lane = position in the parity half
-  constexpr int NT = 2 * 4 * NOPS * NQ;  // 64
-  constexpr int NA = NT / (TM_THREADS / 32);
-  // ---- B tasks.  spin 0: t = tid (map j = t % gs, quad qd = t / gs), NQ gs <= 512, phases loaded to
-  // registers a stage ahead.  spin s: t = tid (sub = t & 3 -> (acc, comp), map j = (t >> 2) % gs,
-  // quad qd = (t >> 2) / gs), NQ gs <= 128, phases read from the staged rows
+  // ---- A: this thread splits float4 t = tid + 512 i (i = 0, 1) of the stage's 1024: unit u = t / (32 NOPS)
+  // = (block, half, quad qd), element (comp cc, parity p, position jj) of the unit -> A(acc p), row
+  // 32 block + 16 half + jj, K chunk cc NQ + qd (four rings)
+  uint32_t a_dst[2];
+  int a_qd[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int t = tid + TM_THREADS * i;
+    const int u = t / (32 * NOPS), w = t % (32 * NOPS);
+    const int cc = w >> 5, p = (w >> 4) & 1, jj = w & 15;
+    const int qd = u % NQ, bh = u / NQ, h = bh & 1, blk = bh >> 1;
+    const int row = blk * 32 + 16 * h + jj, kq = cc * NQ + qd;
+    a_qd[i] = qd;
+    a_dst[i] = uint32_t(((p * 2 + (kq >> 1)) * 2) * S::A_TILE) + kcore_off(row, kq & 1);
+  }
+  // ---- B.  spin 0: task t = tid < NQ gs (map j = t % gs, quad qd = t / gs), phases of its 4 rings
+  // loaded into registers a stage ahead.  spin s: task t = tid (acc = (t >> 1) & 1, comp cc = t & 1,
+  // map j = (t >> 2) % gs, quad qd = (t >> 2) / gs), NQ gs <= 40, phases read from the staged rows
   const int p_t = NOPS == 1 ? tid : tid >> 2;
   const bool p_v = p_t < NQ * gs;
   const int p_j = p_v ? p_t % gs : 0, p_qd = p_v ? p_t / gs : 0;
@@ -742,48 +748,30 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
     const int rs0 = rt_begin + st * RSTAGE;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const int rt = rs0 + 4 * p_qd + i;
-      const int ip = rt - toff;
-      const bool in = p_v && rt >= toff && ip < nrp;
+      const int ip = rs0 + 4 * p_qd + i - toff;
+      const bool in = p_v && ip >= 0 && ip < nrp;
       const int rsth = R - 1 - ip;
       pn[i] = in ? phase[(int64_t(ip) * (mmax + 1) + m) * B + b0 + p_j] : make_float2(0.f, 0.f);
       pv[i] = (in && rsth != ip) ? phase[(int64_t(rsth) * (mmax + 1) + m) * B + b0 + p_j] : make_float2(0.f, 0.f);
     }
   };
   auto store = [&](int st) {
+    const int buf = st & 1;
     const int rs0 = rt_begin + st * RSTAGE;
-    const float* stg = reinterpret_cast<const float*>(c.smem + S::stg(st & 1));
+    const int nvq = max(0, min(NQ, nquads - rs0 / 4));
+    const float* raw = reinterpret_cast<const float*>(c.smem + S::raw(st % NR));
 #pragma unroll
-    for (int it = 0; it < NA; ++it) {
-      const int t = warp + (TM_THREADS / 32) * it;
-      const int qd = t % NQ;
-      int r = t / NQ;
-      const int comp = r % NOPS; r /= NOPS;
-      const int blk = r % 4;
-      const int acc = r / 4;
-      const int b = bb + blk;
-      const int qg = rs0 / 4 + qd;
+    for (int i = 0; i < 2; ++i) {
+      // quads beyond the table were not copied: their rings contribute nothing
       float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (b < nb && qg < nquads) {
-        v = *reinterpret_cast<const float4*>(stg + blk * (G::BLK_BYTES / 4) + qd * UNIT +
-                                             (comp * TB_LB + acc * 32 + lane) * 4);
-        // rings outside [toff, toff + nrp) contribute nothing
-        const int r0 = 4 * qg;
-        if (r0 < toff || r0 + 3 >= rt_end) {
-          if (r0 + 0 < toff || r0 + 0 >= rt_end) v.x = 0.f;
-          if (r0 + 1 < toff || r0 + 1 >= rt_end) v.y = 0.f;
-          if (r0 + 2 < toff || r0 + 2 >= rt_end) v.z = 0.f;
-          if (r0 + 3 < toff || r0 + 3 >= rt_end) v.w = 0.f;
-        }
-      }
-      const int kk = comp * 16 + 4 * qd;  // K index of the chunk (spin 0: comp = 0, qd < 8)
-      const int ks = kk >> 3, kc = (kk >> 2) & 1;
-      const int row = blk * 32 + lane;
-      st_split(c.smem, S::a(acc, ks, 0) + kcore_off(row, kc), S::a(acc, ks, 1) + kcore_off(row, kc), v);
+      if (a_qd[i] < nvq) v = *reinterpret_cast<const float4*>(raw + 4 * (tid + TM_THREADS * i));
+      const uint32_t d = S::a(buf, 0, 0, 0) + a_dst[i];
+      st_split(c.smem, d, d + S::A_TILE, v);
     }
-    if (p_v && NOPS == 1) {
-      const int j = p_j, qd = p_qd;
-      // ring sums (combo 0: N + S) and differences (combo 1: N - S) of 4 rings
+    if (!p_v) return;
+    const int j = p_j, qd = p_qd;
+    if (NOPS == 1) {
+      // ring sums (accumulator 0: N + S) and differences (accumulator 1: N - S) of 4 rings
       float4 cre[2], cim[2];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
@@ -792,22 +780,21 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
         (&cre[1].x)[i] = pn[i].x - pv[i].x;
         (&cim[1].x)[i] = pn[i].y - pv[i].y;
       }
-      const int kk = 4 * qd, ks = kk >> 3, kc = (kk >> 2) & 1;
+      const int ks = qd >> 1, kc = qd & 1;
 #pragma unroll
       for (int acc = 0; acc < 2; ++acc) {
-        st_split(c.smem, S::b(acc, ks, 0) + kcore_off(j, kc), S::b(acc, ks, 1) + kcore_off(j, kc), cre[acc]);
-        st_split(c.smem, S::b(acc, ks, 0) + kcore_off(gs + j, kc), S::b(acc, ks, 1) + kcore_off(gs + j, kc),
-                 cim[acc]);
+        const uint32_t bh = S::b(buf, acc, ks, 0), bl = S::b(buf, acc, ks, 1);
+        st_split(c.smem, bh + kcore_off(j, kc), bl + kcore_off(j, kc), cre[acc]);
+        st_split(c.smem, bh + kcore_off(gs + j, kc), bl + kcore_off(gs + j, kc), cim[acc]);
       }
-    } else if (p_v) {
+    } else {
       // columns (G.re, G.im, C.re, C.im); combo k (0: N + S, 1: N - S) of the rings' (Q, U):
       // Xa(k) = (-Q.re, -Q.im, -U.re, -U.im), Ya(k) = (U.im, -U.re, -Q.im, Q.re)
       // even spin: F+ rows Xa(acc), F- rows Ya(1 - acc); odd spin: F+ rows Ya(acc), F- rows Xa(1 - acc)
-      const int j = p_j, qd = p_qd;
-      const int acc = (tid >> 1) & 1, comp = tid & 1;
-      const int k = comp == 0 ? acc : 1 - acc;
-      const bool use_x = (comp == 0) != (spin_odd != 0);
-      const float4* ph = reinterpret_cast<const float4*>(c.smem + S::stg(st & 1) + G::TAB_BYTES);
+      const int acc = (tid >> 1) & 1, cc = tid & 1;
+      const int k = cc == 0 ? acc : 1 - acc;
+      const bool use_x = (cc == 0) != (spin_odd != 0);
+      const float4* ph = reinterpret_cast<const float4*>(c.smem + S::raw(st % NR) + G::TAB_BYTES);
       float4 p[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
@@ -827,46 +814,71 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
           (&p[0].x)[i] = cv.w; (&p[1].x)[i] = -cv.z; (&p[2].x)[i] = -cv.y; (&p[3].x)[i] = cv.x;
         }
       }
-      const int kk = comp * 16 + 4 * qd, ks = kk >> 3, kc = (kk >> 2) & 1;
+      const int kq = cc * NQ + qd, ks = kq >> 1, kc = kq & 1;
+      const uint32_t bh = S::b(buf, acc, ks, 0), bl = S::b(buf, acc, ks, 1);
 #pragma unroll
       for (int part = 0; part < 4; ++part) {
         const int row = part * gs + j;
-        st_split(c.smem, S::b(acc, ks, 0) + kcore_off(row, kc), S::b(acc, ks, 1) + kcore_off(row, kc), p[part]);
+        st_split(c.smem, bh + kcore_off(row, kc), bl + kcore_off(row, kc), p[part]);
       }
     }
   };
-  uint32_t ph_mma = 0;
-  bool ok = true;
-  issue_stage_copy(0);
-  issue_stage_copy(1);
+  for (int st = 0; st < NR; ++st) issue_raw(st);
   load_phase(0);
-  for (int st = 0; st < nstages; ++st) {
-    if (!tab_wait(c.mbar_full + 8u * uint32_t(st & 1), uint32_t(st >> 1) & 1u, err_flag)) {
-      ok = false;
-      break;
+  bool ok = true, failed = false;
+  int mma_issued = 0;
+  for (int st = 0; st < nst; ++st) {
+    ok = ok && tab_wait(c.mbar_full + 8u * uint32_t(st % NR), uint32_t(st / NR) & 1u);
+    if (ok) {
+      raw_waited = st + 1;
+      store(st);
     }
-    waited = st + 1;
-    store(st);
-    tab_issue_stage<S, NMAX>(c, idesc);
-    issue_stage_copy(st + 2);  // staging buffer st & 1 has been read (barrier inside tab_issue_stage)
-    if (st + 1 < nstages) load_phase(st + 1);
-    ok = tab_finish_stage<NMAX>(c, n, st == 0, ph_mma, err_flag);
-    if (!ok) break;
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    if (__syncthreads_or(!ok)) { failed = true; break; }
+    tc::fence_after_sync();
+    if (tid == 0) {
+      tab_mma<S>(c, st & 1, (st >> 1) & 1, (st & 1) == 0, idesc);
+      tc::mma_commit(c.mbar_mma + 8u * uint32_t(st & 1));
+    }
+    mma_issued = st + 1;
+    issue_raw(st + NR);  // staging buffer st % NR has been read (barrier above)
+    if (st + 1 < nst) load_phase(st + 1);
+    if (st >= 1) {
+      // MMAs of stage st - 1 complete: its operand buffer is free; drain D after the second stage of a period
+      const int sp = st - 1;
+      ok = ok && tab_wait(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u);
+      if (ok && (sp & 1)) {
+        tc::fence_after_sync();
+        tab_drain(c, (sp >> 1) & 1, n, sp == 1);
+      }
+    }
   }
-  if (ok) {
-    // epilogue: TMEM lane = A row = blk * 32 + j (blk = warp & 3); accumulator acc is
-    // l = tab_l(m, bb + blk, acc * 32 + j); the four warps of a lane quarter take every fourth column chunk
-    const int blk = warp & 3, cs = warp >> 2, j = lane;
-    const int b = bb + blk;
+  if (!failed && nst > 0) {
+    const int sp = nst - 1;
+    ok = ok && tab_wait(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u);
+    if (ok) {
+      tc::fence_after_sync();
+      tab_drain(c, (sp >> 1) & 1, n, (sp >> 1) == 0);
+    }
+    tc::fence_before_sync();
+    if (__syncthreads_or(!ok)) failed = true;
+    tc::fence_after_sync();
+  }
+  if (!failed && nst > 0) {
+    // epilogue: TMEM lane = A row = 32 blk + j (blk = warp & 3, j = position in the parity), accumulator
+    // acc is l = m + 64 (bb + blk) + 2 j + acc; the four warps of a lane quarter take every fourth
+    // column chunk
+    const int blk = warp & 3, cs = warp >> 2;
 #pragma unroll 1
     for (int acc = 0; acc < 2; ++acc) {
-      const int l = tab_l(m, b, acc * 32 + j);
-      const bool in = b < nb && l <= lmax;
+      const int l = tab_l(m, bb + blk, lane, acc);
+      const bool in = blk < nblk && l <= lmax;
       const int64_t idx = alm_index(l, m, lmax);
 #pragma unroll 1
       for (int cb = 16 * cs; cb < n; cb += 64) {
-        float s[16];
-        tab_read_sum<NMAX>(c, acc, cb, s);
+        float sm[16];
+        tab_read_sum(c, acc, cb, sm);
         if (!in) continue;
         // columns come in (re, im) pairs of one complex value only when gs is even; write parts one by one
 #pragma unroll
@@ -878,13 +890,19 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
           const double f = lscale ? scale * lscale[int64_t(comp) * nalm + idx] : scale;
           double* dst = reinterpret_cast<double*>(alm + int64_t(b0 + jm) * out_stride + int64_t(comp) * nalm + idx) +
                         (part & 1);
-          *dst = double(s[q]) * f;
+          *dst = double(sm[q]) * f;
         }
       }
     }
-  } else if (threadIdx.x == 0) {
-    for (int k = waited; k < issued; ++k)
-      tc::mbar_wait_bounded(c.mbar_full + 8u * uint32_t(k & 1), uint32_t(k >> 1) & 1u, TB_WAIT_LIMIT);
+  } else if (failed && tid == 0) {
+    atomicExch(err_flag, 1);
+    // MMAs and bulk copies still in flight touch this CTA's memory: wait for them (bounded) before exit
+    if (mma_issued > 0) {
+      const int sp = mma_issued - 1;
+      tc::mbar_wait_bounded(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u, TB_WAIT_LIMIT);
+    }
+    for (int k = raw_waited; k < raw_issued; ++k)
+      tc::mbar_wait_bounded(c.mbar_full + 8u * uint32_t(k % NR), uint32_t(k / NR) & 1u, TB_WAIT_LIMIT);
   }
   tab_end<S>(c);
 }
@@ -923,13 +941,13 @@ int launch_tab_gen(const Plan& P, int spin, const int64_t* d_blockoff, float* ta
   const int nquads = tab_quads(P.Rh);
   dim3 grid(nquads * 4 / TB_TILE, P.mmax + 1);
   if (spin == 0) {
-    const int smem = 32 * (1 * TB_LB * 4 + 4) * sizeof(float);
+    const int smem = 2 * 32 * (tab_unit_floats(1) + 4) * sizeof(float);
     if (set_smem_attr((const void*)tab_gen_kernel<1>, smem)) return PS_ERR_CUDA;
     tab_gen_kernel<1><<<grid, TB_THREADS, smem, st>>>(P.d_rings, P.d_mnorm0, nullptr, P.Rh, P.lmax, 0, d_blockoff,
                                                       nquads, table);
   } else {
     if (!P.d_seed[spin]) return PS_ERR_INVALID;
-    const int smem = 32 * (2 * TB_LB * 4 + 4) * sizeof(float);
+    const int smem = 2 * 32 * (tab_unit_floats(2) + 4) * sizeof(float);
     if (set_smem_attr((const void*)tab_gen_kernel<2>, smem)) return PS_ERR_CUDA;
     tab_gen_kernel<2><<<grid, TB_THREADS, smem, st>>>(P.d_rings, nullptr, P.d_seed[spin], P.Rh, P.lmax, spin,
                                                       d_blockoff, nquads, table);
@@ -953,27 +971,25 @@ int launch_tab_synth(const Plan& P, const float* table, const int64_t* d_blockof
   const double bytes = double(tab_bytes(Rh_table, P.lmax, P.mmax, spin)) * double(P.Rh) / double(Rh_table) +
                        double(B) * (spin == 0 ? 1 : 2) * (16.0 * P.nalm + 8.0 * P.R * (P.mmax + 1));
   StatScope sc(PS_K_LEG_SYNTH, flops, bytes, st);
-  // 128 columns per accumulator for spin 0 (up to 64 maps per pass over the table), 64 for spin s
-  // (16 maps; its staged tiles are twice as large, which leaves shared memory for no more)
-  const int nmax = spin == 0 ? 128 : 64;
+  // TB_NMAX columns per accumulator: up to 40 maps of spin 0 or 20 of spin s per pass over the table
   int ngroups = 1;
-  const int gsize = tab_group_size(B, spin, nmax, ngroups);
+  const int gsize = tab_group_size(B, spin, TB_NMAX, ngroups);
   const int ntiles = ((toff & 3) + P.Rh + TB_TILE - 1) / TB_TILE;
   const int nquads = tab_quads(Rh_table);
   const int64_t nblk = int64_t(ngroups) * ntiles * (P.mmax + 1);
   if (nblk > 0x7fffffff) return PS_ERR_UNSUPPORTED;
   if (spin == 0) {
-    const int smem = int(TabSmem<128, SynthStg<1>::BYTES>::DYN);
-    if (set_smem_attr((const void*)tab_synth_kernel<1, 128>, smem)) return PS_ERR_CUDA;
-    tab_synth_kernel<1, 128><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
-                                                                       P.mmax, almT, phase, B, gsize, ngroups, ntiles,
-                                                                       0, err_flag);
+    const int smem = int(TabSmem<SynthCfg<1>::RAW, SynthCfg<1>::NR>::DYN);
+    if (set_smem_attr((const void*)tab_synth_kernel<1>, smem)) return PS_ERR_CUDA;
+    tab_synth_kernel<1><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+                                                                  P.mmax, almT, phase, B, gsize, ngroups, ntiles, 0,
+                                                                  err_flag);
   } else {
-    const int smem = int(TabSmem<64, SynthStg<2>::BYTES>::DYN);
-    if (set_smem_attr((const void*)tab_synth_kernel<2, 64>, smem)) return PS_ERR_CUDA;
-    tab_synth_kernel<2, 64><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
-                                                                      P.mmax, almT, phase, B, gsize, ngroups, ntiles,
-                                                                      spin & 1, err_flag);
+    const int smem = int(TabSmem<SynthCfg<2>::RAW, SynthCfg<2>::NR>::DYN);
+    if (set_smem_attr((const void*)tab_synth_kernel<2>, smem)) return PS_ERR_CUDA;
+    tab_synth_kernel<2><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+                                                                  P.mmax, almT, phase, B, gsize, ngroups, ntiles,
+                                                                  spin & 1, err_flag);
   }
   PS_LAUNCH_CHECK();
   return PS_OK;
@@ -995,25 +1011,24 @@ int launch_tab_adj(const Plan& P, const float* table, const int64_t* d_blockoff,
   const double bytes = double(tab_bytes(Rh_table, P.lmax, P.mmax, spin)) * double(P.Rh) / double(Rh_table) +
                        double(B) * (spin == 0 ? 1 : 2) * (16.0 * P.nalm + 8.0 * P.R * (P.mmax + 1));
   StatScope sc(PS_K_LEG_ADJOINT, flops, bytes, st);
-  // 128 columns per accumulator: up to 64 maps of spin 0 or 32 of spin s per pass over the table
-  constexpr int nmax = 128;
+  // TB_NMAX columns per accumulator: up to 40 maps of spin 0 or 20 of spin s per pass over the table
   int ngroups = 1;
-  const int gsize = tab_group_size(B, spin, nmax, ngroups);
+  const int gsize = tab_group_size(B, spin, TB_NMAX, ngroups);
   const int nquads = tab_quads(Rh_table);
   const int64_t nblk = int64_t(ngroups) * nwork;
   if (nblk > 0x7fffffff) return PS_ERR_UNSUPPORTED;
   // spin s phase rows are staged by bulk copies, which start on 16-byte boundaries
   if (spin != 0 && (reinterpret_cast<uintptr_t>(phase) & 15u)) return PS_ERR_INVALID;
   if (spin == 0) {
-    const int smem = int(TabSmem<nmax, AdjStg<1>::BYTES>::DYN);
-    if (set_smem_attr((const void*)tab_adj_kernel<1, nmax>, smem)) return PS_ERR_CUDA;
-    tab_adj_kernel<1, nmax><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+    const int smem = int(TabSmem<AdjCfg<1>::RAW, AdjCfg<1>::NR>::DYN);
+    if (set_smem_attr((const void*)tab_adj_kernel<1>, smem)) return PS_ERR_CUDA;
+    tab_adj_kernel<1><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
                                                                       P.mmax, phase, alm, B, gsize, ngroups, d_work,
                                                                       P.nalm, scale, 0, out_stride, lscale, err_flag);
   } else {
-    const int smem = int(TabSmem<nmax, AdjStg<2>::BYTES>::DYN);
-    if (set_smem_attr((const void*)tab_adj_kernel<2, nmax>, smem)) return PS_ERR_CUDA;
-    tab_adj_kernel<2, nmax><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
+    const int smem = int(TabSmem<AdjCfg<2>::RAW, AdjCfg<2>::NR>::DYN);
+    if (set_smem_attr((const void*)tab_adj_kernel<2>, smem)) return PS_ERR_CUDA;
+    tab_adj_kernel<2><<<unsigned(nblk), TM_THREADS, smem, st>>>(table, d_blockoff, nquads, toff, P.Rh, P.lmax,
                                                                       P.mmax, phase, alm, B, gsize, ngroups, d_work,
                                                                       P.nalm, scale, spin & 1, out_stride, lscale,
                                                                       err_flag);
