@@ -75,6 +75,8 @@ constexpr int TB_TILE = 128;     // ring pairs per synthesis tile (MMA M)
 constexpr int TB_THREADS = 128;  // table generation
 constexpr int TM_THREADS = 512;  // the two GEMMs: 16 warps, 4 per TMEM lane quarter
 constexpr uint32_t TB_WAIT_LIMIT = 1u << 24;
+// the warp that issues the bulk copies: not one of the two MMA-issuing warps (0 and 1)
+constexpr int TB_COPY_WARP = 2;
 
 // ------------------------------------------------------------------ table geometry
 // number of table blocks of order m
@@ -83,6 +85,10 @@ __host__ __device__ __forceinline__ int tab_nblocks(int m, int lmax) { return (l
 __host__ __device__ __forceinline__ int tab_l(int m, int b, int j, int par) { return m + TB_LB * b + 2 * j + par; }
 // floats per unit (m, b, h, q): [ncomp][2 parities][16 positions][4 rings]
 __host__ __device__ constexpr int tab_unit_floats(int ncomp) { return ncomp * 2 * 16 * 4; }
+// stride of the units in the table (floats): 16 bytes of padding after each unit, so that a run of
+// units lands in shared memory with the bank-spreading stride the transposing reads need, from one
+// bulk copy (many small copies cap the copy engine at a fraction of HBM bandwidth)
+__host__ __device__ constexpr int tab_unit_stride(int ncomp) { return tab_unit_floats(ncomp) + 4; }
 // unit index of (global block gb = blockoff[m] + b, half h, quad q)
 __host__ __device__ __forceinline__ int64_t tab_unit_index(int64_t gb, int h, int nquads, int q) {
   return (gb * 2 + h) * int64_t(nquads) + q;
@@ -131,7 +137,7 @@ __global__ void __launch_bounds__(TB_THREADS) tab_gen_kernel(const RingInfo* __r
                                                              int spin, const int64_t* __restrict__ blockoff,
                                                              int nquads, float* __restrict__ table) {
   constexpr int UNIT = tab_unit_floats(NOPS);  // floats per unit
-  constexpr int USTR = UNIT + 4;                // padded stride in the stage
+  constexpr int USTR = tab_unit_stride(NOPS);   // padded stride in the stage and the table
   extern __shared__ __align__(16) float tg_stage[];  // [2][32][USTR]
   __shared__ double s_c0[TB_LB], s_c1[TB_LB], s_c2[TB_LB];
   const int m = blockIdx.y, tile = blockIdx.x, tid = threadIdx.x;
@@ -145,6 +151,8 @@ __global__ void __launch_bounds__(TB_THREADS) tab_gen_kernel(const RingInfo* __r
   if (NOPS == 1) tab_seed0(m, g.sth, mnorm[m], f, k);
   else tab_seedS(m, spin, g, seednorm[m], sf, sg, k);
   if (!active) { f = 0.0; sf = 0.0; sg = 0.0; k = 0; }
+  for (int i = tid; i < 2 * 32 * USTR; i += TB_THREADS) tg_stage[i] = 0.f;  // the pads stay zero
+  __syncthreads();
   float* my = tg_stage + (tid >> 2) * USTR + (tid & 3);
   const int nb = tab_nblocks(m, lmax);
   for (int b = 0; b < nb; ++b) {
@@ -201,11 +209,10 @@ __global__ void __launch_bounds__(TB_THREADS) tab_gen_kernel(const RingInfo* __r
     __syncthreads();
     // the 32 units of this tile are contiguous in the table, for each half
     for (int h = 0; h < 2; ++h) {
-      float4* dst = reinterpret_cast<float4*>(table + tab_unit_index(blockoff[m] + b, h, nquads, tile * 32) * UNIT);
-      for (int i = tid; i < 32 * UNIT / 4; i += TB_THREADS) {
-        const int q = i / (UNIT / 4), w = i % (UNIT / 4);
-        dst[i] = *reinterpret_cast<const float4*>(tg_stage + (h * 32 + q) * USTR + 4 * w);
-      }
+      // (padded units: the stage rows are the table's unit stride)
+      float4* dst = reinterpret_cast<float4*>(table + tab_unit_index(blockoff[m] + b, h, nquads, tile * 32) * USTR);
+      const float4* src = reinterpret_cast<const float4*>(tg_stage + h * 32 * USTR);
+      for (int i = tid; i < 32 * USTR / 4; i += TB_THREADS) dst[i] = src[i];
     }
     __syncthreads();
   }
@@ -268,9 +275,9 @@ struct TabSmem {
   static constexpr uint32_t B_OFF = 2 * A_BUF;
   static constexpr uint32_t RAW_OFF = B_OFF + 2 * B_BUF;
   static constexpr uint32_t MISC_OFF = RAW_OFF + NR * RAW;
-  static constexpr uint32_t DYN = MISC_OFF + 128 + 1024;  // + alignment of the base to 1 KB
+  static constexpr uint32_t DYN = MISC_OFF + 256 + 1024;  // + alignment of the base to 1 KB
   static constexpr uint32_t TMEM_COLS = 512;              // D[2][2][TB_NMAX], S[2][TB_NMAX]
-  static_assert(RAW % 16 == 0 && NR <= 4, "staging buffers");
+  static_assert(RAW % 16 == 0 && NR <= 8, "staging buffers");
   __device__ static uint32_t a(int buf, int acc, int ks, int hl) {
     return uint32_t(buf) * A_BUF + uint32_t((acc * 2 + ks) * 2 + hl) * A_TILE;
   }
@@ -306,8 +313,8 @@ __device__ __forceinline__ TabCta tab_begin(uint8_t* smem_raw) {
     tc::tmem_relinquish();
   }
   if (threadIdx.x == 0) {
-    tc::mbar_init(c.mbar_mma, 1);
-    tc::mbar_init(c.mbar_mma + 8, 1);
+    tc::mbar_init(c.mbar_mma, 2);  // one commit from each issuing warp
+    tc::mbar_init(c.mbar_mma + 8, 2);
     for (int i = 0; i < S::NR; ++i) tc::mbar_init(c.mbar_full + 8u * uint32_t(i), 1);
     tc::fence_mbar_init();
   }
@@ -325,31 +332,47 @@ __device__ __forceinline__ void tab_end(const TabCta& c) {
   if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(c.tmem, S::TMEM_COLS);
 }
 
-// one stage's MMAs (thread 0): 2 accumulators x 2 K steps x (hi.hi + hi.lo + lo.hi) from operand
-// buffer buf into D[dbuf]; restart: the first stage of a D period overwrites D.  Both operands
-// K-major.  The tensor core's FP32 accumulator add truncates, with an error relative to the
-// accumulator's magnitude: the small cross terms (hi.lo, lo.hi) go in first, while the accumulator
-// is small, and the hi.hi products last, so that only those adds truncate at full magnitude.
+// MMA issue.  Warp acc (0 or 1) issues the MMAs of accumulator acc, converged, one lane elected per
+// instruction, from descriptors computed once per CTA (buffer 1: the buffer strides added to the
+// start-address fields, which stay below 2^14 x 16 bytes); both warps commit to the stage's barrier
+// (arrival count 2).  A single diverged lane that rebuilt the descriptors between MMAs fed the
+// tensor core at about a third of this rate.
+struct TabIssuer {
+  uint64_t ah[2], al[2], bh[2], bl[2];  // buffer 0, K steps 0 and 1
+  uint64_t da, db;                       // descriptor increments of buffer 1
+  uint32_t d0;                           // TMEM address of D[0][acc]
+};
 template <class S>
-__device__ __forceinline__ void tab_mma(const TabCta& c, int buf, int dbuf, bool restart, uint32_t idesc) {
+__device__ __forceinline__ TabIssuer tab_issuer(const TabCta& c, int acc) {
+  TabIssuer is;
 #pragma unroll
-  for (int acc = 0; acc < 2; ++acc) {
-    const uint32_t d = c.tmem + tcol_d(dbuf, acc);
-    uint64_t ah[2], al[2], bh[2], bl[2];
-#pragma unroll
-    for (int ks = 0; ks < 2; ++ks) {
-      ah[ks] = kdesc(c.sbase + S::a(buf, acc, ks, 0));
-      al[ks] = kdesc(c.sbase + S::a(buf, acc, ks, 1));
-      bh[ks] = kdesc(c.sbase + S::b(buf, acc, ks, 0));
-      bl[ks] = kdesc(c.sbase + S::b(buf, acc, ks, 1));
-    }
-#pragma unroll
-    for (int ks = 0; ks < 2; ++ks) tc::mma_tf32(d, ah[ks], bl[ks], idesc, (restart && ks == 0) ? 0u : 1u);
-#pragma unroll
-    for (int ks = 0; ks < 2; ++ks) tc::mma_tf32(d, al[ks], bh[ks], idesc, 1u);
-#pragma unroll
-    for (int ks = 0; ks < 2; ++ks) tc::mma_tf32(d, ah[ks], bh[ks], idesc, 1u);
+  for (int ks = 0; ks < 2; ++ks) {
+    is.ah[ks] = kdesc(c.sbase + S::a(0, acc, ks, 0));
+    is.al[ks] = kdesc(c.sbase + S::a(0, acc, ks, 1));
+    is.bh[ks] = kdesc(c.sbase + S::b(0, acc, ks, 0));
+    is.bl[ks] = kdesc(c.sbase + S::b(0, acc, ks, 1));
   }
+  is.da = uint64_t(S::A_BUF >> 4);
+  is.db = uint64_t(S::B_BUF >> 4);
+  is.d0 = c.tmem + tcol_d(0, acc);
+  return is;
+}
+// one stage's MMAs of one accumulator: 2 K steps x (hi.hi + hi.lo + lo.hi) from operand buffer buf
+// into D[dbuf]; restart: the first stage of a D period overwrites D.  Both operands K-major.  The
+// tensor core's FP32 accumulator add truncates, with an error relative to the accumulator's
+// magnitude: the small cross terms (hi.lo, lo.hi) go in first, while the accumulator is small, and
+// the hi.hi products last, so that only those adds truncate at full magnitude.
+__device__ __forceinline__ void tab_mma(const TabIssuer& is, int buf, int dbuf, bool restart, uint32_t idesc,
+                                        uint32_t bar) {
+  const uint64_t oa = buf ? is.da : 0, ob = buf ? is.db : 0;
+  const uint32_t d = is.d0 + uint32_t(dbuf * 2 * TB_NMAX);
+  tc::mma_tf32_elect(d, is.ah[0] + oa, is.bl[0] + ob, idesc, restart ? 0u : 1u);
+  tc::mma_tf32_elect(d, is.ah[1] + oa, is.bl[1] + ob, idesc, 1u);
+  tc::mma_tf32_elect(d, is.al[0] + oa, is.bh[0] + ob, idesc, 1u);
+  tc::mma_tf32_elect(d, is.al[1] + oa, is.bh[1] + ob, idesc, 1u);
+  tc::mma_tf32_elect(d, is.ah[0] + oa, is.bh[0] + ob, idesc, 1u);
+  tc::mma_tf32_elect(d, is.ah[1] + oa, is.bh[1] + ob, idesc, 1u);
+  tc::mma_commit_elect(bar);
 }
 
 // S += D[dbuf] (first D period: S = D) for this thread's TMEM lane, columns [0, n) of both
@@ -388,6 +411,76 @@ __device__ __forceinline__ bool tab_wait(uint32_t mbar, uint32_t parity) {
   return __all_sync(0xffffffffu, tc::mbar_wait_bounded(mbar, parity, TB_WAIT_LIMIT)) != 0;
 }
 
+// ---- warp-specialised pipeline (synthesis).  Barriers at the start of the misc area, 8 bytes each:
+// full[8] (staging buffer filled: bulk-copy transactions), raw_free[8] (staging buffer consumed:
+// one arrival per producer warp), op_full[2] (operand buffer written: one per producer warp),
+// mma_done[2] (the stage's MMAs complete: one commit per MMA warp), d_ready[2] (a D period's MMAs
+// complete), d_free[2] (D drained into S: one arrival per drain warp); then an abort flag and the
+// TMEM slot.
+constexpr int WS_MMA_WARPS = 2;    // warps 0, 1: MMA issue, accumulator = warp
+constexpr int WS_COPY_WARP = 2;    // bulk copies
+constexpr int WS_PROD0 = 4;        // warps 4 .. 11: operand producers
+constexpr int WS_NPROD = 8;
+constexpr int WS_DRAIN0 = 12;      // warps 12 .. 15: drain, TMEM lane quarter = warp & 3
+struct TabPipe {
+  uint32_t full, raw_free, op_full, mma_done, d_ready, d_free;  // + 8 * index
+  volatile int* abort;
+};
+template <class S>
+__device__ __forceinline__ TabCta tab_begin_ws(uint8_t* smem_raw, TabPipe& pp) {
+  TabCta c;
+  c.smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  c.sbase = tc::smem_u32(c.smem);
+  const uint32_t misc = c.sbase + S::MISC_OFF;
+  pp.full = misc; pp.raw_free = misc + 64; pp.op_full = misc + 128; pp.mma_done = misc + 144;
+  pp.d_ready = misc + 160; pp.d_free = misc + 176;
+  pp.abort = reinterpret_cast<volatile int*>(c.smem + S::MISC_OFF + 192);
+  c.mbar_mma = pp.mma_done;
+  c.mbar_full = pp.full;
+  uint32_t* slot = reinterpret_cast<uint32_t*>(c.smem + S::MISC_OFF + 224);
+  if ((threadIdx.x >> 5) == 0) {
+    tc::tmem_alloc(tc::smem_u32(slot), S::TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S::NR; ++i) {
+      tc::mbar_init(pp.full + 8u * uint32_t(i), 1);
+      tc::mbar_init(pp.raw_free + 8u * uint32_t(i), WS_NPROD);
+    }
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(pp.op_full + 8u * uint32_t(i), WS_NPROD);
+      tc::mbar_init(pp.mma_done + 8u * uint32_t(i), WS_MMA_WARPS);
+      tc::mbar_init(pp.d_ready + 8u * uint32_t(i), WS_MMA_WARPS);
+      tc::mbar_init(pp.d_free + 8u * uint32_t(i), 4);
+    }
+    *pp.abort = 0;
+    tc::fence_mbar_init();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  c.tmem = *slot;
+  return c;
+}
+// bounded wait of one warp (lane 0 polls, the result is shared): false when the limit is reached
+// or another warp has aborted; the first to give up raises the abort flag and the error flag
+__device__ __forceinline__ bool ws_wait(const TabPipe& pp, uint32_t mbar, uint32_t parity, int* err_flag) {
+  int ok = 1;
+  if ((threadIdx.x & 31) == 0) {
+    ok = 0;
+    for (uint32_t i = 0; i < TB_WAIT_LIMIT; ++i) {
+      if (tc::mbar_try_wait(mbar, parity)) { ok = 1; break; }
+      if ((i & 63) == 63 && *pp.abort) break;
+    }
+    if (!ok && atomicExch(const_cast<int*>(pp.abort), 1) == 0) atomicExch(err_flag, 1);
+  }
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+__device__ __forceinline__ void ws_arrive(uint32_t mbar) {
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
 // ------------------------------------------------------------------ synthesis
 // staging of the synthesis: one half block (32 units) of a 128-ring tile per buffer, each unit at a
 // padded stride (unit + 16 bytes) so that lanes reading different units hit different banks; a
@@ -395,9 +488,9 @@ __device__ __forceinline__ bool tab_wait(uint32_t mbar, uint32_t parity) {
 template <int NOPS>
 struct SynthCfg {
   static constexpr int UNIT = tab_unit_floats(NOPS);
-  static constexpr int USTR = UNIT + 4;
+  static constexpr int USTR = tab_unit_stride(NOPS);
   static constexpr uint32_t RAW = 32u * USTR * 4u;
-  static constexpr int NR = NOPS == 1 ? 4 : 3;
+  static constexpr int NR = NOPS == 1 ? 7 : 3;  // as many as shared memory holds
   static constexpr int SPT = NOPS == 1 ? 1 : 2;  // stages per staged half block
 };
 
@@ -418,6 +511,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
   constexpr int UNIT = G::UNIT;
   constexpr int SPT = G::SPT;
   constexpr int NR = G::NR;
+  constexpr int BSL = NOPS == 1 ? 2 : 1;  // B task slots per producer thread (8 gs <= 320 or 160)
   extern __shared__ uint8_t tab_smem_raw[];
   int bid = blockIdx.x;
   const int grp = bid % ngroups; bid /= ngroups;
@@ -429,7 +523,8 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
   const int n = round16(ncols);
   const uint32_t idesc = tc::idesc_tf32(128, n, 0, 0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  TabCta c = tab_begin<S>(tab_smem_raw);
+  TabPipe pp;
+  TabCta c = tab_begin_ws<S>(tab_smem_raw, pp);
   const int q0 = toff / 4 + tile * 32;  // first table quad of the tile
   const int nvq = max(0, min(32, nquads - q0));
   const int nb = tab_nblocks(m, lmax);
@@ -437,155 +532,199 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
   const int nst = nraw * SPT;
   const int64_t base = alm_index(m, m, lmax);
   const int64_t gb0 = blockoff[m];
-  int raw_issued = 0, raw_waited = 0;  // half blocks whose copies were issued / waited for (uniform)
-  // bulk copies of half block r (block r >> 1, half r & 1) of the tile into staging buffer r % NR
-  // (warp 0: lane q copies unit q)
-  auto issue_raw = [&](int r) {
-    if (r >= nraw) return;
-    raw_issued = r + 1;
-    if (warp != 0) return;
-    const uint32_t bar = c.mbar_full + 8u * uint32_t(r % NR);
-    if (lane == 0) tc::mbar_arrive_expect_tx(bar, uint32_t(nvq) * UNIT * 4u);
-    __syncwarp();  // the transaction count is expected before any unit lands
-    if (lane < nvq)
-      tc::bulk_g2s(c.sbase + S::raw(r % NR) + uint32_t(lane * G::USTR) * 4u,
-                   table + tab_unit_index(gb0 + (r >> 1), r & 1, nquads, q0 + lane) * UNIT, UNIT * 4u, bar);
-  };
-  // ---- A: task t = tid < 256 (quad q = t & 31, r = t >> 5) loads 4 positions x 4 rings of quad q and
-  // stores them transposed: ring 4 q + i of the tile is A row 32 i + q (the 16-byte stores of eight
-  // consecutive lanes fall into eight different bank groups), K = 4 consecutive positions.
-  // spin 0: (parity p, group g) = (r >> 2, r & 3), positions 4 g + i -> A(acc p, ks g >> 1, kc g & 1);
-  // spin s (stage half qq): (comp cc, parity p, group g) = (r >> 2, (r >> 1) & 1, r & 1) at positions
-  // 8 qq + 4 g + i -> A(acc = p for F+, 1 - p for F-; ks cc, kc g)
-  const bool a_v = tid < 256;
-  int a_src;
-  uint32_t a_dst;
-  {
-    const int q = tid & 31, r = (tid >> 5) & 7;
-    int p, g, acc, ks, cc;
-    if (NOPS == 1) {
-      cc = 0; p = r >> 2; g = r & 3; acc = p; ks = g >> 1;
-    } else {
-      cc = r >> 2; p = (r >> 1) & 1; g = r & 1; acc = cc == 0 ? p : 1 - p; ks = cc;
-    }
-    a_src = q * G::USTR + ((cc * 2 + p) * 16 + 4 * g) * 4;  // spin s: + 32 qq
-    a_dst = uint32_t(((acc * 2 + ks) * 2) * S::A_TILE) + kcore_off(q, g & 1);  // row 32 i + q: + 1024 i
-  }
-  // ---- B: task t = 511 - tid < 8 gs (map j = t % gs, (acc, k4) = t / gs), 4 K values of 2 (spin 0) or
-  // 4 (spin s) rows.  K index 4 k4 + i of acc: spin 0 position 16 h + 4 k4 + i of parity acc;
-  // spin s comp cc = k4 >> 1 at position 16 h + 8 qq + 4 (k4 & 1) + i, parity acc (F+) or 1 - acc (F-)
-  const int b_t = TM_THREADS - 1 - tid;  // from the top, away from the A tasks
-  const bool b_v = b_t < 8 * gs;
-  const int b_j = b_v ? b_t % gs : 0, b_ak = b_v ? b_t / gs : 0;
-  const int b_acc = b_ak >> 2, b_k4 = b_ak & 3;
-  const int b_cc = NOPS == 1 ? 0 : b_k4 >> 1;
-  const int b_lofs = NOPS == 1 ? 8 * b_k4 + b_acc : 8 * (b_k4 & 1) + (b_cc == 0 ? b_acc : 1 - b_acc);
-  const int b_ks = b_k4 >> 1, b_kc = b_k4 & 1;
-  float2 ab[NCOMP][4];
-  auto load_alm = [&](int s) {
-    const int r = s / SPT, qq = s % SPT, b = r >> 1, h = r & 1;
-    const int l0 = m + TB_LB * b + 32 * h + 16 * qq + b_lofs;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int l = l0 + 2 * i;
-      const bool v = b_v && l <= lmax;
-      const int64_t o = ((base + (l - m)) * B + b0 + b_j) * NCOMP;
-#pragma unroll
-      for (int cc = 0; cc < NCOMP; ++cc) {
-        const double2 x = v ? almT[o + cc] : make_double2(0.0, 0.0);
-        ab[cc][i] = make_float2(float(x.x), float(x.y));
-      }
-    }
-  };
-  // split and store the operands of stage s into buffer s & 1
-  auto store = [&](int s) {
-    const int buf = s & 1, qq = s % SPT;
-    if (a_v) {
-      const float* u = reinterpret_cast<const float*>(c.smem + S::raw((s / SPT) % NR)) + a_src + 32 * qq;
-      float4 v[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) v[i] = reinterpret_cast<const float4*>(u)[i];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        // ring i of the quad: its values at the 4 positions
-        const float4 w = make_float4((&v[0].x)[i], (&v[1].x)[i], (&v[2].x)[i], (&v[3].x)[i]);
-        const uint32_t d = S::a(buf, 0, 0, 0) + a_dst + uint32_t(i) * kcore_off(32, 0);
-        st_split(c.smem, d, d + S::A_TILE, w);
-      }
-    }
-    if (!b_v) return;
-    const uint32_t bh = S::b(buf, b_acc, b_ks, 0), bl = S::b(buf, b_acc, b_ks, 1);
-    if (NOPS == 1) {
-      const float4 re = make_float4(ab[0][0].x, ab[0][1].x, ab[0][2].x, ab[0][3].x);
-      const float4 im = make_float4(ab[0][0].y, ab[0][1].y, ab[0][2].y, ab[0][3].y);
-      st_split(c.smem, bh + kcore_off(b_j, b_kc), bl + kcore_off(b_j, b_kc), re);
-      st_split(c.smem, bh + kcore_off(gs + b_j, b_kc), bl + kcore_off(gs + b_j, b_kc), im);
-    } else {
-      // F+ rows take X = -(G, C) (even spin) or Y = (C.im, -C.re, -G.im, G.re); F- rows the other one
-      const bool use_x = (b_cc == 0) != (spin_odd != 0);
-      float4 pt[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const float2 Gv = ab[0][i], Cv = ab[NCOMP - 1][i];
-        float p0, p1, p2, p3;
-        if (use_x) { p0 = -Gv.x; p1 = -Gv.y; p2 = -Cv.x; p3 = -Cv.y; }
-        else { p0 = Cv.y; p1 = -Cv.x; p2 = -Gv.y; p3 = Gv.x; }
-        (&pt[0].x)[i] = p0; (&pt[1].x)[i] = p1; (&pt[2].x)[i] = p2; (&pt[3].x)[i] = p3;
-      }
-#pragma unroll
-      for (int part = 0; part < 4; ++part) {
-        const int row = part * gs + b_j;
-        st_split(c.smem, bh + kcore_off(row, b_kc), bl + kcore_off(row, b_kc), pt[part]);
-      }
-    }
-  };
-  for (int r = 0; r < NR; ++r) issue_raw(r);
-  load_alm(0);
-  bool ok = true, failed = false;
-  int mma_issued = 0;
-  for (int s = 0; s < nst; ++s) {
-    const int r = s / SPT, qq = s % SPT;
-    if (qq == 0) {
-      ok = ok && tab_wait(c.mbar_full + 8u * uint32_t(r % NR), uint32_t(r / NR) & 1u);
-      if (ok) raw_waited = r + 1;
-    }
-    if (ok) store(s);
-    tc::fence_proxy_async();
-    tc::fence_before_sync();
-    if (__syncthreads_or(!ok)) { failed = true; break; }
-    tc::fence_after_sync();
-    if (tid == 0) {
-      tab_mma<S>(c, s & 1, (s >> 1) & 1, (s & 1) == 0, idesc);
-      tc::mma_commit(c.mbar_mma + 8u * uint32_t(s & 1));
-    }
-    mma_issued = s + 1;
-    if (qq == SPT - 1) issue_raw(r + NR);  // half block r has been split (barrier above): refill its buffer
-    if (s + 1 < nst) load_alm(s + 1);
-    if (s >= 1) {
-      // MMAs of stage s - 1 complete: its operand buffer is free; drain D after the second stage of a period
-      const int sp = s - 1;
-      ok = ok && tab_wait(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u);
-      if (ok && (sp & 1)) {
-        tc::fence_after_sync();
-        tab_drain(c, (sp >> 1) & 1, n, sp == 1);
-      }
-    }
-  }
-  if (!failed) {
-    const int sp = nst - 1;
-    ok = ok && tab_wait(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u);
-    if (ok) {
+  bool ok = true;
+  int mma_issued = 0, raw_issued = 0;  // this warp's issued stages / half blocks (MMA and copy warps)
+
+  if (warp < WS_MMA_WARPS) {
+    // ---- MMA issue: stage s from operand buffer s & 1 into D[(s >> 1) & 1] (D period = 2 stages)
+    const TabIssuer is = tab_issuer<S>(c, warp);
+    for (int s = 0; s < nst && ok; ++s) {
+      const int p = s >> 1;
+      ok = ws_wait(pp, pp.op_full + 8u * uint32_t(s & 1), uint32_t(p & 1), err_flag);
+      if (ok && (s & 1) == 0 && p >= 2) ok = ws_wait(pp, pp.d_free + 8u * uint32_t(p & 1), uint32_t((p >> 1) - 1) & 1u, err_flag);
+      if (!ok) break;
       tc::fence_after_sync();
-      tab_drain(c, (sp >> 1) & 1, n, (sp >> 1) == 0);
+      tab_mma(is, s & 1, p & 1, (s & 1) == 0, idesc, pp.mma_done + 8u * uint32_t(s & 1));
+      if (s & 1) tc::mma_commit_elect(pp.d_ready + 8u * uint32_t(p & 1));
+      mma_issued = s + 1;
     }
-    tc::fence_before_sync();
-    if (__syncthreads_or(!ok)) failed = true;
-    tc::fence_after_sync();
+  } else if (warp == WS_COPY_WARP) {
+    // ---- bulk copies: half block r (block r >> 1, half r & 1) of the tile into staging buffer r % NR,
+    // its nvq padded units in one copy
+    for (int r = 0; r < nraw; ++r) {
+      if (r >= NR) {
+        ok = ws_wait(pp, pp.raw_free + 8u * uint32_t(r % NR), uint32_t((r / NR) - 1) & 1u, err_flag);
+        if (!ok) break;
+      }
+      const uint32_t bar = pp.full + 8u * uint32_t(r % NR);
+      if (lane == 0) {
+        tc::mbar_arrive_expect_tx(bar, uint32_t(nvq) * G::USTR * 4u);
+        if (nvq > 0)
+          tc::bulk_g2s(c.sbase + S::raw(r % NR), table + tab_unit_index(gb0 + (r >> 1), r & 1, nquads, q0) * G::USTR,
+                       uint32_t(nvq) * G::USTR * 4u, bar);
+      }
+      __syncwarp();
+      raw_issued = r + 1;
+    }
+  } else if (warp >= WS_PROD0 && warp < WS_PROD0 + WS_NPROD) {
+    // ---- operand producers (256 threads, pt = 0..255)
+    const int pt = tid - 32 * WS_PROD0;
+    // A: task pt (quad q = pt & 31, r = pt >> 5) loads 4 positions x 4 rings of quad q and stores them
+    // transposed: ring 4 q + i of the tile is A row 32 i + q (the 16-byte stores of eight consecutive
+    // lanes fall into eight different bank groups), K = 4 consecutive positions.
+    // spin 0: (parity p, group g) = (r >> 2, r & 3), positions 4 g + i -> A(acc p, ks g >> 1, kc g & 1);
+    // spin s (stage half qq): (comp cc, parity p, group g) = (r >> 2, (r >> 1) & 1, r & 1) at positions
+    // 8 qq + 4 g + i -> A(acc = p for F+, 1 - p for F-; ks cc, kc g)
+    int a_src;
+    uint32_t a_dst;
+    {
+      const int q = pt & 31, r = (pt >> 5) & 7;
+      int p, g, acc, ks, cc;
+      if (NOPS == 1) {
+        cc = 0; p = r >> 2; g = r & 3; acc = p; ks = g >> 1;
+      } else {
+        cc = r >> 2; p = (r >> 1) & 1; g = r & 1; acc = cc == 0 ? p : 1 - p; ks = cc;
+      }
+      a_src = q * G::USTR + ((cc * 2 + p) * 16 + 4 * g) * 4;  // spin s: + 32 qq
+      a_dst = uint32_t(((acc * 2 + ks) * 2) * S::A_TILE) + kcore_off(q, g & 1);  // row 32 i + q: + 1024 i
+    }
+    // B: tasks t = pt + 256 k < 8 gs (map j = t % gs, (acc, k4) = t / gs), 4 K values of 2 (spin 0) or
+    // 4 (spin s) rows.  K index 4 k4 + i of acc: spin 0 position 16 h + 4 k4 + i of parity acc;
+    // spin s comp cc = k4 >> 1 at position 16 h + 8 qq + 4 (k4 & 1) + i, parity acc (F+) or 1 - acc (F-)
+    bool b_v[BSL];
+    int b_j[BSL], b_acc[BSL], b_k4[BSL], b_lofs[BSL];
+#pragma unroll
+    for (int k = 0; k < BSL; ++k) {
+      const int t = pt + 256 * k;
+      b_v[k] = t < 8 * gs;
+      b_j[k] = b_v[k] ? t % gs : 0;
+      const int ak = b_v[k] ? t / gs : 0;
+      b_acc[k] = ak >> 2; b_k4[k] = ak & 3;
+      const int cc = NOPS == 1 ? 0 : b_k4[k] >> 1;
+      b_lofs[k] = NOPS == 1 ? 8 * b_k4[k] + b_acc[k] : 8 * (b_k4[k] & 1) + (cc == 0 ? b_acc[k] : 1 - b_acc[k]);
+    }
+    // the next stage's a_lm, loaded as FP64 and converted only when they are split (a conversion next
+    // to the load would wait for it and prefetch nothing)
+    double2 ab[BSL][NCOMP][4];
+    auto load_alm = [&](int s) {
+      const int r = s / SPT, qq = s % SPT, b = r >> 1, h = r & 1;
+#pragma unroll
+      for (int k = 0; k < BSL; ++k) {
+        const int l0 = m + TB_LB * b + 32 * h + 16 * qq + b_lofs[k];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int l = l0 + 2 * i;
+          const bool v = b_v[k] && l <= lmax;
+          const int64_t o = ((base + (l - m)) * B + b0 + b_j[k]) * NCOMP;
+#pragma unroll
+          for (int cc = 0; cc < NCOMP; ++cc) {
+            ab[k][cc][i] = v ? almT[o + cc] : make_double2(0.0, 0.0);
+          }
+        }
+      }
+    };
+    load_alm(0);
+    for (int s = 0; s < nst; ++s) {
+      const int r = s / SPT, qq = s % SPT, buf = s & 1;
+      if (qq == 0) ok = ws_wait(pp, pp.full + 8u * uint32_t(r % NR), uint32_t(r / NR) & 1u, err_flag);
+      if (ok && s >= 2) ok = ws_wait(pp, pp.mma_done + 8u * uint32_t(buf), uint32_t((s - 2) >> 1) & 1u, err_flag);
+      if (!ok) break;
+      {  // A
+        const float* u = reinterpret_cast<const float*>(c.smem + S::raw(r % NR)) + a_src + 32 * qq;
+        float4 v[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[i] = reinterpret_cast<const float4*>(u)[i];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          // ring i of the quad: its values at the 4 positions
+          const float4 w = make_float4((&v[0].x)[i], (&v[1].x)[i], (&v[2].x)[i], (&v[3].x)[i]);
+          const uint32_t d = S::a(buf, 0, 0, 0) + a_dst + uint32_t(i) * kcore_off(32, 0);
+          st_split(c.smem, d, d + S::A_TILE, w);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < BSL; ++k) {  // B
+        if (!b_v[k]) continue;
+        const int ks = b_k4[k] >> 1, kc = b_k4[k] & 1, j = b_j[k];
+        const uint32_t bh = S::b(buf, b_acc[k], ks, 0), bl = S::b(buf, b_acc[k], ks, 1);
+        if (NOPS == 1) {
+          const float4 re = make_float4(float(ab[k][0][0].x), float(ab[k][0][1].x), float(ab[k][0][2].x),
+                                        float(ab[k][0][3].x));
+          const float4 im = make_float4(float(ab[k][0][0].y), float(ab[k][0][1].y), float(ab[k][0][2].y),
+                                        float(ab[k][0][3].y));
+          st_split(c.smem, bh + kcore_off(j, kc), bl + kcore_off(j, kc), re);
+          st_split(c.smem, bh + kcore_off(gs + j, kc), bl + kcore_off(gs + j, kc), im);
+        } else {
+          // F+ rows take X = -(G, C) (even spin) or Y = (C.im, -C.re, -G.im, G.re); F- rows the other one
+          const bool use_x = ((b_k4[k] >> 1) == 0) != (spin_odd != 0);
+          float4 pt4[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float2 Gv = make_float2(float(ab[k][0][i].x), float(ab[k][0][i].y));
+            const float2 Cv = make_float2(float(ab[k][NCOMP - 1][i].x), float(ab[k][NCOMP - 1][i].y));
+            float p0, p1, p2, p3;
+            if (use_x) { p0 = -Gv.x; p1 = -Gv.y; p2 = -Cv.x; p3 = -Cv.y; }
+            else { p0 = Cv.y; p1 = -Cv.x; p2 = -Gv.y; p3 = Gv.x; }
+            (&pt4[0].x)[i] = p0; (&pt4[1].x)[i] = p1; (&pt4[2].x)[i] = p2; (&pt4[3].x)[i] = p3;
+          }
+#pragma unroll
+          for (int part = 0; part < 4; ++part) {
+            const int row = part * gs + j;
+            st_split(c.smem, bh + kcore_off(row, kc), bl + kcore_off(row, kc), pt4[part]);
+          }
+        }
+      }
+      tc::fence_proxy_async();  // the operand stores, visible to the tensor core
+      ws_arrive(pp.op_full + 8u * uint32_t(buf));
+      if (qq == SPT - 1) ws_arrive(pp.raw_free + 8u * uint32_t(r % NR));  // half block r has been read
+      if (s + 1 < nst) load_alm(s + 1);
+    }
+  } else if (warp >= WS_DRAIN0) {
+    // ---- drain: S += D of each D period (first period: S = D), this warp's TMEM lane quarter,
+    // all columns, two 16-column units per wait
+    const uint32_t lane_addr = c.tmem + (uint32_t((warp & 3) * 32) << 16);
+    const int nu = n >> 3;  // units u = (chunk u >> 1, accumulator u & 1)
+    const int npairs = nst >> 1;
+    for (int p = 0; p < npairs; ++p) {
+      ok = ws_wait(pp, pp.d_ready + 8u * uint32_t(p & 1), uint32_t(p >> 1) & 1u, err_flag);
+      if (!ok) break;
+      tc::fence_after_sync();
+      const bool first = p == 0;
+#pragma unroll 1
+      for (int u = 0; u < nu; u += 2) {
+        float d0[16], d1[16], s0[16], s1[16];
+        const bool two = u + 1 < nu;
+        const uint32_t dc0 = lane_addr + tcol_d(p & 1, u & 1) + uint32_t(16 * (u >> 1));
+        const uint32_t sc0 = lane_addr + tcol_s(u & 1) + uint32_t(16 * (u >> 1));
+        const uint32_t dc1 = lane_addr + tcol_d(p & 1, (u + 1) & 1) + uint32_t(16 * ((u + 1) >> 1));
+        const uint32_t sc1 = lane_addr + tcol_s((u + 1) & 1) + uint32_t(16 * ((u + 1) >> 1));
+        tc::tmem_ld16(dc0, d0);
+        if (!first) tc::tmem_ld16(sc0, s0);
+        if (two) {
+          tc::tmem_ld16(dc1, d1);
+          if (!first) tc::tmem_ld16(sc1, s1);
+        }
+        tc::tmem_ld_wait();
+        if (!first) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) { d0[q] += s0[q]; d1[q] += s1[q]; }
+        }
+        tmem_st16(sc0, d0);
+        if (two) tmem_st16(sc1, d1);
+      }
+      tmem_st_wait();
+      tc::fence_before_sync();
+      ws_arrive(pp.d_free + 8u * uint32_t(p & 1));
+    }
   }
+  // every role has finished (or given up)
+  tc::fence_before_sync();
+  const bool failed = __syncthreads_or(!ok) != 0;
+  tc::fence_after_sync();
   if (!failed) {
     // epilogue.  TMEM lane tl = 32 lq + q <-> ring 4 q + lq of the tile (lq = warp & 3).  The sums go
-    // through shared memory (free now) as rows [north/south][lane][map][part], then each ring's row of
-    // gs maps is written with coalesced stores
+    // through shared memory (free now: every MMA and copy has completed) as rows [north/south][lane]
+    // [map][part], then every ring's row of gs maps is written with coalesced stores
     constexpr int RS = TB_NMAX + 1;  // row stride (floats): consecutive lanes in consecutive banks
     static_assert(2 * 128 * RS * 4 <= int(S::MISC_OFF), "epilogue rows exceed the free shared memory");
     float* rows = reinterpret_cast<float*>(c.smem);
@@ -612,7 +751,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
     for (int row = warp; row < 256; row += TM_THREADS / 32) {
       const int ns = row >> 7, t = row & 127;
       const int rt = 4 * q0 + 4 * (t & 31) + (t >> 5);  // table ring of TMEM lane t
-      const int i = rt - toff;    // ring pair of the plan
+      const int i = rt - toff;                          // ring pair of the plan
       if (rt < toff || i >= nrp) continue;
       const int ring = ns == 0 ? i : R - 1 - i;
       if (ns == 1 && ring == i) continue;  // the equator has no south ring
@@ -620,15 +759,14 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
       const float* src = rows + row * RS;
       for (int pos = lane; pos < ncols; pos += 32) dst[pos] = src[pos];
     }
-  } else if (tid == 0) {
-    atomicExch(err_flag, 1);
-    // MMAs and bulk copies still in flight touch this CTA's memory: wait for them (bounded) before exit
-    if (mma_issued > 0) {
-      const int sp = mma_issued - 1;
-      tc::mbar_wait_bounded(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u, TB_WAIT_LIMIT);
-    }
-    for (int k = raw_waited; k < raw_issued; ++k)
-      tc::mbar_wait_bounded(c.mbar_full + 8u * uint32_t(k % NR), uint32_t(k / NR) & 1u, TB_WAIT_LIMIT);
+  } else if (lane == 0 && warp < WS_MMA_WARPS && mma_issued > 0) {
+    // the issued MMAs read this CTA's shared memory and write its TMEM: wait (bounded) for them
+    const int sp = mma_issued - 1;
+    tc::mbar_wait_bounded(pp.mma_done + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u, TB_WAIT_LIMIT);
+  } else if (lane == 0 && warp == WS_COPY_WARP) {
+    // copies in flight land in this CTA's shared memory: wait (bounded) for the last NR
+    for (int k = max(0, raw_issued - NR); k < raw_issued; ++k)
+      tc::mbar_wait_bounded(pp.full + 8u * uint32_t(k % NR), uint32_t(k / NR) & 1u, TB_WAIT_LIMIT);
   }
   tab_end<S>(c);
 }
@@ -642,7 +780,8 @@ struct AdjCfg {
   static constexpr int UNIT = tab_unit_floats(NOPS);
   static constexpr int NQ = NOPS == 1 ? 4 : 2;  // quads per stage
   static constexpr int RSTAGE = 4 * NQ;         // rings per stage
-  static constexpr uint32_t TAB_BYTES = 8u * NQ * UNIT * 4u;
+  static constexpr int USTR = tab_unit_stride(NOPS);
+  static constexpr uint32_t TAB_BYTES = 8u * NQ * USTR * 4u;
   static constexpr int PH_MAPS = TB_NMAX / 4;   // maps per group (spin s)
   static constexpr uint32_t PH_BYTES = NOPS == 2 ? 2u * RSTAGE * PH_MAPS * 16u : 0u;
   static constexpr uint32_t RAW = TAB_BYTES + PH_BYTES;
@@ -682,6 +821,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
   const uint32_t idesc = tc::idesc_tf32(128, n, 0, 0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   TabCta c = tab_begin<S>(tab_smem_raw);
+  const TabIssuer is = tab_issuer<S>(c, warp & 1);
   const int nb = tab_nblocks(m, lmax);
   const int nblk = min(4, nb - bb);
   const int R = 2 * nrp - 1;
@@ -689,16 +829,16 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
   const int nst = (rt_end - rt_begin + RSTAGE - 1) / RSTAGE;
   const int64_t gb0 = blockoff[m] + bb;
   int raw_issued = 0, raw_waited = 0;  // stages whose copies were issued / waited for (uniform)
-  // bulk copies of stage st into staging buffer st % NR (warp 0: lane 2 blk + h the units of block
-  // blk, half h; spin s: lane r < RSTAGE the phase rows of ring r of the stage)
+  // bulk copies of stage st into staging buffer st % NR (lane 2 blk + h: the units of block
+  // blk, half h; spin s: lane r < RSTAGE the phase rows of ring r of the stage); warp TB_COPY_WARP
   auto issue_raw = [&](int st) {
     if (st >= nst) return;
     raw_issued = st + 1;
-    if (warp != 0) return;
+    if (warp != TB_COPY_WARP) return;
     const int rs0 = rt_begin + st * RSTAGE;
     const int qs = rs0 / 4;
     const int nvq = max(0, min(NQ, nquads - qs));
-    uint32_t tx = uint32_t(nblk * 2 * nvq) * UNIT * 4u;
+    uint32_t tx = uint32_t(nblk * 2 * nvq) * G::USTR * 4u;
     const int ip = rs0 + lane - toff;
     const bool ph_n = NOPS == 2 && lane < RSTAGE && ip >= 0 && ip < nrp;
     const bool ph_s = ph_n && R - 1 - ip != ip;
@@ -710,8 +850,8 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
     if (lane == 0) tc::mbar_arrive_expect_tx(bar, tx);
     __syncwarp();  // the transaction count is expected before any copy lands
     if (lane < 8 && (lane >> 1) < nblk && nvq > 0)
-      tc::bulk_g2s(dst + uint32_t(lane * NQ * UNIT) * 4u,
-                   table + tab_unit_index(gb0 + (lane >> 1), lane & 1, nquads, qs) * UNIT, uint32_t(nvq) * UNIT * 4u,
+      tc::bulk_g2s(dst + uint32_t(lane * NQ * G::USTR) * 4u,
+                   table + tab_unit_index(gb0 + (lane >> 1), lane & 1, nquads, qs) * G::USTR, uint32_t(nvq) * G::USTR * 4u,
                    bar);
     if (NOPS == 2) {
       const uint32_t pd = dst + G::TAB_BYTES + uint32_t(lane) * G::PH_MAPS * 16u;
@@ -725,11 +865,12 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
   // = (block, half, quad qd), element (comp cc, parity p, position jj) of the unit -> A(acc p), row
   // 32 block + 16 half + jj, K chunk cc NQ + qd (four rings)
   uint32_t a_dst[2];
-  int a_qd[2];
+  int a_qd[2], a_src[2];
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
     const int t = tid + TM_THREADS * i;
     const int u = t / (32 * NOPS), w = t % (32 * NOPS);
+    a_src[i] = u * G::USTR + 4 * w;  // padded unit u of the staged runs
     const int cc = w >> 5, p = (w >> 4) & 1, jj = w & 15;
     const int qd = u % NQ, bh = u / NQ, h = bh & 1, blk = bh >> 1;
     const int row = blk * 32 + 16 * h + jj, kq = cc * NQ + qd;
@@ -764,7 +905,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
     for (int i = 0; i < 2; ++i) {
       // quads beyond the table were not copied: their rings contribute nothing
       float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (a_qd[i] < nvq) v = *reinterpret_cast<const float4*>(raw + 4 * (tid + TM_THREADS * i));
+      if (a_qd[i] < nvq) v = *reinterpret_cast<const float4*>(raw + a_src[i]);
       const uint32_t d = S::a(buf, 0, 0, 0) + a_dst[i];
       st_split(c.smem, d, d + S::A_TILE, v);
     }
@@ -837,10 +978,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
     tc::fence_before_sync();
     if (__syncthreads_or(!ok)) { failed = true; break; }
     tc::fence_after_sync();
-    if (tid == 0) {
-      tab_mma<S>(c, st & 1, (st >> 1) & 1, (st & 1) == 0, idesc);
-      tc::mma_commit(c.mbar_mma + 8u * uint32_t(st & 1));
-    }
+    if (warp < 2) tab_mma(is, st & 1, (st >> 1) & 1, (st & 1) == 0, idesc, c.mbar_mma + 8u * uint32_t(st & 1));
     mma_issued = st + 1;
     issue_raw(st + NR);  // staging buffer st % NR has been read (barrier above)
     if (st + 1 < nst) load_phase(st + 1);
@@ -933,7 +1071,8 @@ void tab_blockoff(int lmax, int mmax, std::vector<int64_t>& off) {
 int tab_quads(int Rh) { return ((Rh + TB_TILE - 1) / TB_TILE) * TB_TILE / 4; }
 
 size_t tab_bytes(int Rh, int lmax, int mmax, int spin) {
-  return size_t(tab_total_blocks(lmax, mmax)) * size_t(tab_quads(Rh)) * size_t(spin == 0 ? 1 : 2) * TB_LB * 4 *
+  // two half-block units per block and quad, each padded
+  return size_t(tab_total_blocks(lmax, mmax)) * size_t(tab_quads(Rh)) * 2 * size_t(tab_unit_stride(spin == 0 ? 1 : 2)) *
          sizeof(float);
 }
 
@@ -941,13 +1080,13 @@ int launch_tab_gen(const Plan& P, int spin, const int64_t* d_blockoff, float* ta
   const int nquads = tab_quads(P.Rh);
   dim3 grid(nquads * 4 / TB_TILE, P.mmax + 1);
   if (spin == 0) {
-    const int smem = 2 * 32 * (tab_unit_floats(1) + 4) * sizeof(float);
+    const int smem = 2 * 32 * tab_unit_stride(1) * sizeof(float);
     if (set_smem_attr((const void*)tab_gen_kernel<1>, smem)) return PS_ERR_CUDA;
     tab_gen_kernel<1><<<grid, TB_THREADS, smem, st>>>(P.d_rings, P.d_mnorm0, nullptr, P.Rh, P.lmax, 0, d_blockoff,
                                                       nquads, table);
   } else {
     if (!P.d_seed[spin]) return PS_ERR_INVALID;
-    const int smem = 2 * 32 * (tab_unit_floats(2) + 4) * sizeof(float);
+    const int smem = 2 * 32 * tab_unit_stride(2) * sizeof(float);
     if (set_smem_attr((const void*)tab_gen_kernel<2>, smem)) return PS_ERR_CUDA;
     tab_gen_kernel<2><<<grid, TB_THREADS, smem, st>>>(P.d_rings, nullptr, P.d_seed[spin], P.Rh, P.lmax, spin,
                                                       d_blockoff, nquads, table);

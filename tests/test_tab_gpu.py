@@ -103,16 +103,18 @@ def test_table_band_plan_vs_fp64(nside, lmax, k, spin):
 
 @pytest.mark.gpu
 def test_table_sizes_and_refusals():
-    """Table bytes follow Rh (rounded up to 128) x table blocks x 64 l x 4 bytes (x2 for spin s);
-    FP64 plans refuse a table; dropping the tables returns the transforms to the on-the-fly kernels."""
+    """Table bytes: per table block and quad of rings (Rh rounded up to 128), two half-block units of
+    (ncomp x 2 parities x 16 positions x 4 rings) FP32 values plus 16 bytes of padding; FP64 plans refuse
+    a table; dropping the tables returns the transforms to the on-the-fly kernels."""
     import torch
     from polyspec_b200 import _lib
     from polyspec_b200.sht import SHTPlan
     nside, lmax = 32, 70
     pmx = SHTPlan(nside, lmax, prec="mixed", autotune=False, tables=False)
     nblk = sum((lmax - m) // 64 + 1 for m in range(lmax + 1))
-    assert pmx.table_bytes(0) == nblk * 128 * 64 * 4
-    assert pmx.table_bytes(2) == 2 * nblk * 128 * 64 * 4
+    nquads = 128 // 4
+    assert pmx.table_bytes(0) == nblk * nquads * 2 * (1 * 128 + 4) * 4
+    assert pmx.table_bytes(2) == nblk * nquads * 2 * (2 * 128 + 4) * 4
     p64 = SHTPlan(nside, lmax, prec="fp64", autotune=False)
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     assert _lib.lib().ps_plan_build_table(p64._h, 0, st) == _lib.PS_ERR_UNSUPPORTED
