@@ -75,8 +75,6 @@ constexpr int TB_TILE = 128;     // ring pairs per synthesis tile (MMA M)
 constexpr int TB_THREADS = 128;  // table generation
 constexpr int TM_THREADS = 512;  // the two GEMMs: 16 warps, 4 per TMEM lane quarter
 constexpr uint32_t TB_WAIT_LIMIT = 1u << 24;
-// the warp that issues the bulk copies: not one of the two MMA-issuing warps (0 and 1)
-constexpr int TB_COPY_WARP = 2;
 
 // ------------------------------------------------------------------ table geometry
 // number of table blocks of order m
@@ -262,8 +260,8 @@ __device__ __forceinline__ int round16(int x) { return (x + 15) & ~15; }
 
 // Shared memory of one GEMM CTA.  Operand tiles, double-buffered by stage parity:
 // A [buf][acc][ks][hi/lo] 4 KB each (128 rows x 8 K), B [buf][acc][ks][hi/lo] TB_NMAX x 32 B each;
-// then NR staging buffers of RAW bytes for the bulk copies, then the barriers:
-// mbar_mma[2] (MMAs of the stages of that parity complete), mbar_full[NR] (staging buffer filled).
+// then NR staging buffers of RAW bytes for the bulk copies, then the pipeline's barriers, an abort
+// flag and the TMEM slot (TabPipe).
 template <uint32_t RAW, int NR_>
 struct TabSmem {
   static constexpr int NR = NR_;
@@ -295,35 +293,8 @@ __device__ __forceinline__ uint32_t tcol_s(int acc) { return uint32_t((4 + acc) 
 struct TabCta {
   uint8_t* smem;
   uint32_t sbase;
-  uint32_t mbar_mma;   // + 8 * (stage & 1)
-  uint32_t mbar_full;  // + 8 * staging buffer
   uint32_t tmem;
 };
-
-template <class S>
-__device__ __forceinline__ TabCta tab_begin(uint8_t* smem_raw) {
-  TabCta c;
-  c.smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  c.sbase = tc::smem_u32(c.smem);
-  c.mbar_mma = c.sbase + S::MISC_OFF;
-  c.mbar_full = c.sbase + S::MISC_OFF + 16;
-  uint32_t* slot = reinterpret_cast<uint32_t*>(c.smem + S::MISC_OFF + 96);
-  if ((threadIdx.x >> 5) == 0) {
-    tc::tmem_alloc(tc::smem_u32(slot), S::TMEM_COLS);
-    tc::tmem_relinquish();
-  }
-  if (threadIdx.x == 0) {
-    tc::mbar_init(c.mbar_mma, 2);  // one commit from each issuing warp
-    tc::mbar_init(c.mbar_mma + 8, 2);
-    for (int i = 0; i < S::NR; ++i) tc::mbar_init(c.mbar_full + 8u * uint32_t(i), 1);
-    tc::fence_mbar_init();
-  }
-  tc::fence_before_sync();
-  __syncthreads();
-  tc::fence_after_sync();
-  c.tmem = *slot;
-  return c;
-}
 
 template <class S>
 __device__ __forceinline__ void tab_end(const TabCta& c) {
@@ -375,40 +346,11 @@ __device__ __forceinline__ void tab_mma(const TabIssuer& is, int buf, int dbuf, 
   tc::mma_commit_elect(bar);
 }
 
-// S += D[dbuf] (first D period: S = D) for this thread's TMEM lane, columns [0, n) of both
-// accumulators.  Unit u = (16-column chunk u >> 1, accumulator u & 1); the four warps that share
-// a TMEM lane quarter take every fourth unit
-__device__ __forceinline__ void tab_drain(const TabCta& c, int dbuf, int n, bool first) {
-  const uint32_t lane_addr = c.tmem + (uint32_t(((threadIdx.x >> 5) & 3) * 32) << 16);
-  const int nu = n >> 3;
-#pragma unroll 1
-  for (int u = int(threadIdx.x >> 7); u < nu; u += TM_THREADS / 128) {
-    float d[16], sm[16];
-    const int acc = u & 1, cb = 16 * (u >> 1);
-    const uint32_t dc = lane_addr + tcol_d(dbuf, acc) + uint32_t(cb);
-    const uint32_t sc = lane_addr + tcol_s(acc) + uint32_t(cb);
-    tc::tmem_ld16(dc, d);
-    if (!first) tc::tmem_ld16(sc, sm);
-    tc::tmem_ld_wait();
-    if (!first) {
-#pragma unroll
-      for (int q = 0; q < 16; ++q) d[q] += sm[q];
-    }
-    tmem_st16(sc, d);
-  }
-  tmem_st_wait();
-}
-
 // the S columns [cb, cb + 16) of accumulator acc of this thread's lane
 __device__ __forceinline__ void tab_read_sum(const TabCta& c, int acc, int cb, float* v) {
   const uint32_t lane_addr = c.tmem + (uint32_t(((threadIdx.x >> 5) & 3) * 32) << 16);
   tc::tmem_ld16(lane_addr + tcol_s(acc) + uint32_t(cb), v);
   tc::tmem_ld_wait();
-}
-
-// bounded wait, uniform over the warp (false: the limit was reached by some lane)
-__device__ __forceinline__ bool tab_wait(uint32_t mbar, uint32_t parity) {
-  return __all_sync(0xffffffffu, tc::mbar_wait_bounded(mbar, parity, TB_WAIT_LIMIT)) != 0;
 }
 
 // ---- warp-specialised pipeline (synthesis).  Barriers at the start of the misc area, 8 bytes each:
@@ -435,8 +377,6 @@ __device__ __forceinline__ TabCta tab_begin_ws(uint8_t* smem_raw, TabPipe& pp) {
   pp.full = misc; pp.raw_free = misc + 64; pp.op_full = misc + 128; pp.mma_done = misc + 144;
   pp.d_ready = misc + 160; pp.d_free = misc + 176;
   pp.abort = reinterpret_cast<volatile int*>(c.smem + S::MISC_OFF + 192);
-  c.mbar_mma = pp.mma_done;
-  c.mbar_full = pp.full;
   uint32_t* slot = reinterpret_cast<uint32_t*>(c.smem + S::MISC_OFF + 224);
   if ((threadIdx.x >> 5) == 0) {
     tc::tmem_alloc(tc::smem_u32(slot), S::TMEM_COLS);
@@ -508,7 +448,6 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_synth_kernel(const float* _
   using G = SynthCfg<NOPS>;
   using S = TabSmem<G::RAW, G::NR>;
   constexpr int NCOMP = NOPS;
-  constexpr int UNIT = G::UNIT;
   constexpr int SPT = G::SPT;
   constexpr int NR = G::NR;
   constexpr int BSL = NOPS == 1 ? 2 : 1;  // B task slots per producer thread (8 gs <= 320 or 160)
@@ -785,7 +724,7 @@ struct AdjCfg {
   static constexpr int PH_MAPS = TB_NMAX / 4;   // maps per group (spin s)
   static constexpr uint32_t PH_BYTES = NOPS == 2 ? 2u * RSTAGE * PH_MAPS * 16u : 0u;
   static constexpr uint32_t RAW = TAB_BYTES + PH_BYTES;
-  static constexpr int NR = 4;
+  static constexpr int NR = NOPS == 1 ? 7 : 5;  // as many as shared memory holds
 };
 
 // phase [R][mmax+1][B][NOPS] complex64 of ring pairs [0, nrp) -> alm of map b at alm + b * out_stride
@@ -805,7 +744,6 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
   using G = AdjCfg<NOPS>;
   using S = TabSmem<G::RAW, G::NR>;
   constexpr int NCOMP = NOPS;
-  constexpr int UNIT = G::UNIT;
   constexpr int NQ = G::NQ;
   constexpr int RSTAGE = G::RSTAGE;
   constexpr int NR = G::NR;
@@ -820,189 +758,221 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
   const int n = round16(ncols);
   const uint32_t idesc = tc::idesc_tf32(128, n, 0, 0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  TabCta c = tab_begin<S>(tab_smem_raw);
-  const TabIssuer is = tab_issuer<S>(c, warp & 1);
+  TabPipe pp;
+  TabCta c = tab_begin_ws<S>(tab_smem_raw, pp);
   const int nb = tab_nblocks(m, lmax);
   const int nblk = min(4, nb - bb);
   const int R = 2 * nrp - 1;
   const int rt_begin = toff & ~3, rt_end = toff + nrp;
   const int nst = (rt_end - rt_begin + RSTAGE - 1) / RSTAGE;
+  const int npairs = (nst + 1) >> 1;  // D periods (the last may hold one stage)
   const int64_t gb0 = blockoff[m] + bb;
-  int raw_issued = 0, raw_waited = 0;  // stages whose copies were issued / waited for (uniform)
-  // bulk copies of stage st into staging buffer st % NR (lane 2 blk + h: the units of block
-  // blk, half h; spin s: lane r < RSTAGE the phase rows of ring r of the stage); warp TB_COPY_WARP
-  auto issue_raw = [&](int st) {
-    if (st >= nst) return;
-    raw_issued = st + 1;
-    if (warp != TB_COPY_WARP) return;
-    const int rs0 = rt_begin + st * RSTAGE;
-    const int qs = rs0 / 4;
-    const int nvq = max(0, min(NQ, nquads - qs));
-    uint32_t tx = uint32_t(nblk * 2 * nvq) * G::USTR * 4u;
-    const int ip = rs0 + lane - toff;
-    const bool ph_n = NOPS == 2 && lane < RSTAGE && ip >= 0 && ip < nrp;
-    const bool ph_s = ph_n && R - 1 - ip != ip;
-    const uint32_t row_bytes = uint32_t(gs) * 16u;
-    if (NOPS == 2)
-      tx += uint32_t(__popc(__ballot_sync(0xffffffffu, ph_n)) + __popc(__ballot_sync(0xffffffffu, ph_s))) * row_bytes;
-    const uint32_t bar = c.mbar_full + 8u * uint32_t(st % NR);
-    const uint32_t dst = c.sbase + S::raw(st % NR);
-    if (lane == 0) tc::mbar_arrive_expect_tx(bar, tx);
-    __syncwarp();  // the transaction count is expected before any copy lands
-    if (lane < 8 && (lane >> 1) < nblk && nvq > 0)
-      tc::bulk_g2s(dst + uint32_t(lane * NQ * G::USTR) * 4u,
-                   table + tab_unit_index(gb0 + (lane >> 1), lane & 1, nquads, qs) * G::USTR, uint32_t(nvq) * G::USTR * 4u,
-                   bar);
-    if (NOPS == 2) {
-      const uint32_t pd = dst + G::TAB_BYTES + uint32_t(lane) * G::PH_MAPS * 16u;
-      if (ph_n) tc::bulk_g2s(pd, phase + ((int64_t(ip) * (mmax + 1) + m) * B + b0) * NCOMP, row_bytes, bar);
-      if (ph_s)
-        tc::bulk_g2s(pd + uint32_t(RSTAGE) * G::PH_MAPS * 16u,
-                     phase + ((int64_t(R - 1 - ip) * (mmax + 1) + m) * B + b0) * NCOMP, row_bytes, bar);
+  bool ok = true;
+  int mma_issued = 0, raw_issued = 0;  // this warp's issued stages (MMA and copy warps)
+
+  if (warp < WS_MMA_WARPS) {
+    // ---- MMA issue: stage st from operand buffer st & 1 into D[(st >> 1) & 1]
+    const TabIssuer is = tab_issuer<S>(c, warp);
+    for (int st = 0; st < nst; ++st) {
+      const int p = st >> 1;
+      ok = ws_wait(pp, pp.op_full + 8u * uint32_t(st & 1), uint32_t(p & 1), err_flag);
+      if (ok && (st & 1) == 0 && p >= 2) ok = ws_wait(pp, pp.d_free + 8u * uint32_t(p & 1), uint32_t((p >> 1) - 1) & 1u, err_flag);
+      if (!ok) break;
+      tc::fence_after_sync();
+      tab_mma(is, st & 1, p & 1, (st & 1) == 0, idesc, pp.mma_done + 8u * uint32_t(st & 1));
+      if ((st & 1) || st == nst - 1) tc::mma_commit_elect(pp.d_ready + 8u * uint32_t(p & 1));
+      mma_issued = st + 1;
     }
-  };
-  // ---- A: this thread splits float4 t = tid + 512 i (i = 0, 1) of the stage's 1024: unit u = t / (32 NOPS)
-  // = (block, half, quad qd), element (comp cc, parity p, position jj) of the unit -> A(acc p), row
-  // 32 block + 16 half + jj, K chunk cc NQ + qd (four rings)
-  uint32_t a_dst[2];
-  int a_qd[2], a_src[2];
-#pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const int t = tid + TM_THREADS * i;
-    const int u = t / (32 * NOPS), w = t % (32 * NOPS);
-    a_src[i] = u * G::USTR + 4 * w;  // padded unit u of the staged runs
-    const int cc = w >> 5, p = (w >> 4) & 1, jj = w & 15;
-    const int qd = u % NQ, bh = u / NQ, h = bh & 1, blk = bh >> 1;
-    const int row = blk * 32 + 16 * h + jj, kq = cc * NQ + qd;
-    a_qd[i] = qd;
-    a_dst[i] = uint32_t(((p * 2 + (kq >> 1)) * 2) * S::A_TILE) + kcore_off(row, kq & 1);
-  }
-  // ---- B.  spin 0: task t = tid < NQ gs (map j = t % gs, quad qd = t / gs), phases of its 4 rings
-  // loaded into registers a stage ahead.  spin s: task t = tid (acc = (t >> 1) & 1, comp cc = t & 1,
-  // map j = (t >> 2) % gs, quad qd = (t >> 2) / gs), NQ gs <= 40, phases read from the staged rows
-  const int p_t = NOPS == 1 ? tid : tid >> 2;
-  const bool p_v = p_t < NQ * gs;
-  const int p_j = p_v ? p_t % gs : 0, p_qd = p_v ? p_t / gs : 0;
-  float2 pn[4], pv[4];
-  auto load_phase = [&](int st) {
-    if (NOPS != 1) return;
-    const int rs0 = rt_begin + st * RSTAGE;
+  } else if (warp == WS_COPY_WARP) {
+    // ---- bulk copies of stage st into staging buffer st % NR: lane 2 blk + h the units of block blk,
+    // half h; spin s: lane r < RSTAGE the north and south phase rows of ring r of the stage
+    for (int st = 0; st < nst; ++st) {
+      if (st >= NR) {
+        ok = ws_wait(pp, pp.raw_free + 8u * uint32_t(st % NR), uint32_t((st / NR) - 1) & 1u, err_flag);
+        if (!ok) break;
+      }
+      const int rs0 = rt_begin + st * RSTAGE;
+      const int qs = rs0 / 4;
+      const int nvq = max(0, min(NQ, nquads - qs));
+      uint32_t tx = uint32_t(nblk * 2 * nvq) * G::USTR * 4u;
+      const int ip = rs0 + lane - toff;
+      const bool ph_n = NOPS == 2 && lane < RSTAGE && ip >= 0 && ip < nrp;
+      const bool ph_s = ph_n && R - 1 - ip != ip;
+      const uint32_t row_bytes = uint32_t(gs) * 16u;
+      if (NOPS == 2)
+        tx += uint32_t(__popc(__ballot_sync(0xffffffffu, ph_n)) + __popc(__ballot_sync(0xffffffffu, ph_s))) * row_bytes;
+      const uint32_t bar = pp.full + 8u * uint32_t(st % NR);
+      const uint32_t dst = c.sbase + S::raw(st % NR);
+      if (lane == 0) tc::mbar_arrive_expect_tx(bar, tx);
+      __syncwarp();  // the transaction count is expected before any copy lands
+      if (lane < 8 && (lane >> 1) < nblk && nvq > 0)
+        tc::bulk_g2s(dst + uint32_t(lane * NQ * G::USTR) * 4u,
+                     table + tab_unit_index(gb0 + (lane >> 1), lane & 1, nquads, qs) * G::USTR,
+                     uint32_t(nvq) * G::USTR * 4u, bar);
+      if (NOPS == 2) {
+        const uint32_t pd = dst + G::TAB_BYTES + uint32_t(lane) * G::PH_MAPS * 16u;
+        if (ph_n) tc::bulk_g2s(pd, phase + ((int64_t(ip) * (mmax + 1) + m) * B + b0) * NCOMP, row_bytes, bar);
+        if (ph_s)
+          tc::bulk_g2s(pd + uint32_t(RSTAGE) * G::PH_MAPS * 16u,
+                       phase + ((int64_t(R - 1 - ip) * (mmax + 1) + m) * B + b0) * NCOMP, row_bytes, bar);
+      }
+      raw_issued = st + 1;
+    }
+  } else if (warp >= WS_PROD0 && warp < WS_PROD0 + WS_NPROD) {
+    // ---- operand producers (256 threads, pt = 0..255)
+    const int pt = tid - 32 * WS_PROD0;
+    // A: float4 t = pt + 256 i (i = 0..3) of the stage's 1024: unit u = t / (32 NOPS) = (block, half,
+    // quad qd) of the staged runs, element (comp cc, parity p, position jj) -> A(acc p), row
+    // 32 block + 16 half + jj, K chunk cc NQ + qd (four rings)
+    uint32_t a_dst[4];
+    int a_qd[4], a_src[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const int ip = rs0 + 4 * p_qd + i - toff;
-      const bool in = p_v && ip >= 0 && ip < nrp;
-      const int rsth = R - 1 - ip;
-      pn[i] = in ? phase[(int64_t(ip) * (mmax + 1) + m) * B + b0 + p_j] : make_float2(0.f, 0.f);
-      pv[i] = (in && rsth != ip) ? phase[(int64_t(rsth) * (mmax + 1) + m) * B + b0 + p_j] : make_float2(0.f, 0.f);
+      const int t = pt + 256 * i;
+      const int u = t / (32 * NOPS), w = t % (32 * NOPS);
+      a_src[i] = u * G::USTR + 4 * w;  // padded unit u of the staged runs
+      const int cc = w >> 5, p = (w >> 4) & 1, jj = w & 15;
+      const int qd = u % NQ, bh = u / NQ, h = bh & 1, blk = bh >> 1;
+      const int row = blk * 32 + 16 * h + jj, kq = cc * NQ + qd;
+      a_qd[i] = qd;
+      a_dst[i] = uint32_t(((p * 2 + (kq >> 1)) * 2) * S::A_TILE) + kcore_off(row, kq & 1);
     }
-  };
-  auto store = [&](int st) {
-    const int buf = st & 1;
-    const int rs0 = rt_begin + st * RSTAGE;
-    const int nvq = max(0, min(NQ, nquads - rs0 / 4));
-    const float* raw = reinterpret_cast<const float*>(c.smem + S::raw(st % NR));
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      // quads beyond the table were not copied: their rings contribute nothing
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (a_qd[i] < nvq) v = *reinterpret_cast<const float4*>(raw + a_src[i]);
-      const uint32_t d = S::a(buf, 0, 0, 0) + a_dst[i];
-      st_split(c.smem, d, d + S::A_TILE, v);
-    }
-    if (!p_v) return;
-    const int j = p_j, qd = p_qd;
-    if (NOPS == 1) {
-      // ring sums (accumulator 0: N + S) and differences (accumulator 1: N - S) of 4 rings
-      float4 cre[2], cim[2];
+    // B.  spin 0: task pt < NQ gs (map j = pt % gs, quad qd = pt / gs), phases of its 4 rings loaded
+    // into registers a stage ahead.  spin s: task pt (acc = (pt >> 1) & 1, comp cc = pt & 1, map
+    // j = (pt >> 2) % gs, quad qd = (pt >> 2) / gs), NQ gs <= 40, phases read from the staged rows
+    const int p_t = NOPS == 1 ? pt : pt >> 2;
+    const bool p_v = p_t < NQ * gs;
+    const int p_j = p_v ? p_t % gs : 0, p_qd = p_v ? p_t / gs : 0;
+    float2 pn[4], pv[4];
+    auto load_phase = [&](int st) {
+      if (NOPS != 1) return;
+      const int rs0 = rt_begin + st * RSTAGE;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        (&cre[0].x)[i] = pn[i].x + pv[i].x;
-        (&cim[0].x)[i] = pn[i].y + pv[i].y;
-        (&cre[1].x)[i] = pn[i].x - pv[i].x;
-        (&cim[1].x)[i] = pn[i].y - pv[i].y;
+        const int ip = rs0 + 4 * p_qd + i - toff;
+        const bool in = p_v && ip >= 0 && ip < nrp;
+        const int rsth = R - 1 - ip;
+        pn[i] = in ? phase[(int64_t(ip) * (mmax + 1) + m) * B + b0 + p_j] : make_float2(0.f, 0.f);
+        pv[i] = (in && rsth != ip) ? phase[(int64_t(rsth) * (mmax + 1) + m) * B + b0 + p_j] : make_float2(0.f, 0.f);
       }
-      const int ks = qd >> 1, kc = qd & 1;
+    };
+    load_phase(0);
+    for (int st = 0; st < nst; ++st) {
+      const int buf = st & 1;
+      ok = ws_wait(pp, pp.full + 8u * uint32_t(st % NR), uint32_t(st / NR) & 1u, err_flag);
+      if (ok && st >= 2) ok = ws_wait(pp, pp.mma_done + 8u * uint32_t(buf), uint32_t((st - 2) >> 1) & 1u, err_flag);
+      if (!ok) break;
+      const int rs0 = rt_begin + st * RSTAGE;
+      const int nvq = max(0, min(NQ, nquads - rs0 / 4));
+      const float* raw = reinterpret_cast<const float*>(c.smem + S::raw(st % NR));
 #pragma unroll
-      for (int acc = 0; acc < 2; ++acc) {
+      for (int i = 0; i < 4; ++i) {
+        // quads beyond the table were not copied: their rings contribute nothing
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (a_qd[i] < nvq) v = *reinterpret_cast<const float4*>(raw + a_src[i]);
+        const uint32_t d = S::a(buf, 0, 0, 0) + a_dst[i];
+        st_split(c.smem, d, d + S::A_TILE, v);
+      }
+      if (p_v && NOPS == 1) {
+        const int j = p_j, qd = p_qd;
+        // ring sums (accumulator 0: N + S) and differences (accumulator 1: N - S) of 4 rings
+        float4 cre[2], cim[2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          (&cre[0].x)[i] = pn[i].x + pv[i].x;
+          (&cim[0].x)[i] = pn[i].y + pv[i].y;
+          (&cre[1].x)[i] = pn[i].x - pv[i].x;
+          (&cim[1].x)[i] = pn[i].y - pv[i].y;
+        }
+        const int ks = qd >> 1, kc = qd & 1;
+#pragma unroll
+        for (int acc = 0; acc < 2; ++acc) {
+          const uint32_t bh = S::b(buf, acc, ks, 0), bl = S::b(buf, acc, ks, 1);
+          st_split(c.smem, bh + kcore_off(j, kc), bl + kcore_off(j, kc), cre[acc]);
+          st_split(c.smem, bh + kcore_off(gs + j, kc), bl + kcore_off(gs + j, kc), cim[acc]);
+        }
+      } else if (p_v) {
+        // columns (G.re, G.im, C.re, C.im); combo k (0: N + S, 1: N - S) of the rings' (Q, U):
+        // Xa(k) = (-Q.re, -Q.im, -U.re, -U.im), Ya(k) = (U.im, -U.re, -Q.im, Q.re)
+        // even spin: F+ rows Xa(acc), F- rows Ya(1 - acc); odd spin: F+ rows Ya(acc), F- rows Xa(1 - acc)
+        const int j = p_j, qd = p_qd;
+        const int acc = (pt >> 1) & 1, cc = pt & 1;
+        const int k = cc == 0 ? acc : 1 - acc;
+        const bool use_x = (cc == 0) != (spin_odd != 0);
+        const float4* ph = reinterpret_cast<const float4*>(c.smem + S::raw(st % NR) + G::TAB_BYTES);
+        float4 p[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int r = 4 * qd + i;  // ring of the stage
+          const int ip = rs0 + r - toff;
+          const bool in = ip >= 0 && ip < nrp;
+          const bool hs = in && R - 1 - ip != ip;
+          const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+          const float4 nv = in ? ph[r * G::PH_MAPS + j] : z;
+          const float4 sv = hs ? ph[(RSTAGE + r) * G::PH_MAPS + j] : z;
+          const float4 cv = k == 0 ? make_float4(nv.x + sv.x, nv.y + sv.y, nv.z + sv.z, nv.w + sv.w)
+                                   : make_float4(nv.x - sv.x, nv.y - sv.y, nv.z - sv.z, nv.w - sv.w);
+          // cv = (Q.re, Q.im, U.re, U.im) of ring i
+          if (use_x) {
+            (&p[0].x)[i] = -cv.x; (&p[1].x)[i] = -cv.y; (&p[2].x)[i] = -cv.z; (&p[3].x)[i] = -cv.w;
+          } else {
+            (&p[0].x)[i] = cv.w; (&p[1].x)[i] = -cv.z; (&p[2].x)[i] = -cv.y; (&p[3].x)[i] = cv.x;
+          }
+        }
+        const int kq = cc * NQ + qd, ks = kq >> 1, kc = kq & 1;
         const uint32_t bh = S::b(buf, acc, ks, 0), bl = S::b(buf, acc, ks, 1);
-        st_split(c.smem, bh + kcore_off(j, kc), bl + kcore_off(j, kc), cre[acc]);
-        st_split(c.smem, bh + kcore_off(gs + j, kc), bl + kcore_off(gs + j, kc), cim[acc]);
-      }
-    } else {
-      // columns (G.re, G.im, C.re, C.im); combo k (0: N + S, 1: N - S) of the rings' (Q, U):
-      // Xa(k) = (-Q.re, -Q.im, -U.re, -U.im), Ya(k) = (U.im, -U.re, -Q.im, Q.re)
-      // even spin: F+ rows Xa(acc), F- rows Ya(1 - acc); odd spin: F+ rows Ya(acc), F- rows Xa(1 - acc)
-      const int acc = (tid >> 1) & 1, cc = tid & 1;
-      const int k = cc == 0 ? acc : 1 - acc;
-      const bool use_x = (cc == 0) != (spin_odd != 0);
-      const float4* ph = reinterpret_cast<const float4*>(c.smem + S::raw(st % NR) + G::TAB_BYTES);
-      float4 p[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int r = 4 * qd + i;  // ring of the stage
-        const int ip = rs0 + r - toff;
-        const bool in = ip >= 0 && ip < nrp;
-        const bool hs = in && R - 1 - ip != ip;
-        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 nv = in ? ph[r * G::PH_MAPS + j] : z;
-        const float4 sv = hs ? ph[(RSTAGE + r) * G::PH_MAPS + j] : z;
-        const float4 cv = k == 0 ? make_float4(nv.x + sv.x, nv.y + sv.y, nv.z + sv.z, nv.w + sv.w)
-                                 : make_float4(nv.x - sv.x, nv.y - sv.y, nv.z - sv.z, nv.w - sv.w);
-        // cv = (Q.re, Q.im, U.re, U.im) of ring i
-        if (use_x) {
-          (&p[0].x)[i] = -cv.x; (&p[1].x)[i] = -cv.y; (&p[2].x)[i] = -cv.z; (&p[3].x)[i] = -cv.w;
-        } else {
-          (&p[0].x)[i] = cv.w; (&p[1].x)[i] = -cv.z; (&p[2].x)[i] = -cv.y; (&p[3].x)[i] = cv.x;
+        for (int part = 0; part < 4; ++part) {
+          const int row = part * gs + j;
+          st_split(c.smem, bh + kcore_off(row, kc), bl + kcore_off(row, kc), p[part]);
         }
       }
-      const int kq = cc * NQ + qd, ks = kq >> 1, kc = kq & 1;
-      const uint32_t bh = S::b(buf, acc, ks, 0), bl = S::b(buf, acc, ks, 1);
-#pragma unroll
-      for (int part = 0; part < 4; ++part) {
-        const int row = part * gs + j;
-        st_split(c.smem, bh + kcore_off(row, kc), bl + kcore_off(row, kc), p[part]);
-      }
+      tc::fence_proxy_async();  // the operand stores, visible to the tensor core
+      ws_arrive(pp.op_full + 8u * uint32_t(buf));
+      ws_arrive(pp.raw_free + 8u * uint32_t(st % NR));  // the stage's staged units and phase rows are read
+      if (st + 1 < nst) load_phase(st + 1);
     }
-  };
-  for (int st = 0; st < NR; ++st) issue_raw(st);
-  load_phase(0);
-  bool ok = true, failed = false;
-  int mma_issued = 0;
-  for (int st = 0; st < nst; ++st) {
-    ok = ok && tab_wait(c.mbar_full + 8u * uint32_t(st % NR), uint32_t(st / NR) & 1u);
-    if (ok) {
-      raw_waited = st + 1;
-      store(st);
-    }
-    tc::fence_proxy_async();
-    tc::fence_before_sync();
-    if (__syncthreads_or(!ok)) { failed = true; break; }
-    tc::fence_after_sync();
-    if (warp < 2) tab_mma(is, st & 1, (st >> 1) & 1, (st & 1) == 0, idesc, c.mbar_mma + 8u * uint32_t(st & 1));
-    mma_issued = st + 1;
-    issue_raw(st + NR);  // staging buffer st % NR has been read (barrier above)
-    if (st + 1 < nst) load_phase(st + 1);
-    if (st >= 1) {
-      // MMAs of stage st - 1 complete: its operand buffer is free; drain D after the second stage of a period
-      const int sp = st - 1;
-      ok = ok && tab_wait(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u);
-      if (ok && (sp & 1)) {
-        tc::fence_after_sync();
-        tab_drain(c, (sp >> 1) & 1, n, sp == 1);
-      }
-    }
-  }
-  if (!failed && nst > 0) {
-    const int sp = nst - 1;
-    ok = ok && tab_wait(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u);
-    if (ok) {
+  } else if (warp >= WS_DRAIN0) {
+    // ---- drain: S += D of each D period (first period: S = D), this warp's TMEM lane quarter,
+    // all columns, two 16-column units per wait
+    const uint32_t lane_addr = c.tmem + (uint32_t((warp & 3) * 32) << 16);
+    const int nu = n >> 3;  // units u = (chunk u >> 1, accumulator u & 1)
+    for (int p = 0; p < npairs; ++p) {
+      ok = ws_wait(pp, pp.d_ready + 8u * uint32_t(p & 1), uint32_t(p >> 1) & 1u, err_flag);
+      if (!ok) break;
       tc::fence_after_sync();
-      tab_drain(c, (sp >> 1) & 1, n, (sp >> 1) == 0);
+      const bool first = p == 0;
+#pragma unroll 1
+      for (int u = 0; u < nu; u += 2) {
+        float d0[16], d1[16], s0[16], s1[16];
+        const bool two = u + 1 < nu;
+        const uint32_t dc0 = lane_addr + tcol_d(p & 1, u & 1) + uint32_t(16 * (u >> 1));
+        const uint32_t sc0 = lane_addr + tcol_s(u & 1) + uint32_t(16 * (u >> 1));
+        const uint32_t dc1 = lane_addr + tcol_d(p & 1, (u + 1) & 1) + uint32_t(16 * ((u + 1) >> 1));
+        const uint32_t sc1 = lane_addr + tcol_s((u + 1) & 1) + uint32_t(16 * ((u + 1) >> 1));
+        tc::tmem_ld16(dc0, d0);
+        if (!first) tc::tmem_ld16(sc0, s0);
+        if (two) {
+          tc::tmem_ld16(dc1, d1);
+          if (!first) tc::tmem_ld16(sc1, s1);
+        }
+        tc::tmem_ld_wait();
+        if (!first) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) { d0[q] += s0[q]; d1[q] += s1[q]; }
+        }
+        tmem_st16(sc0, d0);
+        if (two) tmem_st16(sc1, d1);
+      }
+      tmem_st_wait();
+      tc::fence_before_sync();
+      ws_arrive(pp.d_free + 8u * uint32_t(p & 1));
     }
-    tc::fence_before_sync();
-    if (__syncthreads_or(!ok)) failed = true;
-    tc::fence_after_sync();
   }
+  // every role has finished (or given up)
+  tc::fence_before_sync();
+  const bool failed = __syncthreads_or(!ok) != 0;
+  tc::fence_after_sync();
   if (!failed && nst > 0) {
     // epilogue: TMEM lane = A row = 32 blk + j (blk = warp & 3, j = position in the parity), accumulator
     // acc is l = m + 64 (bb + blk) + 2 j + acc; the four warps of a lane quarter take every fourth
@@ -1032,15 +1002,14 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tab_adj_kernel(const float* __r
         }
       }
     }
-  } else if (failed && tid == 0) {
-    atomicExch(err_flag, 1);
-    // MMAs and bulk copies still in flight touch this CTA's memory: wait for them (bounded) before exit
-    if (mma_issued > 0) {
-      const int sp = mma_issued - 1;
-      tc::mbar_wait_bounded(c.mbar_mma + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u, TB_WAIT_LIMIT);
-    }
-    for (int k = raw_waited; k < raw_issued; ++k)
-      tc::mbar_wait_bounded(c.mbar_full + 8u * uint32_t(k % NR), uint32_t(k / NR) & 1u, TB_WAIT_LIMIT);
+  } else if (failed && lane == 0 && warp < WS_MMA_WARPS && mma_issued > 0) {
+    // the issued MMAs read this CTA's shared memory and write its TMEM: wait (bounded) for them
+    const int sp = mma_issued - 1;
+    tc::mbar_wait_bounded(pp.mma_done + 8u * uint32_t(sp & 1), uint32_t(sp >> 1) & 1u, TB_WAIT_LIMIT);
+  } else if (failed && lane == 0 && warp == WS_COPY_WARP) {
+    // copies in flight land in this CTA's shared memory: wait (bounded) for the last NR
+    for (int k = max(0, raw_issued - NR); k < raw_issued; ++k)
+      tc::mbar_wait_bounded(pp.full + 8u * uint32_t(k % NR), uint32_t(k / NR) & 1u, TB_WAIT_LIMIT);
   }
   tab_end<S>(c);
 }
