@@ -111,9 +111,14 @@ def test_trained_network_against_plain_cg():
     """What the trained network gains over the plain harmonic CG, at the same
     residual tolerance, on a workload whose operator couples nearby l of an m
     (full sky, latitude-dependent noise): both solvers reach r^T Sigma r /
-    b^T Sigma b < 1e-8 on the recomputed true residual, the learned step count
-    is reported, and the training loss falls.  (On the masked benchmark workload
-    the band network does not help; there the masked-band preconditioner does.)"""
+    b^T Sigma b < 1e-8 on the recomputed true residual, the training loss falls,
+    and the learned CG takes at least 5 % fewer steps than the plain one over 8
+    solves (measured: 98 plain, 80 learned).  On the masked benchmark workload
+    the band network does not gain -- its band blocks cannot represent the per-m
+    coupling of the masked equatorial band or the holes (Nside 256: 2815 learned
+    vs 796 harmonic steps for 33 solves; on top of the masked-band
+    preconditioner 117 vs 63) -- so the benchmark runs the masked-band
+    preconditioner."""
     import torch
     from polyspec_b200 import PolySpec, Weightings
     from polyspec_b200 import workloads as W
@@ -150,5 +155,4 @@ def test_trained_network_against_plain_cg():
         assert bool((cg.dot(r, sig(r)) / cg.dot(b0, sig(b0)) < 1e-7).all()), pre
         its[pre] = int(cg.iters.sum())
     print("CG steps over 8 solves: plain %d, learned %d" % (its["harmonic"], its["learned"]))
-    # the fallback bounds the loss: at most the learned budget (half the steps) more than plain
-    assert its["learned"] <= its["harmonic"] + 8 * 100
+    assert its["learned"] <= 0.95 * its["harmonic"], its
