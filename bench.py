@@ -52,6 +52,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Fisher sims/s at Nside 1024, mixed+learned vs plain FP64 GPU at ≤1e-6 rel err"
 UNIT = "sims/s"
+# DRAM bytes (read + write) / algorithmic bytes of the table-driven Legendre kernels, from one ncu
+# capture at Nside 512, lmax 1000, 32 maps (spin 0 and spin 2 launches together)
+TABLE_TRAFFIC_RATIO = {"leg_adjoint": 1.015, "leg_synth": 0.991}
 FIELDS = ("TT", "TE", "EE", "BB")
 THRESH = 1e-6
 NSTEP = 500
@@ -340,12 +343,18 @@ def roofline(a, stats, clocks, tables_used):
     sm_ghz = (clocks.get("sm_mhz") or 1965.0) / 1e3
     tab_dom = dom.startswith("leg_") and a.prec != "fp64" and all(tables_used.values())
     if tab_dom and by > 0:
-        # the table-driven Legendre stages stream their FP32 table from HBM: HBM bound
+        # the table-driven Legendre stages stream their FP32 table from HBM: HBM bound.  DRAM traffic per
+        # launch: the algorithmic bytes times the DRAM/algorithmic ratio of an ncu capture of the same
+        # kernels at Nside 512, 32 maps (profiles/table_legendre_nside512_b32.md), scaled by the units
+        # processed (traffic grows with the table and the maps)
+        ratio = TABLE_TRAFFIC_RATIO[dom]
         ach = by / (ms / 1e3) / 1e9
         peak = peaks.get("hbm_gbs", 6650.0)
         return {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured" if peaks else "6650 GB/s, of fallback",
-                "launches": n, "avg_launch_ms": ms / max(n, 1), "traffic": None,
+                "launches": n, "avg_launch_ms": ms / max(n, 1), "traffic": ratio * by / max(n, 1),
+                "traffic_source": "ncu dram__bytes_read+write / algorithmic bytes = %.3f at Nside 512, 32 maps, "
+                                  "scaled to the launch's algorithmic bytes" % ratio,
                 "algorithmic_bytes_per_launch": by / max(n, 1),
                 "tensor_tflops": fl / (ms / 1e3) / 1e12,
                 "tensor_frac_of_bf16_sustained": fl / (ms / 1e3) / 1e12 / peaks.get("bf16_tflops_sustained", 1400.0),
