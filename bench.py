@@ -78,7 +78,7 @@ def parse():
     p.add_argument("--lmax", type=int, default=2048)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="fisher-teb", choices=["fisher-teb", "pspec-t64"],
-                   help="fisher-teb: the headline (default); pspec-t64: PSpecBin T at Nside 64, lmax 128, ideal "
+                   help="fisher-teb: the headline (default); pspec-t64: PSpecBin T at Nside 64, lmax 191, ideal "
                         "S^-1 of the latitude-masked map, Fisher from seeds 1-10, beside the CPU oracle port")
     return p.parse_args()
 
@@ -533,14 +533,15 @@ def run_cuda(a):
 
 # ---------------------------------------------------------------------- PSpecBin T at Nside 64
 def pspec_t64(a):
-    """PSpecBin plain, T only: Nside 64, lmax 128, 8 bins of 16 from l = 2, C_l = 1000/(l+10)^2,
+    """PSpecBin plain, T only: Nside 64, lmax 191 (the reference's default 3 Nside - 1), 8 bins of 16 from
+    l = 2 (up to l = 130, within lmax as PSpecBin requires), C_l = 1000/(l+10)^2,
     30' beam, |lat| < 15 deg cut with a 5 deg cosine taper, applySinv = ideal S^-1 of the masked
     map; one step = the Fisher contributions of seeds 1-10 (polyspec/pspec_bin.py:94-164) and the
     numerator of the seed-0 GRF.  FP64 on the GPU and, on the host, the oracle restatement."""
     import torch
     from polyspec_b200 import PolySpec, Weightings, PSpecBin
     from polyspec_b200 import workloads as Wl
-    nside, lmax = 64, 128
+    nside, lmax = 64, 191
     cl = Wl.fiducial_cl(lmax, False)
     b = Wl.gaussian_beam(lmax, 30.0)
     cltot = {'TT': cl['TT'] * b ** 2}
@@ -549,7 +550,7 @@ def pspec_t64(a):
     seeds = list(range(1, 11))
     line = {"metric": "PSpecBin Fisher sims/s (T, Nside 64)", "unit": "sims/s", "n_gpus": 1, "steps": a.steps,
             "warmup": a.warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "PSpecBin T, Nside 64, lmax 128, 8 bins of 16 from l=2, 30' beam, |lat|<15 deg "
+            "config": {"workload": "PSpecBin T, Nside 64, lmax 191, 8 bins of 16 from l=2, 30' beam, |lat|<15 deg "
                                    "cut + 5 deg taper, ideal S^-1, Fisher seeds 1-10 per step"}}
     base = PolySpec(nside, dict(cltot), beam=[b], pol=False, lmax=lmax, prec="fp64")
     wts = Weightings(base, mask[None], {'TT': cl['TT']})
