@@ -161,6 +161,29 @@ int ps_legendre_adjoint(const ps_plan* plan, const double* phase, double* alm, i
 int ps_synthesis_noalloc(const ps_plan* plan, const double* alm, double* map, int batch, int spin,
                          cudaStream_t stream);
 
+/* Mixed-size submission (no counterpart in the reference, which calls ducc0 once
+ * per map): n single-map transforms of any plans, spins and directions run as one
+ * batched ps_synthesis / ps_adjoint per group of equal (plan, direction, spin,
+ * scale), largest groups first, in one stream order.  An item's input and output
+ * are one map's alm [ncomp][nalm] complex128 or map [ncomp][npix] float64 (ncomp
+ * 1 for spin 0, 2 for spin s).  A group whose inputs (outputs) already sit back
+ * to back in item order is read (written) in place; otherwise they are gathered
+ * into (scattered from) the workspace with one device copy per item.  Nothing is
+ * allocated and nothing synchronises, so a submission can be captured in a CUDA
+ * graph.  Items must not overlap each other's outputs. */
+enum { PS_DIR_SYNTHESIS = 0, PS_DIR_ADJOINT = 1 };
+typedef struct ps_work_item {
+  const ps_plan* plan;
+  int direction; /* PS_DIR_SYNTHESIS: alm -> map; PS_DIR_ADJOINT: map -> alm times scale */
+  int spin;
+  const double* in;
+  double* out;
+  double scale; /* adjoint only */
+} ps_work_item;
+int ps_batch_workspace_bytes(const ps_work_item* items, int n, size_t* bytes);
+int ps_batch_submit(const ps_work_item* items, int n, void* workspace, size_t workspace_bytes,
+                    cudaStream_t stream);
+
 /* ---------------------------------------------------- pixel-space products
  * Elementwise products of maps of n elements (real = float64, complex =
  * complex128, all contiguous), the per-element products of the reference's
@@ -292,6 +315,45 @@ int ps_lm_matvec3(const double* S, const double* pre, const double* post, const 
 int ps_lm_dot_workspace_bytes(int batch, int64_t nalm, size_t* bytes);
 int ps_lm_dot(const double* x, const double* y, const double* w, int batch, int64_t nalm, double* out,
               void* workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/* ---------------------------------------------------------------- masked CG solve
+ * The conjugate-gradient solve of the optimal S^-1 filter, A x = b with
+ *   A = C^-1 + B Y^H W Y B   (CGD._apply_A, polyspec/weighting.py:297-299)
+ * and the harmonic preconditioner M = Sigma (weighting.py:306-307), run as the
+ * reference's CGD.run(nstep = max_iter, thresh = tol) (weighting.py:217-367) on
+ * `batch` independent right-hand sides.  Every system keeps its own alpha, beta
+ * and stopping test err = r^T M r / b^T M b (m-weighted inner products,
+ * weighting.py:255) and stops at the first step with err < tol, or after
+ * max_iter steps; the systems still running are compacted after each step, so
+ * the work is the sum of the separate solves' work.
+ *
+ * ps_cg_create binds a plan and the operator's arrays, all device memory that
+ * the caller owns and keeps alive for the object's lifetime:
+ *   nfield  1 (T; spin 0) or 3 (T, E, B; spin 0 and spin 2)
+ *   inv_cl  C^-1 [nfield][nfield][nalm] float64 (real, per lm)
+ *   sigma   Sigma [nfield][nfield][nalm] float64 (the preconditioner)
+ *   beam    [nfield][nalm] float64, or NULL (no beam)
+ *   weight  the pixel weight W N^-1 W / A_pix, [nfield][npix] float64 (T; T, Q, U)
+ *   scale   the adjoint's normalisation (pi / (3 nside^2) for to_lm)
+ * The operator runs fused (ps_sht_weighted_roundtrip) on a mixed plan holding
+ * the Legendre tables of its spins, else as ps_synthesis, weighting, ps_adjoint.
+ *
+ * ps_cg_solve: b [batch][nfield][nalm] complex128 (CGD's b0 = B Y^H W N^-1 d);
+ * x0 the initial guess in the same layout or NULL (zero); x receives x0 + the
+ * CG solution (CGD.get_wiener_lm).  iters [batch] and final_err [batch] are HOST
+ * arrays (may be NULL) that receive each system's step count and last err.
+ * The call synchronises `stream` once per step to read the stopping tests.  It
+ * returns PS_ERR_NOT_CONVERGED, with x holding the last iterate, when a system
+ * did not reach tol in max_iter steps (the reference prints a warning then).
+ * A system with b^T M b = 0 stops at step 0 with x = x0 and err 0 (the
+ * reference divides by zero there). */
+typedef struct ps_cg ps_cg;
+int ps_cg_create(const ps_plan* plan, int nfield, const double* inv_cl, const double* sigma, const double* beam,
+                 const double* weight, double scale, ps_cg** cg);
+int ps_cg_destroy(ps_cg* cg);
+int ps_cg_workspace_bytes(const ps_cg* cg, int batch, size_t* bytes);
+int ps_cg_solve(ps_cg* cg, const double* b, const double* x0, double* x, int batch, int max_iter, double tol,
+                int* iters, double* final_err, void* workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* ------------------------------------------------------------- binned bispectrum (BSpecBin)
  * Map sets are planar complex: map m is [2][npix] float64 (real plane, then

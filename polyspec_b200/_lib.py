@@ -129,11 +129,30 @@ SIGNATURES = {
                                       _c_void_p]),
     "ps_lm_dot": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int64, _c_void_p, _c_void_p, _c_size_t,
                            _c_void_p]),
+    "ps_batch_workspace_bytes": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_size_t)]),
+    "ps_batch_submit": (_c_int, [_c_void_p, _c_int, _c_void_p, _c_size_t, _c_void_p]),
+    "ps_cg_create": (_c_int, [_c_void_p, _c_int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_double,
+                              ctypes.POINTER(_c_void_p)]),
+    "ps_cg_destroy": (_c_int, [_c_void_p]),
+    "ps_cg_workspace_bytes": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_size_t)]),
+    "ps_cg_solve": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_double,
+                             ctypes.POINTER(_c_int), ctypes.POINTER(_c_double), _c_void_p, _c_size_t, _c_void_p]),
     "ps_stats_enable_timing": (_c_int, [_c_int]),
     "ps_stats_reset": (_c_int, []),
     "ps_stats_get": (_c_int, [_c_int, ctypes.POINTER(_c_int64), ctypes.POINTER(_c_double),
                               ctypes.POINTER(_c_double), ctypes.POINTER(_c_double)]),
 }
+
+
+
+class WorkItem(ctypes.Structure):
+    """ps_work_item of ps_batch_submit (one single-map transform)."""
+    _fields_ = [("plan", _c_void_p), ("direction", _c_int), ("spin", _c_int), ("inp", _c_void_p),
+                ("out", _c_void_p), ("scale", _c_double)]
+
+
+PS_DIR_SYNTHESIS = 0
+PS_DIR_ADJOINT = 1
 
 # pixel-product ops and radial-sum kinds (enums of include/pscuda.h, in order)
 PIX_OPS = ["multiply", "multiply_asym", "multiplyC", "multiplyC_asym", "multiplyCC", "multiplyCC_asym", "multiply2",
