@@ -316,6 +316,27 @@ int ps_lm_dot_workspace_bytes(int batch, int64_t nalm, size_t* bytes);
 int ps_lm_dot(const double* x, const double* y, const double* w, int batch, int64_t nalm, double* out,
               void* workspace, size_t workspace_bytes, cudaStream_t stream);
 
+/* ------------------------------------------------ masked-band CG preconditioner
+ * M r = Sigma r + Sigma B L^H Om^1/2 K_m^-1 Om^1/2 L B Sigma r (per order m; the m = 0 part
+ * of the correction real), L the Legendre synthesis stage on a band plan (ps_plan_band) of
+ * `plan`, on n = 3 R_b band coordinates (T rings, then Q rings, then U rings).  No
+ * counterpart in the reference (its CG offers 'harmonic' and 'pseudo_inverse',
+ * polyspec/weighting.py:301-324); built on its weighting (Sigma, :76-78) and CG operator
+ * (:297-299).  ps_cutprec_create converts kinv = K_m^-1 (complex64 [mmax+1][n][n]) into the
+ * tensor-core layout of the per-m GEMM, BF16 (planes = 1) or BF16 hi + lo (planes = 2), in
+ * memory the object owns (enqueued on `stream`); om_half [n], sigma [3][3][nalm] and beam
+ * [3][nalm] (float64) stay the caller's.  The band plan must be mixed with the Legendre
+ * tables of spins 0 and 2 built on its parent (PS_ERR_UNSUPPORTED otherwise).
+ * ps_cutprec_apply: out = M r for r [batch][3][nalm] complex128 (out != r). */
+typedef struct ps_cutprec ps_cutprec;
+int ps_cutprec_create(const ps_plan* plan, const ps_plan* band, const void* kinv, int n, int planes,
+                      const double* om_half, const double* sigma, const double* beam, cudaStream_t stream,
+                      ps_cutprec** out);
+int ps_cutprec_destroy(ps_cutprec* c);
+int ps_cutprec_workspace_bytes(const ps_cutprec* c, int batch, size_t* bytes);
+int ps_cutprec_apply(const ps_cutprec* c, const double* r, double* out, int batch, void* workspace,
+                     size_t workspace_bytes, cudaStream_t stream);
+
 /* ---------------------------------------------------------------- masked CG solve
  * The conjugate-gradient solve of the optimal S^-1 filter, A x = b with
  *   A = C^-1 + B Y^H W Y B   (CGD._apply_A, polyspec/weighting.py:297-299)

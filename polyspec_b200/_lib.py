@@ -131,6 +131,11 @@ SIGNATURES = {
                            _c_void_p]),
     "ps_batch_workspace_bytes": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_batch_submit": (_c_int, [_c_void_p, _c_int, _c_void_p, _c_size_t, _c_void_p]),
+    "ps_cutprec_create": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p, _c_void_p, _c_void_p,
+                                   _c_void_p, ctypes.POINTER(_c_void_p)]),
+    "ps_cutprec_destroy": (_c_int, [_c_void_p]),
+    "ps_cutprec_workspace_bytes": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_size_t)]),
+    "ps_cutprec_apply": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_void_p, _c_size_t, _c_void_p]),
     "ps_cg_create": (_c_int, [_c_void_p, _c_int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_double,
                               ctypes.POINTER(_c_void_p)]),
     "ps_cg_destroy": (_c_int, [_c_void_p]),

@@ -807,4 +807,28 @@ int roundtrip_view(const ps_plan* plan, int spin, RoundtripView& v) {
   v.ncls = int(plan->cls_len.size());
   return PS_OK;
 }
+
+// The Legendre tables of a mixed band plan (owned by its parent), for the masked-band
+// preconditioner (ps_cutprec.cu); PS_ERR_UNSUPPORTED for other plans or a spin without a table.
+struct BandView {
+  const Plan* P;
+  const float* tab;
+  const int64_t* off;
+  const int2* work;
+  int nwork, Rh_table, toff;
+};
+int band_view(const ps_plan* band, int spin, BandView& v) {
+  if (!band || !band->is_band || band->p.prec != PS_PREC_MIXED) return PS_ERR_UNSUPPORTED;
+  if (spin > 0 && !band->p.d_seed[spin]) return PS_ERR_INVALID;
+  TabRef tr;
+  if (!table_for(band, spin, tr)) return PS_ERR_UNSUPPORTED;
+  v.P = &band->p;
+  v.tab = tr.tab;
+  v.off = tr.off;
+  v.work = tr.work;
+  v.nwork = tr.nwork;
+  v.Rh_table = tr.Rh_table;
+  v.toff = tr.toff;
+  return PS_OK;
+}
 }  // namespace ps

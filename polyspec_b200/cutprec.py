@@ -65,7 +65,7 @@ def ring_ranges(nside):
 
 
 class CutPreconditioner:
-    def __init__(self, weightings, chunk=64, dtype=torch.complex64):
+    def __init__(self, weightings, chunk=64, dtype=torch.complex64, native=None, planes=2):
         W = weightings
         base = W.base
         if not base.pol:
@@ -123,8 +123,33 @@ class CutPreconditioner:
         self.dtype = dtype
         self._build(chunk)
         self._use = self._band
+        # one native call per application (ps_cutprec_apply: band stages on the plan's Legendre
+        # tables, K_m^-1 on the tensor cores in BF16 (planes=1) or BF16 hi + lo (planes=2)) when
+        # the plan is mixed with both tables; the torch composition below otherwise.  Measured at
+        # Nside 1024 (6 systems to 1e-8): planes=2 takes the CG steps of the complex64 product
+        # (55), planes=1 costs 15 % more (63)
+        self._native = None
+        self.planes = planes
+        if native is not False and base.prec != "fp64" and dtype == torch.complex64:
+            for spin in (0, 2):
+                P._maybe_table(spin)
+            h = ctypes.c_void_p()
+            rc = _lib.lib().ps_cutprec_create(P._h, self._band, _vp(self.Kinv), 3 * self.Rb, int(planes),
+                                              _vp(self.om_half), _vp(self.sigma_r), _vp(self.beam), _stream(),
+                                              ctypes.byref(h))
+            if rc == _lib.PS_OK:
+                self._native = h
+                self._nws = None
+                torch.cuda.current_stream().synchronize()
+                self.Kinv = None  # the object holds its own BF16 copy
+            elif native:
+                _lib.check("ps_cutprec_create", rc)
 
     def __del__(self):
+        h = getattr(self, "_native", None)
+        if h is not None and h.value and _lib._lib is not None:
+            _lib.lib().ps_cutprec_destroy(h)
+            self._native = None
         for name in ("_band", "_band64", "_own64"):
             h = getattr(self, name, None)
             if h is not None and h.value and _lib._lib is not None:
@@ -210,6 +235,18 @@ class CutPreconditioner:
     # ---------------------------------------------------------------- application
     def apply(self, r):
         """M r for r complex128 [B, 3, nlm]."""
+        if self.enabled and self._native is not None:
+            r = r.contiguous()
+            B = r.shape[0]
+            out = torch.empty_like(r)
+            n = ctypes.c_size_t()
+            _lib.call("ps_cutprec_workspace_bytes", self._native, B, ctypes.byref(n))
+            if self._nws is None or self._nws.numel() < n.value:
+                self._nws = None
+                self._nws = torch.empty(int(n.value), dtype=torch.uint8, device=r.device)
+            _lib.call("ps_cutprec_apply", self._native, _vp(r), _vp(out), B, _vp(self._nws), self._nws.numel(),
+                      _stream())
+            return out
         s = self._sigma(r)
         if not self.enabled:
             return s
