@@ -315,6 +315,20 @@ int ps_lm_matvec3(const double* S, const double* pre, const double* post, const 
 int ps_lm_dot_workspace_bytes(int batch, int64_t nalm, size_t* bytes);
 int ps_lm_dot(const double* x, const double* y, const double* w, int batch, int64_t nalm, double* out,
               void* workspace, size_t workspace_bytes, cudaStream_t stream);
+/* The fused updates of one batched CG step (weighting.py:326-339 per system):
+ * ps_lm_matvec3_add: y += S x (the C^-1 term added to the round trip's output);
+ * ps_lm_quad_dot: out[n] = Sum w Re(x conj(S x)) without storing S x (the stopping
+ * statistic r^T Sigma r; workspace as ps_lm_dot_workspace_bytes);
+ * ps_cg_xr_update: x[slot[n]] += alpha[n] p[n], r[n] -= alpha[n] q[n] on rows of `per`
+ * complex128 values (slot: int64 [batch] or NULL for the identity: x stays full-size
+ * while p, r, q hold the systems still running);
+ * ps_cg_direction: p[n] = z[n] + beta[n] p[n]. */
+int ps_lm_matvec3_add(const double* S, const double* x, double* y, int batch, int64_t nalm, cudaStream_t stream);
+int ps_lm_quad_dot(const double* S, const double* x, const double* w, int batch, int64_t nalm, double* out,
+                   void* workspace, size_t workspace_bytes, cudaStream_t stream);
+int ps_cg_xr_update(double* x, const int64_t* slot, const double* alpha, const double* p, double* r, const double* q,
+                    int batch, int64_t per, cudaStream_t stream);
+int ps_cg_direction(double* p, const double* z, const double* beta, int batch, int64_t per, cudaStream_t stream);
 
 /* ------------------------------------------------ masked-band CG preconditioner
  * M r = Sigma r + Sigma B L^H Om^1/2 K_m^-1 Om^1/2 L B Sigma r (per order m; the m = 0 part

@@ -131,6 +131,12 @@ SIGNATURES = {
                            _c_void_p]),
     "ps_batch_workspace_bytes": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_batch_submit": (_c_int, [_c_void_p, _c_int, _c_void_p, _c_size_t, _c_void_p]),
+    "ps_lm_matvec3_add": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int64, _c_void_p]),
+    "ps_lm_quad_dot": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int64, _c_void_p, _c_void_p, _c_size_t,
+                                _c_void_p]),
+    "ps_cg_xr_update": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, _c_int64,
+                                 _c_void_p]),
+    "ps_cg_direction": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int64, _c_void_p]),
     "ps_cutprec_create": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p, _c_void_p, _c_void_p,
                                    _c_void_p, ctypes.POINTER(_c_void_p)]),
     "ps_cutprec_destroy": (_c_int, [_c_void_p]),

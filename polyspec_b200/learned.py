@@ -213,12 +213,11 @@ class LearnedBandPreconditioner:
         for _ in range(nstep):
             if not bool(cg.active.any()):
                 break
-            act = cg.active.clone()
             cg.step()
             cg.active &= ~(cg.err < thresh_collect)
-            idx = torch.nonzero(act).flatten()
+            idx = cg.slots  # the rows of cg.r: the systems that took this step
             if idx.numel():
-                self.add_pairs(cg.r[idx], target(cg.r[idx], xstar[idx] - cg.x[idx]))
+                self.add_pairs(cg.r, target(cg.r, xstar[idx] - cg.x[idx]))
         return cg
 
     # ---------------------------------------------------------------- training

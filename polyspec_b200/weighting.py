@@ -283,9 +283,11 @@ class BatchedCGD:
     """B independent copies of the reference CG (polyspec/weighting.py:217-367): vectors
     are [B, nfield, nlm] and each right-hand side keeps its own alpha, beta and stopping
     test (err_b = rz_b / rz0_b < thresh freezes system b, as a separate run would stop).
-    Every step gathers the systems still active and applies A and M to them as one
-    batched SHT pair, so the work is the sum of the separate runs' work, not B times
-    the slowest run's."""
+    r and p hold only the systems still running (rows dropped once, when a system
+    stops), and A and M apply to them as one batched SHT pair, so the work is the sum
+    of the separate runs' work, not B times the slowest run's.  The vector updates are
+    fused kernels (x += alpha p with r -= alpha Ap, p = z + beta p, C^-1 p added to the
+    round trip in place, r^T Sigma r without storing Sigma r)."""
 
     def __init__(self, weightings, d, x0, preconditioner='harmonic', learned_max_steps=None):
         self.base = weightings.base
@@ -314,11 +316,13 @@ class BatchedCGD:
         self.rz = self.dot(self.r, z)
         if preconditioner in ('learned', 'cut'):
             # the stopping test uses Sigma whatever M is (no M b0 needed)
-            self.stat0 = self.dot(b0, self._sigma(b0))
+            self.stat0 = self._quad_sigma(b0)
             self.rz0 = self.stat0
         else:
             self.rz0 = self.dot(b0, self._apply_M(b0, self.use_learned))
         self.p = z
+        # rows of r and p: the systems still running (slots = their indices); x stays full-size
+        self.slots = torch.arange(B, device=b.device)
         self.i = 0
         self.iters = torch.zeros(B, dtype=torch.int64, device=b.device)
         self.active = torch.ones(B, dtype=torch.bool, device=b.device)
@@ -336,7 +340,13 @@ class BatchedCGD:
         """Stopping statistic: rz/rz0 of the plain CG (= r^T Sigma r / b^T Sigma b)."""
         if self.preconditioner not in ('learned', 'cut'):
             return rz / self.rz0[idx]
-        return self.dot(r, self._sigma(r)) / self.stat0[idx]
+        return self._quad_sigma(r) / self.stat0[idx]
+
+    def _quad_sigma(self, r):
+        """r^T Sigma r per system (m-weighted; Sigma r not stored for T, E, B)."""
+        if self._pol(r):
+            return lmops.quad_dot(self.W.real3('Sigma'), r, self.w)
+        return self.dot(r, self._sigma(r))
 
     def dot(self, a, b):
         if self._pol(a):
@@ -362,11 +372,19 @@ class BatchedCGD:
                 B, nf = ilm.shape[0], ilm.shape[1]
                 self.base.n_SHTs_reverse += B * (1 + (nf == 3))
                 self.base.n_SHTs_forward += B * (1 + (nf == 3))
-                return self._apply_Cinv(ilm) + out
+                return self._add_Cinv(ilm, out)
         beam = self.base.dev('beam_lm')
         m = self.base.to_map_batch(ilm * beam)
         m = m * (self.W.d_WNW / self.W.pixel_area)
-        return self._apply_Cinv(ilm) + self.base.to_lm_batch(m) * beam
+        y = self.base.to_lm_batch(m)
+        y *= beam
+        return self._add_Cinv(ilm, y)
+
+    def _add_Cinv(self, ilm, y):
+        """y + C^-1 ilm (in place on y for T, E, B)."""
+        if self._pol(ilm) and y.is_contiguous():
+            return lmops.matvec3_add(self.W.real3('inv_Cl'), ilm, y)
+        return self._apply_Cinv(ilm) + y
 
     def _fallback_M(self, r):
         """Preconditioner of a system the learned CG hands back: the learned operator's own base
@@ -398,22 +416,33 @@ class BatchedCGD:
         raise Exception("Unknown preconditioner %s specified!" % self.preconditioner)
 
     def step(self):
-        idx = torch.nonzero(self.active).flatten()
+        keep = self.active[self.slots]
+        if not bool(keep.all()):
+            # systems stopped since the last step: drop their rows (once, not every step)
+            self.r = self.r[keep]
+            self.p = self.p[keep]
+            self.slots = self.slots[keep]
+        idx = self.slots
         if idx.numel() == 0:
             return
-        full = idx.numel() == self.active.numel()
-        p = self.p if full else self.p[idx]
-        r = self.r if full else self.r[idx]
+        p, r = self.p, self.r
         rz = self.rz[idx]
         lm = self.use_learned[idx]
         Ap = self._apply_A(p)
         alpha = rz / self.dot(p, Ap)
-        x_new = (self.x if full else self.x[idx]) + alpha[:, None, None] * p
-        r = r - alpha[:, None, None] * Ap
+        fused = r.is_contiguous() and p.is_contiguous() and Ap.is_contiguous() and self.x.is_contiguous()
+        if fused:
+            lmops.xr_update(self.x, idx, alpha, p, r, Ap)  # x[idx] += alpha p, r -= alpha Ap
+        else:
+            self.x[idx] = self.x[idx] + alpha[:, None, None] * p
+            r = r - alpha[:, None, None] * Ap
         z = self._apply_M(r, lm)
         next_rz = self.dot(r, z)
         beta = next_rz / rz
-        p = z + beta[:, None, None] * p
+        if fused and z.is_contiguous():
+            lmops.direction(p, z, beta)  # p = z + beta p
+        else:
+            p = z + beta[:, None, None] * p
         if self.preconditioner == 'learned':
             # fallback: a learned system whose r^T M r is not positive and finite, or that
             # has used its learned step budget, restarts as plain harmonic CG from x
@@ -426,12 +455,7 @@ class BatchedCGD:
                 next_rz[bad] = self.dot(r[bad], zs)
                 lm = lm & ~bad
                 self.use_learned[idx] = lm
-        if full:
-            self.x, self.r, self.p = x_new, r, p
-        else:
-            self.x[idx] = x_new
-            self.r[idx] = r
-            self.p[idx] = p
+        self.r, self.p = r, p
         self.err[idx] = self._stop_stat(r, next_rz, lm, idx)
         self.rz[idx] = next_rz
         self.iters[idx] += 1
