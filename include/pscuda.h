@@ -90,6 +90,13 @@ int ps_plan_set_tile(ps_plan* plan, int direction, int spin, int tile);
  * fit, PS_ERR_UNSUPPORTED on FP64 or band plans.  ps_plan_drop_tables frees
  * them (after synchronising the device); ps_plan_has_table tells whether a
  * spin's transforms use one. */
+/* Table format of the tables a plan builds next (tables already built keep theirs):
+ * PS_TAB_TF32X3 -- FP32 values, split into TF32 hi + lo by the GEMM kernels (3 products);
+ * PS_TAB_BF16X3 -- the same FP32 values stored as BF16 hi + mid + lo planes (24 significant
+ * bits) already in the tensor core's operand layout, 1.5x the bytes, streamed into the MMAs
+ * by bulk copies with no operand splitting (kind::f16, 6 products). */
+enum { PS_TAB_TF32X3 = 0, PS_TAB_BF16X3 = 1 };
+int ps_plan_set_table_format(ps_plan* plan, int format);
 int ps_plan_table_bytes(const ps_plan* plan, int spin, size_t* bytes);
 int ps_plan_build_table(ps_plan* plan, int spin, cudaStream_t stream);
 int ps_plan_has_table(const ps_plan* plan, int spin, int* has);

@@ -38,6 +38,7 @@ SIGNATURES = {
     "ps_synthesis_noalloc": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_void_p]),
     "ps_plan_band": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_void_p)]),
     "ps_plan_set_tile": (_c_int, [_c_void_p, _c_int, _c_int, _c_int]),
+    "ps_plan_set_table_format": (_c_int, [_c_void_p, _c_int]),
     "ps_plan_table_bytes": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_plan_build_table": (_c_int, [_c_void_p, _c_int, _c_void_p]),
     "ps_plan_has_table": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(_c_int)]),

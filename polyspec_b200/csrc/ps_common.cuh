@@ -66,6 +66,9 @@ struct Plan {
   int64_t* d_tab_off;
   int2* d_tab_work;
   int tab_nwork;
+  // format of each built table (PS_TAB_TF32X3 or PS_TAB_BF16X3) and of the tables built next
+  int tab_fmt[4];
+  int tab_fmt_build;
 };
 
 // ---------------------------------------------------------------------------

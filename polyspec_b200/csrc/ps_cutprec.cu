@@ -31,17 +31,17 @@ struct ps_plan;
 
 namespace ps {
 int launch_tab_synth(const Plan& P, const float* table, const int64_t* d_blockoff, int Rh_table, int toff,
-                     const double2* almT, float2* phase, int B, int spin, int* err_flag, cudaStream_t st);
+                     const double2* almT, float2* phase, int B, int spin, int* err_flag, cudaStream_t st, int fmt);
 int launch_tab_adj(const Plan& P, const float* table, const int64_t* d_blockoff, const int2* d_work, int nwork,
                    int Rh_table, int toff, const float2* phase, double2* alm, int B, int spin, double scale,
-                   int64_t out_stride, const double* lscale, int* err_flag, cudaStream_t st);
+                   int64_t out_stride, const double* lscale, int* err_flag, cudaStream_t st, int fmt);
 // the band plan's Legendre tables (owned by its parent plan), resolved by the plan code
 struct BandView {
   const Plan* P;
   const float* tab;
   const int64_t* off;
   const int2* work;
-  int nwork, Rh_table, toff;
+  int nwork, Rh_table, toff, fmt;
 };
 int band_view(const ps_plan* band, int spin, BandView& v);
 }  // namespace ps
@@ -483,7 +483,8 @@ extern "C" int ps_cutprec_apply(const ps_cutprec* c, const double* r, double* ou
       cut_gather<<<cut_grid(nalm * batch * nc), 256, 0, stream>>>(o, c->beam, spin ? 1 : 0, nc, almT, batch, nalm);
       PS_LAUNCH_CHECK();
     }
-    rc = launch_tab_synth(*v.P, v.tab, v.off, v.Rh_table, v.toff, almT, spin ? ph2 : ph0, batch, spin, err, stream);
+    rc = launch_tab_synth(*v.P, v.tab, v.off, v.Rh_table, v.toff, almT, spin ? ph2 : ph0, batch, spin, err, stream,
+                          v.fmt);
     if (rc != PS_OK) return rc;
   }
   // W = K_m^-1 Y per order, at most CUT_BMAX systems per pass, written back over the phases
@@ -505,7 +506,7 @@ extern "C" int ps_cutprec_apply(const ps_cutprec* c, const double* r, double* ou
     const BandView& v = spin ? v2 : v0;
     const int c0 = spin ? 1 : 0;
     rc = launch_tab_adj(*v.P, v.tab, v.off, v.work, v.nwork, v.Rh_table, v.toff, spin ? ph2 : ph0, a + c0 * nalm,
-                        batch, spin, 1.0, 3 * nalm, c->beam + c0 * nalm, err, stream);
+                        batch, spin, 1.0, 3 * nalm, c->beam + c0 * nalm, err, stream, v.fmt);
     if (rc != PS_OK) return rc;
   }
   int lmax = 0;

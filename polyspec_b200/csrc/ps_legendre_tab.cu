@@ -1073,8 +1073,17 @@ static int tab_group_size(int B, int spin, int nmax, int& ngroups) {
 
 // The table of ring pairs [toff, toff + nrp) of a plan with Rh_table ring pairs (a band plan reads its
 // parent's table at an offset).
+int launch_tab3_synth(const Plan& P, const uint16_t* table, const int64_t* d_blockoff, int Rh_table, int toff,
+                      const double2* almT, float2* phase, int B, int spin, int* err_flag, cudaStream_t st);
+int launch_tab3_adj(const Plan& P, const uint16_t* table, const int64_t* d_blockoff, const int2* d_work, int nwork,
+                    int Rh_table, int toff, const float2* phase, double2* alm, int B, int spin, double scale,
+                    int64_t out_stride, const double* lscale, int* err_flag, cudaStream_t st);
+
 int launch_tab_synth(const Plan& P, const float* table, const int64_t* d_blockoff, int Rh_table, int toff,
-                     const double2* almT, float2* phase, int B, int spin, int* err_flag, cudaStream_t st) {
+                     const double2* almT, float2* phase, int B, int spin, int* err_flag, cudaStream_t st, int fmt) {
+  if (fmt == PS_TAB_BF16X3)
+    return launch_tab3_synth(P, reinterpret_cast<const uint16_t*>(table), d_blockoff, Rh_table, toff, almT, phase, B,
+                             spin, err_flag, st);
   const double flops = double(spin == 0 ? 4 : 16) * double(P.Rh) * double(P.nalm) * B;
   const double bytes = double(tab_bytes(Rh_table, P.lmax, P.mmax, spin)) * double(P.Rh) / double(Rh_table) +
                        double(B) * (spin == 0 ? 1 : 2) * (16.0 * P.nalm + 8.0 * P.R * (P.mmax + 1));
@@ -1114,7 +1123,10 @@ void tab_adj_work(int lmax, int mmax, std::vector<int2>& work) {
 // times scale and, when lscale is given, lscale[comp][idx]
 int launch_tab_adj(const Plan& P, const float* table, const int64_t* d_blockoff, const int2* d_work, int nwork,
                    int Rh_table, int toff, const float2* phase, double2* alm, int B, int spin, double scale,
-                   int64_t out_stride, const double* lscale, int* err_flag, cudaStream_t st) {
+                   int64_t out_stride, const double* lscale, int* err_flag, cudaStream_t st, int fmt) {
+  if (fmt == PS_TAB_BF16X3)
+    return launch_tab3_adj(P, reinterpret_cast<const uint16_t*>(table), d_blockoff, d_work, nwork, Rh_table, toff,
+                           phase, alm, B, spin, scale, out_stride, lscale, err_flag, st);
   const double flops = double(spin == 0 ? 4 : 16) * double(P.Rh) * double(P.nalm) * B;
   const double bytes = double(tab_bytes(Rh_table, P.lmax, P.mmax, spin)) * double(P.Rh) / double(Rh_table) +
                        double(B) * (spin == 0 ? 1 : 2) * (16.0 * P.nalm + 8.0 * P.R * (P.mmax + 1));

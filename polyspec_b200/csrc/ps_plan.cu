@@ -37,14 +37,16 @@ int mx_adjoint_tiles(const Plan& P);
 int launch_reduce_partials_f32(const float2* partial, double2* alm, int ntiles, int B, int ncomp, int64_t nalm,
                                double scale, int bofs, int sms, cudaStream_t st);
 size_t tab_bytes(int Rh, int lmax, int mmax, int spin);
+size_t tab3_bytes(int Rh, int lmax, int mmax, int spin);
+int launch_tab3_gen(const Plan& P, int spin, const int64_t* d_blockoff, uint16_t* table, cudaStream_t st);
 void tab_blockoff(int lmax, int mmax, std::vector<int64_t>& off);
 void tab_adj_work(int lmax, int mmax, std::vector<int2>& work);
 int launch_tab_gen(const Plan& P, int spin, const int64_t* d_blockoff, float* table, cudaStream_t st);
 int launch_tab_synth(const Plan& P, const float* table, const int64_t* d_blockoff, int Rh_table, int toff,
-                     const double2* almT, float2* phase, int B, int spin, int* err_flag, cudaStream_t st);
+                     const double2* almT, float2* phase, int B, int spin, int* err_flag, cudaStream_t st, int fmt);
 int launch_tab_adj(const Plan& P, const float* table, const int64_t* d_blockoff, const int2* d_work, int nwork,
                    int Rh_table, int toff, const float2* phase, double2* alm, int B, int spin, double scale,
-                   int64_t out_stride, const double* lscale, int* err_flag, cudaStream_t st);
+                   int64_t out_stride, const double* lscale, int* err_flag, cudaStream_t st, int fmt);
 }  // namespace ps
 
 struct ps_plan {
@@ -125,7 +127,7 @@ struct TabRef {
   const float* tab;
   const int64_t* off;
   const int2* work;
-  int nwork, Rh_table, toff;
+  int nwork, Rh_table, toff, fmt;
 };
 bool table_for(const ps_plan* plan, int spin, TabRef& t) {
   const ps_plan* owner = plan->is_band ? plan->parent : plan;
@@ -136,6 +138,7 @@ bool table_for(const ps_plan* plan, int spin, TabRef& t) {
   t.nwork = owner->p.tab_nwork;
   t.Rh_table = owner->p.Rh;
   t.toff = owner->p.Rh - plan->p.Rh;
+  t.fmt = owner->p.tab_fmt[spin];
   return true;
 }
 
@@ -179,7 +182,8 @@ int ps_plan_create(int nside, int lmax, int mmax, int spin_mask, int prec, ps_pl
   P.R = 4 * nside - 1; P.Rh = 2 * nside;
   P.npix = 12 * int64_t(nside) * nside;
   P.nalm = int64_t(lmax + 1) * (lmax + 2) / 2;
-  for (int s = 0; s < 4; ++s) { P.d_seed[s] = nullptr; P.d_tab[s] = nullptr; }
+  for (int s = 0; s < 4; ++s) { P.d_seed[s] = nullptr; P.d_tab[s] = nullptr; P.tab_fmt[s] = PS_TAB_TF32X3; }
+  P.tab_fmt_build = PS_TAB_TF32X3;
   P.d_tab_off = nullptr;
   P.d_tab_work = nullptr;
   P.tab_nwork = 0;
@@ -430,7 +434,15 @@ int ps_plan_destroy(ps_plan* plan) {
 int ps_plan_table_bytes(const ps_plan* plan, int spin, size_t* bytes) {
   if (!plan || !bytes || spin < 0 || spin > 3) return PS_ERR_INVALID;
   const ps::Plan& P = plan->p;
-  *bytes = ps::tab_bytes(P.Rh, P.lmax, P.mmax, spin);
+  *bytes = P.tab_fmt_build == PS_TAB_BF16X3 ? ps::tab3_bytes(P.Rh, P.lmax, P.mmax, spin)
+                                             : ps::tab_bytes(P.Rh, P.lmax, P.mmax, spin);
+  return PS_OK;
+}
+
+int ps_plan_set_table_format(ps_plan* plan, int format) {
+  if (!plan || (format != PS_TAB_TF32X3 && format != PS_TAB_BF16X3)) return PS_ERR_INVALID;
+  if (plan->is_band || plan->p.prec != PS_PREC_MIXED) return PS_ERR_UNSUPPORTED;
+  plan->p.tab_fmt_build = format;
   return PS_OK;
 }
 
@@ -470,12 +482,17 @@ int ps_plan_build_table(ps_plan* plan, int spin, cudaStream_t stream) {
     P.tab_nwork = int(work.size());
   }
   void* t = nullptr;
-  if (cudaMalloc(&t, ps::tab_bytes(P.Rh, P.lmax, P.mmax, spin)) != cudaSuccess) {
+  const int fmt = P.tab_fmt_build;
+  const size_t tb = fmt == PS_TAB_BF16X3 ? ps::tab3_bytes(P.Rh, P.lmax, P.mmax, spin)
+                                         : ps::tab_bytes(P.Rh, P.lmax, P.mmax, spin);
+  if (cudaMalloc(&t, tb) != cudaSuccess) {
     cudaGetLastError();
     return PS_ERR_NOMEM;
   }
-  const int rc = ps::launch_tab_gen(P, spin, P.d_tab_off, static_cast<float*>(t), stream);
+  const int rc = fmt == PS_TAB_BF16X3 ? ps::launch_tab3_gen(P, spin, P.d_tab_off, static_cast<uint16_t*>(t), stream)
+                                      : ps::launch_tab_gen(P, spin, P.d_tab_off, static_cast<float*>(t), stream);
   if (rc != PS_OK) { cudaFree(t); return rc; }
+  P.tab_fmt[spin] = fmt;
   plan->tab_alloc[spin] = t;
   P.d_tab[spin] = static_cast<float*>(t);
   return PS_OK;
@@ -595,7 +612,8 @@ int ps_legendre_synthesis(const ps_plan* plan, const double* alm, double* phase,
                                              align256(size_t(P.nalm) * batch * ncomp * sizeof(double2)));
     TabRef tr;
     if (table_for(plan, spin, tr))
-      rc = ps::launch_tab_synth(P, tr.tab, tr.off, tr.Rh_table, tr.toff, almT, ph32, batch, spin, P.d_err, stream);
+      rc = ps::launch_tab_synth(P, tr.tab, tr.off, tr.Rh_table, tr.toff, almT, ph32, batch, spin, P.d_err, stream,
+                                tr.fmt);
     else
       rc = ps::launch_legendre_synth_tc(P, almT, ph32, batch, spin, P.d_err, stream);
     if (rc) return rc;
@@ -626,7 +644,7 @@ int ps_legendre_adjoint(const ps_plan* plan, const double* phase, double* alm, i
     if (table_for(plan, spin, tr))
       return ps::launch_tab_adj(P, tr.tab, tr.off, tr.work, tr.nwork, tr.Rh_table, tr.toff, ph32,
                                 reinterpret_cast<double2*>(alm), batch, spin, scale, int64_t(ncomp) * P.nalm, nullptr,
-                                P.d_err, stream);
+                                P.d_err, stream, tr.fmt);
     const int ch = adjoint_chunk(P, batch, spin);
     for (int b0 = 0; b0 < batch; b0 += ch) {
       const int bc = std::min(ch, batch - b0);
@@ -684,7 +702,8 @@ int ps_synthesis(const ps_plan* plan, const double* alm, double* map, int batch,
     float2* phase = reinterpret_cast<float2*>(phase_ptr);
     TabRef tr;
     if (table_for(plan, spin, tr))
-      rc = ps::launch_tab_synth(P, tr.tab, tr.off, tr.Rh_table, tr.toff, almT, phase, batch, spin, P.d_err, stream);
+      rc = ps::launch_tab_synth(P, tr.tab, tr.off, tr.Rh_table, tr.toff, almT, phase, batch, spin, P.d_err, stream,
+                                tr.fmt);
     else
       rc = ps::launch_legendre_synth_tc(P, almT, phase, batch, spin, P.d_err, stream);
     if (rc) return rc;
@@ -736,7 +755,7 @@ int ps_adjoint(const ps_plan* plan, const double* map, double* alm, int batch, i
     if (table_for(plan, spin, tr))
       return ps::launch_tab_adj(P, tr.tab, tr.off, tr.work, tr.nwork, tr.Rh_table, tr.toff, phase,
                                 reinterpret_cast<double2*>(alm), batch, spin, scale, int64_t(ncomp) * P.nalm, nullptr,
-                                P.d_err, stream);
+                                P.d_err, stream, tr.fmt);
     const int ch = adjoint_chunk(P, batch, spin);
     for (int b0 = 0; b0 < batch; b0 += ch) {
       const int bc = std::min(ch, batch - b0);
@@ -787,6 +806,7 @@ struct RoundtripView {
   const int* cls_off_n;
   const int* cls_cnt_n;
   int ncls;
+  int fmt;
 };
 int roundtrip_view(const ps_plan* plan, int spin, RoundtripView& v) {
   if (plan->is_band || plan->p.prec != PS_PREC_MIXED) return PS_ERR_UNSUPPORTED;
@@ -805,6 +825,7 @@ int roundtrip_view(const ps_plan* plan, int spin, RoundtripView& v) {
   v.cls_off_n = plan->cls_off_n.data();
   v.cls_cnt_n = plan->cls_cnt_n.data();
   v.ncls = int(plan->cls_len.size());
+  v.fmt = tr.fmt;
   return PS_OK;
 }
 
@@ -815,7 +836,7 @@ struct BandView {
   const float* tab;
   const int64_t* off;
   const int2* work;
-  int nwork, Rh_table, toff;
+  int nwork, Rh_table, toff, fmt;
 };
 int band_view(const ps_plan* band, int spin, BandView& v) {
   if (!band || !band->is_band || band->p.prec != PS_PREC_MIXED) return PS_ERR_UNSUPPORTED;
@@ -829,6 +850,7 @@ int band_view(const ps_plan* band, int spin, BandView& v) {
   v.nwork = tr.nwork;
   v.Rh_table = tr.Rh_table;
   v.toff = tr.toff;
+  v.fmt = tr.fmt;
   return PS_OK;
 }
 }  // namespace ps

@@ -18,10 +18,10 @@ struct ps_plan;
 
 namespace ps {
 int launch_tab_synth(const Plan& P, const float* table, const int64_t* d_blockoff, int Rh_table, int toff,
-                     const double2* almT, float2* phase, int B, int spin, int* err_flag, cudaStream_t st);
+                     const double2* almT, float2* phase, int B, int spin, int* err_flag, cudaStream_t st, int fmt);
 int launch_tab_adj(const Plan& P, const float* table, const int64_t* d_blockoff, const int2* d_work, int nwork,
                    int Rh_table, int toff, const float2* phase, double2* alm, int B, int spin, double scale,
-                   int64_t out_stride, const double* lscale, int* err_flag, cudaStream_t st);
+                   int64_t out_stride, const double* lscale, int* err_flag, cudaStream_t st, int fmt);
 int launch_ring_roundtrip_f32(const Plan& P, const int* d_list, int nrings, int work_len, float2* phase,
                               const double* weight, int nf, int pack, cudaStream_t st);
 
@@ -61,6 +61,7 @@ struct RoundtripView {
   const int* cls_off_n;
   const int* cls_cnt_n;
   int ncls;
+  int fmt;
 };
 int roundtrip_view(const ps_plan* plan, int spin, RoundtripView& v);
 
@@ -106,7 +107,7 @@ extern "C" int ps_sht_weighted_roundtrip(const ps_plan* plan, const double* alm_
                                                       almT, batch, ncomp, P.nalm);
     PS_LAUNCH_CHECK();
   }
-  rc = ps::launch_tab_synth(P, v.tab, v.off, P.Rh, 0, almT, phase, batch, spin, P.d_err, stream);
+  rc = ps::launch_tab_synth(P, v.tab, v.off, P.Rh, 0, almT, phase, batch, spin, P.d_err, stream, v.fmt);
   if (rc) return rc;
   for (int c = 0; c < v.ncls; ++c) {
     rc = ps::launch_ring_roundtrip_f32(P, v.ring_lists + (spin ? v.cls_off[c] : v.cls_off_n[c]),
@@ -115,5 +116,5 @@ extern "C" int ps_sht_weighted_roundtrip(const ps_plan* plan, const double* alm_
     if (rc) return rc;
   }
   return ps::launch_tab_adj(P, v.tab, v.off, v.work, v.nwork, P.Rh, 0, phase, reinterpret_cast<double2*>(alm_out),
-                            batch, spin, scale, alm_stride, lscale, P.d_err, stream);
+                            batch, spin, scale, alm_stride, lscale, P.d_err, stream, v.fmt);
 }

@@ -40,7 +40,7 @@ def nalm(lmax):
 
 class SHTPlan:
     def __init__(self, nside, lmax=None, spins=(0, 1, 2, 3), prec="fp64", device=None, autotune=True,
-                 tables="auto", table_fraction=None):
+                 tables="auto", table_fraction=None, table_format=None):
         if not torch.cuda.is_available():
             raise RuntimeError("the CUDA backend needs a GPU (no CPU fallback)")
         self.nside = int(nside)
@@ -59,6 +59,15 @@ class SHTPlan:
                       _lib.PS_PREC_FP64 if prec == "fp64" else _lib.PS_PREC_MIXED, ctypes.byref(h))
         self._h = h
         self._ws = None
+        # Legendre table format of a mixed plan: 'tf32x3' (FP32 values, split by the kernels) or
+        # 'bf16x3' (BF16 hi + mid + lo planes in the tensor core's operand layout, 1.5x the bytes)
+        if table_format is None:
+            table_format = os.environ.get("PS_TABLE_FORMAT", "tf32x3")
+        if table_format not in ("tf32x3", "bf16x3"):
+            raise ValueError("table_format must be 'tf32x3' or 'bf16x3'")
+        self.table_format = table_format
+        if prec != "fp64":
+            _lib.call("ps_plan_set_table_format", h, 1 if table_format == "bf16x3" else 0)
         # autotuning: tile shapes of this plan and, for mixed precision, an FP64 plan
         # beside it for the small-batch path
         self._h64 = None

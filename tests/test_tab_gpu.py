@@ -3,8 +3,8 @@ backend: batches that fill several map groups (up to 32 maps of spin 0 or 16 of
 spin s per CTA), orders with several l groups, and band plans (ps_plan_band) that
 read the parent's table at their ring offset.  Tolerances as for the mixed
 backend: 1e-5 relative (max-norm) per transform at these sizes (the FP32 phases
-and FFTs, TF32x3 products and the tensor core's truncating accumulation over
-32-term stages)."""
+and FFTs, TF32x3 or BF16x3 products and the tensor core's truncating accumulation
+over 32-term stages), for both table formats."""
 import ctypes
 
 import numpy as np
@@ -26,16 +26,17 @@ def _rel(x, ref):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fmt", ["tf32x3", "bf16x3"])
 @pytest.mark.parametrize("nside,lmax", [(16, 47), (64, 200), (256, 511)])
 @pytest.mark.parametrize("spin", [0, 1, 2])
 @pytest.mark.parametrize("batch", [2, 33, 70])
-def test_table_transforms_vs_fp64(nside, lmax, spin, batch):
+def test_table_transforms_vs_fp64(nside, lmax, spin, batch, fmt):
     import torch
     from polyspec_b200.sht import SHTPlan
     if nside == 256 and batch == 70:
         batch = 34
     p64 = SHTPlan(nside, lmax, prec="fp64", autotune=False)
-    pmx = SHTPlan(nside, lmax, prec="mixed", autotune=False, tables=True)
+    pmx = SHTPlan(nside, lmax, prec="mixed", autotune=False, tables=True, table_format=fmt)
     alm = _alm(p64, batch, spin, 10 * nside + spin + batch)
     out = pmx.synthesis(alm, spin)
     ref = p64.synthesis(alm, spin)
@@ -52,16 +53,17 @@ def test_table_transforms_vs_fp64(nside, lmax, spin, batch):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fmt", ["tf32x3", "bf16x3"])
 @pytest.mark.parametrize("nside,lmax,k", [(16, 40, 5), (64, 150, 13), (128, 256, 64)])
 @pytest.mark.parametrize("spin", [0, 2])
-def test_table_band_plan_vs_fp64(nside, lmax, k, spin):
+def test_table_band_plan_vs_fp64(nside, lmax, k, spin, fmt):
     """Legendre stages of a band plan (the k ring pairs nearest the equator) of a mixed plan
     with a table, against the band plan of an FP64 plan: ps_legendre_synthesis and the adjoint."""
     import torch
     from polyspec_b200 import _lib
     from polyspec_b200.sht import SHTPlan
     p64 = SHTPlan(nside, lmax, prec="fp64", autotune=False)
-    pmx = SHTPlan(nside, lmax, prec="mixed", autotune=False, tables=True)
+    pmx = SHTPlan(nside, lmax, prec="mixed", autotune=False, tables=True, table_format=fmt)
     assert pmx.build_table(spin, force=True)
     bands = {}
     for name, P in (("fp64", p64), ("mixed", pmx)):
@@ -115,6 +117,10 @@ def test_table_sizes_and_refusals():
     nquads = 128 // 4
     assert pmx.table_bytes(0) == nblk * nquads * 2 * (1 * 128 + 4) * 4
     assert pmx.table_bytes(2) == nblk * nquads * 2 * (2 * 128 + 4) * 4
+    # BF16x3: per block and slab of 16 rings, 3 planes of (ncomp x 2 parities x 32 positions x 16 rings)
+    p3 = SHTPlan(nside, lmax, prec="mixed", autotune=False, tables=False, table_format="bf16x3")
+    assert p3.table_bytes(0) == nblk * (128 // 16) * 3 * 2 * 32 * 16 * 2
+    assert p3.table_bytes(2) == nblk * (128 // 16) * 3 * 2 * 2 * 32 * 16 * 2
     p64 = SHTPlan(nside, lmax, prec="fp64", autotune=False)
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     assert _lib.lib().ps_plan_build_table(p64._h, 0, st) == _lib.PS_ERR_UNSUPPORTED
