@@ -19,8 +19,8 @@
 // grid is (groups of fields, rings of one work length), fields fastest, so that the
 // CTAs of all maps of a ring run together and share in L2 the sectors of the ring's
 // phases (stored map-innermost).
-// FFTs are radix-2 with stages fused in pairs (one barrier and one shared-memory
-// round trip per two stages): decimation in frequency for power-of-two rings,
+// FFTs are radix-2 with stages fused in threes (one barrier and one shared-memory
+// round trip per three stages): decimation in frequency for power-of-two rings,
 // Bluestein's chirp-z convolution of power-of-two length M >= 2 nphi - 1 for the
 // others.  Rings are launched in classes of equal work length.  The ring rotations
 // e^{i m phi0} and the Bluestein chirps come from tables of the plan (computed in FP64
@@ -48,28 +48,63 @@ __device__ __forceinline__ float2 twid(const float2* __restrict__ tw, int j, int
   return w;
 }
 
-// Decimation in frequency (natural order in, bit-reversed out) on a[0..2^logn),
-// by the T threads with local index u; stages fused in pairs.
+// Decimation in frequency (natural order in, bit-reversed out) on a[0..2^logn), by the T threads
+// with local index u; stages fused in threes (one barrier and one shared-memory round trip per
+// three radix-2 stages, the eight points of a butterfly group in registers), the last one or two
+// stages as one radix-2 or radix-4 pass.
 __device__ void fft_dif_f(float2* a, int logn, int sign, const float2* __restrict__ tw, int twlog, int u, int T) {
   const int n = 1 << logn;
   int s = logn;
-  for (; s >= 2; s -= 2) {
-    const int q = 1 << (s - 2);
-    for (int t = u; t < n / 4; t += T) {
-      const int blk = t >> (s - 2), j = t & (q - 1);
-      const int i0 = blk * 4 * q + j, i1 = i0 + q, i2 = i0 + 2 * q, i3 = i0 + 3 * q;
-      const float2 x0 = a[i0], x1 = a[i1], x2 = a[i2], x3 = a[i3];
-      const float2 y0 = fadd2(x0, x2), y2 = fmul2(fsub2(x0, x2), twid(tw, j, s, twlog, sign));
-      const float2 y1 = fadd2(x1, x3), y3 = fmul2(fsub2(x1, x3), twid(tw, j + q, s, twlog, sign));
-      const float2 w = twid(tw, j, s - 1, twlog, sign);
-      a[i0] = fadd2(y0, y1);
-      a[i1] = fmul2(fsub2(y0, y1), w);
-      a[i2] = fadd2(y2, y3);
-      a[i3] = fmul2(fsub2(y2, y3), w);
+  for (; s >= 3; s -= 3) {
+    const int q = 1 << (s - 3);
+    for (int t = u; t < n / 8; t += T) {
+      const int blk = t >> (s - 3), j = t & (q - 1);
+      const int i0 = blk * 8 * q + j;
+      float2 x[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) x[k] = a[i0 + k * q];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {  // stage s: pairs (k, k + 4)
+        const float2 d = fsub2(x[k], x[k + 4]);
+        x[k] = fadd2(x[k], x[k + 4]);
+        x[k + 4] = fmul2(d, twid(tw, j + k * q, s, twlog, sign));
+      }
+      const float2 w0 = twid(tw, j, s - 1, twlog, sign), w1 = twid(tw, j + q, s - 1, twlog, sign);
+#pragma unroll
+      for (int h = 0; h < 8; h += 4) {  // stage s - 1: pairs (k, k + 2) of each half
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const float2 d = fsub2(x[h + k], x[h + k + 2]);
+          x[h + k] = fadd2(x[h + k], x[h + k + 2]);
+          x[h + k + 2] = fmul2(d, k ? w1 : w0);
+        }
+      }
+      const float2 w2 = twid(tw, j, s - 2, twlog, sign);
+#pragma unroll
+      for (int k = 0; k < 8; k += 2) {  // stage s - 2: pairs (k, k + 1)
+        const float2 d = fsub2(x[k], x[k + 1]);
+        x[k] = fadd2(x[k], x[k + 1]);
+        x[k + 1] = fmul2(d, w2);
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[i0 + k * q] = x[k];
     }
     __syncthreads();
   }
-  if (s == 1) {
+  if (s == 2) {
+    for (int t = u; t < n / 4; t += T) {
+      const int i0 = 4 * t;
+      const float2 x0 = a[i0], x1 = a[i0 + 1], x2 = a[i0 + 2], x3 = a[i0 + 3];
+      const float2 y0 = fadd2(x0, x2), y2 = fmul2(fsub2(x0, x2), twid(tw, 0, 2, twlog, sign));
+      const float2 y1 = fadd2(x1, x3), y3 = fmul2(fsub2(x1, x3), twid(tw, 1, 2, twlog, sign));
+      const float2 w = twid(tw, 0, 1, twlog, sign);
+      a[i0] = fadd2(y0, y1);
+      a[i0 + 1] = fmul2(fsub2(y0, y1), w);
+      a[i0 + 2] = fadd2(y2, y3);
+      a[i0 + 3] = fmul2(fsub2(y2, y3), w);
+    }
+    __syncthreads();
+  } else if (s == 1) {
     for (int t = u; t < n / 2; t += T) {
       const float2 x0 = a[2 * t], x1 = a[2 * t + 1];
       a[2 * t] = fadd2(x0, x1);
@@ -79,11 +114,12 @@ __device__ void fft_dif_f(float2* a, int logn, int sign, const float2* __restric
   }
 }
 
-// Decimation in time (bit-reversed order in, natural out); stages fused in pairs.
+// Decimation in time (bit-reversed order in, natural out): the first one or two stages as one
+// radix-2 or radix-4 pass, then stages fused in threes.
 __device__ void fft_dit_f(float2* a, int logn, int sign, const float2* __restrict__ tw, int twlog, int u, int T) {
   const int n = 1 << logn;
   int s = 1;
-  if (logn & 1) {
+  if (logn % 3 == 1) {
     for (int t = u; t < n / 2; t += T) {
       const float2 x0 = a[2 * t], x1 = a[2 * t + 1];
       a[2 * t] = fadd2(x0, x1);
@@ -91,22 +127,56 @@ __device__ void fft_dit_f(float2* a, int logn, int sign, const float2* __restric
     }
     __syncthreads();
     s = 2;
-  }
-  for (; s + 1 <= logn; s += 2) {
-    const int q = 1 << (s - 1);
+  } else if (logn % 3 == 2) {
     for (int t = u; t < n / 4; t += T) {
-      const int blk = t >> (s - 1), j = t & (q - 1);
-      const int i0 = blk * 4 * q + j, i1 = i0 + q, i2 = i0 + 2 * q, i3 = i0 + 3 * q;
-      const float2 ws = twid(tw, j, s, twlog, sign);
-      const float2 v1 = fmul2(a[i1], ws), v3 = fmul2(a[i3], ws);
-      const float2 x0 = a[i0], x2 = a[i2];
+      const int i0 = 4 * t;
+      const float2 ws = twid(tw, 0, 1, twlog, sign);
+      const float2 v1 = fmul2(a[i0 + 1], ws), v3 = fmul2(a[i0 + 3], ws);
+      const float2 x0 = a[i0], x2 = a[i0 + 2];
       const float2 y0 = fadd2(x0, v1), y1 = fsub2(x0, v1), y2 = fadd2(x2, v3), y3 = fsub2(x2, v3);
-      const float2 v2 = fmul2(y2, twid(tw, j, s + 1, twlog, sign));
-      const float2 v3b = fmul2(y3, twid(tw, j + q, s + 1, twlog, sign));
+      const float2 v2 = fmul2(y2, twid(tw, 0, 2, twlog, sign));
+      const float2 v3b = fmul2(y3, twid(tw, 1, 2, twlog, sign));
       a[i0] = fadd2(y0, v2);
-      a[i2] = fsub2(y0, v2);
-      a[i1] = fadd2(y1, v3b);
-      a[i3] = fsub2(y1, v3b);
+      a[i0 + 2] = fsub2(y0, v2);
+      a[i0 + 1] = fadd2(y1, v3b);
+      a[i0 + 3] = fsub2(y1, v3b);
+    }
+    __syncthreads();
+    s = 3;
+  }
+  for (; s + 2 <= logn; s += 3) {
+    const int q = 1 << (s - 1);
+    for (int t = u; t < n / 8; t += T) {
+      const int blk = t >> (s - 1), j = t & (q - 1);
+      const int i0 = blk * 8 * q + j;
+      float2 x[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) x[k] = a[i0 + k * q];
+      const float2 w0 = twid(tw, j, s, twlog, sign);
+#pragma unroll
+      for (int k = 0; k < 8; k += 2) {  // stage s: pairs (k, k + 1)
+        const float2 v = fmul2(x[k + 1], w0);
+        x[k + 1] = fsub2(x[k], v);
+        x[k] = fadd2(x[k], v);
+      }
+      const float2 w1a = twid(tw, j, s + 1, twlog, sign), w1b = twid(tw, j + q, s + 1, twlog, sign);
+#pragma unroll
+      for (int h = 0; h < 8; h += 4) {  // stage s + 1: pairs (k, k + 2) of each half
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const float2 v = fmul2(x[h + k + 2], k ? w1b : w1a);
+          x[h + k + 2] = fsub2(x[h + k], v);
+          x[h + k] = fadd2(x[h + k], v);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {  // stage s + 2: pairs (k, k + 4)
+        const float2 v = fmul2(x[k + 4], twid(tw, j + k * q, s + 2, twlog, sign));
+        x[k + 4] = fsub2(x[k], v);
+        x[k] = fadd2(x[k], v);
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[i0 + k * q] = x[k];
     }
     __syncthreads();
   }
