@@ -77,6 +77,8 @@ def parse():
     p.add_argument("--nside", type=int, default=1024)
     p.add_argument("--lmax", type=int, default=2048)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--sims-per-step", type=int, default=1,
+                   help="Fisher contributions per step, their K (N_p + 1) systems solved as one batch")
     p.add_argument("--workload", default="fisher-teb", choices=["fisher-teb", "pspec-t64"],
                    help="fisher-teb: the headline (default); pspec-t64: PSpecBin T at Nside 64, lmax 191, ideal "
                         "S^-1 of the latitude-masked map, Fisher from seeds 1-10, beside the CPU oracle port")
@@ -247,15 +249,28 @@ def psb_rows_maps(base, mask, l_bins, a_lm):
     return psb.d_mask[None] * base.to_map_batch(alms)
 
 
-def timed_steps(psb, seeds, batched, wts=None):
-    """CUDA-event time (ms) of compute_fisher_contribution over `seeds` (GRF drawn on the device
-    inside each step) and the CG steps of each solve of the last one."""
+def fisher_step(psb, seeds, batched, a_lms=None):
+    """One step: the Fisher contributions of the simulations `seeds` (GRF drawn on the device, or host
+    a_lms), several as one batched solve (PSpecBin.compute_fisher_contributions)."""
+    if len(seeds) == 1:
+        return psb.compute_fisher_contribution(seeds[0], batched=batched, rng="device",
+                                               a_lm=None if a_lms is None else a_lms[0])
+    return psb.compute_fisher_contributions(seeds, rng="device", a_lms=a_lms)
+
+
+def groups(seeds, k):
+    return [seeds[i:i + k] for i in range(0, len(seeds), k)]
+
+
+def timed_steps(psb, seed_groups, batched, wts=None):
+    """CUDA-event time (ms) of the Fisher steps over `seed_groups` (GRF drawn on the device inside each
+    step) and the CG steps of each solve of the last one."""
     import torch
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record()
-    for s in seeds:
-        psb.compute_fisher_contribution(s, batched=batched, rng="device")
+    for g in seed_groups:
+        fisher_step(psb, g, batched)
     e1.record()
     torch.cuda.synchronize()
     iters = None
@@ -400,9 +415,11 @@ def run_cuda(a):
     mask = setup[3]
     base, wts, psb, setup_s = build_arm(a, setup, a.prec, a.precond, a.tables)
     batched = not a.unbatched
-    seeds = replica_seeds(rank, a.warmup + 2 * a.steps)
-    for s in seeds[:a.warmup]:
-        psb.compute_fisher_contribution(s, batched=batched, rng="device")
+    K = max(1, a.sims_per_step)
+    seeds = replica_seeds(rank, (a.warmup + 2 * a.steps) * K)
+    steps_seeds = groups(seeds, K)  # warm-up, timed, end-to-end steps
+    for g in steps_seeds[:a.warmup]:
+        fisher_step(psb, g, batched)
     torch.cuda.synchronize()
     plan = base.plan()
     tables_used = {s: bool(plan.has_table(s)) for s in (0, 2)} if a.prec != "fp64" else {0: False, 2: False}
@@ -421,7 +438,7 @@ def run_cuda(a):
     clk.start()
     # a profiler started with --profile-from-start off (ncu) captures the timed steps only
     torch.cuda.profiler.start()
-    t_ms, solve_iters = timed_steps(psb, seeds[a.warmup:a.warmup + a.steps], batched, wts)
+    t_ms, solve_iters = timed_steps(psb, steps_seeds[a.warmup:a.warmup + a.steps], batched, wts)
     torch.cuda.profiler.stop()
     barrier()
     clocks = clk.stop()
@@ -431,33 +448,34 @@ def run_cuda(a):
     rev = (base.n_SHTs_reverse - r0) / a.steps
     if world > 1:
         t_ms = max_over_ranks(t_ms, "cuda")
-    value = world * a.steps / (t_ms / 1e3)
+    value = world * a.steps * K / (t_ms / 1e3)
 
     # ---- end to end through the public API: host a_lm (pinned) in, the Fisher matrix out
-    host_a = [base.generate_data(seed=s + int(1e7), output_type="harmonic", deconvolve_beam=True, rng="device")
-              .cpu().pin_memory() for s in seeds[a.warmup + a.steps:]]
+    e2e_groups = steps_seeds[a.warmup + a.steps:]
+    host_a = [[base.generate_data(seed=s + int(1e7), output_type="harmonic", deconvolve_beam=True, rng="device")
+               .cpu().pin_memory() for s in g] for g in e2e_groups]
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     t0 = time.time()
-    for k, s in enumerate(seeds[a.warmup + a.steps:]):
-        fish = psb.compute_fisher_contribution(s, a_lm=host_a[k], batched=batched)
+    for k, g in enumerate(e2e_groups):
+        fish = fisher_step(psb, g, batched, a_lms=host_a[k])
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = max(e0.elapsed_time(e1), (time.time() - t0) * 1e3)
     barrier()
     if world > 1:
         e2e_ms = max_over_ranks(e2e_ms, "cuda")
-    e2e = {"value": world * a.steps / (e2e_ms / 1e3), "unit": UNIT,
-           "h2d_bytes_per_step": int(host_a[0].numel() * host_a[0].element_size()),
+    e2e = {"value": world * a.steps * K / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(sum(h.numel() * h.element_size() for h in host_a[0])),
            "d2h_bytes_per_step": int(fish.nbytes)}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": t_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if a.prec == "fp64" else "f32+tf32", "data": "synthetic",
             "config": dict(workload_config(a), parallelism="replicas x%d" % world, prec=a.prec,
-                           preconditioner=a.precond, batched=batched,
+                           preconditioner=a.precond, batched=batched, sims_per_step=K,
                            legendre_tables={"spin%d" % s: v for s, v in tables_used.items()}),
             "measured_arm": "%s precision, %s preconditioner%s" % (
                 a.prec, {"cut": "masked-band (cut)", "harmonic": "harmonic", "learned": "learned on cut"}[a.precond],
@@ -467,7 +485,8 @@ def run_cuda(a):
             "roofline": roofline(a, stats, clocks, tables_used), "clocks": clocks,
             "sht_teb_per_step": {"synthesis": rev / 2.0, "adjoint": fwd / 2.0},
             "cg_iters_of_each_solve": solve_iters,
-            "kernel_ms": {k: round(v[1], 3) for k, v in stats.items() if v[0]}}
+            "kernel_ms": {k: round(v[1], 3) for k, v in stats.items() if v[0]},
+            "peak_device_gb": round(torch.cuda.max_memory_allocated() / 1e9, 1)}
 
     if a.prec != "fp64" and not a.no_fp64_compare and world == 1:
         # ---- accuracy on the timed configuration, then the FP64 arms
@@ -485,10 +504,10 @@ def run_cuda(a):
             "fisher": fisher_errs(fish_mx, fish_64), "tolerance": 1e-6,
             "cg_steps_alm_solve": {"mixed": ith_mx, "fp64": ith_64},
             "cg_steps_fisher_solves_equal": itf_mx == itf_64}
-        psb64.compute_fisher_contribution(99991, batched=batched, rng="device")  # warm-up
-        ms64, it64 = timed_steps(psb64, [99992 + i for i in range(a.fp64_steps)], batched, wts64)
+        fisher_step(psb64, [99991 - j for j in range(K)], batched)  # warm-up
+        ms64, it64 = timed_steps(psb64, groups([99992 + i for i in range(a.fp64_steps * K)], K), batched, wts64)
         line["fp64_same_preconditioner_gpu"] = {
-            "value": a.fp64_steps / (ms64 / 1e3), "unit": UNIT, "ms_per_step": ms64 / a.fp64_steps,
+            "value": a.fp64_steps * K / (ms64 / 1e3), "unit": UNIT, "ms_per_step": ms64 / a.fp64_steps,
             "steps": a.fp64_steps, "warmup": 1, "dtype": "f64", "preconditioner": a.precond,
             "preconditioner_setup_s": setup64, "cg_iters_of_each_solve": it64,
             "note": "FP64 backend (FP64 Legendre + FP64 ring FFTs), same preconditioner, batching and stopping rule"}
@@ -496,10 +515,10 @@ def run_cuda(a):
         release()
         if a.precond != "harmonic":
             base_h, wts_h, psb_h, _ = build_arm(a, setup, "fp64", "harmonic", "off")
-            psb_h.compute_fisher_contribution(99981, batched=batched, rng="device")
-            msh, ith = timed_steps(psb_h, [99982 + i for i in range(a.fp64_steps)], batched, wts_h)
+            fisher_step(psb_h, [99981 - j for j in range(K)], batched)
+            msh, ith = timed_steps(psb_h, groups([99982 + i for i in range(a.fp64_steps * K)], K), batched, wts_h)
             line["plain_fp64_gpu"] = {
-                "value": a.fp64_steps / (msh / 1e3), "unit": UNIT, "ms_per_step": msh / a.fp64_steps,
+                "value": a.fp64_steps * K / (msh / 1e3), "unit": UNIT, "ms_per_step": msh / a.fp64_steps,
                 "steps": a.fp64_steps, "warmup": 1, "dtype": "f64", "preconditioner": "harmonic",
                 "cg_iters_of_each_solve": ith,
                 "note": "FP64 backend with the reference's harmonic CG, same batching and stopping rule"}
@@ -518,13 +537,14 @@ def run_cuda(a):
         t_step = s.step()
         it_plain = (line.get("plain_fp64_gpu") or {}).get("cg_iters_of_each_solve")
         if it_plain:
-            per_sim = len(it_plain) * s.t_setup + sum(it_plain) * t_step
+            per_sim = (len(it_plain) * s.t_setup + sum(it_plain) * t_step) / K
             line["cpu_baseline"] = {
                 "value": 1.0 / per_sim, "unit": UNIT, "cores": s.cores, "kind": "port",
                 "sample": "one CG step (%.2f s: TEB synthesis + adjoint, harmonic preconditioner) and the fixed cost "
                           "of one solve (%.1f s) of the oracle restatement at the full workload, scaled by the %d CG "
-                          "steps of the 33 solves of the reference algorithm (harmonic CG, FP64) counted on the "
-                          "plain FP64 arm of this run" % (t_step, s.t_setup, sum(it_plain))}
+                          "steps of the %d solves of %d simulation(s) of the reference algorithm (harmonic CG, FP64) "
+                          "counted on the plain FP64 arm of this run" % (t_step, s.t_setup, sum(it_plain),
+                                                                         len(it_plain), K)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

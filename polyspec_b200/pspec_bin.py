@@ -144,6 +144,42 @@ class PSpecBin:
         fish = 0.5 * torch.real(Q_S.conj() @ Q_A.T)
         return fish.cpu().numpy()
 
+    def compute_fisher_contributions(self, seeds, verb=False, rng='numpy', a_lms=None):
+        """Fisher contributions [K, N_p, N_p] of K GRF simulations (seeds, or beam-deconvolved harmonics
+        a_lms), each as compute_fisher_contribution (polyspec/pspec_bin.py:94-164), with one batched S^-1
+        solve of all K (N_p + 1) right-hand sides.  The systems are independent and each keeps its own
+        stopping test, so the solve of the union is the solves of the parts; batching the simulations
+        shares the last CG steps, which few systems of each simulation still take, between them."""
+        K = len(a_lms) if a_lms is not None else len(seeds)
+        if self.ones_mask or not hasattr(self.applySinv, 'batched'):
+            return np.stack([self.compute_fisher_contribution(None if seeds is None else seeds[k], verb=verb,
+                                                              batched=True, rng=rng,
+                                                              a_lm=None if a_lms is None else a_lms[k])
+                             for k in range(K)])
+        alms, nrows = [], []
+        for k in range(K):
+            if a_lms is None:
+                a_lm = self.base.generate_data(seed=seeds[k] + int(1e7), output_type='harmonic',
+                                               deconvolve_beam=True, rng=rng)
+            else:
+                a_lm = a_lms[k]
+            a_lm, _ = self.base._in(a_lm, torch.complex128)
+            rows = self._Q2_rows(self.base.applyAinv(a_lm, input_type='harmonic'))
+            alms.append(torch.stack([self.d_beam * a_lm] + [self.d_beam * r for r in rows]))
+            nrows.append(len(rows))
+        maps = self.d_mask[None] * self.base.to_map_batch(torch.cat(alms))
+        del alms
+        sol = self.applySinv.batched(maps)
+        del maps
+        out, o = [], 0
+        for k in range(K):
+            s = sol[o:o + nrows[k] + 1]
+            o += nrows[k] + 1
+            Q_S = torch.stack([(self.d_mw * r).reshape(-1) for r in self._Q2_rows(s[0])])
+            Q_A = s[1:].reshape(nrows[k], -1)
+            out.append(0.5 * torch.real(Q_S.conj() @ Q_A.T))
+        return torch.stack(out).cpu().numpy()
+
     def compute_fisher(self, N_it, verb=False):
         """Monte Carlo Fisher matrix over seeds 0..N_it-1 (polyspec/pspec_bin.py:166-179)."""
         fish = np.zeros((self.N_p, self.N_p))

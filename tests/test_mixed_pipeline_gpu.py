@@ -44,3 +44,26 @@ def test_mixed_pipeline_matches_fp64():
     f64s = p64.compute_fisher_contribution(1, a_lm=a, batched=False)
     assert np.linalg.norm(f64s - f64) / np.linalg.norm(f64) < 1e-10
     torch.cuda.synchronize()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,precond", [("mixed", "cut"), ("fp64", "harmonic")])
+def test_fisher_contributions_of_several_simulations(prec, precond):
+    """compute_fisher_contributions solves the K (N_p + 1) systems of K simulations as one batch; each
+    system keeps its own stopping test, so every contribution equals compute_fisher_contribution of its
+    simulation (to 1e-8 of sqrt(F_ii F_jj): only the reduction order of the batch's dot products differs)."""
+    from polyspec_b200 import PolySpec, Weightings, PSpecBin
+    from polyspec_b200 import workloads as W
+    nside, lmax = 32, 64
+    cl, cltot, beam, mask, noise, l_bins = W.cg_fisher_setup(nside, lmax, n_holes=40, fwhm_arcmin=40.0, nbins=4)
+    base = PolySpec(nside, dict(cltot), beam=list(beam), pol=True, lmax=lmax, prec=prec, autotune=False)
+    wts = Weightings(base, mask, dict(cl), noise_cov=noise)
+    app = wts.make_applySinv("optimal", preconditioner=precond, nstep=300, thresh=1e-10)
+    psb = PSpecBin(base, mask, app, l_bins, fields=["TT", "TE", "EE", "BB"])
+    a_lms = [base.generate_data(seed=200 + k, output_type="harmonic", deconvolve_beam=True) for k in range(3)]
+    many = psb.compute_fisher_contributions(None, a_lms=a_lms)
+    assert many.shape == (3, psb.N_p, psb.N_p)
+    for k in range(3):
+        one = psb.compute_fisher_contribution(0, a_lm=a_lms[k], batched=True)
+        scale = np.sqrt(np.outer(np.abs(np.diag(one)), np.abs(np.diag(one))))
+        assert np.max(np.abs(many[k] - one) / scale) < 1e-8, k
