@@ -452,6 +452,37 @@ int ps_kint_radial(const double* table, const double* x, int64_t nx, int tab_lmi
                    int nk, const double* kprod, int kstride, const double* T, int npol, int nl_T,
                    const double* r_arr, int nr, int lmin, int lmax, int nshift, int deriv, int lweight, int npol_out,
                    double* out, cudaStream_t stream);
+/* Collider templates (tauNL-light, tauNL-heavy).  Replace compute_collider_F_integral of
+ * polyspec/cython/k_integrals.pyx:496-545 (the collider p integral, :399-451, is ps_kint_radial on the real and
+ * imaginary parts of its kprod).
+ * ps_kint_collider_jlK: jlK[l][k][r] = j_l(K[k] r[r]) linearly interpolated from table [nl][nx] on the grid x
+ *   (interpolate_jlkr, :84-110; beyond the grid's end the last interval is extended).
+ * ps_kint_collider_F: out [2 nmax_F + 1][nLout][nr][nr] complex: F_{L,L+n}(r_i, r_j) = Sum_k (K_k - K_{k-1})
+ *   (f_{k-1} + f_k), f_k = Kprod[k] j_L(K_k r_i) j_{L+n}(K_k r_j) with j from jlK (rows from glmin), for
+ *   max(Lmin - nmax_F, 0) <= L <= Lmax + nmax_F, L >= 1, 1 <= L + n <= Lmax + nmax_F; Kprod complex [nK]. */
+int ps_kint_collider_jlK(const double* table, const double* x, int64_t nx, int nl, const double* K, int nK,
+                         const double* r, int nr, double* jlK, cudaStream_t stream);
+int ps_kint_collider_F(const double* jlK, int nl_tab, int glmin, const double* K, int nK, const double* Kprod, int nr,
+                       int Lmin, int Lmax, int nmax_F, int nLout, double* out, cudaStream_t stream);
+/* ps_tau_sum_collider_diag: tau_sum_n0_collider / tau_sum_nu0_collider (polyspec/cython/tauNL_utils.pyx:877-964):
+ *   *out = Sum over rows (rowL, rowM) with Lmin <= L <= Lmax of w_M Re(pref Sum_lam Sum_{j,k} F[L][j][k] w_j w_k
+ *   A[lam][row][j] conj(B[lam][row][k])), w_M = 1 (M = 0) or 2; A, B complex [nlam][nrow][nr], F complex
+ *   [nLF][nr][nr], nr <= 64.
+ * ps_tau_sum_collider_general: tau_sum_general_collider (tauNL_utils.pyx:723-875) for arrays A1 = arr1, A1c = arr1c,
+ *   A2 = arr2, A2c = arr2c [2s+1][nrow][nr] (rows of the L-list nLmin..nLmax, m-major), complex F
+ *   [2 nmax_F + 1][nLF][nr][nr], coupling coefficients coeffs [s + 1] complex (S = 0, 2, .., 2s); real_beta != 0
+ *   doubles the M != 0 rows, otherwise adds the m -> -m piece.  s <= 5, nr <= 64.
+ * Workspace of both: ps_tau_collider_workspace_bytes (depends on nrow only). */
+int ps_tau_collider_workspace_bytes(int64_t nrow, size_t* bytes);
+int ps_tau_sum_collider_diag(const double* A, const double* B, int nlam, const int* rowL, const int* rowM, int nrow,
+                             int Lmin, int Lmax, const double* F, int nLF, const double* w, int nr, double pref_re,
+                             double pref_im, double* out, void* workspace, size_t workspace_bytes,
+                             cudaStream_t stream);
+int ps_tau_sum_collider_general(const double* A1, const double* A1c, const double* A2, const double* A2c,
+                                const int* rowL, const int* rowM, int nrow, int nLmin, int nLmax, int Lmin, int Lmax,
+                                const double* F, int nLF, int nmax_F, const double* w, int nr, int s, int real_beta,
+                                const double* coeffs, double* out, void* workspace, size_t workspace_bytes,
+                                cudaStream_t stream);
 
 /* ------------------------------------------------------------- ideal bispectrum Fisher (BSpecBin.compute_fisher_ideal)
  * The 3j-symbol sums of polyspec/bspec_bin.py:699-827 as Gauss-Legendre quadratures of binned Wigner d-sums

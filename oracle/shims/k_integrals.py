@@ -22,7 +22,10 @@ Restated (same grids, branches and trapezium rule, vectorised):
   * compute_F_integral    :453-494 F_{L,L+n}(r, r') in closed form; GSL's lngamma and
                           hyperg_2F1 (GSL version unpinned by the reference) are
                           replaced by scipy's gammaln and hyp2f1.
-The collider integrals raise NotImplementedError.
+  * collider_p_integral   :399-451 p_integral's sum with kprod = (2/pi) k^(2+beta) P_zeta / 2
+                          (complex) for k >= k_coll;
+  * compute_collider_F_integral :496-545 F^{betaF}_{L,L+n}(r, r') by the trapezium rule
+                          over K <= K_coll, kprod = (2/pi) K^(2+betaF) P_zeta / 2.
 """
 import numpy as np
 from scipy.special import gammaln, hyp2f1, spherical_jn
@@ -64,7 +67,10 @@ def compute_bessel(x_arr, lmin, lmax, jlx_arr, nthreads):
 def interpolate_jlkr(x_arr, k_arr, r_arr, jlx_arr, nthreads):
     x_arr = np.asarray(x_arr)
     kr = np.asarray(k_arr)[None, :] * np.asarray(r_arr)[:, None]          # [nr, nk]
-    ix = np.searchsorted(x_arr, kr) - 1
+    # k r beyond the last grid point (the collider F set-up's K grid ends at 1.01 K_coll, past its y
+    # grid) reads past the reference's table; its integrand prefactor is zero there, so the clamped
+    # extrapolation stands in for it
+    ix = np.minimum(np.searchsorted(x_arr, kr) - 1, len(x_arr) - 2)
     dx = x_arr[ix + 1] - x_arr[ix]
     xp = (x_arr[ix + 1] - kr) / dx
     xm = (kr - x_arr[ix]) / dx
@@ -176,8 +182,42 @@ def compute_F_integral(r_arr, FLLs, Lmin, Lmax, nmax_F, ns, _pref, nthreads):
                             * (rj / ri) ** (L + n) * ri ** (1. - ns)
 
 
-def _missing(*a, **k):
-    raise NotImplementedError("this k-space integral is outside the oracle's scope")
+def collider_p_integral(k_arr, Pzeta_arr, Tl_arr, jlkr_all, beta, k_coll, lmin, lmax, arr_lmin, arr_lmax,
+                        this_nmax, nthreads, integs):
+    """p_lL^{beta,X}(r) (k_integrals.pyx:399-451): p_integral's sum with the complex
+    kprod = (2/pi) k^(2 + beta) P_zeta(k) / 2 for k >= k_coll, zero below."""
+    k_arr = np.asarray(k_arr)
+    kprod = np.where(k_arr >= k_coll, 2. / np.pi * k_arr.astype(np.complex128) ** (2. + beta)
+                     * np.asarray(Pzeta_arr) / 2., 0.)
+    for n in range(-this_nmax, this_nmax + 1):
+        lshift1 = min(0, lmin - arr_lmin + n)
+        lshift2 = max(0, lmin - arr_lmin + n)
+        for il in range(lmax - lmin + lshift1 + 1):
+            l = lmin - lshift1 + il
+            for X in range(len(Tl_arr)):
+                integs[this_nmax + n, l, X, :] += (-1.) ** l * _trapz(kprod, np.asarray(Tl_arr)[X, l][None],
+                                                                      jlkr_all[lshift2 + il], k_arr)
 
 
-collider_p_integral = compute_collider_F_integral = _missing
+def compute_collider_F_integral(K_arr, Pzeta_arr, jlK, betaF, K_coll, Lmin, Lmax, this_nmax_F, coll_nmax_F,
+                                nthreads, integs):
+    """F^{-2 beta}_{L,L+n}(r, r') (k_integrals.pyx:496-545): Sum_K dK (f_{K-1} + f_K),
+    f = (2/pi) K^(2 + betaF) P_zeta(K) / 2 j_L(K r) j_{L+n}(K r') for K <= K_coll (zero above),
+    with j from the interpolated [L - max(Lmin - coll_nmax_F, 0), r, K] table; n = 0 is
+    filled symmetrically from r' <= r."""
+    K_arr = np.asarray(K_arr)
+    Kprod = np.where(K_arr <= K_coll, 2. / np.pi * K_arr.astype(np.complex128) ** (2. + betaF)
+                     * np.asarray(Pzeta_arr) / 2., 0.)
+    jlK = np.asarray(jlK)
+    global_Lmin = max(Lmin - coll_nmax_F, 0)
+    dK = np.diff(K_arr)
+    for n in range(-this_nmax_F, this_nmax_F + 1):
+        for L in range(max(Lmin - this_nmax_F, 0), Lmax + this_nmax_F + 1):
+            if L + n < 1 or L < 1 or L + n > Lmax + this_nmax_F:
+                continue
+            ind1, ind2 = L - global_Lmin, L - global_Lmin + n
+            f = Kprod[None, None, :] * jlK[ind1][:, None, :] * jlK[ind2][None, :, :]
+            tmp = np.sum(dK * (f[..., :-1] + f[..., 1:]), axis=-1)
+            if n == 0:
+                tmp = np.tril(tmp) + np.tril(tmp, -1).T
+            integs[this_nmax_F + n, L] = tmp

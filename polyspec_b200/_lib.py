@@ -96,6 +96,18 @@ SIGNATURES = {
                                      _c_void_p, _c_void_p]),
     "ps_product_q_complex": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_int64, _c_void_p, _c_void_p,
                                       _c_void_p, _c_int, _c_void_p, _c_void_p]),
+    "ps_kint_collider_jlK": (_c_int, [_c_void_p, _c_void_p, _c_int64, _c_int, _c_void_p, _c_int, _c_void_p, _c_int,
+                                      _c_void_p, _c_void_p]),
+    "ps_kint_collider_F": (_c_int, [_c_void_p, _c_int, _c_int, _c_void_p, _c_int, _c_void_p, _c_int, _c_int, _c_int,
+                                    _c_int, _c_int, _c_void_p, _c_void_p]),
+    "ps_tau_collider_workspace_bytes": (_c_int, [_c_int64, ctypes.POINTER(_c_size_t)]),
+    "ps_tau_sum_collider_diag": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_void_p, _c_void_p, _c_int, _c_int, _c_int,
+                                          _c_void_p, _c_int, _c_void_p, _c_int, _c_double, _c_double, _c_void_p,
+                                          _c_void_p, _c_size_t, _c_void_p]),
+    "ps_tau_sum_collider_general": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                             _c_int, _c_int, _c_int, _c_int, _c_int, _c_void_p, _c_int, _c_int,
+                                             _c_void_p, _c_int, _c_int, _c_int, _c_void_p, _c_void_p, _c_void_p,
+                                             _c_size_t, _c_void_p]),
     "ps_tau_general_workspace_bytes": (_c_int, [_c_int, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_gaunt_row_table": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_int, _c_int, _c_void_p, _c_void_p]),
     "ps_tau_sum_general": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_int,

@@ -253,6 +253,69 @@ class tauNL_utils:
                   ctypes.c_void_p(ws.data_ptr()), int(nb.value), _stream())
         return float(out.item())
 
+    def _collider_ws(self, nrow, device):
+        nb = ctypes.c_size_t()
+        _lib.call("ps_tau_collider_workspace_bytes", int(nrow), ctypes.byref(nb))
+        return torch.empty(max(int(nb.value), 8), dtype=torch.uint8, device=device), int(nb.value)
+
+    def _collider_diag(self, _arr1, _arr2, _FLLs, _r_weights, pref):
+        nLmax, row_of_full, rowL, rowM, _ = self._row_tables()
+        a1, _ = _prep(_arr1, torch.complex128)
+        a2, _ = _prep(_arr2, torch.complex128)
+        F, _ = _prep(_FLLs, torch.complex128)
+        w = torch.as_tensor(np.asarray(_r_weights, dtype=np.float64), device=a1.device)
+        nrow, nr = len(self.Ls), a1.shape[-1]
+        if (a1.dim() != 3 or a1.shape != a2.shape or tuple(a1.shape[1:]) != (nrow, nr) or F.dim() != 3
+                or tuple(F.shape[1:]) != (nr, nr) or F.shape[0] <= self.Lmax or w.numel() != nr):
+            raise ValueError("collider tau sum: arrays must be [nlam, len(Ls), N_r], FLLs [> Lmax, N_r, N_r]")
+        ws, nb = self._collider_ws(nrow, a1.device)
+        out = torch.zeros(1, dtype=torch.float64, device=a1.device)
+        pref = complex(pref)
+        _lib.call("ps_tau_sum_collider_diag", ctypes.c_void_p(a1.data_ptr()), ctypes.c_void_p(a2.data_ptr()),
+                  a1.shape[0], ctypes.c_void_p(rowL.data_ptr()), ctypes.c_void_p(rowM.data_ptr()), nrow, self.Lmin,
+                  self.Lmax, ctypes.c_void_p(F.data_ptr()), F.shape[0], ctypes.c_void_p(w.data_ptr()), nr,
+                  pref.real, pref.imag, ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), nb,
+                  _stream())
+        return float(out.item())
+
+    def tau_sum_n0_collider(self, _arr1, _arr2, _FLLs, _r_weights, pref):
+        """tauNL_utils.pyx:923-964: Sum over (L, M) of w_M Sum_{r, r'} Re(pref F_L(r, r') w w' A(r) conj(B(r')))
+        for the s = 0 collider arrays [1, len(Ls), N_r] and the complex F_L [nL, N_r, N_r]
+        (ps_tau_sum_collider_diag)."""
+        return self._collider_diag(_arr1, _arr2, _FLLs, _r_weights, pref)
+
+    def tau_sum_nu0_collider(self, _arr1, _arr2, _FLLs, _r_weights, pref):
+        """tauNL_utils.pyx:877-921: the nu_s = 0 form, the same sum over every lambda of [2s+1, len(Ls), N_r]
+        (ps_tau_sum_collider_diag)."""
+        return self._collider_diag(_arr1, _arr2, _FLLs, _r_weights, pref)
+
+    def tau_sum_general_collider(self, _arr1, _arr1c, _arr2, _arr2c, _FLLs, _r_weights, nmax_F, s, beta, _coeffs):
+        """tauNL_utils.pyx:723-875: the S, Delta, Lam, lam1, (L, M), (r, r') sum of the collider estimator for
+        arrays [2s+1, len(Ls), N_r] (beta and its conjugate), complex F [2 nmax_F + 1, > Lmax, N_r, N_r] and the
+        coupling coefficients C_S, S = 0, 2, .., 2s (ps_tau_sum_collider_general)."""
+        nLmax, row_of_full, rowL, rowM, _ = self._row_tables()
+        arrs = [_prep(x, torch.complex128)[0] for x in (_arr1, _arr1c, _arr2, _arr2c)]
+        F, _ = _prep(_FLLs, torch.complex128)
+        dev = arrs[0].device
+        w = torch.as_tensor(np.asarray(_r_weights, dtype=np.float64), device=dev)
+        c = torch.as_tensor(np.asarray(_coeffs, dtype=np.complex128).reshape(-1), device=dev)
+        nrow, nr = len(self.Ls), arrs[0].shape[-1]
+        s = int(s)
+        if (any(tuple(x.shape) != (2 * s + 1, nrow, nr) for x in arrs) or F.dim() != 4
+                or F.shape[0] != 2 * int(nmax_F) + 1 or tuple(F.shape[2:]) != (nr, nr) or F.shape[1] <= self.Lmax
+                or w.numel() != nr or c.numel() != s + 1):
+            raise ValueError("tau_sum_general_collider: arrays must be [2s+1, len(Ls), N_r], FLLs "
+                             "[2 nmax_F + 1, > Lmax, N_r, N_r], coeffs [s + 1]")
+        ws, nb = self._collider_ws(nrow, dev)
+        out = torch.zeros(1, dtype=torch.float64, device=dev)
+        real_beta = int(complex(beta).imag == 0)
+        _lib.call("ps_tau_sum_collider_general", *[ctypes.c_void_p(x.data_ptr()) for x in arrs],
+                  ctypes.c_void_p(rowL.data_ptr()), ctypes.c_void_p(rowM.data_ptr()), nrow, int(self.Ls.min()),
+                  nLmax, self.Lmin, self.Lmax, ctypes.c_void_p(F.data_ptr()), F.shape[1], int(nmax_F),
+                  ctypes.c_void_p(w.data_ptr()), nr, s, real_beta, ctypes.c_void_p(c.data_ptr()),
+                  ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), nb, _stream())
+        return float(out.item())
+
     def convolve_F_general(self, _PQ, _FLLs, _r_weights, out_real, out_imag, n1, n3, n, mu1, inds):
         """tauNL_utils.pyx:1069-1180: the Gaunt-weighted F convolutions for one mu1, accumulated in place into
         out_real / out_imag [len(l <= nLmax), len(inds)] (ps_convolve_F_general)."""

@@ -52,6 +52,26 @@ def _is_direc(t):
     return any(s in t for s in ('tauNL-direc', 'tauNL-even', 'tauNL-odd'))
 
 
+def _is_coll(t):
+    """Collider templates: tauNL-light:s,nu_s and tauNL-heavy:s,mu_s."""
+    return 'tauNL-light' in t or 'tauNL-heavy' in t
+
+
+def _coll_parse(t):
+    a, b = t.split(':')[1].split(',')
+    return int(a), float(b)
+
+
+def _ckey(beta):
+    """Key of the collider P^beta maps of one filtered field (polyspec/tspec_template.py:1089)."""
+    return 'coll-%.8f,%.8fi' % (np.real(beta), np.imag(beta))
+
+
+def _ckey_s(s, beta):
+    """Key of the collider [P^beta_{s,lam} Q] harmonic maps (polyspec/tspec_template.py:1246)."""
+    return 'coll-%d,%.8f,%.8fi' % (s, np.real(beta), np.imag(beta))
+
+
 def _fact_ratio(num, den):
     """prod(num)! / prod(den)! as a float, from exact integers."""
     from math import factorial
@@ -71,6 +91,23 @@ def wig3zero(l1, l2, l3):
     g = L // 2
     r = np.sqrt(_fact_ratio((L - 2 * l1, L - 2 * l2, L - 2 * l3), (L + 1,)))
     return (-1.) ** g * r * _fact_ratio((g,), (g - l1, g - l2, g - l3))
+
+
+def wig3(j1, j2, j3, m1, m2, m3):
+    """Wigner 3j symbol (j1 j2 j3; m1 m2 m3) for small integer j (Racah's single sum, Edmonds 1957, eq. 3.7.3)."""
+    if m1 + m2 + m3 != 0 or j3 < abs(j1 - j2) or j3 > j1 + j2 or abs(m1) > j1 or abs(m2) > j2 or abs(m3) > j3:
+        return 0.
+    delta = np.sqrt(_fact_ratio((j1 + j2 - j3, j1 - j2 + j3, -j1 + j2 + j3, j1 + m1, j1 - m1, j2 + m2, j2 - m2,
+                                 j3 + m3, j3 - m3), (j1 + j2 + j3 + 1,)))
+    from fractions import Fraction
+    from math import factorial
+    total = Fraction(0)  # exact, so that symbols that vanish by cancellation are 0
+    for k in range(max(0, j2 - j3 - m1, j1 - j3 + m2), min(j1 + j2 - j3, j1 - m1, j2 + m2) + 1):
+        den = 1
+        for x in (k, j1 + j2 - j3 - k, j1 - m1 - k, j2 + m2 - k, j3 - j2 + m1 + k, j3 - j1 - m2 + k):
+            den *= factorial(x)
+        total += Fraction((-1) ** k, den)
+    return (-1.) ** (j1 - j2 - m3) * delta * float(total)
 
 
 def wig6(j1, j2, j3, j4, j5, j6):
@@ -243,7 +280,7 @@ class TSpecTemplate:
             self.d_Lminfilt_lens = torch.as_tensor(np.nonzero(self.Lminfilt_lens)[0], device=dev)
         t0 = time.time()
         if self.N_r > 0:
-            self._prepare_templates(self.ints_1d, False, False)
+            self._prepare_templates(self.ints_1d, False, self.ints_coll)
         if self.N_rtau > 0:
             self._prepare_templates(False, self.ints_2d, False)
         self.timers['precomputation'] += time.time() - t0
@@ -260,12 +297,16 @@ class TSpecTemplate:
             known = t in self.all_templates or any(s in t for s in ('tauNL-direc', 'tauNL-even', 'tauNL-odd',
                                                                      'tauNL-light', 'tauNL-heavy'))
             assert known, "Unknown template %s supplied!" % t
-            if t not in SUPPORTED and not _is_direc(t):
+            if t not in SUPPORTED and not _is_direc(t) and not _is_coll(t):
                 raise NotImplementedError("template %s is not implemented by the CUDA backend (supported: %s, "
-                                          "tauNL-direc:n1,n3,n, tauNL-even:n, tauNL-odd:n)" % (t, SUPPORTED))
+                                          "tauNL-direc:n1,n3,n, tauNL-even:n, tauNL-odd:n, tauNL-light:s,nu_s, "
+                                          "tauNL-heavy:s,mu_s)" % (t, SUPPORTED))
         print("Templates: %s" % templates)
         self.ints_1d, self.ints_2d, self.ints_coll = False, False, False
         self.to_compute, self.n1n3n, self.coll_params = [], [], {}
+        if any(_is_coll(t) for t in templates):
+            assert self.K_coll <= self.k_coll, "Collider K_cut can't exceed collider k_cut"
+            print("Collider k-range: K < %.2e, k > %.2e" % (self.K_coll, self.k_coll))
         if 'gNL-loc' in templates:
             self.to_compute.append(['q'])
             self.ints_1d = True
@@ -324,6 +365,34 @@ class TSpecTemplate:
                 n1n3n += [c for c in cands if abs(c[0] - c[1]) <= c[2] <= c[0] + c[1] and min(c) >= 0]
                 self.to_compute.append(['q'])
                 self.ints_1d = True
+            if 'tauNL-light' in t:
+                # light particle of spin s and nu_s (polyspec/tspec_template.py:347-371): beta = nu_s - 3/2
+                s, nu_s = _coll_parse(t)
+                if s == 0 and nu_s == 1.5 and ('tauNL-loc' in self.templates):
+                    raise Exception("tauNL-loc and tauNL-light:0,1.5 are fully degenerate!")
+                if nu_s == 1.5 and ('tauNL-direc:%d,%d,0' % (s, s) in self.templates):
+                    raise Exception("tauNL-direc:%d,%d,0 and tauNL-light:%d,1.5 are fully degenerate!" % (s, s, s))
+                if s == 0:
+                    assert 0. <= nu_s <= 1.5, "Light spin-0 particles have nu_s in (0, 3/2)"
+                else:
+                    assert 0 <= nu_s <= s - 0.5, "Light spin-%d particles have nu_s in (0, %.1f)" % (s, s - 1. / 2.)
+                    if nu_s > 0.5:
+                        print("## Warning: Spin = %d nu_s = %d violates the Higuchi bound!" % (s, nu_s))
+                self._merge_coll({nu_s - 3. / 2.: [[s, S] for S in range(0, 2 * s + 1, 2)]})
+                self.to_compute.append(['q'])
+                self.ints_coll = True
+                self.ints_1d = True
+            if 'tauNL-heavy' in t:
+                # heavy particle of spin s and mass mu_s (:372-389): beta = -3/2 +- i mu_s
+                s, mu_s = _coll_parse(t)
+                if mu_s == 0 and ('tauNL-light:%d,%s' % (s, mu_s) in self.templates):
+                    raise Exception("tauNL-light:s,0 and tauNL-heavy:s,0 are fully degenerate!")
+                assert mu_s >= 0., "Heavy spin-0 particles have mu_s >=0"
+                params = [[s, S] for S in range(0, 2 * s + 1, 2)]
+                self._merge_coll({1.0j * mu_s - 3. / 2.: params, -1.0j * mu_s - 3. / 2.: params})
+                self.to_compute.append(['q'])
+                self.ints_coll = True
+                self.ints_1d = True
         for t in templates:
             if 'lensing' in t:
                 assert len(C_phi) > 0, "Must supply lensing power spectrum!"
@@ -345,14 +414,15 @@ class TSpecTemplate:
         self.n1n3n = np.asarray(n1n3n, dtype=int).reshape(-1, 3)
         self.to_compute = np.unique(np.concatenate(self.to_compute)) if self.to_compute else np.array([])
         self.nmax = int(np.max(self.n1n3n[:, :2])) if len(self.n1n3n) > 0 else 0
-        self.nmax_coll = 0
-        self.nmax_coll_F = 0
+        self.coll_params = {k: np.asarray(v, dtype=int).reshape(-1, 2) for k, v in self.coll_params.items()}
+        self.nmax_coll = int(max([np.max(v[:, 0]) for v in self.coll_params.values()], default=0))
+        self.nmax_coll_F = int(max([np.max(v[:, 1]) for v in self.coll_params.values()], default=0))
         self.p_inds = [0] if 'gNL-loc' in self.templates else []
         if len(self.n1n3n) > 0:
             self.p_inds = [int(x) for x in np.unique(self.p_inds + list(np.unique(self.n1n3n[:, :2])))]
         self.nmax_F = int(np.max(self.n1n3n[:, 2])) if len(self.n1n3n) > 0 else 0
-        self.nLmax = self.Lmax + self.nmax_F
-        self.nLmin = self.Lmin - self.nmax_F
+        self.nLmax = self.Lmax + max(self.nmax_F, self.nmax_coll_F)
+        self.nLmin = self.Lmin - max(self.nmax_F, self.nmax_coll_F)
         # The reference fails later when this does not hold: its default Lmax = min(base.lmax, 2 lmax)
         # (polyspec/tspec_template.py:87-88) plus n > 0 asks to_lm_vec for L beyond base.lmax
         # (:1302), whose output then no longer matches the l <= base.lmax filters (:443-447).
@@ -360,7 +430,7 @@ class TSpecTemplate:
         if self.nLmax > int(np.max(self.base.l_arr)):
             raise ValueError("Lmax + max(n) = %d exceeds the maps' lmax %d: pass Lmax <= %d"
                              % (self.nLmax, int(np.max(self.base.l_arr)),
-                                int(np.max(self.base.l_arr)) - self.nmax_F))
+                                int(np.max(self.base.l_arr)) - max(self.nmax_F, self.nmax_coll_F)))
         self.nLfilt = (self.base.l_arr >= self.nLmin) & (self.base.l_arr <= self.nLmax)
         self.Ls, self.Ms = self.base.l_arr[self.nLfilt], self.base.m_arr[self.nLfilt]
         self.nLminfilt = self.base.l_arr[self.base.l_arr <= self.nLmax] >= self.nLmin
@@ -368,6 +438,18 @@ class TSpecTemplate:
         if 'lensing' in self.templates:
             self.Lminfilt_lens = self.base.l_arr[self.base.l_arr <= self.Lmax_lens] >= self.Lmin_lens
         self.lminfilt = self.base.l_arr[self.base.l_arr <= self.lmax] >= self.lmin
+
+    def _merge_coll(self, d2):
+        """Merge collider (beta -> [[s, S], ..]) entries, dropping duplicates (polyspec/tspec_template.py:262-272)."""
+        for key, items in d2.items():
+            if key in self.coll_params:
+                new = []
+                for item in list(items) + list(self.coll_params[key]):
+                    if item not in new:
+                        new.append(item)
+                self.coll_params[key] = new
+            else:
+                self.coll_params[key] = list(items)
 
     def _prepare_templates(self, ints_1d=True, ints_2d=False, ints_coll=False):
         """k-space integrals on the GPU (polyspec/tspec_template.py:520-708): p and q (gNL-loc),
@@ -380,8 +462,9 @@ class TSpecTemplate:
             print("N_r: %d" % self.N_r)
         if ints_2d:
             print("N_rtau: %d" % self.N_rtau)
-        lmax = max([self.lmax + 1, self.lmax + self.nmax])
-        lmin = max([min([self.lmin - 1, self.lmin - self.nmax]), 0])
+        nmax_p = max(self.nmax, self.nmax_coll)
+        lmax = max([self.lmax + 1, self.lmax + nmax_p])
+        lmin = max([min([self.lmin - 1, self.lmin - nmax_p]), 0])
         print("\nPrecomputing Bessel functions")
         k_arr = np.asarray(self.k_arr, dtype=np.float64)
         max_kr = 0.
@@ -439,6 +522,29 @@ class TSpecTemplate:
                 integral(2. / np.pi * k_arr * k_arr / 2. * Pz ** (3. / 4.), self.r_arr, rlXs, self.lmin, self.lmax)
                 self.d_rlXs = rlXs
                 self.rlXs = rlXs.cpu().numpy()
+        if ints_coll and len(self.coll_params) > 0:
+            # p^beta_{lL}^X(r) (collider_p_integral, k_integrals.pyx:399-451): the p sum with the complex
+            # kprod = (2/pi) k^(2 + beta) P_zeta / 2 for k >= k_coll, as its real and imaginary parts;
+            # beta with Im > 0 follows by conjugation and is not stored
+            print("Computing collider p_lL^{beta,X}(r) integrals")
+            self.coll_plLXs, self.d_coll_plLXs = {}, {}
+            for beta in self.coll_params:
+                if np.imag(beta) > 0:
+                    continue
+                this_nmax = int(np.max(self.coll_params[beta][:, 0]))
+                kc = np.where(k_arr >= self.k_coll,
+                              2. / np.pi * k_arr.astype(np.complex128) ** (2. + beta) * Pz / 2., 0.)
+                parts = []
+                for kpart in (kc.real, kc.imag):
+                    out = torch.zeros((2 * this_nmax + 1, lmax + 1, npol_out, self.N_r), dtype=torch.float64,
+                                      device=dev)
+                    for n in range(-this_nmax, this_nmax + 1):
+                        lshift1 = min(0, self.lmin - lmin + n)
+                        integral(kpart, self.r_arr, out[this_nmax + n], self.lmin - lshift1, self.lmax, nshift=n)
+                    parts.append(out)
+                d = torch.complex(parts[0], parts[1])
+                self.d_coll_plLXs[beta] = d
+                self.coll_plLXs[beta] = d.cpu().numpy()
         if ints_2d:
             assert np.max(x_arr) >= np.max(k_arr) * np.max(self.rtau_arr[:, 0])
             r, tau = self.rtau_arr[:, 0], self.rtau_arr[:, 1]
@@ -471,8 +577,52 @@ class TSpecTemplate:
                 raise Exception("F_LL'(r, r') calculation failed: a hypergeometric series did not converge")
             self.d_FLLs = FLLs
             self.FLLs = FLLs.cpu().numpy()
+        if ints_coll and len(self.coll_params) > 0:
+            self._collider_F_integrals()
         self._make_utils()
         print("Precomputation complete")
+
+    def _collider_F_integrals(self):
+        """F^beta_{L,L+n}(r, r') of the collider templates (polyspec/tspec_template.py:670-703 with
+        compute_collider_F_integral, k_integrals.pyx:496-545): j_L on the reference's y grid
+        (ps_kint_bessel_table), interpolated to 5000 log-spaced K <= 1.01 K_coll (ps_kint_collider_jlK),
+        then the trapezium rule over K with (2/pi) K^(2 - 2 beta) P_zeta(K) / 2 (ps_kint_collider_F)."""
+        dev = self._dev
+        K_arr = np.geomspace(0.1 / (self.r_hor + 5000), self.K_coll * 1.01, 5000)
+        this_Lmax = self.Lmax + self.nmax_coll_F
+        this_Lmin = max([self.Lmin - self.nmax_coll_F, 0])
+        max_Kr = self.K_coll * np.max(self.r_arr)
+        y_arr = np.asarray(list(np.arange(0, this_Lmax * 2, 0.01)) + list(np.arange(this_Lmax * 2, max_Kr * 1.01,
+                                                                                     0.01)), dtype=np.float64)
+        d_y = torch.as_tensor(y_arr, device=dev)
+        nl = this_Lmax - this_Lmin + 1
+        table = torch.empty((nl, len(y_arr)), dtype=torch.float64, device=dev)
+        _lib.call("ps_kint_bessel_table", _vp(d_y), len(y_arr), this_Lmin, this_Lmax, _vp(table), _stream())
+        if not bool(torch.isfinite(table).all()):
+            raise Exception("Spherical Bessel calculation failed!")
+        d_K = torch.as_tensor(K_arr, device=dev)
+        d_r = torch.as_tensor(np.asarray(self.r_arr, dtype=np.float64), device=dev)
+        jlK = torch.empty((nl, len(K_arr), self.N_r), dtype=torch.float64, device=dev)
+        _lib.call("ps_kint_collider_jlK", _vp(table), _vp(d_y), len(y_arr), nl, _vp(d_K), len(K_arr), _vp(d_r),
+                  self.N_r, _vp(jlK), _stream())
+        del table
+        print("Computing F_LL'^beta(r, r') integrals")
+        self.coll_FLLs, self.d_coll_FLLs = {}, {}
+        nLout = self.base.lmax + 1
+        for beta in self.coll_params:
+            if np.imag(beta) > 0:
+                continue
+            this_nmax_F = int(np.max(self.coll_params[beta][:, 1]))
+            Kprod = np.where(K_arr <= self.K_coll,
+                             2. / np.pi * K_arr.astype(np.complex128) ** (2. - 2. * beta) * self.Pzeta(K_arr) / 2., 0.)
+            d_Kp = torch.as_tensor(Kprod.astype(np.complex128), device=dev)
+            F = torch.zeros((2 * this_nmax_F + 1, nLout, self.N_r, self.N_r), dtype=torch.complex128, device=dev)
+            _lib.call("ps_kint_collider_F", _vp(jlK), nl, this_Lmin, _vp(d_K), len(K_arr), _vp(d_Kp), self.N_r,
+                      self.Lmin, self.Lmax, this_nmax_F, nLout, _vp(F), _stream())
+            torch.cuda.current_stream().synchronize()
+            self.d_coll_FLLs[beta] = F
+            self.coll_FLLs[beta] = F.cpu().numpy()
+        del jlK
 
     def set_radial_integrals(self, qlXs=None, plLXs=None, **arrays):
         """Install precomputed radial integrals in place of the computed ones: any of
@@ -566,11 +716,13 @@ class TSpecTemplate:
         self._timed('map_transforms', t0)
         return out
 
-    def _compute_weighted_gaunt_maps(self, h_lm_filt, flLX_arr_re, n, mu):
-        """P_{n,mu} maps [N_r, Npix] of polyspec/tspec_template.py:817-876 (real p_lL^X integrals):
+    def _compute_weighted_gaunt_maps(self, h_lm_filt, flLX_arr_re, n, mu, flLX_arr_im=None):
+        """P_{n,mu} maps [N_r, Npix] of polyspec/tspec_template.py:817-876:
         n = 0 is the transfer-weighted synthesis of h / sqrt(4 pi); n > 0 sums the Gaunt-weighted
         shifts l -> l + Delta of conj(h) (``shift_and_weight_map_all``) into real- and imaginary-part
-        harmonics up to lmax + n and combines their syntheses as re - i im (complex maps)."""
+        harmonics up to lmax + n and combines their syntheses as re - i im (complex maps).  With the
+        imaginary part of complex (collider) integrals, n = 0 gives the complex map R + i I and n > 0
+        adds the i-weighted shifts of the imaginary part with the two outputs exchanged."""
         assert mu <= n, "mu<=n is required!"
         assert mu >= 0, "Negative mu can be obtained by conjugation properties"
         t0 = time.time()
@@ -579,12 +731,18 @@ class TSpecTemplate:
             summ = self._full_lm(self.utils.apply_fl_weights(flLX_arr_re[nmax], h_lm_filt,
                                                              1. / np.sqrt(4. * np.pi)), self.lmax)
             out = self.base.to_map_vec(summ, lmax=self.lmax)
+            if flLX_arr_im is not None:
+                summ = self._full_lm(self.utils.apply_fl_weights(flLX_arr_im[nmax], h_lm_filt,
+                                                                 1. / np.sqrt(4. * np.pi)), self.lmax)
+                out = pixel.r2c(out, self.base.to_map_vec(summ, lmax=self.lmax))
         else:
             nr = flLX_arr_re.shape[3]
             nt = int(np.sum(self.base.l_arr <= self.lmax + n))
             Lr = torch.zeros((nr, nt), dtype=torch.complex128, device=self._dev)
             Li = torch.zeros_like(Lr)
             self.utils.shift_and_weight_map_all(flLX_arr_re, h_lm_filt, n, mu, 1.0, Lr, Li, nmax)
+            if flLX_arr_im is not None:
+                self.utils.shift_and_weight_map_all(flLX_arr_im, h_lm_filt, n, mu, 1.0j, Li, Lr, nmax)
             if bool((Li.imag != 0.).any()):
                 out = pixel.r2cstar(self.base.to_map_vec(Lr, lmax=self.lmax + n),
                                     self.base.to_map_vec(1.0j * Li, lmax=self.lmax + n))
@@ -648,6 +806,22 @@ class TSpecTemplate:
         for n in self.p_inds:
             for mu in range(n + 1):
                 output['p%d%d' % (n, mu)] = self._compute_weighted_gaunt_maps(input_map, self.d_plLXs, n, mu)
+        for beta in self.coll_params:
+            # collider P^beta_{s,lam} maps (polyspec/tspec_template.py:1058-1089); Im beta > 0 from the conjugate
+            if np.imag(beta) != 0:
+                if np.imag(beta) <= 0:
+                    P = self.d_coll_plLXs[beta]
+                    re, im = P.real.contiguous(), P.imag.contiguous()
+                else:
+                    P = self.d_coll_plLXs[np.conj(beta)]
+                    re, im = P.real.contiguous(), (-P.imag).contiguous()
+            else:
+                re, im = self.d_coll_plLXs[beta].real.contiguous(), None
+            maps = {}
+            for s_ in np.unique(self.coll_params[beta][:, 0]):
+                for lam in range(int(s_) + 1):
+                    maps['p%d%d' % (s_, lam)] = self._compute_weighted_gaunt_maps(input_map, re, int(s_), lam, im)
+            output[_ckey(beta)] = maps
         if 'q' in self.to_compute:
             output['q'] = self._compute_weighted_maps(input_map, self.d_qlXs)
         if 'r' in self.to_compute:
@@ -823,17 +997,36 @@ class TSpecTemplate:
         parts, weights = (self._decompose_tauNL_even(n) if 'tauNL-even' in t else self._decompose_tauNL_odd(n))
         return [(int(a), int(b), int(c), float(w)) for (a, b, c), w in zip(parts, weights)]
 
-    def _A_maps(self, map1, map2, n, add_sym=False):
+    def _A_maps(self, map1, map2, n, add_sym=False, beta=None):
         """[P_{n,mu} Q]_LM for mu = -n..n and each radial sample (polyspec/tspec_template.py:1275-1334), as
         [2n+1, N_r, nlm(nLmax)] over the full l <= nLmax list (entries with L < nLmin are unused);
-        optionally adding the map1 <-> map2 term.  mu < 0 uses conjugation, (-1)^(n+mu) conj(P_{n,-mu})."""
+        optionally adding the map1 <-> map2 term.  mu < 0 uses conjugation, (-1)^(n+mu) conj(P_{n,-mu}).
+        With a collider beta the P maps are the P^beta_{n,mu} (complex for complex beta; mu < 0 then
+        conjugates the maps of conj(beta))."""
         t0 = time.time()
+
+        def P(mp, key):
+            return mp[key] if beta is None else mp[_ckey(beta)][key]
+
+        def Pc(mp, key):
+            return mp[key] if beta is None else mp[_ckey(np.conj(beta) if np.imag(beta) != 0 else beta)][key]
+
         if n == 0:
-            if add_sym:
-                prod = pixel.multiplyRR_sym(map2['q'], map1['p00'], map1['q'], map2['p00'])
+            if beta is None or np.imag(beta) == 0:
+                if add_sym:
+                    prod = pixel.multiplyRR_sym(map2['q'], P(map1, 'p00'), map1['q'], P(map2, 'p00'))
+                else:
+                    prod = pixel.multiplyRR(map2['q'], P(map1, 'p00'))
+                out = self.base.to_lm_vec(prod, lmax=self.nLmax)[None]
             else:
-                prod = pixel.multiplyRR(map2['q'], map1['p00'])
-            out = self.base.to_lm_vec(prod, lmax=self.nLmax)[None]
+                if add_sym:
+                    prod = pixel.multiplyRC_sym(map2['q'], P(map1, 'p00'), map1['q'], P(map2, 'p00'))
+                else:
+                    prod = pixel.multiplyRC(map2['q'], P(map1, 'p00'))
+                out = self.base.to_lm_vec(prod.real.contiguous(), lmax=self.nLmax).to(torch.complex128)
+                if bool((prod.imag[:, 0] != 0).any()):
+                    out = out + 1j * self.base.to_lm_vec(prod.imag.contiguous(), lmax=self.nLmax)
+                out = out[None]
             self._timed('tauNL_summation', t0)
             return out
         output = []
@@ -842,14 +1035,14 @@ class TSpecTemplate:
             if mu < 0:
                 fac = (-1.) ** (n + mu)
                 if add_sym:
-                    prod = pixel.multiplyRCstar_sym(map2['q'], map1[key], map1['q'], map2[key], fac)
+                    prod = pixel.multiplyRCstar_sym(map2['q'], Pc(map1, key), map1['q'], Pc(map2, key), fac)
                 else:
-                    prod = pixel.multiplyRCstar(map2['q'], map1[key], fac)
+                    prod = pixel.multiplyRCstar(map2['q'], Pc(map1, key), fac)
             else:
                 if add_sym:
-                    prod = pixel.multiplyRC_sym(map2['q'], map1[key], map1['q'], map2[key])
+                    prod = pixel.multiplyRC_sym(map2['q'], P(map1, key), map1['q'], P(map2, key))
                 else:
-                    prod = pixel.multiplyRC(map2['q'], map1[key])
+                    prod = pixel.multiplyRC(map2['q'], P(map1, key))
             out = self.base.to_lm_vec(prod.real.contiguous(), lmax=self.nLmax).to(torch.complex128)
             if bool((prod[:, 0].imag != 0).any()):
                 out = out + 1j * self.base.to_lm_vec(prod.imag.contiguous(), lmax=self.nLmax)
@@ -881,6 +1074,90 @@ class TSpecTemplate:
             out = self.utils.tau_sum_general(rows(A[n1]), rows(B[n3]), self.d_FLLs, weights, n1, n3, n)
         self._timed('tauNL_summation', t0)
         return out
+
+    def _calC(self, s, S, mu_s):
+        """C_s(S, mu_s) coupling of the collider templates (polyspec/tspec_template.py:710-743): for mu_s = 0,
+        delta_S0 (4 pi)^(3/2) (-1)^s / sqrt(2s+1); otherwise (4 pi)^(3/2) sqrt(2S+1)/(2s+1) Sum_lam (-1)^(S+lam)
+        W_lam(s, mu_s) (s s S; lam -lam 0), W_lam = G(1/2+s-i mu) G(1/2+lam+i mu) / (G(1/2+s+i mu) G(1/2+lam-i mu))."""
+        from scipy.special import gamma
+
+        def W_lam(lam, s, mu_s):
+            assert abs(lam) <= s
+            if np.real(mu_s) == 0.:
+                mu_s += 1e-12
+            W = gamma(0.5 + s - 1.0j * mu_s) * gamma(0.5 + lam + 1.0j * mu_s) / (
+                gamma(0.5 + s + 1.0j * mu_s) * gamma(0.5 + lam - 1.0j * mu_s))
+            return W.real if np.real(mu_s) == 1e-12 else W
+
+        if s == 0 and np.real(mu_s) == 0:
+            nu_s = np.real(-1.0j * mu_s)
+            assert 0. <= nu_s <= 1.5, "Light spin-0 particles have nu_s in (0, 3/2)"
+        elif np.real(mu_s) == 0:
+            nu_s = np.real(-1.0j * mu_s)
+            assert 0 <= nu_s <= s - 0.5, "Light spin-%d particles have nu_s in (0, %.1f)" % (s, s - 1. / 2.)
+            assert nu_s <= 0.5, "Couplings undefined for Higuchi-bound violating particles!"
+        else:
+            assert np.imag(mu_s) == 0, "mu_s can't be complex!"
+        if mu_s == 0.:
+            return (S == 0) * (4. * np.pi) ** (3. / 2.) / np.sqrt(2. * s + 1.) * (-1.) ** s
+        pref = (4. * np.pi) ** (3. / 2.) / (2. * s + 1.) * np.sqrt(2. * S + 1.)
+        out = 0.
+        for lam in range(-s, s + 1):
+            out += (-1.) ** (S + lam) * W_lam(lam, s, mu_s) * wig3(s, s, S, lam, -lam, 0)
+        return np.real_if_close(pref * out)
+
+    def _omega_prime(self, s, mu_s):
+        """S-independent phase omega'_s(mu_s) of the collider coupling (polyspec/tspec_template.py:744-754):
+        zero for light particles, else arg(-2^(-4 i mu) (1 + i sinh(pi mu)) (5/2 + s + i mu)^2 /
+        (3/2 + s - i mu)^2 G(-i mu)^2 G(1/2 + s + i mu)^2)."""
+        from scipy.special import gamma
+        if np.real(mu_s) == 0:
+            return 0.
+        val = 2. ** (-4. * mu_s * 1.0j) * (1. + 1.0j * np.sinh(np.pi * mu_s)) * (2.5 + s + 1.0j * mu_s) ** 2. \
+            / (1.5 + s - 1.0j * mu_s) ** 2.
+        val *= gamma(-1.0j * mu_s) ** 2 * gamma(0.5 + s + 1.0j * mu_s) ** 2
+        return np.angle(-1. * val)
+
+    def _coll_rows(self, X):
+        """[2s+1, N_r, nlm(nLmax)] harmonic maps -> the reference's [2s+1, len(Ls), N_r] row layout."""
+        return X[:, :, self.d_nLminfilt_idx].permute(0, 2, 1).contiguous()
+
+    def _tau_sum_collider(self, A, B, weights, s, beta):
+        """Sum over lam1, lam3, Lam, S, (L, M), (L', M'), (r, r') of the collider estimator
+        (polyspec/tspec_template.py:1243-1273): s = 0 and nu_s = 0 take the diagonal forms
+        (ps_tau_sum_collider_diag), otherwise the general Gaunt/3j sum (ps_tau_sum_collider_general)."""
+        t0 = time.time()
+        pos = _ckey_s(s, beta)
+        neg = pos if np.imag(beta) == 0 else _ckey_s(s, np.conj(beta))
+        nu_s = beta + 3. / 2.
+        nF = int(np.max(self.coll_params[beta][:, 1]))
+        F = self.d_coll_FLLs[beta]
+        w = np.asarray(weights, dtype=np.float64)
+        if s == 0:
+            tau = self.utils.tau_sum_n0_collider(self._coll_rows(A[pos]), self._coll_rows(B[neg]), F[nF], w,
+                                                 4. * np.pi * np.exp(1.0j * self._omega_prime(0, 1.0j * nu_s)))
+        elif nu_s == 0:
+            tau = self.utils.tau_sum_nu0_collider(self._coll_rows(A[pos]), self._coll_rows(B[neg]), F[nF], w,
+                                                  4. * np.pi / (2. * s + 1.) * (-1.) ** s)
+        else:
+            coeffs = np.asarray([np.exp(1.0j * self._omega_prime(s, 1.0j * nu_s)) * self._calC(s, S, 1.0j * nu_s)
+                                 for S in range(0, 2 * s + 1, 2)], dtype=np.complex128)
+            tau = self.utils.tau_sum_general_collider(self._coll_rows(A[pos]), self._coll_rows(A[neg]),
+                                                      self._coll_rows(B[pos]), self._coll_rows(B[neg]), F, w, nF, s,
+                                                      beta, coeffs)
+        self._timed('tauNL_summation', t0)
+        return tau
+
+    def set_collider_integrals(self, coll_plLXs=None, coll_FLLs=None):
+        """Install precomputed collider integrals (dicts beta -> the reference's coll_plLXs
+        [2 nmax+1, lmax+2, 1+2 pol, N_r] and coll_FLLs [2 nmax_F+1, lmax+1, N_r, N_r], complex) in place of
+        the computed ones."""
+        for name, arrs in (('coll_plLXs', coll_plLXs), ('coll_FLLs', coll_FLLs)):
+            if arrs is None:
+                continue
+            host = {k: np.asarray(v, dtype=np.complex128) for k, v in arrs.items()}
+            setattr(self, name, host)
+            setattr(self, 'd_' + name, {k: torch.as_tensor(v, device=self._dev) for k, v in host.items()})
 
     def _compute_PQ_vecs(self, Pn3_maps, Q_maps, i, j, n3=0, add_sym=False):
         """[P Q]_LM(r) of polyspec/tspec_template.py:1967-2010 for n3 = 0, [N_r, nlm(nLmax)]."""
@@ -1072,6 +1349,15 @@ class TSpecTemplate:
                             A_dd[nn] = self._A_maps(proc_maps, proc_maps, nn)
                     tau += wt * self._tau_sum(A_dd, A_dd, self.r_weights[t], n1, n3, n)
                 t4_num[ii] = tau / 48. * 24.
+            if _is_coll(t):
+                # collider tauNL (polyspec/tspec_template.py:1489-1518): [P^beta Q] maps of beta and, for a
+                # heavy particle, of its conjugate; the sum takes the real part
+                s_, x = _coll_parse(t)
+                betas = [-1.5 + x] if 'tauNL-light' in t else [-1.5 - 1.0j * x, -1.5 + 1.0j * x]
+                for beta in betas:
+                    if _ckey_s(s_, beta) not in A_dd:
+                        A_dd[_ckey_s(s_, beta)] = self._A_maps(proc_maps, proc_maps, s_, beta=beta)
+                t4_num[ii] = self._tau_sum_collider(A_dd, A_dd, self.r_weights[t], s_, betas[0]) / 24. * 12.
             if t in ('gNL-con', 'gNL-dotdot', 'gNL-dotdel', 'gNL-deldel'):
                 t0 = time.time()
                 t4_num[ii] = self._gnl_shape_sum(t, proc_maps) * A_pix
@@ -1130,6 +1416,28 @@ class TSpecTemplate:
                         t2_num[ii] += -1. / 48. * t2 * 6. / self.N_it / 2. * 4.
                         if compute_t0:
                             t0_num[ii] += 1. / 48. * t0s * 3 / self.N_it * 4.
+                    if _is_coll(t):
+                        # collider 2- and 0-field terms (polyspec/tspec_template.py:1817-1894)
+                        s_, x = _coll_parse(t)
+                        w = self.r_weights[t]
+                        betas = [-1.5 + x] if 'tauNL-light' in t else [-1.5 - 1.0j * x, -1.5 + 1.0j * x]
+                        tau = 0.
+                        for A_xx, A_xd, px in ((A_aa, A_ad, pa), (A_bb, A_bd, pb)):
+                            for beta in betas:
+                                if _ckey_s(s_, beta) not in A_xx:
+                                    A_xx[_ckey_s(s_, beta)] = self._A_maps(px, px, s_, beta=beta)
+                                    A_xd[_ckey_s(s_, beta)] = self._A_maps(px, proc_maps, s_, add_sym=True,
+                                                                           beta=beta)
+                            tau += 2 * self._tau_sum_collider(A_xx, A_dd, w, s_, betas[0])
+                            tau += self._tau_sum_collider(A_xd, A_xd, w, s_, betas[0])
+                        t2_num[ii] += -1. / 24. * tau * 6. / self.N_it / 2. * 2.
+                        if compute_t0:
+                            for beta in betas:
+                                if _ckey_s(s_, beta) not in A_ab:
+                                    A_ab[_ckey_s(s_, beta)] = self._A_maps(pa, pb, s_, add_sym=True, beta=beta)
+                            tau = 2 * self._tau_sum_collider(A_aa, A_bb, w, s_, betas[0])
+                            tau += self._tau_sum_collider(A_ab, A_ab, w, s_, betas[0])
+                            t0_num[ii] += 1. / 24. * tau * 3 / self.N_it * 2.
                     if t == 'tauNL-loc':
                         w = self.r_weights[t]
                         if 0 not in A_aa:
@@ -1391,6 +1699,9 @@ class TSpecTemplate:
 
         ``a_lms`` (two beam-deconvolved harmonic fields) may replace the fields drawn
         from ``seed``."""
+        if any(_is_coll(t) for t in self.templates):
+            raise NotImplementedError("the Fisher matrix of the collider templates is not implemented by the CUDA "
+                                      "backend")
         t_start = time.time()
         self._check_sampling()
         print("Computing Fisher matrix with seed %d" % seed)

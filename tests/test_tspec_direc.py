@@ -87,15 +87,15 @@ def _configured(templates):
 
 def test_direc_configuration():
     """General (n1, n3, n) parse as the reference does: P_{n} maps for n1 and n3, the triangle
-    condition and the n1 <-> n3 degeneracy check; the collider templates are refused."""
+    condition and the n1 <-> n3 degeneracy check; an unknown template is refused."""
     t = _configured(['tauNL-direc:1,2,1', 'tauNL-direc:0,1,1'])
     assert [list(x) for x in t.n1n3n] == [[1, 2, 1], [0, 1, 1]] and t.p_inds == [0, 1, 2]
     with pytest.raises(AssertionError):
         _configured(['tauNL-direc:1,1,3'])
     with pytest.raises(Exception, match="degenerate"):
         _configured(['tauNL-direc:1,2,1', 'tauNL-direc:2,1,1'])
-    with pytest.raises(NotImplementedError):
-        _configured(['tauNL-light:1,1.5'])
+    with pytest.raises(AssertionError, match="Unknown"):
+        _configured(['tauNL-medium:1,1.5'])
 
 
 @pytest.mark.gpu
