@@ -483,6 +483,20 @@ int ps_tau_sum_collider_general(const double* A1, const double* A1c, const doubl
                                 const double* F, int nLF, int nmax_F, const double* w, int nr, int s, int real_beta,
                                 const double* coeffs, double* out, void* workspace, size_t workspace_bytes,
                                 cudaStream_t stream);
+/* ps_convolve_F_collider: convolve_F_general_collider (tauNL_utils.pyx:1197-1355) for one lam1: PQ, cPQ complex
+ *   [2s+1][nrow][nr] (the [P^beta Q] and [P^beta* Q] vectors; s = 0: [1][nrow][nr]), complex F [2 nmax_F + 1][nLF][nrF]
+ *   [nrF] read at the radial indices inds [nr], S_weights [s + 1] complex (C_S e^{i omega'}, S = 0, 2, .., 2s);
+ *   out_re / out_im complex [len(l <= nLmax)][nr] += plus + minus / plus - minus at full_of_row[row].
+ * ps_pF_map_complex: compute_pF_map_complex (tauNL_utils.pyx:1357-1446): out complex [npol][nl] += the Gaunt-weighted
+ *   shifts of plus / minus (complex [nlm(lmax_in)][nin]) times the complex p [nshift][lsize][npol][nrp] (read at
+ *   inds [nin]) and w [nin], for the l-list (ls, ms) and -n1 <= mu1 <= n1. */
+int ps_convolve_F_collider(const double* PQ, const double* cPQ, const int* rowL, const int* rowM,
+                           const int* full_of_row, int nrow, int nLmin, int nLmax, int Lmin, int Lmax, const double* F,
+                           int nLF, int nrF, int nmax_F, const double* w, const int* inds, int nr, int s, int lam1,
+                           const double* S_weights, double* out_re, double* out_im, cudaStream_t stream);
+int ps_pF_map_complex(const double* plus, const double* minus, int lmax_in, int nin, const double* p, int nshift,
+                      int lsize, int npol, int nrp, const double* w, const int* inds, const int* ls, const int* ms,
+                      int64_t nl, int n1, int mu1, int nmax, double* out, cudaStream_t stream);
 
 /* ------------------------------------------------------------- ideal bispectrum Fisher (BSpecBin.compute_fisher_ideal)
  * The 3j-symbol sums of polyspec/bspec_bin.py:699-827 as Gauss-Legendre quadratures of binned Wigner d-sums

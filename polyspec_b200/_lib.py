@@ -108,6 +108,13 @@ SIGNATURES = {
                                              _c_int, _c_int, _c_int, _c_int, _c_int, _c_void_p, _c_int, _c_int,
                                              _c_void_p, _c_int, _c_int, _c_int, _c_void_p, _c_void_p, _c_void_p,
                                              _c_size_t, _c_void_p]),
+    "ps_convolve_F_collider": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, _c_int,
+                                        _c_int, _c_int, _c_int, _c_void_p, _c_int, _c_int, _c_int, _c_void_p,
+                                        _c_void_p, _c_int, _c_int, _c_int, _c_void_p, _c_void_p, _c_void_p,
+                                        _c_void_p]),
+    "ps_pF_map_complex": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_void_p, _c_int, _c_int, _c_int, _c_int,
+                                   _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int64, _c_int, _c_int, _c_int,
+                                   _c_void_p, _c_void_p]),
     "ps_tau_general_workspace_bytes": (_c_int, [_c_int, _c_int, ctypes.POINTER(_c_size_t)]),
     "ps_gaunt_row_table": (_c_int, [_c_void_p, _c_void_p, _c_int, _c_int, _c_int, _c_int, _c_void_p, _c_void_p]),
     "ps_tau_sum_general": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, _c_int, _c_int,

@@ -25,6 +25,14 @@
 //    v_k = Sum_j A_j w_j F_{L,L+Delta}(r_j, r_k) (F rows read coalesced, A broadcast), then
 //    every (S, Lam) term adds Re(pref B_k w_k v_k).  Per-block partial sums, then one
 //    ordered reduction.
+//  * ps_convolve_F_collider: convolve_F_general_collider (tauNL_utils.pyx:1197-1355) for one
+//    lam1: the S = 0 term (diagonal in (L, M)) and the S > 0 Gaunt- and 3j-coupled terms of
+//    F^beta_{L,L+Delta}(r_j, r_k) [P^beta Q]_{L',M'}(r_k), accumulated as the "plus" (M' = M - Lam)
+//    and "minus" (M' = -M - Lam, conjugated F) parts and written as plus + minus, plus - minus
+//    into the full l-list.  One warp per row, lanes own the output radial index j.
+//  * ps_pF_map_complex: compute_pF_map_complex (tauNL_utils.pyx:1357-1446): the Gaunt-weighted
+//    shifts (l + Delta, m - mu1) and (l + Delta, -m - mu1) of the [Q F_PQ] harmonics times the
+//    complex p^beta_{l,l+Delta}(r_j) w_j, summed over j.  One thread per (u, l m).
 #include "ps_common.cuh"
 #include "ps_gaunt.cuh"
 #include "ps_stats.cuh"
@@ -171,7 +179,6 @@ coll_general_kernel(const double2* __restrict__ A1, const double2* __restrict__ 
   const int lane = threadIdx.x & 31;
   const int64_t gw = int64_t(blockIdx.x) * kCollWarps + (threadIdx.x >> 5);
   const int64_t nw = int64_t(gridDim.x) * kCollWarps;
-  const int ns = 2 * s + 1;
   double acc = 0.0;
   for (int64_t i = gw; i < nrow; i += nw) {
     const int L = rowL[i], M = rowM[i];
@@ -237,6 +244,151 @@ coll_general_kernel(const double2* __restrict__ A1, const double2* __restrict__ 
     }
   }
   block_partial(acc, partial);
+}
+
+template <int KT>
+__global__ void __launch_bounds__(32 * kCollWarps)
+coll_conv_kernel(const double2* __restrict__ PQ, const double2* __restrict__ cPQ, const int* __restrict__ rowL,
+                 const int* __restrict__ rowM, const int* __restrict__ full_of_row, int nrow, int nLmin, int nLmax,
+                 int Lmin, int Lmax, const double2* __restrict__ F, int nLF, int nrF, int nF,
+                 const double* __restrict__ w, const int* __restrict__ inds, int nr, int s, int lam1,
+                 const double2* __restrict__ Sw, double2* __restrict__ out_re, double2* __restrict__ out_im) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = int64_t(blockIdx.x) * kCollWarps + (threadIdx.x >> 5);
+  const int64_t nw = int64_t(gridDim.x) * kCollWarps;
+  const double inv = 1.0 / (sqrt(2.0 * s + 1.0) * sqrt(4.0 * M_PI) * 2.0);
+  for (int64_t i = gw; i < nrow; i += nw) {
+    const int L = rowL[i], M = rowM[i];
+    if (L < Lmin || L > Lmax || L >= nLF) continue;
+    double2 plus[KT], minus[KT];
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) plus[kt] = minus[kt] = make_double2(0.0, 0.0);
+    // S = 0: diagonal in (L, M)
+    const double2 S0 = Sw[0];
+    if (S0.x != 0.0 || S0.y != 0.0) {
+      const double2 pref = cscale(S0, (((s - lam1) & 1) ? -inv : inv) * (M == 0 ? 2.0 : 1.0));
+      const double2 pref_m = cscale(cconj(S0), inv);
+      const double2* a = PQ + (int64_t(s - lam1) * nrow + i) * nr;
+      const double2* c = cPQ + (int64_t(s + lam1) * nrow + i) * nr;
+      const double2* FL = F + (int64_t(nF) * nLF + L) * nrF * nrF;
+#pragma unroll
+      for (int kt = 0; kt < KT; ++kt) {
+        const int j = lane + 32 * kt;
+        if (j >= nr) continue;
+        const double2* Fj = FL + int64_t(inds[j]) * nrF;
+        double2 tp = make_double2(0.0, 0.0), tm = make_double2(0.0, 0.0);
+        for (int k = 0; k < nr; ++k) {
+          const double wk = w[k];
+          if (wk == 0.0) continue;
+          const double2 f = Fj[inds[k]];
+          tp = cadd(tp, cscale(cmul(a[k], f), wk));
+          if (M != 0) tm = cadd(tm, cscale(cmul(c[k], cconj(f)), wk));
+        }
+        plus[kt] = cadd(plus[kt], cmul(tp, pref));
+        if (M != 0) minus[kt] = cadd(minus[kt], cmul(tm, pref_m));
+      }
+    }
+    // S > 0
+    for (int S = 2; S <= 2 * s; S += 2) {
+      const double2 SwS = Sw[S / 2];
+      for (int Delta = -S; Delta <= S; Delta += 2) {
+        const int Lp = L + Delta;
+        if (Lp < Lmin || Lp > Lmax || abs(Delta) > nF) continue;
+        const double2* FL = F + (int64_t(nF + Delta) * nLF + L) * nrF * nrF;
+        for (int lam = -S; lam <= S; ++lam) {
+          const int lam3 = -lam1 - lam;
+          if (abs(lam3) > s) continue;
+          const double tj = threej_small(s, s, S, lam1, lam3, lam);
+          const double2 pref = cscale(cmul(SwS, ipow(Delta)), tj);
+          if (pref.x == 0.0 && pref.y == 0.0) continue;
+          for (int part = 0; part < 2; ++part) {
+            if (part == 1 && M == 0) break;
+            const int Mp = part == 0 ? M - lam : -M - lam;
+            if (abs(Mp) > Lp) continue;
+            const double g = part == 0 ? gaunt_small(L, Lp, S, -M, M - lam, lam) : gaunt_small(L, Lp, S, M, -M - lam, lam);
+            double sg;
+            if (part == 0) sg = Mp >= 0 ? ((M & 1) ? -1.0 : 1.0) : (((M + Mp + s + lam3) & 1) ? -1.0 : 1.0);
+            else sg = Mp >= 0 ? 1.0 : (((Mp + s + lam3) & 1) ? -1.0 : 1.0);
+            if (part == 1 || M != 0) sg *= 0.5;
+            const double2 gaunt = cscale(part == 0 ? pref : cconj(pref), g * sg);
+            if (gaunt.x == 0.0 && gaunt.y == 0.0) continue;
+            const int lmp = lm_row_index(Lp, Mp, nLmin, nLmax);
+            const double2* b = Mp >= 0 ? PQ + (int64_t(s + lam3) * nrow + lmp) * nr
+                                       : cPQ + (int64_t(s - lam3) * nrow + lmp) * nr;
+#pragma unroll
+            for (int kt = 0; kt < KT; ++kt) {
+              const int j = lane + 32 * kt;
+              if (j >= nr) continue;
+              const double2* Fj = FL + int64_t(inds[j]) * nrF;
+              double2 ks = make_double2(0.0, 0.0);
+              for (int k = 0; k < nr; ++k) {
+                const double wk = w[k];
+                if (wk == 0.0) continue;
+                const double2 f = Fj[inds[k]];
+                double2 v;
+                if (part == 0) v = cmul(Mp >= 0 ? b[k] : cconj(b[k]), f);
+                else v = cmul(Mp >= 0 ? cconj(b[k]) : b[k], cconj(f));
+                ks = cadd(ks, cscale(v, wk));
+              }
+              if (part == 0) plus[kt] = cadd(plus[kt], cmul(ks, gaunt));
+              else minus[kt] = cadd(minus[kt], cmul(ks, gaunt));
+            }
+          }
+        }
+      }
+    }
+    const int full = full_of_row[i];
+    if (full < 0) continue;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+      const int j = lane + 32 * kt;
+      if (j >= nr) continue;
+      const int64_t o = int64_t(full) * nr + j;
+      out_re[o] = cadd(out_re[o], cadd(plus[kt], minus[kt]));
+      out_im[o] = cadd(out_im[o], csub(plus[kt], minus[kt]));
+    }
+  }
+}
+
+__global__ void pF_complex_kernel(const double2* __restrict__ plus, const double2* __restrict__ minus, int lmax_in,
+                                  int nin, const double2* __restrict__ p, int lsize, int npol, int nrp,
+                                  const double* __restrict__ w, const int* __restrict__ inds,
+                                  const int* __restrict__ ls, const int* __restrict__ ms, int64_t nl, int n1, int mu1,
+                                  int nmax, double2* __restrict__ out) {
+  const int64_t total = nl * npol;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = t % nl;
+    const int u = int(t / nl);
+    const int l = ls[i], m = ms[i];
+    double2 acc = make_double2(0.0, 0.0);
+    for (int Delta = -n1; Delta <= n1; Delta += 2) {
+      const int lp = l + Delta;
+      if (lp > lmax_in || lp < 0) continue;
+      const double2* pp = p + ((int64_t(nmax + Delta) * lsize + l) * npol + u) * nrp;
+      for (int part = 0; part < 2; ++part) {
+        const int mp = part == 0 ? m - mu1 : -m - mu1;
+        if (abs(mp) > lp) continue;
+        const int64_t idx = int64_t(abs(mp)) * (lmax_in + 1) + lp - int64_t(abs(mp)) * (abs(mp) + 1) / 2;
+        const double G = part == 0 ? gaunt_small(l, lp, n1, m, -mp, -mu1) : gaunt_small(l, lp, n1, -m, -mp, -mu1);
+        if (G == 0.0) continue;
+        double2 gp = part == 0 ? cscale(ipow(Delta), ((m & 1) ? -0.25 : 0.25) * G) : cscale(ipow(-Delta), 0.25 * G);
+        double2 s = make_double2(0.0, 0.0);
+        for (int j = 0; j < nin; ++j) {
+          const double wj = w[j];
+          if (wj == 0.0) continue;
+          const double2 pj = pp[inds[j]];
+          double2 v;
+          if (part == 0) v = mp >= 0 ? cmul(plus[idx * nin + j], pj) : cmul(cconj(minus[idx * nin + j]), pj);
+          else v = mp >= 0 ? cconj(cmul(plus[idx * nin + j], pj)) : cmul(minus[idx * nin + j], cconj(pj));
+          s = cadd(s, cscale(v, wj));
+        }
+        // gm = gp (-1)^mp, and the minus branch of part 1 carries a further (-1)^mp
+        if (mp < 0 && part == 0 && (mp & 1)) gp = cscale(gp, -1.0);
+        acc = cadd(acc, cmul(gp, s));
+      }
+    }
+    out[int64_t(u) * nl + i] = cadd(out[int64_t(u) * nl + i], acc);
+  }
 }
 
 __global__ void coll_sum_partials(const double* __restrict__ partial, int64_t n, double* __restrict__ out) {
@@ -349,6 +501,53 @@ extern "C" int ps_tau_sum_collider_general(const double* A1, const double* A1c, 
         a1, a1c, a2, a2c, rowL, rowM, nrow, nLmin, nLmax, Lmin, Lmax, f, nLF, nmax_F, w, nr, s, real_beta, c, part);
   PS_LAUNCH_CHECK();
   coll_sum_partials<<<1, 256, 0, stream>>>(part, nblk, out);
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}
+
+extern "C" int ps_convolve_F_collider(const double* PQ, const double* cPQ, const int* rowL, const int* rowM,
+                                      const int* full_of_row, int nrow, int nLmin, int nLmax, int Lmin, int Lmax,
+                                      const double* F, int nLF, int nrF, int nmax_F, const double* w, const int* inds,
+                                      int nr, int s, int lam1, const double* S_weights, double* out_re,
+                                      double* out_im, cudaStream_t stream) {
+  if (!PQ || !cPQ || !rowL || !rowM || !full_of_row || !F || !w || !inds || !S_weights || !out_re || !out_im ||
+      nrow <= 0 || nr <= 0 || nr > 64 || nrF < nr || s < 0 || s > 5 || abs(lam1) > s || nmax_F < 0 || nLF <= Lmax ||
+      nLmin < 0 || nLmax < nLmin || Lmin < nLmin || Lmax > nLmax)
+    return PS_ERR_INVALID;
+  StatScope sc(PS_K_PIXEL, 0.0, 16.0 * double(nrow) * nr * nr * (2 * s + 1) * (2 * s + 1), stream);
+  const int64_t g = coll_grid(nrow);
+  const double2* a = reinterpret_cast<const double2*>(PQ);
+  const double2* c = reinterpret_cast<const double2*>(cPQ);
+  const double2* f = reinterpret_cast<const double2*>(F);
+  const double2* sw = reinterpret_cast<const double2*>(S_weights);
+  double2* ore = reinterpret_cast<double2*>(out_re);
+  double2* oim = reinterpret_cast<double2*>(out_im);
+  if (nr <= 32)
+    coll_conv_kernel<1><<<unsigned(g), 32 * kCollWarps, 0, stream>>>(a, c, rowL, rowM, full_of_row, nrow, nLmin,
+                                                                    nLmax, Lmin, Lmax, f, nLF, nrF, nmax_F, w, inds,
+                                                                    nr, s, lam1, sw, ore, oim);
+  else
+    coll_conv_kernel<2><<<unsigned(g), 32 * kCollWarps, 0, stream>>>(a, c, rowL, rowM, full_of_row, nrow, nLmin,
+                                                                    nLmax, Lmin, Lmax, f, nLF, nrF, nmax_F, w, inds,
+                                                                    nr, s, lam1, sw, ore, oim);
+  PS_LAUNCH_CHECK();
+  return PS_OK;
+}
+
+extern "C" int ps_pF_map_complex(const double* plus, const double* minus, int lmax_in, int nin, const double* p,
+                                 int nshift, int lsize, int npol, int nrp, const double* w, const int* inds,
+                                 const int* ls, const int* ms, int64_t nl, int n1, int mu1, int nmax, double* out,
+                                 cudaStream_t stream) {
+  if (!plus || !minus || !p || !w || !inds || !ls || !ms || !out || lmax_in < 0 || nin <= 0 || nshift != 2 * nmax + 1 ||
+      n1 < 0 || n1 > 16 || n1 > nmax || abs(mu1) > n1 || npol <= 0 || nl <= 0 || nrp <= 0)
+    return PS_ERR_INVALID;
+  StatScope sc(PS_K_PIXEL, 0.0, 16.0 * double(nl) * npol * nin * (n1 + 1) * 2, stream);
+  int64_t g = (nl * npol + 127) / 128;
+  if (g > 148 * 64) g = 148 * 64;
+  pF_complex_kernel<<<int(g), 128, 0, stream>>>(reinterpret_cast<const double2*>(plus),
+                                                reinterpret_cast<const double2*>(minus), lmax_in, nin,
+                                                reinterpret_cast<const double2*>(p), lsize, npol, nrp, w, inds, ls, ms,
+                                                nl, n1, mu1, nmax, reinterpret_cast<double2*>(out));
   PS_LAUNCH_CHECK();
   return PS_OK;
 }

@@ -395,6 +395,70 @@ class tauNL_utils:
         else:
             _output[...] = out.cpu().numpy()
 
+    def compute_pF_map_complex(self, _input_plus, _input_minus, _plLXs, _r_weights, n1, mu1, nmax, lmax, _output,
+                               inds):
+        """tauNL_utils.pyx:1357-1446: _output [npol, len(ls)] += the Gaunt-weighted shifts of the inputs
+        ([nlm(lmax), len(inds)] complex) times the complex collider p^beta_{l,l+Delta}^X(r) w_r, in place
+        (ps_pF_map_complex); -n1 <= mu1 <= n1."""
+        plus, _ = _prep(_input_plus, torch.complex128)
+        minus, _ = _prep(_input_minus, torch.complex128)
+        pl, _ = _prep(_plLXs, torch.complex128)
+        w = torch.as_tensor(np.asarray(_r_weights, dtype=np.float64), device=plus.device)
+        ind = _i32(inds)
+        if not hasattr(self, '_d_ms'):
+            self._d_ms = torch.as_tensor(self.ms, device=_dev())
+            self._d_ls32 = torch.as_tensor(self.ls, device=_dev())
+        nshift, lsize, npol, nrp = pl.shape
+        out, _ = _prep(_output, torch.complex128)
+        _lib.call("ps_pF_map_complex", ctypes.c_void_p(plus.data_ptr()), ctypes.c_void_p(minus.data_ptr()),
+                  int(lmax), plus.shape[1], ctypes.c_void_p(pl.data_ptr()), nshift, lsize, npol, nrp,
+                  ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(ind.data_ptr()),
+                  ctypes.c_void_p(self._d_ls32.data_ptr()), ctypes.c_void_p(self._d_ms.data_ptr()), len(self.ls),
+                  int(n1), int(mu1), int(nmax), ctypes.c_void_p(out.data_ptr()), _stream())
+        if isinstance(_output, torch.Tensor):
+            if _output.data_ptr() != out.data_ptr():
+                _output.copy_(out)
+        else:
+            _output[...] = out.cpu().numpy()
+
+    def convolve_F_general_collider(self, PQ, cPQ, FLLs, r_weights, out_real, out_imag, s, lam1, nmax_F, S_weights,
+                                    inds):
+        """tauNL_utils.pyx:1197-1355: the collider F convolution for one lam1, accumulated in place into
+        out_real / out_imag [len(l <= nLmax), len(inds)] (ps_convolve_F_collider)."""
+        nLmax, row_of_full, rowL, rowM, full_of_row = self._row_tables()
+        a, _ = _prep(PQ, torch.complex128)
+        c, _ = _prep(cPQ, torch.complex128)
+        F, _ = _prep(FLLs, torch.complex128)
+        dev = a.device
+        w = torch.as_tensor(np.asarray(r_weights, dtype=np.float64), device=dev)
+        sw = torch.as_tensor(np.asarray(S_weights, dtype=np.complex128).reshape(-1), device=dev)
+        ind = _i32(inds)
+        nrow, nr = len(self.Ls), a.shape[-1]
+        if (a.shape != c.shape or a.dim() != 3 or tuple(a.shape[1:]) != (nrow, nr) or F.dim() != 4
+                or F.shape[0] != 2 * int(nmax_F) + 1 or F.shape[2] != F.shape[3] or F.shape[1] <= self.Lmax
+                or ind.numel() != nr or sw.numel() != int(s) + 1):
+            raise ValueError("convolve_F_general_collider: PQ, cPQ [2s+1, len(Ls), len(inds)], FLLs "
+                             "[2 nmax_F + 1, > Lmax, N_r, N_r], S_weights [s + 1]")
+        ore, _ = _prep(out_real, torch.complex128)
+        oim, _ = _prep(out_imag, torch.complex128)
+        _lib.call("ps_convolve_F_collider", ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(c.data_ptr()),
+                  ctypes.c_void_p(rowL.data_ptr()), ctypes.c_void_p(rowM.data_ptr()),
+                  ctypes.c_void_p(full_of_row.data_ptr()), nrow, int(self.Ls.min()), nLmax, self.Lmin, self.Lmax,
+                  ctypes.c_void_p(F.data_ptr()), F.shape[1], F.shape[2], int(nmax_F), ctypes.c_void_p(w.data_ptr()),
+                  ctypes.c_void_p(ind.data_ptr()), nr, int(s), int(lam1), ctypes.c_void_p(sw.data_ptr()),
+                  ctypes.c_void_p(ore.data_ptr()), ctypes.c_void_p(oim.data_ptr()), _stream())
+        for dst, src in ((out_real, ore), (out_imag, oim)):
+            if isinstance(dst, torch.Tensor):
+                if dst.data_ptr() != src.data_ptr():
+                    dst.copy_(src)
+            else:
+                dst[...] = src.cpu().numpy()
+
+    def convolve_F_n000_real(self, PQ, FLLs, r_weights, out, nmax_F, inds):
+        """tauNL_utils.pyx:997-1023: convolve_F_n000 with the real part of a complex (collider) F."""
+        F = FLLs.real.contiguous() if isinstance(FLLs, torch.Tensor) else np.ascontiguousarray(np.real(FLLs))
+        self.convolve_F_n000(PQ, F, r_weights, out, nmax_F, inds)
+
     def shift_and_weight_map_all(self, flX, h_lm, n, mu, weight, Larr_real, Larr_imag, nmax):
         """Gaunt-weighted l-shifts of the transfer-weighted harmonics (tauNL_utils.pyx:407-512):
         Larr_real/imag [N_r, nlm(lmax + n)] += Sum over shifts Delta of the (L = l + Delta, |mu -+ m|)
@@ -631,6 +695,50 @@ def r2cstar_inplace(re_arr, im_arr, out_arr, mu_index, nthreads=0):
         out_arr[mu_index] = torch.as_tensor(v, device=out_arr.device)
     else:
         out_arr[mu_index] = v.cpu().numpy() if isinstance(v, torch.Tensor) else v
+
+
+def compute_productP_all(P_map, F_PQ, weights, pq_inds, F_inds, nthreads=0):
+    """ideal_fisher.pyx:160-175: Sum_i w_i Re(P[pq_i] F_PQ[F_i]) for complex P (real [N_r, Npix])."""
+    P, as_torch = _prep(P_map, torch.complex128)
+    F, _ = _prep(F_PQ, torch.complex128)
+    out = torch.zeros(P.shape[1:], dtype=torch.float64, device=P.device)
+    for w, ip, iF in zip(np.asarray(weights, dtype=np.float64), pq_inds, F_inds):
+        out += float(w) * (P[int(ip)] * F[int(iF)]).real
+    return _ret(out, as_torch)
+
+
+def compute_productPnmu_all(Pnmu_maps, conjPnmu_maps, F_PQ, weights, n1, pq_inds, F_inds, nthreads=0):
+    """ideal_fisher.pyx:216-234: Sum_i w_i Re(P[pq_i, 0] F[F_i, n1] + Sum_{mu >= 1} (P[pq_i, mu] F[F_i, n1 + mu]
+    + (-1)^(n1-mu) conj(Pc[pq_i, mu]) F[F_i, n1 - mu])) for the complex collider P^beta maps and those of conj(beta)."""
+    P, as_torch = _prep(Pnmu_maps, torch.complex128)
+    Pc, _ = _prep(conjPnmu_maps, torch.complex128)
+    F, _ = _prep(F_PQ, torch.complex128)
+    n1 = int(n1)
+    out = torch.zeros(P.shape[2:], dtype=torch.float64, device=P.device)
+    for w, ip, iF in zip(np.asarray(weights, dtype=np.float64), pq_inds, F_inds):
+        ip, iF = int(ip), int(iF)
+        acc = P[ip, 0] * F[iF, n1]
+        for mu1 in range(1, n1 + 1):
+            acc = acc + P[ip, mu1] * F[iF, n1 + mu1] + (-1.) ** (n1 - mu1) * Pc[ip, mu1].conj() * F[iF, n1 - mu1]
+        out += float(w) * acc.real
+    return _ret(out, as_torch)
+
+
+def complex_to_complex_transpose(map1, map2, nthreads=0):
+    """ideal_fisher.pyx:291-303: out[0] = map1 + i map2, out[1] = map1 - i map2 (no transpose)."""
+    a, as_torch = _prep(map1, torch.complex128)
+    b, _ = _prep(map2, torch.complex128)
+    return _ret(torch.stack([a + 1j * b, a - 1j * b]).contiguous(), as_torch)
+
+
+def integrate_pq_complex(flXs, P_FPQ_plus, P_FPQ_minus, ls, r_weights, out, inds, nthreads=0):
+    """ideal_fisher.pyx:378-391: out[X, lm] += Sum_i 0.25 w_i (f[l, X, inds i] plus[lm, i] + conj(f) minus[lm, i])
+    for complex f, as the two real radial sums of Re f (plus + minus) / 2 and Im f i (plus - minus) / 2."""
+    f, _ = _prep(flXs, torch.complex128)
+    pp, _ = _prep(P_FPQ_plus, torch.complex128)
+    mm, _ = _prep(P_FPQ_minus, torch.complex128)
+    integrate_pq(f.real.contiguous(), 0.5 * (pp + mm), ls, r_weights, out, inds)
+    integrate_pq(f.imag.contiguous(), 0.5j * (pp - mm), ls, r_weights, out, inds)
 
 
 def integrate_pq(flXs, P_FPQ, ls, r_weights, out, inds, nthreads=0):

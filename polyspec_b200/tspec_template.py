@@ -840,6 +840,23 @@ class TSpecTemplate:
                 out[n] = torch.stack([torch.stack([self._compute_weighted_gaunt_maps(m, self.d_plLXs, n, mu)
                                                    for mu in range(n + 1)]) for m in input_maps])
             return out
+        if filtering == 'coll-P':
+            # collider P^beta_{s,lam} maps [2, s+1, N_r, Npix] per (beta, s) (polyspec/tspec_template.py:995-1019)
+            out = {}
+            for beta in self.coll_params:
+                if np.imag(beta) == 0:
+                    re, im = self.d_coll_plLXs[beta].real.contiguous(), None
+                elif np.imag(beta) < 0:
+                    re, im = self.d_coll_plLXs[beta].real.contiguous(), self.d_coll_plLXs[beta].imag.contiguous()
+                else:
+                    P = self.d_coll_plLXs[np.conj(beta)]
+                    re, im = P.real.contiguous(), (-P.imag).contiguous()
+                for s_ in np.unique(self.coll_params[beta][:, 0]):
+                    s_ = int(s_)
+                    out[beta, s_] = torch.stack([torch.stack([
+                        self._compute_weighted_gaunt_maps(m, re, s_, lam, im).to(torch.complex128)
+                        for lam in range(s_ + 1)]) for m in input_maps])
+            return out
         spin0 = {'Q': 'd_qlXs', 'R': 'd_rlXs', 'A': 'd_alXs', 'B': 'd_blXs'}
         if filtering in spin0:
             return torch.stack([self._compute_weighted_maps(m, getattr(self, spin0[filtering])) for m in input_maps])
@@ -1158,6 +1175,184 @@ class TSpecTemplate:
             host = {k: np.asarray(v, dtype=np.complex128) for k, v in arrs.items()}
             setattr(self, name, host)
             setattr(self, 'd_' + name, {k: torch.as_tensor(v, device=self._dev) for k, v in host.items()})
+
+    def _coll_lm(self, x):
+        """Harmonic rows [len(Ls), N_r] of maps [N_r, Npix] up to nLmax."""
+        return self.base.to_lm_vec(x.contiguous(), lmax=self.nLmax)[:, self.d_nLminfilt_idx].T
+
+    def _compute_coll_PQ_vecs(self, Ps_maps, Q_maps, i, j, s, beta, add_sym=False, conjPs_maps=None):
+        """[P^beta_{s,lam} Q]_LM vectors [2s+1, len(Ls), N_r] of polyspec/tspec_template.py:2012-2137, and for complex
+        beta those of the conjugate maps."""
+        def prod(P1, P2, lam, fac=None):
+            if fac is None:
+                if add_sym:
+                    return pixel.multiplyRC_sym(Q_maps[j], P1[i, lam], Q_maps[i], P2[j, lam])
+                return pixel.multiplyRC(Q_maps[j], P1[i, lam])
+            if add_sym:
+                return pixel.multiplyRCstar_sym(Q_maps[j], P1[i, lam], Q_maps[i], P2[j, lam], fac)
+            return pixel.multiplyRCstar(Q_maps[j], P1[i, lam], fac)
+
+        if s == 0:  # with complex beta the conjugate vector is a - i b of the same product (the reference's :2016-2033)
+            pm = prod(Ps_maps, Ps_maps, 0)
+            if np.imag(beta) == 0:
+                return self._coll_lm(pm.real)[None]
+            a, b = self._coll_lm(pm.real), self._coll_lm(pm.imag)
+            return (a + 1j * b)[None], (a - 1j * b)[None]
+        nrow = int(np.sum(self.nLminfilt))
+        nr = Q_maps.shape[1]
+        PQ = torch.zeros((2 * s + 1, nrow, nr), dtype=torch.complex128, device=self._dev)
+        if conjPs_maps is None:
+            assert np.imag(beta) == 0.
+            for lam3 in range(s + 1):
+                pm = prod(Ps_maps, Ps_maps, lam3)
+                if lam3 == 0 and s % 2 == 0:
+                    PQ[s] = self._coll_lm(pm.real)
+                elif lam3 == 0:
+                    PQ[s] = 1.0j * self._coll_lm(pm.imag)
+                else:
+                    pr, pi = self._coll_lm(pm.real), 1.0j * self._coll_lm(pm.imag)
+                    PQ[s + lam3] = pr + pi
+                    PQ[s - lam3] = (-1.) ** (s - lam3) * (pr - pi)
+            return PQ
+        cPQ = torch.zeros_like(PQ)
+        for lam3 in range(-s, s + 1):
+            if lam3 < 0:
+                pm = prod(conjPs_maps, conjPs_maps, -lam3, (-1.) ** (s + lam3))
+            else:
+                pm = prod(Ps_maps, Ps_maps, lam3)
+            PQ[s + lam3] = self._coll_lm(pm.real) + 1.0j * self._coll_lm(pm.imag)
+        if np.imag(beta) == 0:
+            return PQ, PQ
+        for lam3 in range(-s, s + 1):
+            if lam3 < 0:
+                pm = prod(Ps_maps, Ps_maps, -lam3, (-1.) ** (s + lam3))
+            else:
+                pm = prod(conjPs_maps, conjPs_maps, lam3)
+            cPQ[s + lam3] = self._coll_lm(pm.real) + 1.0j * self._coll_lm(pm.imag)
+        return PQ, cPQ
+
+    def _coll_S_weights(self, s, nu_s):
+        return np.asarray([self._calC(s, S, 1.0j * nu_s) * np.exp(1.0j * self._omega_prime(s, 1.0j * nu_s))
+                           for S in range(0, 2 * s + 1, 2)], dtype=np.complex128)
+
+    def _convolve_coll_F(self, PQ_vecs, r_weights, s, beta, conjPQ_vecs=None):
+        """Sum_S C_S F^beta * [P^beta_{s,lam3} Q] maps for every lam1 (polyspec/tspec_template.py:2192-2283):
+        [s+1 (real beta) or 2s+1, N_r, Npix] complex; s = 0 with real beta uses the real part of F."""
+        nr = self.N_r
+        inds = np.arange(nr, dtype=np.int32)
+        nu_s = beta + 1.5
+        nF = int(np.max(self.coll_params[beta][:, 1]))
+        F = self.d_coll_FLLs[beta]
+        nfull = len(self.nLminfilt)
+        b = self.base
+
+        def maps(o_re, o_im):
+            if bool((o_im != 0.).any()):
+                return pixel.r2cstar(b.to_map_vec(o_re.T.contiguous(), lmax=self.nLmax),
+                                     b.to_map_vec((1.0j * o_im).T.contiguous(), lmax=self.nLmax))
+            return b.to_map_vec(o_re.T.contiguous(), lmax=self.nLmax).to(torch.complex128)
+
+        if s == 0 and np.imag(beta) == 0:
+            out = torch.zeros((nfull, nr), dtype=torch.complex128, device=self._dev)
+            self.utils.convolve_F_n000_real(PQ_vecs[0], F, r_weights, out, nF, inds)
+            out *= (4. * np.pi) ** (3. / 2.)
+            return b.to_map_vec(out.T.contiguous(), lmax=self.nLmax).to(torch.complex128)[None]
+        Sw = self._coll_S_weights(s, nu_s)
+        cPQ = PQ_vecs if conjPQ_vecs is None else conjPQ_vecs
+        lams = range(s + 1) if np.imag(beta) == 0 else range(-s, s + 1)
+        out = torch.zeros((len(lams), nr, b.Npix), dtype=torch.complex128, device=self._dev)
+        for idx, lam1 in enumerate(lams):
+            o_re = torch.zeros((nfull, nr), dtype=torch.complex128, device=self._dev)
+            o_im = torch.zeros_like(o_re)
+            self.utils.convolve_F_general_collider(PQ_vecs, cPQ, F, r_weights, o_re, o_im, s, lam1, nF, Sw, inds)
+            if s == 0:
+                out[idx] = pixel.r2cstar(b.to_map_vec(o_re.T.contiguous(), lmax=self.nLmax),
+                                         b.to_map_vec((1.0j * o_im).T.contiguous(), lmax=self.nLmax))
+            else:
+                out[idx] = maps(o_re, o_im)
+        return out
+
+    def _coll_F_PQ(self, Ps_maps, Q_maps, r_weights, s, beta, conjPs_maps=None):
+        """F^beta_L * [P^beta_{s,lam} Q]_LM maps of the (1, 1), (2, 2) and symmetrised (1, 2) pairs
+        (polyspec/tspec_template.py:2308-2337): [3, s+1 or 2s+1, N_r, Npix] complex."""
+        out = []
+        for i1, i2 in ((0, 0), (1, 1), (0, 1)):
+            t0 = time.time()
+            if np.imag(beta) == 0:
+                PQ = self._compute_coll_PQ_vecs(Ps_maps, Q_maps, i1, i2, s, beta, add_sym=(i1 != i2))
+                out.append(self._convolve_coll_F(PQ, r_weights, s, beta))
+            else:
+                PQ, cPQ = self._compute_coll_PQ_vecs(Ps_maps, Q_maps, i1, i2, s, beta, add_sym=(i1 != i2),
+                                                     conjPs_maps=conjPs_maps)
+                out.append(self._convolve_coll_F(PQ, r_weights, s, beta, conjPQ_vecs=cPQ))
+            self._timed('fish_convolve', t0)
+        return torch.stack(out)
+
+    def _Q4_contributions_coll(self, Pn1_maps, Q_maps, F_PQ, pq_inds, F_inds, r_weights, weights, n1, beta,
+                               conjPn1_maps=None):
+        """One Q4 row of a collider template (polyspec/tspec_template.py:2340-2495 with beta_coll): the q_l^X radial
+        sum of [P^beta F_PQ]_lm plus the p^beta-weighted sums of the shifted [Q F_PQ]_lm."""
+        t0 = time.time()
+        b = self.base
+        w = np.asarray(r_weights, dtype=np.float64)
+        nr = Q_maps.shape[1]
+        inds = np.arange(nr, dtype=np.int32)
+        out = torch.zeros((1 + 2 * self.pol, len(self.ls)), dtype=torch.complex128, device=self._dev)
+        this_nmax = int(np.max(self.coll_params[beta][:, 0]))
+        P = self.d_coll_plLXs[beta]
+        cplx = np.imag(beta) != 0
+        if n1 == 0:
+            prod = pixel.compute_productP_all(Pn1_maps[:, 0], F_PQ[:, 0], weights, pq_inds, F_inds)
+            lm = b.to_lm_vec(prod, lmax=self.lmax)[:, self.d_lminfilt]
+            pixel.integrate_pq(self.d_qlXs, lm.T, self.ls, w, out, inds)
+            if cplx:
+                prod = pixel.compute_productQ_complex_all(Q_maps, F_PQ, weights, pq_inds, F_inds, 0)
+                re = b.to_lm_vec(prod.real.contiguous(), lmax=self.lmax)[:, self.d_lminfilt].T
+                im = b.to_lm_vec(prod.imag.contiguous(), lmax=self.lmax)[:, self.d_lminfilt].T
+                plus, minus = pixel.complex_to_complex_transpose(re, im)
+                pixel.integrate_pq_complex(P[this_nmax], plus, minus, self.ls, w / np.sqrt(4. * np.pi), out, inds)
+            else:
+                prod = pixel.compute_productQ_real_all(Q_maps, F_PQ, weights, pq_inds, F_inds, 0)
+                plus = b.to_lm_vec(prod, lmax=self.lmax)[:, self.d_lminfilt].T
+                pixel.integrate_pq(P[this_nmax].real.contiguous(), plus, self.ls, w / np.sqrt(4. * np.pi), out, inds)
+            self._timed('fish_deriv', t0)
+            return out
+        if cplx:
+            prod = pixel.compute_productPnmu_all(Pn1_maps, conjPn1_maps, F_PQ, weights, n1, pq_inds, F_inds)
+        else:
+            prod = pixel.compute_productPnmu_sym_all(Pn1_maps, F_PQ, weights, n1, pq_inds, F_inds)
+        lm = b.to_lm_vec(prod, lmax=self.lmax)[:, self.d_lminfilt]
+        pixel.integrate_pq(self.d_qlXs, lm.T, self.ls, w, out, inds)
+        lmx = min(self.lmax + n1, b.lmax)
+        for mu1 in range(-n1, n1 + 1):
+            if cplx:
+                mu1_index = n1 + mu1
+            else:
+                if mu1 < 0:
+                    continue
+                mu1_index = mu1
+            if bool((F_PQ[F_inds[0], mu1_index, :, 0].imag != 0).any()):
+                prod = pixel.compute_productQ_complex_all(Q_maps, F_PQ, weights, pq_inds, F_inds, mu1_index)
+                pm = pixel.complex_to_complex(b.to_lm_vec(prod.real.contiguous(), lmax=lmx),
+                                              b.to_lm_vec(prod.imag.contiguous(), lmax=lmx))
+                plus, minus = pm[0], pm[1]
+            else:
+                prod = pixel.compute_productQ_real_all(Q_maps, F_PQ, weights, pq_inds, F_inds, mu1_index)
+                plus = b.to_lm_vec(prod, lmax=lmx).T.to(torch.complex128).contiguous()
+                minus = plus
+            if cplx:
+                self.utils.compute_pF_map_complex(plus, minus, P, w, n1, mu1, this_nmax, lmx, out, inds)
+            else:
+                self.utils.compute_pF_map_real(plus, minus, P.real.contiguous(), w, n1, mu1, this_nmax, lmx, out,
+                                               inds)
+        self._timed('fish_deriv', t0)
+        return out
+
+    def _get_Q4_perms_coll(self, P_maps, Q_maps, F_PQ, r_weights, n1, beta, conjP_maps=None):
+        """The four Q4 rows (111, 222, 112, 122) of a collider template (polyspec/tspec_template.py:2521-2554)."""
+        rows = (([0], [0], [12.]), ([1], [1], [12.]), ([1, 0], [0, 2], [4., 4.]), ([0, 1], [1, 2], [4., 4.]))
+        return torch.stack([self._Q4_contributions_coll(P_maps, Q_maps, F_PQ, p, f, r_weights, w, n1, beta,
+                                                        conjP_maps) for p, f, w in rows])
 
     def _compute_PQ_vecs(self, Pn3_maps, Q_maps, i, j, n3=0, add_sym=False):
         """[P Q]_LM(r) of polyspec/tspec_template.py:1967-2010 for n3 = 0, [N_r, nlm(nLmax)]."""
@@ -1699,9 +1894,6 @@ class TSpecTemplate:
 
         ``a_lms`` (two beam-deconvolved harmonic fields) may replace the fields drawn
         from ``seed``."""
-        if any(_is_coll(t) for t in self.templates):
-            raise NotImplementedError("the Fisher matrix of the collider templates is not implemented by the CUDA "
-                                      "backend")
         t_start = time.time()
         self._check_sampling()
         print("Computing Fisher matrix with seed %d" % seed)
@@ -1752,6 +1944,8 @@ class TSpecTemplate:
                 V_maps = self._filter_pair(U, 'V')
             if len(self.p_inds) > 0:
                 P_maps = self._filter_pair(U, 'P')
+            if len(self.coll_params) > 0:
+                coll_P = self._filter_pair(U, 'coll-P')
             Qs = torch.zeros((4, nt, 1 + 2 * self.pol, len(self.ls)), dtype=torch.complex128, device=self._dev)
             for ii, t in enumerate(self.templates):
                 if t == 'gNL-loc':
@@ -1805,6 +1999,16 @@ class TSpecTemplate:
                             F_vecs = self._F_PQ_n(P_maps[c], Q_maps, w, a, c, n)
                             Qs[:, ii] += wt * self._get_Q4_perms_n(P_maps[a], Q_maps, F_vecs, w, a)
                         del F_vecs
+                if _is_coll(t):
+                    # collider Q-derivative (polyspec/tspec_template.py:2691-2706, 2896-2914)
+                    w = self.r_weights[t]
+                    s_, x = _coll_parse(t)
+                    beta = -1.5 + x if 'tauNL-light' in t else -1.5 - 1.0j * x
+                    Ps = coll_P[beta, s_]
+                    cPs = coll_P[np.conj(beta), s_] if np.imag(beta) != 0 else None
+                    F_vecs = self._coll_F_PQ(Ps, Q_maps, w, s_, beta, conjPs_maps=cPs)
+                    Qs[:, ii] += self._get_Q4_perms_coll(Ps, Q_maps, F_vecs, w, s_, beta, cPs)
+                    del F_vecs
                 if t == 'gNL-dotdel':
                     Qs[:, ii] = self._dotdel_Q(A_maps, B_maps, C_maps, self.rtau_weights[t])
                 if t == 'gNL-deldel':

@@ -7,14 +7,15 @@ integrals (k_integrals.pyx:399-545, restated by the oracle shim).
 
 The collider p^beta and F^beta integrals computed on the GPU are compared with the fixture's
 (1e-9 of the largest magnitude per beta); the numerators (4-field, and with the 2- and 0-field
-terms of one simulation pair) with the fixture's integrals injected, to 1e-9 relative per
-entry, and with the GPU's own integrals to 1e-7."""
+terms of one simulation pair) and the Fisher contribution of seed 1 with the fixture's integrals
+injected, to 1e-9 relative per entry (Fisher entries relative to sqrt(F_ii F_jj)), and the
+numerator with the GPU's own integrals to 1e-7."""
 import os
 
 import numpy as np
 import pytest
 
-from test_tspec import rel_each
+from test_tspec import rel_each, fisher_err
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 TOL = 1e-9
@@ -82,6 +83,16 @@ def test_numerator(pol):
     tst.generate_sims(1)
     assert rel_each(tst.Tl_numerator(d["data"], include_disconnected_term=False), d["tl_num_4"]) < TOL
     assert rel_each(tst.Tl_numerator(d["data"], include_disconnected_term=True), d["tl_num_full"]) < TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pol", [False, True])
+def test_fisher_contribution(pol):
+    """compute_fisher_contribution(1): the collider Q-derivatives (convolve_F_general_collider,
+    convolve_F_n000_real, compute_pF_map_complex / _real of tauNL_utils.pyx:997-1446) against the fixture,
+    each entry to 1e-9 of sqrt(F_ii F_jj)."""
+    d, tst = _build(pol)
+    assert fisher_err(tst.compute_fisher_contribution(1), d["fisher_seed1"]) < TOL
 
 
 @pytest.mark.gpu
