@@ -1,6 +1,7 @@
 """Template trispectrum estimator on the GPU (mirror of polyspec/tspec_template.py)
 for the gNL-loc, gNL-con, EFTI (gNL-dotdot, gNL-dotdel, gNL-deldel), tauNL-loc,
-direction-dependent tauNL-direc:n1,n3,n, lensing and point-source templates.
+direction-dependent tauNL-direc:n1,n3,n, tauNL-even:n, tauNL-odd:n, collider
+tauNL-light:s,nu_s and tauNL-heavy:s,mu_s, lensing and point-source templates.
 
 ``TSpecTemplate(base, mask, applySinv, templates, k_arr, Tl_arr, lmin, lmax, ...)``
 keeps the reference constructor, its checks and attributes (l- and L-ranges and
@@ -8,9 +9,8 @@ filters, ``to_compute``, ``p_inds``, ``qlXs``, ``plLXs``, ``rlXs``, ``alXs``,
 ``blXs``, ``clXs``, ``timers``), the
 simulation handling (``generate_sims``, ``load_sims``) and the estimator methods
 (``Tl_numerator``, ``compute_fisher_contribution``, ``compute_fisher``,
-``Tl_unwindowed``, ``report_timings``, ``reset_timings``).  The reference's
-tauNL-even/odd combinations and its collider templates raise NotImplementedError,
-as do the radial-sampling optimisers.
+``Tl_unwindowed``, ``report_timings``, ``reset_timings``).  The radial-sampling
+optimisers raise NotImplementedError.
 
 ``applySinv`` receives and returns CUDA tensors (as for PSpecBin/BSpecBin here);
 one with a ``.batched`` method filters the 4 x n_templates Q rows of the Fisher
@@ -29,6 +29,11 @@ Device mapping:
   the (P Q)_LM maps are a product kernel plus a batched adjoint to Lmax; the sum
   over (L, M, r, r') and the F-convolution of the Fisher derivative are
   ``ps_tau_convolve_F``.
+* Collider templates: the complex p^beta integrals are ``ps_kint_radial`` on the real
+  and imaginary parts of the k-weight, F^beta is ``ps_kint_collider_jlK`` +
+  ``ps_kint_collider_F``; the tau sums are ``ps_tau_sum_collider_diag`` (s = 0 and
+  nu_s = 0) and ``ps_tau_sum_collider_general``; the Fisher derivative convolves with
+  ``ps_convolve_F_collider`` and shifts with ``ps_pF_map_complex``.
 * Numerators: the radial pixel sums ``gnl_*(_disc)_sum``; lensing and point
   source sums are device reductions.
 * Fisher: the ``multiply*`` products, a batched spin-0 or spin-1 adjoint over the
