@@ -41,7 +41,6 @@ namespace ps {
 namespace {
 
 constexpr int kCollWarps = 8;
-constexpr int64_t kCollMaxBlocks = 148 * 8;
 
 __global__ void coll_jlK_kernel(const double* __restrict__ table, const double* __restrict__ xs, int64_t nx, int nl,
                                 const double* __restrict__ K, int nK, const double* __restrict__ r, int nr,
@@ -404,9 +403,12 @@ __global__ void coll_sum_partials(const double* __restrict__ partial, int64_t n,
   if (threadIdx.x == 0) out[0] = red[0];
 }
 
+// CTAs of the per-row kernels: one per kCollWarps rows, at most 8 per SM of the current device; the
+// workspace query and the launches size by this one function (one partial sum per CTA)
 int64_t coll_grid(int64_t nrow) {
+  const int64_t cap = int64_t(device_sms()) * 8;
   const int64_t g = (nrow + kCollWarps - 1) / kCollWarps;
-  return g > kCollMaxBlocks ? kCollMaxBlocks : (g < 1 ? 1 : g);
+  return g > cap ? cap : (g < 1 ? 1 : g);
 }
 
 }  // namespace

@@ -28,7 +28,8 @@ S^-1 filter) per precision: device time, kernel time per kind, the numerator
 with two simulations, and the mixed-vs-FP64 Fisher difference.
 
     python -m polyspec_b200.profile_cli tspecbin [--nside 128 --lmax 255 --nbins 6]
-    python -m polyspec_b200.profile_cli tspec [--nside 512 --lmax 1000 --nr 24 --templates gNL-loc,...]
+    python -m polyspec_b200.profile_cli tspec [--nside 512 --lmax 1000 --nr 24 --templates gNL-loc,...
+                                               --K-coll 0.1]
 
 the binned trispectrum (T+E) and the template trispectrum (gNL-loc, lensing,
 point source): Fisher contribution and numerator times, FP64 and mixed.
@@ -262,7 +263,8 @@ def tspec(a):
         tst = TSpecTemplate(base, w['mask'], wts.make_applySinv('ideal'), templates,
                             w['k_arr'], w['Tl_arr'], w['lmin'], w['lmax'], r_values=w['r_values'],
                             r_weights=r_weights, rtau_values=w['rtau_values'], rtau_weights=w['rtau_weights'],
-                            C_phi=w['C_phi'], C_lens_weight=w['C_lens_weight'], Lmax=a.Lmax)
+                            C_phi=w['C_phi'], C_lens_weight=w['C_lens_weight'], Lmax=a.Lmax,
+                            K_coll=a.K_coll, k_coll=a.K_coll)
         torch.cuda.synchronize()
         t_setup = time.time() - t0
         a_lms = [base.generate_data(seed=21 + i, deconvolve_beam=True, output_type='harmonic', rng='device')
@@ -430,6 +432,8 @@ def main(argv=None):
                    help="exchange-momentum L range top (default min(3 Nside - 1, 2 lmax); templates with n > 0 "
                         "need Lmax + n <= 3 Nside - 1)")
     t.add_argument("--templates", default="gNL-loc,lensing,point-source")
+    t.add_argument("--K-coll", dest="K_coll", type=float, default=0.1,
+                   help="collider cut-offs K_coll = k_coll (tauNL-light:s,nu_s / tauNL-heavy:s,mu_s templates)")
     tb = sub.add_parser("tspecbin")
     tb.add_argument("--nside", type=int, default=128)
     tb.add_argument("--lmax", type=int, default=255)
