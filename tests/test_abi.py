@@ -47,3 +47,21 @@ def test_invalid_arguments_are_rejected_without_touching_the_gpu():
     assert L.ps_plan_create(16, 10, 9, 1, 0, ctypes.byref(ctypes.c_void_p())) == -1
     assert L.ps_synthesis(None, None, None, 1, 0, None, 0, None) == -1
     assert L.ps_adjoint(None, None, None, 1, 0, 1.0, None, 0, None) == -1
+
+
+def test_collider_entry_points_reject_invalid_arguments_without_the_gpu():
+    """The collider entry points validate pointers and sizes on the host before any launch."""
+    from polyspec_b200 import _lib
+    L = _lib.lib()
+    nb = ctypes.c_size_t()
+    assert L.ps_tau_collider_workspace_bytes(0, ctypes.byref(nb)) == -1
+    assert L.ps_kint_collider_jlK(None, None, 10, 1, None, 1, None, 1, None, None) == -1
+    assert L.ps_kint_collider_F(None, 1, 0, None, 1, None, 1, 2, 10, 0, 11, None, None) == -1
+    assert L.ps_tau_sum_collider_diag(None, None, 1, None, None, 1, 2, 10, None, 11, None, 1, 1.0, 0.0, None, None,
+                                      0, None) == -1
+    assert L.ps_tau_sum_collider_general(None, None, None, None, None, None, 1, 0, 10, 2, 10, None, 11, 2, None, 1,
+                                         1, 1, None, None, None, 0, None) == -1
+    assert L.ps_convolve_F_collider(None, None, None, None, None, 1, 0, 10, 2, 10, None, 11, 1, 2, None, None, 1, 1,
+                                    0, None, None, None, None) == -1
+    assert L.ps_pF_map_complex(None, None, 10, 1, None, 3, 11, 1, 1, None, None, None, None, 1, 1, 0, 1, None,
+                               None) == -1
