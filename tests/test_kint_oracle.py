@@ -1,6 +1,6 @@
 """The oracle's k-space integral restatement (oracle/shims/k_integrals.py) on the
-CPU: j_l' from the recurrence against scipy's derivative, and the (r, tau)
-integrals against the golden fixtures made through the reference."""
+CPU: j_l' from the recurrence against scipy's derivative, and the (r, tau) and
+collider integrals against the golden fixtures made through the reference."""
 import os
 
 import numpy as np
@@ -110,3 +110,42 @@ def test_F_integral_shifted_against_mpmath():
                                                         - mpmath.loggamma(i3))
                 exact = float(pf * mpmath.hyp2f1(i1, i2, i3, x) * pw * big ** (1 - ns))
                 assert abs(F[2 + n, L, i, j] - exact) <= 1e-11 * abs(exact), (n, L, i, j)
+
+
+def test_collider_integrals_match_fixture():
+    """The shim's collider p^beta and F^beta integrals (collider_p_integral, compute_collider_F_integral) from the
+    collider fixture's inputs, on the reference's grids (polyspec/tspec_template.py:536-703), T only: beta =
+    nu_s - 3/2 for the light particles and -3/2 - i mu_s for the heavy ones (Im beta > 0 is not stored)."""
+    from oracle.shims import k_integrals as ki
+    d = dict(np.load(os.path.join(GOLD, "tspec_collider_nside16_t.npz")))
+    k, T, r = d["k_arr"], d["Tl_arr"], d["r_values"]
+    lmin_t, lmax_t, Lmin, Lmax, K_coll = 2, 30, 2, 40, 0.01
+    Pzeta = lambda kk: 2. * np.pi ** 2. / kk ** 3 * 2.1e-9 * (kk / 0.05) ** (0.96 - 1)
+    params = {-0.8: [[0, 0]], -1.2: [[1, 0], [1, 2]], -1.5: [[1, 0], [1, 2]], -1.5 - 0.5j: [[0, 0]],
+              -1.5 - 0.8j: [[1, 0], [1, 2]]}
+    nmax_coll, nmax_coll_F = 1, 2
+    lmax = max(lmax_t + 1, lmax_t + nmax_coll)
+    lmin = max(min(lmin_t - 1, lmin_t - nmax_coll), 0)
+    max_kr = max(k) * max(r)
+    x = np.asarray(list(np.arange(0, lmax * 2, 0.01)) + list(np.arange(lmax * 2, min(max_kr * 1.01, lmax * 100), 0.1)))
+    jlx = np.zeros((lmax - lmin + 1, len(x)))
+    ki.compute_bessel(x, lmin, lmax, jlx, 1)
+    jall = ki.interpolate_jlkr(x, k, r, jlx, 1)
+    for beta, pr in params.items():
+        nm = max(p[0] for p in pr)
+        out = np.zeros((2 * nm + 1, lmax + 1, 1, len(r)), dtype=np.complex128)
+        ki.collider_p_integral(k, Pzeta(k), T, jall, beta, K_coll, lmin_t, lmax_t, lmin, lmax, nm, 1, out)
+        ref = d["coll_plLXs_%.8f,%.8f" % (np.real(beta), np.imag(beta))]
+        assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max(), beta
+    K = np.geomspace(0.1 / (14163.032903769747 + 5000), K_coll * 1.01, 5000)
+    Lt_max, Lt_min = Lmax + nmax_coll_F, max(Lmin - nmax_coll_F, 0)
+    y = np.asarray(list(np.arange(0, Lt_max * 2, 0.01)) + list(np.arange(Lt_max * 2, K_coll * max(r) * 1.01, 0.01)))
+    jly = np.zeros((Lt_max - Lt_min + 1, len(y)))
+    ki.compute_bessel(y, Lt_min, Lt_max, jly, 1)
+    jlK = ki.interpolate_jlkr(y, K, r, jly, 1)
+    for beta, pr in params.items():
+        nF = max(p[1] for p in pr)
+        out = np.zeros((2 * nF + 1, 48, len(r), len(r)), dtype=np.complex128)
+        ki.compute_collider_F_integral(K, Pzeta(K), jlK, -2. * beta, K_coll, Lmin, Lmax, nF, nmax_coll_F, 1, out)
+        ref = d["coll_FLLs_%.8f,%.8f" % (np.real(beta), np.imag(beta))]
+        assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max(), beta
